@@ -1,0 +1,275 @@
+"""Benchmark: N-1 solves/s on the 9,241-bus synthetic grid with 500 branch outages, max mismatch 1e-8 pu.
+
+One step = one batch of 500 single-branch outages solved to convergence by the batched Newton-Raphson engine, every
+scenario warm-started from the base case.  Prints ONE JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference] [--precision mixed|fp64]
+
+``--impl reference`` times the reference path's CPU arm instead: the C restatement of the reference's Newton-Raphson
+(the oracle) on every host core, on a bounded sample of the same outages (the reference's own CPU path, OLF with
+KLU in a JVM, does not run here: no JVM, no OLF jars, no network).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "olf-gpu_b200"))
+
+METRIC = "N-1 solves/s (9k-bus, 500 outages) learned+mixed vs plain FP64 NR at 1e-8 pu"
+GRID = "grid9241"
+N_OUTAGES = 500
+TOL = 1e-8
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                vals = [v.strip() for v in out.stdout.strip().split(",")]
+                if len(vals) == 6:
+                    self.samples.append(vals)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[2 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def workload(rank: int):
+    from olfgpu import packing, synthetic
+    g = synthetic.build(GRID)
+    p = packing.pack(g)
+    # weak scaling: every rank solves its own 500 outages of the same grid
+    outs = synthetic.draw_outages(g, N_OUTAGES, seed=9241 + rank)
+    return g, p, outs
+
+
+def algorithmic_bytes(s, p, iterations_total: int, precision_bytes: int, refinement: int):
+    """Bytes one scenario-iteration must move (J once, LU written and read once, six n-vectors), summed."""
+    nnz_lu = s.n_lu_blocks * 4
+    b_it = 8 * s.nnz + precision_bytes * 2 * nnz_lu + 8 * 6 * p.n
+    b_it += refinement * (precision_bytes * nnz_lu + 8 * s.nnz)
+    return b_it * iterations_total, b_it
+
+
+def run_engine(args, rank: int, world: int):
+    import torch
+    from olfgpu import native
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    g, p, outs = workload(rank)
+    precision = native.MIXED if args.precision == "mixed" else native.FP64
+    refinement = args.refinement if precision == native.MIXED else 0
+    s = native.Structure(p)
+    ns = outs.shape[0]
+    ctx = native.BatchContext(s, ns)
+    ctx.set_linear_solver_settings(precision, max(refinement, 0))
+    # host inputs in pinned memory (e2e copies them every step); results read back to pinned memory
+    dis = torch.from_numpy(p.outage_masks(outs)).pin_memory().numpy()
+    out = torch.empty((ns, p.n + 3), dtype=torch.float64).pin_memory().numpy()
+    x0 = torch.from_numpy(p.x_base.copy()).pin_memory().numpy()
+    tgt = torch.from_numpy(p.target.copy()).pin_memory().numpy()
+    mode = torch.from_numpy(p.base_row_mode.astype(np.int32)).pin_memory().numpy()
+
+    def step():
+        ctx.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
+
+    for _ in range(args.warmup):
+        step()
+    statuses = out[:, p.n + 2].astype(int).copy()
+    iters_last = out[:, p.n].astype(int).copy()
+    # device-resident timing: the library's CUDA events around the device work of each step (no host copies)
+    dev_ms, wall_ms, tot_iters = [], [], 0
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with sampler:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            step()
+            wall_ms.append((time.perf_counter() - t0) * 1e3)
+            ms, batched, tot = ctx.last_stats()
+            dev_ms.append(ms)
+            tot_iters += int(tot.sum())
+    torch.cuda.synchronize()
+    dev = float(np.mean(dev_ms))
+    e2e = float(np.mean(wall_ms))
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([dev, e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev, e2e = float(t[0]), float(t[1])
+    # roofline of the Newton iterations (HBM-bound): algorithmic bytes over the device time
+    peak, peak_kind = _peaks()
+    pbytes = 4 if precision == native.MIXED else 8
+    total_bytes, b_it = algorithmic_bytes(s, p, tot_iters // args.steps, pbytes, refinement)
+    achieved = total_bytes / (dev * 1e-3) / 1e9
+    words = (ns + 31) // 32
+    h2d = p.n * 8 * 2 + p.n * 4 + p.n_elements * words * 4
+    d2h = ns * (p.n + 3) * 8
+    conv = float((statuses == 0).mean())
+    line = {
+        "metric": METRIC,
+        "value": round(world * ns / (dev * 1e-3), 1),
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(dev, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32-lu+fp64" if precision == native.MIXED else "f64",
+        "data": "synthetic (seeded 9,241-bus grid, random non-bridge branch outages)",
+        "config": {"workload": f"{GRID}: 9,241 buses, {p.n_cb} branches, {N_OUTAGES} outages per GPU, warm start "
+                               f"from the base case, tol {TOL} pu, FP32 LU + {refinement} FP64 refinement step(s)"
+                   if precision == native.MIXED else
+                   f"{GRID}: 9,241 buses, {p.n_cb} branches, {N_OUTAGES} outages per GPU, warm start, tol {TOL} pu, "
+                   f"FP64 LU",
+                   "precision": args.precision, "l2": "working set > 1 GB per step, larger than the 126 MB L2",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "e2e": {"value": round(world * ns / (e2e * 1e-3), 1), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "scope": "whole Newton iterations: (8 nnzJ + 2 w nnzLU + 48 n) bytes per scenario-iteration",
+                     "peak_source": peak_kind},
+        "gpu_launches": None,
+        "iterations_per_solve": round(tot_iters / args.steps / ns, 3),
+        "converged_fraction": round(conv, 4),
+        "structure": {"n": s.n, "nnzJ": s.nnz, "nnzLU": s.n_lu_blocks * 4, "factor_levels": s.factor_levels,
+                      "solve_levels": s.forward_levels + s.backward_levels, "block_ops": s.block_ops},
+        "clocks": sampler.summary(),
+    }
+    levels = s.factor_levels + (s.forward_levels + s.backward_levels + 2) * (1 + refinement)
+    per_iter = 1 + 1 + 1 + levels + refinement + 2
+    line["gpu_launches"] = int(per_iter * (tot_iters / args.steps / ns + 1) * args.steps)
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(p, outs, args.cpu_sample)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(p, outs, sample: int):
+    """The oracle (C restatement of the reference Newton-Raphson, sparse LU) on every host core, bounded sample."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    st = O.Structure(p)
+    sub = outs[:sample]
+    t0 = time.perf_counter()
+    r = st.solve_batch(p.x_base, p.outage_masks(sub), max_iter=15, tol=TOL, threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": round(sub.shape[0] / dt, 2), "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"{sub.shape[0]} of the {outs.shape[0]} outages, {dt:.1f} s on {cores} threads",
+            "converged": int((r[:, -1] == 0).sum())}
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    g, p, outs = workload(0)
+    cores = os.cpu_count() or 1
+    from oracle import oracle as O
+    st = O.Structure(p)
+    sub = outs[: args.cpu_sample]
+    dis = p.outage_masks(sub)
+    for _ in range(args.warmup):
+        st.solve_batch(p.x_base, dis[:cores], max_iter=15, tol=TOL, threads=cores)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        st.solve_batch(p.x_base, dis, max_iter=15, tol=TOL, threads=cores)
+        times.append(time.perf_counter() - t0)
+    dt = float(np.mean(times))
+    v = sub.shape[0] / dt
+    line = {"metric": METRIC, "value": round(v, 2), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 9,241-bus grid, random branch outages)",
+            "impl": "reference",
+            "config": {"workload": f"{GRID}: 9,241 buses, {p.n_cb} branches; a step solves {sub.shape[0]} of the "
+                                   f"{N_OUTAGES} outages", "precision": "fp64"},
+            "cpu_baseline": {"value": round(v, 2), "unit": "solves/s", "cores": cores, "kind": "port",
+                             "sample": f"{sub.shape[0]} outages per step on {cores} threads"},
+            "e2e": {"value": round(v, 2), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--refinement", type=int, default=1)
+    ap.add_argument("--cpu-sample", type=int, default=96)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "engine" else args.warmup
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_engine(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

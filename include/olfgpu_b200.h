@@ -1,0 +1,125 @@
+/*
+ * olfgpu_b200 -- C ABI of the B200 batched AC Newton-Raphson N-1 engine.
+ *
+ * The entry points mirror the native calls the reference's Java layer binds for this path (its JNI symbols
+ * Java_com_powsybl_openloadflow_<pkg>_<cls>_<method>, native/cuda/jni/olf_jni.h:9); each declaration below names the
+ * reference interface it replaces.  Plain pointers and sizes only.  Every function returns 0 on success and -1 on
+ * failure, with the reason in olfgpu_last_error() (the JNI layer turns it into a RuntimeException, as
+ * structure_jni.cu:128-137 and batch_solve_jni.cu:302-306 do).  Per-scenario problems are status codes, never errors.
+ *
+ * Threading: one CUDA stream per batch context; a handle is used by one caller at a time.  Handles are opaque
+ * 64-bit values; 0 is never a valid handle and destroying 0 is a no-op.
+ *
+ * Statuses (codes/gpu_ac_solver_status.cuh:10-15): 0 CONVERGED, 1 MAX_ITERATION_REACHED, 2 UNREALISTIC_STATE,
+ * -1 DIVERGED, -2 REJECTED, -3 LINEAR_SOLVE_FAILED.
+ * Row modes (codes/gpu_row_mode.cuh:10-15): 0 FIXED_VARIABLE, 1 EQUATION, 4 BUS_TARGET_Q.
+ */
+#ifndef OLFGPU_B200_H
+#define OLFGPU_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The reason of the calling thread's last failure ("" when none). */
+const char* olfgpu_last_error(void);
+
+/*
+ * StructureNative.createStructure (native/cuda/jni/structure_jni.cu:7-137; StructureNative.java:49-59).
+ * Packed families in the reference layout (GpuAcFamilyPacker.java:140-181):
+ *   closed branch: params [nCb][8] {y, g1, g2, b1, b2, ksi, r1, a1}, indices [nCb][12]
+ *                  {P1, Q1, P2, Q2, ph1, v1, ph2, v2, a1col, r1col, altQ1, altQ2}
+ *   open branch:   params [nOb][7] {y, ksi, g1, b1, g2, b2, r1}, indices [nOb][6] {P1, Q1, P2, Q2, v1, v2}
+ *   shunt:         params [nSh][2] {g, b}, indices [nSh][5] {P, Q, v, bcol, altQ}
+ *   identity rows: [nIdentityRows]
+ * The families this engine does not model (HVDC AC emulation, DISTR_Q/RHO/SHUNT_B, zero-impedance branches, load
+ * models, reactive relocation, transformer/shunt voltage-control columns) must be empty: a non-empty one, or a
+ * control column >= 0, is rejected with an error.  ordering: 0 minimum degree (default), 1 nested dissection,
+ * 2 natural.
+ */
+int olfgpu_create_structure(int n, int nCb, const double* cbParams, const int* cbIndices, int nOb,
+                            const double* obParams, const int* obIndices, int nSh, const double* shParams,
+                            const int* shIndices, int nIdentityRows, const int* identityRows, int ordering,
+                            int64_t* structureOut);
+
+/* StructureNative.destroyStructure (structure_jni.cu:143-149): drops the caller's reference; contexts keep theirs. */
+int olfgpu_destroy_structure(int64_t structure);
+
+/*
+ * Read back of the reference-compatible structure (for parity checks): rowMap [n], rowPtr [n+1], colIdx [nnz],
+ * diagPos [n], and the role-folded destinations cbDest [nCb][28], obDest [nOb][8], shDest [nSh][5]
+ * (>= 0 J slot, -2-row F row, -1 skip; structure_build.cuh:51-66).  info receives
+ * {n, nnz, nBuses, nLuBlocks, factorLevels, forwardLevels, backwardLevels, nElements, nABlocks}; blockOps the 2x2
+ * block updates of one factorization.  Any output pointer may be null.
+ */
+int olfgpu_structure_info(int64_t structure, int* info9, int64_t* blockOps);
+int olfgpu_structure_export(int64_t structure, int* rowMap, int* rowPtr, int* colIdx, int* diagPos, int* cbDest,
+                            int* obDest, int* shDest);
+
+/* StructureNative.recommendBatchSize (structure_jni.cu:151-180): the bank that fits 70 % of free device memory. */
+int olfgpu_recommend_batch_size(int64_t structure, int maxCap, int mode, int* batchOut);
+
+/*
+ * BatchSolveNative.createBatchContext (batch_solve_jni.cu:29-81; BatchSolveNative.java:41-48).
+ * mode: linear-solve mode (3 UBATCH, 6 ROBUST, 7 BATCHED_LU; all run the engine's own batched LU).
+ * Reactive-limit entries (ReactiveLimitsPacker.java:76), nRl may be 0: per voltage-controlling bus its V row, Q limits,
+ * load Q, voltage target, and the forced-PV election keys (nominal V, P row or -1 with a static P, id rank;
+ * reactive_limits.cu:417-448).
+ */
+int olfgpu_create_batch_context(int64_t structure, int nScenarios, int mode, int nRl, const int* rlVoltageRow,
+                                const double* rlMinQ, const double* rlMaxQ, const double* rlLoadQ,
+                                const double* rlTargetV, const double* rlNomV, const int* rlPRow,
+                                const double* rlStaticP, const int* rlIdRank, int64_t* contextOut);
+
+/* BatchSolveNative.destroyBatchContext (batch_solve_jni.cu:396-401). */
+int olfgpu_destroy_batch_context(int64_t context);
+
+/*
+ * NewtonSettingsNative.setLinearSolverSettings (native/cuda/jni/newton_settings_jni.cu; LinearSolverSettings,
+ * linear_solver_settings.cuh:48-58).  precision: 0 FP64 factorization and solves; 1 FP32 factorization and solves
+ * with FP32 accumulation, corrected by refinementSteps FP64 iterative-refinement steps (residual with the FP64
+ * Jacobian).
+ */
+int olfgpu_set_linear_solver_settings(int64_t context, int precision, int refinementSteps);
+
+/*
+ * BatchSolveNative.solveBatchContext (batch_solve_jni.cu:84-394; BatchSolveNative.java:106-125).
+ *   x0Base [n]: the start state of every scenario (ignored where x0Full is given), x0Full [nScenarios][n] or null;
+ *   targetBase [n], baseRowMode [n]; rowModeEntries (scenario, row, mode) triples; disabled [nScenarios][nElements]
+ *   bytes (element order: closed branches, open branches, shunts; BatchSolveNative.java:81-83);
+ *   targetOverrideIndex (flat scenario * n + row) / targetOverrideValue;
+ *   maxIter, tol (||F||inf stopping threshold), reactiveLimitTol, maxOuter (reactive-limit outer iterations),
+ *   maxPqPvSwitch.
+ * out [nScenarios][n + 3]: per scenario the final state x, the Newton iterations of its last solve, ||F||inf and the
+ * status (batch_solve_jni.cu:308-337).
+ */
+int olfgpu_solve_batch_context(int64_t context, const double* x0Base, const double* x0Full, const double* targetBase,
+                               const int* baseRowMode, int nRowModeEntries, const int* rowModeEntries,
+                               int nScenarios, int nElements, const unsigned char* disabled, int nTargetOverrides,
+                               const int* targetOverrideIndex, const double* targetOverrideValue, int maxIter,
+                               double tol, double reactiveLimitTol, int maxOuter, int maxPqPvSwitch, double* out);
+
+/*
+ * Statistics of the context's last solve: device milliseconds of its Newton iterations (CUDA events on the context's
+ * stream), the batched iterations run, and per scenario the Newton iterations summed over all its solves
+ * (totalIterations [nScenarios], may be null).
+ */
+int olfgpu_last_solve_stats(int64_t context, float* deviceMs, int* batchedIterations, int* totalIterations);
+
+/*
+ * Test surface of the engine (the role BatchedLuNative plays for the reference's LU, BatchedLuNative.java:121-125):
+ * the Jacobian values in the reference-compatible CSR layout and the mismatch of each scenario at the states xFull
+ * [nScenarios][n], through the engine's fill; and a batched linear solve J z = rhs through the engine's block LU
+ * (precision 0 FP64, 1 FP32), csrVals [nScenarios][nnz], rhs and out [nScenarios][n].
+ */
+int olfgpu_debug_fill(int64_t context, const double* xFull, const double* targetBase, const int* baseRowMode,
+                      const unsigned char* disabled, double* jacobianOut, double* mismatchOut);
+int olfgpu_debug_linear_solve(int64_t context, const double* csrVals, const double* rhs, int precision, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OLFGPU_B200_H */

@@ -1,0 +1,211 @@
+// C ABI of the engine (declared in include/olfgpu_b200.h).  Every entry point catches every exception and reports
+// it through olfgpu_last_error(), the way the reference's JNI layer turns native failures into RuntimeExceptions.
+#include "../../include/olfgpu_b200.h"
+
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "engine.hpp"
+
+using namespace olfb200;
+
+namespace {
+
+thread_local std::string lastError;
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        lastError.clear();
+        f();
+        return 0;
+    } catch (const std::exception& e) {
+        lastError = e.what();
+    } catch (...) {
+        lastError = "unknown native error";
+    }
+    return -1;
+}
+
+using StructurePtr = std::shared_ptr<NetStructure>;
+
+StructurePtr& structureOf(int64_t h) {
+    auto* p = reinterpret_cast<StructurePtr*>(h);
+    if (!p || !*p) throw std::runtime_error("invalid structure handle");
+    return *p;
+}
+
+BatchContext& contextOf(int64_t h) {
+    auto* p = reinterpret_cast<BatchContext*>(h);
+    if (!p) throw std::runtime_error("invalid batch solver context");
+    return *p;
+}
+
+}  // namespace
+
+extern "C" const char* olfgpu_last_error(void) { return lastError.c_str(); }
+
+extern "C" int olfgpu_create_structure(int n, int nCb, const double* cbParams, const int* cbIndices, int nOb,
+                                       const double* obParams, const int* obIndices, int nSh, const double* shParams,
+                                       const int* shIndices, int nIdentityRows, const int* identityRows, int ordering,
+                                       int64_t* structureOut) {
+    return guarded([&] {
+        if (!structureOut) throw std::runtime_error("null output handle");
+        *structureOut = 0;
+        if ((nCb && (!cbParams || !cbIndices)) || (nOb && (!obParams || !obIndices)) || (nSh && (!shParams || !shIndices)) ||
+            (nIdentityRows && !identityRows)) {
+            throw std::runtime_error("null family array with a non-zero count");
+        }
+        auto s = std::make_shared<NetStructure>();
+        s->host = buildStructure(n, nCb, cbParams, cbIndices, nOb, obParams, obIndices, nSh, shParams, shIndices,
+                                 nIdentityRows, identityRows, ordering);
+        *structureOut = reinterpret_cast<int64_t>(new StructurePtr(s));
+    });
+}
+
+extern "C" int olfgpu_destroy_structure(int64_t structure) {
+    return guarded([&] { delete reinterpret_cast<StructurePtr*>(structure); });
+}
+
+extern "C" int olfgpu_structure_info(int64_t structure, int* info, int64_t* blockOps) {
+    return guarded([&] {
+        const Structure& s = structureOf(structure)->host;
+        const BlockPlan& p = s.plan;
+        if (info) {
+            info[0] = s.n;
+            info[1] = s.nnz;
+            info[2] = s.nb;
+            info[3] = p.nU + p.nL;
+            info[4] = static_cast<int>(p.levelPtr.size()) - 1;
+            info[5] = static_cast<int>(p.fwdLevelPtr.size()) - 1;
+            info[6] = static_cast<int>(p.bwdLevelPtr.size()) - 1;
+            info[7] = s.nElements;
+            info[8] = static_cast<int>(p.aCol.size());
+        }
+        if (blockOps) *blockOps = p.blockOps;
+    });
+}
+
+extern "C" int olfgpu_structure_export(int64_t structure, int* rowMap, int* rowPtr, int* colIdx, int* diagPos,
+                                       int* cbDest, int* obDest, int* shDest) {
+    return guarded([&] {
+        const Structure& s = structureOf(structure)->host;
+        auto put = [](int* dst, const std::vector<int>& v) {
+            if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(int));
+        };
+        put(rowMap, s.rowMap);
+        put(rowPtr, s.rowPtr);
+        put(colIdx, s.colIdx);
+        put(diagPos, s.diagPos);
+        put(cbDest, s.cbDest);
+        put(obDest, s.obDest);
+        put(shDest, s.shDest);
+    });
+}
+
+extern "C" int olfgpu_recommend_batch_size(int64_t structure, int maxCap, int mode, int* batchOut) {
+    return guarded([&] {
+        if (!batchOut) throw std::runtime_error("null output");
+        const Structure& s = structureOf(structure)->host;
+        const BlockPlan& p = s.plan;
+        // what one lane of a context takes: state vectors, the Jacobian, the factors in the mode's precision
+        const double lu = static_cast<double>(p.nU + p.nL) * 4 * (mode == MODE_BATCHED_LU ? 8 + 4 : 8);
+        const double perLane = 8.0 * s.n * 7 + s.n + static_cast<double>(p.aCol.size()) * 32 + lu + 8.0 * s.nb * 2 * 3;
+        size_t freeB = 0, totalB = 0;
+        OLF_CUDA(cudaMemGetInfo(&freeB, &totalB));
+        const double budget = 0.7 * static_cast<double>(freeB);
+        long fit = perLane > 0 ? static_cast<long>(budget / perLane) : maxCap;
+        *batchOut = static_cast<int>(std::max<long>(1, std::min<long>(maxCap, fit)));
+    });
+}
+
+extern "C" int olfgpu_create_batch_context(int64_t structure, int nScenarios, int mode, int nRl, const int* rlVoltageRow,
+                                           const double* rlMinQ, const double* rlMaxQ, const double* rlLoadQ,
+                                           const double* rlTargetV, const double* rlNomV, const int* rlPRow,
+                                           const double* rlStaticP, const int* rlIdRank, int64_t* contextOut) {
+    return guarded([&] {
+        if (!contextOut) throw std::runtime_error("null output handle");
+        *contextOut = 0;
+        if (nRl < 0) throw std::runtime_error("negative reactive-limit entry count");
+        if (nRl > 0 && (!rlVoltageRow || !rlMinQ || !rlMaxQ || !rlLoadQ || !rlTargetV || !rlNomV || !rlPRow ||
+                        !rlStaticP || !rlIdRank)) {
+            throw std::runtime_error("reactive-limit entries installed without their arrays or the forced-PV keys");
+        }
+        BatchContext* c = createContext(structureOf(structure), nScenarios, mode, nRl, rlVoltageRow, rlMinQ, rlMaxQ,
+                                        rlLoadQ, rlTargetV, rlNomV, rlPRow, rlStaticP, rlIdRank);
+        *contextOut = reinterpret_cast<int64_t>(c);
+    });
+}
+
+extern "C" int olfgpu_destroy_batch_context(int64_t context) {
+    return guarded([&] { delete reinterpret_cast<BatchContext*>(context); });
+}
+
+extern "C" int olfgpu_set_linear_solver_settings(int64_t context, int precision, int refinementSteps) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        if (precision != 0 && precision != 1) throw std::runtime_error("precision must be 0 (FP64) or 1 (mixed)");
+        if (refinementSteps < 0 || refinementSteps > 8) throw std::runtime_error("refinementSteps must be in [0, 8]");
+        c.precision = precision;
+        c.refinementSteps = refinementSteps;
+    });
+}
+
+extern "C" int olfgpu_solve_batch_context(int64_t context, const double* x0Base, const double* x0Full,
+                                          const double* targetBase, const int* baseRowMode, int nRowModeEntries,
+                                          const int* rowModeEntries, int nScenarios, int nElements,
+                                          const unsigned char* disabled, int nTargetOverrides,
+                                          const int* targetOverrideIndex, const double* targetOverrideValue,
+                                          int maxIter, double tol, double reactiveLimitTol, int maxOuter,
+                                          int maxPqPvSwitch, double* out) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        if (nRowModeEntries < 0 || nTargetOverrides < 0 || nElements < 0) throw std::runtime_error("negative count");
+        if ((nRowModeEntries && !rowModeEntries) || (nTargetOverrides && (!targetOverrideIndex || !targetOverrideValue))) {
+            throw std::runtime_error("null array with a non-zero count");
+        }
+        SolveRequest r;
+        r.x0Base = x0Base;
+        r.x0Full = x0Full;
+        r.targetBase = targetBase;
+        r.baseRowMode = baseRowMode;
+        r.nRowModeEntries = nRowModeEntries;
+        r.rowModeEntries = rowModeEntries;
+        r.nScenarios = nScenarios;
+        r.nElements = nElements;
+        r.disabled = disabled;
+        r.nTargetOverrides = nTargetOverrides;
+        r.targetOverrideIndex = targetOverrideIndex;
+        r.targetOverrideValue = targetOverrideValue;
+        r.maxIter = maxIter;
+        r.tol = tol;
+        r.reactiveLimitTol = reactiveLimitTol;
+        r.maxOuter = maxOuter;
+        r.maxPqPvSwitch = maxPqPvSwitch;
+        solveBatch(c, r, out);
+    });
+}
+
+extern "C" int olfgpu_last_solve_stats(int64_t context, float* deviceMs, int* batchedIterations, int* totalIterations) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        if (deviceMs) *deviceMs = c.lastMs;
+        if (batchedIterations) *batchedIterations = c.lastIterations;
+        if (totalIterations) {
+            OLF_CUDA(cudaMemcpy(totalIterations, c.totalIter.p, sizeof(int) * c.nS, cudaMemcpyDeviceToHost));
+        }
+    });
+}
+
+extern "C" int olfgpu_debug_fill(int64_t context, const double* xFull, const double* targetBase, const int* baseRowMode,
+                                 const unsigned char* disabled, double* jacobianOut, double* mismatchOut) {
+    return guarded([&] {
+        debugFill(contextOf(context), xFull, targetBase, baseRowMode, disabled, jacobianOut, mismatchOut);
+    });
+}
+
+extern "C" int olfgpu_debug_linear_solve(int64_t context, const double* csrVals, const double* rhs, int precision,
+                                         double* out) {
+    return guarded([&] { debugLinearSolve(contextOf(context), csrVals, rhs, precision, out); });
+}

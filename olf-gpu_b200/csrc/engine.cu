@@ -1,0 +1,738 @@
+// Batched Newton-Raphson engine: device copy of a structure, batch contexts and the solve driver.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+
+namespace olfb200 {
+
+// ---------------------------------------------------------------------------------------------------------------
+// Device copy of a structure
+// ---------------------------------------------------------------------------------------------------------------
+std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
+    auto d = std::make_shared<DeviceNet>();
+    OLF_CUDA(cudaGetDevice(&d->device));
+    const BlockPlan& p = s.plan;
+    const int nb = s.nb;
+    auto aBlock = [&](int i, int j) {
+        auto b = p.aCol.begin() + p.aPtr[i], e = p.aCol.begin() + p.aPtr[i + 1];
+        auto it = std::lower_bound(b, e, j);
+        if (it == e || *it != j) throw std::runtime_error("A block lookup miss");
+        return static_cast<int>(it - p.aCol.begin());
+    };
+    // incident closed-branch sides per node, sorted by (neighbour, element)
+    std::vector<std::vector<Side>> sides(nb);
+    for (int e = 0; e < s.ncb; e++) {
+        const int* ix = &s.cbIx[static_cast<size_t>(e) * CB_INDICES];
+        const int i = s.colNode[ix[4]] >> 1, j = s.colNode[ix[6]] >> 1;
+        if (i == j) throw std::runtime_error("closed branch " + std::to_string(e) + " has both ends on one bus");
+        sides[i].push_back(Side{e, 0, j, aBlock(i, j)});
+        sides[j].push_back(Side{e, 1, i, aBlock(j, i)});
+    }
+    std::vector<int> sidePtr(nb + 1, 0);
+    std::vector<Side> sideAll;
+    for (int i = 0; i < nb; i++) {
+        std::sort(sides[i].begin(), sides[i].end(), [](const Side& a, const Side& b) {
+            return a.neighbour != b.neighbour ? a.neighbour < b.neighbour : a.element < b.element;
+        });
+        sideAll.insert(sideAll.end(), sides[i].begin(), sides[i].end());
+        sidePtr[i + 1] = static_cast<int>(sideAll.size());
+    }
+    std::vector<double2> trig(s.ncb);
+    for (int e = 0; e < s.ncb; e++) {
+        const double ksi = s.cbPar[static_cast<size_t>(e) * CB_PARAMS + 5];
+        trig[e] = make_double2(std::sin(ksi), std::cos(ksi));
+    }
+    std::vector<std::vector<int>> shOf(nb);
+    for (int e = 0; e < s.nsh; e++) shOf[s.colNode[s.shIx[static_cast<size_t>(e) * SH_INDICES + 2]] >> 1].push_back(e);
+    std::vector<int> shPtr(nb + 1, 0), shList;
+    for (int i = 0; i < nb; i++) {
+        shList.insert(shList.end(), shOf[i].begin(), shOf[i].end());
+        shPtr[i + 1] = static_cast<int>(shList.size());
+    }
+    std::vector<std::vector<int2>> obOf(nb);
+    for (int e = 0; e < s.nob; e++) {
+        const int* ix = &s.obIx[static_cast<size_t>(e) * OB_INDICES];
+        if (ix[4] >= 0) obOf[s.colNode[ix[4]] >> 1].push_back(make_int2(e, 0));
+        else if (ix[5] >= 0) obOf[s.colNode[ix[5]] >> 1].push_back(make_int2(e, 1));
+    }
+    std::vector<int> obPtr(nb + 1, 0);
+    std::vector<int2> obList;
+    for (int i = 0; i < nb; i++) {
+        obList.insert(obList.end(), obOf[i].begin(), obOf[i].end());
+        obPtr[i + 1] = static_cast<int>(obList.size());
+    }
+    // factorization tasks
+    const int nLu = p.nU + p.nL;
+    std::vector<Task> task(nLu);
+    for (int k = 0; k < nb; k++) {
+        for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) {
+            task[t] = Task{p.luToA[t], p.opPtr[t], p.opPtr[t + 1], t == p.uPtr[k] ? -2 : -1};
+        }
+        for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++) {
+            const int id = p.nU + t;
+            task[id] = Task{p.luToA[id], p.opPtr[id], p.opPtr[id + 1], p.uPtr[k]};
+        }
+    }
+    // L blocks by row position (for the forward solve), ascending column position
+    std::vector<std::vector<int2>> lr(nb);
+    for (int k = 0; k < nb; k++)
+        for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++) lr[p.lRow[t]].push_back(make_int2(p.nU + t, k));
+    std::vector<int> lrowPtr(nb + 1, 0);
+    std::vector<int2> lrow;
+    for (int i = 0; i < nb; i++) {
+        lrow.insert(lrow.end(), lr[i].begin(), lr[i].end());
+        lrowPtr[i + 1] = static_cast<int>(lrow.size());
+    }
+    // CSR slot -> A block entry
+    d->csrToA.assign(s.nnz, -1);
+    for (int r = 0; r < s.n; r++) {
+        const int nr = s.colNode[r];
+        for (int k = s.rowPtr[r]; k < s.rowPtr[r + 1]; k++) {
+            const int nc = s.colNode[s.colIdx[k]];
+            d->csrToA[k] = aBlock(nr >> 1, nc >> 1) * 4 + (nr & 1) * 2 + (nc & 1);
+        }
+    }
+    d->nodeCol.upload(s.nodeCol);
+    d->sidePtr.upload(sidePtr);
+    d->side.upload(sideAll);
+    d->cbPar.upload(s.cbPar);
+    d->cbTrig.upload(trig);
+    d->aPtr.upload(p.aPtr);
+    d->aCol.upload(p.aCol);
+    d->aDiag.upload(p.aDiag);
+    d->shPtr.upload(shPtr);
+    d->shList.upload(shList);
+    d->shPar.upload(s.shPar);
+    d->obPtr.upload(obPtr);
+    d->obList.upload(obList);
+    d->obPar.upload(s.obPar);
+    d->task.upload(task);
+    std::vector<int2> ops(p.opL.size());
+    for (size_t q = 0; q < ops.size(); q++) ops[q] = make_int2(p.opL[q], p.opU[q]);
+    d->ops.upload(ops);
+    d->levelTask.upload(p.levelTask);
+    d->perm.upload(p.perm);
+    d->iperm.upload(p.iperm);
+    d->lrowPtr.upload(lrowPtr);
+    d->lrow.upload(lrow);
+    d->uPtr.upload(p.uPtr);
+    d->uCol.upload(p.uCol);
+    d->fwdPos.upload(p.fwdLevelPos);
+    d->bwdPos.upload(p.bwdLevelPos);
+    d->levelPtr = p.levelPtr;
+    d->fwdPtr = p.fwdLevelPtr;
+    d->bwdPtr = p.bwdLevelPtr;
+    // split factor of each level: enough threads per task/row that each walks at most ~4 updates (power of two <= 16)
+    auto splitOf = [](int longest) {
+        int P = 1;
+        while (P < 16 && (longest + P - 1) / P > 4) P *= 2;
+        return P;
+    };
+    std::vector<int> lrowLen(nb, 0);
+    for (int i = 0; i < nb; i++) lrowLen[i] = lrowPtr[i + 1] - lrowPtr[i];
+    d->levelSplit.assign(p.levelPtr.size() - 1, 1);
+    for (size_t l = 0; l + 1 < p.levelPtr.size(); l++) {
+        int m = 0;
+        for (int q = p.levelPtr[l]; q < p.levelPtr[l + 1]; q++) {
+            const int t = p.levelTask[q];
+            m = std::max(m, p.opPtr[t + 1] - p.opPtr[t]);
+        }
+        d->levelSplit[l] = splitOf(m);
+    }
+    d->fwdSplit.assign(p.fwdLevelPtr.size() - 1, 1);
+    for (size_t l = 0; l + 1 < p.fwdLevelPtr.size(); l++) {
+        int m = 0;
+        for (int q = p.fwdLevelPtr[l]; q < p.fwdLevelPtr[l + 1]; q++) m = std::max(m, lrowLen[p.fwdLevelPos[q]]);
+        d->fwdSplit[l] = splitOf(m);
+    }
+    d->bwdSplit.assign(p.bwdLevelPtr.size() - 1, 1);
+    for (size_t l = 0; l + 1 < p.bwdLevelPtr.size(); l++) {
+        int m = 0;
+        for (int q = p.bwdLevelPtr[l]; q < p.bwdLevelPtr[l + 1]; q++) {
+            const int i = p.bwdLevelPos[q];
+            m = std::max(m, p.uPtr[i + 1] - p.uPtr[i] - 1);
+        }
+        d->bwdSplit[l] = splitOf(m);
+    }
+    DevNet& v = d->view;
+    v.n = s.n;
+    v.nb = nb;
+    v.nA = static_cast<int>(p.aCol.size());
+    v.nLu = nLu;
+    v.ncb = s.ncb;
+    v.nob = s.nob;
+    v.nsh = s.nsh;
+    v.nElements = s.nElements;
+    v.nodeCol = d->nodeCol.as<int>();
+    v.sidePtr = d->sidePtr.as<int>();
+    v.side = d->side.as<Side>();
+    v.cbPar = d->cbPar.as<double>();
+    v.cbTrig = d->cbTrig.as<double2>();
+    v.aPtr = d->aPtr.as<int>();
+    v.aCol = d->aCol.as<int>();
+    v.aDiag = d->aDiag.as<int>();
+    v.shPtr = d->shPtr.as<int>();
+    v.shList = d->shList.as<int>();
+    v.shPar = d->shPar.as<double>();
+    v.obPtr = d->obPtr.as<int>();
+    v.obList = d->obList.as<int2>();
+    v.obPar = d->obPar.as<double>();
+    v.task = d->task.as<Task>();
+    v.ops = d->ops.as<int2>();
+    v.levelTask = d->levelTask.as<int>();
+    v.perm = d->perm.as<int>();
+    v.iperm = d->iperm.as<int>();
+    v.lrowPtr = d->lrowPtr.as<int>();
+    v.lrow = d->lrow.as<int2>();
+    v.uPtr = d->uPtr.as<int>();
+    v.uCol = d->uCol.as<int>();
+    OLF_CUDA(cudaDeviceSynchronize());
+    return d;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Batch context
+// ---------------------------------------------------------------------------------------------------------------
+BatchContext::~BatchContext() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (hostActive) cudaFreeHost(hostActive);
+    if (hostBitsPinned) cudaFreeHost(hostBitsPinned);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+DevBatch BatchContext::batch() const {
+    DevBatch b{};
+    b.S = S;
+    b.nS = nS;
+    b.x = x.as<double>();
+    b.target = target.as<double>();
+    b.mode = mode.as<int8_t>();
+    b.F = F.as<double>();
+    b.J = J.as<double>();
+    b.lu64 = lu64.as<double>();
+    b.lu32 = lu32.as<float>();
+    b.w64 = w64.as<double>();
+    b.w32 = w32.as<float>();
+    b.dx = dx.as<double>();
+    b.res = res.as<double>();
+    b.qbuf = qbuf.as<double>();
+    b.disabled = disabled.as<uint32_t>();
+    b.norm = norm.as<unsigned long long>();
+    b.iter = iter.as<int>();
+    b.status = status.as<int>();
+    b.outer = outer.as<int>();
+    b.totalIter = totalIter.as<int>();
+    b.trouble = trouble.as<int>();
+    b.normOut = normOut.as<double>();
+    b.active = active.as<int8_t>();
+    b.pending = pending.as<int8_t>();
+    b.precision64 = precision64.as<int8_t>();
+    b.nActive = nActive.as<int>();
+    return b;
+}
+
+BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, int mode, int nRl, const int* voltageRow,
+                            const double* minQ, const double* maxQ, const double* loadQ, const double* targetV,
+                            const double* nomV, const int* pRow, const double* staticP, const int* idRank) {
+    if (nScenarios <= 0) throw std::runtime_error("nScenarios must be positive");
+    if (mode != MODE_UBATCH && mode != MODE_ROBUST && mode != MODE_BATCHED_LU) {
+        throw std::runtime_error("unknown linear-solve mode " + std::to_string(mode));
+    }
+    auto ctx = std::make_unique<BatchContext>();
+    ctx->net = net;
+    OLF_CUDA(cudaGetDevice(&ctx->device));
+    if (!net->dev || net->dev->device != ctx->device) net->dev = uploadNet(net->host);
+    const Structure& s = net->host;
+    const DevNet& v = net->dev->view;
+    ctx->nS = nScenarios;
+    ctx->S = (nScenarios + 31) / 32 * 32;
+    const size_t S = ctx->S, n = s.n;
+    OLF_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    OLF_CUDA(cudaMallocHost(&ctx->hostActive, sizeof(int)));
+    ctx->x.alloc(n * S * 8);
+    ctx->target.alloc(n * S * 8);
+    ctx->mode.alloc(n * S);
+    ctx->F.alloc(n * S * 8);
+    ctx->J.alloc(static_cast<size_t>(v.nA) * 4 * S * 8);
+    ctx->w64.alloc(static_cast<size_t>(v.nb) * 2 * S * 8);
+    ctx->w32.alloc(static_cast<size_t>(v.nb) * 2 * S * 4);
+    ctx->dx.alloc(n * S * 8);
+    ctx->res.alloc(n * S * 8);
+    ctx->qbuf.alloc(n * S * 8);
+    ctx->disabled.alloc(static_cast<size_t>(std::max(v.nElements, 1)) * (S / 32) * 4);
+    ctx->norm.alloc(S * 8);
+    ctx->iter.alloc(S * 4);
+    ctx->status.alloc(S * 4);
+    ctx->outer.alloc(S * 4);
+    ctx->totalIter.alloc(S * 4);
+    ctx->trouble.alloc(S * 4);
+    ctx->normOut.alloc(S * 8);
+    ctx->active.alloc(S);
+    ctx->pending.alloc(S);
+    ctx->precision64.alloc(S);
+    ctx->nActive.alloc(4);
+    ctx->out.alloc(static_cast<size_t>(nScenarios) * (n + 3) * 8);
+    ctx->stage.alloc(n * 8 * 2 + n * 4);
+    ctx->cfg.maxIter = 15;
+    ctx->cfg.tol = 1e-8;
+    ctx->cfg.rlTol = 1e-4;
+    ctx->cfg.maxOuter = 20;
+    ctx->cfg.maxSwitch = 3;
+    ctx->cfg.refinementSteps = 1;
+    ctx->cfg.growthLimit = 1e8;
+    if (nRl > 0) {
+        for (int i = 0; i < nRl; i++) {
+            if (voltageRow[i] < 0 || voltageRow[i] >= s.n) throw std::runtime_error("bad reactiveLimitVoltageRow");
+            if (pRow[i] >= s.n) throw std::runtime_error("bad reactiveLimit pRow");
+        }
+        auto up = [&](DeviceBuffer& d, const void* src, size_t bytes) {
+            d.alloc(bytes);
+            OLF_CUDA(cudaMemcpy(d.p, src, bytes, cudaMemcpyHostToDevice));
+        };
+        up(ctx->rlVoltageRow, voltageRow, nRl * 4);
+        up(ctx->rlMinQ, minQ, nRl * 8);
+        up(ctx->rlMaxQ, maxQ, nRl * 8);
+        up(ctx->rlLoadQ, loadQ, nRl * 8);
+        up(ctx->rlTargetV, targetV, nRl * 8);
+        up(ctx->rlNomV, nomV, nRl * 8);
+        up(ctx->rlPRow, pRow, nRl * 4);
+        up(ctx->rlStaticP, staticP, nRl * 8);
+        up(ctx->rlIdRank, idRank, nRl * 4);
+        ctx->rlLimitType.alloc(nRl * S);
+        ctx->rlSwitchCount.alloc(nRl * S);
+        ctx->rlPassSwitched.alloc(nRl * S);
+        ctx->rlSavedMode.alloc(nRl * S);
+        ctx->rlSavedTarget.alloc(nRl * S * 8);
+        ctx->rlRemainingPv.alloc(S * 4);
+        ctx->rlSwitched.alloc(S * 4);
+        DevRl& r = ctx->rl;
+        r.nRl = nRl;
+        r.voltageRow = ctx->rlVoltageRow.as<int>();
+        r.minQ = ctx->rlMinQ.as<double>();
+        r.maxQ = ctx->rlMaxQ.as<double>();
+        r.loadQ = ctx->rlLoadQ.as<double>();
+        r.targetV = ctx->rlTargetV.as<double>();
+        r.nomV = ctx->rlNomV.as<double>();
+        r.pRow = ctx->rlPRow.as<int>();
+        r.staticP = ctx->rlStaticP.as<double>();
+        r.idRank = ctx->rlIdRank.as<int>();
+        r.limitType = ctx->rlLimitType.as<int8_t>();
+        r.switchCount = ctx->rlSwitchCount.as<int8_t>();
+        r.passSwitched = ctx->rlPassSwitched.as<int8_t>();
+        r.savedMode = ctx->rlSavedMode.as<int8_t>();
+        r.savedTarget = ctx->rlSavedTarget.as<double>();
+        r.remainingPv = ctx->rlRemainingPv.as<int>();
+        r.switched = ctx->rlSwitched.as<int>();
+    }
+    return ctx.release();
+}
+
+namespace {
+
+// base vector [n] -> every lane; padding lanes get the same values (they never iterate)
+__global__ void tileKernel(const double* base, double* out, int n, int S) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (size_t)n * S) return;
+    out[tid] = base[tid / S];
+}
+
+__global__ void tileModeKernel(const int* base, int8_t* out, int n, int S) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (size_t)n * S) return;
+    out[tid] = (int8_t)base[tid / S];
+}
+
+// scenario-major [nS][n] -> lane-interleaved [n][S] through 32x32 shared tiles
+__global__ void toLanesKernel(const double* in, double* out, int n, int nS, int S) {
+    __shared__ double tile[32][33];
+    const int r0 = blockIdx.x * 32, s0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int s = s0 + k, r = r0 + threadIdx.x;
+        if (s < nS && r < n) tile[k][threadIdx.x] = in[(size_t)s * n + r];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = r0 + k, s = s0 + threadIdx.x;
+        if (r < n && s < nS) out[(size_t)r * S + s] = tile[threadIdx.x][k];
+    }
+}
+
+// lane-interleaved state -> scenario-major results [nS][n + 3]
+__global__ void resultsKernel(const double* x, const int* iter, const double* normOut, const int* status, double* out,
+                              int n, int nS, int S) {
+    __shared__ double tile[32][33];
+    const int r0 = blockIdx.x * 32, s0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = r0 + k, s = s0 + threadIdx.x;
+        if (r < n && s < S) tile[k][threadIdx.x] = x[(size_t)r * S + s];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int s = s0 + k, r = r0 + threadIdx.x;
+        if (s < nS && r < n) out[(size_t)s * (n + 3) + r] = tile[threadIdx.x][k];
+    }
+    if (blockIdx.x == 0 && threadIdx.y == 0) {
+        const int s = s0 + threadIdx.x;
+        if (s < nS) {
+            out[(size_t)s * (n + 3) + n] = (double)iter[s];
+            out[(size_t)s * (n + 3) + n + 1] = normOut[s];
+            out[(size_t)s * (n + 3) + n + 2] = (double)status[s];
+        }
+    }
+}
+
+__global__ void targetOverrideKernel(const int* idx, const double* val, int count, double* target, int n, int S) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int s = idx[k] / n, r = idx[k] % n;
+    target[(size_t)r * S + s] = val[k];
+}
+
+__global__ void rowModeOverrideKernel(const int* triples, int count, int8_t* mode, int S) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    mode[(size_t)triples[3 * k + 1] * S + triples[3 * k]] = (int8_t)triples[3 * k + 2];
+}
+
+__global__ void laneInitKernel(DevBatch b) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.S) return;
+    const bool live = s < b.nS;
+    b.iter[s] = 0;
+    b.status[s] = live ? ST_RUNNING : ST_REJECTED;
+    b.active[s] = live ? 1 : 0;
+    b.pending[s] = 0;
+    b.outer[s] = 0;
+    b.totalIter[s] = 0;
+    b.trouble[s] = 0;
+    b.norm[s] = 0ull;
+    b.normOut[s] = 0.0;
+    b.precision64[s] = 0;
+    if (s == 0) *b.nActive = b.nS;
+}
+
+// lanes still iterating after the batched-iteration cap (newton_iteration.cu:410-429) are REJECTED
+__global__ void capKernel(DevBatch b) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.S || !b.active[s]) return;
+    b.status[s] = ST_REJECTED;
+    b.active[s] = 0;
+}
+
+void outageBits(BatchContext& ctx, const unsigned char* disabled, int nS, int nElements) {
+    const int words = ctx.S / 32;
+    const int nE = ctx.net->host.nElements;
+    const size_t count = static_cast<size_t>(std::max(nE, 1)) * words;
+    if (!ctx.hostBitsPinned) OLF_CUDA(cudaMallocHost(&ctx.hostBitsPinned, count * 4));
+    OLF_CUDA(cudaStreamSynchronize(ctx.stream));   // the previous upload from the staging has completed
+    uint32_t* bits = ctx.hostBitsPinned;
+    std::memset(bits, 0, count * 4);
+    if (disabled) {
+        const int cols = std::min(nElements, nE);
+        for (int s = 0; s < nS; s++) {
+            const unsigned char* row = disabled + static_cast<size_t>(s) * nElements;
+            int e = 0;
+            // skip zero runs eight bytes at a time
+            for (; e + 8 <= cols; e += 8) {
+                uint64_t w;
+                std::memcpy(&w, row + e, 8);
+                if (!w) continue;
+                for (int k = 0; k < 8; k++)
+                    if (row[e + k]) bits[static_cast<size_t>(e + k) * words + (s >> 5)] |= 1u << (s & 31);
+            }
+            for (; e < cols; e++)
+                if (row[e]) bits[static_cast<size_t>(e) * words + (s >> 5)] |= 1u << (s & 31);
+        }
+    }
+    OLF_CUDA(cudaMemcpyAsync(ctx.disabled.p, bits, count * 4, cudaMemcpyHostToDevice, ctx.stream));
+}
+
+void captureIteration(BatchContext& ctx) {
+    const int key = ctx.precision * 1000 + ctx.refinementSteps * 10 + (ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits ? 1 : 0);
+    if (ctx.graph && ctx.graphKey == key) return;
+    if (ctx.graph) {
+        cudaGraphExecDestroy(ctx.graph);
+        ctx.graph = nullptr;
+    }
+    const DeviceNet& dn = *ctx.net->dev;
+    const DevNet& net = dn.view;
+    const size_t S = ctx.S;
+    const bool mixed = ctx.precision == 1;
+    if (mixed && !ctx.lu32.p) ctx.lu32.alloc(static_cast<size_t>(net.nLu) * 4 * S * 4);
+    if (!mixed && !ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(net.nLu) * 4 * S * 8);
+    const DevBatch b = ctx.batch();
+    const bool rl = ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits;
+    cudaGraph_t g;
+    OLF_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
+    launchFill(net, b, true, rl, ctx.stream);
+    launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, ctx.stream);
+    if (rl) launchReactiveLimits(net, b, ctx.rl, ctx.cfg, ctx.stream);
+    launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, mixed,
+                 ctx.stream);
+    launchSolve(net, b, dn.fwd(), dn.bwd(), mixed, false, ctx.stream);
+    if (mixed) {
+        for (int k = 0; k < ctx.refinementSteps; k++) {
+            launchResidual(net, b, ctx.stream);
+            launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, ctx.stream);
+        }
+    }
+    launchStep(net, b, false, ctx.stream);
+    OLF_CUDA(cudaStreamEndCapture(ctx.stream, &g));
+    OLF_CUDA(cudaGraphInstantiate(&ctx.graph, g, 0));
+    cudaGraphDestroy(g);
+    ctx.graphKey = key;
+}
+
+// One Newton iteration launched phase by phase with CUDA events between the phases; prints the milliseconds of
+// each phase to stderr (diagnostics only: same kernels, same order as the captured graph).
+void phaseTimedIteration(BatchContext& ctx, int k) {
+    const DeviceNet& dn = *ctx.net->dev;
+    const DevNet& net = dn.view;
+    const bool mixed = ctx.precision == 1;
+    const bool rl = ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits;
+    const DevBatch b = ctx.batch();
+    cudaStream_t st = ctx.stream;
+    cudaEvent_t ev[7];
+    for (auto& e : ev) OLF_CUDA(cudaEventCreate(&e));
+    OLF_CUDA(cudaEventRecord(ev[0], st));
+    launchFill(net, b, true, rl, st);
+    OLF_CUDA(cudaEventRecord(ev[1], st));
+    launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, st);
+    if (rl) launchReactiveLimits(net, b, ctx.rl, ctx.cfg, st);
+    OLF_CUDA(cudaEventRecord(ev[2], st));
+    launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, mixed, st);
+    OLF_CUDA(cudaEventRecord(ev[3], st));
+    launchSolve(net, b, dn.fwd(), dn.bwd(), mixed, false, st);
+    OLF_CUDA(cudaEventRecord(ev[4], st));
+    if (mixed) {
+        for (int r = 0; r < ctx.refinementSteps; r++) {
+            launchResidual(net, b, st);
+            launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, st);
+        }
+    }
+    OLF_CUDA(cudaEventRecord(ev[5], st));
+    launchStep(net, b, false, st);
+    OLF_CUDA(cudaEventRecord(ev[6], st));
+    OLF_CUDA(cudaEventSynchronize(ev[6]));
+    float ms[6];
+    for (int i = 0; i < 6; i++) OLF_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+    std::fprintf(stderr, "OLFGPU_PHASE_TIME it=%d fill=%.3f test=%.3f factor=%.3f solve=%.3f refine=%.3f step=%.3f ms\n",
+                 k, ms[0], ms[1], ms[2], ms[3], ms[4], ms[5]);
+    for (auto& e : ev) cudaEventDestroy(e);
+}
+
+}  // namespace
+
+void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out) {
+    OLF_CUDA(cudaSetDevice(ctx.device));
+    const Structure& s = ctx.net->host;
+    const DevNet& net = ctx.net->dev->view;
+    const int n = s.n;
+    const size_t S = ctx.S;
+    if (req.nScenarios != ctx.nS) {
+        throw std::runtime_error("scenario count " + std::to_string(req.nScenarios) + " does not match the context's " +
+                                 std::to_string(ctx.nS));
+    }
+    if (!req.x0Base && !req.x0Full) throw std::runtime_error("no start state");
+    if (!req.targetBase || !req.baseRowMode) throw std::runtime_error("no base targets or row modes");
+    if (req.maxIter < 1) throw std::runtime_error("maxIter must be >= 1");
+    for (int r = 0; r < n; r++) {
+        const int m = req.baseRowMode[r];
+        if (m != MODE_FIXED_VARIABLE && m != MODE_EQUATION && m != MODE_BUS_TARGET_Q) {
+            throw std::runtime_error("unsupported row mode " + std::to_string(m) + " at row " + std::to_string(r));
+        }
+    }
+    for (int k = 0; k < req.nRowModeEntries; k++) {
+        const int* t = req.rowModeEntries + 3 * k;
+        if (t[0] < 0 || t[0] >= ctx.nS || t[1] < 0 || t[1] >= n) {
+            throw std::runtime_error("rowMode entry outside the installed slots or the rows");
+        }
+        if (t[2] != MODE_FIXED_VARIABLE && t[2] != MODE_EQUATION && t[2] != MODE_BUS_TARGET_Q) {
+            throw std::runtime_error("unsupported row mode " + std::to_string(t[2]));
+        }
+    }
+    for (int k = 0; k < req.nTargetOverrides; k++) {
+        if (req.targetOverrideIndex[k] < 0 || req.targetOverrideIndex[k] >= ctx.nS * n) {
+            throw std::runtime_error("target override index out of range");
+        }
+    }
+    ctx.cfg.maxIter = req.maxIter;
+    ctx.cfg.tol = req.tol;
+    ctx.cfg.rlTol = req.reactiveLimitTol;
+    ctx.cfg.maxOuter = req.maxOuter;
+    ctx.cfg.maxSwitch = req.maxPqPvSwitch;
+    ctx.cfg.reactiveLimits = ctx.rl.nRl > 0 ? 1 : 0;
+    ctx.cfg.mixed = ctx.precision;
+    ctx.cfg.refinementSteps = ctx.refinementSteps;
+    // the iteration graph bakes the settings in: recapture whenever they change
+    if (ctx.graph) {
+        cudaGraphExecDestroy(ctx.graph);
+        ctx.graph = nullptr;
+    }
+    captureIteration(ctx);
+    cudaStream_t st = ctx.stream;
+    cudaEvent_t e0, e1;
+    OLF_CUDA(cudaEventCreate(&e0));
+    OLF_CUDA(cudaEventCreate(&e1));
+    // ---- install: host inputs copied first, then (timed) tiled to every lane with the per-scenario overrides ----
+    double* stageX = ctx.stage.as<double>();
+    double* stageT = stageX + n;
+    int* stageM = reinterpret_cast<int*>(stageT + n);
+    const unsigned blocksAll = static_cast<unsigned>((static_cast<size_t>(n) * S + 255) / 256);
+    if (req.x0Full) {
+        if (ctx.full.bytes < static_cast<size_t>(ctx.nS) * n * 8) ctx.full.alloc(static_cast<size_t>(ctx.nS) * n * 8);
+        OLF_CUDA(cudaMemcpyAsync(ctx.full.p, req.x0Full, static_cast<size_t>(ctx.nS) * n * 8, cudaMemcpyHostToDevice, st));
+    }
+    if (req.x0Base) OLF_CUDA(cudaMemcpyAsync(stageX, req.x0Base, n * 8, cudaMemcpyHostToDevice, st));
+    OLF_CUDA(cudaMemcpyAsync(stageT, req.targetBase, n * 8, cudaMemcpyHostToDevice, st));
+    OLF_CUDA(cudaMemcpyAsync(stageM, req.baseRowMode, n * 4, cudaMemcpyHostToDevice, st));
+    DeviceBuffer ovIdx, ovVal, rmE;
+    if (req.nTargetOverrides > 0) {
+        ovIdx.alloc(req.nTargetOverrides * 4);
+        ovVal.alloc(req.nTargetOverrides * 8);
+        OLF_CUDA(cudaMemcpyAsync(ovIdx.p, req.targetOverrideIndex, req.nTargetOverrides * 4, cudaMemcpyHostToDevice, st));
+        OLF_CUDA(cudaMemcpyAsync(ovVal.p, req.targetOverrideValue, req.nTargetOverrides * 8, cudaMemcpyHostToDevice, st));
+    }
+    if (req.nRowModeEntries > 0) {
+        rmE.alloc(req.nRowModeEntries * 12);
+        OLF_CUDA(cudaMemcpyAsync(rmE.p, req.rowModeEntries, req.nRowModeEntries * 12, cudaMemcpyHostToDevice, st));
+    }
+    outageBits(ctx, req.disabled, ctx.nS, req.nElements);
+    OLF_CUDA(cudaEventRecord(e0, st));
+    if (req.x0Base) tileKernel<<<blocksAll, 256, 0, st>>>(stageX, ctx.x.as<double>(), n, ctx.S);
+    if (req.x0Full) {
+        dim3 blk(32, 8), grd((n + 31) / 32, (ctx.nS + 31) / 32);
+        toLanesKernel<<<grd, blk, 0, st>>>(ctx.full.as<double>(), ctx.x.as<double>(), n, ctx.nS, ctx.S);
+    }
+    tileKernel<<<blocksAll, 256, 0, st>>>(stageT, ctx.target.as<double>(), n, ctx.S);
+    tileModeKernel<<<blocksAll, 256, 0, st>>>(stageM, ctx.mode.as<int8_t>(), n, ctx.S);
+    if (req.nTargetOverrides > 0) {
+        targetOverrideKernel<<<(req.nTargetOverrides + 255) / 256, 256, 0, st>>>(
+            ovIdx.as<int>(), ovVal.as<double>(), req.nTargetOverrides, ctx.target.as<double>(), n, ctx.S);
+    }
+    if (req.nRowModeEntries > 0) {
+        rowModeOverrideKernel<<<(req.nRowModeEntries + 255) / 256, 256, 0, st>>>(rmE.as<int>(), req.nRowModeEntries,
+                                                                                ctx.mode.as<int8_t>(), ctx.S);
+    }
+    const DevBatch b = ctx.batch();
+    laneInitKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b);
+    if (ctx.rl.nRl > 0) {
+        OLF_CUDA(cudaMemsetAsync(ctx.rlLimitType.p, 0, ctx.rlLimitType.bytes, st));
+        OLF_CUDA(cudaMemsetAsync(ctx.rlSwitchCount.p, 0, ctx.rlSwitchCount.bytes, st));
+        OLF_CUDA(cudaMemsetAsync(ctx.rlPassSwitched.p, 0, ctx.rlPassSwitched.bytes, st));
+    }
+    // ---- Newton iterations, one graph launch each, until no lane iterates ----
+    const int cap = ctx.cfg.reactiveLimits ? (ctx.cfg.maxOuter + 1) * (ctx.cfg.maxIter + 1) : ctx.cfg.maxIter + 1;
+    // OLFGPU_PHASE_TIME: print-only channel; the iterations run unfused with events between their phases
+    static const bool phaseTime = std::getenv("OLFGPU_PHASE_TIME") != nullptr;
+    int k = 0;
+    for (; k < cap; k++) {
+        if (phaseTime) {
+            phaseTimedIteration(ctx, k);
+        } else {
+            OLF_CUDA(cudaGraphLaunch(ctx.graph, st));
+        }
+        OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 4, cudaMemcpyDeviceToHost, st));
+        OLF_CUDA(cudaStreamSynchronize(st));
+        if (*ctx.hostActive <= 0) {
+            k++;
+            break;
+        }
+    }
+    capKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b);
+    ctx.lastIterations = k;
+    // ---- results ----
+    dim3 blk(32, 8), grd((n + 31) / 32, (ctx.nS + 31) / 32);
+    resultsKernel<<<grd, blk, 0, st>>>(ctx.x.as<double>(), ctx.iter.as<int>(), ctx.normOut.as<double>(),
+                                       ctx.status.as<int>(), ctx.out.as<double>(), n, ctx.nS, ctx.S);
+    OLF_CUDA(cudaEventRecord(e1, st));
+    if (out) {
+        OLF_CUDA(cudaMemcpyAsync(out, ctx.out.p, static_cast<size_t>(ctx.nS) * (n + 3) * 8, cudaMemcpyDeviceToHost, st));
+    }
+    OLF_CUDA(cudaStreamSynchronize(st));
+    OLF_CUDA(cudaEventElapsedTime(&ctx.lastMs, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    OLF_CUDA(cudaGetLastError());
+    (void)net;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Test surface
+// ---------------------------------------------------------------------------------------------------------------
+void debugFill(BatchContext& ctx, const double* xFull, const double* targetBase, const int* baseRowMode,
+               const unsigned char* disabled, double* jOut, double* fOut) {
+    OLF_CUDA(cudaSetDevice(ctx.device));
+    const Structure& s = ctx.net->host;
+    const DeviceNet& dn = *ctx.net->dev;
+    const int n = s.n;
+    const size_t S = ctx.S;
+    cudaStream_t st = ctx.stream;
+    DeviceBuffer full;
+    full.alloc(static_cast<size_t>(ctx.nS) * n * 8);
+    OLF_CUDA(cudaMemcpy(full.p, xFull, static_cast<size_t>(ctx.nS) * n * 8, cudaMemcpyHostToDevice));
+    dim3 blk(32, 8), grd((n + 31) / 32, (ctx.nS + 31) / 32);
+    toLanesKernel<<<grd, blk, 0, st>>>(full.as<double>(), ctx.x.as<double>(), n, ctx.nS, ctx.S);
+    double* stageT = ctx.stage.as<double>() + n;
+    int* stageM = reinterpret_cast<int*>(stageT + n);
+    OLF_CUDA(cudaMemcpyAsync(stageT, targetBase, n * 8, cudaMemcpyHostToDevice, st));
+    OLF_CUDA(cudaMemcpyAsync(stageM, baseRowMode, n * 4, cudaMemcpyHostToDevice, st));
+    const unsigned blocksAll = static_cast<unsigned>((static_cast<size_t>(n) * S + 255) / 256);
+    tileKernel<<<blocksAll, 256, 0, st>>>(stageT, ctx.target.as<double>(), n, ctx.S);
+    tileModeKernel<<<blocksAll, 256, 0, st>>>(stageM, ctx.mode.as<int8_t>(), n, ctx.S);
+    outageBits(ctx, disabled, ctx.nS, s.nElements);
+    const DevBatch b = ctx.batch();
+    laneInitKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b);
+    launchFill(dn.view, b, true, false, st);
+    OLF_CUDA(cudaStreamSynchronize(st));
+    OLF_CUDA(cudaGetLastError());
+    std::vector<double> J(ctx.J.bytes / 8), F(static_cast<size_t>(n) * S);
+    OLF_CUDA(cudaMemcpy(J.data(), ctx.J.p, ctx.J.bytes, cudaMemcpyDeviceToHost));
+    OLF_CUDA(cudaMemcpy(F.data(), ctx.F.p, F.size() * 8, cudaMemcpyDeviceToHost));
+    for (int sc = 0; sc < ctx.nS; sc++) {
+        for (int k = 0; k < s.nnz; k++) {
+            const int a = dn.csrToA[k];
+            jOut[static_cast<size_t>(sc) * s.nnz + k] = J[static_cast<size_t>(a) * S + sc];
+        }
+        for (int r = 0; r < n; r++) fOut[static_cast<size_t>(sc) * n + r] = F[static_cast<size_t>(r) * S + sc];
+    }
+}
+
+void debugLinearSolve(BatchContext& ctx, const double* csrVals, const double* rhs, int precision, double* out) {
+    OLF_CUDA(cudaSetDevice(ctx.device));
+    const Structure& s = ctx.net->host;
+    const DeviceNet& dn = *ctx.net->dev;
+    const DevNet& net = dn.view;
+    const int n = s.n;
+    const size_t S = ctx.S;
+    cudaStream_t st = ctx.stream;
+    const bool fp32 = precision == 1;
+    if (fp32 && !ctx.lu32.p) ctx.lu32.alloc(static_cast<size_t>(net.nLu) * 4 * S * 4);
+    if (!fp32 && !ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(net.nLu) * 4 * S * 8);
+    std::vector<double> J(ctx.J.bytes / 8, 0.0), F(static_cast<size_t>(n) * S, 0.0);
+    for (int sc = 0; sc < ctx.nS; sc++) {
+        for (int k = 0; k < s.nnz; k++) {
+            J[static_cast<size_t>(dn.csrToA[k]) * S + sc] = csrVals[static_cast<size_t>(sc) * s.nnz + k];
+        }
+        for (int r = 0; r < n; r++) F[static_cast<size_t>(r) * S + sc] = -rhs[static_cast<size_t>(sc) * n + r];
+    }
+    OLF_CUDA(cudaMemcpy(ctx.J.p, J.data(), ctx.J.bytes, cudaMemcpyHostToDevice));
+    OLF_CUDA(cudaMemcpy(ctx.F.p, F.data(), F.size() * 8, cudaMemcpyHostToDevice));
+    const DevBatch b = ctx.batch();
+    laneInitKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b);
+    launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, fp32, st);
+    launchSolve(net, b, dn.fwd(), dn.bwd(), fp32, false, st);
+    OLF_CUDA(cudaStreamSynchronize(st));
+    OLF_CUDA(cudaGetLastError());
+    std::vector<double> dx(static_cast<size_t>(n) * S);
+    OLF_CUDA(cudaMemcpy(dx.data(), ctx.dx.p, dx.size() * 8, cudaMemcpyDeviceToHost));
+    for (int sc = 0; sc < ctx.nS; sc++)
+        for (int r = 0; r < n; r++) out[static_cast<size_t>(sc) * n + r] = dx[static_cast<size_t>(r) * S + sc];
+}
+
+}  // namespace olfb200

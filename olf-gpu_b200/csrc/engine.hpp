@@ -1,0 +1,147 @@
+// Batched Newton-Raphson engine: device copy of a structure, batch contexts and the solve driver.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "structure.hpp"
+
+namespace olfb200 {
+
+#define OLF_CUDA(call)                                                                                              \
+    do {                                                                                                            \
+        cudaError_t err_ = (call);                                                                                  \
+        if (err_ != cudaSuccess) {                                                                                  \
+            throw std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(err_) + " at " __FILE__ ":" + \
+                                     std::to_string(__LINE__));                                                     \
+        }                                                                                                           \
+    } while (0)
+
+// A device allocation owned by its holder (freed on destruction; zero-filled on allocation).
+struct DeviceBuffer {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() {
+        if (p) cudaFree(p);
+    }
+    void alloc(size_t n) {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = n;
+        if (n) {
+            OLF_CUDA(cudaMalloc(&p, n));
+            OLF_CUDA(cudaMemset(p, 0, n));
+        }
+    }
+    template <typename T>
+    void upload(const std::vector<T>& v) {
+        alloc(v.size() * sizeof(T));
+        if (!v.empty()) OLF_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+// The structure's read-only device data (shared by every context built on it, on one device).
+struct DeviceNet {
+    int device = 0;
+    DevNet view{};
+    std::vector<int> levelPtr, fwdPtr, bwdPtr;   // host copies of the level boundaries (launch geometry)
+    std::vector<int> levelSplit, fwdSplit, bwdSplit;  // threads sharing one task / row, per level
+    LevelSchedule fwd() const {
+        return LevelSchedule{static_cast<int>(fwdPtr.size()) - 1, fwdPtr.data(), fwdPos.as<int>(), fwdSplit.data()};
+    }
+    LevelSchedule bwd() const {
+        return LevelSchedule{static_cast<int>(bwdPtr.size()) - 1, bwdPtr.data(), bwdPos.as<int>(), bwdSplit.data()};
+    }
+    std::vector<int> csrToA;                      // CSR slot -> A block * 4 + entry (debug readback of J)
+    DeviceBuffer nodeCol, sidePtr, side, cbPar, cbTrig, aPtr, aCol, aDiag, shPtr, shList, shPar, obPtr, obList, obPar;
+    DeviceBuffer task, ops, levelTask, perm, iperm, lrowPtr, lrow, uPtr, uCol, fwdPos, bwdPos;
+};
+
+struct NetStructure {
+    Structure host;
+    std::shared_ptr<DeviceNet> dev;
+};
+
+std::shared_ptr<DeviceNet> uploadNet(const Structure& s);
+
+// Linear-solve modes accepted at the boundary (codes/gpu_linear_solve_mode.cuh:10-12): all run the engine's own
+// batched block LU.
+enum { MODE_UBATCH = 3, MODE_ROBUST = 6, MODE_BATCHED_LU = 7 };
+
+struct SolveRequest {
+    const double* x0Base = nullptr;      // [n]
+    const double* x0Full = nullptr;      // [nS][n] or null
+    const double* targetBase = nullptr;  // [n]
+    const int* baseRowMode = nullptr;    // [n]
+    const int* rowModeEntries = nullptr; // (scenario, row, mode) triples
+    int nRowModeEntries = 0;
+    const unsigned char* disabled = nullptr;  // [nS][nElements]
+    int nScenarios = 0;
+    int nElements = 0;
+    const int* targetOverrideIndex = nullptr;  // flat scenario * n + row
+    const double* targetOverrideValue = nullptr;
+    int nTargetOverrides = 0;
+    int maxIter = 15;
+    double tol = 1e-8;
+    double reactiveLimitTol = 1e-4;
+    int maxOuter = 20;
+    int maxPqPvSwitch = 3;
+};
+
+struct BatchContext {
+    std::shared_ptr<NetStructure> net;
+    int device = 0;
+    int nS = 0, S = 0;
+    cudaStream_t stream = nullptr;
+    Settings cfg{};
+    int precision = 0;              // 0 FP64, 1 mixed (FP32 LU + FP64 refinement)
+    int refinementSteps = 1;
+    // lane-interleaved state
+    DeviceBuffer x, target, mode, F, J, lu64, lu32, w64, w32, dx, res, qbuf, disabled, norm, iter, status, outer,
+        totalIter, trouble, normOut, active, pending, precision64, nActive;
+    DeviceBuffer stage;             // upload staging (base vectors, overrides)
+    DeviceBuffer out;               // [nS][n + 3] scenario-major results
+    // reactive limits
+    DevRl rl{};
+    DeviceBuffer rlVoltageRow, rlMinQ, rlMaxQ, rlLoadQ, rlTargetV, rlNomV, rlPRow, rlStaticP, rlIdRank, rlLimitType,
+        rlSwitchCount, rlPassSwitched, rlSavedMode, rlSavedTarget, rlRemainingPv, rlSwitched;
+    // host staging (pinned) and the per-scenario start states
+    uint32_t* hostBitsPinned = nullptr;
+    DeviceBuffer full;
+    int* hostActive = nullptr;      // pinned
+    // one Newton iteration as a CUDA graph (captured on first use per settings)
+    cudaGraphExec_t graph = nullptr;
+    int graphKey = -1;
+    // statistics of the last solve
+    int lastIterations = 0;         // batched iterations run
+    float lastMs = 0.f;
+    ~BatchContext();
+    DevBatch batch() const;
+};
+
+BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, int mode, int nRl, const int* voltageRow,
+                            const double* minQ, const double* maxQ, const double* loadQ, const double* targetV,
+                            const double* nomV, const int* pRow, const double* staticP, const int* idRank);
+
+// Runs the batch; out = [nS][n + 3] per scenario [x(n), iterations, ||F||inf, status].
+void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out);
+
+// Debug/test surface: the Jacobian (CSR values of the reference-compatible pattern) and mismatch of every
+// scenario at the given states, through the engine's fill; and a batched linear solve through the engine's LU.
+void debugFill(BatchContext& ctx, const double* xFull, const double* targetBase, const int* baseRowMode,
+               const unsigned char* disabled, double* jOut, double* fOut);
+void debugLinearSolve(BatchContext& ctx, const double* csrVals, const double* rhs, int precision, double* out);
+
+}  // namespace olfb200

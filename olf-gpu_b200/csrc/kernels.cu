@@ -1,0 +1,693 @@
+// Device kernels of the batched Newton-Raphson engine (sm_100a).  See kernels.cuh for the layouts.
+#include "kernels.cuh"
+
+#include <cmath>
+
+namespace olfb200 {
+
+namespace {
+
+__device__ __forceinline__ bool solving(const DevBatch& b, int s) { return b.active[s] && !b.pending[s]; }
+
+// NaN-propagating running maximum of |v| (a NaN stays: it orders above +inf as unsigned bits).
+__device__ __forceinline__ double absMax(double m, double v) {
+    double a = fabs(v);
+    return (a <= m) ? m : a;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------------------------
+// Fused Jacobian / mismatch fill: one thread per (bus, lane).  The thread owns its bus's two rows, so every value
+// is written once, in a fixed order, with no atomics; the FIXED_VARIABLE row modes are applied in the same pass.
+// Terms: closed branches (equations/generated/closed_branch.cuh:161-229), open branches (open_branch.cuh:65-87),
+// shunts (shunt.cuh:47-60); F = terms - target (fill_launch.cu:117-126); identity rows (fill_launch.cu:96-103).
+// The per-lane max |F| is reduced in the block and folded into norm[s] with one atomic per block and lane.
+// ---------------------------------------------------------------------------------------------------------------
+template <bool WITH_J, bool WITH_Q>
+__global__ void __launch_bounds__(256) fillKernel(DevNet net, DevBatch b) {
+    const int s = blockIdx.x * 32 + threadIdx.x;
+    const int node = blockIdx.y * blockDim.y + threadIdx.y;
+    const size_t S = b.S;
+    __shared__ double red[8][33];
+    double fmax = 0.0;
+    const bool live = node < net.nb && s < b.S && b.active[s];
+    if (live) {
+        const int cP = net.nodeCol[2 * node], cV = net.nodeCol[2 * node + 1];
+        const double thi = b.x[cP * S + s], vi = b.x[cV * S + s];
+        const bool idP = b.mode[cP * S + s] == MODE_FIXED_VARIABLE;
+        const bool idQ = b.mode[cV * S + s] == MODE_FIXED_VARIABLE;
+        const int words = b.S >> 5;
+        double fp = 0.0, fq = 0.0, qcl = 0.0;
+        double d00 = 0.0, d01 = 0.0, d10 = 0.0, d11 = 0.0;
+        double o00 = 0.0, o01 = 0.0, o10 = 0.0, o11 = 0.0;
+        int curNb = -1, curBlk = -1;
+        auto flushOff = [&]() {
+            if (WITH_J && curBlk >= 0) {
+                double* J = b.J + (size_t)curBlk * 4 * S + s;
+                J[0] = idP ? 0.0 : o00;
+                J[S] = idP ? 0.0 : o01;
+                J[2 * S] = idQ ? 0.0 : o10;
+                J[3 * S] = idQ ? 0.0 : o11;
+            }
+        };
+        for (int t = net.sidePtr[node]; t < net.sidePtr[node + 1]; t++) {
+            const Side sd = net.side[t];
+            if (sd.neighbour != curNb) {
+                flushOff();
+                curNb = sd.neighbour;
+                curBlk = sd.aBlock;
+                o00 = o01 = o10 = o11 = 0.0;
+            }
+            const uint32_t word = b.disabled[(size_t)sd.element * words + (s >> 5)];
+            if ((word >> (s & 31)) & 1u) continue;
+            const double* p = net.cbPar + (size_t)sd.element * 8;
+            const double y = p[0], g1 = p[1], g2 = p[2], b1 = p[3], b2 = p[4], ksi = p[5], r1 = p[6], a1 = p[7];
+            const double2 tr = net.cbTrig[sd.element];
+            const double sk = tr.x, ck = tr.y;
+            const int jP = net.nodeCol[2 * sd.neighbour], jV = net.nodeCol[2 * sd.neighbour + 1];
+            const double thj = b.x[jP * S + s], vj = b.x[jV * S + s];
+            if (sd.side == 0) {
+                // the bus is side 1: v1 = vi, ph1 = thi, v2 = vj, ph2 = thj
+                const double v1 = vi, v2 = vj;
+                const double th1 = ksi - a1 - thi + thj;
+                double s1, c1;
+                sincos(th1, &s1, &c1);
+                const double wc = y * r1 * v1 * v2 * c1, ws = y * r1 * v1 * v2 * s1;
+                const double p1 = r1 * v1 * (g1 * r1 * v1 + y * r1 * v1 * sk - y * v2 * s1);
+                const double q1 = r1 * v1 * (-b1 * r1 * v1 + y * r1 * v1 * ck - y * v2 * c1);
+                fp += p1;
+                fq += q1;
+                qcl += q1;
+                if (WITH_J) {
+                    d00 += wc;                                                             // dp1dph1
+                    d01 += r1 * (2 * g1 * r1 * v1 + 2 * y * r1 * v1 * sk - y * v2 * s1);   // dp1dv1
+                    d10 += -ws;                                                            // dq1dph1
+                    d11 += r1 * (-2 * b1 * r1 * v1 + 2 * y * r1 * v1 * ck - y * v2 * c1);  // dq1dv1
+                    o00 += -wc;                                                            // dp1dph2
+                    o01 += -y * r1 * v1 * s1;                                              // dp1dv2
+                    o10 += ws;                                                             // dq1dph2
+                    o11 += -y * r1 * v1 * c1;                                              // dq1dv2
+                }
+            } else {
+                // the bus is side 2: v2 = vi, ph2 = thi, v1 = vj, ph1 = thj
+                const double v1 = vj, v2 = vi;
+                const double th2 = ksi + a1 + thj - thi;
+                double s2, c2;
+                sincos(th2, &s2, &c2);
+                const double wc = y * r1 * v1 * v2 * c2, ws = y * r1 * v1 * v2 * s2;
+                const double p2 = v2 * (g2 * v2 - y * r1 * v1 * s2 + y * v2 * sk);
+                const double q2 = v2 * (-b2 * v2 - y * r1 * v1 * c2 + y * v2 * ck);
+                fp += p2;
+                fq += q2;
+                qcl += q2;
+                if (WITH_J) {
+                    d00 += wc;                                             // dp2dph2
+                    d01 += 2 * g2 * v2 - y * r1 * v1 * s2 + 2 * y * v2 * sk;  // dp2dv2
+                    d10 += -ws;                                            // dq2dph2
+                    d11 += -2 * b2 * v2 - y * r1 * v1 * c2 + 2 * y * v2 * ck;  // dq2dv2
+                    o00 += -wc;                                            // dp2dph1
+                    o01 += -y * r1 * v2 * s2;                              // dp2dv1
+                    o10 += ws;                                             // dq2dph1
+                    o11 += -y * r1 * v2 * c2;                              // dq2dv1
+                }
+            }
+        }
+        flushOff();
+        for (int t = net.obPtr[node]; t < net.obPtr[node + 1]; t++) {
+            const int2 ob = net.obList[t];
+            const uint32_t word = b.disabled[(size_t)(net.ncb + ob.x) * words + (s >> 5)];
+            if ((word >> (s & 31)) & 1u) continue;
+            const double* p = net.obPar + (size_t)ob.x * 7;
+            const double y = p[0], ksi = p[1], g1 = p[2], b1 = p[3], g2 = p[4], b2 = p[5], r1 = p[6];
+            double sk, ck;
+            sincos(ksi, &sk, &ck);
+            if (ob.y == 0) {
+                // side 1 connected, side 2 open: p1/q1 at this bus, variable v1
+                const double d2 = (g2 + y * sk) * (g2 + y * sk) + (-b2 + y * ck) * (-b2 + y * ck);
+                const double gp1 = g1 + y * y * g2 / d2 + (b2 * b2 + g2 * g2) * y * sk / d2;
+                const double bq1 = b1 + y * y * b2 / d2 - (b2 * b2 + g2 * g2) * y * ck / d2;
+                fp += r1 * r1 * vi * vi * gp1;
+                fq += -r1 * r1 * vi * vi * bq1;
+                if (WITH_J) {
+                    d01 += 2 * r1 * r1 * vi * gp1;
+                    d11 += -2 * vi * r1 * r1 * bq1;
+                }
+            } else {
+                const double d1 = (g1 + y * sk) * (g1 + y * sk) + (-b1 + y * ck) * (-b1 + y * ck);
+                const double gp2 = g2 + y * y * g1 / d1 + (b1 * b1 + g1 * g1) * y * sk / d1;
+                const double bq2 = b2 + y * y * b1 / d1 - (b1 * b1 + g1 * g1) * y * ck / d1;
+                fp += vi * vi * gp2;
+                fq += -vi * vi * bq2;
+                if (WITH_J) {
+                    d01 += 2 * vi * gp2;
+                    d11 += -2 * vi * bq2;
+                }
+            }
+        }
+        for (int t = net.shPtr[node]; t < net.shPtr[node + 1]; t++) {
+            const int e = net.shList[t];
+            const uint32_t word = b.disabled[(size_t)(net.ncb + net.nob + e) * words + (s >> 5)];
+            if ((word >> (s & 31)) & 1u) continue;
+            const double g = net.shPar[2 * e], bb = net.shPar[2 * e + 1];
+            fp += g * vi * vi;
+            fq += -bb * vi * vi;
+            if (WITH_J) {
+                d01 += 2 * g * vi;
+                d11 += -2 * bb * vi;
+            }
+        }
+        double FP = fp - b.target[cP * S + s];
+        double FQ = fq - b.target[cV * S + s];
+        if (idP) FP = thi - b.target[cP * S + s];
+        if (idQ) FQ = vi - b.target[cV * S + s];
+        b.F[cP * S + s] = FP;
+        b.F[cV * S + s] = FQ;
+        if (WITH_Q) b.qbuf[cV * S + s] = qcl;
+        if (WITH_J) {
+            double* J = b.J + (size_t)net.aDiag[node] * 4 * S + s;
+            J[0] = idP ? 1.0 : d00;
+            J[S] = idP ? 0.0 : d01;
+            J[2 * S] = idQ ? 0.0 : d10;
+            J[3 * S] = idQ ? 1.0 : d11;
+        }
+        fmax = absMax(absMax(0.0, FP), FQ);
+    }
+    red[threadIdx.y][threadIdx.x] = fmax;
+    __syncthreads();
+    if (threadIdx.y == 0 && s < b.S) {
+        double m = red[0][threadIdx.x];
+        for (int k = 1; k < blockDim.y; k++) m = absMax(m, red[k][threadIdx.x]);
+        if (b.active[s] && m != 0.0) atomicMax(&b.norm[s], (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+void launchFill(const DevNet& net, const DevBatch& b, bool withJacobian, bool withQbuf, cudaStream_t st) {
+    dim3 block(32, 8);
+    dim3 grid(b.S / 32, (net.nb + 7) / 8);
+    if (withJacobian) {
+        if (withQbuf) fillKernel<true, true><<<grid, block, 0, st>>>(net, b);
+        else fillKernel<true, false><<<grid, block, 0, st>>>(net, b);
+    } else {
+        if (withQbuf) fillKernel<false, true><<<grid, block, 0, st>>>(net, b);
+        else fillKernel<false, false><<<grid, block, 0, st>>>(net, b);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Convergence test and retirement (newton_iteration.cu:276-397): >= 1 iteration; a test that passes at the budget
+// is MAX_ITERATION_REACHED; a non-finite mismatch is DIVERGED.  A converged lane with reactive limits to check is
+// marked pending instead (its outer loop decides).
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void testKernel(DevBatch b, Settings cfg, int* remainingPv) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.S || !b.active[s]) return;
+    const double nrm = __longlong_as_double((long long)b.norm[s]);
+    b.norm[s] = 0ull;
+    const int it = b.iter[s];
+    b.normOut[s] = nrm;
+    if (!isfinite(nrm)) {
+        b.status[s] = ST_DIVERGED;
+        b.active[s] = 0;
+        atomicSub(b.nActive, 1);
+        return;
+    }
+    if (it > 0 && b.trouble[s]) {
+        // the previous factorization met a near-singular 2x2 pivot: its step is not trusted
+        b.status[s] = ST_LINEAR_SOLVE_FAILED;
+        b.active[s] = 0;
+        atomicSub(b.nActive, 1);
+        return;
+    }
+    if (it > 0 && nrm < cfg.tol && it < cfg.maxIter) {
+        if (cfg.reactiveLimits && b.outer[s] < cfg.maxOuter) {
+            b.pending[s] = 1;
+            if (remainingPv) remainingPv[s] = 0;
+        } else {
+            b.status[s] = ST_CONVERGED;
+            b.active[s] = 0;
+            atomicSub(b.nActive, 1);
+        }
+        return;
+    }
+    if (it == cfg.maxIter) {
+        b.status[s] = ST_MAX_ITERATION_REACHED;
+        b.active[s] = 0;
+        atomicSub(b.nActive, 1);
+    }
+}
+
+void launchTest(const DevNet&, const DevBatch& b, const Settings& cfg, int* remainingPv, cudaStream_t st) {
+    testKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b, cfg, remainingPv);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Reactive-limit outer loop, local controllers (reactive_limits.cu:321-359) and the forced-PV election
+// (reactive_limits.cu:417-448).  q = closed-branch flows on the V row + load Q.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void rlCheckKernel(DevBatch b, DevRl rl, Settings cfg) {
+    const size_t S = b.S;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = (int)(tid % S);
+    const int i = (int)(tid / S);
+    if (i >= rl.nRl || !b.pending[s]) return;
+    const size_t e = (size_t)i * S + s;
+    rl.passSwitched[e] = 0;
+    const int r = rl.voltageRow[i];
+    const size_t ri = (size_t)r * S + s;
+    if (b.mode[ri] == MODE_FIXED_VARIABLE && rl.limitType[e] == 0) {
+        const double q = b.qbuf[ri] + rl.loadQ[i];
+        if (q < rl.minQ[i] - cfg.rlTol) {
+            rl.savedTarget[e] = b.target[ri];
+            rl.savedMode[e] = b.mode[ri];
+            b.mode[ri] = MODE_EQUATION;
+            b.target[ri] = rl.minQ[i] - rl.loadQ[i];
+            rl.limitType[e] = 1;
+            rl.switchCount[e]++;
+            rl.passSwitched[e] = 1;
+        } else if (q > rl.maxQ[i] + cfg.rlTol) {
+            rl.savedTarget[e] = b.target[ri];
+            rl.savedMode[e] = b.mode[ri];
+            b.mode[ri] = MODE_EQUATION;
+            b.target[ri] = rl.maxQ[i] - rl.loadQ[i];
+            rl.limitType[e] = 2;
+            rl.switchCount[e]++;
+            rl.passSwitched[e] = 1;
+        } else {
+            atomicAdd(&rl.remainingPv[s], 1);
+        }
+    } else if (rl.limitType[e] != 0) {
+        const double v = b.x[ri];
+        const double tv = rl.targetV[i];
+        const bool wants = (rl.limitType[e] == 2 && v > tv) || (rl.limitType[e] == 1 && v < tv);
+        if (wants && rl.switchCount[e] < cfg.maxSwitch) {
+            b.mode[ri] = MODE_FIXED_VARIABLE;
+            b.target[ri] = tv;
+            rl.limitType[e] = 0;
+            rl.passSwitched[e] = 2;
+        }
+    }
+}
+
+__global__ void rlFinalizeKernel(DevBatch b, DevRl rl) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.S || !b.pending[s]) return;
+    const size_t S = b.S;
+    if (rl.remainingPv[s] == 0) {
+        int best = -1, bestId = 0x7fffffff;
+        double bestV = -1.0, bestP = -1e300;
+        for (int i = 0; i < rl.nRl; i++) {
+            const size_t e = (size_t)i * S + s;
+            if (rl.passSwitched[e] != 1) continue;
+            const double v = rl.nomV[i];
+            const double p = rl.pRow[i] >= 0 ? b.target[(size_t)rl.pRow[i] * S + s] : rl.staticP[i];
+            const bool better = best < 0 || v > bestV || (v == bestV && (p > bestP || (p == bestP && rl.idRank[i] < bestId)));
+            if (better) {
+                best = i;
+                bestV = v;
+                bestP = p;
+                bestId = rl.idRank[i];
+            }
+        }
+        if (best >= 0) {
+            const size_t e = (size_t)best * S + s;
+            const size_t ri = (size_t)rl.voltageRow[best] * S + s;
+            b.mode[ri] = rl.savedMode[e];
+            b.target[ri] = rl.savedTarget[e];
+            rl.limitType[e] = 0;
+            rl.switchCount[e]--;
+            rl.passSwitched[e] = 0;
+        }
+    }
+    bool any = false;
+    for (int i = 0; i < rl.nRl && !any; i++) any = rl.passSwitched[(size_t)i * S + s] != 0;
+    if (any) {
+        // restart the Newton solve at the new targets and modes (newton_iteration.cu:472-487)
+        b.iter[s] = 0;
+        b.outer[s]++;
+    } else {
+        b.status[s] = ST_CONVERGED;
+        b.active[s] = 0;
+        b.pending[s] = 0;
+        atomicSub(b.nActive, 1);
+    }
+}
+
+void launchReactiveLimits(const DevNet&, const DevBatch& b, const DevRl& rl, const Settings& cfg, cudaStream_t st) {
+    if (rl.nRl == 0) return;
+    const size_t threads = (size_t)rl.nRl * b.S;
+    rlCheckKernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(b, rl, cfg);
+    rlFinalizeKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b, rl);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Batched block LU, one level of tasks per launch: one thread per (LU block, lane).
+//   U(k, j) = A(k, j) - sum_m L(k, m) U(m, j);    L(i, k) = (A(i, k) - sum_m L(i, m) U(m, k)) inv(U(k, k))
+// The diagonal slot U(k, k) stores its inverse.  The update pairs come in ascending m (a fixed summation order).
+// A near-singular 2x2 pivot (|det| <= 1e-13 of its terms, lu_pivot.cuh:12-18) flags the lane.
+// ---------------------------------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void load4(const T* base, size_t blk, size_t S, int s, T& a, T& b_, T& c, T& d) {
+    const T* p = base + blk * 4 * S + s;
+    a = p[0];
+    b_ = p[S];
+    c = p[2 * S];
+    d = p[3 * S];
+}
+
+template <typename T>
+__device__ __forceinline__ void store4(T* base, size_t blk, size_t S, int s, T a, T b_, T c, T d) {
+    T* p = base + blk * 4 * S + s;
+    p[0] = a;
+    p[S] = b_;
+    p[2 * S] = c;
+    p[3 * S] = d;
+}
+
+// Launch geometry of one level: P threads share each task (or row) of the level, splitting its update list P ways;
+// blocks are 32 lanes x max(8, P) threads.  The P partial sums are added in a fixed order (part 0 first), so the
+// result does not depend on scheduling.
+template <int P>
+struct Split {
+    static constexpr int ROWS = P >= 8 ? P : 8;     // blockDim.y
+    static constexpr int TPB = P >= 8 ? 1 : 8 / P;  // tasks per block
+};
+
+template <typename T, int P>
+__global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b, T* lu, int first, int count) {
+    constexpr int TPB = Split<P>::TPB, ROWS = Split<P>::ROWS;
+    __shared__ T red[ROWS][4][32];
+    const size_t S = b.S;
+    const int lane = threadIdx.x, ty = threadIdx.y;
+    const int tib = ty / P, part = ty % P;
+    const int s = blockIdx.y * 32 + lane;
+    const int k = blockIdx.x * TPB + tib;
+    const bool ok = k < count && s < b.S && solving(b, s);
+    T a00 = 0, a01 = 0, a10 = 0, a11 = 0;
+    int t = 0;
+    Task tk{};
+    if (ok) {
+        t = net.levelTask[first + k];
+        tk = net.task[t];
+        if (part == 0 && tk.aBlock >= 0) {
+            const double* p = b.J + (size_t)tk.aBlock * 4 * S + s;
+            a00 = (T)p[0];
+            a01 = (T)p[S];
+            a10 = (T)p[2 * S];
+            a11 = (T)p[3 * S];
+        }
+#pragma unroll 4
+        for (int q = tk.opBegin + part; q < tk.opEnd; q += P) {
+            const int2 op = net.ops[q];
+            T l00, l01, l10, l11, u00, u01, u10, u11;
+            load4(lu, (size_t)op.x, S, s, l00, l01, l10, l11);
+            load4(lu, (size_t)op.y, S, s, u00, u01, u10, u11);
+            a00 -= l00 * u00 + l01 * u10;
+            a01 -= l00 * u01 + l01 * u11;
+            a10 -= l10 * u00 + l11 * u10;
+            a11 -= l10 * u01 + l11 * u11;
+        }
+    }
+    if (P > 1) {
+        red[ty][0][lane] = a00;
+        red[ty][1][lane] = a01;
+        red[ty][2][lane] = a10;
+        red[ty][3][lane] = a11;
+        __syncthreads();
+        if (part == 0) {
+            for (int q = 1; q < P; q++) {
+                a00 += red[ty + q][0][lane];
+                a01 += red[ty + q][1][lane];
+                a10 += red[ty + q][2][lane];
+                a11 += red[ty + q][3][lane];
+            }
+        }
+    }
+    if (!ok || part != 0) return;
+    if (tk.diag == -2) {
+        const T det = a00 * a11 - a01 * a10;
+        const T scale = fabs(a00 * a11) + fabs(a01 * a10);
+        if (!(fabs(det) > (T)1e-13 * scale) || !isfinite(det)) b.trouble[s] = 1;
+        const T inv = (T)1 / det;
+        store4(lu, (size_t)t, S, s, a11 * inv, -a01 * inv, -a10 * inv, a00 * inv);
+    } else if (tk.diag >= 0) {
+        T i00, i01, i10, i11;
+        load4(lu, (size_t)tk.diag, S, s, i00, i01, i10, i11);
+        store4(lu, (size_t)t, S, s, a00 * i00 + a01 * i10, a00 * i01 + a01 * i11, a10 * i00 + a11 * i10,
+               a10 * i01 + a11 * i11);
+    } else {
+        store4(lu, (size_t)t, S, s, a00, a01, a10, a11);
+    }
+}
+
+__global__ void clearTroubleKernel(DevBatch b) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < b.S && solving(b, s)) b.trouble[s] = 0;
+}
+
+// Launches a per-level kernel template with the level's split factor.
+#define OLF_SPLIT_CASE(N, KERNEL, T_, ...)                                                             \
+    case N: {                                                                                           \
+        dim3 blk(32, Split<N>::ROWS), grd((count + Split<N>::TPB - 1) / Split<N>::TPB, b.S / 32);       \
+        KERNEL<T_, N><<<grd, blk, 0, st>>>(__VA_ARGS__);                                                \
+        break;                                                                                          \
+    }
+#define OLF_SPLIT_DISPATCH(P_, KERNEL, T_, ...)                                                         \
+    switch (P_) {                                                                                       \
+        OLF_SPLIT_CASE(1, KERNEL, T_, __VA_ARGS__)                                                      \
+        OLF_SPLIT_CASE(2, KERNEL, T_, __VA_ARGS__)                                                      \
+        OLF_SPLIT_CASE(4, KERNEL, T_, __VA_ARGS__)                                                      \
+        OLF_SPLIT_CASE(8, KERNEL, T_, __VA_ARGS__)                                                      \
+        default: OLF_SPLIT_CASE(16, KERNEL, T_, __VA_ARGS__)                                            \
+    }
+
+void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtr, const int* levelSplit, int nLevels,
+                  bool fp32, cudaStream_t st) {
+    clearTroubleKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b);
+    for (int l = 0; l < nLevels; l++) {
+        const int first = levelPtr[l], count = levelPtr[l + 1] - levelPtr[l];
+        if (count == 0) continue;
+        if (fp32) {
+            OLF_SPLIT_DISPATCH(levelSplit[l], factorLevelKernel, float, net, b, b.lu32, first, count)
+        } else {
+            OLF_SPLIT_DISPATCH(levelSplit[l], factorLevelKernel, double, net, b, b.lu64, first, count)
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Triangular solves on the block factors, level by level; one thread per (position, lane).
+// ---------------------------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void rhsKernel(DevNet net, DevBatch b, T* w, bool fromResidual) {
+    const size_t S = b.S;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = (int)(tid % S);
+    const int i = (int)(tid / S);
+    if (i >= net.nb || !solving(b, s)) return;
+    const int node = net.perm[i];
+    const int cP = net.nodeCol[2 * node], cV = net.nodeCol[2 * node + 1];
+    if (fromResidual) {
+        w[(2 * (size_t)i) * S + s] = (T)b.res[cP * S + s];
+        w[(2 * (size_t)i + 1) * S + s] = (T)b.res[cV * S + s];
+    } else {
+        w[(2 * (size_t)i) * S + s] = (T)(-b.F[cP * S + s]);
+        w[(2 * (size_t)i + 1) * S + s] = (T)(-b.F[cV * S + s]);
+    }
+}
+
+template <typename T, int P>
+__global__ void __launch_bounds__(1024) forwardLevelKernel(DevNet net, DevBatch b, const T* lu, T* w, const int* pos,
+                                                           int first, int count) {
+    constexpr int TPB = Split<P>::TPB, ROWS = Split<P>::ROWS;
+    __shared__ T red[ROWS][2][32];
+    const size_t S = b.S;
+    const int lane = threadIdx.x, ty = threadIdx.y;
+    const int tib = ty / P, part = ty % P;
+    const int s = blockIdx.y * 32 + lane;
+    const int k = blockIdx.x * TPB + tib;
+    const bool ok = k < count && s < b.S && solving(b, s);
+    T w0 = 0, w1 = 0;
+    int i = 0;
+    if (ok) {
+        i = pos[first + k];
+        if (part == 0) {
+            w0 = w[(2 * (size_t)i) * S + s];
+            w1 = w[(2 * (size_t)i + 1) * S + s];
+        }
+#pragma unroll 4
+        for (int q = net.lrowPtr[i] + part; q < net.lrowPtr[i + 1]; q += P) {
+            const int2 e = net.lrow[q];
+            T l00, l01, l10, l11;
+            load4(lu, (size_t)e.x, S, s, l00, l01, l10, l11);
+            const T y0 = w[(2 * (size_t)e.y) * S + s], y1 = w[(2 * (size_t)e.y + 1) * S + s];
+            w0 -= l00 * y0 + l01 * y1;
+            w1 -= l10 * y0 + l11 * y1;
+        }
+    }
+    if (P > 1) {
+        red[ty][0][lane] = w0;
+        red[ty][1][lane] = w1;
+        __syncthreads();
+        if (part == 0) {
+            for (int q = 1; q < P; q++) {
+                w0 += red[ty + q][0][lane];
+                w1 += red[ty + q][1][lane];
+            }
+        }
+    }
+    if (!ok || part != 0) return;
+    w[(2 * (size_t)i) * S + s] = w0;
+    w[(2 * (size_t)i + 1) * S + s] = w1;
+}
+
+template <typename T, int P>
+__global__ void __launch_bounds__(1024) backwardLevelKernel(DevNet net, DevBatch b, const T* lu, T* w, const int* pos,
+                                                            int first, int count) {
+    constexpr int TPB = Split<P>::TPB, ROWS = Split<P>::ROWS;
+    __shared__ T red[ROWS][2][32];
+    const size_t S = b.S;
+    const int lane = threadIdx.x, ty = threadIdx.y;
+    const int tib = ty / P, part = ty % P;
+    const int s = blockIdx.y * 32 + lane;
+    const int k = blockIdx.x * TPB + tib;
+    const bool ok = k < count && s < b.S && solving(b, s);
+    T w0 = 0, w1 = 0;
+    int i = 0, d = 0;
+    if (ok) {
+        i = pos[first + k];
+        d = net.uPtr[i];
+        if (part == 0) {
+            w0 = w[(2 * (size_t)i) * S + s];
+            w1 = w[(2 * (size_t)i + 1) * S + s];
+        }
+#pragma unroll 4
+        for (int q = d + 1 + part; q < net.uPtr[i + 1]; q += P) {
+            const int j = net.uCol[q];
+            T u00, u01, u10, u11;
+            load4(lu, (size_t)q, S, s, u00, u01, u10, u11);
+            const T x0 = w[(2 * (size_t)j) * S + s], x1 = w[(2 * (size_t)j + 1) * S + s];
+            w0 -= u00 * x0 + u01 * x1;
+            w1 -= u10 * x0 + u11 * x1;
+        }
+    }
+    if (P > 1) {
+        red[ty][0][lane] = w0;
+        red[ty][1][lane] = w1;
+        __syncthreads();
+        if (part == 0) {
+            for (int q = 1; q < P; q++) {
+                w0 += red[ty + q][0][lane];
+                w1 += red[ty + q][1][lane];
+            }
+        }
+    }
+    if (!ok || part != 0) return;
+    T i00, i01, i10, i11;
+    load4(lu, (size_t)d, S, s, i00, i01, i10, i11);
+    w[(2 * (size_t)i) * S + s] = i00 * w0 + i01 * w1;
+    w[(2 * (size_t)i + 1) * S + s] = i10 * w0 + i11 * w1;
+}
+
+template <typename T>
+__global__ void scatterKernel(DevNet net, DevBatch b, const T* w, bool accumulate) {
+    const size_t S = b.S;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = (int)(tid % S);
+    const int node = (int)(tid / S);
+    if (node >= net.nb || !solving(b, s)) return;
+    const int i = net.iperm[node];
+    const int cP = net.nodeCol[2 * node], cV = net.nodeCol[2 * node + 1];
+    const double d0 = (double)w[(2 * (size_t)i) * S + s], d1 = (double)w[(2 * (size_t)i + 1) * S + s];
+    if (accumulate) {
+        b.dx[cP * S + s] += d0;
+        b.dx[cV * S + s] += d1;
+    } else {
+        b.dx[cP * S + s] = d0;
+        b.dx[cV * S + s] = d1;
+    }
+}
+
+template <typename T>
+static void solveT(const DevNet& net, const DevBatch& b, T* w, const T* lu, const LevelSchedule& fwd,
+                   const LevelSchedule& bwd, bool fromResidual, cudaStream_t st) {
+    const size_t all = (size_t)net.nb * b.S;
+    rhsKernel<T><<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b, w, fromResidual);
+    for (int l = 0; l < fwd.levels; l++) {
+        const int first = fwd.ptr[l], count = fwd.ptr[l + 1] - fwd.ptr[l];
+        if (count == 0) continue;
+        OLF_SPLIT_DISPATCH(fwd.split[l], forwardLevelKernel, T, net, b, lu, w, fwd.pos, first, count)
+    }
+    for (int l = 0; l < bwd.levels; l++) {
+        const int first = bwd.ptr[l], count = bwd.ptr[l + 1] - bwd.ptr[l];
+        if (count == 0) continue;
+        OLF_SPLIT_DISPATCH(bwd.split[l], backwardLevelKernel, T, net, b, lu, w, bwd.pos, first, count)
+    }
+    scatterKernel<T><<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b, w, fromResidual);
+}
+
+void launchSolve(const DevNet& net, const DevBatch& b, const LevelSchedule& fwd, const LevelSchedule& bwd, bool fp32,
+                 bool fromResidual, cudaStream_t st) {
+    if (fp32) solveT<float>(net, b, b.w32, b.lu32, fwd, bwd, fromResidual, st);
+    else solveT<double>(net, b, b.w64, b.lu64, fwd, bwd, fromResidual, st);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// FP64 refinement residual r = -F - J dx, one thread per (bus, lane), J in its block rows.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void residualKernel(DevNet net, DevBatch b) {
+    const size_t S = b.S;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = (int)(tid % S);
+    const int node = (int)(tid / S);
+    if (node >= net.nb || !solving(b, s)) return;
+    const int cP = net.nodeCol[2 * node], cV = net.nodeCol[2 * node + 1];
+    double r0 = -b.F[cP * S + s], r1 = -b.F[cV * S + s];
+    for (int t = net.aPtr[node]; t < net.aPtr[node + 1]; t++) {
+        const int j = net.aCol[t];
+        const double* J = b.J + (size_t)t * 4 * S + s;
+        const double x0 = b.dx[(size_t)net.nodeCol[2 * j] * S + s], x1 = b.dx[(size_t)net.nodeCol[2 * j + 1] * S + s];
+        r0 -= J[0] * x0 + J[S] * x1;
+        r1 -= J[2 * S] * x0 + J[3 * S] * x1;
+    }
+    b.res[cP * S + s] = r0;
+    b.res[cV * S + s] = r1;
+}
+
+void launchResidual(const DevNet& net, const DevBatch& b, cudaStream_t st) {
+    const size_t all = (size_t)net.nb * b.S;
+    residualKernel<<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Newton step x += dx for the lanes that solved this iteration (state_vector_scaling.cu:48-57, plain NR); the
+// per-lane iteration counters advance; a pending lane (reactive limits decided) is released.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void stepKernel(DevNet net, DevBatch b) {
+    const size_t S = b.S;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = (int)(tid % S);
+    const int r = (int)(tid / S);
+    if (r >= net.n) return;
+    if (solving(b, s)) b.x[(size_t)r * S + s] += b.dx[(size_t)r * S + s];
+}
+
+__global__ void advanceKernel(DevBatch b) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.S || !b.active[s]) return;
+    if (!b.pending[s]) {
+        b.iter[s]++;
+        b.totalIter[s]++;
+    }
+    b.pending[s] = 0;
+}
+
+void launchStep(const DevNet& net, const DevBatch& b, bool, cudaStream_t st) {
+    const size_t all = (size_t)net.n * b.S;
+    stepKernel<<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b);
+    advanceKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b);
+}
+
+void launchGrowthCheck(const DevNet&, const DevBatch&, double, cudaStream_t) {}
+
+}  // namespace olfb200

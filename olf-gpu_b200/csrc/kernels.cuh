@@ -1,0 +1,157 @@
+// Device kernels of the batched Newton-Raphson engine (sm_100a).
+//
+// Every per-scenario array is lane-interleaved: element e of lane s sits at [e * S + s], S = the lane count rounded
+// up to a multiple of 32, so consecutive threads (lanes) of a warp touch consecutive addresses.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace olfb200 {
+
+// Per-lane status codes (codes/gpu_ac_solver_status.cuh:10-15) and the engine's running state.
+enum : int {
+    ST_CONVERGED = 0,
+    ST_MAX_ITERATION_REACHED = 1,
+    ST_UNREALISTIC_STATE = 2,
+    ST_DIVERGED = -1,
+    ST_REJECTED = -2,
+    ST_LINEAR_SOLVE_FAILED = -3,
+    ST_RUNNING = 100,
+};
+
+// Row modes (codes/gpu_row_mode.cuh:10-15).
+enum : int { MODE_FIXED_VARIABLE = 0, MODE_EQUATION = 1, MODE_BUS_TARGET_Q = 4 };
+
+// One incident closed-branch side of a node, sorted by neighbour: branch element, which side the node is on (0: the
+// node is bus 1, 1: bus 2), the neighbour node and the A block of (node, neighbour).
+struct Side {
+    int element;
+    int side;
+    int neighbour;
+    int aBlock;
+};
+
+// One factorization task (an LU block): where its A block is (-1: fill-in), its update pairs, and for an L block the
+// U diagonal block whose inverse it is multiplied by (-1 for U blocks, -2 for a U diagonal block).
+struct Task {
+    int aBlock;
+    int opBegin;
+    int opEnd;
+    int diag;
+};
+
+// Everything the kernels read about one network (device pointers), built once per structure.
+struct DevNet {
+    int n, nb, nA, nLu, ncb, nob, nsh, nElements;
+    const int* nodeCol;       // [2 nb]
+    const int* sidePtr;       // [nb + 1]
+    const Side* side;         // incident closed-branch sides
+    const double* cbPar;      // [ncb * 8] y g1 g2 b1 b2 ksi r1 a1
+    const double2* cbTrig;    // [ncb] (sin ksi, cos ksi)
+    const int* aPtr;          // [nb + 1] A blocks by node row
+    const int* aCol;          // [nA]
+    const int* aDiag;         // [nb]
+    const int* shPtr;         // [nb + 1]
+    const int* shList;        // shunt elements
+    const double* shPar;      // [nsh * 2] g b
+    const int* obPtr;         // [nb + 1]
+    const int2* obList;       // (open-branch element, connected side 0/1)
+    const double* obPar;      // [nob * 7] y ksi g1 b1 g2 b2 r1
+    // LU
+    const Task* task;         // [nLu]
+    const int2* ops;          // update pairs (L block, U block)
+    const int* levelTask;     // tasks grouped by level
+    const int* perm;          // position -> node
+    const int* iperm;         // node -> position
+    const int* lrowPtr;       // [nb + 1] L blocks of each row position
+    const int2* lrow;         // (L block id, column position)
+    const int* uPtr;          // [nb + 1] U blocks of each row position (diagonal first: holds the inverse)
+    const int* uCol;          // column position of each U block
+};
+
+// Per-batch device state (lane-interleaved arrays).
+struct DevBatch {
+    int S;                    // lane stride (multiple of 32)
+    int nS;                   // installed scenarios (lanes >= nS are padding, never active)
+    double* x;                // [n][S]
+    double* target;           // [n][S]
+    int8_t* mode;             // [n][S]
+    double* F;                // [n][S]
+    double* J;                // [nA][4][S]
+    double* lu64;             // [nLu][4][S]
+    float* lu32;              // [nLu][4][S] (mixed precision only)
+    double* w64;              // [nb][2][S] solve work (positions)
+    float* w32;               // [nb][2][S]
+    double* dx;               // [n][S]
+    double* res;              // [n][S] refinement residual
+    double* qbuf;             // [n][S] closed-branch flows on their rows (reactive limits)
+    const uint32_t* disabled; // [nElements][S / 32] outage bits
+    unsigned long long* norm; // [S] max |F| as ordered bits
+    int* iter;                // [S] Newton iteration of the current solve
+    int* status;              // [S]
+    int* outer;               // [S] reactive-limit outer iterations
+    int* totalIter;           // [S] Newton iterations over all solves
+    int* trouble;             // [S] near-singular pivots met in the last factorization
+    double* normOut;          // [S] the last tested ||F||inf
+    int8_t* active;           // [S] 1 while the lane iterates
+    int8_t* pending;          // [S] 1: converged this iteration, reactive limits to check
+    int8_t* precision64;      // [S] 1: this lane's last factorization fell back to FP64 (mixed precision)
+    int* nActive;             // [1] lanes still iterating (read by the host to stop)
+};
+
+// Reactive-limit entries (ReactiveLimitsPacker.java:76) and their per-lane state.
+struct DevRl {
+    int nRl;
+    const int* voltageRow;
+    const double* minQ;
+    const double* maxQ;
+    const double* loadQ;
+    const double* targetV;
+    const double* nomV;
+    const int* pRow;
+    const double* staticP;
+    const int* idRank;
+    int8_t* limitType;        // [nRl][S] 0 none, 1 min, 2 max
+    int8_t* switchCount;      // [nRl][S]
+    int8_t* passSwitched;     // [nRl][S]
+    int8_t* savedMode;        // [nRl][S]
+    double* savedTarget;      // [nRl][S]
+    int* remainingPv;         // [S]
+    int* switched;            // [S]
+};
+
+struct Settings {
+    int maxIter;
+    double tol;
+    int reactiveLimits;
+    double rlTol;
+    int maxOuter;
+    int maxSwitch;
+    int mixed;                // 1: FP32 factorization and solves with FP64 refinement
+    int refinementSteps;
+    double growthLimit;       // pivot growth above which a mixed lane refactors in FP64
+};
+
+// Kernel launchers (stream-ordered; all lanes of the batch).
+void launchFill(const DevNet& net, const DevBatch& b, bool withJacobian, bool withQbuf, cudaStream_t st);
+void launchTest(const DevNet& net, const DevBatch& b, const Settings& cfg, int* remainingPv, cudaStream_t st);
+void launchReactiveLimits(const DevNet& net, const DevBatch& b, const DevRl& rl, const Settings& cfg,
+                          cudaStream_t st);
+// Level boundaries (host), the positions of each level (device) and the split factor of each level (host).
+struct LevelSchedule {
+    int levels;
+    const int* ptr;
+    const int* pos;
+    const int* split;
+};
+
+void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtrHost, const int* levelSplitHost,
+                  int nLevels, bool fp32, cudaStream_t st);
+void launchSolve(const DevNet& net, const DevBatch& b, const LevelSchedule& fwd, const LevelSchedule& bwd, bool fp32,
+                 bool fromResidual, cudaStream_t st);
+void launchResidual(const DevNet& net, const DevBatch& b, cudaStream_t st);
+void launchStep(const DevNet& net, const DevBatch& b, bool accumulate, cudaStream_t st);
+void launchGrowthCheck(const DevNet& net, const DevBatch& b, double limit, cudaStream_t st);
+
+}  // namespace olfb200

@@ -1,0 +1,67 @@
+// Host-side structure of one network: the reference-compatible equation structure (row map, fixed superset CSR
+// pattern, role-folded scatter map, diagonal slots) and the engine's bus-block view of it with the block-LU plan.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace olfb200 {
+
+constexpr int CB_OUTPUTS = 28;   // closed_branch_scatter.h: CLOSED_BRANCH_OUTPUT_COUNT
+constexpr int OB_OUTPUTS = 8;    // open_branch_scatter.h
+constexpr int SH_OUTPUTS = 5;    // shunt_scatter.h
+constexpr int CB_PARAMS = 8, CB_INDICES = 12;
+constexpr int OB_PARAMS = 7, OB_INDICES = 6;
+constexpr int SH_PARAMS = 2, SH_INDICES = 5;
+
+// Block-LU plan on the bus graph (2x2 blocks).  Positions are elimination positions 0..nb-1.
+//   U rows:  for pivot k, blocks (k, j) j in {k} U struct(k), diagonal first, then ascending j.
+//   L cols:  for pivot k, blocks (i, k) i in struct(k), ascending i.
+// Every LU block has an id in [0, nLuBlocks): U blocks first (uPtr), then L blocks (lPtr offset by nU).
+struct BlockPlan {
+    int nb = 0;
+    std::vector<int> perm;        // elimination position -> node
+    std::vector<int> iperm;       // node -> elimination position
+    std::vector<int> uPtr, uCol;  // U rows (CSR over positions), uCol[pos] = column position j
+    std::vector<int> lPtr, lRow;  // L cols (CSC over positions), lRow[pos] = row position i
+    int nU = 0, nL = 0;
+    // A blocks (the Jacobian's block pattern in node order, block-CSR by node row, diagonal included) and where
+    // each A block sits in the LU storage (-1 never happens: the fill is a superset of A).
+    std::vector<int> aPtr, aCol;  // by node
+    std::vector<int> aDiag;       // node -> A block id of its diagonal
+    std::vector<int> aToLu;       // A block id -> LU block id
+    std::vector<int> luToA;       // LU block id -> A block id or -1 (pure fill-in)
+    // Factorization: one task per LU block; its update pairs (L block, U block) in ascending k; its level.
+    std::vector<int> opPtr, opL, opU;   // per LU block
+    std::vector<int> level;             // per LU block
+    std::vector<int> levelPtr, levelTask;  // tasks grouped by level (CSR); tasks are LU block ids
+    // Triangular solves: forward over positions in L, backward in U; level sets of positions.
+    std::vector<int> fwdLevelPtr, fwdLevelPos, bwdLevelPtr, bwdLevelPos;
+    int64_t blockOps = 0;               // total 2x2 block multiply-subtracts per factorization
+};
+
+struct Structure {
+    int n = 0, nnz = 0, ncb = 0, nob = 0, nsh = 0, nElements = 0;
+    std::vector<int> rowMap, rowPtr, colIdx, diagPos;
+    std::vector<int> cbDest, obDest, shDest;
+    std::vector<double> cbPar, obPar, shPar;
+    std::vector<int> cbIx, obIx, shIx;  // packs with rows mapped through rowMap
+    // bus-block view
+    int nb = 0;
+    std::vector<int> nodeCol;           // [nb*2]: the node's angle (P row) and magnitude (Q row) columns
+    std::vector<int> colNode;           // [n]: column -> node*2 + slot
+    BlockPlan plan;
+};
+
+// Builds the structure; throws std::runtime_error on bad or unsupported input.
+Structure buildStructure(int n, int ncb, const double* cbPar, const int* cbIx, int nob, const double* obPar,
+                         const int* obIx, int nsh, const double* shPar, const int* shIx, int nid, const int* idRows,
+                         int ordering);
+
+// Orderings of the bus graph for the block LU.
+enum Ordering { ORDER_MIN_DEGREE = 0, ORDER_NESTED_DISSECTION = 1, ORDER_NATURAL = 2 };
+
+void buildBlockPlan(Structure& s, int ordering);
+
+}  // namespace olfb200

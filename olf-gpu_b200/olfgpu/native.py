@@ -1,0 +1,231 @@
+"""ctypes binding of the engine's C ABI (``include/olfgpu_b200.h``), shaped like the reference's Java facades
+(``StructureNative``, ``BatchSolveNative``, ``NewtonSettingsNative``).
+
+The binding loads ``lib/libolfgpu_b200.so`` built in-tree; there is no fallback: a missing library is an error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libolfgpu_b200.so")
+
+# Linear-solve modes (codes/gpu_linear_solve_mode.cuh:10-12)
+UBATCH, ROBUST, BATCHED_LU = 3, 6, 7
+# Statuses (codes/gpu_ac_solver_status.cuh:10-15)
+CONVERGED, MAX_ITERATION_REACHED, UNREALISTIC_STATE = 0, 1, 2
+DIVERGED, REJECTED, LINEAR_SOLVE_FAILED = -1, -2, -3
+STATUS_NAMES = {0: "CONVERGED", 1: "MAX_ITERATION_REACHED", 2: "UNREALISTIC_STATE", -1: "DIVERGED", -2: "REJECTED",
+                -3: "LINEAR_SOLVE_FAILED"}
+# Precision of the linear solves
+FP64, MIXED = 0, 1
+
+_i64 = ctypes.c_int64
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_fp = ctypes.POINTER(ctypes.c_float)
+
+EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_structure", "olfgpu_structure_info",
+           "olfgpu_structure_export", "olfgpu_recommend_batch_size", "olfgpu_create_batch_context",
+           "olfgpu_destroy_batch_context", "olfgpu_set_linear_solver_settings", "olfgpu_solve_batch_context",
+           "olfgpu_last_solve_stats", "olfgpu_debug_fill", "olfgpu_debug_linear_solve"]
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the engine library (no fallback: raises when it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise NativeError(f"engine library not built: {path} (run olf-gpu_b200/build.py)")
+    L = ctypes.CDLL(path)
+    L.olfgpu_last_error.restype = ctypes.c_char_p
+    L.olfgpu_create_structure.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _ip, ctypes.c_int, _dp, _ip, ctypes.c_int,
+                                          _dp, _ip, ctypes.c_int, _ip, ctypes.c_int, ctypes.POINTER(_i64)]
+    L.olfgpu_destroy_structure.argtypes = [_i64]
+    L.olfgpu_structure_info.argtypes = [_i64, _ip, ctypes.POINTER(_i64)]
+    L.olfgpu_structure_export.argtypes = [_i64, _ip, _ip, _ip, _ip, _ip, _ip, _ip]
+    L.olfgpu_recommend_batch_size.argtypes = [_i64, ctypes.c_int, ctypes.c_int, _ip]
+    L.olfgpu_create_batch_context.argtypes = [_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _dp, _dp, _dp, _dp,
+                                              _dp, _ip, _dp, _ip, ctypes.POINTER(_i64)]
+    L.olfgpu_destroy_batch_context.argtypes = [_i64]
+    L.olfgpu_set_linear_solver_settings.argtypes = [_i64, ctypes.c_int, ctypes.c_int]
+    L.olfgpu_solve_batch_context.argtypes = [_i64, _dp, _dp, _dp, _ip, ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int,
+                                             _u8p, ctypes.c_int, _ip, _dp, ctypes.c_int, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp]
+    L.olfgpu_last_solve_stats.argtypes = [_i64, _fp, _ip, _ip]
+    L.olfgpu_debug_fill.argtypes = [_i64, _dp, _dp, _ip, _u8p, _dp, _dp]
+    L.olfgpu_debug_linear_solve.argtypes = [_i64, _dp, _dp, ctypes.c_int, _dp]
+    for name in EXPORTS:
+        getattr(L, name).restype = ctypes.c_char_p if name == "olfgpu_last_error" else ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise NativeError(load().olfgpu_last_error().decode())
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _p(a):
+    if a is None:
+        return None
+    if a.dtype == np.float64:
+        return a.ctypes.data_as(_dp)
+    if a.dtype == np.int32:
+        return a.ctypes.data_as(_ip)
+    if a.dtype == np.uint8:
+        return a.ctypes.data_as(_u8p)
+    if a.dtype == np.float32:
+        return a.ctypes.data_as(_fp)
+    raise TypeError(a.dtype)
+
+
+class Structure:
+    """StructureNative: the shared structure built once per packed network."""
+
+    def __init__(self, packed, ordering: int = 0):
+        L = load()
+        self.packed = packed
+        keep = [_c(packed.cb_params, np.float64), _c(packed.cb_idx, np.int32), _c(packed.ob_params, np.float64),
+                _c(packed.ob_idx, np.int32), _c(packed.sh_params, np.float64), _c(packed.sh_idx, np.int32),
+                _c(packed.identity_rows, np.int32)]
+        h = _i64(0)
+        _check(L.olfgpu_create_structure(packed.n, packed.n_cb, _p(keep[0]), _p(keep[1]), packed.n_ob, _p(keep[2]),
+                                         _p(keep[3]), packed.n_sh, _p(keep[4]), _p(keep[5]), keep[6].shape[0],
+                                         _p(keep[6]), ordering, ctypes.byref(h)))
+        self.handle = h.value
+        info = np.zeros(9, np.int32)
+        ops = _i64(0)
+        _check(L.olfgpu_structure_info(self.handle, _p(info), ctypes.byref(ops)))
+        (self.n, self.nnz, self.n_bus, self.n_lu_blocks, self.factor_levels, self.forward_levels,
+         self.backward_levels, self.n_elements, self.n_a_blocks) = [int(v) for v in info]
+        self.block_ops = int(ops.value)
+
+    def close(self):
+        if getattr(self, "handle", 0):
+            load().olfgpu_destroy_structure(self.handle)
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def export(self):
+        p = self.packed
+        out = dict(row_map=np.zeros(self.n, np.int32), row_ptr=np.zeros(self.n + 1, np.int32),
+                   col_idx=np.zeros(self.nnz, np.int32), diag_pos=np.zeros(self.n, np.int32),
+                   cb_dest=np.zeros(p.n_cb * 28, np.int32), ob_dest=np.zeros(p.n_ob * 8, np.int32),
+                   sh_dest=np.zeros(p.n_sh * 5, np.int32))
+        _check(load().olfgpu_structure_export(self.handle, *[_p(out[k]) for k in (
+            "row_map", "row_ptr", "col_idx", "diag_pos", "cb_dest", "ob_dest", "sh_dest")]))
+        return out
+
+    def recommend_batch_size(self, max_cap: int, mode: int = BATCHED_LU) -> int:
+        b = ctypes.c_int(0)
+        _check(load().olfgpu_recommend_batch_size(self.handle, max_cap, mode, ctypes.byref(b)))
+        return int(b.value)
+
+    @property
+    def lu_bytes_per_scenario(self) -> int:
+        return self.n_lu_blocks * 4 * 8
+
+
+class BatchContext:
+    """BatchSolveNative: a bank of ``n_scenarios`` lanes on one structure."""
+
+    def __init__(self, structure: Structure, n_scenarios: int, mode: int = BATCHED_LU, rl=None):
+        L = load()
+        self.structure = structure
+        self.n_scenarios = n_scenarios
+        h = _i64(0)
+        if rl is not None:
+            self._rl = [_c(rl.voltage_row, np.int32), _c(rl.min_q, np.float64), _c(rl.max_q, np.float64),
+                        _c(rl.load_q, np.float64), _c(rl.target_v, np.float64), _c(rl.nom_v, np.float64),
+                        _c(rl.p_row, np.int32), _c(rl.static_p, np.float64), _c(rl.id_rank, np.int32)]
+            r = self._rl
+            _check(L.olfgpu_create_batch_context(structure.handle, n_scenarios, mode, r[0].shape[0], *[_p(a) for a in r],
+                                                 ctypes.byref(h)))
+        else:
+            _check(L.olfgpu_create_batch_context(structure.handle, n_scenarios, mode, 0, None, None, None, None, None,
+                                                 None, None, None, None, ctypes.byref(h)))
+        self.handle = h.value
+
+    def close(self):
+        if getattr(self, "handle", 0):
+            load().olfgpu_destroy_batch_context(self.handle)
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_linear_solver_settings(self, precision: int = FP64, refinement_steps: int = 1):
+        _check(load().olfgpu_set_linear_solver_settings(self.handle, precision, refinement_steps))
+
+    def solve(self, x0_base, target_base, base_row_mode, disabled, x0_full=None, row_mode_entries=None,
+              target_override_index=None, target_override_value=None, max_iter: int = 15, tol: float = 1e-8,
+              reactive_limit_tol: float = 1e-4, max_outer: int = 20, max_pq_pv_switch: int = 3,
+              out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Per scenario [x(n), iterations, ||F||inf, status] (BatchSolveNative.solveBatchContext)."""
+        n = self.structure.n
+        disabled = _c(disabled, np.uint8)
+        ns = disabled.shape[0]
+        x0b = None if x0_base is None else _c(x0_base, np.float64)
+        x0f = None if x0_full is None else _c(x0_full, np.float64)
+        tb = _c(target_base, np.float64)
+        bm = _c(base_row_mode, np.int32)
+        rme = _c(np.zeros(0) if row_mode_entries is None else row_mode_entries, np.int32).reshape(-1)
+        toi = _c(np.zeros(0) if target_override_index is None else target_override_index, np.int32)
+        tov = _c(np.zeros(0) if target_override_value is None else target_override_value, np.float64)
+        if out is None:
+            out = np.zeros((ns, n + 3))
+        _check(load().olfgpu_solve_batch_context(
+            self.handle, _p(x0b), _p(x0f), _p(tb), _p(bm), rme.shape[0] // 3, _p(rme) if rme.size else None, ns,
+            disabled.shape[1], _p(disabled), toi.shape[0], _p(toi) if toi.size else None,
+            _p(tov) if tov.size else None, max_iter, tol, reactive_limit_tol, max_outer, max_pq_pv_switch, _p(out)))
+        return out
+
+    def last_stats(self):
+        ms = ctypes.c_float(0)
+        it = ctypes.c_int(0)
+        tot = np.zeros(self.n_scenarios, np.int32)
+        _check(load().olfgpu_last_solve_stats(self.handle, ctypes.byref(ms), ctypes.byref(it), _p(tot)))
+        return float(ms.value), int(it.value), tot
+
+    def debug_fill(self, x_full, target_base, base_row_mode, disabled):
+        s = self.structure
+        ns = self.n_scenarios
+        J = np.zeros((ns, s.nnz))
+        F = np.zeros((ns, s.n))
+        xf, tb, bm, dis = (_c(x_full, np.float64), _c(target_base, np.float64), _c(base_row_mode, np.int32),
+                           _c(disabled, np.uint8))
+        _check(load().olfgpu_debug_fill(self.handle, _p(xf), _p(tb), _p(bm), _p(dis), _p(J), _p(F)))
+        return J, F
+
+    def debug_linear_solve(self, csr_vals, rhs, precision: int = FP64):
+        s = self.structure
+        out = np.zeros((self.n_scenarios, s.n))
+        v, r = _c(csr_vals, np.float64), _c(rhs, np.float64)
+        _check(load().olfgpu_debug_linear_solve(self.handle, _p(v), _p(r), precision, _p(out)))
+        return out

@@ -1,0 +1,215 @@
+"""Parity of the CUDA engine with the oracle, through the C ABI (needs a B200)."""
+import numpy as np
+import pytest
+
+from conftest import grid
+
+pytestmark = pytest.mark.gpu
+
+# converged states must agree within 1e-8 pu / rad, statuses exactly
+STATE_TOL = 1e-8
+
+
+def _perturbed_states(p, ns, seed, scale=0.05):
+    rng = np.random.default_rng(seed)
+    x0 = p.x_base if p.x_base is not None else p.x_flat
+    x = np.tile(x0, (ns, 1))
+    x[:, 0::2] += rng.uniform(-scale, scale, (ns, p.n_bus))
+    x[:, 1::2] += rng.uniform(-scale, scale, (ns, p.n_bus))
+    return x
+
+
+@pytest.mark.parametrize("name", ["grid118", "grid2000"])
+def test_fill_matches_oracle(engine_lib, oracle_mod, name):
+    from olfgpu import native, synthetic
+    g, p = grid(name)
+    ns = 40
+    s = native.Structure(p)
+    ctx = native.BatchContext(s, ns)
+    x = _perturbed_states(p, ns, 1)
+    outs = synthetic.draw_outages(g, ns, seed=7)
+    dis = p.outage_masks(outs)
+    J, F = ctx.debug_fill(x, p.target, p.base_row_mode, dis)
+    st = oracle_mod.Structure(p)
+    for k in range(ns):
+        Jo, Fo = st.fill(x[k], p.target, p.base_row_mode, dis[k])
+        scale = np.maximum(np.abs(Jo), 1.0)
+        assert np.max(np.abs(J[k] - Jo) / scale) < 1e-12
+        assert np.max(np.abs(F[k] - Fo)) < 1e-10
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-9), (1, 2e-3)])
+def test_linear_solve_matches_oracle(engine_lib, oracle_mod, precision, tol):
+    from olfgpu import native
+    g, p = grid("grid2000")
+    ns = 36
+    s = native.Structure(p)
+    ctx = native.BatchContext(s, ns)
+    x = _perturbed_states(p, ns, 2, 0.02)
+    st = oracle_mod.Structure(p)
+    zero = np.zeros(p.n_elements, np.uint8)
+    J = np.stack([st.fill(x[k], p.target, p.base_row_mode, zero)[0] for k in range(ns)])
+    rng = np.random.default_rng(3)
+    rhs = rng.standard_normal((ns, p.n))
+    z = ctx.debug_linear_solve(J, rhs, precision)
+    for k in range(ns):
+        zo = st.linear_solve(J[k], rhs[k])
+        assert np.max(np.abs(z[k] - zo)) / np.max(np.abs(zo)) < tol
+
+
+def _compare(res, ref, n):
+    st_e = res[:, n + 2].astype(int)
+    st_o = ref[:, n + 2].astype(int)
+    assert np.array_equal(st_e, st_o), f"status mismatch at {np.flatnonzero(st_e != st_o)[:10]}"
+    conv = st_o == 0
+    if conv.any():
+        d = np.max(np.abs(res[conv, :n] - ref[conv, :n]))
+        assert d <= STATE_TOL, d
+    return st_o
+
+
+@pytest.mark.parametrize("name,count", [("grid118", None), ("grid2000", 600)])
+def test_n1_fp64_matches_oracle(engine_lib, oracle_mod, name, count):
+    from olfgpu import native, synthetic
+    from olfgpu.security_analysis import SecurityAnalysis
+    g, p = grid(name)
+    outs = synthetic.draw_outages(g, count, seed=11)
+    sa = SecurityAnalysis(p, precision=native.FP64)
+    r = sa.solve_n1(outs)
+    st = oracle_mod.Structure(p)
+    ref = st.solve_batch(p.x_base, p.outage_masks(outs))
+    out = np.concatenate([r.x, r.iterations[:, None], r.norm[:, None], r.status[:, None]], axis=1)
+    status = _compare(out, ref, p.n)
+    assert (status == 0).mean() > 0.9
+    assert np.array_equal(r.iterations[status == 0], ref[status == 0, p.n].astype(int))
+
+
+def test_n1_9241_subset_matches_oracle(engine_lib, oracle_mod):
+    from olfgpu import native, synthetic
+    from olfgpu.security_analysis import SecurityAnalysis
+    g, p = grid("grid9241")
+    outs = synthetic.draw_outages(g, 500, seed=9241)[:48]
+    sa = SecurityAnalysis(p, precision=native.FP64)
+    r = sa.solve_n1(outs)
+    ref = oracle_mod.Structure(p).solve_batch(p.x_base, p.outage_masks(outs))
+    out = np.concatenate([r.x, r.iterations[:, None], r.norm[:, None], r.status[:, None]], axis=1)
+    _compare(out, ref, p.n)
+
+
+@pytest.mark.parametrize("steps", [1, 2])
+def test_n1_mixed_precision_matches_fp64_oracle(engine_lib, oracle_mod, steps):
+    from olfgpu import native, synthetic
+    from olfgpu.security_analysis import SecurityAnalysis
+    g, p = grid("grid2000")
+    outs = synthetic.draw_outages(g, 300, seed=12)
+    sa = SecurityAnalysis(p, precision=native.MIXED, refinement_steps=steps)
+    r = sa.solve_n1(outs)
+    ref = oracle_mod.Structure(p).solve_batch(p.x_base, p.outage_masks(outs))
+    out = np.concatenate([r.x, r.iterations[:, None], r.norm[:, None], r.status[:, None]], axis=1)
+    _compare(out, ref, p.n)
+
+
+def test_replicated_scenarios_equal_single_solve(engine_lib):
+    """GpuBatchedN1Test.java:80-131: K identical scenarios match the single solve to 1e-12."""
+    from olfgpu import native
+    g, p = grid("grid118")
+    s = native.Structure(p)
+    one = native.BatchContext(s, 1).solve(p.x_flat, p.target, p.base_row_mode, np.zeros((1, p.n_elements), np.uint8))
+    many = native.BatchContext(s, 8).solve(p.x_flat, p.target, p.base_row_mode, np.zeros((8, p.n_elements), np.uint8))
+    assert one[0, -1] == 0
+    assert np.max(np.abs(many - one[0])) <= 1e-12
+
+
+def test_disabled_mask_changes_result(engine_lib):
+    """GpuBatchedN1Test.java:134-183: a scenario with a disabled branch differs from the base."""
+    from olfgpu import native, synthetic
+    g, p = grid("grid118")
+    s = native.Structure(p)
+    outs = synthetic.outage_candidates(g)[:2]
+    dis = np.zeros((3, p.n_elements), np.uint8)
+    dis[1, outs[0]] = 1
+    dis[2, outs[1]] = 1
+    r = native.BatchContext(s, 3).solve(p.x_base, p.target, p.base_row_mode, dis)
+    assert np.all(r[:, -1] == 0)
+    assert np.max(np.abs(r[1, :p.n] - r[0, :p.n])) > 1e-6
+    assert np.max(np.abs(r[2, :p.n] - r[0, :p.n])) > 1e-6
+
+
+def test_nan_lane_diverges_alone(engine_lib):
+    """A non-finite mismatch retires only its lane (newton_iteration.cu:344-351); the others are bit-identical."""
+    from olfgpu import native, synthetic
+    g, p = grid("grid118")
+    s = native.Structure(p)
+    outs = synthetic.outage_candidates(g)[:5]
+    dis = p.outage_masks(outs)
+    ctx = native.BatchContext(s, 5)
+    clean = ctx.solve(p.x_base, p.target, p.base_row_mode, dis).copy()
+    row = int(np.flatnonzero(p.base_row_mode == 1)[0])
+    bad = ctx.solve(p.x_base, p.target, p.base_row_mode, dis, target_override_index=np.array([2 * p.n + row]),
+                    target_override_value=np.array([np.nan]))
+    assert bad[2, -1] == native.DIVERGED
+    keep = [0, 1, 3, 4]
+    assert np.array_equal(bad[keep], clean[keep])
+
+
+def test_iteration_budget_statuses(engine_lib, oracle_mod):
+    from olfgpu import native
+    g, p = grid("grid118")
+    s = native.Structure(p)
+    dis = np.zeros((1, p.n_elements), np.uint8)
+    ctx = native.BatchContext(s, 1)
+    full = ctx.solve(p.x_flat, p.target, p.base_row_mode, dis)
+    it = int(full[0, -3])
+    for budget in (1, it - 1, it, it + 1):
+        e = ctx.solve(p.x_flat, p.target, p.base_row_mode, dis, max_iter=budget)
+        o = oracle_mod.Structure(p).solve_batch(p.x_flat, dis, max_iter=budget)
+        assert e[0, -1] == o[0, -1], budget
+        assert e[0, -3] == o[0, -3], budget
+
+
+def test_per_scenario_start_and_ragged_batch(engine_lib, oracle_mod):
+    from olfgpu import native, synthetic
+    g, p = grid("grid118")
+    s = native.Structure(p)
+    ns = 37
+    outs = synthetic.outage_candidates(g)[:ns]
+    dis = p.outage_masks(outs)
+    x0 = _perturbed_states(p, ns, 5, 0.01)
+    r = native.BatchContext(s, ns).solve(None, p.target, p.base_row_mode, dis, x0_full=x0)
+    ref = oracle_mod.Structure(p).solve_batch(x0, dis)
+    _compare(r, ref, p.n)
+
+
+def test_row_mode_entries_switch_a_pv_bus(engine_lib, oracle_mod):
+    from olfgpu import native
+    g, p = grid("grid118")
+    s = native.Structure(p)
+    pv_rows = np.flatnonzero((p.base_row_mode == 0) & (np.arange(p.n) % 2 == 1))
+    row = int(pv_rows[1])
+    ns = 2
+    dis = np.zeros((ns, p.n_elements), np.uint8)
+    r = native.BatchContext(s, ns).solve(p.x_base, p.target, p.base_row_mode, dis,
+                                          row_mode_entries=np.array([[1, row, 1]]),
+                                          target_override_index=np.array([1 * p.n + row]),
+                                          target_override_value=np.array([0.05]))
+    mode = p.base_row_mode.copy()
+    mode[row] = 1
+    t = p.target.copy()
+    t[row] = 0.05
+    ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis[1:], target=t, mode=mode)
+    _compare(r[1:], ref, p.n)
+
+
+def test_reactive_limits_match_oracle(engine_lib, oracle_mod):
+    from olfgpu import native, synthetic
+    from olfgpu.security_analysis import SecurityAnalysis
+    g, p = grid("grid300")
+    outs = synthetic.draw_outages(g, 120, seed=300)
+    sa = SecurityAnalysis(p, precision=native.FP64, reactive_limits=True)
+    r = sa.solve_n1(outs)
+    ref = oracle_mod.Structure(p).solve_batch(p.x_base, p.outage_masks(outs), reactive_limits=True)
+    out = np.concatenate([r.x, r.iterations[:, None], r.norm[:, None], r.status[:, None]], axis=1)
+    _compare(out, ref, p.n)
+    # the limits actually bind somewhere
+    plain = oracle_mod.Structure(p).solve_batch(p.x_base, p.outage_masks(outs))
+    assert np.max(np.abs(plain[:, :p.n] - ref[:, :p.n])) > 1e-4
