@@ -85,6 +85,21 @@ int olfgpu_destroy_batch_context(int64_t context);
 int olfgpu_set_linear_solver_settings(int64_t context, int precision, int refinementSteps);
 
 /*
+ * Schedule of the Newton iterations (no counterpart in the reference, which launches per dependency step and per
+ * level and reads norms back every iteration): schedule 0 launches one kernel per wide dependency level over all
+ * lanes and the narrow levels (<= 48 tasks) of each phase in one launch of tiles of lanesPerTile (1, 2 or 4; 0: one
+ * launch per level throughout), captured as one CUDA graph per Newton iteration; schedule 1 runs the whole Newton
+ * loop in one persistent launch, one CTA per tile of lanesPerTile (1, 2, 4 or 8) lanes with `threads` (256 or 512)
+ * threads; schedule -1 lets the next solve time every
+ * candidate on its batch and keep the fastest (the autotuner).  olfgpu_get_schedule reports the schedule in force
+ * and, after an autotuned solve, up to maxResults timings {schedule, lanesPerTile, threads, ms} into results
+ * (nResults receives their count).
+ */
+int olfgpu_set_schedule(int64_t context, int schedule, int lanesPerTile, int threads);
+int olfgpu_get_schedule(int64_t context, int* schedule, int* lanesPerTile, int* threads, int maxResults,
+                        double* results, int* nResults);
+
+/*
  * BatchSolveNative.solveBatchContext (batch_solve_jni.cu:84-394; BatchSolveNative.java:106-125).
  *   x0Base [n]: the start state of every scenario (ignored where x0Full is given), x0Full [nScenarios][n] or null;
  *   targetBase [n], baseRowMode [n]; rowModeEntries (scenario, row, mode) triples; disabled [nScenarios][nElements]

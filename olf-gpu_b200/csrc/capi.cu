@@ -2,6 +2,7 @@
 // it through olfgpu_last_error(), the way the reference's JNI layer turns native failures into RuntimeExceptions.
 #include "../../include/olfgpu_b200.h"
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -149,6 +150,50 @@ extern "C" int olfgpu_set_linear_solver_settings(int64_t context, int precision,
         if (refinementSteps < 0 || refinementSteps > 8) throw std::runtime_error("refinementSteps must be in [0, 8]");
         c.precision = precision;
         c.refinementSteps = refinementSteps;
+    });
+}
+
+extern "C" int olfgpu_set_schedule(int64_t context, int schedule, int lanesPerTile, int threads) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        if (schedule == -1) {
+            c.autotunePending = true;
+            return;
+        }
+        if (schedule != SCHEDULE_LEVELS && schedule != SCHEDULE_PERSISTENT) throw std::runtime_error("unknown schedule");
+        if (schedule == SCHEDULE_LEVELS) {
+            if (lanesPerTile != 0 && lanesPerTile != 1 && lanesPerTile != 2 && lanesPerTile != 4) {
+                throw std::runtime_error("level schedule: lanesPerTile of the narrow levels must be 0, 1, 2 or 4");
+            }
+            c.narrowLanes = lanesPerTile;
+        } else {
+            if (lanesPerTile != 1 && lanesPerTile != 2 && lanesPerTile != 4 && lanesPerTile != 8) {
+                throw std::runtime_error("lanesPerTile must be 1, 2, 4 or 8");
+            }
+            if (threads != 256 && threads != 512) throw std::runtime_error("threads must be 256 or 512");
+            c.lanesPerTile = lanesPerTile;
+            c.threads = threads;
+        }
+        c.schedule = schedule;
+        c.autotunePending = false;
+    });
+}
+
+extern "C" int olfgpu_get_schedule(int64_t context, int* schedule, int* lanesPerTile, int* threads, int maxResults,
+                                   double* results, int* nResults) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        if (schedule) *schedule = c.schedule;
+        if (lanesPerTile) *lanesPerTile = c.schedule == SCHEDULE_LEVELS ? c.narrowLanes : c.lanesPerTile;
+        if (threads) *threads = c.threads;
+        const int k = std::min<int>(maxResults, static_cast<int>(c.tuning.size()));
+        for (int i = 0; results && i < k; i++) {
+            results[4 * i] = c.tuning[i].schedule;
+            results[4 * i + 1] = c.tuning[i].lanesPerTile;
+            results[4 * i + 2] = c.tuning[i].threads;
+            results[4 * i + 3] = c.tuning[i].ms;
+        }
+        if (nResults) *nResults = static_cast<int>(c.tuning.size());
     });
 }
 

@@ -150,6 +150,50 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
         for (int q = p.fwdLevelPtr[l]; q < p.fwdLevelPtr[l + 1]; q++) m = std::max(m, lrowLen[p.fwdLevelPos[q]]);
         d->fwdSplit[l] = splitOf(m);
     }
+    // longest update list per level (the persistent kernel sizes its per-level split from it)
+    std::vector<int> levelLongest(p.levelPtr.size() - 1, 0), fwdLongest(p.fwdLevelPtr.size() - 1, 0),
+        bwdLongest(p.bwdLevelPtr.size() - 1, 0);
+    for (size_t l = 0; l + 1 < p.levelPtr.size(); l++)
+        for (int q = p.levelPtr[l]; q < p.levelPtr[l + 1]; q++) {
+            const int t = p.levelTask[q];
+            levelLongest[l] = std::max(levelLongest[l], p.opPtr[t + 1] - p.opPtr[t]);
+        }
+    for (size_t l = 0; l + 1 < p.fwdLevelPtr.size(); l++)
+        for (int q = p.fwdLevelPtr[l]; q < p.fwdLevelPtr[l + 1]; q++)
+            fwdLongest[l] = std::max(fwdLongest[l], lrowLen[p.fwdLevelPos[q]]);
+    for (size_t l = 0; l + 1 < p.bwdLevelPtr.size(); l++)
+        for (int q = p.bwdLevelPtr[l]; q < p.bwdLevelPtr[l + 1]; q++) {
+            const int i = p.bwdLevelPos[q];
+            bwdLongest[l] = std::max(bwdLongest[l], p.uPtr[i + 1] - p.uPtr[i] - 1);
+        }
+    d->levelPtrD.upload(p.levelPtr);
+    d->levelLongestD.upload(levelLongest);
+    d->fwdPtrD.upload(p.fwdLevelPtr);
+    d->fwdLongestD.upload(fwdLongest);
+    d->bwdPtrD.upload(p.bwdLevelPtr);
+    d->bwdLongestD.upload(bwdLongest);
+    d->persistent.nLevels = static_cast<int>(p.levelPtr.size()) - 1;
+    d->persistent.nFwd = static_cast<int>(p.fwdLevelPtr.size()) - 1;
+    d->persistent.nBwd = static_cast<int>(p.bwdLevelPtr.size()) - 1;
+    d->persistent.levelPtr = d->levelPtrD.as<int>();
+    d->persistent.levelLongest = d->levelLongestD.as<int>();
+    d->persistent.fwdPtr = d->fwdPtrD.as<int>();
+    d->persistent.fwdLongest = d->fwdLongestD.as<int>();
+    d->persistent.fwdPos = d->fwdPos.as<int>();
+    d->persistent.bwdPtr = d->bwdPtrD.as<int>();
+    d->persistent.bwdLongest = d->bwdLongestD.as<int>();
+    d->persistent.bwdPos = d->bwdPos.as<int>();
+    // the narrow levels: the factorization / forward tail and the backward head whose levels hold <= NARROW tasks
+    constexpr int NARROW = 48;
+    auto countOf = [](const std::vector<int>& ptr, size_t l) { return ptr[l + 1] - ptr[l]; };
+    d->factorFrom = static_cast<int>(p.levelPtr.size()) - 1;
+    while (d->factorFrom > 0 && countOf(p.levelPtr, d->factorFrom - 1) <= NARROW) d->factorFrom--;
+    d->fwdFrom = static_cast<int>(p.fwdLevelPtr.size()) - 1;
+    while (d->fwdFrom > 0 && countOf(p.fwdLevelPtr, d->fwdFrom - 1) <= NARROW) d->fwdFrom--;
+    d->bwdUntil = 0;
+    while (d->bwdUntil < static_cast<int>(p.bwdLevelPtr.size()) - 1 && countOf(p.bwdLevelPtr, d->bwdUntil) <= NARROW) {
+        d->bwdUntil++;
+    }
     d->bwdSplit.assign(p.bwdLevelPtr.size() - 1, 1);
     for (size_t l = 0; l + 1 < p.bwdLevelPtr.size(); l++) {
         int m = 0;
@@ -453,7 +497,8 @@ void outageBits(BatchContext& ctx, const unsigned char* disabled, int nS, int nE
 }
 
 void captureIteration(BatchContext& ctx) {
-    const int key = ctx.precision * 1000 + ctx.refinementSteps * 10 + (ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits ? 1 : 0);
+    const int key = ctx.narrowLanes * 100000 + ctx.precision * 1000 + ctx.refinementSteps * 10 +
+                    (ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits ? 1 : 0);
     if (ctx.graph && ctx.graphKey == key) return;
     if (ctx.graph) {
         cudaGraphExecDestroy(ctx.graph);
@@ -472,13 +517,15 @@ void captureIteration(BatchContext& ctx) {
     launchFill(net, b, true, rl, ctx.stream);
     launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, ctx.stream);
     if (rl) launchReactiveLimits(net, b, ctx.rl, ctx.cfg, ctx.stream);
-    launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, mixed,
+    const Hybrid hy = ctx.hybrid();
+    const Hybrid* hp = ctx.narrowLanes > 0 ? &hy : nullptr;
+    launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, mixed, hp,
                  ctx.stream);
-    launchSolve(net, b, dn.fwd(), dn.bwd(), mixed, false, ctx.stream);
+    launchSolve(net, b, dn.fwd(), dn.bwd(), mixed, false, hp, ctx.stream);
     if (mixed) {
         for (int k = 0; k < ctx.refinementSteps; k++) {
             launchResidual(net, b, ctx.stream);
-            launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, ctx.stream);
+            launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, ctx.stream);
         }
     }
     launchStep(net, b, false, ctx.stream);
@@ -505,14 +552,17 @@ void phaseTimedIteration(BatchContext& ctx, int k) {
     launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, st);
     if (rl) launchReactiveLimits(net, b, ctx.rl, ctx.cfg, st);
     OLF_CUDA(cudaEventRecord(ev[2], st));
-    launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, mixed, st);
+    const Hybrid hy = ctx.hybrid();
+    const Hybrid* hp = ctx.narrowLanes > 0 ? &hy : nullptr;
+    launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, mixed, hp,
+                 st);
     OLF_CUDA(cudaEventRecord(ev[3], st));
-    launchSolve(net, b, dn.fwd(), dn.bwd(), mixed, false, st);
+    launchSolve(net, b, dn.fwd(), dn.bwd(), mixed, false, hp, st);
     OLF_CUDA(cudaEventRecord(ev[4], st));
     if (mixed) {
         for (int r = 0; r < ctx.refinementSteps; r++) {
             launchResidual(net, b, st);
-            launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, st);
+            launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, st);
         }
     }
     OLF_CUDA(cudaEventRecord(ev[5], st));
@@ -528,12 +578,164 @@ void phaseTimedIteration(BatchContext& ctx, int k) {
 
 }  // namespace
 
+namespace {
+
+// Host inputs of a solve copied to the device (staging and persistent override buffers); no kernel runs here.
+void uploadInputs(BatchContext& ctx, const SolveRequest& req) {
+    const int n = ctx.net->host.n;
+    cudaStream_t st = ctx.stream;
+    double* stageX = ctx.stage.as<double>();
+    double* stageT = stageX + n;
+    int* stageM = reinterpret_cast<int*>(stageT + n);
+    ctx.hasX0Base = req.x0Base != nullptr;
+    ctx.hasX0Full = req.x0Full != nullptr;
+    if (req.x0Full) {
+        if (ctx.full.bytes < static_cast<size_t>(ctx.nS) * n * 8) ctx.full.alloc(static_cast<size_t>(ctx.nS) * n * 8);
+        OLF_CUDA(cudaMemcpyAsync(ctx.full.p, req.x0Full, static_cast<size_t>(ctx.nS) * n * 8, cudaMemcpyHostToDevice, st));
+    }
+    if (req.x0Base) OLF_CUDA(cudaMemcpyAsync(stageX, req.x0Base, n * 8, cudaMemcpyHostToDevice, st));
+    OLF_CUDA(cudaMemcpyAsync(stageT, req.targetBase, n * 8, cudaMemcpyHostToDevice, st));
+    OLF_CUDA(cudaMemcpyAsync(stageM, req.baseRowMode, n * 4, cudaMemcpyHostToDevice, st));
+    ctx.nTargetOverrides = req.nTargetOverrides;
+    if (req.nTargetOverrides > 0) {
+        if (ctx.ovIdx.bytes < static_cast<size_t>(req.nTargetOverrides) * 4) {
+            ctx.ovIdx.alloc(req.nTargetOverrides * 4);
+            ctx.ovVal.alloc(req.nTargetOverrides * 8);
+        }
+        OLF_CUDA(cudaMemcpyAsync(ctx.ovIdx.p, req.targetOverrideIndex, req.nTargetOverrides * 4, cudaMemcpyHostToDevice, st));
+        OLF_CUDA(cudaMemcpyAsync(ctx.ovVal.p, req.targetOverrideValue, req.nTargetOverrides * 8, cudaMemcpyHostToDevice, st));
+    }
+    ctx.nRowModeEntries = req.nRowModeEntries;
+    if (req.nRowModeEntries > 0) {
+        if (ctx.rowModeE.bytes < static_cast<size_t>(req.nRowModeEntries) * 12) ctx.rowModeE.alloc(req.nRowModeEntries * 12);
+        OLF_CUDA(cudaMemcpyAsync(ctx.rowModeE.p, req.rowModeEntries, req.nRowModeEntries * 12, cudaMemcpyHostToDevice, st));
+    }
+    outageBits(ctx, req.disabled, ctx.nS, req.nElements);
+}
+
+// Device-side install of the uploaded inputs: every lane gets the base vectors, then the per-scenario overrides; lane
+// state and reactive-limit state reset.  Repeatable (the autotuner reinstalls the same batch for every candidate).
+void installLanes(BatchContext& ctx) {
+    const int n = ctx.net->host.n;
+    const size_t S = ctx.S;
+    cudaStream_t st = ctx.stream;
+    double* stageX = ctx.stage.as<double>();
+    double* stageT = stageX + n;
+    int* stageM = reinterpret_cast<int*>(stageT + n);
+    const unsigned blocksAll = static_cast<unsigned>((static_cast<size_t>(n) * S + 255) / 256);
+    if (ctx.hasX0Base) tileKernel<<<blocksAll, 256, 0, st>>>(stageX, ctx.x.as<double>(), n, ctx.S);
+    if (ctx.hasX0Full) {
+        dim3 blk(32, 8), grd((n + 31) / 32, (ctx.nS + 31) / 32);
+        toLanesKernel<<<grd, blk, 0, st>>>(ctx.full.as<double>(), ctx.x.as<double>(), n, ctx.nS, ctx.S);
+    }
+    tileKernel<<<blocksAll, 256, 0, st>>>(stageT, ctx.target.as<double>(), n, ctx.S);
+    tileModeKernel<<<blocksAll, 256, 0, st>>>(stageM, ctx.mode.as<int8_t>(), n, ctx.S);
+    if (ctx.nTargetOverrides > 0) {
+        targetOverrideKernel<<<(ctx.nTargetOverrides + 255) / 256, 256, 0, st>>>(
+            ctx.ovIdx.as<int>(), ctx.ovVal.as<double>(), ctx.nTargetOverrides, ctx.target.as<double>(), n, ctx.S);
+    }
+    if (ctx.nRowModeEntries > 0) {
+        rowModeOverrideKernel<<<(ctx.nRowModeEntries + 255) / 256, 256, 0, st>>>(ctx.rowModeE.as<int>(),
+                                                                                ctx.nRowModeEntries,
+                                                                                ctx.mode.as<int8_t>(), ctx.S);
+    }
+    laneInitKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(ctx.batch());
+    if (ctx.rl.nRl > 0) {
+        OLF_CUDA(cudaMemsetAsync(ctx.rlLimitType.p, 0, ctx.rlLimitType.bytes, st));
+        OLF_CUDA(cudaMemsetAsync(ctx.rlSwitchCount.p, 0, ctx.rlSwitchCount.bytes, st));
+        OLF_CUDA(cudaMemsetAsync(ctx.rlPassSwitched.p, 0, ctx.rlPassSwitched.bytes, st));
+    }
+}
+
+int roundCap(const BatchContext& ctx) {
+    return ctx.cfg.reactiveLimits ? (ctx.cfg.maxOuter + 1) * (ctx.cfg.maxIter + 1) : ctx.cfg.maxIter + 1;
+}
+
+// The Newton iterations under the context's schedule; returns the batched iterations run (level launches) or 0.
+int runIterations(BatchContext& ctx) {
+    cudaStream_t st = ctx.stream;
+    const DeviceNet& dn = *ctx.net->dev;
+    const bool mixed = ctx.precision == 1;
+    const size_t S = ctx.S;
+    if (mixed && !ctx.lu32.p) ctx.lu32.alloc(static_cast<size_t>(dn.view.nLu) * 4 * S * 4);
+    if (!mixed && !ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(dn.view.nLu) * 4 * S * 8);
+    const int cap = roundCap(ctx);
+    if (ctx.schedule == SCHEDULE_PERSISTENT) {
+        PersistentPlan plan = dn.persistent;
+        plan.maxRounds = cap;
+        launchPersistent(dn.view, ctx.batch(), ctx.rl, ctx.cfg, plan, ctx.lanesPerTile, ctx.threads, mixed, st);
+        OLF_CUDA(cudaGetLastError());
+        return 0;
+    }
+    captureIteration(ctx);
+    static const bool phaseTime = std::getenv("OLFGPU_PHASE_TIME") != nullptr;
+    int k = 0;
+    for (; k < cap; k++) {
+        if (phaseTime) phaseTimedIteration(ctx, k);
+        else OLF_CUDA(cudaGraphLaunch(ctx.graph, st));
+        OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 4, cudaMemcpyDeviceToHost, st));
+        OLF_CUDA(cudaStreamSynchronize(st));
+        if (*ctx.hostActive <= 0) {
+            k++;
+            break;
+        }
+    }
+    capKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(ctx.batch());
+    return k;
+}
+
+// Times every candidate schedule on the installed batch and keeps the fastest (the batch is reinstalled before each).
+void autotune(BatchContext& ctx) {
+    struct Candidate { int schedule, lanes, threads; };
+    std::vector<Candidate> cands;
+    for (int narrow : {0, 1, 2, 4}) cands.push_back({SCHEDULE_LEVELS, narrow, 256});
+    for (int lanes : {2, 4})
+        for (int threads : {256, 512}) cands.push_back({SCHEDULE_PERSISTENT, lanes, threads});
+    cudaEvent_t e0, e1;
+    OLF_CUDA(cudaEventCreate(&e0));
+    OLF_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    Candidate pick = cands[0];
+    ctx.tuning.clear();
+    for (const Candidate& c : cands) {
+        ctx.schedule = c.schedule;
+        if (c.schedule == SCHEDULE_LEVELS) {
+            ctx.narrowLanes = c.lanes;
+        } else {
+            ctx.lanesPerTile = c.lanes;
+            ctx.threads = c.threads;
+        }
+        installLanes(ctx);
+        OLF_CUDA(cudaEventRecord(e0, ctx.stream));
+        runIterations(ctx);
+        OLF_CUDA(cudaEventRecord(e1, ctx.stream));
+        OLF_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        OLF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        ctx.tuning.push_back({c.schedule, c.lanes, c.threads, ms});
+        if (ms < best) {
+            best = ms;
+            pick = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx.schedule = pick.schedule;
+    if (pick.schedule == SCHEDULE_LEVELS) {
+        ctx.narrowLanes = pick.lanes;
+    } else {
+        ctx.lanesPerTile = pick.lanes;
+        ctx.threads = pick.threads;
+    }
+    ctx.autotunePending = false;
+}
+
+}  // namespace
+
 void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out) {
     OLF_CUDA(cudaSetDevice(ctx.device));
     const Structure& s = ctx.net->host;
-    const DevNet& net = ctx.net->dev->view;
     const int n = s.n;
-    const size_t S = ctx.S;
     if (req.nScenarios != ctx.nS) {
         throw std::runtime_error("scenario count " + std::to_string(req.nScenarios) + " does not match the context's " +
                                  std::to_string(ctx.nS));
@@ -561,92 +763,30 @@ void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out) {
             throw std::runtime_error("target override index out of range");
         }
     }
-    ctx.cfg.maxIter = req.maxIter;
-    ctx.cfg.tol = req.tol;
-    ctx.cfg.rlTol = req.reactiveLimitTol;
-    ctx.cfg.maxOuter = req.maxOuter;
-    ctx.cfg.maxSwitch = req.maxPqPvSwitch;
-    ctx.cfg.reactiveLimits = ctx.rl.nRl > 0 ? 1 : 0;
-    ctx.cfg.mixed = ctx.precision;
-    ctx.cfg.refinementSteps = ctx.refinementSteps;
-    // the iteration graph bakes the settings in: recapture whenever they change
-    if (ctx.graph) {
+    Settings cfg = ctx.cfg;
+    cfg.maxIter = req.maxIter;
+    cfg.tol = req.tol;
+    cfg.rlTol = req.reactiveLimitTol;
+    cfg.maxOuter = req.maxOuter;
+    cfg.maxSwitch = req.maxPqPvSwitch;
+    cfg.reactiveLimits = ctx.rl.nRl > 0 ? 1 : 0;
+    cfg.mixed = ctx.precision;
+    cfg.refinementSteps = ctx.refinementSteps;
+    if (std::memcmp(&cfg, &ctx.cfg, sizeof(Settings)) != 0 && ctx.graph) {
+        // the level-launch graph bakes the settings in
         cudaGraphExecDestroy(ctx.graph);
         ctx.graph = nullptr;
     }
-    captureIteration(ctx);
+    ctx.cfg = cfg;
     cudaStream_t st = ctx.stream;
+    uploadInputs(ctx, req);
+    if (ctx.autotunePending) autotune(ctx);
     cudaEvent_t e0, e1;
     OLF_CUDA(cudaEventCreate(&e0));
     OLF_CUDA(cudaEventCreate(&e1));
-    // ---- install: host inputs copied first, then (timed) tiled to every lane with the per-scenario overrides ----
-    double* stageX = ctx.stage.as<double>();
-    double* stageT = stageX + n;
-    int* stageM = reinterpret_cast<int*>(stageT + n);
-    const unsigned blocksAll = static_cast<unsigned>((static_cast<size_t>(n) * S + 255) / 256);
-    if (req.x0Full) {
-        if (ctx.full.bytes < static_cast<size_t>(ctx.nS) * n * 8) ctx.full.alloc(static_cast<size_t>(ctx.nS) * n * 8);
-        OLF_CUDA(cudaMemcpyAsync(ctx.full.p, req.x0Full, static_cast<size_t>(ctx.nS) * n * 8, cudaMemcpyHostToDevice, st));
-    }
-    if (req.x0Base) OLF_CUDA(cudaMemcpyAsync(stageX, req.x0Base, n * 8, cudaMemcpyHostToDevice, st));
-    OLF_CUDA(cudaMemcpyAsync(stageT, req.targetBase, n * 8, cudaMemcpyHostToDevice, st));
-    OLF_CUDA(cudaMemcpyAsync(stageM, req.baseRowMode, n * 4, cudaMemcpyHostToDevice, st));
-    DeviceBuffer ovIdx, ovVal, rmE;
-    if (req.nTargetOverrides > 0) {
-        ovIdx.alloc(req.nTargetOverrides * 4);
-        ovVal.alloc(req.nTargetOverrides * 8);
-        OLF_CUDA(cudaMemcpyAsync(ovIdx.p, req.targetOverrideIndex, req.nTargetOverrides * 4, cudaMemcpyHostToDevice, st));
-        OLF_CUDA(cudaMemcpyAsync(ovVal.p, req.targetOverrideValue, req.nTargetOverrides * 8, cudaMemcpyHostToDevice, st));
-    }
-    if (req.nRowModeEntries > 0) {
-        rmE.alloc(req.nRowModeEntries * 12);
-        OLF_CUDA(cudaMemcpyAsync(rmE.p, req.rowModeEntries, req.nRowModeEntries * 12, cudaMemcpyHostToDevice, st));
-    }
-    outageBits(ctx, req.disabled, ctx.nS, req.nElements);
     OLF_CUDA(cudaEventRecord(e0, st));
-    if (req.x0Base) tileKernel<<<blocksAll, 256, 0, st>>>(stageX, ctx.x.as<double>(), n, ctx.S);
-    if (req.x0Full) {
-        dim3 blk(32, 8), grd((n + 31) / 32, (ctx.nS + 31) / 32);
-        toLanesKernel<<<grd, blk, 0, st>>>(ctx.full.as<double>(), ctx.x.as<double>(), n, ctx.nS, ctx.S);
-    }
-    tileKernel<<<blocksAll, 256, 0, st>>>(stageT, ctx.target.as<double>(), n, ctx.S);
-    tileModeKernel<<<blocksAll, 256, 0, st>>>(stageM, ctx.mode.as<int8_t>(), n, ctx.S);
-    if (req.nTargetOverrides > 0) {
-        targetOverrideKernel<<<(req.nTargetOverrides + 255) / 256, 256, 0, st>>>(
-            ovIdx.as<int>(), ovVal.as<double>(), req.nTargetOverrides, ctx.target.as<double>(), n, ctx.S);
-    }
-    if (req.nRowModeEntries > 0) {
-        rowModeOverrideKernel<<<(req.nRowModeEntries + 255) / 256, 256, 0, st>>>(rmE.as<int>(), req.nRowModeEntries,
-                                                                                ctx.mode.as<int8_t>(), ctx.S);
-    }
-    const DevBatch b = ctx.batch();
-    laneInitKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b);
-    if (ctx.rl.nRl > 0) {
-        OLF_CUDA(cudaMemsetAsync(ctx.rlLimitType.p, 0, ctx.rlLimitType.bytes, st));
-        OLF_CUDA(cudaMemsetAsync(ctx.rlSwitchCount.p, 0, ctx.rlSwitchCount.bytes, st));
-        OLF_CUDA(cudaMemsetAsync(ctx.rlPassSwitched.p, 0, ctx.rlPassSwitched.bytes, st));
-    }
-    // ---- Newton iterations, one graph launch each, until no lane iterates ----
-    const int cap = ctx.cfg.reactiveLimits ? (ctx.cfg.maxOuter + 1) * (ctx.cfg.maxIter + 1) : ctx.cfg.maxIter + 1;
-    // OLFGPU_PHASE_TIME: print-only channel; the iterations run unfused with events between their phases
-    static const bool phaseTime = std::getenv("OLFGPU_PHASE_TIME") != nullptr;
-    int k = 0;
-    for (; k < cap; k++) {
-        if (phaseTime) {
-            phaseTimedIteration(ctx, k);
-        } else {
-            OLF_CUDA(cudaGraphLaunch(ctx.graph, st));
-        }
-        OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 4, cudaMemcpyDeviceToHost, st));
-        OLF_CUDA(cudaStreamSynchronize(st));
-        if (*ctx.hostActive <= 0) {
-            k++;
-            break;
-        }
-    }
-    capKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b);
-    ctx.lastIterations = k;
-    // ---- results ----
+    installLanes(ctx);
+    ctx.lastIterations = runIterations(ctx);
     dim3 blk(32, 8), grd((n + 31) / 32, (ctx.nS + 31) / 32);
     resultsKernel<<<grd, blk, 0, st>>>(ctx.x.as<double>(), ctx.iter.as<int>(), ctx.normOut.as<double>(),
                                        ctx.status.as<int>(), ctx.out.as<double>(), n, ctx.nS, ctx.S);
@@ -659,7 +799,6 @@ void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     OLF_CUDA(cudaGetLastError());
-    (void)net;
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -725,8 +864,9 @@ void debugLinearSolve(BatchContext& ctx, const double* csrVals, const double* rh
     OLF_CUDA(cudaMemcpy(ctx.F.p, F.data(), F.size() * 8, cudaMemcpyHostToDevice));
     const DevBatch b = ctx.batch();
     laneInitKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b);
-    launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, fp32, st);
-    launchSolve(net, b, dn.fwd(), dn.bwd(), fp32, false, st);
+    launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, fp32,
+                 nullptr, st);
+    launchSolve(net, b, dn.fwd(), dn.bwd(), fp32, false, nullptr, st);
     OLF_CUDA(cudaStreamSynchronize(st));
     OLF_CUDA(cudaGetLastError());
     std::vector<double> dx(static_cast<size_t>(n) * S);

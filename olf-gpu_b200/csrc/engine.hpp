@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "persistent.cuh"
 #include "structure.hpp"
 
 namespace olfb200 {
@@ -67,6 +68,9 @@ struct DeviceNet {
     std::vector<int> csrToA;                      // CSR slot -> A block * 4 + entry (debug readback of J)
     DeviceBuffer nodeCol, sidePtr, side, cbPar, cbTrig, aPtr, aCol, aDiag, shPtr, shList, shPar, obPtr, obList, obPar;
     DeviceBuffer task, ops, levelTask, perm, iperm, lrowPtr, lrow, uPtr, uCol, fwdPos, bwdPos;
+    DeviceBuffer levelPtrD, levelLongestD, fwdPtrD, fwdLongestD, bwdPtrD, bwdLongestD;
+    PersistentPlan persistent{};
+    int factorFrom = 0, fwdFrom = 0, bwdUntil = 0;   // narrow-level boundaries of the level schedule
 };
 
 struct NetStructure {
@@ -75,6 +79,15 @@ struct NetStructure {
 };
 
 std::shared_ptr<DeviceNet> uploadNet(const Structure& s);
+
+// Schedules of the Newton iterations: one launch per dependency level (captured in a CUDA graph per iteration), or
+// the persistent kernel with one CTA per lane tile running the whole loop.
+enum { SCHEDULE_LEVELS = 0, SCHEDULE_PERSISTENT = 1 };
+
+struct TuningResult {
+    int schedule, lanesPerTile, threads;
+    float ms;
+};
 
 // Linear-solve modes accepted at the boundary (codes/gpu_linear_solve_mode.cuh:10-12): all run the engine's own
 // batched block LU.
@@ -111,7 +124,23 @@ struct BatchContext {
     // lane-interleaved state
     DeviceBuffer x, target, mode, F, J, lu64, lu32, w64, w32, dx, res, qbuf, disabled, norm, iter, status, outer,
         totalIter, trouble, normOut, active, pending, precision64, nActive;
-    DeviceBuffer stage;             // upload staging (base vectors, overrides)
+    DeviceBuffer stage;             // upload staging (base vectors)
+    DeviceBuffer ovIdx, ovVal, rowModeE;  // per-scenario overrides of the installed batch
+    int nTargetOverrides = 0, nRowModeEntries = 0;
+    bool hasX0Base = false, hasX0Full = false;
+    // schedule of the Newton iterations (set explicitly or picked by the autotuner on the next solve)
+    int schedule = SCHEDULE_LEVELS;
+    int lanesPerTile = 2;
+    int threads = 512;
+    bool autotunePending = false;
+    int narrowLanes = 2;            // level schedule: lanes per tile of the narrow-level range launches (0: none)
+    Hybrid hybrid() const {
+        const DeviceNet& d = *net->dev;
+        Hybrid h{d.factorFrom, d.fwdFrom, d.bwdUntil, narrowLanes, d.persistent};
+        h.plan.maxRounds = 1;
+        return h;
+    }
+    std::vector<TuningResult> tuning;
     DeviceBuffer out;               // [nS][n + 3] scenario-major results
     // reactive limits
     DevRl rl{};

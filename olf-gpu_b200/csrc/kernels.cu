@@ -11,8 +11,8 @@ __device__ __forceinline__ bool solving(const DevBatch& b, int s) { return b.act
 
 // NaN-propagating running maximum of |v| (a NaN stays: it orders above +inf as unsigned bits).
 __device__ __forceinline__ double absMax(double m, double v) {
-    double a = fabs(v);
-    return (a <= m) ? m : a;
+    const double a = fabs(v);
+    return (a > m || a != a) ? a : m;   // a NaN in either argument stays
 }
 
 }  // namespace
@@ -462,9 +462,10 @@ __global__ void clearTroubleKernel(DevBatch b) {
     }
 
 void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtr, const int* levelSplit, int nLevels,
-                  bool fp32, cudaStream_t st) {
+                  bool fp32, const Hybrid* hybrid, cudaStream_t st) {
     clearTroubleKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b);
-    for (int l = 0; l < nLevels; l++) {
+    const int wide = hybrid ? hybrid->factorFrom : nLevels;
+    for (int l = 0; l < wide; l++) {
         const int first = levelPtr[l], count = levelPtr[l + 1] - levelPtr[l];
         if (count == 0) continue;
         if (fp32) {
@@ -473,6 +474,7 @@ void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtr, con
             OLF_SPLIT_DISPATCH(levelSplit[l], factorLevelKernel, double, net, b, b.lu64, first, count)
         }
     }
+    if (hybrid) launchFactorRange(net, b, hybrid->plan, wide, nLevels, hybrid->lanes, fp32, st);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -610,15 +612,20 @@ __global__ void scatterKernel(DevNet net, DevBatch b, const T* w, bool accumulat
 
 template <typename T>
 static void solveT(const DevNet& net, const DevBatch& b, T* w, const T* lu, const LevelSchedule& fwd,
-                   const LevelSchedule& bwd, bool fromResidual, cudaStream_t st) {
+                   const LevelSchedule& bwd, bool fromResidual, const Hybrid* hybrid, cudaStream_t st) {
     const size_t all = (size_t)net.nb * b.S;
+    const bool fp32 = sizeof(T) == 4;
     rhsKernel<T><<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b, w, fromResidual);
-    for (int l = 0; l < fwd.levels; l++) {
+    const int fwdWide = hybrid ? hybrid->fwdFrom : fwd.levels;
+    for (int l = 0; l < fwdWide; l++) {
         const int first = fwd.ptr[l], count = fwd.ptr[l + 1] - fwd.ptr[l];
         if (count == 0) continue;
         OLF_SPLIT_DISPATCH(fwd.split[l], forwardLevelKernel, T, net, b, lu, w, fwd.pos, first, count)
     }
-    for (int l = 0; l < bwd.levels; l++) {
+    if (hybrid) launchSolveRange(net, b, hybrid->plan, 0, fwdWide, fwd.levels, hybrid->lanes, fp32, st);
+    const int bwdNarrow = hybrid ? hybrid->bwdUntil : 0;
+    if (hybrid) launchSolveRange(net, b, hybrid->plan, 1, 0, bwdNarrow, hybrid->lanes, fp32, st);
+    for (int l = bwdNarrow; l < bwd.levels; l++) {
         const int first = bwd.ptr[l], count = bwd.ptr[l + 1] - bwd.ptr[l];
         if (count == 0) continue;
         OLF_SPLIT_DISPATCH(bwd.split[l], backwardLevelKernel, T, net, b, lu, w, bwd.pos, first, count)
@@ -627,9 +634,9 @@ static void solveT(const DevNet& net, const DevBatch& b, T* w, const T* lu, cons
 }
 
 void launchSolve(const DevNet& net, const DevBatch& b, const LevelSchedule& fwd, const LevelSchedule& bwd, bool fp32,
-                 bool fromResidual, cudaStream_t st) {
-    if (fp32) solveT<float>(net, b, b.w32, b.lu32, fwd, bwd, fromResidual, st);
-    else solveT<double>(net, b, b.w64, b.lu64, fwd, bwd, fromResidual, st);
+                 bool fromResidual, const Hybrid* hybrid, cudaStream_t st) {
+    if (fp32) solveT<float>(net, b, b.w32, b.lu32, fwd, bwd, fromResidual, hybrid, st);
+    else solveT<double>(net, b, b.w64, b.lu64, fwd, bwd, fromResidual, hybrid, st);
 }
 
 // ---------------------------------------------------------------------------------------------------------------

@@ -138,6 +138,34 @@ void launchFill(const DevNet& net, const DevBatch& b, bool withJacobian, bool wi
 void launchTest(const DevNet& net, const DevBatch& b, const Settings& cfg, int* remainingPv, cudaStream_t st);
 void launchReactiveLimits(const DevNet& net, const DevBatch& b, const DevRl& rl, const Settings& cfg,
                           cudaStream_t st);
+// The dependency levels the persistent kernel walks (device pointers) and, per level, the longest update list of its
+// tasks/rows (sets how many threads share a task).
+struct PersistentPlan {
+    int nLevels, nFwd, nBwd;
+    const int* levelPtr;
+    const int* levelLongest;
+    const int* fwdPtr;
+    const int* fwdLongest;
+    const int* fwdPos;
+    const int* bwdPtr;
+    const int* bwdLongest;
+    const int* bwdPos;
+    int maxRounds;           // batched-iteration cap: lanes still iterating after it are REJECTED
+};
+
+// Level ranges for every tile of `lanes` lanes in one launch (the narrow levels of the level schedule).
+void launchFactorRange(const DevNet& net, const DevBatch& b, const PersistentPlan& plan, int l0, int l1, int lanes,
+                       bool fp32, cudaStream_t st);
+void launchSolveRange(const DevNet& net, const DevBatch& b, const PersistentPlan& plan, int dir, int l0, int l1,
+                      int lanes, bool fp32, cudaStream_t st);
+
+// The narrow levels of the level schedule run as one range launch per phase: factorization levels >= factorFrom,
+// forward levels >= fwdFrom, backward levels < bwdUntil, in tiles of `lanes` lanes.
+struct Hybrid {
+    int factorFrom, fwdFrom, bwdUntil, lanes;
+    PersistentPlan plan;
+};
+
 // Level boundaries (host), the positions of each level (device) and the split factor of each level (host).
 struct LevelSchedule {
     int levels;
@@ -147,9 +175,9 @@ struct LevelSchedule {
 };
 
 void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtrHost, const int* levelSplitHost,
-                  int nLevels, bool fp32, cudaStream_t st);
+                  int nLevels, bool fp32, const Hybrid* hybrid, cudaStream_t st);
 void launchSolve(const DevNet& net, const DevBatch& b, const LevelSchedule& fwd, const LevelSchedule& bwd, bool fp32,
-                 bool fromResidual, cudaStream_t st);
+                 bool fromResidual, const Hybrid* hybrid, cudaStream_t st);
 void launchResidual(const DevNet& net, const DevBatch& b, cudaStream_t st);
 void launchStep(const DevNet& net, const DevBatch& b, bool accumulate, cudaStream_t st);
 void launchGrowthCheck(const DevNet& net, const DevBatch& b, double limit, cudaStream_t st);

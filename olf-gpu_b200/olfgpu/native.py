@@ -33,7 +33,10 @@ _fp = ctypes.POINTER(ctypes.c_float)
 EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_structure", "olfgpu_structure_info",
            "olfgpu_structure_export", "olfgpu_recommend_batch_size", "olfgpu_create_batch_context",
            "olfgpu_destroy_batch_context", "olfgpu_set_linear_solver_settings", "olfgpu_solve_batch_context",
-           "olfgpu_last_solve_stats", "olfgpu_debug_fill", "olfgpu_debug_linear_solve"]
+           "olfgpu_last_solve_stats", "olfgpu_debug_fill", "olfgpu_debug_linear_solve", "olfgpu_set_schedule",
+           "olfgpu_get_schedule"]
+# Schedules of the Newton iterations
+LEVELS, PERSISTENT, AUTOTUNE = 0, 1, -1
 
 
 class NativeError(RuntimeError):
@@ -68,6 +71,8 @@ def load(path: str = LIB_PATH):
     L.olfgpu_last_solve_stats.argtypes = [_i64, _fp, _ip, _ip]
     L.olfgpu_debug_fill.argtypes = [_i64, _dp, _dp, _ip, _u8p, _dp, _dp]
     L.olfgpu_debug_linear_solve.argtypes = [_i64, _dp, _dp, ctypes.c_int, _dp]
+    L.olfgpu_set_schedule.argtypes = [_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.olfgpu_get_schedule.argtypes = [_i64, _ip, _ip, _ip, ctypes.c_int, _dp, _ip]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_char_p if name == "olfgpu_last_error" else ctypes.c_int
     _lib = L
@@ -182,6 +187,18 @@ class BatchContext:
 
     def set_linear_solver_settings(self, precision: int = FP64, refinement_steps: int = 1):
         _check(load().olfgpu_set_linear_solver_settings(self.handle, precision, refinement_steps))
+
+    def set_schedule(self, schedule: int, lanes_per_tile: int = 2, threads: int = 512):
+        _check(load().olfgpu_set_schedule(self.handle, schedule, lanes_per_tile, threads))
+
+    def schedule(self):
+        """(schedule, lanes per tile, threads) in force and the autotuner's timings [(schedule, lanes, threads, ms)]."""
+        sc, la, th, nr = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        res = np.zeros(4 * 32)
+        _check(load().olfgpu_get_schedule(self.handle, ctypes.byref(sc), ctypes.byref(la), ctypes.byref(th), 32,
+                                          _p(res), ctypes.byref(nr)))
+        tuning = [tuple(res[4 * i:4 * i + 4]) for i in range(min(nr.value, 32))]
+        return (sc.value, la.value, th.value), tuning
 
     def solve(self, x0_base, target_base, base_row_mode, disabled, x0_full=None, row_mode_entries=None,
               target_override_index=None, target_override_value=None, max_iter: int = 15, tol: float = 1e-8,

@@ -213,3 +213,52 @@ def test_reactive_limits_match_oracle(engine_lib, oracle_mod):
     # the limits actually bind somewhere
     plain = oracle_mod.Structure(p).solve_batch(p.x_base, p.outage_masks(outs))
     assert np.max(np.abs(plain[:, :p.n] - ref[:, :p.n])) > 1e-4
+
+
+@pytest.mark.parametrize("schedule,lanes,threads", [(0, 0, 256), (0, 1, 256), (0, 2, 256), (0, 4, 256), (1, 1, 256),
+                                                    (1, 2, 512), (1, 4, 512), (1, 8, 256)])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_schedules_match_oracle(engine_lib, oracle_mod, schedule, lanes, threads, precision):
+    """Every schedule (level launches, persistent tiles of 1-8 lanes) gives the oracle's states and statuses."""
+    from olfgpu import native, synthetic
+    g, p = grid("grid2000")
+    outs = synthetic.draw_outages(g, 150, seed=21)
+    dis = p.outage_masks(outs)
+    s = native.Structure(p)
+    ctx = native.BatchContext(s, outs.shape[0])
+    ctx.set_linear_solver_settings(precision, 1)
+    ctx.set_schedule(schedule, lanes, threads)
+    r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
+    ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis)
+    _compare(r, ref, p.n)
+
+
+def test_autotuner_picks_a_schedule_and_keeps_results(engine_lib, oracle_mod):
+    from olfgpu import native, synthetic
+    g, p = grid("grid2000")
+    outs = synthetic.draw_outages(g, 64, seed=22)
+    dis = p.outage_masks(outs)
+    s = native.Structure(p)
+    ctx = native.BatchContext(s, outs.shape[0])
+    ctx.set_schedule(native.AUTOTUNE)
+    r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
+    (sc, lanes, threads), tuning = ctx.schedule()
+    assert len(tuning) == 8
+    best = min(tuning, key=lambda t: t[3])
+    assert (sc, lanes, threads) == (int(best[0]), int(best[1]), int(best[2]))
+    ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis)
+    _compare(r, ref, p.n)
+
+
+def test_persistent_reactive_limits_match_oracle(engine_lib, oracle_mod):
+    from olfgpu import native, synthetic
+    g, p = grid("grid300")
+    outs = synthetic.draw_outages(g, 64, seed=301)
+    dis = p.outage_masks(outs)
+    s = native.Structure(p)
+    for sched in (0, 1):
+        ctx = native.BatchContext(s, outs.shape[0], rl=p.rl)
+        ctx.set_schedule(sched, 2, 256)
+        r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
+        ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis, reactive_limits=True)
+        _compare(r, ref, p.n)
