@@ -133,6 +133,24 @@ int olfgpu_debug_fill(int64_t context, const double* xFull, const double* target
                       const unsigned char* disabled, double* jacobianOut, double* mismatchOut);
 int olfgpu_debug_linear_solve(int64_t context, const double* csrVals, const double* rhs, int precision, double* out);
 
+/*
+ * Batched linear solve J z = rhs that allocates no memory (this entry point has no counterpart in the reference).
+ * It is for callers that cannot allocate device memory while they solve: a host whose GPU memory is reserved up front
+ * and handed out by someone else (a JVM or service that sized its pools at start-up), or a code path that must not
+ * call cudaMalloc / cudaFree because those calls synchronise the whole device.  The caller passes device buffers:
+ * csrValsDevice [nScenarios][nnz] (the reference-compatible CSR layout of olfgpu_structure_export), rhsDevice and
+ * outDevice [nScenarios][n]; precision 0 factors in FP64, 1 in FP32.  The work is enqueued on `stream` (a
+ * cudaStream_t, null for the legacy default stream) and the call returns without waiting for it.
+ * Scratch: one fixed 64 MiB device array inside the library, which every GPU that loads the library holds until the
+ * process exits; a batch whose Jacobian, factors and work vectors do not fit is rejected with an error naming the
+ * largest batch that fits.  The structure must already be on the current device (creating a batch context on it
+ * uploads it).  The first call on each device looks up the array's address (set-up, no allocation); make that first
+ * call before any stream capture.  All calls share the one array and it keeps the previous call's contents (what must
+ * start at zero is cleared on every call): calls whose work overlaps on the GPU race, so order them on one stream.
+ */
+int olfgpu_linear_solve_noalloc(int64_t structure, int nScenarios, const double* csrValsDevice,
+                                const double* rhsDevice, double* outDevice, int precision, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -254,3 +254,16 @@ extern "C" int olfgpu_debug_linear_solve(int64_t context, const double* csrVals,
                                          double* out) {
     return guarded([&] { debugLinearSolve(contextOf(context), csrVals, rhs, precision, out); });
 }
+
+namespace olfb200 {
+void linearSolveNoAlloc(const std::shared_ptr<NetStructure>& net, int nScenarios, const double* csrVals,
+                        const double* rhs, double* out, int precision, cudaStream_t st);
+}
+
+extern "C" int olfgpu_linear_solve_noalloc(int64_t structure, int nScenarios, const double* csrValsDevice,
+                                           const double* rhsDevice, double* outDevice, int precision, void* stream) {
+    return guarded([&] {
+        linearSolveNoAlloc(structureOf(structure), nScenarios, csrValsDevice, rhsDevice, outDevice, precision,
+                           static_cast<cudaStream_t>(stream));
+    });
+}

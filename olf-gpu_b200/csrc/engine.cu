@@ -97,6 +97,7 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
             d->csrToA[k] = aBlock(nr >> 1, nc >> 1) * 4 + (nr & 1) * 2 + (nc & 1);
         }
     }
+    d->csrToAD.upload(d->csrToA);
     d->nodeCol.upload(s.nodeCol);
     d->sidePtr.upload(sidePtr);
     d->side.upload(sideAll);

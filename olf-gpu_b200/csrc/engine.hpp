@@ -66,6 +66,7 @@ struct DeviceNet {
         return LevelSchedule{static_cast<int>(bwdPtr.size()) - 1, bwdPtr.data(), bwdPos.as<int>(), bwdSplit.data()};
     }
     std::vector<int> csrToA;                      // CSR slot -> A block * 4 + entry (debug readback of J)
+    DeviceBuffer csrToAD;                         // the same map on the device
     DeviceBuffer nodeCol, sidePtr, side, cbPar, cbTrig, aPtr, aCol, aDiag, shPtr, shList, shPar, obPtr, obList, obPar;
     DeviceBuffer task, ops, levelTask, perm, iperm, lrowPtr, lrow, uPtr, uCol, fwdPos, bwdPos;
     DeviceBuffer levelPtrD, levelLongestD, fwdPtrD, fwdLongestD, bwdPtrD, bwdLongestD;

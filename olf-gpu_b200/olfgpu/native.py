@@ -34,7 +34,7 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_structure_export", "olfgpu_recommend_batch_size", "olfgpu_create_batch_context",
            "olfgpu_destroy_batch_context", "olfgpu_set_linear_solver_settings", "olfgpu_solve_batch_context",
            "olfgpu_last_solve_stats", "olfgpu_debug_fill", "olfgpu_debug_linear_solve", "olfgpu_set_schedule",
-           "olfgpu_get_schedule"]
+           "olfgpu_get_schedule", "olfgpu_linear_solve_noalloc"]
 # Schedules of the Newton iterations
 LEVELS, PERSISTENT, AUTOTUNE = 0, 1, -1
 
@@ -73,6 +73,8 @@ def load(path: str = LIB_PATH):
     L.olfgpu_debug_linear_solve.argtypes = [_i64, _dp, _dp, ctypes.c_int, _dp]
     L.olfgpu_set_schedule.argtypes = [_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.olfgpu_get_schedule.argtypes = [_i64, _ip, _ip, _ip, ctypes.c_int, _dp, _ip]
+    L.olfgpu_linear_solve_noalloc.argtypes = [_i64, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_int, ctypes.c_void_p]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_char_p if name == "olfgpu_last_error" else ctypes.c_int
     _lib = L
@@ -148,6 +150,13 @@ class Structure:
         b = ctypes.c_int(0)
         _check(load().olfgpu_recommend_batch_size(self.handle, max_cap, mode, ctypes.byref(b)))
         return int(b.value)
+
+    def linear_solve_noalloc(self, n_scenarios: int, csr_vals_ptr: int, rhs_ptr: int, out_ptr: int,
+                             precision: int = FP64, stream: int = 0):
+        """olfgpu_linear_solve_noalloc on caller-owned device buffers (raw device addresses); enqueues and returns."""
+        _check(load().olfgpu_linear_solve_noalloc(self.handle, n_scenarios, ctypes.c_void_p(csr_vals_ptr),
+                                                  ctypes.c_void_p(rhs_ptr), ctypes.c_void_p(out_ptr), precision,
+                                                  ctypes.c_void_p(stream)))
 
     @property
     def lu_bytes_per_scenario(self) -> int:
