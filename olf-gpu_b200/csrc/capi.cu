@@ -185,7 +185,7 @@ extern "C" int olfgpu_get_schedule(int64_t context, int* schedule, int* lanesPer
         BatchContext& c = contextOf(context);
         if (schedule) *schedule = c.schedule;
         if (lanesPerTile) *lanesPerTile = c.schedule == SCHEDULE_LEVELS ? c.narrowLanes : c.lanesPerTile;
-        if (threads) *threads = c.threads;
+        if (threads) *threads = c.schedule == SCHEDULE_LEVELS ? 256 : c.threads;   // range kernels run 256 threads
         const int k = std::min<int>(maxResults, static_cast<int>(c.tuning.size()));
         for (int i = 0; results && i < k; i++) {
             results[4 * i] = c.tuning[i].schedule;

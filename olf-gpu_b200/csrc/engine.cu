@@ -245,6 +245,7 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
 // ---------------------------------------------------------------------------------------------------------------
 BatchContext::~BatchContext() {
     if (graph) cudaGraphExecDestroy(graph);
+    if (graphSolve) cudaGraphExecDestroy(graphSolve);
     if (hostActive) cudaFreeHost(hostActive);
     if (hostBitsPinned) cudaFreeHost(hostBitsPinned);
     if (stream) cudaStreamDestroy(stream);
@@ -298,7 +299,7 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
     ctx->S = (nScenarios + 31) / 32 * 32;
     const size_t S = ctx->S, n = s.n;
     OLF_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    OLF_CUDA(cudaMallocHost(&ctx->hostActive, sizeof(int)));
+    OLF_CUDA(cudaMallocHost(&ctx->hostActive, 2 * sizeof(int)));
     ctx->x.alloc(n * S * 8);
     ctx->target.alloc(n * S * 8);
     ctx->mode.alloc(n * S);
@@ -320,7 +321,7 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
     ctx->active.alloc(S);
     ctx->pending.alloc(S);
     ctx->precision64.alloc(S);
-    ctx->nActive.alloc(4);
+    ctx->nActive.alloc(8);
     ctx->out.alloc(static_cast<size_t>(nScenarios) * (n + 3) * 8);
     ctx->stage.alloc(n * 8 * 2 + n * 4);
     ctx->cfg.maxIter = 15;
@@ -505,6 +506,10 @@ void captureIteration(BatchContext& ctx) {
         cudaGraphExecDestroy(ctx.graph);
         ctx.graph = nullptr;
     }
+    if (ctx.graphSolve) {
+        cudaGraphExecDestroy(ctx.graphSolve);
+        ctx.graphSolve = nullptr;
+    }
     const DeviceNet& dn = *ctx.net->dev;
     const DevNet& net = dn.view;
     const size_t S = ctx.S;
@@ -513,11 +518,19 @@ void captureIteration(BatchContext& ctx) {
     if (!mixed && !ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(net.nLu) * 4 * S * 8);
     const DevBatch b = ctx.batch();
     const bool rl = ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits;
+    // part 1: fill, test, reactive limits, count of the lanes that factorize
     cudaGraph_t g;
     OLF_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
+    launchIterationStart(b, ctx.stream);
     launchFill(net, b, true, rl, ctx.stream);
     launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, ctx.stream);
     if (rl) launchReactiveLimits(net, b, ctx.rl, ctx.cfg, ctx.stream);
+    launchCountSolving(b, ctx.stream);
+    OLF_CUDA(cudaStreamEndCapture(ctx.stream, &g));
+    OLF_CUDA(cudaGraphInstantiate(&ctx.graph, g, 0));
+    cudaGraphDestroy(g);
+    // part 2: factorization, solves, refinement, step
+    OLF_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
     const Hybrid hy = ctx.hybrid();
     const Hybrid* hp = ctx.narrowLanes > 0 ? &hy : nullptr;
     launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, mixed, hp,
@@ -531,7 +544,7 @@ void captureIteration(BatchContext& ctx) {
     }
     launchStep(net, b, false, ctx.stream);
     OLF_CUDA(cudaStreamEndCapture(ctx.stream, &g));
-    OLF_CUDA(cudaGraphInstantiate(&ctx.graph, g, 0));
+    OLF_CUDA(cudaGraphInstantiate(&ctx.graphSolve, g, 0));
     cudaGraphDestroy(g);
     ctx.graphKey = key;
 }
@@ -548,6 +561,7 @@ void phaseTimedIteration(BatchContext& ctx, int k) {
     cudaEvent_t ev[7];
     for (auto& e : ev) OLF_CUDA(cudaEventCreate(&e));
     OLF_CUDA(cudaEventRecord(ev[0], st));
+    launchIterationStart(b, st);
     launchFill(net, b, true, rl, st);
     OLF_CUDA(cudaEventRecord(ev[1], st));
     launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, st);
@@ -672,14 +686,25 @@ int runIterations(BatchContext& ctx) {
     static const bool phaseTime = std::getenv("OLFGPU_PHASE_TIME") != nullptr;
     int k = 0;
     for (; k < cap; k++) {
-        if (phaseTime) phaseTimedIteration(ctx, k);
-        else OLF_CUDA(cudaGraphLaunch(ctx.graph, st));
-        OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 4, cudaMemcpyDeviceToHost, st));
+        if (phaseTime) {
+            phaseTimedIteration(ctx, k);
+            OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 8, cudaMemcpyDeviceToHost, st));
+            OLF_CUDA(cudaStreamSynchronize(st));
+            if (ctx.hostActive[0] <= 0) {
+                k++;
+                break;
+            }
+            continue;
+        }
+        OLF_CUDA(cudaGraphLaunch(ctx.graph, st));
+        OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 8, cudaMemcpyDeviceToHost, st));
         OLF_CUDA(cudaStreamSynchronize(st));
-        if (*ctx.hostActive <= 0) {
+        if (ctx.hostActive[0] <= 0) {
             k++;
             break;
         }
+        // no lane factorizes this iteration (only restarts pending): skip the factor / solve graph
+        if (ctx.hostActive[1] > 0) OLF_CUDA(cudaGraphLaunch(ctx.graphSolve, st));
     }
     capKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(ctx.batch());
     return k;

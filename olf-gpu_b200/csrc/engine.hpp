@@ -152,7 +152,8 @@ struct BatchContext {
     DeviceBuffer full;
     int* hostActive = nullptr;      // pinned
     // one Newton iteration as a CUDA graph (captured on first use per settings)
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr;       // fill, test, reactive limits
+    cudaGraphExec_t graphSolve = nullptr;  // factorization, solves, refinement, step
     int graphKey = -1;
     // statistics of the last solve
     int lastIterations = 0;         // batched iterations run

@@ -681,13 +681,37 @@ __global__ void stepKernel(DevNet net, DevBatch b) {
 
 __global__ void advanceKernel(DevBatch b) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= b.S || !b.active[s]) return;
-    if (!b.pending[s]) {
-        b.iter[s]++;
-        b.totalIter[s]++;
-    }
-    b.pending[s] = 0;
+    if (s >= b.S || !b.active[s] || b.pending[s]) return;
+    b.iter[s]++;
+    b.totalIter[s]++;
 }
+
+// Start of an iteration: the lanes a reactive-limit check restarted last iteration solve again.
+__global__ void releasePendingKernel(DevBatch b) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < b.S) b.pending[s] = 0;
+}
+
+// After the test: how many lanes factorize this iteration (the host skips the factor/solve graph when none does).
+__global__ void countSolvingKernel(DevBatch b) {
+    __shared__ int part[32];
+    int c = 0;
+    for (int s = threadIdx.x; s < b.S; s += blockDim.x) c += (b.active[s] && !b.pending[s]) ? 1 : 0;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
+        b.nActive[1] = t;
+    }
+}
+
+void launchIterationStart(const DevBatch& b, cudaStream_t st) {
+    releasePendingKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b);
+}
+
+void launchCountSolving(const DevBatch& b, cudaStream_t st) { countSolvingKernel<<<1, 1024, 0, st>>>(b); }
 
 void launchStep(const DevNet& net, const DevBatch& b, bool, cudaStream_t st) {
     const size_t all = (size_t)net.n * b.S;

@@ -97,7 +97,7 @@ struct DevBatch {
     int8_t* active;           // [S] 1 while the lane iterates
     int8_t* pending;          // [S] 1: converged this iteration, reactive limits to check
     int8_t* precision64;      // [S] 1: this lane's last factorization fell back to FP64 (mixed precision)
-    int* nActive;             // [1] lanes still iterating (read by the host to stop)
+    int* nActive;             // [2] lanes still iterating, lanes factorizing this iteration (read by the host)
 };
 
 // Reactive-limit entries (ReactiveLimitsPacker.java:76) and their per-lane state.
@@ -181,5 +181,7 @@ void launchSolve(const DevNet& net, const DevBatch& b, const LevelSchedule& fwd,
 void launchResidual(const DevNet& net, const DevBatch& b, cudaStream_t st);
 void launchStep(const DevNet& net, const DevBatch& b, bool accumulate, cudaStream_t st);
 void launchGrowthCheck(const DevNet& net, const DevBatch& b, double limit, cudaStream_t st);
+void launchIterationStart(const DevBatch& b, cudaStream_t st);
+void launchCountSolving(const DevBatch& b, cudaStream_t st);
 
 }  // namespace olfb200
