@@ -134,6 +134,45 @@ int olfgpu_debug_fill(int64_t context, const double* xFull, const double* target
 int olfgpu_debug_linear_solve(int64_t context, const double* csrVals, const double* rhs, int precision, double* out);
 
 /*
+ * Learned warm start (no counterpart in the reference): kernels of a message-passing graph network over the bus
+ * graph, BF16 weights and activations with FP32 accumulation, on caller-owned device buffers, enqueued on `stream`.
+ * Row-major matrices; M rows = samples x buses.
+ *   gemm:     Y = [A1 | A2] . W (+ bias), z = relu ? max(Y, 0) : Y (saved to saveZ if given), out = z (+ residual);
+ *             shapes (K1, K2, N) in {(16,0,64), (64,0,128), (64,64,64), (64,0,16), (128,0,64)}; tensor cores.
+ *   gemm_dw:  dW = [A1 | A2]^T dZ and db = column sums of dZ, summed over at most maxChunks row chunks in a fixed order
+ *             (partial holds maxChunks * (K * N + N) floats); shapes (16,0,64), (64,0,128), (64,64,64), (64,0,16).
+ *   copy_cols: dst[r, dstCol0 + c] (+)= src[r, srcCol0 + c], FP32.
+ *   message_forward:  agg[b, i] = sum over directed edges e = (j -> i) not in sample b's outaged branch of
+ *             relu(P[b, j] + Q[b, i] + C[e] + bmsg), PQ rows = [P | Q] (128 BF16), agg rows 64 BF16.
+ *   message_backward: dPQ (FP32) and dC (FP32, summed over samples) of the same, by recomputation.
+ *   edge_project (C = Es . We) and its backward; relu_grad; adam (FP32 master weights, BF16 copy and transpose);
+ *   mse (loss partials and its gradient).
+ * olfgpu_gnn_last_error() reports the calling thread's last failure of these functions.
+ */
+const char* olfgpu_gnn_last_error(void);
+int olfgpu_gnn_gemm(int M, int K1, int K2, int N, const void* A1, const void* A2, const void* W, const float* bias,
+                    int relu, const void* residual, void* outBf16, float* outF32, int ldo, void* saveZ, void* stream);
+int olfgpu_gnn_gemm_dw(int M, int K1, int K2, int N, const void* A1, const void* A2, const void* dZ, float* dW,
+                       float* db, float* partial, int maxChunks, void* stream);
+int olfgpu_gnn_message_forward(int B, int nb, const int* inPtr, const int* inEdge, const int* edgeSrc,
+                               const int* edgeBranch, const int* outage, const void* PQ, const float* C,
+                               const float* bmsg, void* agg, void* stream);
+int olfgpu_gnn_message_backward(int B, int nb, int nEdges, const int* inPtr, const int* inEdge, const int* outPtr,
+                                const int* outEdge, const int* edgeSrc, const int* edgeDst, const int* edgeBranch,
+                                const int* outage, const void* PQ, const float* C, const float* bmsg,
+                                const float* dAgg, float* dPQ, float* dC, void* stream);
+int olfgpu_gnn_edge_project(int nEdges, const float* Es, const float* We, float* C, void* stream);
+int olfgpu_gnn_edge_project_backward(int nEdges, const float* Es, const float* dC, float* dWe, float* dbmsg,
+                                     void* stream);
+int olfgpu_gnn_relu_grad(long long count, int N, int ldd, const float* dOut, const void* z, void* dz, float* dzF32,
+                         void* stream);
+int olfgpu_gnn_adam(int count, int K, int N, float* w, const float* grad, float* m, float* v, float lr, float beta1,
+                    float beta2, float eps, int step, void* wBf16, void* wTBf16, void* stream);
+int olfgpu_gnn_mse(int M, int ldo, const float* out, const float* target, float* dOut, float* partial, void* stream);
+int olfgpu_gnn_copy_cols(int M, int ncols, const float* src, int lds, int srcCol0, float* dst, int ldd, int dstCol0,
+                         int accumulate, void* stream);
+
+/*
  * Batched linear solve J z = rhs that allocates no memory (this entry point has no counterpart in the reference).
  * It is for callers that cannot allocate device memory while they solve: a host whose GPU memory is reserved up front
  * and handed out by someone else (a JVM or service that sized its pools at start-up), or a code path that must not

@@ -1,0 +1,532 @@
+// Kernels of the learned warm start: a message-passing graph network over the bus graph, BF16 weights and
+// activations with FP32 accumulation.  Tensor-core GEMMs (mma.sync m16n8k16 BF16 -> FP32) for the dense layers and
+// their weight gradients; CUDA-core gather kernels for the messages.  Every reduction runs in a fixed order, so
+// forward and backward are deterministic.
+//
+// Shapes: M rows = samples x buses; feature widths K, N are multiples of 16 / 8 (<= 128).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/olfgpu_b200.h"
+
+namespace olfb200 {
+namespace gnn {
+
+namespace {
+
+__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Y[M x N] = [A1 | A2][M x (K1 + K2)] . W[(K1 + K2) x N] (+ bias), z = relu ? max(Y, 0) : Y, saved to saveZ when given;
+// out = z (+ residual) to outB (bf16) and / or outF (fp32).  4 warps per CTA, each warp 16 rows x N columns; W staged
+// transposed in shared memory.  Rows are walked grid-stride in 64-row chunks.
+template <int K1, int K2, int N>
+__global__ void __launch_bounds__(128) gemmKernel(int M, const __nv_bfloat16* __restrict__ A1,
+                                                  const __nv_bfloat16* __restrict__ A2,
+                                                  const __nv_bfloat16* __restrict__ W, const float* __restrict__ bias,
+                                                  int relu, const __nv_bfloat16* __restrict__ residual,
+                                                  __nv_bfloat16* outB, float* outF, int ldo,
+                                                  __nv_bfloat16* saveZ) {
+    constexpr int K = K1 + K2;
+    constexpr int KP = K + 8;   // padded row of the transposed weights (bank spread)
+    constexpr int NT = N / 8;
+    __shared__ __align__(16) __nv_bfloat16 wt[N * KP];
+    for (int i = threadIdx.x; i < K * N; i += blockDim.x) {
+        const int k = i / N, n = i % N;
+        wt[n * KP + k] = W[i];
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    for (int base = (blockIdx.x * 4 + warp) * 16; base < M; base += gridDim.x * 64) {
+        float acc[NT][4];
+#pragma unroll
+        for (int j = 0; j < NT; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+        const int r0 = base + g, r1 = base + g + 8;
+#pragma unroll
+        for (int ks = 0; ks < K / 16; ks++) {
+            const int kb = ks * 16;
+            const __nv_bfloat16* src = kb < K1 ? A1 : A2;
+            const int ld = kb < K1 ? K1 : K2;
+            const int kc = kb < K1 ? kb : kb - K1;
+            uint32_t a[4];
+            const uint32_t z = 0u;
+            a[0] = r0 < M ? *reinterpret_cast<const uint32_t*>(src + (size_t)r0 * ld + kc + 2 * t) : z;
+            a[1] = r1 < M ? *reinterpret_cast<const uint32_t*>(src + (size_t)r1 * ld + kc + 2 * t) : z;
+            a[2] = r0 < M ? *reinterpret_cast<const uint32_t*>(src + (size_t)r0 * ld + kc + 2 * t + 8) : z;
+            a[3] = r1 < M ? *reinterpret_cast<const uint32_t*>(src + (size_t)r1 * ld + kc + 2 * t + 8) : z;
+#pragma unroll
+            for (int j = 0; j < NT; j++) {
+                const __nv_bfloat16* wrow = wt + (j * 8 + g) * KP + kb;
+                uint32_t bfrag[2];
+                bfrag[0] = *reinterpret_cast<const uint32_t*>(wrow + 2 * t);
+                bfrag[1] = *reinterpret_cast<const uint32_t*>(wrow + 2 * t + 8);
+                mma16816(acc[j], a, bfrag);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NT; j++) {
+            const int c = j * 8 + 2 * t;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int r = h == 0 ? r0 : r1;
+                if (r >= M) continue;
+                float v0 = acc[j][2 * h], v1 = acc[j][2 * h + 1];
+                if (bias) {
+                    v0 += bias[c];
+                    v1 += bias[c + 1];
+                }
+                if (relu) {
+                    v0 = fmaxf(v0, 0.f);
+                    v1 = fmaxf(v1, 0.f);
+                }
+                if (saveZ) {
+                    saveZ[(size_t)r * N + c] = __float2bfloat16(v0);
+                    saveZ[(size_t)r * N + c + 1] = __float2bfloat16(v1);
+                }
+                if (residual) {
+                    v0 += __bfloat162float(residual[(size_t)r * N + c]);
+                    v1 += __bfloat162float(residual[(size_t)r * N + c + 1]);
+                }
+                if (outB) {
+                    outB[(size_t)r * ldo + c] = __float2bfloat16(v0);
+                    outB[(size_t)r * ldo + c + 1] = __float2bfloat16(v1);
+                }
+                if (outF) {
+                    outF[(size_t)r * ldo + c] = v0;
+                    outF[(size_t)r * ldo + c + 1] = v1;
+                }
+            }
+        }
+    }
+}
+
+// Partial weight gradients: chunk c of the rows contributes P_c[K x N] = [A1|A2]_c^T dZ_c and colsum(dZ_c); one CTA
+// per chunk, 16-row slices staged in shared memory, tensor-core tiles (m over K, n over N, k over rows).
+template <int K1, int K2, int N>
+__global__ void __launch_bounds__(128) gemmDwKernel(int M, int rowsPerChunk, const __nv_bfloat16* __restrict__ A1,
+                                                    const __nv_bfloat16* __restrict__ A2,
+                                                    const __nv_bfloat16* __restrict__ dZ, float* partial) {
+    constexpr int K = K1 + K2;
+    constexpr int MT = K / 16, NT = N / 8, TILES = MT * NT;
+    constexpr int PER_WARP = (TILES + 3) / 4;
+    __shared__ __align__(16) __nv_bfloat16 as[16][K + 8];
+    __shared__ __align__(16) __nv_bfloat16 ds[16][N + 8];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int row0 = blockIdx.x * rowsPerChunk;
+    const int row1 = min(M, row0 + rowsPerChunk);
+    float acc[PER_WARP][4];
+#pragma unroll
+    for (int i = 0; i < PER_WARP; i++) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
+    float colsum = 0.f;   // thread tid < N sums column tid of dZ
+    for (int base = row0; base < row1; base += 16) {
+        for (int i = threadIdx.x; i < 16 * K; i += blockDim.x) {
+            const int r = i / K, k = i % K, row = base + r;
+            __nv_bfloat16 v = __float2bfloat16(0.f);
+            if (row < row1) v = k < K1 ? A1[(size_t)row * K1 + k] : A2[(size_t)row * K2 + (k - K1)];
+            as[r][k] = v;
+        }
+        for (int i = threadIdx.x; i < 16 * N; i += blockDim.x) {
+            const int r = i / N, n = i % N, row = base + r;
+            ds[r][n] = row < row1 ? dZ[(size_t)row * N + n] : __float2bfloat16(0.f);
+        }
+        __syncthreads();
+        if (threadIdx.x < N) {
+            for (int r = 0; r < 16; r++) colsum += __bfloat162float(ds[r][threadIdx.x]);
+        }
+#pragma unroll
+        for (int i = 0; i < PER_WARP; i++) {
+            const int tile = warp * PER_WARP + i;
+            if (tile >= TILES) break;
+            const int m0 = (tile / NT) * 16, n0 = (tile % NT) * 8;
+            uint32_t a[4], b[2];
+            // A_mma(m, kk) = as[kk][m0 + m]; B_mma(kk, n) = ds[kk][n0 + n]
+            a[0] = pack2(as[2 * t][m0 + g], as[2 * t + 1][m0 + g]);
+            a[1] = pack2(as[2 * t][m0 + g + 8], as[2 * t + 1][m0 + g + 8]);
+            a[2] = pack2(as[2 * t + 8][m0 + g], as[2 * t + 9][m0 + g]);
+            a[3] = pack2(as[2 * t + 8][m0 + g + 8], as[2 * t + 9][m0 + g + 8]);
+            b[0] = pack2(ds[2 * t][n0 + g], ds[2 * t + 1][n0 + g]);
+            b[1] = pack2(ds[2 * t + 8][n0 + g], ds[2 * t + 9][n0 + g]);
+            mma16816(acc[i], a, b);
+        }
+        __syncthreads();
+    }
+    float* out = partial + (size_t)blockIdx.x * (K * N + N);
+#pragma unroll
+    for (int i = 0; i < PER_WARP; i++) {
+        const int tile = warp * PER_WARP + i;
+        if (tile >= TILES) break;
+        const int m0 = (tile / NT) * 16, n0 = (tile % NT) * 8;
+        out[(m0 + g) * N + n0 + 2 * t] = acc[i][0];
+        out[(m0 + g) * N + n0 + 2 * t + 1] = acc[i][1];
+        out[(m0 + g + 8) * N + n0 + 2 * t] = acc[i][2];
+        out[(m0 + g + 8) * N + n0 + 2 * t + 1] = acc[i][3];
+    }
+    if (threadIdx.x < N) out[K * N + threadIdx.x] = colsum;
+}
+
+// dW[K x N], db[N] = sums of the chunk partials in chunk order.
+__global__ void reducePartialsKernel(int chunks, int KN, int N, const float* partial, float* dW, float* db) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= KN + N) return;
+    float s = 0.f;
+    for (int c = 0; c < chunks; c++) s += partial[(size_t)c * (KN + N) + i];
+    if (i < KN) dW[i] = s;
+    else if (db) db[i - KN] = s;
+}
+
+// Messages into bus i of sample b: agg[b, i] = sum over directed edges e = (j -> i) of
+// relu(P[b, j] + Q[b, i] + C[e] + bmsg), the edge dropped in the sample whose outaged branch it belongs to.
+// PQ rows hold [P | Q] (128 features).  One warp per (sample, bus), two features per lane.
+__global__ void messageForwardKernel(int B, int nb, const int* inPtr, const int* inEdge, const int* edgeSrc,
+                                     const int* edgeBranch, const int* outage, const __nv_bfloat16* PQ, const float* C,
+                                     const float* bmsg, __nv_bfloat16* agg) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= B * nb) return;
+    const int b = warp / nb, i = warp % nb;
+    const int f = 2 * lane;
+    const size_t qi = ((size_t)b * nb + i) * 128 + 64 + f;
+    const float q0 = __bfloat162float(PQ[qi]) + bmsg[f], q1 = __bfloat162float(PQ[qi + 1]) + bmsg[f + 1];
+    float a0 = 0.f, a1 = 0.f;
+    const int out = outage[b];
+    for (int p = inPtr[i]; p < inPtr[i + 1]; p++) {
+        const int e = inEdge[p];
+        if (edgeBranch[e] == out) continue;
+        const size_t pj = ((size_t)b * nb + edgeSrc[e]) * 128 + f;
+        a0 += fmaxf(__bfloat162float(PQ[pj]) + q0 + C[(size_t)e * 64 + f], 0.f);
+        a1 += fmaxf(__bfloat162float(PQ[pj + 1]) + q1 + C[(size_t)e * 64 + f + 1], 0.f);
+    }
+    agg[((size_t)b * nb + i) * 64 + f] = __float2bfloat16(a0);
+    agg[((size_t)b * nb + i) * 64 + f + 1] = __float2bfloat16(a1);
+}
+
+// Backward of the messages.  dQ[b, i] = sum over e into i of g_e; dP[b, j] = sum over e out of j of g_e, with
+// g_e = dAgg[b, dst(e)] * [pre_e > 0] recomputed from the saved P, Q.  Written into dPQ [rows x 128] (fp32).
+__global__ void messageBackwardNodesKernel(int B, int nb, const int* inPtr, const int* inEdge, const int* outPtr,
+                                           const int* outEdge, const int* edgeSrc, const int* edgeDst,
+                                           const int* edgeBranch, const int* outage, const __nv_bfloat16* PQ,
+                                           const float* C, const float* bmsg, const float* dAgg, float* dPQ) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= B * nb) return;
+    const int b = warp / nb, v = warp % nb;
+    const int f = 2 * lane;
+    const int out = outage[b];
+    const size_t rowV = (size_t)b * nb + v;
+    // as destination: dQ[v]
+    {
+        const float q0 = __bfloat162float(PQ[rowV * 128 + 64 + f]) + bmsg[f];
+        const float q1 = __bfloat162float(PQ[rowV * 128 + 64 + f + 1]) + bmsg[f + 1];
+        const float d0 = dAgg[rowV * 64 + f], d1 = dAgg[rowV * 64 + f + 1];
+        float s0 = 0.f, s1 = 0.f;
+        for (int p = inPtr[v]; p < inPtr[v + 1]; p++) {
+            const int e = inEdge[p];
+            if (edgeBranch[e] == out) continue;
+            const size_t pj = ((size_t)b * nb + edgeSrc[e]) * 128 + f;
+            if (__bfloat162float(PQ[pj]) + q0 + C[(size_t)e * 64 + f] > 0.f) s0 += d0;
+            if (__bfloat162float(PQ[pj + 1]) + q1 + C[(size_t)e * 64 + f + 1] > 0.f) s1 += d1;
+        }
+        dPQ[rowV * 128 + 64 + f] = s0;
+        dPQ[rowV * 128 + 64 + f + 1] = s1;
+    }
+    // as source: dP[v]
+    {
+        const float p0 = __bfloat162float(PQ[rowV * 128 + f]), p1 = __bfloat162float(PQ[rowV * 128 + f + 1]);
+        float s0 = 0.f, s1 = 0.f;
+        for (int p = outPtr[v]; p < outPtr[v + 1]; p++) {
+            const int e = outEdge[p];
+            if (edgeBranch[e] == out) continue;
+            const size_t rowI = (size_t)b * nb + edgeDst[e];
+            const float pre0 = p0 + __bfloat162float(PQ[rowI * 128 + 64 + f]) + bmsg[f] + C[(size_t)e * 64 + f];
+            const float pre1 = p1 + __bfloat162float(PQ[rowI * 128 + 64 + f + 1]) + bmsg[f + 1] + C[(size_t)e * 64 + f + 1];
+            if (pre0 > 0.f) s0 += dAgg[rowI * 64 + f];
+            if (pre1 > 0.f) s1 += dAgg[rowI * 64 + f + 1];
+        }
+        dPQ[rowV * 128 + f] = s0;
+        dPQ[rowV * 128 + f + 1] = s1;
+    }
+}
+
+// dC[e] = sum over samples of g_e (one warp per directed edge, two features per lane); dbmsg from the partials of
+// dC summed over edges in edge order by the caller's reduction.
+__global__ void messageBackwardEdgesKernel(int B, int nb, int nEdges, const int* edgeSrc, const int* edgeDst,
+                                           const int* edgeBranch, const int* outage, const __nv_bfloat16* PQ,
+                                           const float* C, const float* bmsg, const float* dAgg, float* dC) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= nEdges) return;
+    const int e = warp, f = 2 * lane;
+    const int j = edgeSrc[e], i = edgeDst[e];
+    float s0 = 0.f, s1 = 0.f;
+    for (int b = 0; b < B; b++) {
+        if (edgeBranch[e] == outage[b]) continue;
+        const size_t rj = ((size_t)b * nb + j) * 128, ri = ((size_t)b * nb + i) * 128;
+        const float pre0 = __bfloat162float(PQ[rj + f]) + __bfloat162float(PQ[ri + 64 + f]) + bmsg[f] + C[(size_t)e * 64 + f];
+        const float pre1 = __bfloat162float(PQ[rj + f + 1]) + __bfloat162float(PQ[ri + 64 + f + 1]) + bmsg[f + 1] +
+                           C[(size_t)e * 64 + f + 1];
+        const size_t ai = ((size_t)b * nb + i) * 64 + f;
+        if (pre0 > 0.f) s0 += dAgg[ai];
+        if (pre1 > 0.f) s1 += dAgg[ai + 1];
+    }
+    dC[(size_t)e * 64 + f] = s0;
+    dC[(size_t)e * 64 + f + 1] = s1;
+}
+
+// C[e] = Estatic[e] (4 features) . We[4 x 64] (fp32, edge-wise).
+__global__ void edgeProjectKernel(int nEdges, const float* Es, const float* We, float* C) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nEdges * 64) return;
+    const int e = i / 64, f = i % 64;
+    float s = 0.f;
+    for (int k = 0; k < 4; k++) s += Es[e * 4 + k] * We[k * 64 + f];
+    C[i] = s;
+}
+
+// dWe[4 x 64] = Es^T dC, dbmsg[64] = column sums of dC (edge order), one thread per output.
+__global__ void edgeProjectBackwardKernel(int nEdges, const float* Es, const float* dC, float* dWe, float* dbmsg) {
+    const int i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i >= 5 * 64) return;
+    const int k = i / 64, f = i % 64;
+    float s = 0.f;
+    for (int e = 0; e < nEdges; e++) s += (k < 4 ? Es[e * 4 + k] : 1.f) * dC[(size_t)e * 64 + f];
+    if (k < 4) dWe[k * 64 + f] = s;
+    else dbmsg[f] = s;
+}
+
+// dz = dOut * [z > 0] (relu) or dOut, stored bf16 [M x N] from fp32 [M x ldd]; optionally adds dOut to accum.
+__global__ void reluGradKernel(size_t count, int N, int ldd, const float* dOut, const __nv_bfloat16* z,
+                               __nv_bfloat16* dz, float* dzF) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const size_t r = i / N;
+    const int c = (int)(i % N);
+    float v = dOut[r * ldd + c];
+    if (z && __bfloat162float(z[i]) <= 0.f) v = 0.f;
+    if (dz) dz[i] = __float2bfloat16(v);
+    if (dzF) dzF[i] = v;
+}
+
+// Adam on fp32 master weights; writes the bf16 copy and the bf16 transpose (K x N -> N x K) the kernels read.
+__global__ void adamKernel(int count, int K, int N, float* w, const float* grad, float* m, float* v, float lr,
+                           float beta1, float beta2, float eps, float c1, float c2, __nv_bfloat16* wB,
+                           __nv_bfloat16* wT) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float gr = grad[i];
+    const float mi = beta1 * m[i] + (1.f - beta1) * gr;
+    const float vi = beta2 * v[i] + (1.f - beta2) * gr * gr;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    if (wB) wB[i] = __float2bfloat16(wi);
+    if (wT) {
+        const int k = i / N, n = i % N;
+        wT[n * K + k] = __float2bfloat16(wi);
+    }
+}
+
+// Mean squared error over the first 2 columns of out [M x ldo] against target [M x 2]; dOut [M x ldo] (zero beyond
+// column 1) and per-block partial sums of the squared error.
+__global__ void mseKernel(int M, int ldo, const float* out, const float* target, float* dOut, float* partial,
+                          float scale) {
+    __shared__ float red[256];
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    float s = 0.f;
+    if (r < M) {
+        for (int c = 0; c < ldo; c++) {
+            float d = 0.f;
+            if (c < 2) {
+                const float e = out[(size_t)r * ldo + c] - target[(size_t)r * 2 + c];
+                s += e * e;
+                d = 2.f * e * scale;
+            }
+            dOut[(size_t)r * ldo + c] = d;
+        }
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+// dst[r, dstCol0 + c] (+)= src[r, srcCol0 + c] for c < ncols (fp32).
+__global__ void copyColsKernel(long long count, int ncols, const float* src, int lds, int srcCol0, float* dst, int ldd,
+                               int dstCol0, int accumulate) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const long long r = i / ncols;
+    const int c = (int)(i % ncols);
+    const float v = src[r * lds + srcCol0 + c];
+    float* d = dst + r * ldd + dstCol0 + c;
+    *d = accumulate ? *d + v : v;
+}
+
+int gridFor(long long rows, int per) {
+    long long blocks = (rows + per - 1) / per;
+    return (int)(blocks < 148 * 16 ? (blocks < 1 ? 1 : blocks) : 148 * 16);
+}
+
+}  // namespace
+
+}  // namespace gnn
+}  // namespace olfb200
+
+using namespace olfb200::gnn;
+
+namespace {
+thread_local std::string gnnError;
+
+template <typename F>
+int gnnGuard(F&& f) {
+    try {
+        gnnError.clear();
+        f();
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(e));
+        return 0;
+    } catch (const std::exception& e) {
+        gnnError = e.what();
+    }
+    return -1;
+}
+}  // namespace
+
+extern "C" const char* olfgpu_gnn_last_error(void) { return gnnError.c_str(); }
+
+extern "C" int olfgpu_gnn_gemm(int M, int K1, int K2, int N, const void* A1, const void* A2, const void* W,
+                               const float* bias, int relu, const void* residual, void* outBf16, float* outF32,
+                               int ldo, void* saveZ, void* stream) {
+    return gnnGuard([&] {
+        const int grid = gridFor(M, 64);
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        auto a1 = static_cast<const __nv_bfloat16*>(A1);
+        auto a2 = static_cast<const __nv_bfloat16*>(A2);
+        auto w = static_cast<const __nv_bfloat16*>(W);
+        auto res = static_cast<const __nv_bfloat16*>(residual);
+        auto ob = static_cast<__nv_bfloat16*>(outBf16);
+        auto sz = static_cast<__nv_bfloat16*>(saveZ);
+#define OLF_GEMM(a, b2, c) gemmKernel<a, b2, c><<<grid, 128, 0, st>>>(M, a1, a2, w, bias, relu, res, ob, outF32, ldo, sz)
+        if (K1 == 16 && K2 == 0 && N == 64) OLF_GEMM(16, 0, 64);
+        else if (K1 == 64 && K2 == 0 && N == 128) OLF_GEMM(64, 0, 128);
+        else if (K1 == 64 && K2 == 64 && N == 64) OLF_GEMM(64, 64, 64);
+        else if (K1 == 64 && K2 == 0 && N == 16) OLF_GEMM(64, 0, 16);
+        else if (K1 == 128 && K2 == 0 && N == 64) OLF_GEMM(128, 0, 64);
+        else throw std::runtime_error("unsupported GEMM shape");
+#undef OLF_GEMM
+    });
+}
+
+extern "C" int olfgpu_gnn_gemm_dw(int M, int K1, int K2, int N, const void* A1, const void* A2, const void* dZ,
+                                  float* dW, float* db, float* partial, int maxChunks, void* stream) {
+    return gnnGuard([&] {
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        int chunks = maxChunks < 1 ? 1 : maxChunks;
+        int rows = (M + chunks - 1) / chunks;
+        rows = (rows + 15) / 16 * 16;
+        chunks = (M + rows - 1) / rows;
+        auto a1 = static_cast<const __nv_bfloat16*>(A1);
+        auto a2 = static_cast<const __nv_bfloat16*>(A2);
+        auto dz = static_cast<const __nv_bfloat16*>(dZ);
+#define OLF_DW(a, b2, c) gemmDwKernel<a, b2, c><<<chunks, 128, 0, st>>>(M, rows, a1, a2, dz, partial)
+        if (K1 == 16 && K2 == 0 && N == 64) OLF_DW(16, 0, 64);
+        else if (K1 == 64 && K2 == 0 && N == 128) OLF_DW(64, 0, 128);
+        else if (K1 == 64 && K2 == 64 && N == 64) OLF_DW(64, 64, 64);
+        else if (K1 == 64 && K2 == 0 && N == 16) OLF_DW(64, 0, 16);
+        else throw std::runtime_error("unsupported weight-gradient shape");
+#undef OLF_DW
+        const int KN = (K1 + K2) * N;
+        reducePartialsKernel<<<(KN + N + 255) / 256, 256, 0, st>>>(chunks, KN, N, partial, dW, db);
+    });
+}
+
+extern "C" int olfgpu_gnn_message_forward(int B, int nb, const int* inPtr, const int* inEdge, const int* edgeSrc,
+                                          const int* edgeBranch, const int* outage, const void* PQ, const float* C,
+                                          const float* bmsg, void* agg, void* stream) {
+    return gnnGuard([&] {
+        const long long warps = (long long)B * nb;
+        messageForwardKernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+            B, nb, inPtr, inEdge, edgeSrc, edgeBranch, outage, static_cast<const __nv_bfloat16*>(PQ), C, bmsg,
+            static_cast<__nv_bfloat16*>(agg));
+    });
+}
+
+extern "C" int olfgpu_gnn_message_backward(int B, int nb, int nEdges, const int* inPtr, const int* inEdge,
+                                           const int* outPtr, const int* outEdge, const int* edgeSrc,
+                                           const int* edgeDst, const int* edgeBranch, const int* outage,
+                                           const void* PQ, const float* C, const float* bmsg, const float* dAgg,
+                                           float* dPQ, float* dC, void* stream) {
+    return gnnGuard([&] {
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        const long long warps = (long long)B * nb;
+        auto pq = static_cast<const __nv_bfloat16*>(PQ);
+        messageBackwardNodesKernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(
+            B, nb, inPtr, inEdge, outPtr, outEdge, edgeSrc, edgeDst, edgeBranch, outage, pq, C, bmsg, dAgg, dPQ);
+        messageBackwardEdgesKernel<<<(unsigned)(((long long)nEdges * 32 + 255) / 256), 256, 0, st>>>(
+            B, nb, nEdges, edgeSrc, edgeDst, edgeBranch, outage, pq, C, bmsg, dAgg, dC);
+    });
+}
+
+extern "C" int olfgpu_gnn_edge_project(int nEdges, const float* Es, const float* We, float* C, void* stream) {
+    return gnnGuard([&] {
+        edgeProjectKernel<<<(nEdges * 64 + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(nEdges, Es, We, C);
+    });
+}
+
+extern "C" int olfgpu_gnn_edge_project_backward(int nEdges, const float* Es, const float* dC, float* dWe,
+                                                float* dbmsg, void* stream) {
+    return gnnGuard([&] {
+        edgeProjectBackwardKernel<<<(5 * 64 + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(nEdges, Es, dC,
+                                                                                                     dWe, dbmsg);
+    });
+}
+
+extern "C" int olfgpu_gnn_relu_grad(long long count, int N, int ldd, const float* dOut, const void* z, void* dz,
+                                    float* dzF32, void* stream) {
+    return gnnGuard([&] {
+        reluGradKernel<<<(unsigned)((count + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+            (size_t)count, N, ldd, dOut, static_cast<const __nv_bfloat16*>(z), static_cast<__nv_bfloat16*>(dz), dzF32);
+    });
+}
+
+extern "C" int olfgpu_gnn_adam(int count, int K, int N, float* w, const float* grad, float* m, float* v, float lr,
+                               float beta1, float beta2, float eps, int step, void* wBf16, void* wTBf16, void* stream) {
+    return gnnGuard([&] {
+        const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+        adamKernel<<<(count + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+            count, K, N, w, grad, m, v, lr, beta1, beta2, eps, c1, c2, static_cast<__nv_bfloat16*>(wBf16),
+            static_cast<__nv_bfloat16*>(wTBf16));
+    });
+}
+
+extern "C" int olfgpu_gnn_mse(int M, int ldo, const float* out, const float* target, float* dOut, float* partial,
+                              void* stream) {
+    return gnnGuard([&] {
+        mseKernel<<<(M + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(M, ldo, out, target, dOut, partial,
+                                                                                  1.f / (2.f * (float)M));
+    });
+}
+
+extern "C" int olfgpu_gnn_copy_cols(int M, int ncols, const float* src, int lds, int srcCol0, float* dst, int ldd,
+                                    int dstCol0, int accumulate, void* stream) {
+    return gnnGuard([&] {
+        const long long count = (long long)M * ncols;
+        copyColsKernel<<<(unsigned)((count + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+            count, ncols, src, lds, srcCol0, dst, ldd, dstCol0, accumulate);
+    });
+}

@@ -211,14 +211,15 @@ __device__ void solveLevels(const DevNet& net, const DevBatch& b, const T* lu, T
 
 }  // namespace
 
+// The whole Newton loop of one tile of L lanes (the tile index picks the lanes); the body of both persistent kernels.
 template <typename T, int L>
-__global__ void __launch_bounds__(512) newtonPersistentKernel(DevNet net, DevBatch b, DevRl rl, Settings cfg,
-                                                              PersistentPlan plan) {
+__device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl, const Settings& cfg,
+                           const PersistentPlan& plan, int tile) {
     const int tid = threadIdx.x;
     const int lane = tid % L;
     const int slot = tid / L;
     const int slots = blockDim.x / L;
-    const int s0 = blockIdx.x * L;
+    const int s0 = tile * L;
     const int s = s0 + lane;
     const size_t S = b.S;
     T* lu = sizeof(T) == 8 ? reinterpret_cast<T*>(b.lu64) : reinterpret_cast<T*>(b.lu32);
@@ -576,6 +577,46 @@ __global__ void __launch_bounds__(512) newtonPersistentKernel(DevNet net, DevBat
         b.active[sl] = 0;
         b.trouble[sl] = ts.trouble[tid];
     }
+}
+
+template <typename T, int L>
+__global__ void __launch_bounds__(512) newtonPersistentKernel(DevNet net, DevBatch b, DevRl rl, Settings cfg,
+                                                              PersistentPlan plan) {
+    newtonTile<T, L>(net, b, rl, cfg, plan, blockIdx.x);
+}
+
+// One launch over several grids: CTA k runs tile (k - tileBegin) of the item whose tile range holds k.
+template <typename T, int L>
+__global__ void __launch_bounds__(512) newtonMultiKernel(const MultiItem* items, int nItems) {
+    __shared__ MultiItem it;    // the item's descriptors staged once per CTA (read on every access of the loop)
+    if (threadIdx.x == 0) {
+        int k = 0;
+        while (k + 1 < nItems && static_cast<int>(blockIdx.x) >= items[k + 1].tileBegin) k++;
+        it = items[k];
+    }
+    __syncthreads();
+    newtonTile<T, L>(it.net, it.b, it.rl, it.cfg, it.plan, blockIdx.x - it.tileBegin);
+}
+
+void launchMulti(const MultiItem* itemsDevice, int nItems, int totalTiles, int lanesPerTile, int threads, bool fp32,
+                 cudaStream_t st) {
+#define OLF_MULTI(T_, L_) newtonMultiKernel<T_, L_><<<totalTiles, threads, 0, st>>>(itemsDevice, nItems)
+    if (fp32) {
+        switch (lanesPerTile) {
+            case 1: OLF_MULTI(float, 1); break;
+            case 2: OLF_MULTI(float, 2); break;
+            case 4: OLF_MULTI(float, 4); break;
+            default: OLF_MULTI(float, 8); break;
+        }
+    } else {
+        switch (lanesPerTile) {
+            case 1: OLF_MULTI(double, 1); break;
+            case 2: OLF_MULTI(double, 2); break;
+            case 4: OLF_MULTI(double, 4); break;
+            default: OLF_MULTI(double, 8); break;
+        }
+    }
+#undef OLF_MULTI
 }
 
 // Factorization levels [l0, l1) for every tile (the narrow top of the elimination tree in the level schedule).

@@ -1,0 +1,257 @@
+"""Learned warm start for batched N-1: data from the engine's own solves, training on the GPU with the library's
+kernels, and prediction of every scenario's start state, with the plain Newton judging every scenario.
+
+* Training data: for load scalings s ~ U[0.8, 1.2] of the grid, the base case is solved on the engine, then a batch of
+  random non-bridge branch outages warm-started from it; each converged scenario gives one sample (the base case's
+  node features, the outaged branch, the per-bus change (dVm, dVa) of the solution).
+* Prediction: x0 = base state + the network's (dVm, dVa); identity rows (slack angle, PV magnitudes) start at their
+  targets.  Any scenario the Newton does not converge from the learned start is solved again from the base-case
+  start (the fallback), so the result never depends on the network beyond the iteration count.
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+from typing import List, Optional
+
+import numpy as np
+
+from . import native, packing
+from .gnn import FEAT_IN, GraphData, WarmStartNet
+
+
+N_FEAT = 7            # per-bus base-case features; columns 7..9 carry the per-sample outage features
+
+
+def branch_flows(g, x_base: np.ndarray):
+    """Base-case active and reactive flow leaving bus 1 (side 1) of every closed branch (pi model, per unit)."""
+    vm, va = x_base[1::2], x_base[0::2]
+    y = 1.0 / np.hypot(g.r, g.x)
+    ksi = np.arctan2(g.r, g.x)
+    v1, v2, r1 = vm[g.f], vm[g.t], g.ratio
+    th = ksi - va[g.f] + va[g.t]
+    p1 = r1 * v1 * (y * r1 * v1 * np.sin(ksi) - y * v2 * np.sin(th))
+    q1 = r1 * v1 * (-g.b / 2 * r1 * v1 + y * r1 * v1 * np.cos(ksi) - y * v2 * np.cos(th))
+    return p1, q1
+
+
+def node_features(p, x_base: np.ndarray) -> np.ndarray:
+    """[nb, 7]: base-case Vm, Va, net P, net Q (PQ rows; 0 on voltage-controlled rows), PQ / PV / slack flags."""
+    nb = p.n_bus
+    vm, va = x_base[1::2], x_base[0::2]
+    P = p.target[0::2].copy()
+    slack = p.base_row_mode[0::2] == packing.FIXED_VARIABLE
+    P[slack] = 0.0
+    pv = p.base_row_mode[1::2] == packing.FIXED_VARIABLE
+    Q = np.where(pv, 0.0, p.target[1::2])
+    return np.stack([vm, va, P, Q, (~pv).astype(float), (pv & ~slack).astype(float), slack.astype(float)], axis=1)
+
+
+@dataclasses.dataclass
+class Dataset:
+    x: "object"          # [nScalings, nb, 16] bf16 normalised node features (outage columns zero)
+    t: "object"          # [nSamples, nb, 2] fp32 normalised targets
+    scaling: "object"    # [nSamples] int64 index into x
+    outage: "object"     # [nSamples] int32 closed-branch index
+    flows: "object"      # [nScalings, nBranches, 2] fp32 base-case (P, Q) flows, already scaled by flow_std
+    feat_mean: np.ndarray
+    feat_std: np.ndarray
+    tgt_std: np.ndarray
+    flow_std: float
+
+
+class LearnedStart:
+    def __init__(self, grid, layers: int = 4, seed: int = 0, net: Optional[WarmStartNet] = None):
+        self.grid = grid
+        self.graph = GraphData.from_grid(grid)
+        self.net = net or WarmStartNet(self.graph, layers, seed)
+        self.feat_mean = None
+        self.feat_std = None
+        self.tgt_std = None
+        self.flow_std = 1.0
+
+    # ------------------------------------------------------------------------------------------------------------
+    def solve_base(self, g, x_start: np.ndarray) -> np.ndarray:
+        p = packing.pack(g, with_reactive_limits=False)
+        s = native.Structure(p)
+        ctx = native.BatchContext(s, 1)
+        r = ctx.solve(x_start, p.target, p.base_row_mode, np.zeros((1, p.n_elements), np.uint8))
+        if int(r[0, -1]) != native.CONVERGED:
+            raise RuntimeError("base case does not converge")
+        return r[0, :p.n].copy()
+
+    def generate(self, n_scalings: int, outages_per_scaling: int, seed: int, lo: float = 0.8, hi: float = 1.2,
+                 precision: int = native.FP64) -> Dataset:
+        """Samples from the engine's own N-1 solves at n_scalings random load scalings."""
+        import torch
+        from . import synthetic
+        rng = np.random.default_rng(seed)
+        base_grid = self.grid
+        p0 = packing.pack(base_grid, with_reactive_limits=False)
+        x_ref = p0.x_base if p0.x_base is not None else p0.x_flat
+        cand = synthetic.outage_candidates(base_grid)
+        feats, targets, scal, outs, flows = [], [], [], [], []
+        s0 = native.Structure(p0)
+        ctx = native.BatchContext(s0, outages_per_scaling)
+        ctx.set_linear_solver_settings(precision, 1)
+        for k in range(n_scalings):
+            sc = float(rng.uniform(lo, hi))
+            g = base_grid.scaled(sc)
+            p = packing.pack(g, with_reactive_limits=False)
+            try:
+                xb = self.solve_base(g, x_ref)
+            except RuntimeError:
+                continue                                    # no base case at this loading: no sample
+            o = np.sort(rng.choice(cand, size=outages_per_scaling, replace=False))
+            r = ctx.solve(xb, p.target, p.base_row_mode, p.outage_masks(o))
+            ok = r[:, -1] == native.CONVERGED
+            idx = len(feats)
+            feats.append(node_features(p, xb))
+            flows.append(np.stack(branch_flows(g, xb), axis=1))
+            d = np.stack([r[ok, 1:p.n:2] - xb[1::2], r[ok, 0:p.n:2] - xb[0::2]], axis=2)   # [k, nb, 2]
+            targets.append(d.astype(np.float32))
+            scal.append(np.full(int(ok.sum()), idx, np.int64))
+            outs.append(o[ok].astype(np.int32))
+        if not feats:
+            raise RuntimeError("no load scaling had a solvable base case")
+        f = np.stack(feats)                                         # [nS, nb, 7]
+        mean = f.reshape(-1, N_FEAT).mean(0)
+        std = np.maximum(f.reshape(-1, N_FEAT).std(0), 1e-6)
+        mean[4:] = 0.0
+        std[4:] = 1.0
+        fx = np.zeros((f.shape[0], f.shape[1], FEAT_IN), np.float32)
+        fx[..., :N_FEAT] = (f - mean) / std
+        fl = np.stack(flows).astype(np.float32)
+        flow_std = float(max(fl.std(), 1e-6))
+        t = np.concatenate(targets)
+        tstd = np.maximum(t.reshape(-1, 2).std(0), 1e-9).astype(np.float32)
+        dev = torch.device("cuda")
+        self.feat_mean, self.feat_std, self.tgt_std, self.flow_std = mean, std, tstd, flow_std
+        return Dataset(torch.from_numpy(fx).to(dev).to(torch.bfloat16), torch.from_numpy(t / tstd).to(dev),
+                       torch.from_numpy(np.concatenate(scal)).to(dev), torch.from_numpy(np.concatenate(outs)).to(dev),
+                       torch.from_numpy(fl / flow_std).to(dev), mean, std, tstd, flow_std)
+
+    def _batch_inputs(self, xs, flows, outages):
+        """Node inputs [B * nb, 16] bf16: the scaling's features plus the per-sample outage columns (7..9)."""
+        import torch
+        g = self.grid
+        B = outages.shape[0]
+        nb = self.graph.nb
+        x = xs.clone() if xs.dim() == 3 else xs.unsqueeze(0).expand(B, nb, FEAT_IN).clone()
+        fidx = torch.from_numpy(g.f.astype(np.int64)).to(x.device)[outages.long()]
+        tidx = torch.from_numpy(g.t.astype(np.int64)).to(x.device)[outages.long()]
+        rows = torch.arange(B, device=x.device)
+        fl = flows[rows, outages.long()] if flows.dim() == 3 else flows[outages.long()]
+        one = torch.ones(B, device=x.device, dtype=x.dtype)
+        x[rows, fidx, N_FEAT] = one
+        x[rows, tidx, N_FEAT] = one
+        x[rows, fidx, N_FEAT + 1] = fl[:, 0].to(x.dtype)
+        x[rows, tidx, N_FEAT + 1] = (-fl[:, 0]).to(x.dtype)
+        x[rows, fidx, N_FEAT + 2] = fl[:, 1].to(x.dtype)
+        x[rows, tidx, N_FEAT + 2] = (-fl[:, 1]).to(x.dtype)
+        return x.reshape(B * nb, FEAT_IN).contiguous()
+
+    def train(self, data: Dataset, epochs: int = 3, batch: int = 32, lr: float = 2e-3, seed: int = 0,
+              log: Optional[list] = None, max_seconds: Optional[float] = None) -> List[float]:
+        """Adam on minibatches; the learning rate decays linearly to 10 % over the run.  Returns per-epoch losses."""
+        import torch
+        self.feat_mean, self.feat_std, self.tgt_std = data.feat_mean, data.feat_std, data.tgt_std
+        self.flow_std = data.flow_std
+        n = data.t.shape[0]
+        nb = self.graph.nb
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(seed)
+        steps_total = epochs * max(1, n // batch)
+        step = 0
+        losses = []
+        t0 = time.time()
+        for ep in range(epochs):
+            perm = torch.randperm(n, device="cuda", generator=gen)
+            acc, cnt = 0.0, 0
+            for a in range(0, n - batch + 1, batch):
+                idx = perm[a:a + batch]
+                out = data.outage[idx].contiguous()
+                sc = data.scaling[idx]
+                x0 = self._batch_inputs(data.x[sc], data.flows[sc], out)
+                tg = data.t[idx].reshape(batch * nb, 2).contiguous()
+                rate = lr * (1.0 - 0.9 * step / max(1, steps_total))
+                loss = self.net.loss_and_grad(x0, out, tg)
+                self.net.adam(rate)
+                acc += loss
+                cnt += 1
+                step += 1
+                if log is not None and step % 100 == 0:
+                    log.append((step, loss))
+                if max_seconds is not None and time.time() - t0 > max_seconds:
+                    break
+            losses.append(acc / max(cnt, 1))
+            if max_seconds is not None and time.time() - t0 > max_seconds:
+                break
+        torch.cuda.synchronize()
+        return losses
+
+    # ------------------------------------------------------------------------------------------------------------
+    def predict(self, p, x_base: np.ndarray, outages: np.ndarray, chunk: int = 128):
+        """Start states [nS, n] (float64, on the host) for the outages, from the base case state."""
+        import torch
+        nb = p.n_bus
+        f = node_features(p, x_base)
+        fx = np.zeros((nb, FEAT_IN), np.float32)
+        fx[:, :N_FEAT] = (f - self.feat_mean) / self.feat_std
+        xf = torch.from_numpy(fx).cuda().to(torch.bfloat16)
+        # branch impedances do not depend on the loading: the flows come from this grid's branches and x_base
+        fl = torch.from_numpy(np.stack(branch_flows(self.grid, x_base), axis=1).astype(np.float32) /
+                              self.flow_std).cuda()
+        outs = torch.from_numpy(np.asarray(outages, np.int32)).cuda()
+        ns = outs.shape[0]
+        res = torch.empty((ns, nb, 2), dtype=torch.float32, device="cuda")
+        for a in range(0, ns, chunk):
+            b = min(ns, a + chunk)
+            o = outs[a:b].contiguous()
+            x0 = self._batch_inputs(xf, fl, o)
+            out = self.net.forward(x0, o)
+            res[a:b] = out[:, :2].reshape(b - a, nb, 2)
+        d = res.cpu().numpy().astype(np.float64) * self.tgt_std
+        x0 = np.tile(x_base, (ns, 1))
+        x0[:, 1::2] += d[:, :, 0]
+        x0[:, 0::2] += d[:, :, 1]
+        ident = p.base_row_mode == packing.FIXED_VARIABLE
+        x0[:, ident] = p.target[ident]
+        return x0
+
+    def save(self, path: str):
+        self.net.save(path, {"feat_mean": self.feat_mean, "feat_std": self.feat_std, "tgt_std": self.tgt_std,
+                             "flow_std": np.array(self.flow_std), "fingerprint": fingerprint(self.grid)})
+
+    @staticmethod
+    def load(path: str, grid) -> "LearnedStart":
+        graph = GraphData.from_grid(grid)
+        net, extra = WarmStartNet.load(path, graph)
+        if not np.array_equal(extra["fingerprint"], fingerprint(grid)):
+            raise ValueError("checkpoint was trained on another grid")
+        ls = LearnedStart(grid, net=net)
+        ls.feat_mean, ls.feat_std, ls.tgt_std = extra["feat_mean"], extra["feat_std"], extra["tgt_std"]
+        ls.flow_std = float(extra["flow_std"])
+        return ls
+
+
+def fingerprint(grid) -> np.ndarray:
+    """A few numbers that identify the grid's topology and parameters."""
+    return np.array([grid.n_bus, grid.f.shape[0], float(np.sum(grid.f * 7 + grid.t * 13)), float(np.sum(grid.r)),
+                     float(np.sum(grid.x)), float(grid.scale)])
+
+
+def solve_with_fallback(ctx, p, x0_learned: np.ndarray, x_base: np.ndarray, disabled: np.ndarray, **kw):
+    """Solve from the learned starts; scenarios that did not converge are solved again from the base start."""
+    r = ctx.solve(None, p.target, p.base_row_mode, disabled, x0_full=x0_learned, **kw).copy()
+    _, _, tot = ctx.last_stats()
+    tot = tot.copy()
+    bad = np.flatnonzero(r[:, -1] != native.CONVERGED)
+    if bad.size:
+        x0 = x0_learned.copy()
+        x0[bad] = x_base
+        r2 = ctx.solve(None, p.target, p.base_row_mode, disabled, x0_full=x0, **kw)
+        _, _, tot2 = ctx.last_stats()
+        r[bad] = r2[bad]
+        tot[bad] += tot2[bad]
+    return r, tot, bad

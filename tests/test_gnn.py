@@ -1,0 +1,167 @@
+"""Learned warm start: the library's BF16 graph-network kernels against float64 references (needs a B200)."""
+import numpy as np
+import pytest
+
+from conftest import grid
+
+pytestmark = pytest.mark.gpu
+
+# BF16 activations and weights with FP32 accumulation: ~3 significant digits
+REL_FWD = 3e-2
+REL_GRAD = 6e-2
+
+
+def _bf16_round(a):
+    import torch
+    return torch.from_numpy(np.asarray(a, np.float32)).to(torch.bfloat16).to(torch.float64).numpy()
+
+
+@pytest.mark.parametrize("k1,k2,n", [(16, 0, 64), (64, 0, 128), (64, 64, 64), (64, 0, 16), (128, 0, 64)])
+def test_gemm_matches_float64(engine_lib, k1, k2, n):
+    import torch
+    from olfgpu import gnn
+    rng = np.random.default_rng(k1 + k2 + n)
+    M = 1000
+    a1 = rng.standard_normal((M, k1)).astype(np.float32)
+    a2 = rng.standard_normal((M, k2)).astype(np.float32) if k2 else None
+    w = (rng.standard_normal((k1 + k2, n)) / 8).astype(np.float32)
+    bias = rng.standard_normal(n).astype(np.float32)
+    res = rng.standard_normal((M, n)).astype(np.float32)
+    d = lambda x: torch.from_numpy(x).cuda().to(torch.bfloat16).contiguous()  # noqa: E731
+    A1, A2, W, R = d(a1), (d(a2) if k2 else None), d(w), d(res)
+    B = torch.from_numpy(bias).cuda()
+    out = torch.empty((M, n), dtype=torch.float32, device="cuda")
+    z = torch.empty((M, n), dtype=torch.bfloat16, device="cuda")
+    gnn._call("olfgpu_gnn_gemm", M, k1, k2, n, gnn._ptr(A1), gnn._ptr(A2), gnn._ptr(W), gnn._ptr(B), 1, gnn._ptr(R),
+              None, gnn._ptr(out), n, gnn._ptr(z), gnn._stream())
+    torch.cuda.synchronize()
+    aa = np.concatenate([_bf16_round(a1)] + ([_bf16_round(a2)] if k2 else []), axis=1)
+    ref_z = np.maximum(aa @ _bf16_round(w) + bias, 0)
+    ref = ref_z + _bf16_round(res)
+    assert np.max(np.abs(out.cpu().numpy() - ref)) / np.max(np.abs(ref)) < 1e-5
+    assert np.max(np.abs(z.float().cpu().numpy() - ref_z)) / np.max(np.abs(ref_z)) < 1e-2
+
+
+@pytest.mark.parametrize("k1,k2,n", [(16, 0, 64), (64, 0, 128), (64, 64, 64), (64, 0, 16)])
+def test_weight_gradient_matches_float64(engine_lib, k1, k2, n):
+    import torch
+    from olfgpu import gnn
+    rng = np.random.default_rng(7 + k1 + n)
+    M = 5000
+    a1 = rng.standard_normal((M, k1)).astype(np.float32)
+    a2 = rng.standard_normal((M, k2)).astype(np.float32) if k2 else None
+    dz = rng.standard_normal((M, n)).astype(np.float32)
+    d = lambda x: torch.from_numpy(x).cuda().to(torch.bfloat16).contiguous()  # noqa: E731
+    dw = torch.empty((k1 + k2, n), dtype=torch.float32, device="cuda")
+    db = torch.empty(n, dtype=torch.float32, device="cuda")
+    partial = torch.empty(37 * ((k1 + k2) * n + n), dtype=torch.float32, device="cuda")
+    A1, A2, DZ = d(a1), (d(a2) if k2 else None), d(dz)      # keep the inputs alive until the kernel has run
+    gnn._call("olfgpu_gnn_gemm_dw", M, k1, k2, n, gnn._ptr(A1), gnn._ptr(A2), gnn._ptr(DZ), gnn._ptr(dw),
+              gnn._ptr(db), gnn._ptr(partial), 37, gnn._stream())
+    torch.cuda.synchronize()
+    aa = np.concatenate([_bf16_round(a1)] + ([_bf16_round(a2)] if k2 else []), axis=1)
+    ref = aa.T @ _bf16_round(dz)
+    assert np.max(np.abs(dw.cpu().numpy() - ref)) / np.max(np.abs(ref)) < 1e-4
+    assert np.max(np.abs(db.cpu().numpy() - _bf16_round(dz).sum(0))) < 1e-2
+
+
+def _small_problem(name="grid118", B=4, seed=0):
+    import torch
+    from olfgpu import synthetic
+    from olfgpu.gnn import FEAT_IN, GraphData, WarmStartNet, init_params
+    g, p = grid(name)
+    graph = GraphData.from_grid(g)
+    rng = np.random.default_rng(seed)
+    params = init_params(4, seed)
+    # give the biases and the padded output columns non-trivial values so every path is exercised
+    for k in params:
+        if k.startswith("b_"):
+            params[k] = (rng.standard_normal(params[k].shape) * 0.05).astype(np.float32)
+    net = WarmStartNet(graph, 4, params=params)
+    x0 = np.zeros((B * g.n_bus, FEAT_IN), np.float32)
+    x0[:, :7] = rng.standard_normal((B * g.n_bus, 7))
+    outs = synthetic.outage_candidates(g)[:B].astype(np.int32)
+    target = rng.standard_normal((B * g.n_bus, 2)).astype(np.float32)
+    x0b = torch.from_numpy(x0).cuda().to(torch.bfloat16)
+    gnp = {k: getattr(graph, k).cpu().numpy() for k in ("src", "dst", "branch", "es")}
+    return g, graph, net, params, x0, x0b, outs, target, gnp
+
+
+def test_forward_and_gradients_match_the_float64_oracle(engine_lib):
+    import torch
+    from oracle import gnn_oracle
+    g, graph, net, params, x0, x0b, outs, target, gnp = _small_problem()
+    out = net.forward(x0b, torch.from_numpy(outs).cuda(), keep=False).cpu().numpy()
+    loss_ref, out_ref, grads_ref = gnn_oracle.loss_and_grads(params, _bf16_round(x0), outs, target, gnp, g.n_bus, 4)
+    assert np.max(np.abs(out[:, :2] - out_ref[:, :2])) / np.max(np.abs(out_ref[:, :2])) < REL_FWD
+    loss = net.loss_and_grad(x0b, torch.from_numpy(outs).cuda(), torch.from_numpy(target).cuda())
+    assert abs(loss - loss_ref) / loss_ref < REL_FWD
+    for k, gr in grads_ref.items():
+        mine = net.grad[k].cpu().numpy().reshape(gr.shape)
+        if k == "w_out" or k == "b_out":
+            mine, gr = mine[..., :2], gr[..., :2]
+        rel = np.linalg.norm(mine - gr) / max(np.linalg.norm(gr), 1e-12)
+        assert rel < REL_GRAD, (k, rel)
+
+
+def test_backward_is_deterministic(engine_lib):
+    import torch
+    g, graph, net, params, x0, x0b, outs, target, gnp = _small_problem(B=6, seed=3)
+    o = torch.from_numpy(outs).cuda()
+    t = torch.from_numpy(target).cuda()
+    net.loss_and_grad(x0b, o, t)
+    first = {k: v.clone() for k, v in net.grad.items()}
+    net.loss_and_grad(x0b, o, t)
+    for k in first:
+        assert torch.equal(first[k], net.grad[k]), k
+
+
+def test_checkpoint_resume_is_exact(engine_lib, tmp_path):
+    import torch
+    from olfgpu.gnn import WarmStartNet
+    g, graph, net, params, x0, x0b, outs, target, gnp = _small_problem(B=3, seed=5)
+    o, t = torch.from_numpy(outs).cuda(), torch.from_numpy(target).cuda()
+    for _ in range(3):
+        net.loss_and_grad(x0b, o, t)
+        net.adam(1e-3)
+    path = str(tmp_path / "ckpt.npz")
+    net.save(path)
+    for _ in range(2):
+        net.loss_and_grad(x0b, o, t)
+        net.adam(1e-3)
+    resumed, _ = WarmStartNet.load(path, graph)
+    for _ in range(2):
+        resumed.loss_and_grad(x0b, o, t)
+        resumed.adam(1e-3)
+    for k in net.w:
+        assert torch.equal(net.w[k], resumed.w[k]), k
+
+
+def test_learned_start_trains_and_saves_newton_iterations(engine_lib, oracle_mod):
+    """On the 2,000-bus grid: training lowers the loss; the learned start needs fewer Newton iterations than the
+    base-case start on held-out outages at a fresh load scaling, and every scenario still matches the oracle."""
+    from olfgpu import native, packing, synthetic
+    from olfgpu.learned_start import LearnedStart, solve_with_fallback
+    g, p = grid("grid2000")
+    ls = LearnedStart(g, seed=1)
+    data = ls.generate(n_scalings=24, outages_per_scaling=128, seed=2, lo=0.9, hi=1.1)
+    losses = ls.train(data, epochs=3, batch=16, lr=2e-3)
+    assert losses[-1] < 0.5 * losses[0]
+    gs = g.scaled(1.03)
+    ps = packing.pack(gs, with_reactive_limits=False)
+    xb = ls.solve_base(gs, p.x_base)
+    rng = np.random.default_rng(99)
+    outs = np.sort(rng.choice(synthetic.outage_candidates(g), size=160, replace=False))
+    dis = ps.outage_masks(outs)
+    s = native.Structure(ps)
+    ctx = native.BatchContext(s, outs.shape[0])
+    base = ctx.solve(xb, ps.target, ps.base_row_mode, dis).copy()
+    _, _, it_base = ctx.last_stats()
+    it_base = it_base.copy()
+    x0 = ls.predict(ps, xb, outs)
+    learned, it_learned, bad = solve_with_fallback(ctx, ps, x0, xb, dis)
+    ref = oracle_mod.Structure(ps).solve_batch(xb, dis)
+    assert np.array_equal(learned[:, -1], ref[:, -1])
+    conv = ref[:, -1] == 0
+    assert np.max(np.abs(learned[conv, :p.n] - ref[conv, :p.n])) <= 1e-8
+    assert it_learned[conv].mean() < it_base[conv].mean()
