@@ -24,7 +24,7 @@ import numpy as np
 from . import native
 
 H = 64
-FEAT_IN = 16          # 7 node features padded to the 16-column tensor-core tile
+FEAT_IN = 16          # 10 input features (7 per bus, 3 of the scenario's outage) padded to the 16-column MMA tile
 FEAT_OUT = 16         # 2 outputs padded to 16 columns
 
 
