@@ -124,6 +124,32 @@ int olfgpu_solve_batch_context(int64_t context, const double* x0Base, const doub
 int olfgpu_last_solve_stats(int64_t context, float* deviceMs, int* batchedIterations, int* totalIterations);
 
 /*
+ * Uneven batching across grids (no counterpart in the reference, whose GpuBatchedAcSecurityAnalysis runs one network
+ * per batch).  olfgpu_stage_batch_context validates a request and uploads its inputs exactly as
+ * olfgpu_solve_batch_context does, without running it.  A multi-grid context groups batch contexts of different
+ * structures on one device and one precision; olfgpu_solve_multi_context runs every member's staged batch through ONE
+ * persistent launch (one CTA per tile of lanesPerTile lanes of any member, the whole Newton loop with reactive limits
+ * inside; captured with the result gathers in a CUDA graph) and writes member i's results into outs[i]
+ * ([nScenarios_i][n_i + 3], as olfgpu_solve_batch_context; null skips the copy); deviceMs receives the device time
+ * from the first install to the last result.  Members' olfgpu_last_solve_stats report their per-scenario iterations
+ * afterwards.  olfgpu_set_multi_schedule fixes the tile (lanesPerTile 1, 2, 4 or 8; threads 256 or 512; order 0 as
+ * given, 1 the grids with the most buses first) or, with lanesPerTile -1, lets the next solve time every candidate
+ * and keep the fastest; olfgpu_get_multi_schedule reports the schedule in force and the timings
+ * {lanesPerTile, threads, order, ms} of the last autotune.
+ */
+int olfgpu_stage_batch_context(int64_t context, const double* x0Base, const double* x0Full, const double* targetBase,
+                               const int* baseRowMode, int nRowModeEntries, const int* rowModeEntries,
+                               int nScenarios, int nElements, const unsigned char* disabled, int nTargetOverrides,
+                               const int* targetOverrideIndex, const double* targetOverrideValue, int maxIter,
+                               double tol, double reactiveLimitTol, int maxOuter, int maxPqPvSwitch);
+int olfgpu_create_multi_context(int nContexts, const int64_t* contexts, int64_t* multiOut);
+int olfgpu_destroy_multi_context(int64_t multi);
+int olfgpu_set_multi_schedule(int64_t multi, int lanesPerTile, int threads, int order);
+int olfgpu_get_multi_schedule(int64_t multi, int* lanesPerTile, int* threads, int* order, int maxResults,
+                              double* results, int* nResults);
+int olfgpu_solve_multi_context(int64_t multi, double* const* outs, float* deviceMs);
+
+/*
  * Test surface of the engine (the role BatchedLuNative plays for the reference's LU, BatchedLuNative.java:121-125):
  * the Jacobian values in the reference-compatible CSR layout and the mismatch of each scenario at the states xFull
  * [nScenarios][n], through the engine's fill; and a batched linear solve J z = rhs through the engine's block LU

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "engine.hpp"
 
@@ -41,6 +42,42 @@ BatchContext& contextOf(int64_t h) {
     auto* p = reinterpret_cast<BatchContext*>(h);
     if (!p) throw std::runtime_error("invalid batch solver context");
     return *p;
+}
+
+MultiContext& multiOf(int64_t h) {
+    auto* p = reinterpret_cast<MultiContext*>(h);
+    if (!p) throw std::runtime_error("invalid multi-grid context");
+    return *p;
+}
+
+SolveRequest requestOf(const double* x0Base, const double* x0Full, const double* targetBase, const int* baseRowMode,
+                       int nRowModeEntries, const int* rowModeEntries, int nScenarios, int nElements,
+                       const unsigned char* disabled, int nTargetOverrides, const int* targetOverrideIndex,
+                       const double* targetOverrideValue, int maxIter, double tol, double reactiveLimitTol,
+                       int maxOuter, int maxPqPvSwitch) {
+    if (nRowModeEntries < 0 || nTargetOverrides < 0 || nElements < 0) throw std::runtime_error("negative count");
+    if ((nRowModeEntries && !rowModeEntries) || (nTargetOverrides && (!targetOverrideIndex || !targetOverrideValue))) {
+        throw std::runtime_error("null array with a non-zero count");
+    }
+    SolveRequest r;
+    r.x0Base = x0Base;
+    r.x0Full = x0Full;
+    r.targetBase = targetBase;
+    r.baseRowMode = baseRowMode;
+    r.nRowModeEntries = nRowModeEntries;
+    r.rowModeEntries = rowModeEntries;
+    r.nScenarios = nScenarios;
+    r.nElements = nElements;
+    r.disabled = disabled;
+    r.nTargetOverrides = nTargetOverrides;
+    r.targetOverrideIndex = targetOverrideIndex;
+    r.targetOverrideValue = targetOverrideValue;
+    r.maxIter = maxIter;
+    r.tol = tol;
+    r.reactiveLimitTol = reactiveLimitTol;
+    r.maxOuter = maxOuter;
+    r.maxPqPvSwitch = maxPqPvSwitch;
+    return r;
 }
 
 }  // namespace
@@ -206,29 +243,86 @@ extern "C" int olfgpu_solve_batch_context(int64_t context, const double* x0Base,
                                           int maxPqPvSwitch, double* out) {
     return guarded([&] {
         BatchContext& c = contextOf(context);
-        if (nRowModeEntries < 0 || nTargetOverrides < 0 || nElements < 0) throw std::runtime_error("negative count");
-        if ((nRowModeEntries && !rowModeEntries) || (nTargetOverrides && (!targetOverrideIndex || !targetOverrideValue))) {
-            throw std::runtime_error("null array with a non-zero count");
-        }
-        SolveRequest r;
-        r.x0Base = x0Base;
-        r.x0Full = x0Full;
-        r.targetBase = targetBase;
-        r.baseRowMode = baseRowMode;
-        r.nRowModeEntries = nRowModeEntries;
-        r.rowModeEntries = rowModeEntries;
-        r.nScenarios = nScenarios;
-        r.nElements = nElements;
-        r.disabled = disabled;
-        r.nTargetOverrides = nTargetOverrides;
-        r.targetOverrideIndex = targetOverrideIndex;
-        r.targetOverrideValue = targetOverrideValue;
-        r.maxIter = maxIter;
-        r.tol = tol;
-        r.reactiveLimitTol = reactiveLimitTol;
-        r.maxOuter = maxOuter;
-        r.maxPqPvSwitch = maxPqPvSwitch;
+        const SolveRequest r = requestOf(x0Base, x0Full, targetBase, baseRowMode, nRowModeEntries, rowModeEntries,
+                                         nScenarios, nElements, disabled, nTargetOverrides, targetOverrideIndex,
+                                         targetOverrideValue, maxIter, tol, reactiveLimitTol, maxOuter, maxPqPvSwitch);
         solveBatch(c, r, out);
+    });
+}
+
+extern "C" int olfgpu_stage_batch_context(int64_t context, const double* x0Base, const double* x0Full,
+                                          const double* targetBase, const int* baseRowMode, int nRowModeEntries,
+                                          const int* rowModeEntries, int nScenarios, int nElements,
+                                          const unsigned char* disabled, int nTargetOverrides,
+                                          const int* targetOverrideIndex, const double* targetOverrideValue,
+                                          int maxIter, double tol, double reactiveLimitTol, int maxOuter,
+                                          int maxPqPvSwitch) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        const SolveRequest r = requestOf(x0Base, x0Full, targetBase, baseRowMode, nRowModeEntries, rowModeEntries,
+                                         nScenarios, nElements, disabled, nTargetOverrides, targetOverrideIndex,
+                                         targetOverrideValue, maxIter, tol, reactiveLimitTol, maxOuter, maxPqPvSwitch);
+        stageRequest(c, r);
+    });
+}
+
+extern "C" int olfgpu_create_multi_context(int nContexts, const int64_t* contexts, int64_t* multiOut) {
+    return guarded([&] {
+        if (!multiOut) throw std::runtime_error("null output handle");
+        *multiOut = 0;
+        if (nContexts < 1 || !contexts) throw std::runtime_error("no batch contexts");
+        std::vector<BatchContext*> members;
+        for (int i = 0; i < nContexts; i++) members.push_back(&contextOf(contexts[i]));
+        *multiOut = reinterpret_cast<int64_t>(createMultiContext(members));
+    });
+}
+
+extern "C" int olfgpu_destroy_multi_context(int64_t multi) {
+    return guarded([&] { delete reinterpret_cast<MultiContext*>(multi); });
+}
+
+extern "C" int olfgpu_set_multi_schedule(int64_t multi, int lanesPerTile, int threads, int order) {
+    return guarded([&] {
+        MultiContext& m = multiOf(multi);
+        if (lanesPerTile == -1) {
+            m.autotunePending = true;
+            return;
+        }
+        if (lanesPerTile != 1 && lanesPerTile != 2 && lanesPerTile != 4 && lanesPerTile != 8) {
+            throw std::runtime_error("lanesPerTile must be 1, 2, 4 or 8 (or -1: autotune)");
+        }
+        if (threads != 256 && threads != 512) throw std::runtime_error("threads must be 256 or 512");
+        if (order != 0 && order != 1) throw std::runtime_error("order must be 0 (as given) or 1 (most buses first)");
+        m.lanesPerTile = lanesPerTile;
+        m.threads = threads;
+        m.order = order;
+        m.autotunePending = false;
+    });
+}
+
+extern "C" int olfgpu_get_multi_schedule(int64_t multi, int* lanesPerTile, int* threads, int* order, int maxResults,
+                                         double* results, int* nResults) {
+    return guarded([&] {
+        MultiContext& m = multiOf(multi);
+        if (lanesPerTile) *lanesPerTile = m.lanesPerTile;
+        if (threads) *threads = m.threads;
+        if (order) *order = m.order;
+        const int k = std::min<int>(maxResults, static_cast<int>(m.tuning.size()));
+        for (int i = 0; results && i < k; i++) {
+            results[4 * i] = m.tuning[i].lanesPerTile;
+            results[4 * i + 1] = m.tuning[i].threads;
+            results[4 * i + 2] = m.tuning[i].order;
+            results[4 * i + 3] = m.tuning[i].ms;
+        }
+        if (nResults) *nResults = static_cast<int>(m.tuning.size());
+    });
+}
+
+extern "C" int olfgpu_solve_multi_context(int64_t multi, double* const* outs, float* deviceMs) {
+    return guarded([&] {
+        MultiContext& m = multiOf(multi);
+        solveMulti(m, outs);
+        if (deviceMs) *deviceMs = m.lastMs;
     });
 }
 

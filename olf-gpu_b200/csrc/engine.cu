@@ -758,7 +758,7 @@ void autotune(BatchContext& ctx) {
 
 }  // namespace
 
-void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out) {
+void stageRequest(BatchContext& ctx, const SolveRequest& req) {
     OLF_CUDA(cudaSetDevice(ctx.device));
     const Structure& s = ctx.net->host;
     const int n = s.n;
@@ -804,8 +804,14 @@ void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out) {
         ctx.graph = nullptr;
     }
     ctx.cfg = cfg;
-    cudaStream_t st = ctx.stream;
     uploadInputs(ctx, req);
+    ctx.staged = true;
+}
+
+void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out) {
+    stageRequest(ctx, req);
+    const int n = ctx.net->host.n;
+    cudaStream_t st = ctx.stream;
     if (ctx.autotunePending) autotune(ctx);
     cudaEvent_t e0, e1;
     OLF_CUDA(cudaEventCreate(&e0));
@@ -824,6 +830,180 @@ void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out) {
     OLF_CUDA(cudaEventElapsedTime(&ctx.lastMs, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    OLF_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Several grids in one persistent launch
+// ---------------------------------------------------------------------------------------------------------------
+MultiContext::~MultiContext() {
+    if (graph) cudaGraphExecDestroy(graph);
+    for (cudaEvent_t e : ready) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+    if (hostItems) cudaFreeHost(hostItems);
+}
+
+MultiContext* createMultiContext(const std::vector<BatchContext*>& members) {
+    if (members.empty()) throw std::runtime_error("a multi-grid context needs at least one batch context");
+    const int device = members[0]->device;
+    for (const BatchContext* c : members) {
+        if (!c) throw std::runtime_error("null batch context");
+        if (c->device != device) throw std::runtime_error("the batch contexts of a multi-grid launch share one device");
+    }
+    for (size_t i = 0; i < members.size(); i++)
+        for (size_t j = i + 1; j < members.size(); j++)
+            if (members[i] == members[j]) throw std::runtime_error("a batch context appears twice");
+    OLF_CUDA(cudaSetDevice(device));
+    auto m = std::make_unique<MultiContext>();
+    m->members = members;
+    m->device = device;
+    OLF_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+    m->ready.resize(members.size());
+    for (auto& e : m->ready) OLF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    m->itemsDev.alloc(members.size() * sizeof(MultiItem));
+    OLF_CUDA(cudaMallocHost(&m->hostItems, members.size() * sizeof(MultiItem)));
+    return m.release();
+}
+
+namespace {
+
+int tilesOf(const BatchContext& c, int lanes) { return (c.nS + lanes - 1) / lanes; }
+
+// Member order of the launch: as given, or the grids with the most buses first (their tiles run longest, so they
+// are dispatched first and the small grids' tiles fill the tail).
+std::vector<int> launchOrder(const MultiContext& m, int order) {
+    std::vector<int> idx(m.members.size());
+    for (size_t i = 0; i < idx.size(); i++) idx[i] = static_cast<int>(i);
+    if (order == 1) {
+        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+            return m.members[a]->net->host.n > m.members[b]->net->host.n;
+        });
+    }
+    return idx;
+}
+
+// Lanes of every member reset to their staged inputs, then the one launch (and the members' result gathers).
+void runMulti(MultiContext& m, bool fp32) {
+    cudaStream_t st = m.stream;
+    for (size_t i = 0; i < m.members.size(); i++) {
+        BatchContext& c = *m.members[i];
+        installLanes(c);
+        OLF_CUDA(cudaEventRecord(m.ready[i], c.stream));
+        OLF_CUDA(cudaStreamWaitEvent(st, m.ready[i], 0));
+    }
+    const std::vector<int> idx = launchOrder(m, m.order);
+    int tile = 0;
+    for (size_t k = 0; k < idx.size(); k++) {
+        BatchContext& c = *m.members[idx[k]];
+        MultiItem& it = m.hostItems[k];
+        it.net = c.net->dev->view;
+        it.b = c.batch();
+        it.rl = c.rl;
+        it.cfg = c.cfg;
+        it.plan = c.net->dev->persistent;
+        it.plan.maxRounds = roundCap(c);
+        it.tileBegin = tile;
+        tile += tilesOf(c, m.lanesPerTile);
+    }
+    OLF_CUDA(cudaMemcpyAsync(m.itemsDev.p, m.hostItems, m.members.size() * sizeof(MultiItem), cudaMemcpyHostToDevice,
+                             st));
+    const int key = (m.lanesPerTile * 1024 + m.threads) * 2 + (fp32 ? 1 : 0);
+    if (!m.graph || m.graphKey != key) {
+        if (m.graph) cudaGraphExecDestroy(m.graph);
+        m.graph = nullptr;
+        cudaGraph_t g;
+        OLF_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        launchMulti(m.itemsDev.as<MultiItem>(), static_cast<int>(m.members.size()), tile, m.lanesPerTile, m.threads,
+                    fp32, st);
+        for (BatchContext* c : m.members) {
+            const int n = c->net->host.n;
+            dim3 blk(32, 8), grd((n + 31) / 32, (c->nS + 31) / 32);
+            resultsKernel<<<grd, blk, 0, st>>>(c->x.as<double>(), c->iter.as<int>(), c->normOut.as<double>(),
+                                               c->status.as<int>(), c->out.as<double>(), n, c->nS, c->S);
+        }
+        OLF_CUDA(cudaStreamEndCapture(st, &g));
+        OLF_CUDA(cudaGraphInstantiate(&m.graph, g, 0));
+        cudaGraphDestroy(g);
+        m.graphKey = key;
+    }
+    OLF_CUDA(cudaGraphLaunch(m.graph, st));
+}
+
+void autotuneMulti(MultiContext& m, bool fp32) {
+    cudaEvent_t e0, e1;
+    OLF_CUDA(cudaEventCreate(&e0));
+    OLF_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    MultiTuning pick{};
+    m.tuning.clear();
+    for (int lanes : {1, 2, 4, 8})
+        for (int threads : {256, 512})
+            for (int order : {0, 1}) {
+                m.lanesPerTile = lanes;
+                m.threads = threads;
+                m.order = order;
+                OLF_CUDA(cudaEventRecord(e0, m.stream));
+                runMulti(m, fp32);
+                OLF_CUDA(cudaEventRecord(e1, m.stream));
+                OLF_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                OLF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                m.tuning.push_back({lanes, threads, order, ms});
+                if (ms < best) {
+                    best = ms;
+                    pick = m.tuning.back();
+                }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    m.lanesPerTile = pick.lanesPerTile;
+    m.threads = pick.threads;
+    m.order = pick.order;
+    m.autotunePending = false;
+}
+
+}  // namespace
+
+void solveMulti(MultiContext& m, double* const* outs) {
+    OLF_CUDA(cudaSetDevice(m.device));
+    const int precision = m.members[0]->precision;
+    for (BatchContext* c : m.members) {
+        if (!c->staged) throw std::runtime_error("every batch context of a multi-grid launch must be staged first");
+        if (c->precision != precision) {
+            throw std::runtime_error("the batch contexts of a multi-grid launch share one precision");
+        }
+    }
+    const bool fp32 = precision == 1;
+    for (BatchContext* c : m.members) {
+        const size_t lu = static_cast<size_t>(c->net->dev->view.nLu) * 4 * c->S;
+        if (fp32 && !c->lu32.p) c->lu32.alloc(lu * 4);
+        if (!fp32 && !c->lu64.p) c->lu64.alloc(lu * 8);
+    }
+    if (m.autotunePending) autotuneMulti(m, fp32);
+    cudaStream_t st = m.stream;
+    cudaEvent_t e0, e1;
+    OLF_CUDA(cudaEventCreate(&e0));
+    OLF_CUDA(cudaEventCreate(&e1));
+    // the members' installs run on their own streams after e0: time from before them
+    OLF_CUDA(cudaEventRecord(e0, st));
+    for (BatchContext* c : m.members) OLF_CUDA(cudaStreamWaitEvent(c->stream, e0, 0));
+    runMulti(m, fp32);
+    OLF_CUDA(cudaEventRecord(e1, st));
+    for (size_t i = 0; i < m.members.size(); i++) {
+        BatchContext& c = *m.members[i];
+        if (outs && outs[i]) {
+            OLF_CUDA(cudaMemcpyAsync(outs[i], c.out.p, static_cast<size_t>(c.nS) * (c.net->host.n + 3) * 8,
+                                     cudaMemcpyDeviceToHost, st));
+        }
+    }
+    OLF_CUDA(cudaStreamSynchronize(st));
+    OLF_CUDA(cudaEventElapsedTime(&m.lastMs, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (BatchContext* c : m.members) {
+        c->lastIterations = 0;
+        c->lastMs = m.lastMs;
+    }
     OLF_CUDA(cudaGetLastError());
 }
 

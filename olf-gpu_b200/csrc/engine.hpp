@@ -158,6 +158,7 @@ struct BatchContext {
     // statistics of the last solve
     int lastIterations = 0;         // batched iterations run
     float lastMs = 0.f;
+    bool staged = false;            // inputs of a request uploaded (a multi-grid launch runs staged contexts)
     ~BatchContext();
     DevBatch batch() const;
 };
@@ -168,6 +169,36 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
 
 // Runs the batch; out = [nS][n + 3] per scenario [x(n), iterations, ||F||inf, status].
 void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out);
+
+// Validates a request and uploads its inputs to the context (the first half of solveBatch).
+void stageRequest(BatchContext& ctx, const SolveRequest& req);
+
+struct MultiTuning {
+    int lanesPerTile, threads, order;
+    float ms;
+};
+
+// Batch contexts of different grids run by one persistent launch (one CTA per lane tile of any member, captured in
+// a CUDA graph with the members' result gathers).  The members stay owned by their creator.
+struct MultiContext {
+    std::vector<BatchContext*> members;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaEvent_t> ready;      // per member: its lanes are installed
+    int lanesPerTile = 2, threads = 256, order = 0;   // order 0: as given, 1: most buses first
+    bool autotunePending = false;
+    std::vector<MultiTuning> tuning;
+    DeviceBuffer itemsDev;
+    MultiItem* hostItems = nullptr;      // pinned
+    cudaGraphExec_t graph = nullptr;
+    int graphKey = -1;
+    float lastMs = 0.f;
+    ~MultiContext();
+};
+
+MultiContext* createMultiContext(const std::vector<BatchContext*>& members);
+// One launch over every member's staged batch; outs[i] (host, may be null) = member i's [nS][n + 3] results.
+void solveMulti(MultiContext& m, double* const* outs);
 
 // Debug/test surface: the Jacobian (CSR values of the reference-compatible pattern) and mismatch of every
 // scenario at the given states, through the engine's fill; and a batched linear solve through the engine's LU.

@@ -34,7 +34,9 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_structure_export", "olfgpu_recommend_batch_size", "olfgpu_create_batch_context",
            "olfgpu_destroy_batch_context", "olfgpu_set_linear_solver_settings", "olfgpu_solve_batch_context",
            "olfgpu_last_solve_stats", "olfgpu_debug_fill", "olfgpu_debug_linear_solve", "olfgpu_set_schedule",
-           "olfgpu_get_schedule", "olfgpu_linear_solve_noalloc"]
+           "olfgpu_get_schedule", "olfgpu_linear_solve_noalloc", "olfgpu_stage_batch_context",
+           "olfgpu_create_multi_context", "olfgpu_destroy_multi_context", "olfgpu_set_multi_schedule",
+           "olfgpu_get_multi_schedule", "olfgpu_solve_multi_context"]
 # Schedules of the Newton iterations
 LEVELS, PERSISTENT, AUTOTUNE = 0, 1, -1
 
@@ -68,6 +70,12 @@ def load(path: str = LIB_PATH):
     L.olfgpu_solve_batch_context.argtypes = [_i64, _dp, _dp, _dp, _ip, ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int,
                                              _u8p, ctypes.c_int, _ip, _dp, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp]
+    L.olfgpu_stage_batch_context.argtypes = L.olfgpu_solve_batch_context.argtypes[:-1]
+    L.olfgpu_create_multi_context.argtypes = [ctypes.c_int, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]
+    L.olfgpu_destroy_multi_context.argtypes = [_i64]
+    L.olfgpu_set_multi_schedule.argtypes = [_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.olfgpu_get_multi_schedule.argtypes = [_i64, _ip, _ip, _ip, ctypes.c_int, _dp, _ip]
+    L.olfgpu_solve_multi_context.argtypes = [_i64, ctypes.POINTER(_dp), _fp]
     L.olfgpu_last_solve_stats.argtypes = [_i64, _fp, _ip, _ip]
     L.olfgpu_debug_fill.argtypes = [_i64, _dp, _dp, _ip, _u8p, _dp, _dp]
     L.olfgpu_debug_linear_solve.argtypes = [_i64, _dp, _dp, ctypes.c_int, _dp]
@@ -214,7 +222,25 @@ class BatchContext:
               reactive_limit_tol: float = 1e-4, max_outer: int = 20, max_pq_pv_switch: int = 3,
               out: Optional[np.ndarray] = None) -> np.ndarray:
         """Per scenario [x(n), iterations, ||F||inf, status] (BatchSolveNative.solveBatchContext)."""
-        n = self.structure.n
+        args, keep = self._request(x0_base, target_base, base_row_mode, disabled, x0_full, row_mode_entries,
+                                   target_override_index, target_override_value, max_iter, tol, reactive_limit_tol,
+                                   max_outer, max_pq_pv_switch)
+        if out is None:
+            out = np.zeros((keep[0].shape[0], self.structure.n + 3))
+        _check(load().olfgpu_solve_batch_context(self.handle, *args, _p(out)))
+        return out
+
+    def stage(self, x0_base, target_base, base_row_mode, disabled, x0_full=None, row_mode_entries=None,
+              target_override_index=None, target_override_value=None, max_iter: int = 15, tol: float = 1e-8,
+              reactive_limit_tol: float = 1e-4, max_outer: int = 20, max_pq_pv_switch: int = 3) -> None:
+        """Validates and uploads a request without running it (run by MultiContext.solve)."""
+        args, keep = self._request(x0_base, target_base, base_row_mode, disabled, x0_full, row_mode_entries,
+                                   target_override_index, target_override_value, max_iter, tol, reactive_limit_tol,
+                                   max_outer, max_pq_pv_switch)
+        _check(load().olfgpu_stage_batch_context(self.handle, *args))
+
+    def _request(self, x0_base, target_base, base_row_mode, disabled, x0_full, row_mode_entries, target_override_index,
+                 target_override_value, max_iter, tol, reactive_limit_tol, max_outer, max_pq_pv_switch):
         disabled = _c(disabled, np.uint8)
         ns = disabled.shape[0]
         x0b = None if x0_base is None else _c(x0_base, np.float64)
@@ -224,13 +250,10 @@ class BatchContext:
         rme = _c(np.zeros(0) if row_mode_entries is None else row_mode_entries, np.int32).reshape(-1)
         toi = _c(np.zeros(0) if target_override_index is None else target_override_index, np.int32)
         tov = _c(np.zeros(0) if target_override_value is None else target_override_value, np.float64)
-        if out is None:
-            out = np.zeros((ns, n + 3))
-        _check(load().olfgpu_solve_batch_context(
-            self.handle, _p(x0b), _p(x0f), _p(tb), _p(bm), rme.shape[0] // 3, _p(rme) if rme.size else None, ns,
-            disabled.shape[1], _p(disabled), toi.shape[0], _p(toi) if toi.size else None,
-            _p(tov) if tov.size else None, max_iter, tol, reactive_limit_tol, max_outer, max_pq_pv_switch, _p(out)))
-        return out
+        args = (_p(x0b), _p(x0f), _p(tb), _p(bm), rme.shape[0] // 3, _p(rme) if rme.size else None, ns,
+                disabled.shape[1], _p(disabled), toi.shape[0], _p(toi) if toi.size else None,
+                _p(tov) if tov.size else None, max_iter, tol, reactive_limit_tol, max_outer, max_pq_pv_switch)
+        return args, (disabled, x0b, x0f, tb, bm, rme, toi, tov)
 
     def last_stats(self):
         ms = ctypes.c_float(0)
@@ -255,3 +278,46 @@ class BatchContext:
         v, r = _c(csr_vals, np.float64), _c(rhs, np.float64)
         _check(load().olfgpu_debug_linear_solve(self.handle, _p(v), _p(r), precision, _p(out)))
         return out
+
+
+class MultiContext:
+    """Batch contexts of different grids run by one persistent launch (olfgpu_solve_multi_context)."""
+
+    def __init__(self, contexts):
+        self.contexts = list(contexts)
+        h = _i64(0)
+        arr = (_i64 * len(self.contexts))(*[c.handle for c in self.contexts])
+        _check(load().olfgpu_create_multi_context(len(self.contexts), arr, ctypes.byref(h)))
+        self.handle = h.value
+
+    def close(self):
+        if getattr(self, "handle", 0):
+            load().olfgpu_destroy_multi_context(self.handle)
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_schedule(self, lanes_per_tile: int, threads: int = 256, order: int = 0):
+        """lanes_per_tile -1: the next solve autotunes (tile lanes x threads x member order)."""
+        _check(load().olfgpu_set_multi_schedule(self.handle, lanes_per_tile, threads, order))
+
+    def schedule(self):
+        """(lanes per tile, threads, order) in force and the autotuner's timings [(lanes, threads, order, ms)]."""
+        la, th, od, nr = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        res = np.zeros(4 * 64)
+        _check(load().olfgpu_get_multi_schedule(self.handle, ctypes.byref(la), ctypes.byref(th), ctypes.byref(od), 64,
+                                                _p(res), ctypes.byref(nr)))
+        return (la.value, th.value, od.value), [tuple(res[4 * i:4 * i + 4]) for i in range(min(nr.value, 64))]
+
+    def solve(self, outs=None):
+        """Runs every member's staged batch; returns (per member [nS][n + 3] results, device ms)."""
+        if outs is None:
+            outs = [np.zeros((c.n_scenarios, c.structure.n + 3)) for c in self.contexts]
+        ptrs = (_dp * len(outs))(*[o.ctypes.data_as(_dp) for o in outs])
+        ms = ctypes.c_float(0)
+        _check(load().olfgpu_solve_multi_context(self.handle, ptrs, ctypes.byref(ms)))
+        return outs, float(ms.value)

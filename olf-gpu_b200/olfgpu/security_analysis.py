@@ -99,3 +99,53 @@ class SecurityAnalysis:
             ms += m
         return BatchResult(outages, out[:, n + 2].astype(int), out[:, n].astype(int), out[:, n + 1], out[:, :n],
                            tot, ms)
+
+
+class MultiGridAnalysis:
+    """N-1 batches of several grids solved by one persistent launch (the engine's multi-grid context).
+
+    Each grid keeps its own structure and a context sized to its batch; ``solve`` stages every grid's outages and runs
+    them together, returning one BatchResult per grid.  ``schedule`` is -1 (autotune on the first solve) or a fixed
+    (lanes per tile, threads, order)."""
+
+    def __init__(self, packed_grids: Sequence[Packed], counts: Sequence[int], precision: int = native.FP64,
+                 refinement_steps: int = 1, reactive_limits: bool = True, schedule=-1):
+        self.packed = list(packed_grids)
+        self.counts = [int(c) for c in counts]
+        self.structures = [native.Structure(p) for p in self.packed]
+        self.contexts = []
+        for p, s, c in zip(self.packed, self.structures, self.counts):
+            ctx = native.BatchContext(s, c, native.BATCHED_LU, p.rl if reactive_limits and p.rl is not None else None)
+            ctx.set_linear_solver_settings(precision, refinement_steps)
+            self.contexts.append(ctx)
+        self.multi = native.MultiContext(self.contexts)
+        if schedule == -1:
+            self.multi.set_schedule(-1)
+        else:
+            self.multi.set_schedule(*schedule)
+
+    def close(self):
+        self.multi.close()
+        for c in self.contexts:
+            c.close()
+        for s in self.structures:
+            s.close()
+
+    def solve(self, outages: Sequence[Sequence[int]], max_iter: int = 15, tol: float = 1e-8,
+              reactive_limit_tol: float = 1e-4, max_outer: int = 20, max_pq_pv_switch: int = 3):
+        """outages[i]: grid i's outaged closed branches (exactly counts[i]); returns ([BatchResult], device ms)."""
+        for p, ctx, c, outs in zip(self.packed, self.contexts, self.counts, outages):
+            outs = np.asarray(outs, dtype=np.int64)
+            if outs.shape[0] != c:
+                raise ValueError(f"expected {c} outages, got {outs.shape[0]}")
+            x0 = p.x_base if p.x_base is not None else p.x_flat
+            ctx.stage(x0, p.target, p.base_row_mode, p.outage_masks(outs), max_iter=max_iter, tol=tol,
+                      reactive_limit_tol=reactive_limit_tol, max_outer=max_outer, max_pq_pv_switch=max_pq_pv_switch)
+        res, ms = self.multi.solve()
+        results = []
+        for p, ctx, outs, out in zip(self.packed, self.contexts, outages, res):
+            n = p.n
+            _, _, tot = ctx.last_stats()
+            results.append(BatchResult(np.asarray(outs), out[:, n + 2].astype(int), out[:, n].astype(int),
+                                       out[:, n + 1], out[:, :n], tot, ms))
+        return results, ms

@@ -519,10 +519,13 @@ def outage_candidates(g: Grid) -> np.ndarray:
     return np.flatnonzero(~br & ~par)
 
 
-def draw_outages(g: Grid, count: Optional[int], seed: int) -> np.ndarray:
-    """``count`` random candidates (all of them, in branch order, when ``count`` is None)."""
+def draw_outages(g: Grid, count: Optional[int], seed: int, replace: bool = False) -> np.ndarray:
+    """``count`` random candidates (all of them, in branch order, when ``count`` is None).  With ``replace`` the draw
+    is with replacement, so a grid with fewer candidates than ``count`` still yields exactly ``count`` outages."""
     cand = outage_candidates(g)
+    rng = np.random.default_rng(seed)
+    if replace and count is not None:
+        return np.sort(rng.choice(cand, size=count, replace=True))
     if count is None or count >= cand.shape[0]:
         return cand
-    rng = np.random.default_rng(seed)
     return np.sort(rng.choice(cand, size=count, replace=False))
