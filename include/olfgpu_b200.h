@@ -58,6 +58,15 @@ int olfgpu_structure_info(int64_t structure, int* info9, int64_t* blockOps);
 int olfgpu_structure_export(int64_t structure, int* rowMap, int* rowPtr, int* colIdx, int* diagPos, int* cbDest,
                             int* obDest, int* shDest);
 
+/*
+ * The block-LU schedule of the structure (no counterpart in the reference): level boundaries of the factorization
+ * (factorLevelPtr [factorLevels + 1], over LU blocks), of the forward and backward solves ([levels + 1], over
+ * elimination positions), and the block updates of each factorization level (levelOps [factorLevels]).  Sizes from
+ * olfgpu_structure_info; any pointer may be null.
+ */
+int olfgpu_structure_levels(int64_t structure, int* factorLevelPtr, int* forwardLevelPtr, int* backwardLevelPtr,
+                            int64_t* levelOps);
+
 /* StructureNative.recommendBatchSize (structure_jni.cu:151-180): the bank that fits 70 % of free device memory. */
 int olfgpu_recommend_batch_size(int64_t structure, int maxCap, int mode, int* batchOut);
 
@@ -122,6 +131,26 @@ int olfgpu_solve_batch_context(int64_t context, const double* x0Base, const doub
  * (totalIterations [nScenarios], may be null).
  */
 int olfgpu_last_solve_stats(int64_t context, float* deviceMs, int* batchedIterations, int* totalIterations);
+
+/*
+ * Phase timing (diagnostics; no counterpart in the reference): with enable = 1 the level schedule launches every
+ * Newton iteration phase by phase between CUDA events on the context's stream instead of replaying its graphs (same
+ * kernels, same order).  olfgpu_last_phase_times writes, for the last solve, the milliseconds of {fill, test,
+ * factorization, solves, refinement, step} summed over its iterations, then the iterations run and the lanes that
+ * factorized summed over them (out8 [8]).
+ */
+int olfgpu_set_phase_timing(int64_t context, int enable);
+int olfgpu_last_phase_times(int64_t context, double* out8);
+
+/*
+ * Fallback start (no counterpart in the reference): with enable = 1, a solve given both x0Full (e.g. learned starts)
+ * and x0Base restarts every scenario whose solve from x0Full ends DIVERGED, MAX_ITERATION_REACHED or
+ * LINEAR_SOLVE_FAILED once from x0Base, inside the same batch (its result, iterations and status are those of the
+ * restarted solve; total iterations count both).  Not available with reactive limits.  olfgpu_last_fallbacks writes
+ * per scenario 1 where the last solve restarted it (fellBack [nScenarios], may be null) and their count.
+ */
+int olfgpu_set_fallback_start(int64_t context, int enable);
+int olfgpu_last_fallbacks(int64_t context, unsigned char* fellBack, int* count);
 
 /*
  * Uneven batching across grids (no counterpart in the reference, whose GpuBatchedAcSecurityAnalysis runs one network

@@ -142,6 +142,30 @@ extern "C" int olfgpu_structure_export(int64_t structure, int* rowMap, int* rowP
     });
 }
 
+extern "C" int olfgpu_structure_levels(int64_t structure, int* factorLevelPtr, int* forwardLevelPtr,
+                                       int* backwardLevelPtr, int64_t* levelOps) {
+    return guarded([&] {
+        const BlockPlan& p = structureOf(structure)->host.plan;
+        auto put = [](int* dst, const std::vector<int>& v) {
+            if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(int));
+        };
+        put(factorLevelPtr, p.levelPtr);
+        put(forwardLevelPtr, p.fwdLevelPtr);
+        put(backwardLevelPtr, p.bwdLevelPtr);
+        if (levelOps) {
+            const int nl = static_cast<int>(p.levelPtr.size()) - 1;
+            for (int l = 0; l < nl; l++) {
+                int64_t ops = 0;
+                for (int k = p.levelPtr[l]; k < p.levelPtr[l + 1]; k++) {
+                    const int t = p.levelTask[k];
+                    ops += p.opPtr[t + 1] - p.opPtr[t];
+                }
+                levelOps[l] = ops;
+            }
+        }
+    });
+}
+
 extern "C" int olfgpu_recommend_batch_size(int64_t structure, int maxCap, int mode, int* batchOut) {
     return guarded([&] {
         if (!batchOut) throw std::runtime_error("null output");
@@ -247,6 +271,41 @@ extern "C" int olfgpu_solve_batch_context(int64_t context, const double* x0Base,
                                          nScenarios, nElements, disabled, nTargetOverrides, targetOverrideIndex,
                                          targetOverrideValue, maxIter, tol, reactiveLimitTol, maxOuter, maxPqPvSwitch);
         solveBatch(c, r, out);
+    });
+}
+
+extern "C" int olfgpu_set_phase_timing(int64_t context, int enable) {
+    return guarded([&] { contextOf(context).phaseTiming = enable != 0; });
+}
+
+extern "C" int olfgpu_last_phase_times(int64_t context, double* out8) {
+    return guarded([&] {
+        const BatchContext& c = contextOf(context);
+        if (!out8) throw std::runtime_error("null output");
+        for (int i = 0; i < 6; i++) out8[i] = c.phaseMs[i];
+        out8[6] = static_cast<double>(c.phaseIterations);
+        out8[7] = static_cast<double>(c.phaseLanes);
+    });
+}
+
+extern "C" int olfgpu_set_fallback_start(int64_t context, int enable) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        if (enable && c.rl.nRl > 0) throw std::runtime_error("the fallback start is not available with reactive limits");
+        c.fallbackStart = enable != 0;
+    });
+}
+
+extern "C" int olfgpu_last_fallbacks(int64_t context, unsigned char* fellBack, int* count) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        std::vector<unsigned char> f(c.nS);
+        OLF_CUDA(cudaSetDevice(c.device));
+        OLF_CUDA(cudaMemcpy(f.data(), c.fellBack.p, c.nS, cudaMemcpyDeviceToHost));
+        int k = 0;
+        for (int i = 0; i < c.nS; i++) k += f[i] ? 1 : 0;
+        if (fellBack) std::memcpy(fellBack, f.data(), c.nS);
+        if (count) *count = k;
     });
 }
 

@@ -279,6 +279,11 @@ DevBatch BatchContext::batch() const {
     b.pending = pending.as<int8_t>();
     b.precision64 = precision64.as<int8_t>();
     b.nActive = nActive.as<int>();
+    b.fallbackX = stage.as<double>();        // the staged base start x0Base
+    b.nFallback = net->host.n;
+    b.fallbackOn = fallbackStart && hasX0Base && hasX0Full ? 1 : 0;
+    b.fallbackLeft = fallbackLeft.as<int8_t>();
+    b.fellBack = fellBack.as<int8_t>();
     return b;
 }
 
@@ -321,6 +326,8 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
     ctx->active.alloc(S);
     ctx->pending.alloc(S);
     ctx->precision64.alloc(S);
+    ctx->fallbackLeft.alloc(S);
+    ctx->fellBack.alloc(S);
     ctx->nActive.alloc(8);
     ctx->out.alloc(static_cast<size_t>(nScenarios) * (n + 3) * 8);
     ctx->stage.alloc(n * 8 * 2 + n * 4);
@@ -459,6 +466,8 @@ __global__ void laneInitKernel(DevBatch b) {
     b.norm[s] = 0ull;
     b.normOut[s] = 0.0;
     b.precision64[s] = 0;
+    b.fallbackLeft[s] = live && b.fallbackOn ? 1 : 0;
+    b.fellBack[s] = 0;
     if (s == 0) *b.nActive = b.nS;
 }
 
@@ -549,9 +558,10 @@ void captureIteration(BatchContext& ctx) {
     ctx.graphKey = key;
 }
 
-// One Newton iteration launched phase by phase with CUDA events between the phases; prints the milliseconds of
-// each phase to stderr (diagnostics only: same kernels, same order as the captured graph).
-void phaseTimedIteration(BatchContext& ctx, int k) {
+// One Newton iteration launched phase by phase with CUDA events between the phases (the same kernels in the same
+// order as the two captured graphs); the phase times and the lanes that factorized accumulate in the context.
+// Returns false when no lane is left iterating.
+bool phaseTimedIteration(BatchContext& ctx) {
     const DeviceNet& dn = *ctx.net->dev;
     const DevNet& net = dn.view;
     const bool mixed = ctx.precision == 1;
@@ -566,29 +576,41 @@ void phaseTimedIteration(BatchContext& ctx, int k) {
     OLF_CUDA(cudaEventRecord(ev[1], st));
     launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, st);
     if (rl) launchReactiveLimits(net, b, ctx.rl, ctx.cfg, st);
+    launchCountSolving(b, st);
     OLF_CUDA(cudaEventRecord(ev[2], st));
-    const Hybrid hy = ctx.hybrid();
-    const Hybrid* hp = ctx.narrowLanes > 0 ? &hy : nullptr;
-    launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, mixed, hp,
-                 st);
-    OLF_CUDA(cudaEventRecord(ev[3], st));
-    launchSolve(net, b, dn.fwd(), dn.bwd(), mixed, false, hp, st);
-    OLF_CUDA(cudaEventRecord(ev[4], st));
-    if (mixed) {
-        for (int r = 0; r < ctx.refinementSteps; r++) {
-            launchResidual(net, b, st);
-            launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, st);
+    OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 8, cudaMemcpyDeviceToHost, st));
+    OLF_CUDA(cudaStreamSynchronize(st));
+    float ms[6] = {0, 0, 0, 0, 0, 0};
+    OLF_CUDA(cudaEventElapsedTime(&ms[0], ev[0], ev[1]));
+    OLF_CUDA(cudaEventElapsedTime(&ms[1], ev[1], ev[2]));
+    const bool live = ctx.hostActive[0] > 0;
+    const int solving = ctx.hostActive[1];
+    if (live && solving > 0) {
+        const Hybrid hy = ctx.hybrid();
+        const Hybrid* hp = ctx.narrowLanes > 0 ? &hy : nullptr;
+        OLF_CUDA(cudaEventRecord(ev[2], st));
+        launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, mixed,
+                     hp, st);
+        OLF_CUDA(cudaEventRecord(ev[3], st));
+        launchSolve(net, b, dn.fwd(), dn.bwd(), mixed, false, hp, st);
+        OLF_CUDA(cudaEventRecord(ev[4], st));
+        if (mixed) {
+            for (int r = 0; r < ctx.refinementSteps; r++) {
+                launchResidual(net, b, st);
+                launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, st);
+            }
         }
+        OLF_CUDA(cudaEventRecord(ev[5], st));
+        launchStep(net, b, false, st);
+        OLF_CUDA(cudaEventRecord(ev[6], st));
+        OLF_CUDA(cudaEventSynchronize(ev[6]));
+        for (int i = 2; i < 6; i++) OLF_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+        ctx.phaseLanes += solving;
     }
-    OLF_CUDA(cudaEventRecord(ev[5], st));
-    launchStep(net, b, false, st);
-    OLF_CUDA(cudaEventRecord(ev[6], st));
-    OLF_CUDA(cudaEventSynchronize(ev[6]));
-    float ms[6];
-    for (int i = 0; i < 6; i++) OLF_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
-    std::fprintf(stderr, "OLFGPU_PHASE_TIME it=%d fill=%.3f test=%.3f factor=%.3f solve=%.3f refine=%.3f step=%.3f ms\n",
-                 k, ms[0], ms[1], ms[2], ms[3], ms[4], ms[5]);
+    for (int i = 0; i < 6; i++) ctx.phaseMs[i] += ms[i];
+    if (live) ctx.phaseIterations++;
     for (auto& e : ev) cudaEventDestroy(e);
+    return live;
 }
 
 }  // namespace
@@ -663,7 +685,8 @@ void installLanes(BatchContext& ctx) {
 }
 
 int roundCap(const BatchContext& ctx) {
-    return ctx.cfg.reactiveLimits ? (ctx.cfg.maxOuter + 1) * (ctx.cfg.maxIter + 1) : ctx.cfg.maxIter + 1;
+    const int solves = ctx.fallbackStart && ctx.hasX0Base && ctx.hasX0Full ? 2 : 1;   // a fallback restart: 2 solves
+    return ctx.cfg.reactiveLimits ? (ctx.cfg.maxOuter + 1) * (ctx.cfg.maxIter + 1) : solves * (ctx.cfg.maxIter + 1);
 }
 
 // The Newton iterations under the context's schedule; returns the batched iterations run (level launches) or 0.
@@ -683,14 +706,15 @@ int runIterations(BatchContext& ctx) {
         return 0;
     }
     captureIteration(ctx);
-    static const bool phaseTime = std::getenv("OLFGPU_PHASE_TIME") != nullptr;
+    if (ctx.phaseTiming) {
+        for (double& v : ctx.phaseMs) v = 0.0;
+        ctx.phaseLanes = 0;
+        ctx.phaseIterations = 0;
+    }
     int k = 0;
     for (; k < cap; k++) {
-        if (phaseTime) {
-            phaseTimedIteration(ctx, k);
-            OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 8, cudaMemcpyDeviceToHost, st));
-            OLF_CUDA(cudaStreamSynchronize(st));
-            if (ctx.hostActive[0] <= 0) {
+        if (ctx.phaseTiming) {
+            if (!phaseTimedIteration(ctx)) {
                 k++;
                 break;
             }
@@ -788,6 +812,9 @@ void stageRequest(BatchContext& ctx, const SolveRequest& req) {
         if (req.targetOverrideIndex[k] < 0 || req.targetOverrideIndex[k] >= ctx.nS * n) {
             throw std::runtime_error("target override index out of range");
         }
+    }
+    if (ctx.fallbackStart && ctx.rl.nRl > 0) {
+        throw std::runtime_error("the fallback start is not available with reactive limits");
     }
     Settings cfg = ctx.cfg;
     cfg.maxIter = req.maxIter;

@@ -124,7 +124,8 @@ struct BatchContext {
     int refinementSteps = 1;
     // lane-interleaved state
     DeviceBuffer x, target, mode, F, J, lu64, lu32, w64, w32, dx, res, qbuf, disabled, norm, iter, status, outer,
-        totalIter, trouble, normOut, active, pending, precision64, nActive;
+        totalIter, trouble, normOut, active, pending, precision64, nActive, fallbackLeft, fellBack;
+    bool fallbackStart = false;     // lanes that fail from x0Full restart once from x0Base (both given)
     DeviceBuffer stage;             // upload staging (base vectors)
     DeviceBuffer ovIdx, ovVal, rowModeE;  // per-scenario overrides of the installed batch
     int nTargetOverrides = 0, nRowModeEntries = 0;
@@ -159,6 +160,11 @@ struct BatchContext {
     int lastIterations = 0;         // batched iterations run
     float lastMs = 0.f;
     bool staged = false;            // inputs of a request uploaded (a multi-grid launch runs staged contexts)
+    // phase timing (level schedule): each iteration launched phase by phase between CUDA events
+    bool phaseTiming = false;
+    double phaseMs[6] = {0, 0, 0, 0, 0, 0};   // fill, test, factorization, solves, refinement, step (summed)
+    long long phaseLanes = 0;       // lanes that factorized, summed over the iterations
+    int phaseIterations = 0;
     ~BatchContext();
     DevBatch batch() const;
 };

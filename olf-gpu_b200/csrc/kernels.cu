@@ -199,6 +199,24 @@ void launchFill(const DevNet& net, const DevBatch& b, bool withJacobian, bool wi
 // is MAX_ITERATION_REACHED; a non-finite mismatch is DIVERGED.  A converged lane with reactive limits to check is
 // marked pending instead (its outer loop decides).
 // ---------------------------------------------------------------------------------------------------------------
+// A lane whose solve failed: restarts from the fallback start when it still may (pending for this iteration, so it
+// neither factorizes nor counts an iteration; the next iteration fills at the fallback state), else retires.
+__device__ void failLane(const DevBatch& b, int s, int status) {
+    if (b.fallbackLeft[s]) {
+        b.fallbackLeft[s] = 0;
+        b.fellBack[s] = 1;
+        b.iter[s] = 0;
+        b.trouble[s] = 0;
+        b.pending[s] = 1;
+        const size_t S = b.S;
+        for (int r = 0; r < b.nFallback; r++) b.x[(size_t)r * S + s] = b.fallbackX[r];
+        return;
+    }
+    b.status[s] = status;
+    b.active[s] = 0;
+    atomicSub(b.nActive, 1);
+}
+
 __global__ void testKernel(DevBatch b, Settings cfg, int* remainingPv) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= b.S || !b.active[s]) return;
@@ -207,16 +225,12 @@ __global__ void testKernel(DevBatch b, Settings cfg, int* remainingPv) {
     const int it = b.iter[s];
     b.normOut[s] = nrm;
     if (!isfinite(nrm)) {
-        b.status[s] = ST_DIVERGED;
-        b.active[s] = 0;
-        atomicSub(b.nActive, 1);
+        failLane(b, s, ST_DIVERGED);
         return;
     }
     if (it > 0 && b.trouble[s]) {
         // the previous factorization met a near-singular 2x2 pivot: its step is not trusted
-        b.status[s] = ST_LINEAR_SOLVE_FAILED;
-        b.active[s] = 0;
-        atomicSub(b.nActive, 1);
+        failLane(b, s, ST_LINEAR_SOLVE_FAILED);
         return;
     }
     if (it > 0 && nrm < cfg.tol && it < cfg.maxIter) {
@@ -230,11 +244,7 @@ __global__ void testKernel(DevBatch b, Settings cfg, int* remainingPv) {
         }
         return;
     }
-    if (it == cfg.maxIter) {
-        b.status[s] = ST_MAX_ITERATION_REACHED;
-        b.active[s] = 0;
-        atomicSub(b.nActive, 1);
-    }
+    if (it == cfg.maxIter) failLane(b, s, ST_MAX_ITERATION_REACHED);
 }
 
 void launchTest(const DevNet&, const DevBatch& b, const Settings& cfg, int* remainingPv, cudaStream_t st) {

@@ -98,6 +98,13 @@ struct DevBatch {
     int8_t* pending;          // [S] 1: converged this iteration, reactive limits to check
     int8_t* precision64;      // [S] 1: this lane's last factorization fell back to FP64 (mixed precision)
     int* nActive;             // [2] lanes still iterating, lanes factorizing this iteration (read by the host)
+    // fallback start: a lane whose solve ends unconverged (diverged, iteration cap, failed linear solve) while its
+    // fallbackLeft flag is set restarts once from fallbackX (the base start, [n]) and marks fellBack
+    const double* fallbackX;
+    int nFallback;            // length of fallbackX (n)
+    int fallbackOn;           // set fallbackLeft for every live lane at install
+    int8_t* fallbackLeft;     // [S]
+    int8_t* fellBack;         // [S]
 };
 
 // Reactive-limit entries (ReactiveLimitsPacker.java:76) and their per-lane state.

@@ -50,6 +50,7 @@ struct TileState {
     int trouble[L];
     int remainingPv[L];
     int any[L];
+    int restart[L];      // failed this iteration and restarts from the fallback start
     unsigned long long norm[L];
     int live;            // any lane of the tile still active
 };
@@ -382,6 +383,7 @@ __device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl
             for (int k = 0; k < slots; k++) nrm = absMaxP(nrm, fred[k][tid]);
             ts.solving[tid] = 0;
             ts.pending[tid] = 0;
+            ts.restart[tid] = 0;
             const int troubled = ts.trouble[tid];
             ts.trouble[tid] = 0;
             if (ts.active[tid]) {
@@ -401,7 +403,12 @@ __device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl
                 } else if (it == cfg.maxIter) {
                     st = ST_MAX_ITERATION_REACHED;
                 }
-                if (st != ST_RUNNING) {
+                if (st != ST_RUNNING && st != ST_CONVERGED && b.fallbackLeft[s0 + tid]) {
+                    b.fallbackLeft[s0 + tid] = 0;      // restart once from the fallback start (next round)
+                    b.fellBack[s0 + tid] = 1;
+                    ts.iter[tid] = 0;
+                    ts.restart[tid] = 1;
+                } else if (st != ST_RUNNING) {
                     ts.status[tid] = st;
                     ts.active[tid] = 0;
                 } else if (!ts.pending[tid]) {
@@ -410,6 +417,9 @@ __device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl
             }
         }
         __syncthreads();
+        if (ts.restart[lane]) {
+            for (int r = slot; r < b.nFallback; r += slots) b.x[(size_t)r * S + s] = b.fallbackX[r];
+        }
         // ---------------- reactive limits (reactive_limits.cu:321-359, 417-448) ----------------
         if (rlOn) {
             bool anyPending = false;

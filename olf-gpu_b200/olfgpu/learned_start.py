@@ -242,16 +242,13 @@ def fingerprint(grid) -> np.ndarray:
 
 
 def solve_with_fallback(ctx, p, x0_learned: np.ndarray, x_base: np.ndarray, disabled: np.ndarray, **kw):
-    """Solve from the learned starts; scenarios that did not converge are solved again from the base start."""
-    r = ctx.solve(None, p.target, p.base_row_mode, disabled, x0_full=x0_learned, **kw).copy()
+    """Solve from the learned starts; a scenario that diverges, reaches the iteration cap or fails its linear solve
+    restarts once from the base start inside the same batch (the engine's fallback start).  Returns (results, total
+    Newton iterations per scenario, indices of the scenarios that fell back)."""
+    ctx.set_fallback_start(True)
+    try:
+        r = ctx.solve(x_base, p.target, p.base_row_mode, disabled, x0_full=x0_learned, **kw).copy()
+    finally:
+        ctx.set_fallback_start(False)
     _, _, tot = ctx.last_stats()
-    tot = tot.copy()
-    bad = np.flatnonzero(r[:, -1] != native.CONVERGED)
-    if bad.size:
-        x0 = x0_learned.copy()
-        x0[bad] = x_base
-        r2 = ctx.solve(None, p.target, p.base_row_mode, disabled, x0_full=x0, **kw)
-        _, _, tot2 = ctx.last_stats()
-        r[bad] = r2[bad]
-        tot[bad] += tot2[bad]
-    return r, tot, bad
+    return r, tot.copy(), ctx.last_fallbacks()

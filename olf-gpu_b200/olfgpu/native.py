@@ -36,7 +36,8 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_last_solve_stats", "olfgpu_debug_fill", "olfgpu_debug_linear_solve", "olfgpu_set_schedule",
            "olfgpu_get_schedule", "olfgpu_linear_solve_noalloc", "olfgpu_stage_batch_context",
            "olfgpu_create_multi_context", "olfgpu_destroy_multi_context", "olfgpu_set_multi_schedule",
-           "olfgpu_get_multi_schedule", "olfgpu_solve_multi_context"]
+           "olfgpu_get_multi_schedule", "olfgpu_solve_multi_context", "olfgpu_set_fallback_start",
+           "olfgpu_last_fallbacks", "olfgpu_set_phase_timing", "olfgpu_last_phase_times", "olfgpu_structure_levels"]
 # Schedules of the Newton iterations
 LEVELS, PERSISTENT, AUTOTUNE = 0, 1, -1
 
@@ -76,6 +77,11 @@ def load(path: str = LIB_PATH):
     L.olfgpu_set_multi_schedule.argtypes = [_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.olfgpu_get_multi_schedule.argtypes = [_i64, _ip, _ip, _ip, ctypes.c_int, _dp, _ip]
     L.olfgpu_solve_multi_context.argtypes = [_i64, ctypes.POINTER(_dp), _fp]
+    L.olfgpu_structure_levels.argtypes = [_i64, _ip, _ip, _ip, ctypes.POINTER(_i64)]
+    L.olfgpu_set_phase_timing.argtypes = [_i64, ctypes.c_int]
+    L.olfgpu_last_phase_times.argtypes = [_i64, _dp]
+    L.olfgpu_set_fallback_start.argtypes = [_i64, ctypes.c_int]
+    L.olfgpu_last_fallbacks.argtypes = [_i64, _u8p, _ip]
     L.olfgpu_last_solve_stats.argtypes = [_i64, _fp, _ip, _ip]
     L.olfgpu_debug_fill.argtypes = [_i64, _dp, _dp, _ip, _u8p, _dp, _dp]
     L.olfgpu_debug_linear_solve.argtypes = [_i64, _dp, _dp, ctypes.c_int, _dp]
@@ -153,6 +159,17 @@ class Structure:
         _check(load().olfgpu_structure_export(self.handle, *[_p(out[k]) for k in (
             "row_map", "row_ptr", "col_idx", "diag_pos", "cb_dest", "ob_dest", "sh_dest")]))
         return out
+
+    def levels(self):
+        """Block-LU schedule: (factor level pointers, block updates per factor level, forward / backward level
+        pointers)."""
+        f = np.zeros(self.factor_levels + 1, np.int32)
+        fw = np.zeros(self.forward_levels + 1, np.int32)
+        bw = np.zeros(self.backward_levels + 1, np.int32)
+        ops = np.zeros(self.factor_levels, np.int64)
+        _check(load().olfgpu_structure_levels(self.handle, _p(f), _p(fw), _p(bw),
+                                              ops.ctypes.data_as(ctypes.POINTER(_i64))))
+        return f, ops, fw, bw
 
     def recommend_batch_size(self, max_cap: int, mode: int = BATCHED_LU) -> int:
         b = ctypes.c_int(0)
@@ -254,6 +271,31 @@ class BatchContext:
                 disabled.shape[1], _p(disabled), toi.shape[0], _p(toi) if toi.size else None,
                 _p(tov) if tov.size else None, max_iter, tol, reactive_limit_tol, max_outer, max_pq_pv_switch)
         return args, (disabled, x0b, x0f, tb, bm, rme, toi, tov)
+
+    def set_phase_timing(self, enable: bool = True):
+        """Level schedule: launch each iteration phase by phase between CUDA events (diagnostics)."""
+        _check(load().olfgpu_set_phase_timing(self.handle, 1 if enable else 0))
+
+    def last_phase_times(self) -> dict:
+        """Milliseconds per phase of the last solve (summed over its iterations), iterations and factorized lanes."""
+        o = np.zeros(8)
+        _check(load().olfgpu_last_phase_times(self.handle, _p(o)))
+        keys = ["fill", "test", "factor", "solve", "refine", "step"]
+        d = {k: float(v) for k, v in zip(keys, o[:6])}
+        d["iterations"] = int(o[6])
+        d["factorized_lanes"] = int(o[7])
+        return d
+
+    def set_fallback_start(self, enable: bool = True):
+        """Scenarios that fail from x0_full restart once from x0_base inside the same solve."""
+        _check(load().olfgpu_set_fallback_start(self.handle, 1 if enable else 0))
+
+    def last_fallbacks(self) -> np.ndarray:
+        """Indices of the scenarios the last solve restarted from the base start."""
+        f = np.zeros(self.n_scenarios, np.uint8)
+        k = ctypes.c_int(0)
+        _check(load().olfgpu_last_fallbacks(self.handle, _p(f), ctypes.byref(k)))
+        return np.flatnonzero(f)
 
     def last_stats(self):
         ms = ctypes.c_float(0)

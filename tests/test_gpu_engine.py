@@ -262,3 +262,44 @@ def test_persistent_reactive_limits_match_oracle(engine_lib, oracle_mod):
         r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
         ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis, reactive_limits=True)
         _compare(r, ref, p.n)
+
+
+@pytest.mark.parametrize("schedule,lanes,threads", [(0, 2, 256), (1, 2, 256)])
+def test_fallback_start_restarts_failed_lanes(engine_lib, oracle_mod, schedule, lanes, threads):
+    """Lanes whose start state fails (NaN: DIVERGED at once) restart from the base start inside the same solve and
+    end with the oracle's base-start result; the other lanes keep their own start and are not restarted."""
+    from olfgpu import native, synthetic
+    g, p = grid("grid2000")
+    outs = synthetic.draw_outages(g, 70, seed=77)
+    dis = p.outage_masks(outs)
+    x0 = np.tile(p.x_base, (outs.shape[0], 1))
+    bad = np.array([0, 5, 33, 69])
+    x0[bad] = np.nan
+    s = native.Structure(p)
+    ctx = native.BatchContext(s, outs.shape[0])
+    ctx.set_schedule(schedule, lanes, threads)
+    ctx.set_fallback_start(True)
+    r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis, x0_full=x0)
+    assert np.array_equal(ctx.last_fallbacks(), bad)
+    ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis)
+    _compare(r, ref, p.n)
+    # without the fallback the NaN lanes diverge
+    ctx.set_fallback_start(False)
+    r2 = ctx.solve(p.x_base, p.target, p.base_row_mode, dis, x0_full=x0)
+    assert np.all(r2[bad, p.n + 2] == -1)
+    assert ctx.last_fallbacks().size == 0
+
+
+def test_phase_timing_reports_every_phase(engine_lib):
+    from olfgpu import native, synthetic
+    g, p = grid("grid2000")
+    outs = synthetic.draw_outages(g, 64, seed=78)
+    s = native.Structure(p)
+    ctx = native.BatchContext(s, outs.shape[0])
+    ref = ctx.solve(p.x_base, p.target, p.base_row_mode, p.outage_masks(outs)).copy()
+    ctx.set_phase_timing(True)
+    r = ctx.solve(p.x_base, p.target, p.base_row_mode, p.outage_masks(outs))
+    ph = ctx.last_phase_times()
+    assert np.array_equal(r, ref)        # same kernels, same order: the same bits
+    assert ph["iterations"] >= 2 and ph["factor"] > 0 and ph["solve"] > 0 and ph["fill"] > 0
+    assert ph["factorized_lanes"] >= outs.shape[0]
