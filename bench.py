@@ -30,6 +30,9 @@ METRIC = "N-1 solves/s (9k-bus, 500 outages) learned+mixed vs plain FP64 NR at 1
 GRID = "grid9241"
 N_OUTAGES = 500
 TOL = 1e-8
+# DRAM bytes (read + write) of one lane's factorization, from an ncu capture of every factorization launch of a
+# small batch (the capture's total over its factorized lanes); scaled to a launch by the lanes it factorizes
+TRAFFIC = {"fp64": None, "mixed": None}
 
 
 def _peaks():
@@ -84,12 +87,12 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def workload(rank: int):
+def workload(rank: int, count: int = N_OUTAGES):
     from olfgpu import packing, synthetic
     g = synthetic.build(GRID)
     p = packing.pack(g)
     # weak scaling: every rank solves its own 500 outages of the same grid
-    outs = synthetic.draw_outages(g, N_OUTAGES, seed=9241 + rank)
+    outs = synthetic.draw_outages(g, count, seed=9241 + rank)
     return g, p, outs
 
 
@@ -108,7 +111,7 @@ def run_engine(args, rank: int, world: int):
     if world > 1:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    g, p, outs = workload(rank)
+    g, p, outs = workload(rank, args.outages)
     precision = native.MIXED if args.precision == "mixed" else native.FP64
     refinement = args.refinement if precision == native.MIXED else 0
     s = native.Structure(p)
@@ -157,6 +160,21 @@ def run_engine(args, rank: int, world: int):
     pbytes = 4 if precision == native.MIXED else 8
     total_bytes, b_it = algorithmic_bytes(s, p, tot_iters // args.steps, pbytes, refinement)
     achieved = total_bytes / (dev * 1e-3) / 1e9
+    # the dominant kernel family, the block-LU factorization (factorLevelKernel + factorRangeKernel launches of one
+    # Newton iteration): one more solve of the same batch, after the timed region, with each phase bracketed by CUDA
+    # events on the context's stream; algorithmic bytes of one lane's factorization = read J once (8 nnzJ) + write and
+    # read the LU once (2 w nnzLU)
+    ctx.set_phase_timing(True)
+    step()
+    ph = ctx.last_phase_times()
+    ctx.set_phase_timing(False)
+    fact_bytes_lane = 8 * s.nnz + 2 * pbytes * s.n_lu_blocks * 4
+    fact_launch_ms = ph["factor"] / max(ph["iterations"], 1)
+    fact_bytes_launch = fact_bytes_lane * ph["factorized_lanes"] / max(ph["iterations"], 1)
+    fact_achieved = fact_bytes_launch / (fact_launch_ms * 1e-3) / 1e9 if fact_launch_ms > 0 else 0.0
+    traffic = TRAFFIC.get(args.precision)
+    if traffic is not None:
+        traffic = int(traffic * ph["factorized_lanes"] / max(ph["iterations"], 1))
     words = (ns + 31) // 32
     h2d = p.n * 8 * 2 + p.n * 4 + p.n_elements * words * 4
     d2h = ns * (p.n + 3) * 8
@@ -174,19 +192,26 @@ def run_engine(args, rank: int, world: int):
         "vs_baseline": None,
         "dtype": "fp32-lu+fp64" if precision == native.MIXED else "f64",
         "data": "synthetic (seeded 9,241-bus grid, random non-bridge branch outages)",
-        "config": {"workload": f"{GRID}: 9,241 buses, {p.n_cb} branches, {N_OUTAGES} outages per GPU, warm start "
+        "config": {"workload": f"{GRID}: 9,241 buses, {p.n_cb} branches, {ns} outages per GPU, warm start "
                                f"from the base case, tol {TOL} pu, FP32 LU + {refinement} FP64 refinement step(s)"
                    if precision == native.MIXED else
-                   f"{GRID}: 9,241 buses, {p.n_cb} branches, {N_OUTAGES} outages per GPU, warm start, tol {TOL} pu, "
+                   f"{GRID}: 9,241 buses, {p.n_cb} branches, {ns} outages per GPU, warm start, tol {TOL} pu, "
                    f"FP64 LU",
                    "precision": args.precision, "l2": "working set > 1 GB per step, larger than the 126 MB L2",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "e2e": {"value": round(world * ns / (e2e * 1e-3), 1), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None,
-                     "scope": "whole Newton iterations: (8 nnzJ + 2 w nnzLU + 48 n) bytes per scenario-iteration",
-                     "peak_source": peak_kind},
+        "roofline": {"bound": "hbm", "achieved": round(fact_achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(fact_achieved / peak, 4), "traffic": traffic,
+                     "kernel": "block-LU factorization of one Newton iteration (factorLevelKernel levels + "
+                               "factorRangeKernel narrow levels)",
+                     "algorithmic_bytes_per_launch": int(fact_bytes_launch), "launch_ms": round(fact_launch_ms, 4),
+                     "unit_bytes": "8 nnzJ + 2 w nnzLU per factorized lane",
+                     "peak_source": f"{peak_kind} copy bandwidth (hbm_gbs)"},
+        "roofline_iteration": {"achieved": round(achieved, 1), "frac": round(achieved / peak, 4),
+                               "scope": "whole Newton iterations: (8 nnzJ + 2 w nnzLU + 48 n) bytes per "
+                                        "scenario-iteration over the step's device time"},
+        "phase_ms": {k: round(v, 3) for k, v in ph.items() if isinstance(v, float)},
         "gpu_launches": None,
         "iterations_per_solve": round(tot_iters / args.steps / ns, 3),
         "converged_fraction": round(conv, 4),
@@ -219,6 +244,143 @@ def cpu_baseline(p, outs, sample: int):
     return {"value": round(sub.shape[0] / dt, 2), "unit": "solves/s", "cores": cores, "kind": "port",
             "sample": f"{sub.shape[0]} of the {outs.shape[0]} outages, {dt:.1f} s on {cores} threads",
             "converged": int((r[:, -1] == 0).sum())}
+
+
+UNEVEN = [("grid300", 1000), ("grid2000q", 1000), ("grid9241q", 500), ("grid13659", 250)]
+
+
+def run_uneven(args, rank: int, world: int):
+    """Uneven batching: four grids (300 / 2,000 / 9,241 / 13,659 buses; 1,000 / 1,000 / 500 / 250 outages, reactive
+    limits on) in ONE persistent graph-captured launch, autotuned schedule beside a fixed one and beside one
+    level-schedule batch per grid run back to back."""
+    import torch
+    from olfgpu import native, packing, synthetic
+    from olfgpu.security_analysis import MultiGridAnalysis
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    precision = native.MIXED if args.precision == "mixed" else native.FP64
+    grids = [synthetic.build(nm) for nm, _ in UNEVEN]
+    packs = [packing.pack(g) for g in grids]
+    counts = [c for _, c in UNEVEN]
+    outs = [synthetic.draw_outages(g, c, seed=7000 + 17 * rank + i, replace=True)
+            for i, (g, c) in enumerate(zip(grids, counts))]
+    total = sum(counts)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        dev, wall = [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            dev.append(fn())
+            wall.append((time.perf_counter() - t0) * 1e3)
+        return float(np.mean(dev)), float(np.mean(wall))
+
+    ma = MultiGridAnalysis(packs, counts, precision=precision, schedule=-1)
+    ma.solve(outs)                                     # autotunes on the first solve
+    pick, tuning = ma.multi.schedule()
+    last = {}
+
+    def multi_step():
+        res, ms = ma.solve(outs)
+        last["res"] = res
+        return ms
+
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
+    with sampler:
+        dev_auto, wall_auto = timed(multi_step)
+    res = last["res"]
+    iters = [int(r.total_iterations.sum()) for r in res]
+    fixed = (2, 256, 0)
+    ma.multi.set_schedule(*fixed)
+    dev_fixed, _ = timed(multi_step)
+    ma.close()
+    # one level-schedule batch per grid, back to back (each grid's own launches)
+    seq = []
+    for p, o in zip(packs, outs):
+        st = native.Structure(p)
+        c = native.BatchContext(st, o.shape[0], native.BATCHED_LU, p.rl)
+        c.set_linear_solver_settings(precision, 1)
+        seq.append((st, c, p, p.outage_masks(o)))
+
+    def seq_step():
+        ms = 0.0
+        for st, c, p, dis in seq:
+            c.solve(p.x_base, p.target, p.base_row_mode, dis, max_iter=15, tol=TOL)
+            ms += c.last_stats()[0]
+        return ms
+    dev_seq, _ = timed(seq_step)
+    peak, peak_kind = _peaks()
+    pbytes = 4 if precision == native.MIXED else 8
+    ref_steps = 1 if precision == native.MIXED else 0
+    tot_bytes = 0
+    for (st, c, p, dis), it in zip(seq, iters):
+        tot_bytes += algorithmic_bytes(st, p, it, pbytes, ref_steps)[0]
+    achieved = tot_bytes / (dev_auto * 1e-3) / 1e9
+    conv = float(np.mean(np.concatenate([r.status == 0 for r in res])))
+    if world > 1:
+        t = torch.tensor([dev_auto, wall_auto], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        dev_auto, wall_auto = float(t[0]), float(t[1])
+    h2d = sum(p.n * 8 * 2 + p.n * 4 + p.n_elements * ((c + 31) // 32) * 4 for p, c in zip(packs, counts))
+    d2h = sum(c * (p.n + 3) * 8 for p, c in zip(packs, counts))
+    line = {
+        "metric": "N-1 solves/s, uneven batch of four grids in one persistent launch (reactive limits on)",
+        "value": round(world * total / (dev_auto * 1e-3), 1), "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_auto, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32-lu+fp64" if precision == native.MIXED else "f64",
+        "data": "synthetic (seeded grids, random non-bridge branch outages drawn with replacement)",
+        "config": {"workload": "grid300 x1000 + grid2000q x1000 + grid9241q x500 + grid13659 x250 outages, "
+                               "Q limits +-U[0.3,0.6] Pmax, reactive-limit outer loop on, tol 1e-8 pu",
+                   "precision": args.precision, "l2": "working set > 1 GB per step, larger than the 126 MB L2",
+                   "autotuned_schedule": {"lanes_per_tile": pick[0], "threads": pick[1],
+                                          "order": ["as given", "most buses first"][pick[2]],
+                                          "ms": round(dev_auto, 3)},
+                   "fixed_schedule": {"lanes_per_tile": fixed[0], "threads": fixed[1], "order": "as given",
+                                      "ms": round(dev_fixed, 3),
+                                      "solves_per_s": round(total / (dev_fixed * 1e-3), 1)},
+                   "per_grid_level_batches": {"ms": round(dev_seq, 3),
+                                              "solves_per_s": round(total / (dev_seq * 1e-3), 1)},
+                   "autotune_candidates": [[int(a), int(b), int(c), round(d, 3)] for a, b, c, d in tuning],
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "e2e": {"value": round(world * total / (wall_auto * 1e-3), 1), "unit": "solves/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "kernel": "newtonMultiKernel (the whole Newton loop of the four grids in one launch)",
+                     "peak_source": f"{peak_kind} copy bandwidth (hbm_gbs)"},
+        "gpu_launches": 1 + 4 + 5 * 4,
+        "iterations_per_solve": round(sum(iters) / total, 3),
+        "converged_fraction": round(conv, 4),
+        "clocks": sampler.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        cores = os.cpu_count() or 1
+        secs = 0.0
+        sample = []
+        for p, o, c in zip(packs, outs, counts):
+            k = max(1, min(c, args.cpu_sample // 4))
+            t0 = time.perf_counter()
+            O.Structure(p).solve_batch(p.x_base, p.outage_masks(o[:k]), max_iter=15, tol=TOL, reactive_limits=True,
+                                       threads=cores)
+            dt = time.perf_counter() - t0
+            secs += dt / k * c
+            sample.append(f"{k}/{c}")
+        line["cpu_baseline"] = {"value": round(total / secs, 2), "unit": "solves/s", "cores": cores, "kind": "port",
+                                "sample": "oracle with reactive limits on " + ", ".join(sample) +
+                                          " outages per grid, scaled to the whole mix"}
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def run_reference(args, rank: int, world: int):
@@ -261,12 +423,18 @@ def main():
     ap.add_argument("--refinement", type=int, default=1)
     ap.add_argument("--cpu-sample", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--outages", type=int, default=N_OUTAGES,
+                    help="outages per GPU (500 is the benchmark; smaller batches are profiling cases)")
+    ap.add_argument("--workload", default="n1", choices=["n1", "uneven"],
+                    help="n1: the 9,241-bus N-1 batch (default); uneven: four grids in one persistent launch")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "engine" else args.warmup
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.workload == "uneven":
+        run_uneven(args, rank, world)
     else:
         run_engine(args, rank, world)
 
