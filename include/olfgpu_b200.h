@@ -144,10 +144,12 @@ int olfgpu_last_phase_times(int64_t context, double* out8);
 
 /*
  * Fallback start (no counterpart in the reference): with enable = 1, a solve given both x0Full (e.g. learned starts)
- * and x0Base restarts every scenario whose solve from x0Full ends DIVERGED, MAX_ITERATION_REACHED or
- * LINEAR_SOLVE_FAILED once from x0Base, inside the same batch (its result, iterations and status are those of the
- * restarted solve; total iterations count both).  Not available with reactive limits.  olfgpu_last_fallbacks writes
- * per scenario 1 where the last solve restarted it (fellBack [nScenarios], may be null) and their count.
+ * and x0Base first keeps, per scenario, whichever of its x0Full row and x0Base has the smaller initial max |F|; then
+ * every scenario whose solve from its x0Full row ends DIVERGED, MAX_ITERATION_REACHED or LINEAR_SOLVE_FAILED restarts
+ * once from x0Base, inside the same batch (its result, iterations and status are those of the restarted solve; total
+ * iterations count both).  Not available with reactive limits.  olfgpu_last_fallbacks writes per scenario 0 (its own
+ * start), 1 (restarted from x0Base after failing) or 2 (x0Base chosen before iterating) into fellBack [nScenarios]
+ * (may be null), and the count of non-zero entries.
  */
 int olfgpu_set_fallback_start(int64_t context, int enable);
 int olfgpu_last_fallbacks(int64_t context, unsigned char* fellBack, int* count);

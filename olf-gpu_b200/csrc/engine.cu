@@ -401,6 +401,32 @@ __global__ void tileModeKernel(const int* base, int8_t* out, int n, int S) {
 }
 
 // scenario-major [nS][n] -> lane-interleaved [n][S] through 32x32 shared tiles
+// Start selection of the fallback mode: the per-lane max |F| of the fill just run moves to out[s] (NaN stays NaN)
+// and the accumulator is cleared for the Newton loop.
+__global__ void takeNormKernel(DevBatch b, double* out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.S) return;
+    out[s] = __longlong_as_double((long long)b.norm[s]);
+    b.norm[s] = 0ull;
+}
+
+// Keeps, per lane, the start with the smaller initial max |F|: x holds the base start, `saved` the lane's own start.
+// A lane that keeps the base start is marked (fellBack = 2) and not restarted again on failure.
+__global__ void chooseStartKernel(DevBatch b, const double* saved, const double* normOwn, const double* normBase, int n) {
+    const size_t S = b.S;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (size_t)n * S) return;
+    const int s = (int)(tid % S);
+    if (s >= b.nS) return;
+    const bool own = normOwn[s] <= normBase[s];      // false when the own start's mismatch is NaN
+    if (own) {
+        b.x[tid] = saved[tid];
+    } else if (tid < S) {
+        b.fellBack[s] = 2;
+        b.fallbackLeft[s] = 0;
+    }
+}
+
 __global__ void toLanesKernel(const double* in, double* out, int n, int nS, int S) {
     __shared__ double tile[32][33];
     const int r0 = blockIdx.x * 32, s0 = blockIdx.y * 32;
@@ -690,6 +716,28 @@ int roundCap(const BatchContext& ctx) {
 }
 
 // The Newton iterations under the context's schedule; returns the batched iterations run (level launches) or 0.
+// Fallback mode, before the first iteration: each lane starts from whichever of its own start (x0Full) and the base
+// start (x0Base) has the smaller max |F| (two mismatch-only fills over all lanes).
+void selectStarts(BatchContext& ctx) {
+    const DeviceNet& dn = *ctx.net->dev;
+    cudaStream_t st = ctx.stream;
+    const int n = ctx.net->host.n;
+    const size_t all = static_cast<size_t>(n) * ctx.S;
+    const DevBatch b = ctx.batch();
+    double* saved = ctx.dx.as<double>();             // free until the first solve
+    double* normOwn = ctx.res.as<double>();          // [S] scratch at the head of the residual buffer
+    double* normBase = normOwn + ctx.S;
+    OLF_CUDA(cudaMemsetAsync(ctx.norm.p, 0, ctx.norm.bytes, st));
+    launchFill(dn.view, b, false, false, st);
+    takeNormKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b, normOwn);
+    OLF_CUDA(cudaMemcpyAsync(saved, ctx.x.p, all * 8, cudaMemcpyDeviceToDevice, st));
+    tileKernel<<<static_cast<unsigned>((all + 255) / 256), 256, 0, st>>>(ctx.stage.as<double>(), ctx.x.as<double>(), n,
+                                                                         ctx.S);
+    launchFill(dn.view, b, false, false, st);
+    takeNormKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b, normBase);
+    chooseStartKernel<<<static_cast<unsigned>((all + 255) / 256), 256, 0, st>>>(b, saved, normOwn, normBase, n);
+}
+
 int runIterations(BatchContext& ctx) {
     cudaStream_t st = ctx.stream;
     const DeviceNet& dn = *ctx.net->dev;
@@ -698,6 +746,7 @@ int runIterations(BatchContext& ctx) {
     if (mixed && !ctx.lu32.p) ctx.lu32.alloc(static_cast<size_t>(dn.view.nLu) * 4 * S * 4);
     if (!mixed && !ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(dn.view.nLu) * 4 * S * 8);
     const int cap = roundCap(ctx);
+    if (ctx.fallbackStart && ctx.hasX0Base && ctx.hasX0Full) selectStarts(ctx);
     if (ctx.schedule == SCHEDULE_PERSISTENT) {
         PersistentPlan plan = dn.persistent;
         plan.maxRounds = cap;

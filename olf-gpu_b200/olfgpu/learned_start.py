@@ -151,13 +151,41 @@ class LearnedStart:
         x[rows, tidx, N_FEAT + 2] = (-fl[:, 1]).to(x.dtype)
         return x.reshape(B * nb, FEAT_IN).contiguous()
 
+    def split(self, data: Dataset, held_out_scalings: int):
+        """(training, held-out) sample indices: the last ``held_out_scalings`` load scalings are held out."""
+        import torch
+        cut = int(data.x.shape[0]) - held_out_scalings
+        mask = data.scaling >= cut
+        return torch.nonzero(~mask).flatten(), torch.nonzero(mask).flatten()
+
+    def evaluate(self, data: Dataset, samples=None, chunk: int = 32):
+        """(mean normalised squared error of the network, of the base start) over the samples: the base start predicts
+        no change, so its error is the mean squared normalised target."""
+        import torch
+        nb = self.graph.nb
+        idx_all = torch.arange(data.t.shape[0], device="cuda") if samples is None else samples
+        err = base = 0.0
+        cnt = 0
+        for a in range(0, idx_all.shape[0], chunk):
+            idx = idx_all[a:a + chunk]
+            out = data.outage[idx].contiguous()
+            x0 = self._batch_inputs(data.x[data.scaling[idx]], data.flows[data.scaling[idx]], out)
+            pred = self.net.forward(x0, out)[:, :2]
+            tg = data.t[idx].reshape(idx.shape[0] * nb, 2)
+            err += float(((pred - tg) ** 2).sum())
+            base += float((tg ** 2).sum())
+            cnt += tg.numel()
+        return err / max(cnt, 1), base / max(cnt, 1)
+
     def train(self, data: Dataset, epochs: int = 3, batch: int = 32, lr: float = 2e-3, seed: int = 0,
-              log: Optional[list] = None, max_seconds: Optional[float] = None) -> List[float]:
-        """Adam on minibatches; the learning rate decays linearly to 10 % over the run.  Returns per-epoch losses."""
+              log: Optional[list] = None, max_seconds: Optional[float] = None, samples=None) -> List[float]:
+        """Adam on minibatches (of ``samples``, default all); the learning rate decays linearly to 10 % over the run.
+        Returns per-epoch losses."""
         import torch
         self.feat_mean, self.feat_std, self.tgt_std = data.feat_mean, data.feat_std, data.tgt_std
         self.flow_std = data.flow_std
-        n = data.t.shape[0]
+        pool = torch.arange(data.t.shape[0], device="cuda") if samples is None else samples
+        n = int(pool.shape[0])
         nb = self.graph.nb
         gen = torch.Generator(device="cuda")
         gen.manual_seed(seed)
@@ -166,7 +194,7 @@ class LearnedStart:
         losses = []
         t0 = time.time()
         for ep in range(epochs):
-            perm = torch.randperm(n, device="cuda", generator=gen)
+            perm = pool[torch.randperm(n, device="cuda", generator=gen)]
             acc, cnt = 0.0, 0
             for a in range(0, n - batch + 1, batch):
                 idx = perm[a:a + batch]

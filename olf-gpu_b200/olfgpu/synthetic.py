@@ -257,11 +257,13 @@ def _open_equivalent(g: Grid):
 
 
 def newton_polar(g: Grid, v0: Optional[np.ndarray] = None, th0: Optional[np.ndarray] = None,
-                 max_iter: int = 30, tol: float = 1e-8, distributed: bool = False):
+                 max_iter: int = 30, tol: float = 1e-8, distributed: bool = False,
+                 pq_gen: Optional[np.ndarray] = None, q_fixed: Optional[np.ndarray] = None):
     """Plain NR in the stable-row form (row 2b: P balance / slack angle, row 2b+1: Q balance / PV voltage).
 
     Returns (converged, iterations, vm, va), plus the generation factor lambda when ``distributed``: then every
-    generator produces gen_p * (1 + lambda) and the slack bus's P balance is one more equation.  Used to calibrate
+    generator produces gen_p * (1 + lambda) and the slack bus's P balance is one more equation.  ``pq_gen`` marks
+    generators that hold their reactive output at ``q_fixed`` instead of their voltage set point.  Used to calibrate
     the loading and the dispatch of the synthetic grids.
     """
     nb = g.n_bus
@@ -276,9 +278,12 @@ def newton_polar(g: Grid, v0: Optional[np.ndarray] = None, th0: Optional[np.ndar
     np.add.at(tgt, 2 * g.load_bus + 1, -g.load_q)
     ident = np.zeros(n, dtype=bool)
     ident[2 * g.slack] = True
-    ident[2 * g.gen_bus + 1] = True
+    pv = np.ones(g.gen_bus.shape[0], dtype=bool) if pq_gen is None else ~pq_gen
+    ident[2 * g.gen_bus[pv] + 1] = True
     tgt[2 * g.slack] = 0.0
-    tgt[2 * g.gen_bus + 1] = g.gen_vset
+    tgt[2 * g.gen_bus[pv] + 1] = g.gen_vset[pv]
+    if pq_gen is not None:
+        np.add.at(tgt, 2 * g.gen_bus[pq_gen] + 1, q_fixed[pq_gen])
     ysh = np.zeros(nb, dtype=complex)
     np.add.at(ysh, g.shunt_bus, g.shunt_g + 1j * g.shunt_b)
     np.add.at(ysh, g.open_bus, _open_equivalent(g))
@@ -375,6 +380,42 @@ def balanced(g: Grid, s: float, vm=None, va=None, max_iter: int = 20):
     return gb, vm2, va2
 
 
+def solve_with_q_limits(g: Grid, max_outer: int = 12):
+    """Base case with the generators' reactive limits: a generator whose reactive output leaves its limits holds it
+    at the limit (PV -> PQ, no switching back).  Returns True when that converges.  Calibration helper only."""
+    if g.base_vm is None:
+        return False
+    pq = np.zeros(g.gen_bus.shape[0], dtype=bool)
+    qf = np.zeros(g.gen_bus.shape[0])
+    vm, va = g.base_vm, g.base_va
+    y = 1.0 / np.hypot(g.r, g.x)
+    ksi = np.arctan2(g.r, g.x)
+    bh = g.b / 2
+    load_q_bus = np.zeros(g.n_bus)
+    np.add.at(load_q_bus, g.load_bus, g.load_q)
+    ysh = np.zeros(g.n_bus, dtype=complex)
+    np.add.at(ysh, g.shunt_bus, g.shunt_g + 1j * g.shunt_b)
+    np.add.at(ysh, g.open_bus, _open_equivalent(g))
+    for _ in range(max_outer):
+        ok, _, vm, va = newton_polar(g, vm, va, max_iter=30, pq_gen=pq, q_fixed=qf)
+        if not ok:
+            return False
+        _, q1, _, q2, _ = _branch_terms(vm[g.f], va[g.f], vm[g.t], va[g.t], y, ksi, 0.0, bh, 0.0, bh, g.ratio)
+        qinj = np.zeros(g.n_bus)
+        np.add.at(qinj, g.f, q1)
+        np.add.at(qinj, g.t, q2)
+        qinj += -ysh.imag * vm * vm
+        qgen = qinj[g.gen_bus] + load_q_bus[g.gen_bus]
+        slack_gen = g.gen_bus == g.slack
+        hi = ~pq & ~slack_gen & (qgen > g.gen_maxq)
+        lo = ~pq & ~slack_gen & (qgen < g.gen_minq)
+        if not (hi.any() or lo.any()):
+            return True
+        qf[hi], qf[lo] = g.gen_maxq[hi], g.gen_minq[lo]
+        pq |= hi | lo
+    return False
+
+
 def calibrate(g: Grid) -> Grid:
     """The grid at the loading its spec asks for, loss-balanced.
 
@@ -438,6 +479,20 @@ def calibrate(g: Grid) -> Grid:
     return r[0]
 
 
+def _within_q_limits(g: Grid) -> Grid:
+    """A grid with reactive limits backs its loading off by 5 % steps until its base case converges with the limits
+    (the reactive-limit outer loop needs a feasible base case)."""
+    cur = g
+    for _ in range(30):
+        if solve_with_q_limits(cur):
+            return cur
+        r = balanced(g, cur.scale / g.scale * 0.95, cur.base_vm, cur.base_va)
+        if r is None:
+            break
+        cur = r[0]
+    raise RuntimeError(f"{g.spec.name}: no loading converges within the reactive limits")
+
+
 _CACHE = {}
 
 
@@ -448,6 +503,8 @@ def build(name: str, calibrate: bool = True) -> Grid:
         g = generate(SPECS[name])
         if calibrate:
             g = globals()["calibrate"](g)
+            if g.spec.q_limits:
+                g = _within_q_limits(g)
         _CACHE[key] = g
     return _CACHE[key]
 
