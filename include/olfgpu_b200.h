@@ -143,6 +143,14 @@ int olfgpu_set_phase_timing(int64_t context, int enable);
 int olfgpu_last_phase_times(int64_t context, double* out8);
 
 /*
+ * Device-resident start states (no counterpart in the reference): while x0FullDevice is set (non-null), every solve
+ * of the context takes its per-scenario start states from that device array [nScenarios][n] on the context's GPU
+ * (e.g. a learned start predicted on the device) instead of the host x0Full argument; null switches back.  The array
+ * must stay valid and unchanged while a solve runs.
+ */
+int olfgpu_set_device_start(int64_t context, const double* x0FullDevice);
+
+/*
  * Fallback start (no counterpart in the reference): with enable = 1, a solve given both x0Full (e.g. learned starts)
  * and x0Base first keeps, per scenario, whichever of its x0Full row and x0Base has the smaller initial max |F|; then
  * every scenario whose solve from its x0Full row ends DIVERGED, MAX_ITERATION_REACHED or LINEAR_SOLVE_FAILED restarts
@@ -228,6 +236,14 @@ int olfgpu_gnn_adam(int count, int K, int N, float* w, const float* grad, float*
 int olfgpu_gnn_mse(int M, int ldo, const float* out, const float* target, float* dOut, float* partial, void* stream);
 int olfgpu_gnn_copy_cols(int M, int ncols, const float* src, int lds, int srcCol0, float* dst, int ldd, int dstCol0,
                          int accumulate, void* stream);
+/*
+ * Learned start states on the device: x0 [nScenarios][2 nb] (device) from the network's output pred
+ * [nScenarios * nb][ldPred] (columns 0, 1: normalised dVm, dVa), de-normalised by stdVm / stdVa and added to the base
+ * state xBase [2 nb]; rows flagged in identity [2 nb] take target [2 nb].  All pointers are device memory.
+ */
+int olfgpu_gnn_compose_start(int nScenarios, int nb, const float* pred, int ldPred, double stdVm, double stdVa,
+                             const double* xBase, const unsigned char* identity, const double* target, double* x0,
+                             void* stream);
 
 /*
  * Batched linear solve J z = rhs that allocates no memory (this entry point has no counterpart in the reference).

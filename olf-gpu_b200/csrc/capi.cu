@@ -288,6 +288,20 @@ extern "C" int olfgpu_last_phase_times(int64_t context, double* out8) {
     });
 }
 
+extern "C" int olfgpu_set_device_start(int64_t context, const double* x0FullDevice) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        if (x0FullDevice) {
+            cudaPointerAttributes a{};
+            OLF_CUDA(cudaPointerGetAttributes(&a, x0FullDevice));
+            if (a.type != cudaMemoryTypeDevice || a.device != c.device) {
+                throw std::runtime_error("x0FullDevice is not device memory of the context's GPU");
+            }
+        }
+        c.deviceStart = x0FullDevice;
+    });
+}
+
 extern "C" int olfgpu_set_fallback_start(int64_t context, int enable) {
     return guarded([&] {
         BatchContext& c = contextOf(context);

@@ -113,8 +113,8 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     d->obList.upload(obList);
     d->obPar.upload(s.obPar);
     d->task.upload(task);
-    std::vector<int2> ops(p.opL.size());
-    for (size_t q = 0; q < ops.size(); q++) ops[q] = make_int2(p.opL[q], p.opU[q]);
+    std::vector<int4> ops(p.opL.size());
+    for (size_t q = 0; q < ops.size(); q++) ops[q] = make_int4(p.opL[q], p.opU[q], p.opD[q], 0);
     d->ops.upload(ops);
     d->levelTask.upload(p.levelTask);
     d->perm.upload(p.perm);
@@ -209,6 +209,7 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     v.nb = nb;
     v.nA = static_cast<int>(p.aCol.size());
     v.nLu = nLu;
+    v.nU = p.nU;
     v.ncb = s.ncb;
     v.nob = s.nob;
     v.nsh = s.nsh;
@@ -228,7 +229,7 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     v.obList = d->obList.as<int2>();
     v.obPar = d->obPar.as<double>();
     v.task = d->task.as<Task>();
-    v.ops = d->ops.as<int2>();
+    v.ops = d->ops.as<int4>();
     v.levelTask = d->levelTask.as<int>();
     v.perm = d->perm.as<int>();
     v.iperm = d->iperm.as<int>();
@@ -651,9 +652,11 @@ void uploadInputs(BatchContext& ctx, const SolveRequest& req) {
     double* stageT = stageX + n;
     int* stageM = reinterpret_cast<int*>(stageT + n);
     ctx.hasX0Base = req.x0Base != nullptr;
-    ctx.hasX0Full = req.x0Full != nullptr;
-    if (req.x0Full) {
+    ctx.hasX0Full = req.x0Full != nullptr || ctx.deviceStart != nullptr;
+    ctx.fullSrc = ctx.deviceStart ? ctx.deviceStart : ctx.full.as<double>();
+    if (req.x0Full && !ctx.deviceStart) {
         if (ctx.full.bytes < static_cast<size_t>(ctx.nS) * n * 8) ctx.full.alloc(static_cast<size_t>(ctx.nS) * n * 8);
+        ctx.fullSrc = ctx.full.as<double>();
         OLF_CUDA(cudaMemcpyAsync(ctx.full.p, req.x0Full, static_cast<size_t>(ctx.nS) * n * 8, cudaMemcpyHostToDevice, st));
     }
     if (req.x0Base) OLF_CUDA(cudaMemcpyAsync(stageX, req.x0Base, n * 8, cudaMemcpyHostToDevice, st));
@@ -689,7 +692,7 @@ void installLanes(BatchContext& ctx) {
     if (ctx.hasX0Base) tileKernel<<<blocksAll, 256, 0, st>>>(stageX, ctx.x.as<double>(), n, ctx.S);
     if (ctx.hasX0Full) {
         dim3 blk(32, 8), grd((n + 31) / 32, (ctx.nS + 31) / 32);
-        toLanesKernel<<<grd, blk, 0, st>>>(ctx.full.as<double>(), ctx.x.as<double>(), n, ctx.nS, ctx.S);
+        toLanesKernel<<<grd, blk, 0, st>>>(ctx.fullSrc, ctx.x.as<double>(), n, ctx.nS, ctx.S);
     }
     tileKernel<<<blocksAll, 256, 0, st>>>(stageT, ctx.target.as<double>(), n, ctx.S);
     tileModeKernel<<<blocksAll, 256, 0, st>>>(stageM, ctx.mode.as<int8_t>(), n, ctx.S);
@@ -839,7 +842,7 @@ void stageRequest(BatchContext& ctx, const SolveRequest& req) {
         throw std::runtime_error("scenario count " + std::to_string(req.nScenarios) + " does not match the context's " +
                                  std::to_string(ctx.nS));
     }
-    if (!req.x0Base && !req.x0Full) throw std::runtime_error("no start state");
+    if (!req.x0Base && !req.x0Full && !ctx.deviceStart) throw std::runtime_error("no start state");
     if (!req.targetBase || !req.baseRowMode) throw std::runtime_error("no base targets or row modes");
     if (req.maxIter < 1) throw std::runtime_error("maxIter must be >= 1");
     for (int r = 0; r < n; r++) {

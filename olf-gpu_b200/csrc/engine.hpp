@@ -126,6 +126,8 @@ struct BatchContext {
     DeviceBuffer x, target, mode, F, J, lu64, lu32, w64, w32, dx, res, qbuf, disabled, norm, iter, status, outer,
         totalIter, trouble, normOut, active, pending, precision64, nActive, fallbackLeft, fellBack;
     bool fallbackStart = false;     // lanes that fail from x0Full restart once from x0Base (both given)
+    const double* deviceStart = nullptr;  // caller's device array [nS][n] used as x0Full by the solves
+    const double* fullSrc = nullptr;      // where the installed x0Full rows come from
     DeviceBuffer stage;             // upload staging (base vectors)
     DeviceBuffer ovIdx, ovVal, rowModeE;  // per-scenario overrides of the installed batch
     int nTargetOverrides = 0, nRowModeEntries = 0;

@@ -407,6 +407,25 @@ int gnnGuard(F&& f) {
 }
 }  // namespace
 
+// Start states from the network's output: per scenario s and bus b, x0[s][2b] (angle) = xBase + dVa * stdVa and
+// x0[s][2b + 1] (magnitude) = xBase + dVm * stdVm, the identity rows (slack angle, PV magnitudes) at their targets.
+__global__ void composeStartKernel(int nS, int nb, const float* pred, int ldp, double stdVm, double stdVa,
+                                   const double* xBase, const unsigned char* identity, const double* target,
+                                   double* x0) {
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = 2 * nb;
+    if (tid >= (long long)nS * n) return;
+    const int s = (int)(tid / n), r = (int)(tid % n), b = r >> 1;
+    double v;
+    if (identity[r]) {
+        v = target[r];
+    } else {
+        const float* o = pred + ((long long)s * nb + b) * ldp;
+        v = xBase[r] + ((r & 1) ? (double)o[0] * stdVm : (double)o[1] * stdVa);
+    }
+    x0[tid] = v;
+}
+
 extern "C" const char* olfgpu_gnn_last_error(void) { return gnnError.c_str(); }
 
 extern "C" int olfgpu_gnn_gemm(int M, int K1, int K2, int N, const void* A1, const void* A2, const void* W,
@@ -528,5 +547,15 @@ extern "C" int olfgpu_gnn_copy_cols(int M, int ncols, const float* src, int lds,
         const long long count = (long long)M * ncols;
         copyColsKernel<<<(unsigned)((count + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
             count, ncols, src, lds, srcCol0, dst, ldd, dstCol0, accumulate);
+    });
+}
+
+extern "C" int olfgpu_gnn_compose_start(int nScenarios, int nb, const float* pred, int ldPred, double stdVm,
+                                        double stdVa, const double* xBase, const unsigned char* identity,
+                                        const double* target, double* x0, void* stream) {
+    return gnnGuard([&] {
+        const long long count = (long long)nScenarios * 2 * nb;
+        composeStartKernel<<<(unsigned)((count + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+            nScenarios, nb, pred, ldPred, stdVm, stdVa, xBase, identity, target, x0);
     });
 }

@@ -352,8 +352,10 @@ void launchReactiveLimits(const DevNet&, const DevBatch& b, const DevRl& rl, con
 
 // ---------------------------------------------------------------------------------------------------------------
 // Batched block LU, one level of tasks per launch: one thread per (LU block, lane).
-//   U(k, j) = A(k, j) - sum_m L(k, m) U(m, j);    L(i, k) = (A(i, k) - sum_m L(i, m) U(m, k)) inv(U(k, k))
-// The diagonal slot U(k, k) stores its inverse.  The update pairs come in ascending m (a fixed summation order).
+//   U(k, j) = A(k, j) - sum_m L~(k, m) inv(D_m) U(m, j);    L~(i, k) = A(i, k) - sum_m L~(i, m) inv(D_m) U(m, k)
+// with D_m = U(m, m), whose slot stores its inverse.  L~ is the unscaled L: it does not wait for its own column's
+// pivot, so the dependency chain is about one level per pivot instead of two; scaleLKernel finally turns every L~
+// into L = L~ inv(D_k) for the triangular solves.  The updates come in ascending m (a fixed summation order).
 // A near-singular 2x2 pivot (|det| <= 1e-13 of its terms, lu_pivot.cuh:12-18) flags the lane.
 // ---------------------------------------------------------------------------------------------------------------
 template <typename T>
@@ -406,16 +408,19 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
             a10 = (T)p[2 * S];
             a11 = (T)p[3 * S];
         }
-#pragma unroll 4
+#pragma unroll 2
         for (int q = tk.opBegin + part; q < tk.opEnd; q += P) {
-            const int2 op = net.ops[q];
-            T l00, l01, l10, l11, u00, u01, u10, u11;
+            const int4 op = net.ops[q];
+            T l00, l01, l10, l11, d00, d01, d10, d11, u00, u01, u10, u11;
             load4(lu, (size_t)op.x, S, s, l00, l01, l10, l11);
+            load4(lu, (size_t)op.z, S, s, d00, d01, d10, d11);
             load4(lu, (size_t)op.y, S, s, u00, u01, u10, u11);
-            a00 -= l00 * u00 + l01 * u10;
-            a01 -= l00 * u01 + l01 * u11;
-            a10 -= l10 * u00 + l11 * u10;
-            a11 -= l10 * u01 + l11 * u11;
+            const T m00 = l00 * d00 + l01 * d10, m01 = l00 * d01 + l01 * d11;
+            const T m10 = l10 * d00 + l11 * d10, m11 = l10 * d01 + l11 * d11;
+            a00 -= m00 * u00 + m01 * u10;
+            a01 -= m00 * u01 + m01 * u11;
+            a10 -= m10 * u00 + m11 * u10;
+            a11 -= m10 * u01 + m11 * u11;
         }
     }
     if (P > 1) {
@@ -440,14 +445,24 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
         if (!(fabs(det) > (T)1e-13 * scale) || !isfinite(det)) b.trouble[s] = 1;
         const T inv = (T)1 / det;
         store4(lu, (size_t)t, S, s, a11 * inv, -a01 * inv, -a10 * inv, a00 * inv);
-    } else if (tk.diag >= 0) {
-        T i00, i01, i10, i11;
-        load4(lu, (size_t)tk.diag, S, s, i00, i01, i10, i11);
-        store4(lu, (size_t)t, S, s, a00 * i00 + a01 * i10, a00 * i01 + a01 * i11, a10 * i00 + a11 * i10,
-               a10 * i01 + a11 * i11);
     } else {
         store4(lu, (size_t)t, S, s, a00, a01, a10, a11);
     }
+}
+
+// The last pass of a factorization: L(i, k) = L~(i, k) inv(D_k) for every L block (ids nU .. nLu - 1).  One thread
+// per (L block, lane): 32 lanes x 8 blocks per CTA.
+template <typename T>
+__global__ void scaleLKernel(DevNet net, DevBatch b, T* lu) {
+    const size_t S = b.S;
+    const int s = blockIdx.y * 32 + threadIdx.x;
+    const int id = net.nU + blockIdx.x * 8 + threadIdx.y;
+    if (id >= net.nLu || s >= b.S || !solving(b, s)) return;
+    T a00, a01, a10, a11, i00, i01, i10, i11;
+    load4(lu, (size_t)id, S, s, a00, a01, a10, a11);
+    load4(lu, (size_t)net.task[id].diag, S, s, i00, i01, i10, i11);
+    store4(lu, (size_t)id, S, s, a00 * i00 + a01 * i10, a00 * i01 + a01 * i11, a10 * i00 + a11 * i10,
+           a10 * i01 + a11 * i11);
 }
 
 __global__ void clearTroubleKernel(DevBatch b) {
@@ -484,7 +499,18 @@ void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtr, con
             OLF_SPLIT_DISPATCH(levelSplit[l], factorLevelKernel, double, net, b, b.lu64, first, count)
         }
     }
-    if (hybrid) launchFactorRange(net, b, hybrid->plan, wide, nLevels, hybrid->lanes, fp32, st);
+    if (hybrid) {
+        // the range kernel ends with the L scaling pass of its tiles
+        launchFactorRange(net, b, hybrid->plan, wide, nLevels, hybrid->lanes, fp32, st);
+    } else {
+        const int nL = net.nLu - net.nU;
+        dim3 blk(32, 8), grd((nL + 7) / 8, b.S / 32);
+        if (fp32) {
+            scaleLKernel<float><<<grd, blk, 0, st>>>(net, b, b.lu32);
+        } else {
+            scaleLKernel<double><<<grd, blk, 0, st>>>(net, b, b.lu64);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------------------------------------

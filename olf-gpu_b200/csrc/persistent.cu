@@ -62,8 +62,9 @@ __device__ __forceinline__ int splitFor(int count, int longest, int slots) {
     return P;
 }
 
-// Factorization levels [l0, l1) of one tile: tasks of a level shared by P slots each (splitFor), partial sums added
-// in a fixed order through shared memory.  `trouble` receives 1 for a lane that meets a near-singular 2x2 pivot.
+// Factorization levels [l0, l1) of one tile, l1 being the last level: tasks of a level shared by P slots each
+// (splitFor), partial sums added in a fixed order through shared memory; then the pass that scales every unscaled L
+// block by its pivot's inverse.  `trouble` receives 1 for a lane that meets a near-singular 2x2 pivot.
 template <typename T, int L>
 __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const int* levelPtr, const int* longest,
                              int l0, int l1, bool solve, int lane, int slot, int slots, int s, T (*red)[4][L],
@@ -92,14 +93,17 @@ __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const 
                 }
 #pragma unroll 2
                 for (int q = tk.opBegin + part; q < tk.opEnd; q += P) {
-                    const int2 op = net.ops[q];
-                    T l00, l01, l10, l11, u00, u01, u10, u11;
+                    const int4 op = net.ops[q];
+                    T l00, l01, l10, l11, d00, d01, d10, d11, u00, u01, u10, u11;
                     ld4(lu, (size_t)op.x, S, s, l00, l01, l10, l11);
+                    ld4(lu, (size_t)op.z, S, s, d00, d01, d10, d11);
                     ld4(lu, (size_t)op.y, S, s, u00, u01, u10, u11);
-                    a00 -= l00 * u00 + l01 * u10;
-                    a01 -= l00 * u01 + l01 * u11;
-                    a10 -= l10 * u00 + l11 * u10;
-                    a11 -= l10 * u01 + l11 * u11;
+                    const T m00 = l00 * d00 + l01 * d10, m01 = l00 * d01 + l01 * d11;
+                    const T m10 = l10 * d00 + l11 * d10, m11 = l10 * d01 + l11 * d11;
+                    a00 -= m00 * u00 + m01 * u10;
+                    a01 -= m00 * u01 + m01 * u11;
+                    a10 -= m10 * u00 + m11 * u10;
+                    a11 -= m10 * u01 + m11 * u11;
                 }
             }
             if (P > 1) {
@@ -124,11 +128,6 @@ __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const 
                     if (!(fabs(det) > (T)1e-13 * scale) || !isfinite(det)) *trouble = 1;
                     const T inv = (T)1 / det;
                     st4(lu, (size_t)t, S, s, a11 * inv, -a01 * inv, -a10 * inv, a00 * inv);
-                } else if (tk.diag >= 0) {
-                    T i00, i01, i10, i11;
-                    ld4(lu, (size_t)tk.diag, S, s, i00, i01, i10, i11);
-                    st4(lu, (size_t)t, S, s, a00 * i00 + a01 * i10, a00 * i01 + a01 * i11, a10 * i00 + a11 * i10,
-                        a10 * i01 + a11 * i11);
                 } else {
                     st4(lu, (size_t)t, S, s, a00, a01, a10, a11);
                 }
@@ -137,6 +136,16 @@ __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const 
         }
         __syncthreads();
     }
+    if (solve) {
+        for (int id = net.nU + slot; id < net.nLu; id += slots) {
+            T a00, a01, a10, a11, i00, i01, i10, i11;
+            ld4(lu, (size_t)id, S, s, a00, a01, a10, a11);
+            ld4(lu, (size_t)net.task[id].diag, S, s, i00, i01, i10, i11);
+            st4(lu, (size_t)id, S, s, a00 * i00 + a01 * i10, a00 * i01 + a01 * i11, a10 * i00 + a11 * i10,
+                a10 * i01 + a11 * i11);
+        }
+    }
+    __syncthreads();
 }
 
 // Triangular-solve levels [l0, l1) of one tile: dir 0 forward (L rows), dir 1 backward (U rows, times the inverse

@@ -622,6 +622,7 @@ void buildBlockPlan(Structure& s, int ordering) {
     for (int id = 0; id < nLu; id++) p.opPtr[id + 1] = p.opPtr[id] + cnt[id];
     p.opL.assign(ops, 0);
     p.opU.assign(ops, 0);
+    p.opD.assign(ops, 0);
     std::vector<int> fillPos(p.opPtr.begin(), p.opPtr.end() - 1);
     for (int m = 0; m < nb; m++) {
         const auto& sm = st[m];
@@ -632,27 +633,25 @@ void buildBlockPlan(Structure& s, int ordering) {
                 int q = fillPos[id]++;
                 p.opL[q] = la;
                 p.opU[q] = uBlock(m, b);
+                p.opD[q] = p.uPtr[m];
             }
         }
     }
-    // levels: U row k (diagonal first) then L column k, for k ascending
+    // levels: a task runs one level after every block its updates read (L~, U and the pivot's inverted diagonal);
+    // unscaled L blocks do not wait for their own column's pivot, which halves the dependency chain
     p.level.assign(nLu, 0);
     int maxLevel = 0;
+    auto levelOf = [&](int id) {
+        int lv = 0;
+        for (int q = p.opPtr[id]; q < p.opPtr[id + 1]; q++) {
+            lv = std::max(lv, std::max(std::max(p.level[p.opL[q]], p.level[p.opU[q]]), p.level[p.opD[q]]) + 1);
+        }
+        p.level[id] = lv;
+        maxLevel = std::max(maxLevel, lv);
+    };
     for (int k = 0; k < nb; k++) {
-        for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) {
-            int lv = 0;
-            for (int q = p.opPtr[t]; q < p.opPtr[t + 1]; q++) lv = std::max(lv, std::max(p.level[p.opL[q]], p.level[p.opU[q]]) + 1);
-            p.level[t] = lv;
-            maxLevel = std::max(maxLevel, lv);
-        }
-        int dk = p.uPtr[k];
-        for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++) {
-            int id = p.nU + t;
-            int lv = p.level[dk] + 1;
-            for (int q = p.opPtr[id]; q < p.opPtr[id + 1]; q++) lv = std::max(lv, std::max(p.level[p.opL[q]], p.level[p.opU[q]]) + 1);
-            p.level[id] = lv;
-            maxLevel = std::max(maxLevel, lv);
-        }
+        for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) levelOf(t);
+        for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++) levelOf(p.nU + t);
     }
     p.levelPtr.assign(maxLevel + 2, 0);
     for (int id = 0; id < nLu; id++) p.levelPtr[p.level[id] + 1]++;

@@ -32,8 +32,11 @@ struct BlockPlan {
     std::vector<int> aDiag;       // node -> A block id of its diagonal
     std::vector<int> aToLu;       // A block id -> LU block id
     std::vector<int> luToA;       // LU block id -> A block id or -1 (pure fill-in)
-    // Factorization: one task per LU block; its update pairs (L block, U block) in ascending k; its level.
-    std::vector<int> opPtr, opL, opU;   // per LU block
+    // Factorization: one task per LU block; its updates (L block, U block, the pivot's diagonal block) in ascending
+    // pivot order; its level.  L blocks are computed unscaled (A(i,k) - sum L~(i,m) inv(D_m) U(m,k)), so an update
+    // applies the pivot's inverted diagonal itself and an L block does not wait for its own column's pivot; one last
+    // pass scales every L block by its pivot's inverse.
+    std::vector<int> opPtr, opL, opU, opD;   // per LU block
     std::vector<int> level;             // per LU block
     std::vector<int> levelPtr, levelTask;  // tasks grouped by level (CSR); tasks are LU block ids
     // Triangular solves: forward over positions in L, backward in U; level sets of positions.

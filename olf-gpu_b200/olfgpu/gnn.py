@@ -46,6 +46,7 @@ def _lib():
             "olfgpu_gnn_adam": [i, i, i, vp, vp, vp, vp, f, f, f, f, i, vp, vp, vp],
             "olfgpu_gnn_mse": [i, i, vp, vp, vp, vp, vp],
             "olfgpu_gnn_copy_cols": [i, i, vp, i, i, vp, i, i, i, vp],
+            "olfgpu_gnn_compose_start": [i, i, vp, i, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp, vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

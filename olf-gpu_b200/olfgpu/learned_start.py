@@ -219,9 +219,11 @@ class LearnedStart:
         return losses
 
     # ------------------------------------------------------------------------------------------------------------
-    def predict(self, p, x_base: np.ndarray, outages: np.ndarray, chunk: int = 128):
-        """Start states [nS, n] (float64, on the host) for the outages, from the base case state."""
+    def predict_device(self, p, x_base: np.ndarray, outages: np.ndarray, chunk: int = 128, out=None):
+        """Start states [nS, n] (float64, a CUDA tensor) for the outages, from the base case state: the network's
+        forward passes and the composition of the states (olfgpu_gnn_compose_start) all run on the device."""
         import torch
+        from .gnn import _call, _ptr, _stream
         nb = p.n_bus
         f = node_features(p, x_base)
         fx = np.zeros((nb, FEAT_IN), np.float32)
@@ -232,20 +234,21 @@ class LearnedStart:
                               self.flow_std).cuda()
         outs = torch.from_numpy(np.asarray(outages, np.int32)).cuda()
         ns = outs.shape[0]
-        res = torch.empty((ns, nb, 2), dtype=torch.float32, device="cuda")
+        xb = torch.from_numpy(np.ascontiguousarray(x_base, np.float64)).cuda()
+        ident = torch.from_numpy((p.base_row_mode == packing.FIXED_VARIABLE).astype(np.uint8)).cuda()
+        tgt = torch.from_numpy(np.ascontiguousarray(p.target, np.float64)).cuda()
+        x0 = torch.empty((ns, p.n), dtype=torch.float64, device="cuda") if out is None else out
         for a in range(0, ns, chunk):
             b = min(ns, a + chunk)
             o = outs[a:b].contiguous()
-            x0 = self._batch_inputs(xf, fl, o)
-            out = self.net.forward(x0, o)
-            res[a:b] = out[:, :2].reshape(b - a, nb, 2)
-        d = res.cpu().numpy().astype(np.float64) * self.tgt_std
-        x0 = np.tile(x_base, (ns, 1))
-        x0[:, 1::2] += d[:, :, 0]
-        x0[:, 0::2] += d[:, :, 1]
-        ident = p.base_row_mode == packing.FIXED_VARIABLE
-        x0[:, ident] = p.target[ident]
+            pred = self.net.forward(self._batch_inputs(xf, fl, o), o)
+            _call("olfgpu_gnn_compose_start", b - a, nb, _ptr(pred), pred.shape[1], float(self.tgt_std[0]),
+                  float(self.tgt_std[1]), _ptr(xb), _ptr(ident), _ptr(tgt), _ptr(x0[a:b]), _stream())
         return x0
+
+    def predict(self, p, x_base: np.ndarray, outages: np.ndarray, chunk: int = 128):
+        """Start states [nS, n] (float64, on the host) for the outages, from the base case state."""
+        return self.predict_device(p, x_base, outages, chunk).cpu().numpy()
 
     def save(self, path: str):
         self.net.save(path, {"feat_mean": self.feat_mean, "feat_std": self.feat_std, "tgt_std": self.tgt_std,
@@ -269,14 +272,25 @@ def fingerprint(grid) -> np.ndarray:
                      float(np.sum(grid.x)), float(grid.scale)])
 
 
-def solve_with_fallback(ctx, p, x0_learned: np.ndarray, x_base: np.ndarray, disabled: np.ndarray, **kw):
-    """Solve from the learned starts; a scenario that diverges, reaches the iteration cap or fails its linear solve
-    restarts once from the base start inside the same batch (the engine's fallback start).  Returns (results, total
-    Newton iterations per scenario, indices of the scenarios that fell back)."""
+def solve_with_fallback(ctx, p, x0_learned, x_base: np.ndarray, disabled: np.ndarray, **kw):
+    """Solve from the learned starts (a host array [nS, n] or a CUDA tensor from predict_device).  Each scenario
+    keeps whichever of its learned start and the base start has the smaller initial mismatch, and a scenario that
+    diverges, reaches the iteration cap or fails its linear solve restarts once from the base start, inside the same
+    batch (the engine's fallback start).  Returns (results, total Newton iterations per scenario, indices of the
+    scenarios that used the base start)."""
+    on_device = hasattr(x0_learned, "data_ptr")
     ctx.set_fallback_start(True)
     try:
-        r = ctx.solve(x_base, p.target, p.base_row_mode, disabled, x0_full=x0_learned, **kw).copy()
+        if on_device:
+            import torch
+            torch.cuda.current_stream().synchronize()      # the prediction ran on torch's stream
+            ctx.set_device_start(x0_learned)
+            r = ctx.solve(x_base, p.target, p.base_row_mode, disabled, **kw).copy()
+        else:
+            r = ctx.solve(x_base, p.target, p.base_row_mode, disabled, x0_full=x0_learned, **kw).copy()
     finally:
         ctx.set_fallback_start(False)
+        if on_device:
+            ctx.set_device_start(None)
     _, _, tot = ctx.last_stats()
     return r, tot.copy(), ctx.last_fallbacks()

@@ -37,7 +37,8 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_get_schedule", "olfgpu_linear_solve_noalloc", "olfgpu_stage_batch_context",
            "olfgpu_create_multi_context", "olfgpu_destroy_multi_context", "olfgpu_set_multi_schedule",
            "olfgpu_get_multi_schedule", "olfgpu_solve_multi_context", "olfgpu_set_fallback_start",
-           "olfgpu_last_fallbacks", "olfgpu_set_phase_timing", "olfgpu_last_phase_times", "olfgpu_structure_levels"]
+           "olfgpu_last_fallbacks", "olfgpu_set_phase_timing", "olfgpu_last_phase_times", "olfgpu_structure_levels",
+           "olfgpu_set_device_start"]
 # Schedules of the Newton iterations
 LEVELS, PERSISTENT, AUTOTUNE = 0, 1, -1
 
@@ -81,6 +82,7 @@ def load(path: str = LIB_PATH):
     L.olfgpu_set_phase_timing.argtypes = [_i64, ctypes.c_int]
     L.olfgpu_last_phase_times.argtypes = [_i64, _dp]
     L.olfgpu_set_fallback_start.argtypes = [_i64, ctypes.c_int]
+    L.olfgpu_set_device_start.argtypes = [_i64, ctypes.c_void_p]
     L.olfgpu_last_fallbacks.argtypes = [_i64, _u8p, _ip]
     L.olfgpu_last_solve_stats.argtypes = [_i64, _fp, _ip, _ip]
     L.olfgpu_debug_fill.argtypes = [_i64, _dp, _dp, _ip, _u8p, _dp, _dp]
@@ -285,6 +287,13 @@ class BatchContext:
         d["iterations"] = int(o[6])
         d["factorized_lanes"] = int(o[7])
         return d
+
+    def set_device_start(self, x0_full_device=None):
+        """Per-scenario start states from a device array [nS, n] float64 (a torch CUDA tensor) for the following
+        solves; None switches back to the host x0_full argument.  Keep the tensor alive while it is set."""
+        ptr = None if x0_full_device is None else ctypes.c_void_p(x0_full_device.data_ptr())
+        self._device_start = x0_full_device
+        _check(load().olfgpu_set_device_start(self.handle, ptr))
 
     def set_fallback_start(self, enable: bool = True):
         """Scenarios that fail from x0_full restart once from x0_base inside the same solve."""
