@@ -30,6 +30,7 @@ METRIC = "N-1 solves/s (9k-bus, 500 outages) learned+mixed vs plain FP64 NR at 1
 GRID = "grid9241"
 N_OUTAGES = 500
 TOL = 1e-8
+CHECKPOINT = os.path.join(ROOT, "olf-gpu_b200", "checkpoints", "warmstart_grid9241.npz")
 # DRAM bytes (read + write) of one lane's factorization, from an ncu capture of every factorization launch of a
 # small batch (the capture's total over its factorized lanes); scaled to a launch by the lanes it factorizes
 TRAFFIC = {"fp64": None, "mixed": None}
@@ -125,8 +126,26 @@ def run_engine(args, rank: int, world: int):
     tgt = torch.from_numpy(p.target.copy()).pin_memory().numpy()
     mode = torch.from_numpy(p.base_row_mode.astype(np.int32)).pin_memory().numpy()
 
+    learned = None
+    if args.start == "learned":
+        from olfgpu.learned_start import LearnedStart
+        learned = LearnedStart.load(args.checkpoint, g)
+        x0_dev = torch.empty((ns, p.n), dtype=torch.float64, device="cuda")
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx.set_fallback_start(True)           # per lane: the better start by initial mismatch, restart on failure
+        ctx.set_device_start(x0_dev)
+
     def step():
+        """One batch; returns the device milliseconds of the learned-start prediction (0 with the base start)."""
+        pred_ms = 0.0
+        if learned is not None:
+            ev0.record()
+            learned.predict_device(p, x0, outs, out=x0_dev)
+            ev1.record()
+            ev1.synchronize()
+            pred_ms = ev0.elapsed_time(ev1)
         ctx.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
+        return pred_ms
 
     for _ in range(args.warmup):
         step()
@@ -139,14 +158,17 @@ def run_engine(args, rank: int, world: int):
         import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
+    pred_total = 0.0
     with sampler:
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            step()
+            pred_ms = step()
             wall_ms.append((time.perf_counter() - t0) * 1e3)
             ms, batched, tot = ctx.last_stats()
-            dev_ms.append(ms)
+            dev_ms.append(ms + pred_ms)
+            pred_total += pred_ms
             tot_iters += int(tot.sum())
+    fallbacks = int(ctx.last_fallbacks().size) if learned is not None else 0
     torch.cuda.synchronize()
     dev = float(np.mean(dev_ms))
     e2e = float(np.mean(wall_ms))
@@ -155,6 +177,18 @@ def run_engine(args, rank: int, world: int):
         t = torch.tensor([dev, e2e], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev, e2e = float(t[0]), float(t[1])
+    # the plain FP64 engine from the base start on the same batch (the comparison the metric names)
+    plain = None
+    if not args.no_plain:
+        ctx64 = native.BatchContext(s, ns)
+        for _ in range(args.warmup):
+            ctx64.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
+        pm = []
+        for _ in range(args.steps):
+            ctx64.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
+            pm.append(ctx64.last_stats()[0])
+        plain = {"solves_per_s": round(ns / (float(np.mean(pm)) * 1e-3), 1), "ms_per_step": round(float(np.mean(pm)), 4)}
+        ctx64.close()
     # roofline of the Newton iterations (HBM-bound): algorithmic bytes over the device time
     peak, peak_kind = _peaks()
     pbytes = 4 if precision == native.MIXED else 8
@@ -177,6 +211,8 @@ def run_engine(args, rank: int, world: int):
         traffic = int(traffic * ph["factorized_lanes"] / max(ph["iterations"], 1))
     words = (ns + 31) // 32
     h2d = p.n * 8 * 2 + p.n * 4 + p.n_elements * words * 4
+    if learned is not None:   # node features, branch flows, outage indices, base state / identity rows / targets
+        h2d += p.n_bus * 16 * 4 + p.n_cb * 2 * 4 + ns * 4 + p.n * (8 + 1 + 8)
     d2h = ns * (p.n + 3) * 8
     conv = float((statuses == 0).mean())
     line = {
@@ -192,11 +228,13 @@ def run_engine(args, rank: int, world: int):
         "vs_baseline": None,
         "dtype": "fp32-lu+fp64" if precision == native.MIXED else "f64",
         "data": "synthetic (seeded 9,241-bus grid, random non-bridge branch outages)",
-        "config": {"workload": f"{GRID}: 9,241 buses, {p.n_cb} branches, {ns} outages per GPU, warm start "
-                               f"from the base case, tol {TOL} pu, FP32 LU + {refinement} FP64 refinement step(s)"
-                   if precision == native.MIXED else
-                   f"{GRID}: 9,241 buses, {p.n_cb} branches, {ns} outages per GPU, warm start, tol {TOL} pu, "
-                   f"FP64 LU",
+        "config": {"workload": f"{GRID}: 9,241 buses, {p.n_cb} branches, {ns} outages per GPU, "
+                               + ("learned warm start (GNN prediction inside the step, per-lane choice against the "
+                                  "base start, fallback to the base start)" if learned is not None else
+                                  "warm start from the base case")
+                               + f", tol {TOL} pu, "
+                               + (f"FP32 LU + {refinement} FP64 refinement step(s)" if precision == native.MIXED
+                                  else "FP64 LU"),
                    "precision": args.precision, "l2": "working set > 1 GB per step, larger than the 126 MB L2",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "e2e": {"value": round(world * ns / (e2e * 1e-3), 1), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
@@ -213,6 +251,11 @@ def run_engine(args, rank: int, world: int):
                                         "scenario-iteration over the step's device time"},
         "phase_ms": {k: round(v, 3) for k, v in ph.items() if isinstance(v, float)},
         "gpu_launches": None,
+        "start": args.start,
+        "plain_fp64_base_start": plain,
+        "learned_start": None if learned is None else {
+            "checkpoint": os.path.relpath(args.checkpoint, ROOT), "prediction_ms_per_step": round(pred_total / args.steps, 4),
+            "scenarios_on_base_start": fallbacks},
         "iterations_per_solve": round(tot_iters / args.steps / ns, 3),
         "converged_fraction": round(conv, 4),
         "structure": {"n": s.n, "nnzJ": s.nnz, "nnzLU": s.n_lu_blocks * 4, "factor_levels": s.factor_levels,
@@ -423,11 +466,17 @@ def main():
     ap.add_argument("--refinement", type=int, default=1)
     ap.add_argument("--cpu-sample", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--start", default=None, choices=["base", "learned"],
+                    help="start states: the base case, or the learned warm start (default when its checkpoint exists)")
+    ap.add_argument("--checkpoint", default=CHECKPOINT)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--outages", type=int, default=N_OUTAGES,
                     help="outages per GPU (500 is the benchmark; smaller batches are profiling cases)")
     ap.add_argument("--workload", default="n1", choices=["n1", "uneven"],
                     help="n1: the 9,241-bus N-1 batch (default); uneven: four grids in one persistent launch")
     args = ap.parse_args()
+    if args.start is None:
+        args.start = "learned" if os.path.exists(args.checkpoint) and args.outages == N_OUTAGES else "base"
     args.warmup = max(args.warmup, 3) if args.impl == "engine" else args.warmup
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -153,7 +153,7 @@ def test_learned_start_trains_and_predicts_closer_starts(engine_lib, oracle_mod)
     after, _ = ls.evaluate(data, held)
     print(f"held-out normalised start error: base start {base_err:.4f}, untrained {before:.4f}, trained {after:.4f}")
     assert after < before and after < base_err
-    gs = g.scaled(1.03)
+    gs = g.scaled(0.97)
     ps = packing.pack(gs, with_reactive_limits=False)
     xb = ls.solve_base(gs, p.x_base)
     rng = np.random.default_rng(99)
