@@ -94,6 +94,19 @@ int olfgpu_destroy_batch_context(int64_t context);
 int olfgpu_set_linear_solver_settings(int64_t context, int precision, int refinementSteps);
 
 /*
+ * Mixed-precision controls (no counterpart in the reference; precision 1 only).  The refinement steps run only in
+ * iterations where some factorizing scenario's max |F| is below refineBelow (default 1e-3; infinity: every iteration):
+ * far from convergence the next Newton iteration corrects the FP32 solve's error itself.  A scenario whose FP32
+ * factorization meets a pivot block with growth above growthLimit (condition estimate max|D| max|inv D|, or max|D|
+ * over the largest entry of its Jacobian block; default 1e4) is flagged: in the level schedule its factorization and
+ * solve are redone in FP64 in the same iteration (and every later one of the solve); the persistent schedules give
+ * its tile the refinement steps instead.  olfgpu_last_fp64_refactors writes per scenario 1 where the last solve
+ * flagged it (flagged [nScenarios], may be null) and their count.
+ */
+int olfgpu_set_mixed_precision_controls(int64_t context, double refineBelow, double growthLimit);
+int olfgpu_last_fp64_refactors(int64_t context, unsigned char* flagged, int* count);
+
+/*
  * Schedule of the Newton iterations (no counterpart in the reference, which launches per dependency step and per
  * level and reads norms back every iteration): schedule 0 launches one kernel per wide dependency level over all
  * lanes and the narrow levels (<= 48 tasks) of each phase in one launch of tiles of lanesPerTile (1, 2 or 4; 0: one

@@ -288,6 +288,29 @@ extern "C" int olfgpu_last_phase_times(int64_t context, double* out8) {
     });
 }
 
+extern "C" int olfgpu_set_mixed_precision_controls(int64_t context, double refineBelow, double growthLimit) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        if (!(refineBelow > 0)) throw std::runtime_error("refineBelow must be positive (infinity: every iteration)");
+        if (!(growthLimit >= 1)) throw std::runtime_error("growthLimit must be >= 1 (infinity: never refactor)");
+        c.refineBelow = refineBelow;
+        c.growthLimit = growthLimit;
+    });
+}
+
+extern "C" int olfgpu_last_fp64_refactors(int64_t context, unsigned char* flagged, int* count) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        std::vector<unsigned char> f(c.nS);
+        OLF_CUDA(cudaSetDevice(c.device));
+        OLF_CUDA(cudaMemcpy(f.data(), c.precision64.p, c.nS, cudaMemcpyDeviceToHost));
+        int k = 0;
+        for (int i = 0; i < c.nS; i++) k += f[i] ? 1 : 0;
+        if (flagged) std::memcpy(flagged, f.data(), c.nS);
+        if (count) *count = k;
+    });
+}
+
 extern "C" int olfgpu_set_device_start(int64_t context, const double* x0FullDevice) {
     return guarded([&] {
         BatchContext& c = contextOf(context);

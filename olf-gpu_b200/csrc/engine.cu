@@ -2,6 +2,7 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -247,7 +248,10 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
 BatchContext::~BatchContext() {
     if (graph) cudaGraphExecDestroy(graph);
     if (graphSolve) cudaGraphExecDestroy(graphSolve);
+    for (cudaGraphExec_t gx : {graphFactor, graphRefine, graph64, graphStep})
+        if (gx) cudaGraphExecDestroy(gx);
     if (hostActive) cudaFreeHost(hostActive);
+    if (countReady) cudaEventDestroy(countReady);
     if (hostBitsPinned) cudaFreeHost(hostBitsPinned);
     if (stream) cudaStreamDestroy(stream);
 }
@@ -285,6 +289,8 @@ DevBatch BatchContext::batch() const {
     b.fallbackOn = fallbackStart && hasX0Base && hasX0Full ? 1 : 0;
     b.fallbackLeft = fallbackLeft.as<int8_t>();
     b.fellBack = fellBack.as<int8_t>();
+    b.growthLimit = growthLimit;
+    b.laneMask = nullptr;
     return b;
 }
 
@@ -305,7 +311,8 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
     ctx->S = (nScenarios + 31) / 32 * 32;
     const size_t S = ctx->S, n = s.n;
     OLF_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    OLF_CUDA(cudaMallocHost(&ctx->hostActive, 2 * sizeof(int)));
+    OLF_CUDA(cudaMallocHost(&ctx->hostActive, 4 * sizeof(int)));
+    OLF_CUDA(cudaEventCreateWithFlags(&ctx->countReady, cudaEventDisableTiming));
     ctx->x.alloc(n * S * 8);
     ctx->target.alloc(n * S * 8);
     ctx->mode.alloc(n * S);
@@ -329,7 +336,7 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
     ctx->precision64.alloc(S);
     ctx->fallbackLeft.alloc(S);
     ctx->fellBack.alloc(S);
-    ctx->nActive.alloc(8);
+    ctx->nActive.alloc(16);
     ctx->out.alloc(static_cast<size_t>(nScenarios) * (n + 3) * 8);
     ctx->stage.alloc(n * 8 * 2 + n * 4);
     ctx->cfg.maxIter = 15;
@@ -338,7 +345,8 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
     ctx->cfg.maxOuter = 20;
     ctx->cfg.maxSwitch = 3;
     ctx->cfg.refinementSteps = 1;
-    ctx->cfg.growthLimit = 1e8;
+    ctx->cfg.growthLimit = ctx->growthLimit;
+    ctx->cfg.refineBelow = ctx->refineBelow;
     if (nRl > 0) {
         for (int i = 0; i < nRl; i++) {
             if (voltageRow[i] < 0 || voltageRow[i] >= s.n) throw std::runtime_error("bad reactiveLimitVoltageRow");
@@ -534,18 +542,46 @@ void outageBits(BatchContext& ctx, const unsigned char* disabled, int nS, int nE
     OLF_CUDA(cudaMemcpyAsync(ctx.disabled.p, bits, count * 4, cudaMemcpyHostToDevice, ctx.stream));
 }
 
+namespace {
+
+cudaGraphExec_t captureInto(cudaStream_t st, const std::function<void()>& body) {
+    cudaGraph_t g;
+    cudaGraphExec_t x = nullptr;
+    OLF_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    body();
+    OLF_CUDA(cudaStreamEndCapture(st, &g));
+    OLF_CUDA(cudaGraphInstantiate(&x, g, 0));
+    cudaGraphDestroy(g);
+    return x;
+}
+
+void dropGraph(cudaGraphExec_t& g) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+}
+
+// The lanes flagged for an FP64 refactor (mixed precision), as a batch view whose LU kernels see only them.
+DevBatch fp64View(BatchContext& ctx) {
+    const size_t S = ctx.S;
+    if (!ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(ctx.net->dev->view.nLu) * 4 * S * 8);
+    DevBatch b = ctx.batch();
+    b.lu64 = ctx.lu64.as<double>();
+    b.laneMask = ctx.precision64.as<int8_t>();
+    return b;
+}
+
+}  // namespace
+
 void captureIteration(BatchContext& ctx) {
     const int key = ctx.narrowLanes * 100000 + ctx.precision * 1000 + ctx.refinementSteps * 10 +
                     (ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits ? 1 : 0);
     if (ctx.graph && ctx.graphKey == key) return;
-    if (ctx.graph) {
-        cudaGraphExecDestroy(ctx.graph);
-        ctx.graph = nullptr;
-    }
-    if (ctx.graphSolve) {
-        cudaGraphExecDestroy(ctx.graphSolve);
-        ctx.graphSolve = nullptr;
-    }
+    dropGraph(ctx.graph);
+    dropGraph(ctx.graphSolve);
+    dropGraph(ctx.graphFactor);
+    dropGraph(ctx.graphRefine);
+    dropGraph(ctx.graph64);
+    dropGraph(ctx.graphStep);
     const DeviceNet& dn = *ctx.net->dev;
     const DevNet& net = dn.view;
     const size_t S = ctx.S;
@@ -554,35 +590,60 @@ void captureIteration(BatchContext& ctx) {
     if (!mixed && !ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(net.nLu) * 4 * S * 8);
     const DevBatch b = ctx.batch();
     const bool rl = ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits;
-    // part 1: fill, test, reactive limits, count of the lanes that factorize
-    cudaGraph_t g;
-    OLF_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
-    launchIterationStart(b, ctx.stream);
-    launchFill(net, b, true, rl, ctx.stream);
-    launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, ctx.stream);
-    if (rl) launchReactiveLimits(net, b, ctx.rl, ctx.cfg, ctx.stream);
-    launchCountSolving(b, ctx.stream);
-    OLF_CUDA(cudaStreamEndCapture(ctx.stream, &g));
-    OLF_CUDA(cudaGraphInstantiate(&ctx.graph, g, 0));
-    cudaGraphDestroy(g);
-    // part 2: factorization, solves, refinement, step
-    OLF_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
+    cudaStream_t st = ctx.stream;
     const Hybrid hy = ctx.hybrid();
     const Hybrid* hp = ctx.narrowLanes > 0 ? &hy : nullptr;
-    launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, mixed, hp,
-                 ctx.stream);
-    launchSolve(net, b, dn.fwd(), dn.bwd(), mixed, false, hp, ctx.stream);
-    if (mixed) {
-        for (int k = 0; k < ctx.refinementSteps; k++) {
-            launchResidual(net, b, ctx.stream);
-            launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, ctx.stream);
+    const int nLevels = static_cast<int>(dn.levelPtr.size()) - 1;
+    // part 1: fill, test, reactive limits, lane counts
+    ctx.graph = captureInto(st, [&] {
+        launchIterationStart(b, st);
+        launchFill(net, b, true, rl, st);
+        launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, st);
+        if (rl) launchReactiveLimits(net, b, ctx.rl, ctx.cfg, st);
+        launchCountSolving(b, mixed ? ctx.cfg.refineBelow : -1.0, st);
+    });
+    if (!mixed) {
+        // part 2 (FP64): factorization, solves, step
+        ctx.graphSolve = captureInto(st, [&] {
+            launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, false, hp, st);
+            launchSolve(net, b, dn.fwd(), dn.bwd(), false, false, hp, st);
+            launchStep(net, b, false, st);
+        });
+    } else {
+        ctx.graphFactor = captureInto(st, [&] {
+            launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, true, hp, st);
+            launchCountFp64(b, st);
+        });
+        ctx.graphSolve = captureInto(st, [&] { launchSolve(net, b, dn.fwd(), dn.bwd(), true, false, hp, st); });
+        if (ctx.refinementSteps > 0) {
+            ctx.graphRefine = captureInto(st, [&] {
+                for (int k = 0; k < ctx.refinementSteps; k++) {
+                    launchResidual(net, b, st);
+                    launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, st);
+                }
+            });
         }
+        ctx.graphStep = captureInto(st, [&] { launchStep(net, b, false, st); });
     }
-    launchStep(net, b, false, ctx.stream);
-    OLF_CUDA(cudaStreamEndCapture(ctx.stream, &g));
-    OLF_CUDA(cudaGraphInstantiate(&ctx.graphSolve, g, 0));
-    cudaGraphDestroy(g);
     ctx.graphKey = key;
+}
+
+// Mixed precision: the FP64 refactor and solve of the flagged lanes (captured on first use: it allocates the FP64
+// factors).
+void launchFp64Redo(BatchContext& ctx) {
+    if (!ctx.graph64) {
+        const DeviceNet& dn = *ctx.net->dev;
+        const DevBatch b64 = fp64View(ctx);
+        const Hybrid hy = ctx.hybrid();
+        const Hybrid* hp = ctx.narrowLanes > 0 ? &hy : nullptr;
+        cudaStream_t st = ctx.stream;
+        ctx.graph64 = captureInto(st, [&] {
+            launchFactor(dn.view, b64, dn.levelPtr.data(), dn.levelSplit.data(),
+                         static_cast<int>(dn.levelPtr.size()) - 1, false, hp, st);
+            launchSolve(dn.view, b64, dn.fwd(), dn.bwd(), false, false, hp, st);
+        });
+    }
+    OLF_CUDA(cudaGraphLaunch(ctx.graph64, ctx.stream));
 }
 
 // One Newton iteration launched phase by phase with CUDA events between the phases (the same kernels in the same
@@ -603,9 +664,9 @@ bool phaseTimedIteration(BatchContext& ctx) {
     OLF_CUDA(cudaEventRecord(ev[1], st));
     launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, st);
     if (rl) launchReactiveLimits(net, b, ctx.rl, ctx.cfg, st);
-    launchCountSolving(b, st);
+    launchCountSolving(b, mixed ? ctx.cfg.refineBelow : -1.0, st);
     OLF_CUDA(cudaEventRecord(ev[2], st));
-    OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 8, cudaMemcpyDeviceToHost, st));
+    OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 12, cudaMemcpyDeviceToHost, st));
     OLF_CUDA(cudaStreamSynchronize(st));
     float ms[6] = {0, 0, 0, 0, 0, 0};
     OLF_CUDA(cudaEventElapsedTime(&ms[0], ev[0], ev[1]));
@@ -615,16 +676,28 @@ bool phaseTimedIteration(BatchContext& ctx) {
     if (live && solving > 0) {
         const Hybrid hy = ctx.hybrid();
         const Hybrid* hp = ctx.narrowLanes > 0 ? &hy : nullptr;
+        const int nLevels = static_cast<int>(dn.levelPtr.size()) - 1;
         OLF_CUDA(cudaEventRecord(ev[2], st));
-        launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, mixed,
-                     hp, st);
+        launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, mixed, hp, st);
+        if (mixed) launchCountFp64(b, st);
         OLF_CUDA(cudaEventRecord(ev[3], st));
         launchSolve(net, b, dn.fwd(), dn.bwd(), mixed, false, hp, st);
         OLF_CUDA(cudaEventRecord(ev[4], st));
         if (mixed) {
-            for (int r = 0; r < ctx.refinementSteps; r++) {
-                launchResidual(net, b, st);
-                launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, st);
+            // refinement steps (in iterations with a lane below the threshold) and the FP64 refactor of flagged lanes
+            if (ctx.hostActive[2] > 0) {
+                for (int r = 0; r < ctx.refinementSteps; r++) {
+                    launchResidual(net, b, st);
+                    launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, st);
+                }
+            }
+            OLF_CUDA(cudaMemcpyAsync(ctx.hostActive + 3, static_cast<int*>(ctx.nActive.p) + 3, 4,
+                                     cudaMemcpyDeviceToHost, st));
+            OLF_CUDA(cudaStreamSynchronize(st));
+            if (ctx.hostActive[3] > 0) {
+                const DevBatch b64 = fp64View(ctx);
+                launchFactor(net, b64, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, false, hp, st);
+                launchSolve(net, b64, dn.fwd(), dn.bwd(), false, false, hp, st);
             }
         }
         OLF_CUDA(cudaEventRecord(ev[5], st));
@@ -773,14 +846,28 @@ int runIterations(BatchContext& ctx) {
             continue;
         }
         OLF_CUDA(cudaGraphLaunch(ctx.graph, st));
-        OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 8, cudaMemcpyDeviceToHost, st));
+        OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 12, cudaMemcpyDeviceToHost, st));
         OLF_CUDA(cudaStreamSynchronize(st));
         if (ctx.hostActive[0] <= 0) {
             k++;
             break;
         }
-        // no lane factorizes this iteration (only restarts pending): skip the factor / solve graph
-        if (ctx.hostActive[1] > 0) OLF_CUDA(cudaGraphLaunch(ctx.graphSolve, st));
+        // no lane factorizes this iteration (only restarts pending): skip the factor / solve graphs
+        if (ctx.hostActive[1] <= 0) continue;
+        if (!mixed) {
+            OLF_CUDA(cudaGraphLaunch(ctx.graphSolve, st));
+            continue;
+        }
+        // mixed: FP32 factorization, then (while the FP32 solves run) the count of lanes flagged for FP64
+        OLF_CUDA(cudaGraphLaunch(ctx.graphFactor, st));
+        OLF_CUDA(cudaMemcpyAsync(ctx.hostActive + 3, static_cast<int*>(ctx.nActive.p) + 3, 4, cudaMemcpyDeviceToHost,
+                                 st));
+        OLF_CUDA(cudaEventRecord(ctx.countReady, st));
+        OLF_CUDA(cudaGraphLaunch(ctx.graphSolve, st));
+        if (ctx.graphRefine && ctx.hostActive[2] > 0) OLF_CUDA(cudaGraphLaunch(ctx.graphRefine, st));
+        OLF_CUDA(cudaEventSynchronize(ctx.countReady));
+        if (ctx.hostActive[3] > 0) launchFp64Redo(ctx);
+        OLF_CUDA(cudaGraphLaunch(ctx.graphStep, st));
     }
     capKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(ctx.batch());
     return k;
@@ -877,6 +964,8 @@ void stageRequest(BatchContext& ctx, const SolveRequest& req) {
     cfg.reactiveLimits = ctx.rl.nRl > 0 ? 1 : 0;
     cfg.mixed = ctx.precision;
     cfg.refinementSteps = ctx.refinementSteps;
+    cfg.refineBelow = ctx.refineBelow;
+    cfg.growthLimit = ctx.growthLimit;
     if (std::memcmp(&cfg, &ctx.cfg, sizeof(Settings)) != 0 && ctx.graph) {
         // the level-launch graph bakes the settings in
         cudaGraphExecDestroy(ctx.graph);

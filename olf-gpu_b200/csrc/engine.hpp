@@ -153,11 +153,17 @@ struct BatchContext {
     // host staging (pinned) and the per-scenario start states
     uint32_t* hostBitsPinned = nullptr;
     DeviceBuffer full;
-    int* hostActive = nullptr;      // pinned
+    int* hostActive = nullptr;      // pinned [4]: lanes iterating, factorizing, to refine, flagged for FP64
+    cudaEvent_t countReady = nullptr;  // mixed: the FP64-flag count has reached the host
     // one Newton iteration as a CUDA graph (captured on first use per settings)
-    cudaGraphExec_t graph = nullptr;       // fill, test, reactive limits
-    cudaGraphExec_t graphSolve = nullptr;  // factorization, solves, refinement, step
+    cudaGraphExec_t graph = nullptr;       // fill, test, reactive limits, lane counts
+    cudaGraphExec_t graphSolve = nullptr;  // FP64: factorization, solves, step; mixed: FP32 solves
+    // mixed precision only: FP32 factorization + count of FP64-flagged lanes; refinement steps; the FP64 refactor and
+    // solve of the flagged lanes; the step
+    cudaGraphExec_t graphFactor = nullptr, graphRefine = nullptr, graph64 = nullptr, graphStep = nullptr;
     int graphKey = -1;
+    double refineBelow = 1e-3;      // mixed: refinement steps only in iterations where a lane's max |F| is below it
+    double growthLimit = 1e4;       // mixed: FP32 pivot growth above which a lane refactors in FP64
     // statistics of the last solve
     int lastIterations = 0;         // batched iterations run
     float lastMs = 0.f;

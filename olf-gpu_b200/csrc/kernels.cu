@@ -7,7 +7,9 @@ namespace olfb200 {
 
 namespace {
 
-__device__ __forceinline__ bool solving(const DevBatch& b, int s) { return b.active[s] && !b.pending[s]; }
+__device__ __forceinline__ bool solving(const DevBatch& b, int s) {
+    return b.active[s] && !b.pending[s] && (!b.laneMask || b.laneMask[s]);
+}
 
 // NaN-propagating running maximum of |v| (a NaN stays: it orders above +inf as unsigned bits).
 __device__ __forceinline__ double absMax(double m, double v) {
@@ -358,6 +360,18 @@ void launchReactiveLimits(const DevNet&, const DevBatch& b, const DevRl& rl, con
 // into L = L~ inv(D_k) for the triangular solves.  The updates come in ascending m (a fixed summation order).
 // A near-singular 2x2 pivot (|det| <= 1e-13 of its terms, lu_pivot.cuh:12-18) flags the lane.
 // ---------------------------------------------------------------------------------------------------------------
+// Mixed precision: flags the lane for an FP64 refactor when an FP32 pivot block D (inverse det^-1 adj D) is badly
+// conditioned (max|D| max|inv D|) or grew against its Jacobian block (max|D| / max|A_kk|) beyond growthLimit.
+template <typename T>
+__device__ __forceinline__ void pivotGrowth(const DevBatch& b, int s, T a00, T a01, T a10, T a11, T inv, T amax) {
+    if (!b.precision64) return;     // a batch without per-lane precision flags (the allocation-free solve)
+    const float dmax = fmaxf(fmaxf(fabsf((float)a00), fabsf((float)a01)), fmaxf(fabsf((float)a10), fabsf((float)a11)));
+    const float imax = dmax * fabsf((float)inv);      // max |adj D| = max |D| for a 2x2 block
+    const float kappa = dmax * imax;
+    const float grow = amax > 0 ? dmax / (float)amax : 1.0f;
+    if (!(kappa <= (float)b.growthLimit) || !(grow <= (float)b.growthLimit)) b.precision64[s] = 1;
+}
+
 template <typename T>
 __device__ __forceinline__ void load4(const T* base, size_t blk, size_t S, int s, T& a, T& b_, T& c, T& d) {
     const T* p = base + blk * 4 * S + s;
@@ -395,7 +409,7 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
     const int s = blockIdx.y * 32 + lane;
     const int k = blockIdx.x * TPB + tib;
     const bool ok = k < count && s < b.S && solving(b, s);
-    T a00 = 0, a01 = 0, a10 = 0, a11 = 0;
+    T a00 = 0, a01 = 0, a10 = 0, a11 = 0, amax = 0;
     int t = 0;
     Task tk{};
     if (ok) {
@@ -407,8 +421,9 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
             a01 = (T)p[S];
             a10 = (T)p[2 * S];
             a11 = (T)p[3 * S];
+            amax = fmax(fmax(fabs(a00), fabs(a01)), fmax(fabs(a10), fabs(a11)));
         }
-#pragma unroll 2
+#pragma unroll 4
         for (int q = tk.opBegin + part; q < tk.opEnd; q += P) {
             const int4 op = net.ops[q];
             T l00, l01, l10, l11, d00, d01, d10, d11, u00, u01, u10, u11;
@@ -444,6 +459,7 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
         const T scale = fabs(a00 * a11) + fabs(a01 * a10);
         if (!(fabs(det) > (T)1e-13 * scale) || !isfinite(det)) b.trouble[s] = 1;
         const T inv = (T)1 / det;
+        if (sizeof(T) == 4) pivotGrowth(b, s, a00, a01, a10, a11, inv, amax);
         store4(lu, (size_t)t, S, s, a11 * inv, -a01 * inv, -a10 * inv, a00 * inv);
     } else {
         store4(lu, (size_t)t, S, s, a00, a01, a10, a11);
@@ -728,18 +744,42 @@ __global__ void releasePendingKernel(DevBatch b) {
     if (s < b.S) b.pending[s] = 0;
 }
 
-// After the test: how many lanes factorize this iteration (the host skips the factor/solve graph when none does).
-__global__ void countSolvingKernel(DevBatch b) {
-    __shared__ int part[32];
-    int c = 0;
-    for (int s = threadIdx.x; s < b.S; s += blockDim.x) c += (b.active[s] && !b.pending[s]) ? 1 : 0;
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+// After the test: how many lanes factorize this iteration (the host skips the factor/solve graph when none does) and
+// how many of those are close enough to convergence for the refinement steps (mode 0); or, after a mixed-precision
+// factorization, how many factorizing lanes are flagged for an FP64 refactor (mode 1).
+__global__ void countLanesKernel(DevBatch b, double refineBelow, int mode) {
+    __shared__ int part[2][32];
+    int c0 = 0, c1 = 0;
+    for (int s = threadIdx.x; s < b.S; s += blockDim.x) {
+        const bool sv = b.active[s] && !b.pending[s];
+        if (mode == 0) {
+            c0 += sv ? 1 : 0;
+            c1 += sv && b.normOut[s] < refineBelow ? 1 : 0;
+        } else {
+            c0 += sv && b.precision64[s] ? 1 : 0;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        c0 += __shfl_down_sync(0xffffffffu, c0, o);
+        c1 += __shfl_down_sync(0xffffffffu, c1, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        part[0][threadIdx.x >> 5] = c0;
+        part[1][threadIdx.x >> 5] = c1;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        int t = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
-        b.nActive[1] = t;
+        int t0 = 0, t1 = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            t0 += part[0][w];
+            t1 += part[1][w];
+        }
+        if (mode == 0) {
+            b.nActive[1] = t0;
+            b.nActive[2] = t1;
+        } else {
+            b.nActive[3] = t0;
+        }
     }
 }
 
@@ -747,7 +787,11 @@ void launchIterationStart(const DevBatch& b, cudaStream_t st) {
     releasePendingKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b);
 }
 
-void launchCountSolving(const DevBatch& b, cudaStream_t st) { countSolvingKernel<<<1, 1024, 0, st>>>(b); }
+void launchCountSolving(const DevBatch& b, double refineBelow, cudaStream_t st) {
+    countLanesKernel<<<1, 1024, 0, st>>>(b, refineBelow, 0);
+}
+
+void launchCountFp64(const DevBatch& b, cudaStream_t st) { countLanesKernel<<<1, 1024, 0, st>>>(b, 0.0, 1); }
 
 void launchStep(const DevNet& net, const DevBatch& b, bool, cudaStream_t st) {
     const size_t all = (size_t)net.n * b.S;
@@ -755,6 +799,5 @@ void launchStep(const DevNet& net, const DevBatch& b, bool, cudaStream_t st) {
     advanceKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b);
 }
 
-void launchGrowthCheck(const DevNet&, const DevBatch&, double, cudaStream_t) {}
 
 }  // namespace olfb200

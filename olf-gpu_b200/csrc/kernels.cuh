@@ -105,6 +105,10 @@ struct DevBatch {
     int fallbackOn;           // set fallbackLeft for every live lane at install
     int8_t* fallbackLeft;     // [S]
     int8_t* fellBack;         // [S]
+    // mixed precision: a FP32 pivot block whose growth (condition estimate max|D| max|inv D|, or max|D| / max|A_kk|)
+    // exceeds growthLimit flags its lane in precision64; laneMask (may be null) restricts the LU kernels to flagged lanes
+    double growthLimit;
+    const int8_t* laneMask;
 };
 
 // Reactive-limit entries (ReactiveLimitsPacker.java:76) and their per-lane state.
@@ -138,6 +142,7 @@ struct Settings {
     int mixed;                // 1: FP32 factorization and solves with FP64 refinement
     int refinementSteps;
     double growthLimit;       // pivot growth above which a mixed lane refactors in FP64
+    double refineBelow;       // refinement steps run in an iteration where a factorizing lane's max |F| is below it
 };
 
 // Kernel launchers (stream-ordered; all lanes of the batch).
@@ -187,8 +192,11 @@ void launchSolve(const DevNet& net, const DevBatch& b, const LevelSchedule& fwd,
                  bool fromResidual, const Hybrid* hybrid, cudaStream_t st);
 void launchResidual(const DevNet& net, const DevBatch& b, cudaStream_t st);
 void launchStep(const DevNet& net, const DevBatch& b, bool accumulate, cudaStream_t st);
-void launchGrowthCheck(const DevNet& net, const DevBatch& b, double limit, cudaStream_t st);
 void launchIterationStart(const DevBatch& b, cudaStream_t st);
-void launchCountSolving(const DevBatch& b, cudaStream_t st);
+// Lanes that factorize this iteration (nActive[1]) and, of those, lanes whose max |F| is below refineBelow
+// (nActive[2]).
+void launchCountSolving(const DevBatch& b, double refineBelow, cudaStream_t st);
+// Factorizing lanes flagged for an FP64 refactor (nActive[3]).
+void launchCountFp64(const DevBatch& b, cudaStream_t st);
 
 }  // namespace olfb200

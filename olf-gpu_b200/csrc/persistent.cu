@@ -51,14 +51,16 @@ struct TileState {
     int remainingPv[L];
     int any[L];
     int restart[L];      // failed this iteration and restarts from the fallback start
+    int refine;          // a factorizing lane of the tile is below the refinement threshold (or flagged)
     unsigned long long norm[L];
     int live;            // any lane of the tile still active
 };
 
-// The split factor of a level with `count` tasks whose longest update list is `longest`: how many slots share a task.
+// The split factor of a level with `count` tasks whose longest update list is `longest`: how many slots share a task
+// (a power of two, up to every slot of the tile for the one-task levels at the top of the elimination tree).
 __device__ __forceinline__ int splitFor(int count, int longest, int slots) {
     int P = 1;
-    while (P < 32 && count * (P * 2) <= slots && (longest + P - 1) / P > 2) P *= 2;
+    while (P < slots && count * (P * 2) <= slots && (longest + P - 1) / P > 2) P *= 2;
     return P;
 }
 
@@ -78,7 +80,7 @@ __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const 
         for (int base = 0; base < count; base += groups) {
             const int kk = base + slot / P;
             const bool ok = solve && kk < count;
-            T a00 = 0, a01 = 0, a10 = 0, a11 = 0;
+            T a00 = 0, a01 = 0, a10 = 0, a11 = 0, amax = 0;
             int t = 0;
             Task tk{};
             if (ok) {
@@ -90,8 +92,9 @@ __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const 
                     a01 = (T)p[S];
                     a10 = (T)p[2 * S];
                     a11 = (T)p[3 * S];
+                    amax = fmax(fmax(fabs(a00), fabs(a01)), fmax(fabs(a10), fabs(a11)));
                 }
-#pragma unroll 2
+#pragma unroll 4
                 for (int q = tk.opBegin + part; q < tk.opEnd; q += P) {
                     const int4 op = net.ops[q];
                     T l00, l01, l10, l11, d00, d01, d10, d11, u00, u01, u10, u11;
@@ -107,18 +110,26 @@ __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const 
                 }
             }
             if (P > 1) {
+                // the P partial sums of a task, added pairwise in a fixed tree order
                 red[slot][0][lane] = a00;
                 red[slot][1][lane] = a01;
                 red[slot][2][lane] = a10;
                 red[slot][3][lane] = a11;
                 __syncthreads();
-                if (part == 0) {
-                    for (int q = 1; q < P; q++) {
-                        a00 += red[slot + q][0][lane];
-                        a01 += red[slot + q][1][lane];
-                        a10 += red[slot + q][2][lane];
-                        a11 += red[slot + q][3][lane];
+                for (int wd = P >> 1; wd > 0; wd >>= 1) {
+                    if (part < wd) {
+                        red[slot][0][lane] += red[slot + wd][0][lane];
+                        red[slot][1][lane] += red[slot + wd][1][lane];
+                        red[slot][2][lane] += red[slot + wd][2][lane];
+                        red[slot][3][lane] += red[slot + wd][3][lane];
                     }
+                    __syncthreads();
+                }
+                if (part == 0) {
+                    a00 = red[slot][0][lane];
+                    a01 = red[slot][1][lane];
+                    a10 = red[slot][2][lane];
+                    a11 = red[slot][3][lane];
                 }
             }
             if (ok && part == 0) {
@@ -127,6 +138,14 @@ __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const 
                     const T scale = fabs(a00 * a11) + fabs(a01 * a10);
                     if (!(fabs(det) > (T)1e-13 * scale) || !isfinite(det)) *trouble = 1;
                     const T inv = (T)1 / det;
+                    if (sizeof(T) == 4 && b.precision64) {
+                        // the pivot-growth flag of the mixed precision (tile schedules answer it with refinement)
+                        const float dmax = fmaxf(fmaxf(fabsf((float)a00), fabsf((float)a01)),
+                                                 fmaxf(fabsf((float)a10), fabsf((float)a11)));
+                        const float kappa = dmax * dmax * fabsf((float)inv);
+                        const float grow = amax > 0 ? dmax / (float)amax : 1.0f;
+                        if (!(kappa <= (float)b.growthLimit) || !(grow <= (float)b.growthLimit)) b.precision64[s] = 1;
+                    }
                     st4(lu, (size_t)t, S, s, a11 * inv, -a01 * inv, -a10 * inv, a00 * inv);
                 } else {
                     st4(lu, (size_t)t, S, s, a00, a01, a10, a11);
@@ -195,11 +214,16 @@ __device__ void solveLevels(const DevNet& net, const DevBatch& b, const T* lu, T
                 red[slot][0][lane] = w0;
                 red[slot][1][lane] = w1;
                 __syncthreads();
-                if (part == 0) {
-                    for (int q = 1; q < P; q++) {
-                        w0 += red[slot + q][0][lane];
-                        w1 += red[slot + q][1][lane];
+                for (int wd = P >> 1; wd > 0; wd >>= 1) {
+                    if (part < wd) {
+                        red[slot][0][lane] += red[slot + wd][0][lane];
+                        red[slot][1][lane] += red[slot + wd][1][lane];
                     }
+                    __syncthreads();
+                }
+                if (part == 0) {
+                    w0 = red[slot][0][lane];
+                    w1 = red[slot][1][lane];
                 }
             }
             if (ok && part == 0) {
@@ -518,7 +542,14 @@ __device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl
             factorLevels<T, L>(net, b, lu, plan.levelPtr, plan.levelLongest, 0, plan.nLevels, solve, lane, slot, slots, s,
                                red, &ts.trouble[lane]);
             // ---------------- solves (one pass, then the refinement passes in mixed precision) ----------------
-            const int passes = 1 + (sizeof(T) == 4 ? cfg.refinementSteps : 0);
+            if (tid == 0) {
+                int r = 0;
+                for (int k = 0; k < L; k++)
+                    r |= ts.solving[k] && (b.normOut[s0 + k] < cfg.refineBelow || b.precision64[s0 + k]);
+                ts.refine = r;
+            }
+            __syncthreads();
+            const int passes = 1 + (sizeof(T) == 4 && ts.refine ? cfg.refinementSteps : 0);
             for (int pass = 0; pass < passes; pass++) {
                 if (pass > 0) {
                     // FP64 residual r = -F - J dx
@@ -645,7 +676,7 @@ __global__ void __launch_bounds__(512) factorRangeKernel(DevNet net, DevBatch b,
     const int tid = threadIdx.x, lane = tid % L, slot = tid / L, slots = blockDim.x / L;
     const int s = blockIdx.x * L + lane;
     T* lu = sizeof(T) == 8 ? reinterpret_cast<T*>(b.lu64) : reinterpret_cast<T*>(b.lu32);
-    const bool solve = b.active[s] && !b.pending[s];
+    const bool solve = b.active[s] && !b.pending[s] && (!b.laneMask || b.laneMask[s]);
     factorLevels<T, L>(net, b, lu, plan.levelPtr, plan.levelLongest, l0, l1, solve, lane, slot, slots, s, red,
                        &b.trouble[s]);
 }
@@ -659,7 +690,7 @@ __global__ void __launch_bounds__(512) solveRangeKernel(DevNet net, DevBatch b, 
     const int s = blockIdx.x * L + lane;
     const T* lu = sizeof(T) == 8 ? reinterpret_cast<const T*>(b.lu64) : reinterpret_cast<const T*>(b.lu32);
     T* w = sizeof(T) == 8 ? reinterpret_cast<T*>(b.w64) : reinterpret_cast<T*>(b.w32);
-    const bool solve = b.active[s] && !b.pending[s];
+    const bool solve = b.active[s] && !b.pending[s] && (!b.laneMask || b.laneMask[s]);
     if (dir == 0) {
         solveLevels<T, L>(net, b, lu, w, plan.fwdPtr, plan.fwdPos, plan.fwdLongest, 0, l0, l1, solve, lane, slot,
                           slots, s, red);

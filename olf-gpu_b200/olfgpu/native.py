@@ -38,7 +38,7 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_create_multi_context", "olfgpu_destroy_multi_context", "olfgpu_set_multi_schedule",
            "olfgpu_get_multi_schedule", "olfgpu_solve_multi_context", "olfgpu_set_fallback_start",
            "olfgpu_last_fallbacks", "olfgpu_set_phase_timing", "olfgpu_last_phase_times", "olfgpu_structure_levels",
-           "olfgpu_set_device_start"]
+           "olfgpu_set_device_start", "olfgpu_set_mixed_precision_controls", "olfgpu_last_fp64_refactors"]
 # Schedules of the Newton iterations
 LEVELS, PERSISTENT, AUTOTUNE = 0, 1, -1
 
@@ -83,6 +83,8 @@ def load(path: str = LIB_PATH):
     L.olfgpu_last_phase_times.argtypes = [_i64, _dp]
     L.olfgpu_set_fallback_start.argtypes = [_i64, ctypes.c_int]
     L.olfgpu_set_device_start.argtypes = [_i64, ctypes.c_void_p]
+    L.olfgpu_set_mixed_precision_controls.argtypes = [_i64, ctypes.c_double, ctypes.c_double]
+    L.olfgpu_last_fp64_refactors.argtypes = [_i64, _u8p, _ip]
     L.olfgpu_last_fallbacks.argtypes = [_i64, _u8p, _ip]
     L.olfgpu_last_solve_stats.argtypes = [_i64, _fp, _ip, _ip]
     L.olfgpu_debug_fill.argtypes = [_i64, _dp, _dp, _ip, _u8p, _dp, _dp]
@@ -287,6 +289,17 @@ class BatchContext:
         d["iterations"] = int(o[6])
         d["factorized_lanes"] = int(o[7])
         return d
+
+    def set_mixed_precision_controls(self, refine_below: float = 1e-3, growth_limit: float = 1e4):
+        """Mixed precision: refinement only below refine_below; FP64 refactor above growth_limit pivot growth."""
+        _check(load().olfgpu_set_mixed_precision_controls(self.handle, refine_below, growth_limit))
+
+    def last_fp64_refactors(self) -> np.ndarray:
+        """Indices of the scenarios whose last solve was flagged for FP64 refactors."""
+        f = np.zeros(self.n_scenarios, np.uint8)
+        k = ctypes.c_int(0)
+        _check(load().olfgpu_last_fp64_refactors(self.handle, _p(f), ctypes.byref(k)))
+        return np.flatnonzero(f)
 
     def set_device_start(self, x0_full_device=None):
         """Per-scenario start states from a device array [nS, n] float64 (a torch CUDA tensor) for the following

@@ -303,3 +303,41 @@ def test_phase_timing_reports_every_phase(engine_lib):
     assert np.array_equal(r, ref)        # same kernels, same order: the same bits
     assert ph["iterations"] >= 2 and ph["factor"] > 0 and ph["solve"] > 0 and ph["fill"] > 0
     assert ph["factorized_lanes"] >= outs.shape[0]
+
+
+def test_pivot_growth_refactors_in_fp64(engine_lib, oracle_mod):
+    """Mixed precision: with the growth limit at its minimum every lane's FP32 factorization is flagged and redone in
+    FP64 in the same iteration, which reproduces the FP64 engine bit for bit; with the default limit no lane of this
+    well-conditioned batch is flagged and the result matches the oracle."""
+    from olfgpu import native, synthetic
+    g, p = grid("grid2000")
+    outs = synthetic.draw_outages(g, 96, seed=91)
+    dis = p.outage_masks(outs)
+    s = native.Structure(p)
+    c64 = native.BatchContext(s, outs.shape[0])
+    r64 = c64.solve(p.x_base, p.target, p.base_row_mode, dis)
+    cm = native.BatchContext(s, outs.shape[0])
+    cm.set_linear_solver_settings(native.MIXED, 1)
+    cm.set_mixed_precision_controls(1e-3, 1.0)
+    rm = cm.solve(p.x_base, p.target, p.base_row_mode, dis)
+    assert cm.last_fp64_refactors().size == outs.shape[0]
+    assert np.array_equal(rm, r64)
+    cm.set_mixed_precision_controls(1e-3, 1e4)
+    rm = cm.solve(p.x_base, p.target, p.base_row_mode, dis)
+    assert cm.last_fp64_refactors().size == 0
+    _compare(rm, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n)
+
+
+@pytest.mark.parametrize("refine_below", [float("inf"), 1e-3, 1e-12])
+def test_adaptive_refinement_matches_oracle(engine_lib, oracle_mod, refine_below):
+    """Refinement in every iteration, near convergence only, or never: the same statuses and states."""
+    from olfgpu import native, synthetic
+    g, p = grid("grid2000")
+    outs = synthetic.draw_outages(g, 96, seed=92)
+    dis = p.outage_masks(outs)
+    s = native.Structure(p)
+    ctx = native.BatchContext(s, outs.shape[0])
+    ctx.set_linear_solver_settings(native.MIXED, 1)
+    ctx.set_mixed_precision_controls(refine_below, 1e4)
+    r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
+    _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n)
