@@ -119,6 +119,8 @@ def run_engine(args, rank: int, world: int):
     ns = outs.shape[0]
     ctx = native.BatchContext(s, ns)
     ctx.set_linear_solver_settings(precision, max(refinement, 0))
+    if args.schedule == "auto":
+        ctx.set_schedule(native.AUTOTUNE)           # the first (warm-up) solve times the candidates
     # host inputs in pinned memory (e2e copies them every step); results read back to pinned memory
     dis = torch.from_numpy(p.outage_masks(outs)).pin_memory().numpy()
     out = torch.empty((ns, p.n + 3), dtype=torch.float64).pin_memory().numpy()
@@ -181,6 +183,8 @@ def run_engine(args, rank: int, world: int):
     plain = None
     if not args.no_plain:
         ctx64 = native.BatchContext(s, ns)
+        if args.schedule == "auto":
+            ctx64.set_schedule(native.AUTOTUNE)
         for _ in range(args.warmup):
             ctx64.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
         pm = []
@@ -209,6 +213,12 @@ def run_engine(args, rank: int, world: int):
     traffic = TRAFFIC.get(args.precision)
     if traffic is not None:
         traffic = int(traffic * ph["factorized_lanes"] / max(ph["iterations"], 1))
+    fact_kernel = ("block-LU factorization of one Newton iteration (factorLevelKernel levels + factorRangeKernel "
+                   "narrow levels)")
+    if ph["iterations"] == 0:
+        # the autotuner picked the persistent schedule: one launch runs the whole Newton loop of the batch
+        fact_kernel = "newtonPersistentKernel (the whole Newton loop of the batch in one launch)"
+        fact_achieved, fact_launch_ms, fact_bytes_launch, traffic = achieved, dev, total_bytes, None
     words = (ns + 31) // 32
     h2d = p.n * 8 * 2 + p.n * 4 + p.n_elements * words * 4
     if learned is not None:   # node features, branch flows, outage indices, base state / identity rows / targets
@@ -241,8 +251,7 @@ def run_engine(args, rank: int, world: int):
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": round(fact_achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(fact_achieved / peak, 4), "traffic": traffic,
-                     "kernel": "block-LU factorization of one Newton iteration (factorLevelKernel levels + "
-                               "factorRangeKernel narrow levels)",
+                     "kernel": fact_kernel,
                      "algorithmic_bytes_per_launch": int(fact_bytes_launch), "launch_ms": round(fact_launch_ms, 4),
                      "unit_bytes": "8 nnzJ + 2 w nnzLU per factorized lane",
                      "peak_source": f"{peak_kind} copy bandwidth (hbm_gbs)"},
@@ -252,6 +261,7 @@ def run_engine(args, rank: int, world: int):
         "phase_ms": {k: round(v, 3) for k, v in ph.items() if isinstance(v, float)},
         "gpu_launches": None,
         "start": args.start,
+        "schedule": dict(zip(["schedule", "lanes_per_tile", "threads"], ctx.schedule()[0])),
         "plain_fp64_base_start": plain,
         "learned_start": None if learned is None else {
             "checkpoint": os.path.relpath(args.checkpoint, ROOT), "prediction_ms_per_step": round(pred_total / args.steps, 4),
@@ -470,6 +480,8 @@ def main():
                     help="start states: the base case, or the learned warm start (default when its checkpoint exists)")
     ap.add_argument("--checkpoint", default=CHECKPOINT)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--schedule", default="auto", choices=["auto", "levels"],
+                    help="auto: the engine's autotuner picks the Newton-iteration schedule on the first solve")
     ap.add_argument("--outages", type=int, default=N_OUTAGES,
                     help="outages per GPU (500 is the benchmark; smaller batches are profiling cases)")
     ap.add_argument("--workload", default="n1", choices=["n1", "uneven"],
