@@ -115,7 +115,7 @@ def run_engine(args, rank: int, world: int):
     g, p, outs = workload(rank, args.outages)
     precision = native.MIXED if args.precision == "mixed" else native.FP64
     refinement = args.refinement if precision == native.MIXED else 0
-    s = native.Structure(p)
+    s = native.Structure(p, native.PLAN_DEFERRED_L if args.plan == "deferred" else 0)
     ns = outs.shape[0]
     ctx = native.BatchContext(s, ns)
     ctx.set_linear_solver_settings(precision, max(refinement, 0))
@@ -261,6 +261,7 @@ def run_engine(args, rank: int, world: int):
         "phase_ms": {k: round(v, 3) for k, v in ph.items() if isinstance(v, float)},
         "gpu_launches": None,
         "start": args.start,
+        "lu_plan": args.plan,
         "schedule": dict(zip(["schedule", "lanes_per_tile", "threads"], ctx.schedule()[0])),
         "plain_fp64_base_start": plain,
         "learned_start": None if learned is None else {
@@ -334,7 +335,8 @@ def run_uneven(args, rank: int, world: int):
             wall.append((time.perf_counter() - t0) * 1e3)
         return float(np.mean(dev)), float(np.mean(wall))
 
-    ma = MultiGridAnalysis(packs, counts, precision=precision, schedule=-1)
+    ordering = native.PLAN_DEFERRED_L if args.plan == "deferred" else 0
+    ma = MultiGridAnalysis(packs, counts, precision=precision, schedule=-1, ordering=ordering)
     ma.solve(outs)                                     # autotunes on the first solve
     pick, tuning = ma.multi.schedule()
     last = {}
@@ -356,7 +358,7 @@ def run_uneven(args, rank: int, world: int):
     # one level-schedule batch per grid, back to back (each grid's own launches)
     seq = []
     for p, o in zip(packs, outs):
-        st = native.Structure(p)
+        st = native.Structure(p, ordering)
         c = native.BatchContext(st, o.shape[0], native.BATCHED_LU, p.rl)
         c.set_linear_solver_settings(precision, 1)
         seq.append((st, c, p, p.outage_masks(o)))
@@ -480,6 +482,8 @@ def main():
                     help="start states: the base case, or the learned warm start (default when its checkpoint exists)")
     ap.add_argument("--checkpoint", default=CHECKPOINT)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--plan", default="scaled", choices=["scaled", "deferred"],
+                    help="block-LU plan: L scaled at its task (default) or deferred (half the levels)")
     ap.add_argument("--schedule", default="auto", choices=["auto", "levels"],
                     help="auto: the engine's autotuner picks the Newton-iteration schedule on the first solve")
     ap.add_argument("--outages", type=int, default=N_OUTAGES,

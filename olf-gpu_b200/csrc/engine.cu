@@ -211,6 +211,7 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     v.nA = static_cast<int>(p.aCol.size());
     v.nLu = nLu;
     v.nU = p.nU;
+    v.deferredL = p.deferredL ? 1 : 0;
     v.ncb = s.ncb;
     v.nob = s.nob;
     v.nsh = s.nsh;

@@ -199,19 +199,23 @@ __global__ void messageForwardKernel(int B, int nb, const int* inPtr, const int*
     if (warp >= B * nb) return;
     const int b = warp / nb, i = warp % nb;
     const int f = 2 * lane;
-    const size_t qi = ((size_t)b * nb + i) * 128 + 64 + f;
-    const float q0 = __bfloat162float(PQ[qi]) + bmsg[f], q1 = __bfloat162float(PQ[qi + 1]) + bmsg[f + 1];
+    // each lane owns a feature pair: one 4-byte bf16x2 / 8-byte float2 access per row (a warp reads 128 / 256 bytes)
+    const float2 q = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(PQ + ((size_t)b * nb + i) * 128 + 64 + f));
+    const float2 bm = *reinterpret_cast<const float2*>(bmsg + f);
+    const float q0 = q.x + bm.x, q1 = q.y + bm.y;
     float a0 = 0.f, a1 = 0.f;
     const int out = outage[b];
-    for (int p = inPtr[i]; p < inPtr[i + 1]; p++) {
+    const int p1 = inPtr[i + 1];
+    for (int p = inPtr[i]; p < p1; p++) {
         const int e = inEdge[p];
         if (edgeBranch[e] == out) continue;
-        const size_t pj = ((size_t)b * nb + edgeSrc[e]) * 128 + f;
-        a0 += fmaxf(__bfloat162float(PQ[pj]) + q0 + C[(size_t)e * 64 + f], 0.f);
-        a1 += fmaxf(__bfloat162float(PQ[pj + 1]) + q1 + C[(size_t)e * 64 + f + 1], 0.f);
+        const float2 pj = __bfloat1622float2(
+            *reinterpret_cast<const __nv_bfloat162*>(PQ + ((size_t)b * nb + edgeSrc[e]) * 128 + f));
+        const float2 c = *reinterpret_cast<const float2*>(C + (size_t)e * 64 + f);
+        a0 += fmaxf(pj.x + q0 + c.x, 0.f);
+        a1 += fmaxf(pj.y + q1 + c.y, 0.f);
     }
-    agg[((size_t)b * nb + i) * 64 + f] = __float2bfloat16(a0);
-    agg[((size_t)b * nb + i) * 64 + f + 1] = __float2bfloat16(a1);
+    *reinterpret_cast<__nv_bfloat162*>(agg + ((size_t)b * nb + i) * 64 + f) = __floats2bfloat162_rn(a0, a1);
 }
 
 // Backward of the messages.  dQ[b, i] = sum over e into i of g_e; dP[b, j] = sum over e out of j of g_e, with

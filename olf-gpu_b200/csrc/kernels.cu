@@ -354,10 +354,11 @@ void launchReactiveLimits(const DevNet&, const DevBatch& b, const DevRl& rl, con
 
 // ---------------------------------------------------------------------------------------------------------------
 // Batched block LU, one level of tasks per launch: one thread per (LU block, lane).
-//   U(k, j) = A(k, j) - sum_m L~(k, m) inv(D_m) U(m, j);    L~(i, k) = A(i, k) - sum_m L~(i, m) inv(D_m) U(m, k)
-// with D_m = U(m, m), whose slot stores its inverse.  L~ is the unscaled L: it does not wait for its own column's
-// pivot, so the dependency chain is about one level per pivot instead of two; scaleLKernel finally turns every L~
-// into L = L~ inv(D_k) for the triangular solves.  The updates come in ascending m (a fixed summation order).
+//   U(k, j) = A(k, j) - sum_m L(k, m) U(m, j);    L(i, k) = (A(i, k) - sum_m L(i, m) U(m, k)) inv(D_k)
+// with D_m = U(m, m), whose slot stores its inverse.  Deferred-L plan: the L blocks stay unscaled (L~) during the
+// factorization and every update applies its pivot's inverse, L~(k, m) inv(D_m) U(m, j), so an L block does not wait
+// for its own column's pivot (about one level per pivot instead of two); scaleLKernel finally turns every L~ into L.
+// The updates come in ascending m (a fixed summation order).
 // A near-singular 2x2 pivot (|det| <= 1e-13 of its terms, lu_pivot.cuh:12-18) flags the lane.
 // ---------------------------------------------------------------------------------------------------------------
 // Mixed precision: flags the lane for an FP64 refactor when an FP32 pivot block D (inverse det^-1 adj D) is badly
@@ -426,12 +427,18 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
 #pragma unroll 4
         for (int q = tk.opBegin + part; q < tk.opEnd; q += P) {
             const int4 op = net.ops[q];
-            T l00, l01, l10, l11, d00, d01, d10, d11, u00, u01, u10, u11;
-            load4(lu, (size_t)op.x, S, s, l00, l01, l10, l11);
-            load4(lu, (size_t)op.z, S, s, d00, d01, d10, d11);
+            T m00, m01, m10, m11, u00, u01, u10, u11;
+            load4(lu, (size_t)op.x, S, s, m00, m01, m10, m11);
             load4(lu, (size_t)op.y, S, s, u00, u01, u10, u11);
-            const T m00 = l00 * d00 + l01 * d10, m01 = l00 * d01 + l01 * d11;
-            const T m10 = l10 * d00 + l11 * d10, m11 = l10 * d01 + l11 * d11;
+            if (op.z >= 0) {   // deferred-L plan: L~(a,m) inv(D_m)
+                T d00, d01, d10, d11;
+                load4(lu, (size_t)op.z, S, s, d00, d01, d10, d11);
+                const T l00 = m00, l01 = m01, l10 = m10, l11 = m11;
+                m00 = l00 * d00 + l01 * d10;
+                m01 = l00 * d01 + l01 * d11;
+                m10 = l10 * d00 + l11 * d10;
+                m11 = l10 * d01 + l11 * d11;
+            }
             a00 -= m00 * u00 + m01 * u10;
             a01 -= m00 * u01 + m01 * u11;
             a10 -= m10 * u00 + m11 * u10;
@@ -461,6 +468,12 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
         const T inv = (T)1 / det;
         if (sizeof(T) == 4) pivotGrowth(b, s, a00, a01, a10, a11, inv, amax);
         store4(lu, (size_t)t, S, s, a11 * inv, -a01 * inv, -a10 * inv, a00 * inv);
+    } else if (tk.diag >= 0 && !net.deferredL) {
+        // default plan: L(i,k) = (...) inv(D_k), the pivot inverted one level earlier
+        T i00, i01, i10, i11;
+        load4(lu, (size_t)tk.diag, S, s, i00, i01, i10, i11);
+        store4(lu, (size_t)t, S, s, a00 * i00 + a01 * i10, a00 * i01 + a01 * i11, a10 * i00 + a11 * i10,
+               a10 * i01 + a11 * i11);
     } else {
         store4(lu, (size_t)t, S, s, a00, a01, a10, a11);
     }
@@ -518,7 +531,7 @@ void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtr, con
     if (hybrid) {
         // the range kernel ends with the L scaling pass of its tiles
         launchFactorRange(net, b, hybrid->plan, wide, nLevels, hybrid->lanes, fp32, st);
-    } else {
+    } else if (net.deferredL) {
         const int nL = net.nLu - net.nU;
         dim3 blk(32, 8), grd((nL + 7) / 8, b.S / 32);
         if (fp32) {

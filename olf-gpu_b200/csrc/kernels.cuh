@@ -44,6 +44,7 @@ struct Task {
 // Everything the kernels read about one network (device pointers), built once per structure.
 struct DevNet {
     int n, nb, nA, nLu, nU, ncb, nob, nsh, nElements;
+    int deferredL;            // 1: the L factor is kept unscaled during the factorization (see structure.hpp)
     const int* nodeCol;       // [2 nb]
     const int* sidePtr;       // [nb + 1]
     const Side* side;         // incident closed-branch sides
@@ -60,7 +61,7 @@ struct DevNet {
     const double* obPar;      // [nob * 7] y ksi g1 b1 g2 b2 r1
     // LU
     const Task* task;         // [nLu]
-    const int4* ops;          // updates (unscaled L block, U block, the pivot's inverted diagonal block, unused)
+    const int4* ops;          // updates (L block, U block, the pivot's inverted diagonal block or -1, unused)
     const int* levelTask;     // tasks grouped by level
     const int* perm;          // position -> node
     const int* iperm;         // node -> position

@@ -65,8 +65,8 @@ __device__ __forceinline__ int splitFor(int count, int longest, int slots) {
 }
 
 // Factorization levels [l0, l1) of one tile, l1 being the last level: tasks of a level shared by P slots each
-// (splitFor), partial sums added in a fixed order through shared memory; then the pass that scales every unscaled L
-// block by its pivot's inverse.  `trouble` receives 1 for a lane that meets a near-singular 2x2 pivot.
+// (splitFor), partial sums added in a fixed order through shared memory; with the deferred-L plan, then the pass that
+// scales every unscaled L block by its pivot's inverse.  `trouble` receives 1 for a lane that meets a near-singular 2x2 pivot.
 template <typename T, int L>
 __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const int* levelPtr, const int* longest,
                              int l0, int l1, bool solve, int lane, int slot, int slots, int s, T (*red)[4][L],
@@ -97,12 +97,18 @@ __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const 
 #pragma unroll 4
                 for (int q = tk.opBegin + part; q < tk.opEnd; q += P) {
                     const int4 op = net.ops[q];
-                    T l00, l01, l10, l11, d00, d01, d10, d11, u00, u01, u10, u11;
-                    ld4(lu, (size_t)op.x, S, s, l00, l01, l10, l11);
-                    ld4(lu, (size_t)op.z, S, s, d00, d01, d10, d11);
+                    T m00, m01, m10, m11, u00, u01, u10, u11;
+                    ld4(lu, (size_t)op.x, S, s, m00, m01, m10, m11);
                     ld4(lu, (size_t)op.y, S, s, u00, u01, u10, u11);
-                    const T m00 = l00 * d00 + l01 * d10, m01 = l00 * d01 + l01 * d11;
-                    const T m10 = l10 * d00 + l11 * d10, m11 = l10 * d01 + l11 * d11;
+                    if (op.z >= 0) {   // deferred-L plan: L~(a,m) inv(D_m)
+                        T d00, d01, d10, d11;
+                        ld4(lu, (size_t)op.z, S, s, d00, d01, d10, d11);
+                        const T l00 = m00, l01 = m01, l10 = m10, l11 = m11;
+                        m00 = l00 * d00 + l01 * d10;
+                        m01 = l00 * d01 + l01 * d11;
+                        m10 = l10 * d00 + l11 * d10;
+                        m11 = l10 * d01 + l11 * d11;
+                    }
                     a00 -= m00 * u00 + m01 * u10;
                     a01 -= m00 * u01 + m01 * u11;
                     a10 -= m10 * u00 + m11 * u10;
@@ -147,6 +153,11 @@ __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const 
                         if (!(kappa <= (float)b.growthLimit) || !(grow <= (float)b.growthLimit)) b.precision64[s] = 1;
                     }
                     st4(lu, (size_t)t, S, s, a11 * inv, -a01 * inv, -a10 * inv, a00 * inv);
+                } else if (tk.diag >= 0 && !net.deferredL) {
+                    T i00, i01, i10, i11;
+                    ld4(lu, (size_t)tk.diag, S, s, i00, i01, i10, i11);
+                    st4(lu, (size_t)t, S, s, a00 * i00 + a01 * i10, a00 * i01 + a01 * i11, a10 * i00 + a11 * i10,
+                        a10 * i01 + a11 * i11);
                 } else {
                     st4(lu, (size_t)t, S, s, a00, a01, a10, a11);
                 }
@@ -155,7 +166,7 @@ __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const 
         }
         __syncthreads();
     }
-    if (solve) {
+    if (solve && net.deferredL) {
         for (int id = net.nU + slot; id < net.nLu; id += slots) {
             T a00, a01, a10, a11, i00, i01, i10, i11;
             ld4(lu, (size_t)id, S, s, a00, a01, a10, a11);

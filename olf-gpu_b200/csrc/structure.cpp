@@ -528,6 +528,8 @@ void buildBlockPlan(Structure& s, int ordering) {
         }
         p.aPtr[a + 1] = static_cast<int>(p.aCol.size());
     }
+    p.deferredL = (ordering & PLAN_DEFERRED_L) != 0;
+    ordering &= ~PLAN_DEFERRED_L;
     // ordering
     if (ordering == ORDER_NATURAL) {
         p.perm.resize(nb);
@@ -633,7 +635,7 @@ void buildBlockPlan(Structure& s, int ordering) {
                 int q = fillPos[id]++;
                 p.opL[q] = la;
                 p.opU[q] = uBlock(m, b);
-                p.opD[q] = p.uPtr[m];
+                p.opD[q] = p.deferredL ? p.uPtr[m] : -1;
             }
         }
     }
@@ -641,17 +643,19 @@ void buildBlockPlan(Structure& s, int ordering) {
     // unscaled L blocks do not wait for their own column's pivot, which halves the dependency chain
     p.level.assign(nLu, 0);
     int maxLevel = 0;
-    auto levelOf = [&](int id) {
-        int lv = 0;
+    auto levelOf = [&](int id, int lv) {
         for (int q = p.opPtr[id]; q < p.opPtr[id + 1]; q++) {
-            lv = std::max(lv, std::max(std::max(p.level[p.opL[q]], p.level[p.opU[q]]), p.level[p.opD[q]]) + 1);
+            int dep = std::max(p.level[p.opL[q]], p.level[p.opU[q]]);
+            if (p.opD[q] >= 0) dep = std::max(dep, p.level[p.opD[q]]);
+            lv = std::max(lv, dep + 1);
         }
         p.level[id] = lv;
         maxLevel = std::max(maxLevel, lv);
     };
     for (int k = 0; k < nb; k++) {
-        for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) levelOf(t);
-        for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++) levelOf(p.nU + t);
+        for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) levelOf(t, 0);
+        // a scaled L block waits for its column's pivot
+        for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++) levelOf(p.nU + t, p.deferredL ? 0 : p.level[p.uPtr[k]] + 1);
     }
     p.levelPtr.assign(maxLevel + 2, 0);
     for (int id = 0; id < nLu; id++) p.levelPtr[p.level[id] + 1]++;

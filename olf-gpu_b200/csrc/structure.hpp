@@ -33,10 +33,12 @@ struct BlockPlan {
     std::vector<int> aToLu;       // A block id -> LU block id
     std::vector<int> luToA;       // LU block id -> A block id or -1 (pure fill-in)
     // Factorization: one task per LU block; its updates (L block, U block, the pivot's diagonal block) in ascending
-    // pivot order; its level.  L blocks are computed unscaled (A(i,k) - sum L~(i,m) inv(D_m) U(m,k)), so an update
-    // applies the pivot's inverted diagonal itself and an L block does not wait for its own column's pivot; one last
-    // pass scales every L block by its pivot's inverse.
-    std::vector<int> opPtr, opL, opU, opD;   // per LU block
+    // pivot order; its level.  Default plan: L(i,k) = (A(i,k) - sum L(i,m) U(m,k)) inv(D_k) when its task runs, one
+    // level after the pivot D_k.  Deferred-L plan: L blocks are computed unscaled (A(i,k) - sum L~(i,m) inv(D_m)
+    // U(m,k)), so an update applies the pivot's inverted diagonal itself and an L block does not wait for its own
+    // column's pivot; one last pass scales every L block by its pivot's inverse.
+    std::vector<int> opPtr, opL, opU, opD;   // per LU block (opD -1: the L block is already scaled)
+    bool deferredL = false;
     std::vector<int> level;             // per LU block
     std::vector<int> levelPtr, levelTask;  // tasks grouped by level (CSR); tasks are LU block ids
     // Triangular solves: forward over positions in L, backward in U; level sets of positions.
@@ -62,8 +64,10 @@ Structure buildStructure(int n, int ncb, const double* cbPar, const int* cbIx, i
                          const int* obIx, int nsh, const double* shPar, const int* shIx, int nid, const int* idRows,
                          int ordering);
 
-// Orderings of the bus graph for the block LU.
+// Orderings of the bus graph for the block LU (low bits), and the plan variant flag: PLAN_DEFERRED_L keeps the L
+// factor unscaled during the factorization (half the dependency levels, one more block read per update).
 enum Ordering { ORDER_MIN_DEGREE = 0, ORDER_NESTED_DISSECTION = 1, ORDER_NATURAL = 2 };
+constexpr int PLAN_DEFERRED_L = 8;
 
 void buildBlockPlan(Structure& s, int ordering);
 

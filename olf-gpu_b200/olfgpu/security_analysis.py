@@ -109,10 +109,10 @@ class MultiGridAnalysis:
     (lanes per tile, threads, order)."""
 
     def __init__(self, packed_grids: Sequence[Packed], counts: Sequence[int], precision: int = native.FP64,
-                 refinement_steps: int = 1, reactive_limits: bool = True, schedule=-1):
+                 refinement_steps: int = 1, reactive_limits: bool = True, schedule=-1, ordering: int = 0):
         self.packed = list(packed_grids)
         self.counts = [int(c) for c in counts]
-        self.structures = [native.Structure(p) for p in self.packed]
+        self.structures = [native.Structure(p, ordering) for p in self.packed]
         self.contexts = []
         for p, s, c in zip(self.packed, self.structures, self.counts):
             ctx = native.BatchContext(s, c, native.BATCHED_LU, p.rl if reactive_limits and p.rl is not None else None)

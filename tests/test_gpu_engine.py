@@ -341,3 +341,21 @@ def test_adaptive_refinement_matches_oracle(engine_lib, oracle_mod, refine_below
     ctx.set_mixed_precision_controls(refine_below, 1e4)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
     _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n)
+
+
+@pytest.mark.parametrize("schedule,lanes,threads", [(0, 2, 256), (0, 0, 256), (1, 2, 256)])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_deferred_l_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes, threads, precision):
+    """The deferred-L block-LU plan (half the factorization levels) gives the oracle's states and statuses."""
+    from olfgpu import native, synthetic
+    g, p = grid("grid2000")
+    outs = synthetic.draw_outages(g, 120, seed=93)
+    dis = p.outage_masks(outs)
+    s = native.Structure(p, ordering=native.PLAN_DEFERRED_L)
+    base = native.Structure(p)
+    assert s.factor_levels < base.factor_levels
+    ctx = native.BatchContext(s, outs.shape[0])
+    ctx.set_linear_solver_settings(precision, 1)
+    ctx.set_schedule(schedule, lanes, threads)
+    r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
+    _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n)
