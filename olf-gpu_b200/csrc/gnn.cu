@@ -93,22 +93,16 @@ __global__ void __launch_bounds__(128) gemmKernel(int M, const __nv_bfloat16* __
                     v0 = fmaxf(v0, 0.f);
                     v1 = fmaxf(v1, 0.f);
                 }
-                if (saveZ) {
-                    saveZ[(size_t)r * N + c] = __float2bfloat16(v0);
-                    saveZ[(size_t)r * N + c + 1] = __float2bfloat16(v1);
-                }
+                // column pairs (c, c + 1): one 4-byte bf16x2 / 8-byte float2 access each
+                if (saveZ) *reinterpret_cast<__nv_bfloat162*>(saveZ + (size_t)r * N + c) = __floats2bfloat162_rn(v0, v1);
                 if (residual) {
-                    v0 += __bfloat162float(residual[(size_t)r * N + c]);
-                    v1 += __bfloat162float(residual[(size_t)r * N + c + 1]);
+                    const float2 rv =
+                        __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(residual + (size_t)r * N + c));
+                    v0 += rv.x;
+                    v1 += rv.y;
                 }
-                if (outB) {
-                    outB[(size_t)r * ldo + c] = __float2bfloat16(v0);
-                    outB[(size_t)r * ldo + c + 1] = __float2bfloat16(v1);
-                }
-                if (outF) {
-                    outF[(size_t)r * ldo + c] = v0;
-                    outF[(size_t)r * ldo + c + 1] = v1;
-                }
+                if (outB) *reinterpret_cast<__nv_bfloat162*>(outB + (size_t)r * ldo + c) = __floats2bfloat162_rn(v0, v1);
+                if (outF) *reinterpret_cast<float2*>(outF + (size_t)r * ldo + c) = make_float2(v0, v1);
             }
         }
     }
