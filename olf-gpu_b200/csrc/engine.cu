@@ -240,6 +240,9 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     v.uPtr = d->uPtr.as<int>();
     v.uCol = d->uCol.as<int>();
     OLF_CUDA(cudaDeviceSynchronize());
+    // the uploads above are pageable cudaMemcpy calls, whose DMA may still be in flight when they return; the
+    // contexts' non-blocking streams would not wait for it
+    OLF_CUDA(cudaDeviceSynchronize());
     return d;
 }
 
@@ -392,6 +395,7 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
         r.remainingPv = ctx->rlRemainingPv.as<int>();
         r.switched = ctx->rlSwitched.as<int>();
     }
+    OLF_CUDA(cudaDeviceSynchronize());   // the reactive-limit uploads (pageable) have landed
     return ctx.release();
 }
 
@@ -1189,7 +1193,8 @@ void debugFill(BatchContext& ctx, const double* xFull, const double* targetBase,
     cudaStream_t st = ctx.stream;
     DeviceBuffer full;
     full.alloc(static_cast<size_t>(ctx.nS) * n * 8);
-    OLF_CUDA(cudaMemcpy(full.p, xFull, static_cast<size_t>(ctx.nS) * n * 8, cudaMemcpyHostToDevice));
+    // stream-ordered: a pageable cudaMemcpy may return before its DMA lands, and ctx.stream does not wait for it
+    OLF_CUDA(cudaMemcpyAsync(full.p, xFull, static_cast<size_t>(ctx.nS) * n * 8, cudaMemcpyHostToDevice, st));
     dim3 blk(32, 8), grd((n + 31) / 32, (ctx.nS + 31) / 32);
     toLanesKernel<<<grd, blk, 0, st>>>(full.as<double>(), ctx.x.as<double>(), n, ctx.nS, ctx.S);
     double* stageT = ctx.stage.as<double>() + n;
@@ -1235,8 +1240,8 @@ void debugLinearSolve(BatchContext& ctx, const double* csrVals, const double* rh
         }
         for (int r = 0; r < n; r++) F[static_cast<size_t>(r) * S + sc] = -rhs[static_cast<size_t>(sc) * n + r];
     }
-    OLF_CUDA(cudaMemcpy(ctx.J.p, J.data(), ctx.J.bytes, cudaMemcpyHostToDevice));
-    OLF_CUDA(cudaMemcpy(ctx.F.p, F.data(), F.size() * 8, cudaMemcpyHostToDevice));
+    OLF_CUDA(cudaMemcpyAsync(ctx.J.p, J.data(), ctx.J.bytes, cudaMemcpyHostToDevice, ctx.stream));
+    OLF_CUDA(cudaMemcpyAsync(ctx.F.p, F.data(), F.size() * 8, cudaMemcpyHostToDevice, ctx.stream));
     const DevBatch b = ctx.batch();
     laneInitKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b);
     launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, fp32,
