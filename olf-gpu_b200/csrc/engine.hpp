@@ -162,7 +162,7 @@ struct BatchContext {
     // solve of the flagged lanes; the step
     cudaGraphExec_t graphFactor = nullptr, graphRefine = nullptr, graph64 = nullptr, graphStep = nullptr;
     int graphKey = -1;
-    double refineBelow = 1e-3;      // mixed: refinement steps only in iterations where a lane's max |F| is below it
+    double refineBelow = 1e-5;      // mixed: refinement steps only in iterations where a lane's max |F| is below it
     double growthLimit = 1e4;       // mixed: FP32 pivot growth above which a lane refactors in FP64
     // statistics of the last solve
     int lastIterations = 0;         // batched iterations run

@@ -292,7 +292,7 @@ class BatchContext:
         d["factorized_lanes"] = int(o[7])
         return d
 
-    def set_mixed_precision_controls(self, refine_below: float = 1e-3, growth_limit: float = 1e4):
+    def set_mixed_precision_controls(self, refine_below: float = 1e-5, growth_limit: float = 1e4):
         """Mixed precision: refinement only below refine_below; FP64 refactor above growth_limit pivot growth."""
         _check(load().olfgpu_set_mixed_precision_controls(self.handle, refine_below, growth_limit))
 
