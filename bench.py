@@ -130,37 +130,26 @@ def run_engine(args, rank: int, world: int):
     mode = torch.from_numpy(p.base_row_mode.astype(np.int32)).pin_memory().numpy()
 
     learned = None
-    state = {"k": 0}
     if args.start == "learned":
         from olfgpu.learned_start import LearnedStart
         learned = LearnedStart.load(args.checkpoint, g)
-        # double-buffered start states: the prediction for the next batch runs on its own stream while the engine
-        # solves the current one (the level launches leave most of the GPU idle)
-        x0_bufs = [torch.empty((ns, p.n), dtype=torch.float64, device="cuda") for _ in range(2)]
-        pred_stream = torch.cuda.Stream()
-        pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(2)]
+        x0_dev = torch.empty((ns, p.n), dtype=torch.float64, device="cuda")
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ctx.set_fallback_start(True)           # per lane: the better start by initial mismatch, restart on failure
-
-        def predict_into(k):
-            with torch.cuda.stream(pred_stream):
-                pev[k % 2][0].record(pred_stream)
-                learned.predict_device(p, x0, outs, out=x0_bufs[k % 2])
-                pev[k % 2][1].record(pred_stream)
-
-        predict_into(0)
+        ctx.set_device_start(x0_dev)
 
     def step():
-        """One batch; returns the device milliseconds of its learned-start prediction (0 with the base start)."""
-        if learned is None:
-            ctx.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
-            return 0.0
-        k = state["k"]
-        pev[k % 2][1].synchronize()            # this batch's start states are ready
-        ctx.set_device_start(x0_bufs[k % 2])
-        predict_into(k + 1)                    # the next batch's prediction overlaps this solve
+        """One batch: the learned-start prediction (on the device), then the solve; returns the prediction's device
+        milliseconds (0 with the base start)."""
+        pred_ms = 0.0
+        if learned is not None:
+            ev0.record()
+            learned.predict_device(p, x0, outs, out=x0_dev)
+            ev1.record()
+            ev1.synchronize()
+            pred_ms = ev0.elapsed_time(ev1)
         ctx.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
-        state["k"] = k + 1
-        return pev[k % 2][0].elapsed_time(pev[k % 2][1])
+        return pred_ms
 
     for _ in range(args.warmup):
         step()
@@ -174,8 +163,6 @@ def run_engine(args, rank: int, world: int):
         import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
-    span0, span1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    span0.record()
     pred_total = 0.0
     with sampler:
         for _ in range(args.steps):
@@ -183,14 +170,9 @@ def run_engine(args, rank: int, world: int):
             pred_ms = step()
             wall_ms.append((time.perf_counter() - t0) * 1e3)
             ms, batched, tot = ctx.last_stats()
-            dev_ms.append(ms)
+            dev_ms.append(ms + pred_ms)
             pred_total += pred_ms
             tot_iters += int(tot.sum())
-    torch.cuda.synchronize()
-    span1.record()
-    span1.synchronize()
-    if learned is not None:
-        dev_ms = [span0.elapsed_time(span1) / args.steps]
     fallbacks = int(ctx.last_fallbacks().size) if learned is not None else 0
     torch.cuda.synchronize()
     dev = float(np.mean(dev_ms))
@@ -260,9 +242,9 @@ def run_engine(args, rank: int, world: int):
         "dtype": "fp32-lu+fp64" if precision == native.MIXED else "f64",
         "data": "synthetic (seeded 9,241-bus grid, random non-bridge branch outages)",
         "config": {"workload": f"{GRID}: 9,241 buses, {p.n_cb} branches, {ns} outages per GPU, "
-                               + ("learned warm start (GNN prediction of each batch on a second stream, overlapping "
-                                  "the previous batch's solve; per-lane choice against the base start by initial "
-                                  "mismatch; fallback to the base start)" if learned is not None else
+                               + ("learned warm start (GNN prediction on the device inside the step; per-lane "
+                                  "choice against the base start by initial mismatch; fallback to the base start)"
+                                  if learned is not None else
                                   "warm start from the base case")
                                + f", tol {TOL} pu, "
                                + (f"FP32 LU + {refinement} FP64 refinement step(s)" if precision == native.MIXED
