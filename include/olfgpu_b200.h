@@ -113,7 +113,8 @@ int olfgpu_last_fp64_refactors(int64_t context, unsigned char* flagged, int* cou
  * lanes and the narrow levels (<= 48 tasks) of each phase in one launch of tiles of lanesPerTile (1, 2 or 4; 0: one
  * launch per level throughout), captured as one CUDA graph per Newton iteration; schedule 1 runs the whole Newton
  * loop in one persistent launch, one CTA per tile of lanesPerTile (1, 2, 4 or 8) lanes with `threads` (256 or 512)
- * threads; schedule -1 lets the next solve time every
+ * threads; schedule 2 runs each factorization and each solve as one cooperative launch over all lanes whose CTAs
+ * meet at a grid barrier between dependency levels (tile arguments ignored); schedule -1 lets the next solve time every
  * candidate on its batch and keep the fastest (the autotuner).  olfgpu_get_schedule reports the schedule in force
  * and, after an autotuned solve, up to maxResults timings {schedule, lanesPerTile, threads, ms} into results
  * (nResults receives their count).

@@ -221,8 +221,12 @@ extern "C" int olfgpu_set_schedule(int64_t context, int schedule, int lanesPerTi
             c.autotunePending = true;
             return;
         }
-        if (schedule != SCHEDULE_LEVELS && schedule != SCHEDULE_PERSISTENT) throw std::runtime_error("unknown schedule");
-        if (schedule == SCHEDULE_LEVELS) {
+        if (schedule != SCHEDULE_LEVELS && schedule != SCHEDULE_PERSISTENT && schedule != SCHEDULE_COOP) {
+            throw std::runtime_error("unknown schedule");
+        }
+        if (schedule == SCHEDULE_COOP) {
+            // cooperative sweeps have no tile parameters
+        } else if (schedule == SCHEDULE_LEVELS) {
             if (lanesPerTile != 0 && lanesPerTile != 1 && lanesPerTile != 2 && lanesPerTile != 4) {
                 throw std::runtime_error("level schedule: lanesPerTile of the narrow levels must be 0, 1, 2 or 4");
             }

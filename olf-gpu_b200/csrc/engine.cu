@@ -205,6 +205,13 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
         }
         d->bwdSplit[l] = splitOf(m);
     }
+    d->levelSplitD.upload(d->levelSplit);
+    d->fwdSplitD.upload(d->fwdSplit);
+    d->bwdSplitD.upload(d->bwdSplit);
+    d->coop = CoopPlan{static_cast<int>(p.levelPtr.size()) - 1, static_cast<int>(p.fwdLevelPtr.size()) - 1,
+                       static_cast<int>(p.bwdLevelPtr.size()) - 1, d->levelPtrD.as<int>(), d->levelSplitD.as<int>(),
+                       d->fwdPtrD.as<int>(), d->fwdPos.as<int>(), d->fwdSplitD.as<int>(), d->bwdPtrD.as<int>(),
+                       d->bwdPos.as<int>(), d->bwdSplitD.as<int>()};
     DevNet& v = d->view;
     v.n = s.n;
     v.nb = nb;
@@ -654,6 +661,60 @@ void launchFp64Redo(BatchContext& ctx) {
 // One Newton iteration launched phase by phase with CUDA events between the phases (the same kernels in the same
 // order as the two captured graphs); the phase times and the lanes that factorized accumulate in the context.
 // Returns false when no lane is left iterating.
+// The factorization / one solve of an iteration under the context's schedule (level launches or cooperative sweeps).
+void factorPhase(BatchContext& ctx, const DevBatch& b, bool fp32) {
+    const DeviceNet& dn = *ctx.net->dev;
+    if (ctx.schedule == SCHEDULE_COOP) {
+        OLF_CUDA(launchFactorCoop(dn.view, b, dn.coop, fp32, ctx.stream));
+        return;
+    }
+    const Hybrid hy = ctx.hybrid();
+    launchFactor(dn.view, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, fp32,
+                 ctx.narrowLanes > 0 ? &hy : nullptr, ctx.stream);
+}
+
+void solvePhase(BatchContext& ctx, const DevBatch& b, bool fp32, bool fromResidual) {
+    const DeviceNet& dn = *ctx.net->dev;
+    if (ctx.schedule == SCHEDULE_COOP) {
+        OLF_CUDA(launchSolveCoop(dn.view, b, dn.coop, fp32, fromResidual, ctx.stream));
+        return;
+    }
+    const Hybrid hy = ctx.hybrid();
+    launchSolve(dn.view, b, dn.fwd(), dn.bwd(), fp32, fromResidual, ctx.narrowLanes > 0 ? &hy : nullptr, ctx.stream);
+}
+
+// One Newton iteration's factorization, solves, refinement, FP64 refactor and step with cooperative sweeps (the
+// cooperative launches are not captured in graphs).
+void coopIteration(BatchContext& ctx) {
+    const DeviceNet& dn = *ctx.net->dev;
+    const bool mixed = ctx.precision == 1;
+    cudaStream_t st = ctx.stream;
+    const DevBatch b = ctx.batch();
+    factorPhase(ctx, b, mixed);
+    if (mixed) {
+        launchCountFp64(b, st);
+        OLF_CUDA(cudaMemcpyAsync(ctx.hostActive + 3, static_cast<int*>(ctx.nActive.p) + 3, 4, cudaMemcpyDeviceToHost,
+                                 st));
+        OLF_CUDA(cudaEventRecord(ctx.countReady, st));
+    }
+    solvePhase(ctx, b, mixed, false);
+    if (mixed) {
+        if (ctx.hostActive[2] > 0) {
+            for (int r = 0; r < ctx.refinementSteps; r++) {
+                launchResidual(dn.view, b, st);
+                solvePhase(ctx, b, true, true);
+            }
+        }
+        OLF_CUDA(cudaEventSynchronize(ctx.countReady));
+        if (ctx.hostActive[3] > 0) {
+            const DevBatch b64 = fp64View(ctx);
+            factorPhase(ctx, b64, false);
+            solvePhase(ctx, b64, false, false);
+        }
+    }
+    launchStep(dn.view, b, false, st);
+}
+
 bool phaseTimedIteration(BatchContext& ctx) {
     const DeviceNet& dn = *ctx.net->dev;
     const DevNet& net = dn.view;
@@ -679,21 +740,18 @@ bool phaseTimedIteration(BatchContext& ctx) {
     const bool live = ctx.hostActive[0] > 0;
     const int solving = ctx.hostActive[1];
     if (live && solving > 0) {
-        const Hybrid hy = ctx.hybrid();
-        const Hybrid* hp = ctx.narrowLanes > 0 ? &hy : nullptr;
-        const int nLevels = static_cast<int>(dn.levelPtr.size()) - 1;
         OLF_CUDA(cudaEventRecord(ev[2], st));
-        launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, mixed, hp, st);
+        factorPhase(ctx, b, mixed);
         if (mixed) launchCountFp64(b, st);
         OLF_CUDA(cudaEventRecord(ev[3], st));
-        launchSolve(net, b, dn.fwd(), dn.bwd(), mixed, false, hp, st);
+        solvePhase(ctx, b, mixed, false);
         OLF_CUDA(cudaEventRecord(ev[4], st));
         if (mixed) {
             // refinement steps (in iterations with a lane below the threshold) and the FP64 refactor of flagged lanes
             if (ctx.hostActive[2] > 0) {
                 for (int r = 0; r < ctx.refinementSteps; r++) {
                     launchResidual(net, b, st);
-                    launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, st);
+                    solvePhase(ctx, b, true, true);
                 }
             }
             OLF_CUDA(cudaMemcpyAsync(ctx.hostActive + 3, static_cast<int*>(ctx.nActive.p) + 3, 4,
@@ -701,8 +759,8 @@ bool phaseTimedIteration(BatchContext& ctx) {
             OLF_CUDA(cudaStreamSynchronize(st));
             if (ctx.hostActive[3] > 0) {
                 const DevBatch b64 = fp64View(ctx);
-                launchFactor(net, b64, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, false, hp, st);
-                launchSolve(net, b64, dn.fwd(), dn.bwd(), false, false, hp, st);
+                factorPhase(ctx, b64, false);
+                solvePhase(ctx, b64, false, false);
             }
         }
         OLF_CUDA(cudaEventRecord(ev[5], st));
@@ -859,6 +917,10 @@ int runIterations(BatchContext& ctx) {
         }
         // no lane factorizes this iteration (only restarts pending): skip the factor / solve graphs
         if (ctx.hostActive[1] <= 0) continue;
+        if (ctx.schedule == SCHEDULE_COOP) {
+            coopIteration(ctx);
+            continue;
+        }
         if (!mixed) {
             OLF_CUDA(cudaGraphLaunch(ctx.graphSolve, st));
             continue;
@@ -883,6 +945,7 @@ void autotune(BatchContext& ctx) {
     struct Candidate { int schedule, lanes, threads; };
     std::vector<Candidate> cands;
     for (int narrow : {0, 1, 2, 4}) cands.push_back({SCHEDULE_LEVELS, narrow, 256});
+    cands.push_back({SCHEDULE_COOP, 0, 512});
     for (int lanes : {2, 4})
         for (int threads : {256, 512}) cands.push_back({SCHEDULE_PERSISTENT, lanes, threads});
     cudaEvent_t e0, e1;

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "coop.cuh"
 #include "persistent.cuh"
 #include "structure.hpp"
 
@@ -69,7 +70,8 @@ struct DeviceNet {
     DeviceBuffer csrToAD;                         // the same map on the device
     DeviceBuffer nodeCol, sidePtr, side, cbPar, cbTrig, aPtr, aCol, aDiag, shPtr, shList, shPar, obPtr, obList, obPar;
     DeviceBuffer task, ops, levelTask, perm, iperm, lrowPtr, lrow, uPtr, uCol, fwdPos, bwdPos;
-    DeviceBuffer levelPtrD, levelLongestD, fwdPtrD, fwdLongestD, bwdPtrD, bwdLongestD;
+    DeviceBuffer levelPtrD, levelLongestD, fwdPtrD, fwdLongestD, bwdPtrD, bwdLongestD, levelSplitD, fwdSplitD, bwdSplitD;
+    CoopPlan coop{};
     PersistentPlan persistent{};
     int factorFrom = 0, fwdFrom = 0, bwdUntil = 0;   // narrow-level boundaries of the level schedule
 };
@@ -83,7 +85,7 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s);
 
 // Schedules of the Newton iterations: one launch per dependency level (captured in a CUDA graph per iteration), or
 // the persistent kernel with one CTA per lane tile running the whole loop.
-enum { SCHEDULE_LEVELS = 0, SCHEDULE_PERSISTENT = 1 };
+enum { SCHEDULE_LEVELS = 0, SCHEDULE_PERSISTENT = 1, SCHEDULE_COOP = 2 };
 
 struct TuningResult {
     int schedule, lanesPerTile, threads;

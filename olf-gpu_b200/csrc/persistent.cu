@@ -57,10 +57,10 @@ struct TileState {
 };
 
 // The split factor of a level with `count` tasks whose longest update list is `longest`: how many slots share a task
-// (a power of two, up to every slot of the tile for the one-task levels at the top of the elimination tree).
+// (a power of two up to 32).
 __device__ __forceinline__ int splitFor(int count, int longest, int slots) {
     int P = 1;
-    while (P < slots && count * (P * 2) <= slots && (longest + P - 1) / P > 2) P *= 2;
+    while (P < 32 && count * (P * 2) <= slots && (longest + P - 1) / P > 2) P *= 2;
     return P;
 }
 
@@ -94,7 +94,7 @@ __device__ void factorLevels(const DevNet& net, const DevBatch& b, T* lu, const 
                     a11 = (T)p[3 * S];
                     amax = fmax(fmax(fabs(a00), fabs(a01)), fmax(fabs(a10), fabs(a11)));
                 }
-#pragma unroll 4
+#pragma unroll 2
                 for (int q = tk.opBegin + part; q < tk.opEnd; q += P) {
                     const int4 op = net.ops[q];
                     T m00, m01, m10, m11, u00, u01, u10, u11;

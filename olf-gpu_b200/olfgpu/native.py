@@ -40,7 +40,7 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_last_fallbacks", "olfgpu_set_phase_timing", "olfgpu_last_phase_times", "olfgpu_structure_levels",
            "olfgpu_set_device_start", "olfgpu_set_mixed_precision_controls", "olfgpu_last_fp64_refactors"]
 # Schedules of the Newton iterations
-LEVELS, PERSISTENT, AUTOTUNE = 0, 1, -1
+LEVELS, PERSISTENT, COOPERATIVE, AUTOTUNE = 0, 1, 2, -1
 # Structure orderings (0 minimum degree, 1 nested dissection, 2 natural) and the deferred-L plan flag
 MIN_DEGREE, NESTED_DISSECTION, NATURAL, PLAN_DEFERRED_L = 0, 1, 2, 8
 

@@ -216,7 +216,7 @@ def test_reactive_limits_match_oracle(engine_lib, oracle_mod):
 
 
 @pytest.mark.parametrize("schedule,lanes,threads", [(0, 0, 256), (0, 1, 256), (0, 2, 256), (0, 4, 256), (1, 1, 256),
-                                                    (1, 2, 512), (1, 4, 512), (1, 8, 256)])
+                                                    (1, 2, 512), (1, 4, 512), (1, 8, 256), (2, 0, 512)])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_schedules_match_oracle(engine_lib, oracle_mod, schedule, lanes, threads, precision):
     """Every schedule (level launches, persistent tiles of 1-8 lanes) gives the oracle's states and statuses."""
@@ -243,7 +243,7 @@ def test_autotuner_picks_a_schedule_and_keeps_results(engine_lib, oracle_mod):
     ctx.set_schedule(native.AUTOTUNE)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
     (sc, lanes, threads), tuning = ctx.schedule()
-    assert len(tuning) == 8
+    assert len(tuning) == 9
     best = min(tuning, key=lambda t: t[3])
     assert (sc, lanes, threads) == (int(best[0]), int(best[1]), int(best[2]))
     ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis)
@@ -256,7 +256,7 @@ def test_persistent_reactive_limits_match_oracle(engine_lib, oracle_mod):
     outs = synthetic.draw_outages(g, 64, seed=301)
     dis = p.outage_masks(outs)
     s = native.Structure(p)
-    for sched in (0, 1):
+    for sched in (0, 1, 2):
         ctx = native.BatchContext(s, outs.shape[0], rl=p.rl)
         ctx.set_schedule(sched, 2, 256)
         r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
@@ -343,7 +343,7 @@ def test_adaptive_refinement_matches_oracle(engine_lib, oracle_mod, refine_below
     _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n)
 
 
-@pytest.mark.parametrize("schedule,lanes,threads", [(0, 2, 256), (0, 0, 256), (1, 2, 256)])
+@pytest.mark.parametrize("schedule,lanes,threads", [(0, 2, 256), (0, 0, 256), (1, 2, 256), (2, 0, 512)])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_deferred_l_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes, threads, precision):
     """The deferred-L block-LU plan (half the factorization levels) gives the oracle's states and statuses."""
@@ -359,3 +359,20 @@ def test_deferred_l_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes,
     ctx.set_schedule(schedule, lanes, threads)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
     _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_cooperative_sweeps_match_level_launches(engine_lib, precision):
+    """The cooperative schedule runs the same arithmetic in the same order as the level launches: identical results."""
+    from olfgpu import native, synthetic
+    g, p = grid("grid2000")
+    outs = synthetic.draw_outages(g, 80, seed=94)
+    dis = p.outage_masks(outs)
+    s = native.Structure(p)
+    res = []
+    for sched in (0, 2):
+        ctx = native.BatchContext(s, outs.shape[0])
+        ctx.set_linear_solver_settings(precision, 1)
+        ctx.set_schedule(sched, 0, 512 if sched == 2 else 256)
+        res.append(ctx.solve(p.x_base, p.target, p.base_row_mode, dis).copy())
+    assert np.array_equal(res[0], res[1])
