@@ -122,6 +122,8 @@ def run_engine(args, rank: int, world: int):
     ctx.set_linear_solver_settings(precision, max(refinement, 0))
     if args.schedule == "auto":
         ctx.set_schedule(native.AUTOTUNE)           # the first (warm-up) solve times the candidates
+    elif args.schedule == "coop":
+        ctx.set_schedule(native.COOPERATIVE, 0, 512)
     # host inputs in pinned memory (e2e copies them every step); results read back to pinned memory
     dis = torch.from_numpy(p.outage_masks(outs)).pin_memory().numpy()
     out = torch.empty((ns, p.n + 3), dtype=torch.float64).pin_memory().numpy()
@@ -488,7 +490,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--plan", default="scaled", choices=["scaled", "deferred"],
                     help="block-LU plan: L scaled at its task (default) or deferred (half the levels)")
-    ap.add_argument("--schedule", default="auto", choices=["auto", "levels"],
+    ap.add_argument("--schedule", default="auto", choices=["auto", "levels", "coop"],
                     help="auto: the engine's autotuner picks the Newton-iteration schedule on the first solve")
     ap.add_argument("--outages", type=int, default=N_OUTAGES,
                     help="outages per GPU (500 is the benchmark; smaller batches are profiling cases)")
