@@ -97,7 +97,9 @@ int olfgpu_set_linear_solver_settings(int64_t context, int precision, int refine
 /*
  * Mixed-precision controls (no counterpart in the reference; precision 1 only).  The refinement steps run only in
  * iterations where some factorizing scenario's max |F| is below refineBelow (default 1e-5; infinity: every iteration):
- * far from convergence the next Newton iteration corrects the FP32 solve's error itself.  A scenario whose FP32
+ * far from convergence the next Newton iteration corrects the FP32 solve's error itself.  Each step computes the FP64
+ * residual r = -F - J dx and runs its correction solve only while some scenario's max |r| exceeds a tenth of the
+ * mismatch tolerance.  A scenario whose FP32
  * factorization meets a pivot block with growth above growthLimit (condition estimate max|D| max|inv D|, or max|D|
  * over the largest entry of its Jacobian block; default 1e4) is flagged: in the level schedule its factorization and
  * solve are redone in FP64 in the same iteration (and every later one of the solve); the persistent schedules give

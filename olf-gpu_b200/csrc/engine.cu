@@ -259,7 +259,7 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
 BatchContext::~BatchContext() {
     if (graph) cudaGraphExecDestroy(graph);
     if (graphSolve) cudaGraphExecDestroy(graphSolve);
-    for (cudaGraphExec_t gx : {graphFactor, graphRefine, graph64, graphStep})
+    for (cudaGraphExec_t gx : {graphFactor, graphResidual, graphCorrect, graph64, graphStep})
         if (gx) cudaGraphExecDestroy(gx);
     if (hostActive) cudaFreeHost(hostActive);
     if (countReady) cudaEventDestroy(countReady);
@@ -302,6 +302,7 @@ DevBatch BatchContext::batch() const {
     b.fellBack = fellBack.as<int8_t>();
     b.growthLimit = growthLimit;
     b.laneMask = nullptr;
+    b.resNorm = resNorm.as<unsigned long long>();
     return b;
 }
 
@@ -346,6 +347,7 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
     ctx->pending.alloc(S);
     ctx->precision64.alloc(S);
     ctx->fallbackLeft.alloc(S);
+    ctx->resNorm.alloc(S * 8);
     ctx->fellBack.alloc(S);
     ctx->nActive.alloc(16);
     ctx->out.alloc(static_cast<size_t>(nScenarios) * (n + 3) * 8);
@@ -591,7 +593,8 @@ void captureIteration(BatchContext& ctx) {
     dropGraph(ctx.graph);
     dropGraph(ctx.graphSolve);
     dropGraph(ctx.graphFactor);
-    dropGraph(ctx.graphRefine);
+    dropGraph(ctx.graphResidual);
+    dropGraph(ctx.graphCorrect);
     dropGraph(ctx.graph64);
     dropGraph(ctx.graphStep);
     const DeviceNet& dn = *ctx.net->dev;
@@ -628,12 +631,12 @@ void captureIteration(BatchContext& ctx) {
         });
         ctx.graphSolve = captureInto(st, [&] { launchSolve(net, b, dn.fwd(), dn.bwd(), true, false, hp, st); });
         if (ctx.refinementSteps > 0) {
-            ctx.graphRefine = captureInto(st, [&] {
-                for (int k = 0; k < ctx.refinementSteps; k++) {
-                    launchResidual(net, b, st);
-                    launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, st);
-                }
+            // one refinement step: the FP64 residual and its check, then (when a lane needs it) the correction solve
+            ctx.graphResidual = captureInto(st, [&] {
+                launchResidual(net, b, st);
+                launchResidualCheck(net, b, REFINE_RESIDUAL * ctx.cfg.tol, st);
             });
+            ctx.graphCorrect = captureInto(st, [&] { launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, st); });
         }
         ctx.graphStep = captureInto(st, [&] { launchStep(net, b, false, st); });
     }
@@ -683,6 +686,22 @@ void solvePhase(BatchContext& ctx, const DevBatch& b, bool fp32, bool fromResidu
     launchSolve(dn.view, b, dn.fwd(), dn.bwd(), fp32, fromResidual, ctx.narrowLanes > 0 ? &hy : nullptr, ctx.stream);
 }
 
+// The refinement steps of a mixed-precision iteration, launched directly: FP64 residual, its per-lane check, and the
+// correction solve only while some lane's residual is above the bound.
+void refinementSteps(BatchContext& ctx, const DevBatch& b) {
+    const DeviceNet& dn = *ctx.net->dev;
+    cudaStream_t st = ctx.stream;
+    for (int r = 0; r < ctx.refinementSteps; r++) {
+        launchResidual(dn.view, b, st);
+        launchResidualCheck(dn.view, b, REFINE_RESIDUAL * ctx.cfg.tol, st);
+        OLF_CUDA(cudaMemcpyAsync(ctx.hostActive + 2, static_cast<int*>(ctx.nActive.p) + 2, 4, cudaMemcpyDeviceToHost,
+                                 st));
+        OLF_CUDA(cudaStreamSynchronize(st));
+        if (ctx.hostActive[2] <= 0) break;
+        solvePhase(ctx, b, true, true);
+    }
+}
+
 // One Newton iteration's factorization, solves, refinement, FP64 refactor and step with cooperative sweeps (the
 // cooperative launches are not captured in graphs).
 void coopIteration(BatchContext& ctx) {
@@ -699,12 +718,7 @@ void coopIteration(BatchContext& ctx) {
     }
     solvePhase(ctx, b, mixed, false);
     if (mixed) {
-        if (ctx.hostActive[2] > 0) {
-            for (int r = 0; r < ctx.refinementSteps; r++) {
-                launchResidual(dn.view, b, st);
-                solvePhase(ctx, b, true, true);
-            }
-        }
+        if (ctx.hostActive[2] > 0) refinementSteps(ctx, b);
         OLF_CUDA(cudaEventSynchronize(ctx.countReady));
         if (ctx.hostActive[3] > 0) {
             const DevBatch b64 = fp64View(ctx);
@@ -748,12 +762,7 @@ bool phaseTimedIteration(BatchContext& ctx) {
         OLF_CUDA(cudaEventRecord(ev[4], st));
         if (mixed) {
             // refinement steps (in iterations with a lane below the threshold) and the FP64 refactor of flagged lanes
-            if (ctx.hostActive[2] > 0) {
-                for (int r = 0; r < ctx.refinementSteps; r++) {
-                    launchResidual(net, b, st);
-                    solvePhase(ctx, b, true, true);
-                }
-            }
+            if (ctx.hostActive[2] > 0) refinementSteps(ctx, b);
             OLF_CUDA(cudaMemcpyAsync(ctx.hostActive + 3, static_cast<int*>(ctx.nActive.p) + 3, 4,
                                      cudaMemcpyDeviceToHost, st));
             OLF_CUDA(cudaStreamSynchronize(st));
@@ -931,7 +940,16 @@ int runIterations(BatchContext& ctx) {
                                  st));
         OLF_CUDA(cudaEventRecord(ctx.countReady, st));
         OLF_CUDA(cudaGraphLaunch(ctx.graphSolve, st));
-        if (ctx.graphRefine && ctx.hostActive[2] > 0) OLF_CUDA(cudaGraphLaunch(ctx.graphRefine, st));
+        if (ctx.graphResidual && ctx.hostActive[2] > 0) {
+            for (int r = 0; r < ctx.refinementSteps; r++) {
+                OLF_CUDA(cudaGraphLaunch(ctx.graphResidual, st));
+                OLF_CUDA(cudaMemcpyAsync(ctx.hostActive + 2, static_cast<int*>(ctx.nActive.p) + 2, 4,
+                                         cudaMemcpyDeviceToHost, st));
+                OLF_CUDA(cudaStreamSynchronize(st));
+                if (ctx.hostActive[2] <= 0) break;   // every lane's FP32 solve already meets the residual bound
+                OLF_CUDA(cudaGraphLaunch(ctx.graphCorrect, st));
+            }
+        }
         OLF_CUDA(cudaEventSynchronize(ctx.countReady));
         if (ctx.hostActive[3] > 0) launchFp64Redo(ctx);
         OLF_CUDA(cudaGraphLaunch(ctx.graphStep, st));

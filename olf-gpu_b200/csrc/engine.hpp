@@ -87,6 +87,10 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s);
 // the persistent kernel with one CTA per lane tile running the whole loop.
 enum { SCHEDULE_LEVELS = 0, SCHEDULE_PERSISTENT = 1, SCHEDULE_COOP = 2 };
 
+// Mixed precision: a refinement step's correction solve runs only while some lane's FP64 residual max |r| is above
+// this fraction of the mismatch tolerance (below it the FP32 solve is already accurate enough for the test).
+constexpr double REFINE_RESIDUAL = 0.1;
+
 struct TuningResult {
     int schedule, lanesPerTile, threads;
     float ms;
@@ -126,7 +130,7 @@ struct BatchContext {
     int refinementSteps = 1;
     // lane-interleaved state
     DeviceBuffer x, target, mode, F, J, lu64, lu32, w64, w32, dx, res, qbuf, disabled, norm, iter, status, outer,
-        totalIter, trouble, normOut, active, pending, precision64, nActive, fallbackLeft, fellBack;
+        totalIter, trouble, normOut, active, pending, precision64, nActive, fallbackLeft, fellBack, resNorm;
     bool fallbackStart = false;     // lanes that fail from x0Full restart once from x0Base (both given)
     const double* deviceStart = nullptr;  // caller's device array [nS][n] used as x0Full by the solves
     const double* fullSrc = nullptr;      // where the installed x0Full rows come from
@@ -162,7 +166,8 @@ struct BatchContext {
     cudaGraphExec_t graphSolve = nullptr;  // FP64: factorization, solves, step; mixed: FP32 solves
     // mixed precision only: FP32 factorization + count of FP64-flagged lanes; refinement steps; the FP64 refactor and
     // solve of the flagged lanes; the step
-    cudaGraphExec_t graphFactor = nullptr, graphRefine = nullptr, graph64 = nullptr, graphStep = nullptr;
+    cudaGraphExec_t graphFactor = nullptr, graphResidual = nullptr, graphCorrect = nullptr, graph64 = nullptr,
+                    graphStep = nullptr;
     int graphKey = -1;
     double refineBelow = 1e-5;      // mixed: refinement steps only in iterations where a lane's max |F| is below it
     double growthLimit = 1e4;       // mixed: FP32 pivot growth above which a lane refactors in FP64

@@ -806,6 +806,47 @@ void launchCountSolving(const DevBatch& b, double refineBelow, cudaStream_t st) 
 
 void launchCountFp64(const DevBatch& b, cudaStream_t st) { countLanesKernel<<<1, 1024, 0, st>>>(b, 0.0, 1); }
 
+// Per-lane max |res| over the rows: 32 lanes x 8 row strands per CTA, reduced in shared memory, one atomic per CTA
+// and lane (non-negative doubles order like their bit patterns; a NaN residual sorts above every number).
+__global__ void residualMaxKernel(DevNet net, DevBatch b) {
+    __shared__ double red[8][32];
+    const int s = blockIdx.x * 32 + threadIdx.x;
+    const size_t S = b.S;
+    double m = 0.0;
+    if (s < b.S && solving(b, s)) {
+        for (int r = blockIdx.y * 8 + threadIdx.y; r < net.n; r += 8 * gridDim.y) m = absMax(m, b.res[(size_t)r * S + s]);
+    }
+    red[threadIdx.y][threadIdx.x] = m;
+    __syncthreads();
+    if (threadIdx.y == 0 && s < b.S) {
+        for (int k = 1; k < 8; k++) m = absMax(m, red[k][threadIdx.x]);
+        if (m != 0.0) atomicMax(&b.resNorm[s], (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+__global__ void countResidualKernel(DevBatch b, double threshold) {
+    __shared__ int part[32];
+    int c = 0;
+    for (int s = threadIdx.x; s < b.S; s += blockDim.x) {
+        const double r = __longlong_as_double((long long)b.resNorm[s]);
+        c += (b.active[s] && !b.pending[s] && !(r <= threshold)) ? 1 : 0;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
+        b.nActive[2] = t;
+    }
+}
+
+void launchResidualCheck(const DevNet& net, const DevBatch& b, double threshold, cudaStream_t st) {
+    cudaMemsetAsync(b.resNorm, 0, sizeof(unsigned long long) * b.S, st);
+    residualMaxKernel<<<dim3(b.S / 32, 64), dim3(32, 8), 0, st>>>(net, b);
+    countResidualKernel<<<1, 1024, 0, st>>>(b, threshold);
+}
+
 void launchStep(const DevNet& net, const DevBatch& b, bool, cudaStream_t st) {
     const size_t all = (size_t)net.n * b.S;
     stepKernel<<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b);

@@ -110,6 +110,7 @@ struct DevBatch {
     // exceeds growthLimit flags its lane in precision64; laneMask (may be null) restricts the LU kernels to flagged lanes
     double growthLimit;
     const int8_t* laneMask;
+    unsigned long long* resNorm;  // [S] max |refinement residual| as ordered bits
 };
 
 // Reactive-limit entries (ReactiveLimitsPacker.java:76) and their per-lane state.
@@ -199,5 +200,8 @@ void launchIterationStart(const DevBatch& b, cudaStream_t st);
 void launchCountSolving(const DevBatch& b, double refineBelow, cudaStream_t st);
 // Factorizing lanes flagged for an FP64 refactor (nActive[3]).
 void launchCountFp64(const DevBatch& b, cudaStream_t st);
+// Mixed precision, after launchResidual: each lane's max |r| and the count of factorizing lanes whose residual is
+// above `threshold` (nActive[2]): the correction solve of a refinement step runs only when some lane needs it.
+void launchResidualCheck(const DevNet& net, const DevBatch& b, double threshold, cudaStream_t st);
 
 }  // namespace olfb200
