@@ -263,6 +263,24 @@ int olfgpu_gnn_compose_start(int nScenarios, int nb, const float* pred, int ldPr
                              void* stream);
 
 /*
+ * Learned-start inference restricted to the buses an outage can reach: a message-passing layer only moves
+ * information one hop, so after L layers a sample differs from the outage-free sample only within L hops of its
+ * outaged branch.  The compact rows (sample rowSample[r], bus rowNode[r]) hold those buses; rowOf [nSamples * nb]
+ * maps (sample, bus) to its row or -1, and a neighbour outside the rows reads the outage-free sample's PQbase row
+ * (identical there).  olfgpu_gnn_message_forward_compact is olfgpu_gnn_message_forward on those rows, with the same
+ * edges, order and arithmetic; olfgpu_gnn_compose_start_compact writes every scenario's start from the outage-free
+ * prediction predBase [nb][ldPred], then its rows from predRows [R][ldPred].  Device pointers throughout.
+ */
+int olfgpu_gnn_message_forward_compact(int R, int nb, const int* rowNode, const int* rowSample, const int* rowOf,
+                                       const int* inPtr, const int* inEdge, const int* edgeSrc, const int* edgeBranch,
+                                       const int* outage, const void* PQ, const void* PQbase, const float* C,
+                                       const float* bmsg, void* agg, void* stream);
+int olfgpu_gnn_compose_start_compact(int nScenarios, int nb, const float* predBase, const float* predRows, int ldPred,
+                                     int R, const int* rowNode, const int* rowSample, double stdVm, double stdVa,
+                                     const double* xBase, const unsigned char* identity, const double* target,
+                                     double* x0, void* stream);
+
+/*
  * Batched linear solve J z = rhs that allocates no memory (this entry point has no counterpart in the reference).
  * It is for callers that cannot allocate device memory while they solve: a host whose GPU memory is reserved up front
  * and handed out by someone else (a JVM or service that sized its pools at start-up), or a code path that must not

@@ -212,6 +212,38 @@ __global__ void messageForwardKernel(int B, int nb, const int* inPtr, const int*
     *reinterpret_cast<__nv_bfloat162*>(agg + ((size_t)b * nb + i) * 64 + f) = __floats2bfloat162_rn(a0, a1);
 }
 
+// The same messages for a compact set of rows (sample rowSample[r], bus rowNode[r]): the buses within reach of each
+// sample's outage.  A neighbour j outside the set takes its P row from PQbase (the outage-free sample, identical there);
+// inside, from PQ at rowOf[sample * nb + j].  Same edges, same order, same arithmetic as messageForwardKernel.
+__global__ void messageForwardCompactKernel(int R, int nb, const int* rowNode, const int* rowSample, const int* rowOf,
+                                            const int* inPtr, const int* inEdge, const int* edgeSrc,
+                                            const int* edgeBranch, const int* outage, const __nv_bfloat16* PQ,
+                                            const __nv_bfloat16* PQbase, const float* C, const float* bmsg,
+                                            __nv_bfloat16* agg) {
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (r >= R) return;
+    const int i = rowNode[r], b = rowSample[r];
+    const int f = 2 * lane;
+    const float2 q = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(PQ + (size_t)r * 128 + 64 + f));
+    const float2 bm = *reinterpret_cast<const float2*>(bmsg + f);
+    const float q0 = q.x + bm.x, q1 = q.y + bm.y;
+    float a0 = 0.f, a1 = 0.f;
+    const int out = outage[b];
+    const int p1 = inPtr[i + 1];
+    for (int p = inPtr[i]; p < p1; p++) {
+        const int e = inEdge[p];
+        if (edgeBranch[e] == out) continue;
+        const int j = edgeSrc[e];
+        const int rj = rowOf[(size_t)b * nb + j];
+        const __nv_bfloat16* src = rj >= 0 ? PQ + (size_t)rj * 128 : PQbase + (size_t)j * 128;
+        const float2 pj = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(src + f));
+        const float2 c = *reinterpret_cast<const float2*>(C + (size_t)e * 64 + f);
+        a0 += fmaxf(pj.x + q0 + c.x, 0.f);
+        a1 += fmaxf(pj.y + q1 + c.y, 0.f);
+    }
+    *reinterpret_cast<__nv_bfloat162*>(agg + (size_t)r * 64 + f) = __floats2bfloat162_rn(a0, a1);
+}
+
 // Backward of the messages.  dQ[b, i] = sum over e into i of g_e; dP[b, j] = sum over e out of j of g_e, with
 // g_e = dAgg[b, dst(e)] * [pre_e > 0] recomputed from the saved P, Q.  Written into dPQ [rows x 128] (fp32).
 __global__ void messageBackwardNodesKernel(int B, int nb, const int* inPtr, const int* inEdge, const int* outPtr,
@@ -405,11 +437,25 @@ int gnnGuard(F&& f) {
 }
 }  // namespace
 
+// Learned start states of the buses in the compact set: x0[s][2b], x0[s][2b + 1] from the compact output row (the
+// identity rows keep their targets, already written by the full composition).
+__global__ void scatterStartKernel(int R, int nb, const int* rowNode, const int* rowSample, const float* pred, int ldp,
+                                   double stdVm, double stdVa, const double* xBase, const unsigned char* identity,
+                                   double* x0) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= R) return;
+    const int b = rowNode[r];
+    const size_t base = (size_t)rowSample[r] * 2 * nb;
+    const float* o = pred + (size_t)r * ldp;
+    if (!identity[2 * b]) x0[base + 2 * b] = xBase[2 * b] + (double)o[1] * stdVa;
+    if (!identity[2 * b + 1]) x0[base + 2 * b + 1] = xBase[2 * b + 1] + (double)o[0] * stdVm;
+}
+
 // Start states from the network's output: per scenario s and bus b, x0[s][2b] (angle) = xBase + dVa * stdVa and
 // x0[s][2b + 1] (magnitude) = xBase + dVm * stdVm, the identity rows (slack angle, PV magnitudes) at their targets.
-__global__ void composeStartKernel(int nS, int nb, const float* pred, int ldp, double stdVm, double stdVa,
-                                   const double* xBase, const unsigned char* identity, const double* target,
-                                   double* x0) {
+__global__ void composeStartKernel(int nS, int nb, const float* pred, int ldp, long long sampleStride, double stdVm,
+                                   double stdVa, const double* xBase, const unsigned char* identity,
+                                   const double* target, double* x0) {
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int n = 2 * nb;
     if (tid >= (long long)nS * n) return;
@@ -418,7 +464,7 @@ __global__ void composeStartKernel(int nS, int nb, const float* pred, int ldp, d
     if (identity[r]) {
         v = target[r];
     } else {
-        const float* o = pred + ((long long)s * nb + b) * ldp;
+        const float* o = pred + (long long)s * sampleStride + (long long)b * ldp;
         v = xBase[r] + ((r & 1) ? (double)o[0] * stdVm : (double)o[1] * stdVa);
     }
     x0[tid] = v;
@@ -554,6 +600,39 @@ extern "C" int olfgpu_gnn_compose_start(int nScenarios, int nb, const float* pre
     return gnnGuard([&] {
         const long long count = (long long)nScenarios * 2 * nb;
         composeStartKernel<<<(unsigned)((count + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-            nScenarios, nb, pred, ldPred, stdVm, stdVa, xBase, identity, target, x0);
+            nScenarios, nb, pred, ldPred, (long long)nb * ldPred, stdVm, stdVa, xBase, identity, target, x0);
+    });
+}
+
+extern "C" int olfgpu_gnn_message_forward_compact(int R, int nb, const int* rowNode, const int* rowSample,
+                                                  const int* rowOf, const int* inPtr, const int* inEdge,
+                                                  const int* edgeSrc, const int* edgeBranch, const int* outage,
+                                                  const void* PQ, const void* PQbase, const float* C,
+                                                  const float* bmsg, void* agg, void* stream) {
+    return gnnGuard([&] {
+        if (R <= 0) return;
+        messageForwardCompactKernel<<<(unsigned)(((long long)R * 32 + 255) / 256), 256, 0,
+                                      static_cast<cudaStream_t>(stream)>>>(
+            R, nb, rowNode, rowSample, rowOf, inPtr, inEdge, edgeSrc, edgeBranch, outage,
+            static_cast<const __nv_bfloat16*>(PQ), static_cast<const __nv_bfloat16*>(PQbase), C, bmsg,
+            static_cast<__nv_bfloat16*>(agg));
+    });
+}
+
+extern "C" int olfgpu_gnn_compose_start_compact(int nScenarios, int nb, const float* predBase, const float* predRows,
+                                                int ldPred, int R, const int* rowNode, const int* rowSample,
+                                                double stdVm, double stdVa, const double* xBase,
+                                                const unsigned char* identity, const double* target, double* x0,
+                                                void* stream) {
+    return gnnGuard([&] {
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        const long long count = (long long)nScenarios * 2 * nb;
+        // every scenario first takes the outage-free prediction, then its own rows
+        composeStartKernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(nScenarios, nb, predBase, ldPred, 0,
+                                                                            stdVm, stdVa, xBase, identity, target, x0);
+        if (R > 0) {
+            scatterStartKernel<<<(R + 255) / 256, 256, 0, st>>>(R, nb, rowNode, rowSample, predRows, ldPred, stdVm,
+                                                                stdVa, xBase, identity, x0);
+        }
     });
 }

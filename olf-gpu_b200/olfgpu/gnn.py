@@ -47,6 +47,9 @@ def _lib():
             "olfgpu_gnn_mse": [i, i, vp, vp, vp, vp, vp],
             "olfgpu_gnn_copy_cols": [i, i, vp, i, i, vp, i, i, i, vp],
             "olfgpu_gnn_compose_start": [i, i, vp, i, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp, vp],
+            "olfgpu_gnn_message_forward_compact": [i, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp],
+            "olfgpu_gnn_compose_start_compact": [i, i, vp, vp, i, i, vp, vp, ctypes.c_double, ctypes.c_double, vp, vp,
+                                                 vp, vp, vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -169,6 +172,47 @@ class WarmStartNet:
         self._partial = None
 
     # ------------------------------------------------------------------------------------------------------------
+    def forward_rows(self, x0, outage, rows=None, base_pq=None, keep_pq: bool = False):
+        """Inference only.  rows None: every bus of every sample (x0 [B * nb, 16]), returning (out, per-layer PQ when
+        keep_pq).  rows = (row_node, row_sample, row_of) device int32 tensors: x0 holds only those rows [R, 16] and a
+        neighbour outside them reads base_pq[l] (the outage-free sample's layer-l PQ, [nb, 128]).  Same arithmetic per
+        row either way."""
+        import torch
+        g = self.graph
+        M = x0.shape[0]
+        B = outage.shape[0]
+        st = _stream()
+        bf = torch.bfloat16
+        h = torch.empty((M, H), dtype=bf, device=self.dev)
+        _call("olfgpu_gnn_gemm", M, FEAT_IN, 0, H, _ptr(x0), None, _ptr(self.wb["w_in"]), _ptr(self.w["b_in"]), 1,
+              None, _ptr(h), None, H, None, st)
+        pqs = []
+        for l in range(self.layers):
+            c = torch.empty((g.n_edges, H), dtype=torch.float32, device=self.dev)
+            _call("olfgpu_gnn_edge_project", g.n_edges, _ptr(g.es), _ptr(self.w[f"w_e{l}"]), _ptr(c), st)
+            pq = torch.empty((M, 2 * H), dtype=bf, device=self.dev)
+            _call("olfgpu_gnn_gemm", M, H, 0, 2 * H, _ptr(h), None, _ptr(self.wb[f"w_pq{l}"]), None, 0, None, _ptr(pq),
+                  None, 2 * H, None, st)
+            agg = torch.empty((M, H), dtype=bf, device=self.dev)
+            if rows is None:
+                _call("olfgpu_gnn_message_forward", B, g.nb, _ptr(g.in_ptr), _ptr(g.in_edge), _ptr(g.src),
+                      _ptr(g.branch), _ptr(outage), _ptr(pq), _ptr(c), _ptr(self.w[f"b_msg{l}"]), _ptr(agg), st)
+            else:
+                rn, rs, ro = rows
+                _call("olfgpu_gnn_message_forward_compact", M, g.nb, _ptr(rn), _ptr(rs), _ptr(ro), _ptr(g.in_ptr),
+                      _ptr(g.in_edge), _ptr(g.src), _ptr(g.branch), _ptr(outage), _ptr(pq), _ptr(base_pq[l]), _ptr(c),
+                      _ptr(self.w[f"b_msg{l}"]), _ptr(agg), st)
+            if keep_pq:
+                pqs.append(pq)
+            hn = torch.empty((M, H), dtype=bf, device=self.dev)
+            _call("olfgpu_gnn_gemm", M, H, H, H, _ptr(h), _ptr(agg), _ptr(self.wb[f"w_upd{l}"]),
+                  _ptr(self.w[f"b_upd{l}"]), 1, _ptr(h), _ptr(hn), None, H, None, st)
+            h = hn
+        out = torch.empty((M, FEAT_OUT), dtype=torch.float32, device=self.dev)
+        _call("olfgpu_gnn_gemm", M, H, 0, FEAT_OUT, _ptr(h), None, _ptr(self.wb["w_out"]), _ptr(self.w["b_out"]), 0,
+              None, None, _ptr(out), FEAT_OUT, None, st)
+        return (out, pqs) if keep_pq else out
+
     def forward(self, x0, outage, keep: bool = False):
         """x0: [B * nb, 16] bf16, outage: [B] int32 (closed-branch index per sample). Returns out [B * nb, 16] fp32."""
         import torch

@@ -172,3 +172,20 @@ def test_learned_start_trains_and_predicts_closer_starts(engine_lib, oracle_mod)
     assert np.array_equal(learned[:, -1], ref[:, -1])
     conv = ref[:, -1] == 0
     assert np.max(np.abs(learned[conv, :p.n] - ref[conv, :p.n])) <= 1e-8
+
+
+def test_compact_inference_equals_full_inference(engine_lib):
+    """Evaluating only the buses within reach of each outage (plus one outage-free pass) gives the full batched
+    forward's start states bit for bit."""
+    from olfgpu import synthetic
+    from olfgpu.learned_start import LearnedStart
+    g, p = grid("grid2000")
+    ls = LearnedStart(g, seed=4)
+    ls.feat_mean, ls.feat_std = np.zeros(7), np.ones(7)
+    ls.tgt_std, ls.flow_std = np.array([0.01, 0.02], np.float32), 1.0
+    outs = synthetic.draw_outages(g, 150, seed=95)
+    full = ls.predict(p, p.x_base, outs, compact=False)
+    compact = ls.predict(p, p.x_base, outs, compact=True)
+    rn, rs, _ = ls.reach(outs)
+    assert rn.shape[0] < 0.2 * outs.shape[0] * p.n_bus      # far fewer rows than the full batch
+    assert np.array_equal(full, compact)
