@@ -116,7 +116,7 @@ def run_engine(args, rank: int, world: int):
     g, p, outs = workload(rank, args.outages)
     precision = native.MIXED if args.precision == "mixed" else native.FP64
     refinement = args.refinement if precision == native.MIXED else 0
-    s = native.Structure(p, native.PLAN_DEFERRED_L if args.plan == "deferred" else 0)
+    s = native.Structure(p, {"deferred": native.PLAN_DEFERRED_L, "dense": native.PLAN_DENSE_FRONT}.get(args.plan, 0))
     ns = outs.shape[0]
     ctx = native.BatchContext(s, ns)
     ctx.set_linear_solver_settings(precision, max(refinement, 0))
@@ -488,8 +488,9 @@ def main():
                     help="start states: the base case, or the learned warm start (default when its checkpoint exists)")
     ap.add_argument("--checkpoint", default=CHECKPOINT)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
-    ap.add_argument("--plan", default="scaled", choices=["scaled", "deferred"],
-                    help="block-LU plan: L scaled at its task (default) or deferred (half the levels)")
+    ap.add_argument("--plan", default="scaled", choices=["scaled", "deferred", "dense"],
+                    help="block-LU plan: L scaled at its task (default), deferred (half the levels) or dense (the "
+                         "trailing dense block factorized in shared memory)")
     ap.add_argument("--schedule", default="auto", choices=["auto", "levels", "coop"],
                     help="auto: the engine's autotuner picks the Newton-iteration schedule on the first solve")
     ap.add_argument("--outages", type=int, default=N_OUTAGES,

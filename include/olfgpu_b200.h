@@ -38,7 +38,9 @@ const char* olfgpu_last_error(void);
  * models, reactive relocation, transformer/shunt voltage-control columns) must be empty: a non-empty one, or a
  * control column >= 0, is rejected with an error.  ordering: 0 minimum degree (default), 1 nested dissection,
  * 2 natural; plus 8 for the deferred-L block-LU plan (the L factor stays unscaled during the factorization: about
- * half the dependency levels, one more 2x2 block read per update).
+ * half the dependency levels, one more 2x2 block read per update), or 16 for the dense-front plan (the trailing
+ * pivots whose blocks are all present, up to 32, are factorized as one dense front in shared memory; not runnable by
+ * the persistent schedules or the multi-grid launch).
  */
 int olfgpu_create_structure(int n, int nCb, const double* cbParams, const int* cbIndices, int nOb,
                             const double* obParams, const int* obIndices, int nSh, const double* shParams,

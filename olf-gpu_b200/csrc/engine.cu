@@ -79,6 +79,9 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
             task[id] = Task{p.luToA[id], p.opPtr[id], p.opPtr[id + 1], p.uPtr[k]};
         }
     }
+    // dense front: a front block's level task applies its updates from before the front and stores the partial sum
+    // (diag -3: no inversion, no scaling); the dense front kernel finishes it
+    for (int id : p.frontBlocks) task[id] = Task{p.luToA[id], p.opPtr[id], p.opOuterEnd[id], -3};
     // L blocks by row position (for the forward solve), ascending column position
     std::vector<std::vector<int2>> lr(nb);
     for (int k = 0; k < nb; k++)
@@ -219,6 +222,13 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     v.nLu = nLu;
     v.nU = p.nU;
     v.deferredL = p.deferredL ? 1 : 0;
+    v.frontStart = p.frontStart;
+    v.frontF = p.frontF;
+    if (p.frontF > 0) {
+        d->frontBlocks.upload(p.frontBlocks);
+        OLF_CUDA(prepareDenseFront(p.frontF));
+    }
+    v.frontBlocks = d->frontBlocks.as<int>();
     v.ncb = s.ncb;
     v.nob = s.nob;
     v.nsh = s.nsh;
@@ -669,6 +679,7 @@ void factorPhase(BatchContext& ctx, const DevBatch& b, bool fp32) {
     const DeviceNet& dn = *ctx.net->dev;
     if (ctx.schedule == SCHEDULE_COOP) {
         OLF_CUDA(launchFactorCoop(dn.view, b, dn.coop, fp32, ctx.stream));
+        launchDenseFront(dn.view, b, fp32, ctx.stream);
         return;
     }
     const Hybrid hy = ctx.hybrid();
@@ -896,6 +907,7 @@ int runIterations(BatchContext& ctx) {
     const int cap = roundCap(ctx);
     if (ctx.fallbackStart && ctx.hasX0Base && ctx.hasX0Full) selectStarts(ctx);
     if (ctx.schedule == SCHEDULE_PERSISTENT) {
+        if (dn.view.frontF > 0) throw std::runtime_error("the persistent schedule does not run dense-front plans");
         PersistentPlan plan = dn.persistent;
         plan.maxRounds = cap;
         launchPersistent(dn.view, ctx.batch(), ctx.rl, ctx.cfg, plan, ctx.lanesPerTile, ctx.threads, mixed, st);
@@ -964,8 +976,10 @@ void autotune(BatchContext& ctx) {
     std::vector<Candidate> cands;
     for (int narrow : {0, 1, 2, 4}) cands.push_back({SCHEDULE_LEVELS, narrow, 256});
     cands.push_back({SCHEDULE_COOP, 0, 512});
-    for (int lanes : {2, 4})
-        for (int threads : {256, 512}) cands.push_back({SCHEDULE_PERSISTENT, lanes, threads});
+    if (ctx.net->dev->view.frontF == 0) {   // the persistent tiles do not run dense-front plans
+        for (int lanes : {2, 4})
+            for (int threads : {256, 512}) cands.push_back({SCHEDULE_PERSISTENT, lanes, threads});
+    }
     cudaEvent_t e0, e1;
     OLF_CUDA(cudaEventCreate(&e0));
     OLF_CUDA(cudaEventCreate(&e1));
@@ -1103,6 +1117,9 @@ MultiContext* createMultiContext(const std::vector<BatchContext*>& members) {
     for (const BatchContext* c : members) {
         if (!c) throw std::runtime_error("null batch context");
         if (c->device != device) throw std::runtime_error("the batch contexts of a multi-grid launch share one device");
+        if (c->net->dev->view.frontF > 0) {
+            throw std::runtime_error("a multi-grid launch runs persistent tiles, which do not run dense-front plans");
+        }
     }
     for (size_t i = 0; i < members.size(); i++)
         for (size_t j = i + 1; j < members.size(); j++)

@@ -69,6 +69,7 @@ struct DeviceNet {
     std::vector<int> csrToA;                      // CSR slot -> A block * 4 + entry (debug readback of J)
     DeviceBuffer csrToAD;                         // the same map on the device
     DeviceBuffer nodeCol, sidePtr, side, cbPar, cbTrig, aPtr, aCol, aDiag, shPtr, shList, shPar, obPtr, obList, obPar;
+    DeviceBuffer frontBlocks;
     DeviceBuffer task, ops, levelTask, perm, iperm, lrowPtr, lrow, uPtr, uCol, fwdPos, bwdPos;
     DeviceBuffer levelPtrD, levelLongestD, fwdPtrD, fwdLongestD, bwdPtrD, bwdLongestD, levelSplitD, fwdSplitD, bwdSplitD;
     CoopPlan coop{};

@@ -540,6 +540,7 @@ void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtr, con
             scaleLKernel<double><<<grd, blk, 0, st>>>(net, b, b.lu64);
         }
     }
+    launchDenseFront(net, b, fp32, st);   // after every level (a dense-front plan is never deferred-L)
 }
 
 // ---------------------------------------------------------------------------------------------------------------

@@ -45,6 +45,8 @@ struct Task {
 struct DevNet {
     int n, nb, nA, nLu, nU, ncb, nob, nsh, nElements;
     int deferredL;            // 1: the L factor is kept unscaled during the factorization (see structure.hpp)
+    int frontStart, frontF;   // dense front: positions frontStart .. nb-1 (frontF = 0: none)
+    const int* frontBlocks;   // [frontF * frontF] LU block of front positions (i, j)
     const int* nodeCol;       // [2 nb]
     const int* sidePtr;       // [nb + 1]
     const Side* side;         // incident closed-branch sides
@@ -203,5 +205,9 @@ void launchCountFp64(const DevBatch& b, cudaStream_t st);
 // Mixed precision, after launchResidual: each lane's max |r| and the count of factorizing lanes whose residual is
 // above `threshold` (nActive[2]): the correction solve of a refinement step runs only when some lane needs it.
 void launchResidualCheck(const DevNet& net, const DevBatch& b, double threshold, cudaStream_t st);
+// The dense front of a dense-front plan (after every factorization level); no-op without a front.  prepareDenseFront
+// raises the kernels' dynamic shared-memory limit for a front of F pivots on the current device.
+void launchDenseFront(const DevNet& net, const DevBatch& b, bool fp32, cudaStream_t st);
+cudaError_t prepareDenseFront(int F);
 
 }  // namespace olfb200

@@ -529,7 +529,9 @@ void buildBlockPlan(Structure& s, int ordering) {
         p.aPtr[a + 1] = static_cast<int>(p.aCol.size());
     }
     p.deferredL = (ordering & PLAN_DEFERRED_L) != 0;
-    ordering &= ~PLAN_DEFERRED_L;
+    const bool denseFront = (ordering & PLAN_DENSE_FRONT) != 0;
+    if (p.deferredL && denseFront) fail("the deferred-L and dense-front plans cannot be combined");
+    ordering &= ~(PLAN_DEFERRED_L | PLAN_DENSE_FRONT);
     // ordering
     if (ordering == ORDER_NATURAL) {
         p.perm.resize(nb);
@@ -639,12 +641,55 @@ void buildBlockPlan(Structure& s, int ordering) {
             }
         }
     }
+    // dense front: the largest trailing set of positions (<= MAX_FRONT) whose blocks are all present
+    p.opOuterEnd.assign(nLu, 0);
+    for (int id = 0; id < nLu; id++) p.opOuterEnd[id] = p.opPtr[id + 1];
+    p.frontStart = nb;
+    p.frontF = 0;
+    p.frontBlocks.clear();
+    if (denseFront) {
+        int F = 0;
+        for (int f = std::min(MAX_FRONT, nb); f >= 2; f--) {
+            const int k0 = nb - f;
+            bool dense = true;
+            for (int k = k0; k < nb && dense; k++) {
+                // U row k holds the diagonal and every later position; L column k every later position
+                dense = p.uPtr[k + 1] - p.uPtr[k] == nb - k && p.lPtr[k + 1] - p.lPtr[k] == nb - 1 - k;
+            }
+            if (dense) {
+                F = f;
+                break;
+            }
+        }
+        if (F >= 4) {
+            p.frontF = F;
+            p.frontStart = nb - F;
+            p.frontBlocks.assign(static_cast<size_t>(F) * F, -1);
+            for (int i = 0; i < F; i++)
+                for (int j = 0; j < F; j++) {
+                    const int a = p.frontStart + i, b = p.frontStart + j;
+                    p.frontBlocks[static_cast<size_t>(i) * F + j] = a <= b ? uBlock(a, b) : lBlock(a, b);
+                }
+            // a front block's task keeps the prefix of its updates whose pivot precedes the front (pivots ascend)
+            std::vector<int> uRow(p.nU);
+            for (int k = 0; k < nb; k++)
+                for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) uRow[t] = k;
+            for (int id : p.frontBlocks) {
+                int q = p.opPtr[id];
+                while (q < p.opPtr[id + 1] && uRow[p.opU[q]] < p.frontStart) q++;
+                p.opOuterEnd[id] = q;
+            }
+        }
+    }
+    std::vector<char> inFront(nLu, 0);
+    for (int id : p.frontBlocks) inFront[id] = 1;
     // levels: a task runs one level after every block its updates read (L~, U and the pivot's inverted diagonal);
     // unscaled L blocks do not wait for their own column's pivot, which halves the dependency chain
     p.level.assign(nLu, 0);
     int maxLevel = 0;
     auto levelOf = [&](int id, int lv) {
-        for (int q = p.opPtr[id]; q < p.opPtr[id + 1]; q++) {
+        if (inFront[id]) lv = 0;   // a front block's partial sum waits for nothing in the front
+        for (int q = p.opPtr[id]; q < p.opOuterEnd[id]; q++) {
             int dep = std::max(p.level[p.opL[q]], p.level[p.opU[q]]);
             if (p.opD[q] >= 0) dep = std::max(dep, p.level[p.opD[q]]);
             lv = std::max(lv, dep + 1);

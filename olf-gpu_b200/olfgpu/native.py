@@ -42,7 +42,7 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
 # Schedules of the Newton iterations
 LEVELS, PERSISTENT, COOPERATIVE, AUTOTUNE = 0, 1, 2, -1
 # Structure orderings (0 minimum degree, 1 nested dissection, 2 natural) and the deferred-L plan flag
-MIN_DEGREE, NESTED_DISSECTION, NATURAL, PLAN_DEFERRED_L = 0, 1, 2, 8
+MIN_DEGREE, NESTED_DISSECTION, NATURAL, PLAN_DEFERRED_L, PLAN_DENSE_FRONT = 0, 1, 2, 8, 16
 
 
 class NativeError(RuntimeError):

@@ -376,3 +376,34 @@ def test_cooperative_sweeps_match_level_launches(engine_lib, precision):
         ctx.set_schedule(sched, 0, 512 if sched == 2 else 256)
         res.append(ctx.solve(p.x_base, p.target, p.base_row_mode, dis).copy())
     assert np.array_equal(res[0], res[1])
+
+
+@pytest.mark.parametrize("schedule,lanes,threads", [(0, 2, 256), (0, 0, 256), (2, 0, 512)])
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", ["grid2000", "grid9241"])
+def test_dense_front_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes, threads, precision, name):
+    """The dense-front plan (the trailing dense block factorized in shared memory) gives the oracle's statuses and
+    states, with fewer dependency levels."""
+    from olfgpu import native, synthetic
+    g, p = grid(name)
+    outs = synthetic.draw_outages(g, 64, seed=96)
+    dis = p.outage_masks(outs)
+    s = native.Structure(p, ordering=native.PLAN_DENSE_FRONT)
+    assert s.factor_levels < native.Structure(p).factor_levels
+    ctx = native.BatchContext(s, outs.shape[0])
+    ctx.set_linear_solver_settings(precision, 1)
+    ctx.set_schedule(schedule, lanes, threads)
+    r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
+    _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n)
+
+
+def test_dense_front_plan_rejected_by_tiles(engine_lib):
+    from olfgpu import native
+    p = grid("grid2000")[1]
+    s = native.Structure(p, ordering=native.PLAN_DENSE_FRONT)
+    ctx = native.BatchContext(s, 4)
+    ctx.set_schedule(native.PERSISTENT, 2, 256)
+    with pytest.raises(native.NativeError, match="dense-front"):
+        ctx.solve(p.x_base, p.target, p.base_row_mode, np.zeros((4, p.n_elements), np.uint8))
+    with pytest.raises(native.NativeError, match="dense-front"):
+        native.MultiContext([ctx])
