@@ -488,9 +488,10 @@ def main():
                     help="start states: the base case, or the learned warm start (default when its checkpoint exists)")
     ap.add_argument("--checkpoint", default=CHECKPOINT)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
-    ap.add_argument("--plan", default="scaled", choices=["scaled", "deferred", "dense"],
-                    help="block-LU plan: L scaled at its task (default), deferred (half the levels) or dense (the "
-                         "trailing dense block factorized in shared memory)")
+    ap.add_argument("--plan", default=None, choices=["scaled", "deferred", "dense"],
+                    help="block-LU plan: L scaled at its task, deferred (half the levels) or dense (the trailing "
+                         "block factorized in shared memory; default for the N-1 workload, whose autotuned schedules "
+                         "all run it); the uneven workload's persistent launch runs the scaled plan")
     ap.add_argument("--schedule", default="auto", choices=["auto", "levels", "coop"],
                     help="auto: the engine's autotuner picks the Newton-iteration schedule on the first solve")
     ap.add_argument("--outages", type=int, default=N_OUTAGES,
@@ -498,6 +499,8 @@ def main():
     ap.add_argument("--workload", default="n1", choices=["n1", "uneven"],
                     help="n1: the 9,241-bus N-1 batch (default); uneven: four grids in one persistent launch")
     args = ap.parse_args()
+    if args.plan is None:
+        args.plan = "scaled" if args.workload == "uneven" else "dense"
     if args.start is None:
         args.start = "learned" if os.path.exists(args.checkpoint) and args.outages == N_OUTAGES else "base"
     args.warmup = max(args.warmup, 3) if args.impl == "engine" else args.warmup

@@ -81,7 +81,8 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     }
     // dense front: a front block's level task applies its updates from before the front and stores the partial sum
     // (diag -3: no inversion, no scaling); the dense front kernel finishes it
-    for (int id : p.frontBlocks) task[id] = Task{p.luToA[id], p.opPtr[id], p.opOuterEnd[id], -3};
+    for (int id : p.frontBlocks)
+        if (id >= 0) task[id] = Task{p.luToA[id], p.opPtr[id], p.opOuterEnd[id], -3};
     // L blocks by row position (for the forward solve), ascending column position
     std::vector<std::vector<int2>> lr(nb);
     for (int k = 0; k < nb; k++)

@@ -1,5 +1,5 @@
-// Dense front of the block LU: the trailing F pivots of the elimination order whose blocks are all present (the root
-// separators at the top of the elimination tree) factorized in shared memory, G lanes per CTA, instead of one
+// Dense front of the block LU: the trailing F pivots of the elimination order (the root separators at the top of the
+// elimination tree; absent blocks are structural zeros) factorized in shared memory, G lanes per CTA, instead of one
 // dependency level per step.  The level tasks of the front blocks have already applied every update from the pivots
 // before the front (in ascending pivot order); the front continues right-looking in ascending pivot order, so every
 // block sees its updates in the same order as the left-looking level tasks, with the same 2x2 expressions.
@@ -25,8 +25,14 @@ __global__ void __launch_bounds__(256) denseFrontKernel(DevNet net, DevBatch b, 
         const int g = idx % G, blk = idx / G, i = blk / F, j = blk % F;
         const int s = s0 + g;
         if (s >= b.S) continue;
-        const T* p = lu + (size_t)net.frontBlocks[blk] * 4 * S + s;
+        const int id = net.frontBlocks[blk];
         T* m = M + (size_t)g * N * LD;
+        if (id < 0) {   // a structural zero of the front stays an exact zero through the elimination
+            m[(2 * i) * LD + 2 * j] = m[(2 * i) * LD + 2 * j + 1] = 0;
+            m[(2 * i + 1) * LD + 2 * j] = m[(2 * i + 1) * LD + 2 * j + 1] = 0;
+            continue;
+        }
+        const T* p = lu + (size_t)id * 4 * S + s;
         m[(2 * i) * LD + 2 * j] = p[0];
         m[(2 * i) * LD + 2 * j + 1] = p[S];
         m[(2 * i + 1) * LD + 2 * j] = p[2 * S];
@@ -112,8 +118,9 @@ __global__ void __launch_bounds__(256) denseFrontKernel(DevNet net, DevBatch b, 
     for (int idx = threadIdx.x; idx < G * F * F; idx += blockDim.x) {
         const int g = idx % G, blk = idx / G, i = blk / F, j = blk % F;
         const int s = s0 + g;
-        if (s >= b.S || !frontSolving(b, s)) continue;
-        T* p = lu + (size_t)net.frontBlocks[blk] * 4 * S + s;
+        const int id = net.frontBlocks[blk];
+        if (s >= b.S || id < 0 || !frontSolving(b, s)) continue;
+        T* p = lu + (size_t)id * 4 * S + s;
         const T* m = M + (size_t)g * N * LD;
         p[0] = m[(2 * i) * LD + 2 * j];
         p[S] = m[(2 * i) * LD + 2 * j + 1];

@@ -641,67 +641,85 @@ void buildBlockPlan(Structure& s, int ordering) {
             }
         }
     }
-    // dense front: the largest trailing set of positions (<= MAX_FRONT) whose blocks are all present
+    // dense front: the trailing F positions (a multiple of 8, <= MAX_FRONT) chosen to leave the fewest dependency
+    // levels; its absent blocks are structural zeros (they stay exact zeros in the dense elimination)
     p.opOuterEnd.assign(nLu, 0);
     for (int id = 0; id < nLu; id++) p.opOuterEnd[id] = p.opPtr[id + 1];
     p.frontStart = nb;
     p.frontF = 0;
     p.frontBlocks.clear();
-    if (denseFront) {
-        int F = 0;
-        for (int f = std::min(MAX_FRONT, nb); f >= 2; f--) {
-            const int k0 = nb - f;
-            bool dense = true;
-            for (int k = k0; k < nb && dense; k++) {
-                // U row k holds the diagonal and every later position; L column k every later position
-                dense = p.uPtr[k + 1] - p.uPtr[k] == nb - k && p.lPtr[k + 1] - p.lPtr[k] == nb - 1 - k;
+    std::vector<int> uRow(p.nU);
+    for (int k = 0; k < nb; k++)
+        for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) uRow[t] = k;
+    auto findBlock = [&](int a, int b) {   // LU block of positions (a, b), or -1 when structurally zero
+        if (a <= b) {
+            if (a == b) return p.uPtr[a];
+            auto lo = p.uCol.begin() + p.uPtr[a] + 1, hi = p.uCol.begin() + p.uPtr[a + 1];
+            auto it = std::lower_bound(lo, hi, b);
+            return it != hi && *it == b ? static_cast<int>(it - p.uCol.begin()) : -1;
+        }
+        auto lo = p.lRow.begin() + p.lPtr[b], hi = p.lRow.begin() + p.lPtr[b + 1];
+        auto it = std::lower_bound(lo, hi, a);
+        return it != hi && *it == a ? p.nU + static_cast<int>(it - p.lRow.begin()) : -1;
+    };
+    // levels of the plan with the front starting at position k0 (k0 = nb: no front); returns the level count
+    std::vector<int> lvl(nLu, 0);
+    auto levelsWith = [&](int k0, std::vector<int>& level) {
+        int mx = -1;
+        auto one = [&](int id, int lv, bool front) {
+            const int end = front ? p.opPtr[id] : p.opPtr[id + 1];
+            int q = p.opPtr[id];
+            for (; q < p.opPtr[id + 1]; q++) {
+                if (front && uRow[p.opU[q]] >= k0) break;   // a front block stops at the first pivot of the front
+                int dep = std::max(level[p.opL[q]], level[p.opU[q]]);
+                if (p.opD[q] >= 0) dep = std::max(dep, level[p.opD[q]]);
+                lv = std::max(lv, dep + 1);
             }
-            if (dense) {
-                F = f;
-                break;
+            (void)end;
+            level[id] = lv;
+            mx = std::max(mx, lv);
+        };
+        for (int k = 0; k < nb; k++) {
+            for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) one(t, 0, k >= k0 && p.uCol[t] >= k0);
+            for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++) {
+                const bool front = k >= k0 && p.lRow[t] >= k0;
+                one(p.nU + t, front || p.deferredL ? 0 : level[p.uPtr[k]] + 1, front);
             }
         }
-        if (F >= 4) {
+        return mx + 1;
+    };
+    if (denseFront) {
+        int bestF = 0;
+        double bestCost = levelsWith(nb, lvl);
+        for (int f = 8; f <= std::min(MAX_FRONT, nb / 2); f += 8) {
+            // a front step costs about a tenth of a level launch
+            const double cost = levelsWith(nb - f, lvl) + 0.1 * f;
+            if (cost < bestCost) {
+                bestCost = cost;
+                bestF = f;
+            }
+        }
+        if (bestF > 0) {
+            const int F = bestF;
             p.frontF = F;
             p.frontStart = nb - F;
             p.frontBlocks.assign(static_cast<size_t>(F) * F, -1);
             for (int i = 0; i < F; i++)
-                for (int j = 0; j < F; j++) {
-                    const int a = p.frontStart + i, b = p.frontStart + j;
-                    p.frontBlocks[static_cast<size_t>(i) * F + j] = a <= b ? uBlock(a, b) : lBlock(a, b);
-                }
+                for (int j = 0; j < F; j++)
+                    p.frontBlocks[static_cast<size_t>(i) * F + j] = findBlock(p.frontStart + i, p.frontStart + j);
             // a front block's task keeps the prefix of its updates whose pivot precedes the front (pivots ascend)
-            std::vector<int> uRow(p.nU);
-            for (int k = 0; k < nb; k++)
-                for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) uRow[t] = k;
             for (int id : p.frontBlocks) {
+                if (id < 0) continue;
                 int q = p.opPtr[id];
                 while (q < p.opPtr[id + 1] && uRow[p.opU[q]] < p.frontStart) q++;
                 p.opOuterEnd[id] = q;
             }
         }
     }
-    std::vector<char> inFront(nLu, 0);
-    for (int id : p.frontBlocks) inFront[id] = 1;
-    // levels: a task runs one level after every block its updates read (L~, U and the pivot's inverted diagonal);
-    // unscaled L blocks do not wait for their own column's pivot, which halves the dependency chain
+    // levels: a task runs one level after every block its updates read (L, U and, deferred-L, the pivot's inverse); a
+    // scaled L block waits for its column's pivot; a front block's partial sum waits for nothing in the front
     p.level.assign(nLu, 0);
-    int maxLevel = 0;
-    auto levelOf = [&](int id, int lv) {
-        if (inFront[id]) lv = 0;   // a front block's partial sum waits for nothing in the front
-        for (int q = p.opPtr[id]; q < p.opOuterEnd[id]; q++) {
-            int dep = std::max(p.level[p.opL[q]], p.level[p.opU[q]]);
-            if (p.opD[q] >= 0) dep = std::max(dep, p.level[p.opD[q]]);
-            lv = std::max(lv, dep + 1);
-        }
-        p.level[id] = lv;
-        maxLevel = std::max(maxLevel, lv);
-    };
-    for (int k = 0; k < nb; k++) {
-        for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) levelOf(t, 0);
-        // a scaled L block waits for its column's pivot
-        for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++) levelOf(p.nU + t, p.deferredL ? 0 : p.level[p.uPtr[k]] + 1);
-    }
+    const int maxLevel = levelsWith(p.frontStart, p.level) - 1;
     p.levelPtr.assign(maxLevel + 2, 0);
     for (int id = 0; id < nLu; id++) p.levelPtr[p.level[id] + 1]++;
     for (int l = 0; l <= maxLevel; l++) p.levelPtr[l + 1] += p.levelPtr[l];

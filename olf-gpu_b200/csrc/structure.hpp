@@ -39,9 +39,9 @@ struct BlockPlan {
     // column's pivot; one last pass scales every L block by its pivot's inverse.
     std::vector<int> opPtr, opL, opU, opD;   // per LU block (opD -1: the L block is already scaled)
     bool deferredL = false;
-    // Dense-front plan: positions frontStart .. nb-1 (frontF pivots, every block present); frontBlocks[i * F + j] is
-    // the LU block of front positions (i, j); a front block's level task applies only its updates from pivots before
-    // the front (opOuterEnd) and stores the partial sum, the dense front kernel does the rest.
+    // Dense-front plan: positions frontStart .. nb-1 (frontF pivots); frontBlocks[i * F + j] is the LU block of front
+    // positions (i, j), -1 for a structural zero; a front block's level task applies only its updates from pivots
+    // before the front (opOuterEnd) and stores the partial sum, the dense front kernel does the rest.
     int frontStart = 0, frontF = 0;
     std::vector<int> frontBlocks, opOuterEnd;
     std::vector<int> level;             // per LU block
@@ -73,10 +73,11 @@ Structure buildStructure(int n, int ncb, const double* cbPar, const int* cbIx, i
 // factor unscaled during the factorization (half the dependency levels, one more block read per update).
 enum Ordering { ORDER_MIN_DEGREE = 0, ORDER_NESTED_DISSECTION = 1, ORDER_NATURAL = 2 };
 constexpr int PLAN_DEFERRED_L = 8;
-// Plan flag: the trailing positions that form a fully dense block (at most MAX_FRONT pivots: the root separators of the
-// elimination tree) are factorized as one dense front in shared memory instead of one dependency level per step.
+// Plan flag: the trailing positions of the elimination order (at most MAX_FRONT pivots, the root separators of the
+// elimination tree, their absent blocks as structural zeros) are factorized as one dense front in shared memory
+// instead of one dependency level per step; the front size leaves the fewest levels.
 constexpr int PLAN_DENSE_FRONT = 16;
-constexpr int MAX_FRONT = 32;
+constexpr int MAX_FRONT = 48;
 
 void buildBlockPlan(Structure& s, int ordering);
 

@@ -40,7 +40,7 @@ class SecurityAnalysis:
     """Holds the structure and one context per chunk width, reused across calls (GpuBatchContextCache)."""
 
     def __init__(self, packed: Packed, precision: int = native.FP64, refinement_steps: int = 1,
-                 reactive_limits: bool = False, ordering: int = 0, max_chunk: int = 4096):
+                 reactive_limits: bool = False, ordering: int = native.PLAN_DENSE_FRONT, max_chunk: int = 4096):
         self.packed = packed
         self.structure = native.Structure(packed, ordering)
         self.precision = precision
