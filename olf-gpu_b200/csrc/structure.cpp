@@ -641,8 +641,8 @@ void buildBlockPlan(Structure& s, int ordering) {
             }
         }
     }
-    // dense front: the trailing F positions (a multiple of 8, <= MAX_FRONT) chosen to leave the fewest dependency
-    // levels; its absent blocks are structural zeros (they stay exact zeros in the dense elimination)
+    // dense front: the trailing F positions; an absent block would be a structural zero (an exact zero through the
+    // dense elimination)
     p.opOuterEnd.assign(nLu, 0);
     for (int id = 0; id < nLu; id++) p.opOuterEnd[id] = p.opPtr[id + 1];
     p.frontStart = nb;
@@ -689,15 +689,15 @@ void buildBlockPlan(Structure& s, int ordering) {
         return mx + 1;
     };
     if (denseFront) {
+        // the largest trailing block (<= MAX_FRONT pivots) with every block present: a front padded with structural
+        // zeros measured slower (more dense work, fewer resident CTAs) than the levels it removed
         int bestF = 0;
-        double bestCost = levelsWith(nb, lvl);
-        for (int f = 8; f <= std::min(MAX_FRONT, nb / 2); f += 8) {
-            // a front step costs about a tenth of a level launch
-            const double cost = levelsWith(nb - f, lvl) + 0.1 * f;
-            if (cost < bestCost) {
-                bestCost = cost;
-                bestF = f;
+        for (int f = std::min(MAX_FRONT, nb); f >= 4 && bestF == 0; f--) {
+            bool dense = true;
+            for (int k = nb - f; k < nb && dense; k++) {
+                dense = p.uPtr[k + 1] - p.uPtr[k] == nb - k && p.lPtr[k + 1] - p.lPtr[k] == nb - 1 - k;
             }
+            if (dense) bestF = f;
         }
         if (bestF > 0) {
             const int F = bestF;

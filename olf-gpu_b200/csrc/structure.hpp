@@ -73,11 +73,11 @@ Structure buildStructure(int n, int ncb, const double* cbPar, const int* cbIx, i
 // factor unscaled during the factorization (half the dependency levels, one more block read per update).
 enum Ordering { ORDER_MIN_DEGREE = 0, ORDER_NESTED_DISSECTION = 1, ORDER_NATURAL = 2 };
 constexpr int PLAN_DEFERRED_L = 8;
-// Plan flag: the trailing positions of the elimination order (at most MAX_FRONT pivots, the root separators of the
-// elimination tree, their absent blocks as structural zeros) are factorized as one dense front in shared memory
-// instead of one dependency level per step; the front size leaves the fewest levels.
+// Plan flag: the trailing positions of the elimination order whose blocks are all present (at most MAX_FRONT pivots,
+// the root separators of the elimination tree) are factorized as one dense front in shared memory instead of one
+// dependency level per step.
 constexpr int PLAN_DENSE_FRONT = 16;
-constexpr int MAX_FRONT = 48;
+constexpr int MAX_FRONT = 32;
 
 void buildBlockPlan(Structure& s, int ordering);
 
