@@ -174,7 +174,7 @@ __device__ void solveVBlock(const DevNet& net, const DevBatch& b, const T* lu, T
         }
         if (dir == 0) {
 #pragma unroll 4
-            for (int q = net.lrowPtr[i] + part; q < net.lrowPtr[i + 1]; q += P) {
+            for (int q = net.lrowPtr[i] + part; q < net.lrowEnd[i]; q += P) {
                 const int2 e = net.lrow[q];
                 T l00, l01, l10, l11;
                 ld4c(lu, (size_t)e.x, S, s, l00, l01, l10, l11);
@@ -219,15 +219,18 @@ __device__ void solveVBlock(const DevNet& net, const DevBatch& b, const T* lu, T
 }
 
 // rhs (from -F or from the refinement residual) -> forward levels -> backward levels -> dx (= or +=).
+// mode 0: everything; 1: rhs and the forward levels; 2: the backward levels and dx (a dense front solve between).
 template <typename T>
 __global__ void __launch_bounds__(512) solveCoopKernel(DevNet net, DevBatch b, const T* lu, T* w, CoopPlan cp,
-                                                       int fromResidual) {
+                                                       int fromResidual, int mode) {
     __shared__ T red[ROWS][2][32];
     cg::grid_group grid = cg::this_grid();
     const size_t S = b.S;
     const long long nthreads = (long long)gridDim.x * blockDim.x * blockDim.y;
     const long long gtid = ((long long)blockIdx.x * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
     const long long cells = (long long)net.nb * b.S;
+    const int vy = b.S / 32;
+    if (mode != 2) {
     for (long long c = gtid; c < cells; c += nthreads) {
         const int s = (int)(c % b.S), i = (int)(c / b.S);
         if (!coopSolving(b, s)) continue;
@@ -239,7 +242,6 @@ __global__ void __launch_bounds__(512) solveCoopKernel(DevNet net, DevBatch b, c
         w[(2 * (size_t)i + 1) * S + s] = (T)r1;
     }
     grid.sync();
-    const int vy = b.S / 32;
     for (int l = 0; l < cp.nFwd; l++) {
         const int first = cp.fwdPtr[l], count = cp.fwdPtr[l + 1] - first, P = cp.fwdSplit[l];
         const int vx = (count + ROWS / P - 1) / (ROWS / P);
@@ -247,6 +249,8 @@ __global__ void __launch_bounds__(512) solveCoopKernel(DevNet net, DevBatch b, c
             solveVBlock<T>(net, b, lu, w, cp.fwdPos, 0, first, count, P, vb % vx, vb / vx, red);
         grid.sync();
     }
+    }
+    if (mode == 1) return;
     for (int l = 0; l < cp.nBwd; l++) {
         const int first = cp.bwdPtr[l], count = cp.bwdPtr[l + 1] - first, P = cp.bwdSplit[l];
         const int vx = (count + ROWS / P - 1) / (ROWS / P);
@@ -294,13 +298,13 @@ cudaError_t factorCoopT(const DevNet& net, const DevBatch& b, T* lu, const CoopP
 
 template <typename T>
 cudaError_t solveCoopT(const DevNet& net, const DevBatch& b, const T* lu, T* w, const CoopPlan& cp, int fromResidual,
-                       cudaStream_t st) {
+                       int mode, cudaStream_t st) {
     static const int grid = coopGrid(solveCoopKernel<T>);
     if (grid <= 0) return cudaErrorLaunchOutOfResources;
     DevNet n2 = net;
     DevBatch b2 = b;
     CoopPlan c2 = cp;
-    void* args[] = {&n2, &b2, &lu, &w, &c2, &fromResidual};
+    void* args[] = {&n2, &b2, &lu, &w, &c2, &fromResidual, &mode};
     return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(solveCoopKernel<T>), dim3(grid), dim3(32, ROWS), args, 0,
                                        st);
 }
@@ -313,8 +317,18 @@ cudaError_t launchFactorCoop(const DevNet& net, const DevBatch& b, const CoopPla
 
 cudaError_t launchSolveCoop(const DevNet& net, const DevBatch& b, const CoopPlan& cp, bool fp32, bool fromResidual,
                             cudaStream_t st) {
-    return fp32 ? solveCoopT<float>(net, b, b.lu32, b.w32, cp, fromResidual ? 1 : 0, st)
-                : solveCoopT<double>(net, b, b.lu64, b.w64, cp, fromResidual ? 1 : 0, st);
+    const int fr = fromResidual ? 1 : 0;
+    if (net.frontF <= 0) {
+        return fp32 ? solveCoopT<float>(net, b, b.lu32, b.w32, cp, fr, 0, st)
+                    : solveCoopT<double>(net, b, b.lu64, b.w64, cp, fr, 0, st);
+    }
+    // dense-front plan: forward levels, the front's dense solves, backward levels
+    cudaError_t e = fp32 ? solveCoopT<float>(net, b, b.lu32, b.w32, cp, fr, 1, st)
+                         : solveCoopT<double>(net, b, b.lu64, b.w64, cp, fr, 1, st);
+    if (e != cudaSuccess) return e;
+    launchDenseFrontSolve(net, b, fp32, st);
+    return fp32 ? solveCoopT<float>(net, b, b.lu32, b.w32, cp, fr, 2, st)
+                : solveCoopT<double>(net, b, b.lu64, b.w64, cp, fr, 2, st);
 }
 
 }  // namespace olfb200

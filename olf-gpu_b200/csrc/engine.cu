@@ -125,6 +125,18 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     d->perm.upload(p.perm);
     d->iperm.upload(p.iperm);
     d->lrowPtr.upload(lrowPtr);
+    // forward-solve row ends: a dense-front row's level task stops at its first front column (the dense front solve
+    // applies the rest); lrow lists ascend in column
+    std::vector<int> lrowEnd(nb);
+    for (int i = 0; i < nb; i++) {
+        int q = lrowPtr[i + 1];
+        if (i >= p.frontStart) {
+            q = lrowPtr[i];
+            while (q < lrowPtr[i + 1] && lrow[q].y < p.frontStart) q++;
+        }
+        lrowEnd[i] = q;
+    }
+    d->lrowEnd.upload(lrowEnd);
     d->lrow.upload(lrow);
     d->uPtr.upload(p.uPtr);
     d->uCol.upload(p.uCol);
@@ -254,6 +266,7 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     v.perm = d->perm.as<int>();
     v.iperm = d->iperm.as<int>();
     v.lrowPtr = d->lrowPtr.as<int>();
+    v.lrowEnd = d->lrowEnd.as<int>();
     v.lrow = d->lrow.as<int2>();
     v.uPtr = d->uPtr.as<int>();
     v.uCol = d->uCol.as<int>();

@@ -70,7 +70,7 @@ struct DeviceNet {
     DeviceBuffer csrToAD;                         // the same map on the device
     DeviceBuffer nodeCol, sidePtr, side, cbPar, cbTrig, aPtr, aCol, aDiag, shPtr, shList, shPar, obPtr, obList, obPar;
     DeviceBuffer frontBlocks;
-    DeviceBuffer task, ops, levelTask, perm, iperm, lrowPtr, lrow, uPtr, uCol, fwdPos, bwdPos;
+    DeviceBuffer task, ops, levelTask, perm, iperm, lrowPtr, lrowEnd, lrow, uPtr, uCol, fwdPos, bwdPos;
     DeviceBuffer levelPtrD, levelLongestD, fwdPtrD, fwdLongestD, bwdPtrD, bwdLongestD, levelSplitD, fwdSplitD, bwdSplitD;
     CoopPlan coop{};
     PersistentPlan persistent{};

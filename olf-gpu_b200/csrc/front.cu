@@ -129,6 +129,81 @@ __global__ void __launch_bounds__(256) denseFrontKernel(DevNet net, DevBatch b, 
     }
 }
 
+// The triangular solves of the front positions, after the forward level tasks have applied every column before the
+// front: forward y_i -= L(i, k) y_k (k ascending), then backward x_i = inv(D_i) y_i and y_r -= U(r, i) x_i (i
+// descending), with the front's factor blocks and solution entries in shared memory.  In place on w.
+template <typename T>
+__global__ void __launch_bounds__(256) denseFrontSolveKernel(DevNet net, DevBatch b, const T* lu, T* w, int G) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* M = reinterpret_cast<T*>(smraw);
+    const int F = net.frontF, N = 2 * F, LD = 2 * F + 1, k0 = net.frontStart;
+    T* Y = M + (size_t)G * N * LD;   // [G][N]
+    const size_t S = b.S;
+    const int s0 = blockIdx.x * G;
+    for (int idx = threadIdx.x; idx < G * F * F; idx += blockDim.x) {
+        const int g = idx % G, blk = idx / G, i = blk / F, j = blk % F;
+        const int s = s0 + g;
+        const int id = net.frontBlocks[blk];
+        if (s >= b.S || id < 0) continue;
+        const T* p = lu + (size_t)id * 4 * S + s;
+        T* m = M + (size_t)g * N * LD;
+        m[(2 * i) * LD + 2 * j] = p[0];
+        m[(2 * i) * LD + 2 * j + 1] = p[S];
+        m[(2 * i + 1) * LD + 2 * j] = p[2 * S];
+        m[(2 * i + 1) * LD + 2 * j + 1] = p[3 * S];
+    }
+    for (int idx = threadIdx.x; idx < G * N; idx += blockDim.x) {
+        const int g = idx % G, r = idx / G, s = s0 + g;
+        if (s < b.S) Y[g * N + r] = w[(2 * (size_t)k0 + r) * S + s];
+    }
+    __syncthreads();
+    for (int k = 0; k < F; k++) {   // forward: the column of pivot k into the later rows
+        for (int idx = threadIdx.x; idx < G * (F - 1 - k); idx += blockDim.x) {
+            const int g = idx % G, i = k + 1 + idx / G, s = s0 + g;
+            if (s >= b.S || !frontSolving(b, s)) continue;
+            const T* m = M + (size_t)g * N * LD;
+            const T* l0 = m + (2 * i) * LD + 2 * k;
+            const T* l1 = l0 + LD;
+            T* y = Y + g * N;
+            const T y0 = y[2 * k], y1 = y[2 * k + 1];
+            y[2 * i] -= l0[0] * y0 + l0[1] * y1;
+            y[2 * i + 1] -= l1[0] * y0 + l1[1] * y1;
+        }
+        __syncthreads();
+    }
+    for (int i = F - 1; i >= 0; i--) {   // backward: pivot i, then its column of U into the earlier rows
+        if (threadIdx.x < G) {
+            const int g = threadIdx.x, s = s0 + g;
+            if (s < b.S && frontSolving(b, s)) {
+                const T* m = M + (size_t)g * N * LD;
+                const T* d0 = m + (2 * i) * LD + 2 * i;
+                const T* d1 = d0 + LD;
+                T* y = Y + g * N;
+                const T w0 = y[2 * i], w1 = y[2 * i + 1];
+                y[2 * i] = d0[0] * w0 + d0[1] * w1;
+                y[2 * i + 1] = d1[0] * w0 + d1[1] * w1;
+            }
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < G * i; idx += blockDim.x) {
+            const int g = idx % G, r = idx / G, s = s0 + g;
+            if (s >= b.S || !frontSolving(b, s)) continue;
+            const T* m = M + (size_t)g * N * LD;
+            const T* u0 = m + (2 * r) * LD + 2 * i;
+            const T* u1 = u0 + LD;
+            T* y = Y + g * N;
+            const T x0 = y[2 * i], x1 = y[2 * i + 1];
+            y[2 * r] -= u0[0] * x0 + u0[1] * x1;
+            y[2 * r + 1] -= u1[0] * x0 + u1[1] * x1;
+        }
+        __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < G * N; idx += blockDim.x) {
+        const int g = idx % G, r = idx / G, s = s0 + g;
+        if (s < b.S && frontSolving(b, s)) w[(2 * (size_t)k0 + r) * S + s] = Y[g * N + r];
+    }
+}
+
 template <typename T>
 constexpr int lanesPerCta() { return sizeof(T) == 8 ? 2 : 4; }
 
@@ -141,14 +216,38 @@ void frontT(const DevNet& net, const DevBatch& b, T* lu, cudaStream_t st) {
     denseFrontKernel<T><<<(b.S + G - 1) / G, 256, frontBytes<T>(net.frontF), st>>>(net, b, lu, G);
 }
 
+template <typename T>
+void frontSolveT(const DevNet& net, const DevBatch& b, const T* lu, T* w, cudaStream_t st) {
+    const int G = lanesPerCta<T>();
+    const size_t bytes = frontBytes<T>(net.frontF) + (size_t)G * 2 * net.frontF * sizeof(T);
+    denseFrontSolveKernel<T><<<(b.S + G - 1) / G, 256, bytes, st>>>(net, b, lu, w, G);
+}
+
 }  // namespace
 
 cudaError_t prepareDenseFront(int F) {
+    const int y64 = lanesPerCta<double>() * 2 * F * 8, y32 = lanesPerCta<float>() * 2 * F * 4;
     cudaError_t e = cudaFuncSetAttribute(denseFrontKernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)frontBytes<double>(F));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(denseFrontKernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)frontBytes<float>(F));
+    if (e == cudaSuccess) {
+        e = cudaFuncSetAttribute(denseFrontKernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)frontBytes<float>(F));
+    }
+    if (e == cudaSuccess) {
+        e = cudaFuncSetAttribute(denseFrontSolveKernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)frontBytes<double>(F) + y64);
+    }
+    if (e == cudaSuccess) {
+        e = cudaFuncSetAttribute(denseFrontSolveKernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)frontBytes<float>(F) + y32);
+    }
+    return e;
+}
+
+void launchDenseFrontSolve(const DevNet& net, const DevBatch& b, bool fp32, cudaStream_t st) {
+    if (net.frontF <= 0) return;
+    if (fp32) frontSolveT<float>(net, b, b.lu32, b.w32, st);
+    else frontSolveT<double>(net, b, b.lu64, b.w64, st);
 }
 
 void launchDenseFront(const DevNet& net, const DevBatch& b, bool fp32, cudaStream_t st) {

@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(1024) forwardLevelKernel(DevNet net, DevBatch 
             w1 = w[(2 * (size_t)i + 1) * S + s];
         }
 #pragma unroll 4
-        for (int q = net.lrowPtr[i] + part; q < net.lrowPtr[i + 1]; q += P) {
+        for (int q = net.lrowPtr[i] + part; q < net.lrowEnd[i]; q += P) {
             const int2 e = net.lrow[q];
             T l00, l01, l10, l11;
             load4(lu, (size_t)e.x, S, s, l00, l01, l10, l11);
@@ -689,6 +689,7 @@ static void solveT(const DevNet& net, const DevBatch& b, T* w, const T* lu, cons
         OLF_SPLIT_DISPATCH(fwd.split[l], forwardLevelKernel, T, net, b, lu, w, fwd.pos, first, count)
     }
     if (hybrid) launchSolveRange(net, b, hybrid->plan, 0, fwdWide, fwd.levels, hybrid->lanes, fp32, st);
+    launchDenseFrontSolve(net, b, fp32, st);   // dense-front plans: the front rows, forward then backward
     const int bwdNarrow = hybrid ? hybrid->bwdUntil : 0;
     if (hybrid) launchSolveRange(net, b, hybrid->plan, 1, 0, bwdNarrow, hybrid->lanes, fp32, st);
     for (int l = bwdNarrow; l < bwd.levels; l++) {

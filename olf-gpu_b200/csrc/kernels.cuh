@@ -68,6 +68,7 @@ struct DevNet {
     const int* perm;          // position -> node
     const int* iperm;         // node -> position
     const int* lrowPtr;       // [nb + 1] L blocks of each row position
+    const int* lrowEnd;       // [nb] end of a row's forward-solve entries (a front row stops before the front columns)
     const int2* lrow;         // (L block id, column position)
     const int* uPtr;          // [nb + 1] U blocks of each row position (diagonal first: holds the inverse)
     const int* uCol;          // column position of each U block
@@ -208,6 +209,8 @@ void launchResidualCheck(const DevNet& net, const DevBatch& b, double threshold,
 // The dense front of a dense-front plan (after every factorization level); no-op without a front.  prepareDenseFront
 // raises the kernels' dynamic shared-memory limit for a front of F pivots on the current device.
 void launchDenseFront(const DevNet& net, const DevBatch& b, bool fp32, cudaStream_t st);
+// The front positions' forward and backward solves (between the forward and the backward level sweeps).
+void launchDenseFrontSolve(const DevNet& net, const DevBatch& b, bool fp32, cudaStream_t st);
 cudaError_t prepareDenseFront(int F);
 
 }  // namespace olfb200

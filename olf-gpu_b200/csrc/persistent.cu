@@ -202,7 +202,7 @@ __device__ void solveLevels(const DevNet& net, const DevBatch& b, const T* lu, T
                     w1 = w[(2 * (size_t)i + 1) * S + s];
                 }
                 if (dir == 0) {
-                    for (int q = net.lrowPtr[i] + part; q < net.lrowPtr[i + 1]; q += P) {
+                    for (int q = net.lrowPtr[i] + part; q < net.lrowEnd[i]; q += P) {
                         const int2 e = net.lrow[q];
                         T l00, l01, l10, l11;
                         ld4(lu, (size_t)e.x, S, s, l00, l01, l10, l11);

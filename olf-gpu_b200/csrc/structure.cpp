@@ -728,21 +728,37 @@ void buildBlockPlan(Structure& s, int ordering) {
         std::vector<int> w(p.levelPtr.begin(), p.levelPtr.end() - 1);
         for (int id = 0; id < nLu; id++) p.levelTask[w[p.level[id]]++] = id;
     }
-    // solve levels: forward f(i) = 1 + max f(k) over k with i in struct(k); backward b(i) = 1 + max b(j), j in struct(i)
+    // solve levels: forward f(i) = 1 + max f(k) over k with i in struct(k); backward b(i) = 1 + max b(j), j in struct(i).
+    // With a dense front, a front position's forward level task only applies the columns before the front (the dense
+    // front solve does the rest), and the front positions are solved backward by the dense front before any level.
+    const int k0 = p.frontStart;
     std::vector<int> fl(nb, 0), bl(nb, 0);
-    for (int k = 0; k < nb; k++)
+    for (int k = 0; k < nb; k++) {
+        if (k >= k0) continue;
         for (int i : st[k]) fl[i] = std::max(fl[i], fl[k] + 1);
-    for (int i = nb - 1; i >= 0; i--)
-        for (int j : st[i]) bl[i] = std::max(bl[i], bl[j] + 1);
+    }
+    for (int i = nb - 1; i >= 0; i--) {
+        if (i >= k0) {
+            bl[i] = -1;
+            continue;
+        }
+        for (int j : st[i])
+            if (j < k0) bl[i] = std::max(bl[i], bl[j] + 1);
+    }
     auto group = [&](const std::vector<int>& lv, std::vector<int>& ptr, std::vector<int>& pos) {
-        int mx = 0;
-        for (int v : lv) mx = std::max(mx, v);
+        int mx = 0, cnt = 0;
+        for (int v : lv) {
+            mx = std::max(mx, v);
+            cnt += v >= 0;
+        }
         ptr.assign(mx + 2, 0);
-        for (int v : lv) ptr[v + 1]++;
+        for (int v : lv)
+            if (v >= 0) ptr[v + 1]++;
         for (int l = 0; l <= mx; l++) ptr[l + 1] += ptr[l];
-        pos.assign(lv.size(), 0);
+        pos.assign(cnt, 0);
         std::vector<int> w(ptr.begin(), ptr.end() - 1);
-        for (int i = 0; i < static_cast<int>(lv.size()); i++) pos[w[lv[i]]++] = i;
+        for (int i = 0; i < static_cast<int>(lv.size()); i++)
+            if (lv[i] >= 0) pos[w[lv[i]]++] = i;
     };
     group(fl, p.fwdLevelPtr, p.fwdLevelPos);
     group(bl, p.bwdLevelPtr, p.bwdLevelPos);
