@@ -124,6 +124,8 @@ def run_engine(args, rank: int, world: int):
         ctx.set_schedule(native.AUTOTUNE)           # the first (warm-up) solve times the candidates
     elif args.schedule == "coop":
         ctx.set_schedule(native.COOPERATIVE, 0, 512)
+    elif args.schedule == "shared":
+        ctx.set_schedule(native.LEVELS_SHARED, 2, 256)
     # host inputs in pinned memory (e2e copies them every step); results read back to pinned memory
     dis = torch.from_numpy(p.outage_masks(outs)).pin_memory().numpy()
     out = torch.empty((ns, p.n + 3), dtype=torch.float64).pin_memory().numpy()
@@ -177,6 +179,7 @@ def run_engine(args, rank: int, world: int):
             tot_iters += int(tot.sum())
     fallbacks = int(ctx.last_fallbacks().size) if learned is not None else 0
     torch.cuda.synchronize()
+    result = out.copy()                         # the last timed solve's states, iterations and statuses
     dev = float(np.mean(dev_ms))
     e2e = float(np.mean(wall_ms))
     if world > 1:
@@ -184,20 +187,37 @@ def run_engine(args, rank: int, world: int):
         t = torch.tensor([dev, e2e], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev, e2e = float(t[0]), float(t[1])
-    # the plain FP64 engine from the base start on the same batch (the comparison the metric names)
-    plain = None
-    if not args.no_plain:
-        ctx64 = native.BatchContext(s, ns)
+
+    def comparison(prec, refine):
+        """The engine from the base start on the same batch at another precision: device time per step, and each
+        scenario's difference from the measured configuration's result (scenarios both converged)."""
+        c = native.BatchContext(s, ns)
+        c.set_linear_solver_settings(prec, refine)
         if args.schedule == "auto":
-            ctx64.set_schedule(native.AUTOTUNE)
+            c.set_schedule(native.AUTOTUNE)
         for _ in range(args.warmup):
-            ctx64.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
+            c.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
         pm = []
         for _ in range(args.steps):
-            ctx64.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
-            pm.append(ctx64.last_stats()[0])
-        plain = {"solves_per_s": round(ns / (float(np.mean(pm)) * 1e-3), 1), "ms_per_step": round(float(np.mean(pm)), 4)}
-        ctx64.close()
+            c.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
+            pm.append(c.last_stats()[0])
+        c.close()
+        both = (result[:, p.n + 2] == 0) & (out[:, p.n + 2] == 0)
+        d = np.abs(result[both, :p.n] - out[both, :p.n])
+        return {"solves_per_s": round(ns / (float(np.mean(pm)) * 1e-3), 1), "ms_per_step": round(float(np.mean(pm)), 4),
+                "vs_measured": {
+                    "max_abs_dVa_rad": float(d[:, 0::2].max()) if both.any() else None,
+                    "max_abs_dVm_pu": float(d[:, 1::2].max()) if both.any() else None,
+                    "same_status": int((result[:, p.n + 2] == out[:, p.n + 2]).sum()),
+                    "extra_iterations_per_solve": round(float(result[:, p.n].mean() - out[:, p.n].mean()), 4)}}
+
+    # the plain FP64 engine from the base start on the same batch (the comparison the metric names) and, with the
+    # learned start, the mixed-precision engine from the base start (what the start alone changes)
+    plain = mixed_base = None
+    if not args.no_plain:
+        plain = comparison(native.FP64, 0)
+        if learned is not None and precision == native.MIXED:
+            mixed_base = comparison(native.MIXED, refinement)
     # roofline of the Newton iterations (HBM-bound): algorithmic bytes over the device time
     peak, peak_kind = _peaks()
     pbytes = 4 if precision == native.MIXED else 8
@@ -226,8 +246,9 @@ def run_engine(args, rank: int, world: int):
         fact_achieved, fact_launch_ms, fact_bytes_launch, traffic = achieved, dev, total_bytes, None
     words = (ns + 31) // 32
     h2d = p.n * 8 * 2 + p.n * 4 + p.n_elements * words * 4
-    if learned is not None:   # node features, branch flows, outage indices, base state / identity rows / targets
-        h2d += p.n_bus * 16 * 4 + p.n_cb * 2 * 4 + ns * 4 + p.n * (8 + 1 + 8)
+    if learned is not None:   # outage indices and the compact rows (bus, scenario) of the outages' reach; the node
+        # features, flows and outage-free pass depend only on the base state and stay on the device between steps
+        h2d += ns * 4 + 2 * 4 * learned.reach(outs)[0].shape[0]
     d2h = ns * (p.n + 3) * 8
     conv = float((statuses == 0).mean())
     line = {
@@ -269,7 +290,9 @@ def run_engine(args, rank: int, world: int):
         "start": args.start,
         "lu_plan": args.plan,
         "schedule": dict(zip(["schedule", "lanes_per_tile", "threads"], ctx.schedule()[0])),
+        "autotune_ms": [[int(a), int(b_), int(c_), round(float(ms), 3)] for a, b_, c_, ms in ctx.schedule()[1]],
         "plain_fp64_base_start": plain,
+        "mixed_base_start": mixed_base,
         "learned_start": None if learned is None else {
             "checkpoint": os.path.relpath(args.checkpoint, ROOT), "prediction_ms_per_step": round(pred_total / args.steps, 4),
             "scenarios_on_base_start": fallbacks},
@@ -492,8 +515,9 @@ def main():
                     help="block-LU plan: L scaled at its task, deferred (half the levels) or dense (the trailing "
                          "block factorized in shared memory; default for the N-1 workload, whose autotuned schedules "
                          "all run it); the uneven workload's persistent launch runs the scaled plan")
-    ap.add_argument("--schedule", default="auto", choices=["auto", "levels", "coop"],
-                    help="auto: the engine's autotuner picks the Newton-iteration schedule on the first solve")
+    ap.add_argument("--schedule", default="auto", choices=["auto", "levels", "coop", "shared"],
+                    help="auto: the engine's autotuner picks the Newton-iteration schedule on the first solve; "
+                         "shared: level launches with the narrow factorization levels in shared memory")
     ap.add_argument("--outages", type=int, default=N_OUTAGES,
                     help="outages per GPU (500 is the benchmark; smaller batches are profiling cases)")
     ap.add_argument("--workload", default="n1", choices=["n1", "uneven"],

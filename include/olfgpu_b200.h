@@ -114,12 +114,16 @@ int olfgpu_last_fp64_refactors(int64_t context, unsigned char* flagged, int* cou
 /*
  * Schedule of the Newton iterations (no counterpart in the reference, which launches per dependency step and per
  * level and reads norms back every iteration): schedule 0 launches one kernel per wide dependency level over all
- * lanes and the narrow levels (<= 48 tasks) of each phase in one launch of tiles of lanesPerTile (1, 2 or 4; 0: one
- * launch per level throughout), captured as one CUDA graph per Newton iteration; schedule 1 runs the whole Newton
- * loop in one persistent launch, one CTA per tile of lanesPerTile (1, 2, 4 or 8) lanes with `threads` (256 or 512)
- * threads; schedule 2 runs each factorization and each solve as one cooperative launch over all lanes whose CTAs
- * meet at a grid barrier between dependency levels (tile arguments ignored); schedule -1 lets the next solve time every
- * candidate on its batch and keep the fastest (the autotuner).  olfgpu_get_schedule reports the schedule in force
+ * lanes and the narrow levels (<= 48 factorization tasks, <= 256 solve rows) of each phase in one launch of tiles of
+ * lanesPerTile (1, 2 or 4; 0: one launch per level throughout), captured as one CUDA graph per Newton iteration;
+ * schedule 1 runs the whole Newton loop in one persistent launch, one CTA per tile of lanesPerTile (1, 2, 4 or 8)
+ * lanes with `threads` (256 or 512) threads; schedule 2 runs each factorization and each solve as one cooperative
+ * launch over all lanes whose CTAs meet at a grid barrier between dependency levels (tile arguments ignored);
+ * schedule 3 is schedule 0 with the narrow factorization levels run in shared memory, one CTA of 256 threads per
+ * lane holding every LU block those levels
+ * produce (lanesPerTile then only sets the solves' narrow-level tiles; plans whose narrow levels do not fit, and
+ * deferred-L plans, fall back to schedule 0); schedule -1 lets the next solve time every candidate on its batch and
+ * keep the fastest (the autotuner).  olfgpu_get_schedule reports the schedule in force
  * and, after an autotuned solve, up to maxResults timings {schedule, lanesPerTile, threads, ms} into results
  * (nResults receives their count).
  */
@@ -271,12 +275,19 @@ int olfgpu_gnn_compose_start(int nScenarios, int nb, const float* pred, int ldPr
  * maps (sample, bus) to its row or -1, and a neighbour outside the rows reads the outage-free sample's PQbase row
  * (identical there).  olfgpu_gnn_message_forward_compact is olfgpu_gnn_message_forward on those rows, with the same
  * edges, order and arithmetic; olfgpu_gnn_compose_start_compact writes every scenario's start from the outage-free
- * prediction predBase [nb][ldPred], then its rows from predRows [R][ldPred].  Device pointers throughout.
+ * prediction predBase [nb][ldPred], then its rows from predRows [R][ldPred].  olfgpu_gnn_compact_inputs builds the
+ * rows' node inputs x [R][16] (BF16) from the outage-free inputs xBase [nb][16]: at an end of the scenario's outaged
+ * branch o (branchFrom[o], branchTo[o]) column nFeat is 1 and the next two hold flows[o][0..1] (float32), negated at
+ * the to end; it also sets rowOf[rowSample[r] * nb + rowNode[r]] = r (the caller fills rowOf with -1 first).  Device
+ * pointers throughout.
  */
 int olfgpu_gnn_message_forward_compact(int R, int nb, const int* rowNode, const int* rowSample, const int* rowOf,
                                        const int* inPtr, const int* inEdge, const int* edgeSrc, const int* edgeBranch,
                                        const int* outage, const void* PQ, const void* PQbase, const float* C,
                                        const float* bmsg, void* agg, void* stream);
+int olfgpu_gnn_compact_inputs(int R, int nb, int nFeat, const int* rowNode, const int* rowSample, const int* outage,
+                              const int* branchFrom, const int* branchTo, const void* xBase, const float* flows, void* x,
+                              int* rowOf, void* stream);
 int olfgpu_gnn_compose_start_compact(int nScenarios, int nb, const float* predBase, const float* predRows, int ldPred,
                                      int R, const int* rowNode, const int* rowSample, double stdVm, double stdVa,
                                      const double* xBase, const unsigned char* identity, const double* target,

@@ -221,9 +221,12 @@ extern "C" int olfgpu_set_schedule(int64_t context, int schedule, int lanesPerTi
             c.autotunePending = true;
             return;
         }
-        if (schedule != SCHEDULE_LEVELS && schedule != SCHEDULE_PERSISTENT && schedule != SCHEDULE_COOP) {
+        if (schedule != SCHEDULE_LEVELS && schedule != SCHEDULE_PERSISTENT && schedule != SCHEDULE_COOP &&
+            schedule != SCHEDULE_LEVELS_SHARED) {
             throw std::runtime_error("unknown schedule");
         }
+        c.regionFactor = schedule == SCHEDULE_LEVELS_SHARED;
+        if (c.regionFactor) schedule = SCHEDULE_LEVELS;
         if (schedule == SCHEDULE_COOP) {
             // cooperative sweeps have no tile parameters
         } else if (schedule == SCHEDULE_LEVELS) {
@@ -248,9 +251,10 @@ extern "C" int olfgpu_get_schedule(int64_t context, int* schedule, int* lanesPer
                                    double* results, int* nResults) {
     return guarded([&] {
         BatchContext& c = contextOf(context);
-        if (schedule) *schedule = c.schedule;
+        if (schedule) *schedule = c.schedule == SCHEDULE_LEVELS && c.regionFactor ? SCHEDULE_LEVELS_SHARED : c.schedule;
         if (lanesPerTile) *lanesPerTile = c.schedule == SCHEDULE_LEVELS ? c.narrowLanes : c.lanesPerTile;
-        if (threads) *threads = c.schedule == SCHEDULE_LEVELS ? 256 : c.threads;   // range kernels run 256 threads
+        // range kernels run 256 threads, as does the shared-memory factorization
+        if (threads) *threads = c.schedule == SCHEDULE_LEVELS ? 256 : c.threads;
         const int k = std::min<int>(maxResults, static_cast<int>(c.tuning.size()));
         for (int i = 0; results && i < k; i++) {
             results[4 * i] = c.tuning[i].schedule;

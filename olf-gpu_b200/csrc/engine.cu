@@ -120,7 +120,6 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     d->task.upload(task);
     std::vector<int4> ops(p.opL.size());
     for (size_t q = 0; q < ops.size(); q++) ops[q] = make_int4(p.opL[q], p.opU[q], p.opD[q], 0);
-    d->ops.upload(ops);
     d->levelTask.upload(p.levelTask);
     d->perm.upload(p.perm);
     d->iperm.upload(p.iperm);
@@ -204,12 +203,64 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     // the narrow levels: the factorization / forward tail and the backward head whose levels hold <= NARROW tasks
     constexpr int NARROW = 48;
     auto countOf = [](const std::vector<int>& ptr, size_t l) { return ptr[l + 1] - ptr[l]; };
-    d->factorFrom = static_cast<int>(p.levelPtr.size()) - 1;
+    // (a dense-front plan ends with the front's assembly level, wide whatever the tree above it: it stays a level
+    // launch after the range)
+    d->factorTo = static_cast<int>(p.levelPtr.size()) - 1 - (p.frontF > 0 ? 1 : 0);
+    d->factorFrom = d->factorTo;
     while (d->factorFrom > 0 && countOf(p.levelPtr, d->factorFrom - 1) <= NARROW) d->factorFrom--;
+    // the shared-memory region: the narrow factorization levels before factorTo whose blocks fit REGION_BYTES (FP64,
+    // one lane: two CTAs per SM); every block they produce gets a slot, in level order, and every update its operands'
+    // slots in ops.w (slot + 1 of the L block in the low 16 bits, of the U block in the high 16 bits, 0 outside).
+    // Deferred-L plans keep the range launches (their updates also read the pivot's inverse).
+    constexpr size_t REGION_BYTES = 110 * 1024;
+    d->regionFrom = d->factorTo;
+    if (!p.deferredL) {
+        d->regionFrom = d->factorFrom;
+        while (d->regionFrom < d->factorTo &&
+               static_cast<size_t>(p.levelPtr[d->factorTo] - p.levelPtr[d->regionFrom]) * 32 > REGION_BYTES) {
+            d->regionFrom++;
+        }
+    }
+    for (int l = d->regionFrom; l < d->factorTo; l++) {   // one round of the CTA per level
+        if (p.levelPtr[l + 1] - p.levelPtr[l] > REGION_THREADS) d->regionFrom = l + 1;
+    }
+    d->regionBase = p.levelPtr[d->regionFrom];
+    d->regionSlots = p.levelPtr[d->factorTo] - d->regionBase;
+    if (d->regionSlots > 0) {
+        std::vector<int> slotOf(nLu, -1);
+        for (int k = 0; k < d->regionSlots; k++) slotOf[p.levelTask[d->regionBase + k]] = k;
+        for (size_t q = 0; q < ops.size(); q++) {
+            ops[q].w = (slotOf[p.opL[q]] + 1) | ((slotOf[p.opU[q]] + 1) << 16);
+        }
+        // per slot: (task, end of its updates, first update with an operand in the region, pivot code: -2 pivot,
+        // -1 / -3 stored as summed, >= 0 the inverted pivot's block outside the region, <= -4 its slot -4 - code).
+        // A slot task's updates with both operands outside the region go first (each group in ascending pivot
+        // order): the prefix kernel applies them, coalesced over the lanes, before the region starts.
+        std::vector<int4> rtask(d->regionSlots);
+        for (int k = 0; k < d->regionSlots; k++) {
+            const int t = p.levelTask[d->regionBase + k];
+            const Task& tk = task[t];
+            std::stable_partition(ops.begin() + tk.opBegin, ops.begin() + tk.opEnd,
+                                  [](const int4& o) { return o.w == 0; });
+            int mid = tk.opBegin;
+            while (mid < tk.opEnd && ops[mid].w == 0) mid++;
+            int diag = tk.diag;
+            if (diag >= 0 && slotOf[diag] >= 0) diag = -4 - slotOf[diag];
+            rtask[k] = make_int4(t, tk.opEnd, mid, diag);
+        }
+        d->regionTask.upload(rtask);
+        // the limit for the largest region any plan can have (one process may hold several structures)
+        OLF_CUDA(prepareRegion(static_cast<int>(REGION_BYTES / 32), static_cast<int>(REGION_BYTES / 32)));
+    }
+    d->ops.upload(ops);
+    // the solves' range covers levels of up to NARROW_SOLVE positions: a solve level's tasks are light (one row of
+    // blocks each), so a tile walks a few hundred of them faster than a launch costs
+    constexpr int NARROW_SOLVE = 256;
     d->fwdFrom = static_cast<int>(p.fwdLevelPtr.size()) - 1;
-    while (d->fwdFrom > 0 && countOf(p.fwdLevelPtr, d->fwdFrom - 1) <= NARROW) d->fwdFrom--;
+    while (d->fwdFrom > 0 && countOf(p.fwdLevelPtr, d->fwdFrom - 1) <= NARROW_SOLVE) d->fwdFrom--;
     d->bwdUntil = 0;
-    while (d->bwdUntil < static_cast<int>(p.bwdLevelPtr.size()) - 1 && countOf(p.bwdLevelPtr, d->bwdUntil) <= NARROW) {
+    while (d->bwdUntil < static_cast<int>(p.bwdLevelPtr.size()) - 1 &&
+           countOf(p.bwdLevelPtr, d->bwdUntil) <= NARROW_SOLVE) {
         d->bwdUntil++;
     }
     d->bwdSplit.assign(p.bwdLevelPtr.size() - 1, 1);
@@ -239,7 +290,7 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     v.frontF = p.frontF;
     if (p.frontF > 0) {
         d->frontBlocks.upload(p.frontBlocks);
-        OLF_CUDA(prepareDenseFront(p.frontF));
+        OLF_CUDA(prepareDenseFront(MAX_FRONT));   // the largest front: the limit serves every structure
     }
     v.frontBlocks = d->frontBlocks.as<int>();
     v.ncb = s.ncb;
@@ -611,7 +662,8 @@ DevBatch fp64View(BatchContext& ctx) {
 }  // namespace
 
 void captureIteration(BatchContext& ctx) {
-    const int key = ctx.narrowLanes * 100000 + ctx.precision * 1000 + ctx.refinementSteps * 10 +
+    const int key = ctx.narrowLanes * 100000 + (ctx.regionFactor ? 50000 : 0) + ctx.precision * 1000 +
+                    ctx.refinementSteps * 10 +
                     (ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits ? 1 : 0);
     if (ctx.graph && ctx.graphKey == key) return;
     dropGraph(ctx.graph);
@@ -631,7 +683,7 @@ void captureIteration(BatchContext& ctx) {
     const bool rl = ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits;
     cudaStream_t st = ctx.stream;
     const Hybrid hy = ctx.hybrid();
-    const Hybrid* hp = ctx.narrowLanes > 0 ? &hy : nullptr;
+    const Hybrid* hp = ctx.useHybrid() ? &hy : nullptr;
     const int nLevels = static_cast<int>(dn.levelPtr.size()) - 1;
     // part 1: fill, test, reactive limits, lane counts
     ctx.graph = captureInto(st, [&] {
@@ -658,7 +710,7 @@ void captureIteration(BatchContext& ctx) {
             // one refinement step: the FP64 residual and its check, then (when a lane needs it) the correction solve
             ctx.graphResidual = captureInto(st, [&] {
                 launchResidual(net, b, st);
-                launchResidualCheck(net, b, REFINE_RESIDUAL * ctx.cfg.tol, st);
+                launchResidualCheck(net, b, REFINE_RESIDUAL * ctx.cfg.tol, ctx.cfg.refineBelow, st);
             });
             ctx.graphCorrect = captureInto(st, [&] { launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, st); });
         }
@@ -674,7 +726,7 @@ void launchFp64Redo(BatchContext& ctx) {
         const DeviceNet& dn = *ctx.net->dev;
         const DevBatch b64 = fp64View(ctx);
         const Hybrid hy = ctx.hybrid();
-        const Hybrid* hp = ctx.narrowLanes > 0 ? &hy : nullptr;
+        const Hybrid* hp = ctx.useHybrid() ? &hy : nullptr;
         cudaStream_t st = ctx.stream;
         ctx.graph64 = captureInto(st, [&] {
             launchFactor(dn.view, b64, dn.levelPtr.data(), dn.levelSplit.data(),
@@ -698,7 +750,7 @@ void factorPhase(BatchContext& ctx, const DevBatch& b, bool fp32) {
     }
     const Hybrid hy = ctx.hybrid();
     launchFactor(dn.view, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, fp32,
-                 ctx.narrowLanes > 0 ? &hy : nullptr, ctx.stream);
+                 ctx.useHybrid() ? &hy : nullptr, ctx.stream);
 }
 
 void solvePhase(BatchContext& ctx, const DevBatch& b, bool fp32, bool fromResidual) {
@@ -708,7 +760,7 @@ void solvePhase(BatchContext& ctx, const DevBatch& b, bool fp32, bool fromResidu
         return;
     }
     const Hybrid hy = ctx.hybrid();
-    launchSolve(dn.view, b, dn.fwd(), dn.bwd(), fp32, fromResidual, ctx.narrowLanes > 0 ? &hy : nullptr, ctx.stream);
+    launchSolve(dn.view, b, dn.fwd(), dn.bwd(), fp32, fromResidual, ctx.useHybrid() ? &hy : nullptr, ctx.stream);
 }
 
 // The refinement steps of a mixed-precision iteration, launched directly: FP64 residual, its per-lane check, and the
@@ -718,7 +770,7 @@ void refinementSteps(BatchContext& ctx, const DevBatch& b) {
     cudaStream_t st = ctx.stream;
     for (int r = 0; r < ctx.refinementSteps; r++) {
         launchResidual(dn.view, b, st);
-        launchResidualCheck(dn.view, b, REFINE_RESIDUAL * ctx.cfg.tol, st);
+        launchResidualCheck(dn.view, b, REFINE_RESIDUAL * ctx.cfg.tol, ctx.cfg.refineBelow, st);
         OLF_CUDA(cudaMemcpyAsync(ctx.hostActive + 2, static_cast<int*>(ctx.nActive.p) + 2, 4, cudaMemcpyDeviceToHost,
                                  st));
         OLF_CUDA(cudaStreamSynchronize(st));
@@ -989,6 +1041,9 @@ void autotune(BatchContext& ctx) {
     struct Candidate { int schedule, lanes, threads; };
     std::vector<Candidate> cands;
     for (int narrow : {0, 1, 2, 4}) cands.push_back({SCHEDULE_LEVELS, narrow, 256});
+    if (ctx.net->dev->regionSlots > 0) {
+        for (int narrow : {0, 2}) cands.push_back({SCHEDULE_LEVELS_SHARED, narrow, 256});
+    }
     cands.push_back({SCHEDULE_COOP, 0, 512});
     if (ctx.net->dev->view.frontF == 0) {   // the persistent tiles do not run dense-front plans
         for (int lanes : {2, 4})
@@ -1000,14 +1055,18 @@ void autotune(BatchContext& ctx) {
     float best = 1e30f;
     Candidate pick = cands[0];
     ctx.tuning.clear();
-    for (const Candidate& c : cands) {
-        ctx.schedule = c.schedule;
-        if (c.schedule == SCHEDULE_LEVELS) {
+    auto apply = [&](const Candidate& c) {
+        ctx.regionFactor = c.schedule == SCHEDULE_LEVELS_SHARED;
+        ctx.schedule = ctx.regionFactor ? SCHEDULE_LEVELS : c.schedule;
+        if (ctx.schedule == SCHEDULE_LEVELS) {
             ctx.narrowLanes = c.lanes;
         } else {
             ctx.lanesPerTile = c.lanes;
             ctx.threads = c.threads;
         }
+    };
+    for (const Candidate& c : cands) {
+        apply(c);
         installLanes(ctx);
         OLF_CUDA(cudaEventRecord(e0, ctx.stream));
         runIterations(ctx);
@@ -1023,13 +1082,7 @@ void autotune(BatchContext& ctx) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    ctx.schedule = pick.schedule;
-    if (pick.schedule == SCHEDULE_LEVELS) {
-        ctx.narrowLanes = pick.lanes;
-    } else {
-        ctx.lanesPerTile = pick.lanes;
-        ctx.threads = pick.threads;
-    }
+    apply(pick);
     ctx.autotunePending = false;
 }
 

@@ -74,7 +74,10 @@ struct DeviceNet {
     DeviceBuffer levelPtrD, levelLongestD, fwdPtrD, fwdLongestD, bwdPtrD, bwdLongestD, levelSplitD, fwdSplitD, bwdSplitD;
     CoopPlan coop{};
     PersistentPlan persistent{};
-    int factorFrom = 0, fwdFrom = 0, bwdUntil = 0;   // narrow-level boundaries of the level schedule
+    int factorFrom = 0, factorTo = 0, fwdFrom = 0, bwdUntil = 0;   // narrow-level boundaries of the level schedule
+    // shared-memory region of the narrow factorization levels [regionFrom, factorTo) (regionSlots 0: none)
+    int regionFrom = 0, regionBase = 0, regionSlots = 0;
+    DeviceBuffer regionTask;
 };
 
 struct NetStructure {
@@ -86,7 +89,9 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s);
 
 // Schedules of the Newton iterations: one launch per dependency level (captured in a CUDA graph per iteration), or
 // the persistent kernel with one CTA per lane tile running the whole loop.
-enum { SCHEDULE_LEVELS = 0, SCHEDULE_PERSISTENT = 1, SCHEDULE_COOP = 2 };
+// SCHEDULE_LEVELS_SHARED is an API value only: the level schedule with the narrow factorization levels in shared
+// memory (BatchContext::regionFactor).
+enum { SCHEDULE_LEVELS = 0, SCHEDULE_PERSISTENT = 1, SCHEDULE_COOP = 2, SCHEDULE_LEVELS_SHARED = 3 };
 
 // Mixed precision: a refinement step's correction solve runs only while some lane's FP64 residual max |r| is above
 // this fraction of the mismatch tolerance (below it the FP32 solve is already accurate enough for the test).
@@ -145,12 +150,20 @@ struct BatchContext {
     int threads = 512;
     bool autotunePending = false;
     int narrowLanes = 2;            // level schedule: lanes per tile of the narrow-level range launches (0: none)
+    bool regionFactor = false;      // level schedule: the narrow factorization levels in shared memory
     Hybrid hybrid() const {
         const DeviceNet& d = *net->dev;
-        Hybrid h{d.factorFrom, d.fwdFrom, d.bwdUntil, narrowLanes, d.persistent};
+        Hybrid h{d.factorFrom, d.factorTo, d.fwdFrom, d.bwdUntil, narrowLanes, d.persistent};
         h.plan.maxRounds = 1;
+        if (regionFactor && d.regionSlots > 0) {
+            h.regionFrom = d.regionFrom;
+            h.regionBase = d.regionBase;
+            h.regionSlots = d.regionSlots;
+            h.regionTask = d.regionTask.as<int4>();
+        }
         return h;
     }
+    bool useHybrid() const { return narrowLanes > 0 || regionFactor; }
     std::vector<TuningResult> tuning;
     DeviceBuffer out;               // [nS][n + 3] scenario-major results
     // reactive limits

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 #include <stdexcept>
 #include <string>
 
@@ -437,6 +438,38 @@ int gnnGuard(F&& f) {
 }
 }  // namespace
 
+// Node inputs of the compact rows: row r copies the outage-free inputs of its bus (16 BF16 columns, 32 B) and, at an
+// end of its scenario's outaged branch, sets the outage columns: flag 1 at column nFeat, the branch's base-case P and
+// Q flow (flows[o][0..1]) at the next two, negated at the to end.  rowOf[sample * nb + bus] = r (the entries of the
+// other buses are left as they are: -1, set by the caller).
+__global__ void compactInputsKernel(int R, int nb, int nFeat, const int* rowNode, const int* rowSample,
+                                    const int* outage, const int* branchFrom, const int* branchTo,
+                                    const __nv_bfloat16* xBase, const float* flows, __nv_bfloat16* x, int* rowOf) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= R) return;
+    const int b = rowNode[r];
+    const int sample = rowSample[r];
+    const int o = outage[sample];
+    rowOf[(size_t)sample * nb + b] = r;
+    const uint4* src = reinterpret_cast<const uint4*>(xBase + (size_t)b * 16);
+    uint4 lo = src[0], hi = src[1];
+    __nv_bfloat16 v[16];
+    memcpy(v, &lo, 16);
+    memcpy(v + 8, &hi, 16);
+    const bool atFrom = b == branchFrom[o], atTo = b == branchTo[o];
+    if (atFrom || atTo) {
+        const float sign = atTo ? -1.0f : 1.0f;
+        v[nFeat] = __float2bfloat16_rn(1.0f);
+        v[nFeat + 1] = __float2bfloat16_rn(sign * flows[2 * o]);
+        v[nFeat + 2] = __float2bfloat16_rn(sign * flows[2 * o + 1]);
+    }
+    memcpy(&lo, v, 16);
+    memcpy(&hi, v + 8, 16);
+    uint4* dst = reinterpret_cast<uint4*>(x + (size_t)r * 16);
+    dst[0] = lo;
+    dst[1] = hi;
+}
+
 // Learned start states of the buses in the compact set: x0[s][2b], x0[s][2b + 1] from the compact output row (the
 // identity rows keep their targets, already written by the full composition).
 __global__ void scatterStartKernel(int R, int nb, const int* rowNode, const int* rowSample, const float* pred, int ldp,
@@ -616,6 +649,18 @@ extern "C" int olfgpu_gnn_message_forward_compact(int R, int nb, const int* rowN
             R, nb, rowNode, rowSample, rowOf, inPtr, inEdge, edgeSrc, edgeBranch, outage,
             static_cast<const __nv_bfloat16*>(PQ), static_cast<const __nv_bfloat16*>(PQbase), C, bmsg,
             static_cast<__nv_bfloat16*>(agg));
+    });
+}
+
+extern "C" int olfgpu_gnn_compact_inputs(int R, int nb, int nFeat, const int* rowNode, const int* rowSample,
+                                         const int* outage, const int* branchFrom, const int* branchTo,
+                                         const void* xBase, const float* flows, void* x, int* rowOf, void* stream) {
+    return gnnGuard([&] {
+        if (R <= 0) return;
+        if (nFeat < 0 || nFeat + 3 > 16) throw std::invalid_argument("outage columns outside the 16 input columns");
+        compactInputsKernel<<<(R + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+            R, nb, nFeat, rowNode, rowSample, outage, branchFrom, branchTo, static_cast<const __nv_bfloat16*>(xBase),
+            flows, static_cast<__nv_bfloat16*>(x), rowOf);
     });
 }
 

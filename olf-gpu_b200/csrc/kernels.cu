@@ -519,7 +519,9 @@ __global__ void clearTroubleKernel(DevBatch b) {
 void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtr, const int* levelSplit, int nLevels,
                   bool fp32, const Hybrid* hybrid, cudaStream_t st) {
     clearTroubleKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b);
-    const int wide = hybrid ? hybrid->factorFrom : nLevels;
+    const bool region = hybrid && hybrid->regionSlots > 0;
+    const bool range = hybrid && !region && hybrid->lanes > 0;
+    const int wide = region ? hybrid->regionFrom : range ? hybrid->factorFrom : nLevels;
     for (int l = 0; l < wide; l++) {
         const int first = levelPtr[l], count = levelPtr[l + 1] - levelPtr[l];
         if (count == 0) continue;
@@ -529,9 +531,19 @@ void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtr, con
             OLF_SPLIT_DISPATCH(levelSplit[l], factorLevelKernel, double, net, b, b.lu64, first, count)
         }
     }
-    if (hybrid) {
-        // the range kernel ends with the L scaling pass of its tiles
-        launchFactorRange(net, b, hybrid->plan, wide, nLevels, hybrid->lanes, fp32, st);
+    if (region || range) {
+        // the range kernel ends with the L scaling pass of its tiles (a deferred-L plan has no front and no region)
+        if (region) launchRegionFactor(net, b, *hybrid, fp32, st);
+        else launchFactorRange(net, b, hybrid->plan, wide, hybrid->factorTo, hybrid->lanes, fp32, st);
+        for (int l = hybrid->factorTo; l < nLevels; l++) {
+            const int first = levelPtr[l], count = levelPtr[l + 1] - levelPtr[l];
+            if (count == 0) continue;
+            if (fp32) {
+                OLF_SPLIT_DISPATCH(levelSplit[l], factorLevelKernel, float, net, b, b.lu32, first, count)
+            } else {
+                OLF_SPLIT_DISPATCH(levelSplit[l], factorLevelKernel, double, net, b, b.lu64, first, count)
+            }
+        }
     } else if (net.deferredL) {
         const int nL = net.nLu - net.nU;
         dim3 blk(32, 8), grd((nL + 7) / 8, b.S / 32);
@@ -683,6 +695,7 @@ static void solveT(const DevNet& net, const DevBatch& b, T* w, const T* lu, cons
     const size_t all = (size_t)net.nb * b.S;
     const bool fp32 = sizeof(T) == 4;
     rhsKernel<T><<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b, w, fromResidual);
+    if (hybrid && hybrid->lanes <= 0) hybrid = nullptr;   // no range launches in the solves
     const int fwdWide = hybrid ? hybrid->fwdFrom : fwd.levels;
     for (int l = 0; l < fwdWide; l++) {
         const int first = fwd.ptr[l], count = fwd.ptr[l + 1] - fwd.ptr[l];
@@ -827,12 +840,14 @@ __global__ void residualMaxKernel(DevNet net, DevBatch b) {
     }
 }
 
-__global__ void countResidualKernel(DevBatch b, double threshold) {
+// Lanes near convergence (max |F| below refineBelow) whose linear residual is above the threshold: a lane further
+// out takes another Newton step anyway, and its FP32 solve error shrinks with its mismatch.
+__global__ void countResidualKernel(DevBatch b, double threshold, double refineBelow) {
     __shared__ int part[32];
     int c = 0;
     for (int s = threadIdx.x; s < b.S; s += blockDim.x) {
         const double r = __longlong_as_double((long long)b.resNorm[s]);
-        c += (b.active[s] && !b.pending[s] && !(r <= threshold)) ? 1 : 0;
+        c += (b.active[s] && !b.pending[s] && b.normOut[s] < refineBelow && !(r <= threshold)) ? 1 : 0;
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
     if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
@@ -844,10 +859,11 @@ __global__ void countResidualKernel(DevBatch b, double threshold) {
     }
 }
 
-void launchResidualCheck(const DevNet& net, const DevBatch& b, double threshold, cudaStream_t st) {
+void launchResidualCheck(const DevNet& net, const DevBatch& b, double threshold, double refineBelow,
+                         cudaStream_t st) {
     cudaMemsetAsync(b.resNorm, 0, sizeof(unsigned long long) * b.S, st);
     residualMaxKernel<<<dim3(b.S / 32, 64), dim3(32, 8), 0, st>>>(net, b);
-    countResidualKernel<<<1, 1024, 0, st>>>(b, threshold);
+    countResidualKernel<<<1, 1024, 0, st>>>(b, threshold, refineBelow);
 }
 
 void launchStep(const DevNet& net, const DevBatch& b, bool, cudaStream_t st) {

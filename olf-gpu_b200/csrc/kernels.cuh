@@ -176,12 +176,25 @@ void launchFactorRange(const DevNet& net, const DevBatch& b, const PersistentPla
 void launchSolveRange(const DevNet& net, const DevBatch& b, const PersistentPlan& plan, int dir, int l0, int l1,
                       int lanes, bool fp32, cudaStream_t st);
 
-// The narrow levels of the level schedule run as one range launch per phase: factorization levels >= factorFrom,
-// forward levels >= fwdFrom, backward levels < bwdUntil, in tiles of `lanes` lanes.
+// The narrow levels of the level schedule run as one range launch per phase: factorization levels [factorFrom,
+// factorTo), forward levels >= fwdFrom, backward levels < bwdUntil, in tiles of `lanes` lanes (0: no range launches).
+// Factorization levels from factorTo on (the dense front's assembly level) are launched level by level after the
+// range.  With regionSlots > 0 the factorization levels [regionFrom, factorTo) run in shared memory instead
+// (launchRegionFactor): slot k holds the block of task levelTask[regionBase + k]; regionTask[k] = (task, end of its
+// updates, first update with an operand in the region, pivot code: -2 pivot, -1 / -3 stored as summed, >= 0 the
+// inverted pivot's block outside the region, <= -4 its slot -4 - code).
 struct Hybrid {
-    int factorFrom, fwdFrom, bwdUntil, lanes;
+    int factorFrom, factorTo, fwdFrom, bwdUntil, lanes;
     PersistentPlan plan;
+    int regionFrom = 0, regionBase = 0, regionSlots = 0;
+    const int4* regionTask = nullptr;
 };
+// The shared-memory factorization of the narrow levels (two launches; no-op when h.regionSlots == 0; every region
+// level holds at most REGION_THREADS tasks).  prepareRegion raises the kernel's dynamic shared-memory limit for nSlots
+// slots and nLevels levels on the current device.
+constexpr int REGION_THREADS = 256;
+void launchRegionFactor(const DevNet& net, const DevBatch& b, const Hybrid& h, bool fp32, cudaStream_t st);
+cudaError_t prepareRegion(int nSlots, int nLevels);
 
 // Level boundaries (host), the positions of each level (device) and the split factor of each level (host).
 struct LevelSchedule {
@@ -203,9 +216,10 @@ void launchIterationStart(const DevBatch& b, cudaStream_t st);
 void launchCountSolving(const DevBatch& b, double refineBelow, cudaStream_t st);
 // Factorizing lanes flagged for an FP64 refactor (nActive[3]).
 void launchCountFp64(const DevBatch& b, cudaStream_t st);
-// Mixed precision, after launchResidual: each lane's max |r| and the count of factorizing lanes whose residual is
-// above `threshold` (nActive[2]): the correction solve of a refinement step runs only when some lane needs it.
-void launchResidualCheck(const DevNet& net, const DevBatch& b, double threshold, cudaStream_t st);
+// Mixed precision, after launchResidual: each lane's max |r| and the count of factorizing lanes with max |F| below
+// refineBelow whose residual is above `threshold` (nActive[2]): the correction solve of a refinement step runs only
+// when some lane needs it.
+void launchResidualCheck(const DevNet& net, const DevBatch& b, double threshold, double refineBelow, cudaStream_t st);
 // The dense front of a dense-front plan (after every factorization level); no-op without a front.  prepareDenseFront
 // raises the kernels' dynamic shared-memory limit for a front of F pivots on the current device.
 void launchDenseFront(const DevNet& net, const DevBatch& b, bool fp32, cudaStream_t st);

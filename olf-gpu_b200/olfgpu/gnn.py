@@ -48,6 +48,7 @@ def _lib():
             "olfgpu_gnn_copy_cols": [i, i, vp, i, i, vp, i, i, i, vp],
             "olfgpu_gnn_compose_start": [i, i, vp, i, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp, vp],
             "olfgpu_gnn_message_forward_compact": [i, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp],
+            "olfgpu_gnn_compact_inputs": [i, i, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp],
             "olfgpu_gnn_compose_start_compact": [i, i, vp, vp, i, i, vp, vp, ctypes.c_double, ctypes.c_double, vp, vp,
                                                  vp, vp, vp],
         }

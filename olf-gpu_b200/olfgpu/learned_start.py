@@ -72,6 +72,7 @@ class LearnedStart:
         self._adj = None
         self._reach_cache = {}
         self._base_cache = {}
+        self._branch_ends = None
 
     # ------------------------------------------------------------------------------------------------------------
     def solve_base(self, g, x_start: np.ndarray) -> np.ndarray:
@@ -296,24 +297,20 @@ class LearnedStart:
         x0 = torch.empty((ns, p.n), dtype=torch.float64, device="cuda") if out is None else out
         std0, std1 = float(self.tgt_std[0]), float(self.tgt_std[1])
         if compact:
-            rn_h, rs_h, ro_h = self.reach(outages)
-            rn = torch.from_numpy(rn_h).cuda()
-            rs = torch.from_numpy(rs_h).cuda()
-            ro = torch.from_numpy(ro_h).cuda()
-            xc = xf[rn.long()].clone()
-            o_l = outs.long()[rs.long()]
-            fidx = torch.from_numpy(self.grid.f.astype(np.int64)).cuda()[o_l]
-            tidx = torch.from_numpy(self.grid.t.astype(np.int64)).cuda()[o_l]
-            flr = fl[o_l]
-            at_f, at_t = rn.long() == fidx, rn.long() == tidx
-            one = torch.ones((), device="cuda", dtype=xc.dtype)
-            xc[at_f, N_FEAT] = one
-            xc[at_t, N_FEAT] = one
-            xc[at_f, N_FEAT + 1] = flr[at_f, 0].to(xc.dtype)
-            xc[at_t, N_FEAT + 1] = (-flr[at_t, 0]).to(xc.dtype)
-            xc[at_f, N_FEAT + 2] = flr[at_f, 1].to(xc.dtype)
-            xc[at_t, N_FEAT + 2] = (-flr[at_t, 1]).to(xc.dtype)
-            rows_out = self.net.forward_rows(xc.contiguous(), outs, rows=(rn, rs, ro), base_pq=base_pq)
+            rn_h, rs_h, _ = self.reach(outages)
+            R = int(rn_h.shape[0])
+            # one host-to-device copy for the row lists; the (sample, bus) -> row map is written on the device
+            packed = torch.from_numpy(np.concatenate([rn_h, rs_h])).cuda()
+            rn, rs = packed[:R], packed[R:]
+            ro = torch.full((ns * nb,), -1, dtype=torch.int32, device="cuda")
+            if self._branch_ends is None:
+                self._branch_ends = (torch.from_numpy(self.grid.f.astype(np.int32)).cuda(),
+                                     torch.from_numpy(self.grid.t.astype(np.int32)).cuda())
+            xc = torch.empty((R, FEAT_IN), dtype=xf.dtype, device="cuda")
+            _call("olfgpu_gnn_compact_inputs", R, nb, N_FEAT, _ptr(rn), _ptr(rs), _ptr(outs),
+                  _ptr(self._branch_ends[0]), _ptr(self._branch_ends[1]), _ptr(xf), _ptr(fl), _ptr(xc), _ptr(ro),
+                  _stream())
+            rows_out = self.net.forward_rows(xc, outs, rows=(rn, rs, ro), base_pq=base_pq)
             _call("olfgpu_gnn_compose_start_compact", ns, nb, _ptr(base_out), _ptr(rows_out), base_out.shape[1],
                   int(rn.shape[0]), _ptr(rn), _ptr(rs), std0, std1, _ptr(xb), _ptr(ident), _ptr(tgt), _ptr(x0),
                   _stream())

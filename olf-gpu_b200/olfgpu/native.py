@@ -39,8 +39,9 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_get_multi_schedule", "olfgpu_solve_multi_context", "olfgpu_set_fallback_start",
            "olfgpu_last_fallbacks", "olfgpu_set_phase_timing", "olfgpu_last_phase_times", "olfgpu_structure_levels",
            "olfgpu_set_device_start", "olfgpu_set_mixed_precision_controls", "olfgpu_last_fp64_refactors"]
-# Schedules of the Newton iterations
-LEVELS, PERSISTENT, COOPERATIVE, AUTOTUNE = 0, 1, 2, -1
+# Schedules of the Newton iterations (LEVELS_SHARED: the level schedule with the narrow factorization levels in
+# shared memory)
+LEVELS, PERSISTENT, COOPERATIVE, LEVELS_SHARED, AUTOTUNE = 0, 1, 2, 3, -1
 # Structure orderings (0 minimum degree, 1 nested dissection, 2 natural) and the deferred-L plan flag
 MIN_DEGREE, NESTED_DISSECTION, NATURAL, PLAN_DEFERRED_L, PLAN_DENSE_FRONT = 0, 1, 2, 8, 16
 

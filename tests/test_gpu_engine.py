@@ -8,6 +8,14 @@ pytestmark = pytest.mark.gpu
 
 # converged states must agree within 1e-8 pu / rad, statuses exactly
 STATE_TOL = 1e-8
+# mixed precision against the FP64 oracle: the last Newton step of a lane comes from an FP32 solve, refined only when
+# its FP64 residual exceeds a tenth of the tolerance, so a converged state can sit a few 1e-8 from the FP64 answer
+# where |J^-1| is large; the statuses stay identical
+MIXED_STATE_TOL = 5e-8
+
+
+def _tol(precision):
+    return MIXED_STATE_TOL if precision == 1 else STATE_TOL
 
 
 def _perturbed_states(p, ns, seed, scale=0.05):
@@ -57,14 +65,14 @@ def test_linear_solve_matches_oracle(engine_lib, oracle_mod, precision, tol):
         assert np.max(np.abs(z[k] - zo)) / np.max(np.abs(zo)) < tol
 
 
-def _compare(res, ref, n):
+def _compare(res, ref, n, tol=STATE_TOL):
     st_e = res[:, n + 2].astype(int)
     st_o = ref[:, n + 2].astype(int)
     assert np.array_equal(st_e, st_o), f"status mismatch at {np.flatnonzero(st_e != st_o)[:10]}"
     conv = st_o == 0
     if conv.any():
         d = np.max(np.abs(res[conv, :n] - ref[conv, :n]))
-        assert d <= STATE_TOL, d
+        assert d <= tol, d
     return st_o
 
 
@@ -106,7 +114,7 @@ def test_n1_mixed_precision_matches_fp64_oracle(engine_lib, oracle_mod, steps):
     r = sa.solve_n1(outs)
     ref = oracle_mod.Structure(p).solve_batch(p.x_base, p.outage_masks(outs))
     out = np.concatenate([r.x, r.iterations[:, None], r.norm[:, None], r.status[:, None]], axis=1)
-    _compare(out, ref, p.n)
+    _compare(out, ref, p.n, MIXED_STATE_TOL)
 
 
 def test_replicated_scenarios_equal_single_solve(engine_lib):
@@ -216,7 +224,8 @@ def test_reactive_limits_match_oracle(engine_lib, oracle_mod):
 
 
 @pytest.mark.parametrize("schedule,lanes,threads", [(0, 0, 256), (0, 1, 256), (0, 2, 256), (0, 4, 256), (1, 1, 256),
-                                                    (1, 2, 512), (1, 4, 512), (1, 8, 256), (2, 0, 512)])
+                                                    (1, 2, 512), (1, 4, 512), (1, 8, 256), (2, 0, 512),
+                                                    (3, 0, 512), (3, 2, 512)])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_schedules_match_oracle(engine_lib, oracle_mod, schedule, lanes, threads, precision):
     """Every schedule (level launches, persistent tiles of 1-8 lanes) gives the oracle's states and statuses."""
@@ -230,7 +239,7 @@ def test_schedules_match_oracle(engine_lib, oracle_mod, schedule, lanes, threads
     ctx.set_schedule(schedule, lanes, threads)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
     ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis)
-    _compare(r, ref, p.n)
+    _compare(r, ref, p.n, _tol(precision))
 
 
 def test_autotuner_picks_a_schedule_and_keeps_results(engine_lib, oracle_mod):
@@ -243,7 +252,7 @@ def test_autotuner_picks_a_schedule_and_keeps_results(engine_lib, oracle_mod):
     ctx.set_schedule(native.AUTOTUNE)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
     (sc, lanes, threads), tuning = ctx.schedule()
-    assert len(tuning) == 9
+    assert len(tuning) == 11      # 4 level, 2 shared-memory level, 1 cooperative, 4 persistent candidates
     best = min(tuning, key=lambda t: t[3])
     assert (sc, lanes, threads) == (int(best[0]), int(best[1]), int(best[2]))
     ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis)
@@ -256,7 +265,7 @@ def test_persistent_reactive_limits_match_oracle(engine_lib, oracle_mod):
     outs = synthetic.draw_outages(g, 64, seed=301)
     dis = p.outage_masks(outs)
     s = native.Structure(p)
-    for sched in (0, 1, 2):
+    for sched in (0, 1, 2, 3):
         ctx = native.BatchContext(s, outs.shape[0], rl=p.rl)
         ctx.set_schedule(sched, 2, 256)
         r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
@@ -325,7 +334,7 @@ def test_pivot_growth_refactors_in_fp64(engine_lib, oracle_mod):
     cm.set_mixed_precision_controls(1e-3, 1e4)
     rm = cm.solve(p.x_base, p.target, p.base_row_mode, dis)
     assert cm.last_fp64_refactors().size == 0
-    _compare(rm, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n)
+    _compare(rm, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n, MIXED_STATE_TOL)
 
 
 @pytest.mark.parametrize("refine_below", [float("inf"), 1e-3, 1e-12])
@@ -340,10 +349,11 @@ def test_adaptive_refinement_matches_oracle(engine_lib, oracle_mod, refine_below
     ctx.set_linear_solver_settings(native.MIXED, 1)
     ctx.set_mixed_precision_controls(refine_below, 1e4)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
-    _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n)
+    _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n, MIXED_STATE_TOL)
 
 
-@pytest.mark.parametrize("schedule,lanes,threads", [(0, 2, 256), (0, 0, 256), (1, 2, 256), (2, 0, 512)])
+@pytest.mark.parametrize("schedule,lanes,threads", [(0, 2, 256), (0, 0, 256), (1, 2, 256), (2, 0, 512),
+                                                    (3, 2, 512)])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_deferred_l_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes, threads, precision):
     """The deferred-L block-LU plan (half the factorization levels) gives the oracle's states and statuses."""
@@ -358,7 +368,7 @@ def test_deferred_l_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes,
     ctx.set_linear_solver_settings(precision, 1)
     ctx.set_schedule(schedule, lanes, threads)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
-    _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n)
+    _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n, _tol(precision))
 
 
 @pytest.mark.parametrize("precision", [0, 1])
@@ -378,7 +388,8 @@ def test_cooperative_sweeps_match_level_launches(engine_lib, precision):
     assert np.array_equal(res[0], res[1])
 
 
-@pytest.mark.parametrize("schedule,lanes,threads", [(0, 2, 256), (0, 0, 256), (2, 0, 512)])
+@pytest.mark.parametrize("schedule,lanes,threads", [(0, 2, 256), (0, 0, 256), (2, 0, 512), (3, 0, 512),
+                                                    (3, 2, 512)])
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("name", ["grid2000", "grid9241"])
 def test_dense_front_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes, threads, precision, name):
@@ -394,7 +405,7 @@ def test_dense_front_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes
     ctx.set_linear_solver_settings(precision, 1)
     ctx.set_schedule(schedule, lanes, threads)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
-    _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n)
+    _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n, _tol(precision))
 
 
 def test_dense_front_plan_rejected_by_tiles(engine_lib):
