@@ -114,8 +114,8 @@ int olfgpu_last_fp64_refactors(int64_t context, unsigned char* flagged, int* cou
 /*
  * Schedule of the Newton iterations (no counterpart in the reference, which launches per dependency step and per
  * level and reads norms back every iteration): schedule 0 launches one kernel per wide dependency level over all
- * lanes and the narrow levels (<= 48 factorization tasks, <= 256 solve rows) of each phase in one launch of tiles of
- * lanesPerTile (1, 2 or 4; 0: one launch per level throughout), captured as one CUDA graph per Newton iteration;
+ * lanes and the narrow levels (<= 48 tasks) of each phase in one launch of tiles of lanesPerTile (1, 2 or 4; 0: one
+ * launch per level throughout), captured as one CUDA graph per Newton iteration;
  * schedule 1 runs the whole Newton loop in one persistent launch, one CTA per tile of lanesPerTile (1, 2, 4 or 8)
  * lanes with `threads` (256 or 512) threads; schedule 2 runs each factorization and each solve as one cooperative
  * launch over all lanes whose CTAs meet at a grid barrier between dependency levels (tile arguments ignored);
