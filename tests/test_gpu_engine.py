@@ -314,7 +314,8 @@ def test_phase_timing_reports_every_phase(engine_lib):
     assert ph["factorized_lanes"] >= outs.shape[0]
 
 
-def test_pivot_growth_refactors_in_fp64(engine_lib, oracle_mod):
+@pytest.mark.parametrize("schedule", [0, 3])
+def test_pivot_growth_refactors_in_fp64(engine_lib, oracle_mod, schedule):
     """Mixed precision: with the growth limit at its minimum every lane's FP32 factorization is flagged and redone in
     FP64 in the same iteration, which reproduces the FP64 engine bit for bit; with the default limit at most a few lanes
     of this well-conditioned batch are flagged (which depends on the FP32 rounding along each lane's iterations) and
@@ -325,8 +326,10 @@ def test_pivot_growth_refactors_in_fp64(engine_lib, oracle_mod):
     dis = p.outage_masks(outs)
     s = native.Structure(p)
     c64 = native.BatchContext(s, outs.shape[0])
+    c64.set_schedule(schedule, 2, 256)
     r64 = c64.solve(p.x_base, p.target, p.base_row_mode, dis)
     cm = native.BatchContext(s, outs.shape[0])
+    cm.set_schedule(schedule, 2, 256)
     cm.set_linear_solver_settings(native.MIXED, 1)
     cm.set_mixed_precision_controls(1e-3, 1.0)
     rm = cm.solve(p.x_base, p.target, p.base_row_mode, dis)
