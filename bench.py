@@ -31,10 +31,10 @@ GRID = "grid9241"
 N_OUTAGES = 500
 TOL = 1e-8
 CHECKPOINT = os.path.join(ROOT, "olf-gpu_b200", "checkpoints", "warmstart_grid9241.npz")
-# DRAM bytes (read + write) of one lane's FP64 factorization, from an ncu capture of every factorization launch of
-# the first Newton iteration of a 64-outage batch (472 MB over 64 lanes); scaled to a launch by the lanes it
-# factorizes
-TRAFFIC = {"fp64": 7.38e6, "mixed": None}
+# DRAM bytes (read + write) of one lane's factorization (dense-front plan, narrow levels in shared memory), from an
+# ncu capture of the 89 factorization launches of the first Newton iteration of a 64-outage batch (FP64: 490.9 MB,
+# FP32 LU: 288.3 MB over 64 lanes); scaled to a launch by the lanes it factorizes
+TRAFFIC = {"fp64": 7.67e6, "mixed": 4.51e6}
 
 
 def _peaks():
@@ -238,8 +238,15 @@ def run_engine(args, rank: int, world: int):
     traffic = TRAFFIC.get(args.precision)
     if traffic is not None:
         traffic = int(traffic * ph["factorized_lanes"] / max(ph["iterations"], 1))
-    fact_kernel = ("block-LU factorization of one Newton iteration (factorLevelKernel levels + factorRangeKernel "
-                   "narrow levels)")
+    sched = ctx.schedule()[0]
+    fact_kernel = "block-LU factorization of one Newton iteration (factorLevelKernel levels"
+    if sched[0] == native.LEVELS_SHARED:
+        fact_kernel += " + regionPrefixKernel / regionFactorKernel narrow levels in shared memory"
+    elif sched[0] == native.LEVELS and sched[1] > 0:
+        fact_kernel += " + factorRangeKernel narrow levels"
+    elif sched[0] == native.COOPERATIVE:
+        fact_kernel = "block-LU factorization of one Newton iteration (factorCoopKernel"
+    fact_kernel += (" + denseFrontKernel)" if args.plan == "dense" else ")")
     if ph["iterations"] == 0:
         # the autotuner picked the persistent schedule: one launch runs the whole Newton loop of the batch
         fact_kernel = "newtonPersistentKernel (the whole Newton loop of the batch in one launch)"

@@ -410,6 +410,7 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
     const int tib = ty / P, part = ty % P;
     const int s = blockIdx.y * 32 + lane;
     const int k = blockIdx.x * TPB + tib;
+    pdlTrigger();
     const bool ok = k < count && s < b.S && solving(b, s);
     T a00 = 0, a01 = 0, a10 = 0, a11 = 0, amax = 0;
     int t = 0;
@@ -417,6 +418,9 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
     if (ok) {
         t = net.levelTask[first + k];
         tk = net.task[t];
+    }
+    pdlWait();   // the previous level's blocks are read from here on
+    if (ok) {
         if (part == 0 && tk.aBlock >= 0) {
             const double* p = b.J + (size_t)tk.aBlock * 4 * S + s;
             a00 = (T)p[0];
@@ -500,11 +504,28 @@ __global__ void clearTroubleKernel(DevBatch b) {
     if (s < b.S && solving(b, s)) b.trouble[s] = 0;
 }
 
-// Launches a per-level kernel template with the level's split factor.
+// Launches a per-level kernel template with the level's split factor, as a programmatic dependent launch: its CTAs
+// may start while the previous level finishes (every level kernel loads its index records, then waits in pdlWait
+// for the previous grid before it touches factor or solution data).
+template <typename... KArgs, typename... Args>
+static void launchLevel(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 #define OLF_SPLIT_CASE(N, KERNEL, T_, ...)                                                             \
     case N: {                                                                                           \
         dim3 blk(32, Split<N>::ROWS), grd((count + Split<N>::TPB - 1) / Split<N>::TPB, b.S / 32);       \
-        KERNEL<T_, N><<<grd, blk, 0, st>>>(__VA_ARGS__);                                                \
+        launchLevel(KERNEL<T_, N>, grd, blk, st, __VA_ARGS__);                                          \
         break;                                                                                          \
     }
 #define OLF_SPLIT_DISPATCH(P_, KERNEL, T_, ...)                                                         \
@@ -587,17 +608,23 @@ __global__ void __launch_bounds__(1024) forwardLevelKernel(DevNet net, DevBatch 
     const int tib = ty / P, part = ty % P;
     const int s = blockIdx.y * 32 + lane;
     const int k = blockIdx.x * TPB + tib;
+    pdlTrigger();
     const bool ok = k < count && s < b.S && solving(b, s);
     T w0 = 0, w1 = 0;
-    int i = 0;
+    int i = 0, q0 = 0, q1 = 0;
     if (ok) {
         i = pos[first + k];
+        q0 = net.lrowPtr[i];
+        q1 = net.lrowEnd[i];
+    }
+    pdlWait();   // the previous level's solution entries are read from here on
+    if (ok) {
         if (part == 0) {
             w0 = w[(2 * (size_t)i) * S + s];
             w1 = w[(2 * (size_t)i + 1) * S + s];
         }
 #pragma unroll 4
-        for (int q = net.lrowPtr[i] + part; q < net.lrowEnd[i]; q += P) {
+        for (int q = q0 + part; q < q1; q += P) {
             const int2 e = net.lrow[q];
             T l00, l01, l10, l11;
             load4(lu, (size_t)e.x, S, s, l00, l01, l10, l11);
@@ -632,18 +659,23 @@ __global__ void __launch_bounds__(1024) backwardLevelKernel(DevNet net, DevBatch
     const int tib = ty / P, part = ty % P;
     const int s = blockIdx.y * 32 + lane;
     const int k = blockIdx.x * TPB + tib;
+    pdlTrigger();
     const bool ok = k < count && s < b.S && solving(b, s);
     T w0 = 0, w1 = 0;
-    int i = 0, d = 0;
+    int i = 0, d = 0, q1 = 0;
     if (ok) {
         i = pos[first + k];
         d = net.uPtr[i];
+        q1 = net.uPtr[i + 1];
+    }
+    pdlWait();   // the previous level's solution entries are read from here on
+    if (ok) {
         if (part == 0) {
             w0 = w[(2 * (size_t)i) * S + s];
             w1 = w[(2 * (size_t)i + 1) * S + s];
         }
 #pragma unroll 4
-        for (int q = d + 1 + part; q < net.uPtr[i + 1]; q += P) {
+        for (int q = d + 1 + part; q < q1; q += P) {
             const int j = net.uCol[q];
             T u00, u01, u10, u11;
             load4(lu, (size_t)q, S, s, u00, u01, u10, u11);

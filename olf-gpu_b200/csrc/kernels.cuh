@@ -74,6 +74,13 @@ struct DevNet {
     const int* uCol;          // column position of each U block
 };
 
+// Programmatic dependent launch (level kernels): pdlTrigger lets the next grid in the stream start its CTAs once
+// every CTA of this grid has started; pdlWait blocks until the previous grid has completed and its writes are
+// visible (immediately when the grid was not launched as a dependent).  Every thread of a level kernel reaches
+// pdlWait, so a level completes only after the one before it.
+__device__ __forceinline__ void pdlTrigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdlWait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Per-batch device state (lane-interleaved arrays).
 struct DevBatch {
     int S;                    // lane stride (multiple of 32)
