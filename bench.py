@@ -126,6 +126,8 @@ def run_engine(args, rank: int, world: int):
         ctx.set_schedule(native.COOPERATIVE, 0, 512)
     elif args.schedule == "shared":
         ctx.set_schedule(native.LEVELS_SHARED, 2, 256)
+    elif args.schedule == "shared-all":
+        ctx.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
     # host inputs in pinned memory (e2e copies them every step); results read back to pinned memory
     dis = torch.from_numpy(p.outage_masks(outs)).pin_memory().numpy()
     out = torch.empty((ns, p.n + 3), dtype=torch.float64).pin_memory().numpy()
@@ -240,7 +242,7 @@ def run_engine(args, rank: int, world: int):
         traffic = int(traffic * ph["factorized_lanes"] / max(ph["iterations"], 1))
     sched = ctx.schedule()[0]
     fact_kernel = "block-LU factorization of one Newton iteration (factorLevelKernel levels"
-    if sched[0] == native.LEVELS_SHARED:
+    if sched[0] in (native.LEVELS_SHARED, native.LEVELS_SHARED_ALL):
         fact_kernel += " + regionPrefixKernel / regionFactorKernel narrow levels in shared memory"
     elif sched[0] == native.LEVELS and sched[1] > 0:
         fact_kernel += " + factorRangeKernel narrow levels"
@@ -522,9 +524,10 @@ def main():
                     help="block-LU plan: L scaled at its task, deferred (half the levels) or dense (the trailing "
                          "block factorized in shared memory; default for the N-1 workload, whose autotuned schedules "
                          "all run it); the uneven workload's persistent launch runs the scaled plan")
-    ap.add_argument("--schedule", default="auto", choices=["auto", "levels", "coop", "shared"],
+    ap.add_argument("--schedule", default="auto", choices=["auto", "levels", "coop", "shared", "shared-all"],
                     help="auto: the engine's autotuner picks the Newton-iteration schedule on the first solve; "
-                         "shared: level launches with the narrow factorization levels in shared memory")
+                         "shared: level launches with the narrow factorization levels in shared memory; shared-all: "
+                         "the solves' narrow levels too")
     ap.add_argument("--outages", type=int, default=N_OUTAGES,
                     help="outages per GPU (500 is the benchmark; smaller batches are profiling cases)")
     ap.add_argument("--workload", default="n1", choices=["n1", "uneven"],

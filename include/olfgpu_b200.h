@@ -120,12 +120,13 @@ int olfgpu_last_fp64_refactors(int64_t context, unsigned char* flagged, int* cou
  * lanes with `threads` (256 or 512) threads; schedule 2 runs each factorization and each solve as one cooperative
  * launch over all lanes whose CTAs meet at a grid barrier between dependency levels (tile arguments ignored);
  * schedule 3 is schedule 0 with the narrow factorization levels run in shared memory, one CTA of 256 threads per
- * lane holding every LU block those levels
- * produce (lanesPerTile then only sets the solves' narrow-level tiles; plans whose narrow levels do not fit, and
- * deferred-L plans, fall back to schedule 0); schedule -1 lets the next solve time every candidate on its batch and
- * keep the fastest (the autotuner).  olfgpu_get_schedule reports the schedule in force
- * and, after an autotuned solve, up to maxResults timings {schedule, lanesPerTile, threads, ms} into results
- * (nResults receives their count).
+ * lane holding every LU block those levels produce (lanesPerTile then only sets the solves' narrow-level tiles; plans
+ * whose narrow levels do not fit, and deferred-L plans, fall back to schedule 0); schedule 4 is schedule 3 with the
+ * solves' narrow levels (the forward tail and the backward head) in shared memory as well, one CTA per lane holding
+ * those rows' solution entries (lanesPerTile ignored); schedule -1 lets the next solve time every candidate on its
+ * batch and keep the fastest (the autotuner).  olfgpu_get_schedule reports the schedule in force and, after an
+ * autotuned solve, up to maxResults timings {schedule, lanesPerTile, threads, ms} into results (nResults receives
+ * their count).
  */
 int olfgpu_set_schedule(int64_t context, int schedule, int lanesPerTile, int threads);
 int olfgpu_get_schedule(int64_t context, int* schedule, int* lanesPerTile, int* threads, int maxResults,

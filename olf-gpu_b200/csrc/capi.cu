@@ -222,10 +222,11 @@ extern "C" int olfgpu_set_schedule(int64_t context, int schedule, int lanesPerTi
             return;
         }
         if (schedule != SCHEDULE_LEVELS && schedule != SCHEDULE_PERSISTENT && schedule != SCHEDULE_COOP &&
-            schedule != SCHEDULE_LEVELS_SHARED) {
+            schedule != SCHEDULE_LEVELS_SHARED && schedule != SCHEDULE_LEVELS_SHARED_ALL) {
             throw std::runtime_error("unknown schedule");
         }
-        c.regionFactor = schedule == SCHEDULE_LEVELS_SHARED;
+        c.regionFactor = schedule == SCHEDULE_LEVELS_SHARED || schedule == SCHEDULE_LEVELS_SHARED_ALL;
+        c.regionSolve = schedule == SCHEDULE_LEVELS_SHARED_ALL;
         if (c.regionFactor) schedule = SCHEDULE_LEVELS;
         if (schedule == SCHEDULE_COOP) {
             // cooperative sweeps have no tile parameters
@@ -251,7 +252,12 @@ extern "C" int olfgpu_get_schedule(int64_t context, int* schedule, int* lanesPer
                                    double* results, int* nResults) {
     return guarded([&] {
         BatchContext& c = contextOf(context);
-        if (schedule) *schedule = c.schedule == SCHEDULE_LEVELS && c.regionFactor ? SCHEDULE_LEVELS_SHARED : c.schedule;
+        if (schedule) {
+            *schedule = c.schedule != SCHEDULE_LEVELS ? c.schedule
+                        : c.regionSolve              ? SCHEDULE_LEVELS_SHARED_ALL
+                        : c.regionFactor             ? SCHEDULE_LEVELS_SHARED
+                                                     : SCHEDULE_LEVELS;
+        }
         if (lanesPerTile) *lanesPerTile = c.schedule == SCHEDULE_LEVELS ? c.narrowLanes : c.lanesPerTile;
         // range kernels run 256 threads, as does the shared-memory factorization
         if (threads) *threads = c.schedule == SCHEDULE_LEVELS ? 256 : c.threads;

@@ -264,6 +264,34 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     while (d->bwdUntil < static_cast<int>(p.bwdLevelPtr.size()) - 1 && countOf(p.bwdLevelPtr, d->bwdUntil) <= NARROW) {
         d->bwdUntil++;
     }
+    // shared-memory solve regions: slot k of the forward tail holds position fwdLevelPos[fwdRegionBase + k], of the
+    // backward head position bwdLevelPos[k]; each L / U entry of a region row carries its column's slot + 1 (0: a
+    // column outside the region, final in global memory before the region's launch).  Both fit far below the default
+    // 48 KB of shared memory on these grids; a larger one is left to the level launches.
+    {
+        constexpr int SOLVE_REGION_SLOTS = 2048;
+        const int nFwd = static_cast<int>(p.fwdLevelPtr.size()) - 1;
+        d->fwdRegionBase = p.fwdLevelPtr[d->fwdFrom];
+        d->fwdRegionSlots = p.fwdLevelPtr[nFwd] - d->fwdRegionBase;
+        d->bwdRegionSlots = p.bwdLevelPtr[d->bwdUntil];
+        if (d->fwdRegionSlots > SOLVE_REGION_SLOTS) d->fwdRegionSlots = 0;
+        if (d->bwdRegionSlots > SOLVE_REGION_SLOTS) d->bwdRegionSlots = 0;
+        std::vector<int> slot(nb, -1);
+        std::vector<int> lrowSlot(std::max<size_t>(lrow.size(), 1), 0), uSlot(std::max<size_t>(p.nU, 1), 0);
+        for (int k = 0; k < d->fwdRegionSlots; k++) slot[p.fwdLevelPos[d->fwdRegionBase + k]] = k;
+        for (int k = 0; k < d->fwdRegionSlots; k++) {
+            const int i = p.fwdLevelPos[d->fwdRegionBase + k];
+            for (int q = lrowPtr[i]; q < lrowEnd[i]; q++) lrowSlot[q] = slot[lrow[q].y] + 1;
+        }
+        std::fill(slot.begin(), slot.end(), -1);
+        for (int k = 0; k < d->bwdRegionSlots; k++) slot[p.bwdLevelPos[k]] = k;
+        for (int k = 0; k < d->bwdRegionSlots; k++) {
+            const int i = p.bwdLevelPos[k];
+            for (int q = p.uPtr[i] + 1; q < p.uPtr[i + 1]; q++) uSlot[q] = slot[p.uCol[q]] + 1;
+        }
+        d->lrowSlot.upload(lrowSlot);
+        d->uSlot.upload(uSlot);
+    }
     d->bwdSplit.assign(p.bwdLevelPtr.size() - 1, 1);
     for (size_t l = 0; l + 1 < p.bwdLevelPtr.size(); l++) {
         int m = 0;
@@ -663,7 +691,8 @@ DevBatch fp64View(BatchContext& ctx) {
 }  // namespace
 
 void captureIteration(BatchContext& ctx) {
-    const int key = ctx.narrowLanes * 100000 + (ctx.regionFactor ? 50000 : 0) + ctx.precision * 1000 +
+    const int key = ctx.narrowLanes * 100000 + (ctx.regionFactor ? 50000 : 0) + (ctx.regionSolve ? 20000 : 0) +
+                    ctx.precision * 1000 +
                     ctx.refinementSteps * 10 +
                     (ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits ? 1 : 0);
     if (ctx.graph && ctx.graphKey == key) return;
@@ -1045,6 +1074,9 @@ void autotune(BatchContext& ctx) {
     if (ctx.net->dev->regionSlots > 0) {
         for (int narrow : {0, 2}) cands.push_back({SCHEDULE_LEVELS_SHARED, narrow, 256});
     }
+    if (ctx.net->dev->fwdRegionSlots > 0 || ctx.net->dev->bwdRegionSlots > 0) {
+        cands.push_back({SCHEDULE_LEVELS_SHARED_ALL, 0, 256});
+    }
     cands.push_back({SCHEDULE_COOP, 0, 512});
     if (ctx.net->dev->view.frontF == 0) {   // the persistent tiles do not run dense-front plans
         for (int lanes : {2, 4})
@@ -1057,7 +1089,8 @@ void autotune(BatchContext& ctx) {
     Candidate pick = cands[0];
     ctx.tuning.clear();
     auto apply = [&](const Candidate& c) {
-        ctx.regionFactor = c.schedule == SCHEDULE_LEVELS_SHARED;
+        ctx.regionFactor = c.schedule == SCHEDULE_LEVELS_SHARED || c.schedule == SCHEDULE_LEVELS_SHARED_ALL;
+        ctx.regionSolve = c.schedule == SCHEDULE_LEVELS_SHARED_ALL;
         ctx.schedule = ctx.regionFactor ? SCHEDULE_LEVELS : c.schedule;
         if (ctx.schedule == SCHEDULE_LEVELS) {
             ctx.narrowLanes = c.lanes;

@@ -78,6 +78,9 @@ struct DeviceNet {
     // shared-memory region of the narrow factorization levels [regionFrom, factorTo) (regionSlots 0: none)
     int regionFrom = 0, regionBase = 0, regionSlots = 0;
     DeviceBuffer regionTask;
+    // shared-memory solve regions: the forward tail [fwdFrom, nFwd) and the backward head [0, bwdUntil) (slots 0: none)
+    int fwdRegionBase = 0, fwdRegionSlots = 0, bwdRegionSlots = 0;
+    DeviceBuffer lrowSlot, uSlot;
 };
 
 struct NetStructure {
@@ -89,9 +92,15 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s);
 
 // Schedules of the Newton iterations: one launch per dependency level (captured in a CUDA graph per iteration), or
 // the persistent kernel with one CTA per lane tile running the whole loop.
-// SCHEDULE_LEVELS_SHARED is an API value only: the level schedule with the narrow factorization levels in shared
-// memory (BatchContext::regionFactor).
-enum { SCHEDULE_LEVELS = 0, SCHEDULE_PERSISTENT = 1, SCHEDULE_COOP = 2, SCHEDULE_LEVELS_SHARED = 3 };
+// SCHEDULE_LEVELS_SHARED and SCHEDULE_LEVELS_SHARED_ALL are API values only: the level schedule with the narrow
+// factorization levels (BatchContext::regionFactor), and also the solves' narrow levels (regionSolve), in shared memory.
+enum {
+    SCHEDULE_LEVELS = 0,
+    SCHEDULE_PERSISTENT = 1,
+    SCHEDULE_COOP = 2,
+    SCHEDULE_LEVELS_SHARED = 3,
+    SCHEDULE_LEVELS_SHARED_ALL = 4
+};
 
 // Mixed precision: a refinement step's correction solve runs only while some lane's FP64 residual max |r| is above
 // this fraction of the mismatch tolerance (below it the FP32 solve is already accurate enough for the test).
@@ -151,6 +160,7 @@ struct BatchContext {
     bool autotunePending = false;
     int narrowLanes = 2;            // level schedule: lanes per tile of the narrow-level range launches (0: none)
     bool regionFactor = false;      // level schedule: the narrow factorization levels in shared memory
+    bool regionSolve = false;       // level schedule: the solves' narrow levels in shared memory too
     Hybrid hybrid() const {
         const DeviceNet& d = *net->dev;
         Hybrid h{d.factorFrom, d.factorTo, d.fwdFrom, d.bwdUntil, narrowLanes, d.persistent};
@@ -161,9 +171,17 @@ struct BatchContext {
             h.regionSlots = d.regionSlots;
             h.regionTask = d.regionTask.as<int4>();
         }
+        if (regionSolve) {
+            h.solveRegion = true;
+            h.fwdRegionBase = d.fwdRegionBase;
+            h.fwdRegionSlots = d.fwdRegionSlots;
+            h.bwdRegionSlots = d.bwdRegionSlots;
+            h.lrowSlot = d.lrowSlot.as<int>();
+            h.uSlot = d.uSlot.as<int>();
+        }
         return h;
     }
-    bool useHybrid() const { return narrowLanes > 0 || regionFactor; }
+    bool useHybrid() const { return narrowLanes > 0 || regionFactor || regionSolve; }
     std::vector<TuningResult> tuning;
     DeviceBuffer out;               // [nS][n + 3] scenario-major results
     // reactive limits

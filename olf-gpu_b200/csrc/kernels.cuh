@@ -195,12 +195,21 @@ struct Hybrid {
     PersistentPlan plan;
     int regionFrom = 0, regionBase = 0, regionSlots = 0;
     const int4* regionTask = nullptr;
+    // the solves' narrow levels in shared memory (launchSolveRegion): the forward tail [fwdFrom, nFwd) (slot k: position
+    // fwdPos[fwdRegionBase + k]) and the backward head [0, bwdUntil) (slot k: position bwdPos[k]); lrowSlot / uSlot:
+    // per L / U entry, the slot + 1 of its column in the region of its row, 0 outside
+    bool solveRegion = false;
+    int fwdRegionBase = 0, fwdRegionSlots = 0, bwdRegionSlots = 0;
+    const int* lrowSlot = nullptr;
+    const int* uSlot = nullptr;
 };
 // The shared-memory factorization of the narrow levels (two launches; no-op when h.regionSlots == 0; every region
 // level holds at most REGION_THREADS tasks).  prepareRegion raises the kernel's dynamic shared-memory limit for nSlots
 // slots and nLevels levels on the current device.
 constexpr int REGION_THREADS = 256;
 void launchRegionFactor(const DevNet& net, const DevBatch& b, const Hybrid& h, bool fp32, cudaStream_t st);
+// One sweep's narrow solve levels in shared memory (dir 0 the forward tail, 1 the backward head), one CTA per lane.
+void launchSolveRegion(const DevNet& net, const DevBatch& b, const Hybrid& h, bool fp32, int dir, cudaStream_t st);
 cudaError_t prepareRegion(int nSlots, int nLevels);
 
 // Level boundaries (host), the positions of each level (device) and the split factor of each level (host).

