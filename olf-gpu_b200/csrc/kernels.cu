@@ -24,11 +24,12 @@ __device__ __forceinline__ double absMax(double m, double v) {
 // is written once, in a fixed order, with no atomics; the FIXED_VARIABLE row modes are applied in the same pass.
 // Terms: closed branches (equations/generated/closed_branch.cuh:161-229), open branches (open_branch.cuh:65-87),
 // shunts (shunt.cuh:47-60); F = terms - target (fill_launch.cu:117-126); identity rows (fill_launch.cu:96-103).
-// The per-lane max |F| is reduced in the block and folded into norm[s] with one atomic per block and lane.  Four
-// resident CTAs per SM (64 registers): the fill is latency-bound, and occupancy pays more than a few spilled registers.
+// The per-lane max |F| is reduced in the block and folded into norm[s] with one atomic per block and lane.  Five
+// resident CTAs per SM: the fill is latency-bound, and occupancy pays more than a few spilled registers (measured per
+// 500-lane fill: 2 CTAs 535 us, 4 CTAs 324 us; per step, 3 CTAs 2 % slower and 5 CTAs 0.5 % faster than 4).
 // ---------------------------------------------------------------------------------------------------------------
 template <bool WITH_J, bool WITH_Q>
-__global__ void __launch_bounds__(256, 4) fillKernel(DevNet net, DevBatch b) {
+__global__ void __launch_bounds__(256, 5) fillKernel(DevNet net, DevBatch b) {
     const int s = blockIdx.x * 32 + threadIdx.x;
     const int node = blockIdx.y * blockDim.y + threadIdx.y;
     const size_t S = b.S;
