@@ -279,10 +279,20 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
         std::vector<int> slot(nb, -1);
         std::vector<int> lrowSlot(std::max<size_t>(lrow.size(), 1), 0), uSlot(std::max<size_t>(p.nU, 1), 0);
         for (int k = 0; k < d->fwdRegionSlots; k++) slot[p.fwdLevelPos[d->fwdRegionBase + k]] = k;
+        // a forward-tail row's entries whose columns lie outside the region go first (each group in ascending column):
+        // solvePrefixKernel applies them, coalesced over the lanes, before the region starts at fwdRegionStart[k]
+        std::vector<int> fwdStart(std::max(d->fwdRegionSlots, 1), 0);
         for (int k = 0; k < d->fwdRegionSlots; k++) {
             const int i = p.fwdLevelPos[d->fwdRegionBase + k];
-            for (int q = lrowPtr[i]; q < lrowEnd[i]; q++) lrowSlot[q] = slot[lrow[q].y] + 1;
+            std::stable_partition(lrow.begin() + lrowPtr[i], lrow.begin() + lrowEnd[i],
+                                  [&](const int2& e) { return slot[e.y] < 0; });
+            int q = lrowPtr[i];
+            while (q < lrowEnd[i] && slot[lrow[q].y] < 0) q++;
+            fwdStart[k] = q;
+            for (q = lrowPtr[i]; q < lrowEnd[i]; q++) lrowSlot[q] = slot[lrow[q].y] + 1;
         }
+        d->lrow.upload(lrow);
+        d->fwdRegionStart.upload(fwdStart);
         std::fill(slot.begin(), slot.end(), -1);
         for (int k = 0; k < d->bwdRegionSlots; k++) slot[p.bwdLevelPos[k]] = k;
         for (int k = 0; k < d->bwdRegionSlots; k++) {

@@ -80,7 +80,7 @@ struct DeviceNet {
     DeviceBuffer regionTask;
     // shared-memory solve regions: the forward tail [fwdFrom, nFwd) and the backward head [0, bwdUntil) (slots 0: none)
     int fwdRegionBase = 0, fwdRegionSlots = 0, bwdRegionSlots = 0;
-    DeviceBuffer lrowSlot, uSlot;
+    DeviceBuffer lrowSlot, uSlot, fwdRegionStart;
 };
 
 struct NetStructure {
@@ -178,6 +178,7 @@ struct BatchContext {
             h.bwdRegionSlots = d.bwdRegionSlots;
             h.lrowSlot = d.lrowSlot.as<int>();
             h.uSlot = d.uSlot.as<int>();
+            h.fwdRegionStart = d.fwdRegionStart.as<int>();
         }
         return h;
     }

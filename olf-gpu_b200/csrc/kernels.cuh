@@ -197,11 +197,13 @@ struct Hybrid {
     const int4* regionTask = nullptr;
     // the solves' narrow levels in shared memory (launchSolveRegion): the forward tail [fwdFrom, nFwd) (slot k: position
     // fwdPos[fwdRegionBase + k]) and the backward head [0, bwdUntil) (slot k: position bwdPos[k]); lrowSlot / uSlot:
-    // per L / U entry, the slot + 1 of its column in the region of its row, 0 outside
+    // per L / U entry, the slot + 1 of its column in the region of its row, 0 outside; fwdRegionStart[k]: the first
+    // entry of forward slot k's row with a column in the region (the entries before it go to the prefix launch)
     bool solveRegion = false;
     int fwdRegionBase = 0, fwdRegionSlots = 0, bwdRegionSlots = 0;
     const int* lrowSlot = nullptr;
     const int* uSlot = nullptr;
+    const int* fwdRegionStart = nullptr;
 };
 // The shared-memory factorization of the narrow levels (two launches; no-op when h.regionSlots == 0; every region
 // level holds at most REGION_THREADS tasks).  prepareRegion raises the kernel's dynamic shared-memory limit for nSlots

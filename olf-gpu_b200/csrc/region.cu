@@ -11,6 +11,9 @@
 // the U block in the high 16 bits, 0 outside the region) or from global memory, and writes each finished block to
 // both.  The expressions per block are those of factorLevelKernel (pivot inverse, L scaled by the inverted pivot,
 // the near-singular and pivot-growth checks); the P partial sums of a task are combined by a fixed butterfly.
+//
+// The solves' narrow levels (solveRegionKernel, schedule 4) follow the same pattern: the forward tail and the backward
+// head of the triangular sweeps, one CTA per lane, the solution entries of their rows in shared memory.
 #include "kernels.cuh"
 
 namespace olfb200 {
@@ -110,7 +113,6 @@ struct RegionItem {
     T d[4];         // the inverted pivot outside the region (L tasks, part 0)
 };
 
-template <typename T>
 __device__ __forceinline__ int regionSplit(int count, int threads) {
     int P = 1;   // threads per task: a power of two <= 32, so a task's threads share a warp
     while (P < 32 && 2 * P * count <= threads) P *= 2;
@@ -121,7 +123,7 @@ template <typename T>
 __device__ __forceinline__ void regionFetch(const DevNet& net, const T* lu, size_t S, int s, const int* lvl, int li,
                                             int base, const int4* rtask, RegionItem<T>& it) {
     const int first = lvl[li], count = lvl[li + 1] - first;
-    const int P = regionSplit<T>(count, blockDim.x);
+    const int P = regionSplit(count, blockDim.x);
     const int k = threadIdx.x / P, part = threadIdx.x % P;
     it.rt.x = -1;
     it.op.x = -1;
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(REGION_THREADS, 2) regionFactorKernel(DevNet n
         const RegionItem<T> cur = next;
         if (li + 1 < l1 - l0) regionFetch(net, lu, S, s, lvl, li + 1, base, rtask, next);
         const int count = lvl[li + 1] - lvl[li];
-        const int P = regionSplit<T>(count, blockDim.x);
+        const int P = regionSplit(count, blockDim.x);
         const int part = threadIdx.x % P;
         T acc[4] = {0, 0, 0, 0};
         if (cur.rt.x >= 0 && cur.op.x >= 0) {
@@ -273,7 +275,7 @@ template <typename T, int DIR>
 __global__ void __launch_bounds__(REGION_THREADS) solveRegionKernel(DevNet net, DevBatch b, const T* lu, T* w,
                                                                     const int* levelPtr, const int* pos, int l0,
                                                                     int l1, int base, int nSlots,
-                                                                    const int* entrySlot) {
+                                                                    const int* entrySlot, const int* rowStart) {
     extern __shared__ __align__(16) unsigned char regionSmem[];
     T* ws = reinterpret_cast<T*>(regionSmem);                                  // [nSlots][2]
     int* lvl = reinterpret_cast<int*>(ws + 2 * (size_t)nSlots + (nSlots & 1));   // [l1 - l0 + 1]
@@ -292,14 +294,14 @@ __global__ void __launch_bounds__(REGION_THREADS) solveRegionKernel(DevNet net, 
     T nM[4], nD[4];   // the first entry's block; (backward, part 0) the row's inverted pivot
     auto fetch = [&](int li) {
         const int first = lvl[li], count = lvl[li + 1] - first;
-        const int P = regionSplit<T>(count, blockDim.x);
+        const int P = regionSplit(count, blockDim.x);
         const int k = threadIdx.x / P, part = threadIdx.x % P;
         nPos = -1;
         nBlk = -1;
         if (k >= count) return;
         nPos = pos[first + k];
         if (DIR == 0) {
-            nQ0 = net.lrowPtr[nPos];
+            nQ0 = rowStart[first - base + k];   // the entries before it went to the prefix launch
             nQ1 = net.lrowEnd[nPos];
         } else {
             nQ0 = net.uPtr[nPos] + 1;
@@ -331,7 +333,7 @@ __global__ void __launch_bounds__(REGION_THREADS) solveRegionKernel(DevNet net, 
         }
         if (li + 1 < l1 - l0) fetch(li + 1);
         const int first = lvl[li], count = lvl[li + 1] - first;
-        const int P = regionSplit<T>(count, blockDim.x);
+        const int P = regionSplit(count, blockDim.x);
         const int k = threadIdx.x / P, part = threadIdx.x % P;
         T a0 = 0, a1 = 0;
         if (iPos >= 0 && blk0 >= 0) {
@@ -391,6 +393,31 @@ __global__ void __launch_bounds__(REGION_THREADS) solveRegionKernel(DevNet net, 
     }
 }
 
+// The forward tail's prefix: for each region row, the entries whose columns lie outside the region (final before it
+// starts), w_i -= L(i, c) w_c, one thread per (row, lane), lanes coalesced.
+template <typename T>
+__global__ void __launch_bounds__(256) solvePrefixKernel(DevNet net, DevBatch b, const T* lu, T* w, const int* pos,
+                                                         int base, int nSlots, const int* rowStart) {
+    const int s = blockIdx.y * 32 + threadIdx.x;
+    const int k = blockIdx.x * 8 + threadIdx.y;
+    if (k >= nSlots || s >= b.S || !regionSolving(b, s)) return;
+    const size_t S = b.S;
+    const int i = pos[base + k];
+    const int q1 = rowStart[k];
+    T w0 = w[(2 * (size_t)i) * S + s], w1 = w[(2 * (size_t)i + 1) * S + s];
+#pragma unroll 2
+    for (int q = net.lrowPtr[i]; q < q1; q++) {
+        const int2 e = net.lrow[q];
+        T m[4];
+        ld4g(lu, e.x, S, s, m);
+        const T y0 = w[(2 * (size_t)e.y) * S + s], y1 = w[(2 * (size_t)e.y + 1) * S + s];
+        w0 -= m[0] * y0 + m[1] * y1;
+        w1 -= m[2] * y0 + m[3] * y1;
+    }
+    w[(2 * (size_t)i) * S + s] = w0;
+    w[(2 * (size_t)i + 1) * S + s] = w1;
+}
+
 template <typename T>
 size_t regionBytes(int nSlots, int nLevels) {
     return (size_t)nSlots * 4 * sizeof(T) + (sizeof(T) == 4 ? (size_t)nSlots * 4 : 0) + (size_t)(nLevels + 1) * 4;
@@ -413,13 +440,16 @@ template <typename T>
 void solveRegionT(const DevNet& net, const DevBatch& b, const T* lu, T* w, const Hybrid& h, int dir, cudaStream_t st) {
     if (dir == 0) {
         if (h.fwdRegionSlots <= 0) return;
+        dim3 blk(32, 8), grd((h.fwdRegionSlots + 7) / 8, b.S / 32);
+        solvePrefixKernel<T><<<grd, blk, 0, st>>>(net, b, lu, w, h.plan.fwdPos, h.fwdRegionBase, h.fwdRegionSlots,
+                                                 h.fwdRegionStart);
         solveRegionKernel<T, 0><<<b.S, REGION_THREADS, solveRegionBytes<T>(h.fwdRegionSlots, h.plan.nFwd - h.fwdFrom),
                                   st>>>(net, b, lu, w, h.plan.fwdPtr, h.plan.fwdPos, h.fwdFrom, h.plan.nFwd,
-                                        h.fwdRegionBase, h.fwdRegionSlots, h.lrowSlot);
+                                        h.fwdRegionBase, h.fwdRegionSlots, h.lrowSlot, h.fwdRegionStart);
     } else {
         if (h.bwdRegionSlots <= 0) return;
         solveRegionKernel<T, 1><<<b.S, REGION_THREADS, solveRegionBytes<T>(h.bwdRegionSlots, h.bwdUntil), st>>>(
-            net, b, lu, w, h.plan.bwdPtr, h.plan.bwdPos, 0, h.bwdUntil, 0, h.bwdRegionSlots, h.uSlot);
+            net, b, lu, w, h.plan.bwdPtr, h.plan.bwdPos, 0, h.bwdUntil, 0, h.bwdRegionSlots, h.uSlot, nullptr);
     }
 }
 
