@@ -68,3 +68,38 @@ def test_bad_inputs_are_errors_not_crashes(engine_lib):
         native.Structure(q)
     with pytest.raises(native.NativeError, match="invalid structure handle"):
         native._check(native.load().olfgpu_structure_info(0, None, None))
+
+
+@pytest.mark.parametrize("plan", ["scaled", "deferred", "dense"])
+def test_level_schedules_cover_every_block_once(engine_lib, plan):
+    """The factorization levels hold every LU block exactly once with every block update, and the forward and
+    backward solve levels every row (a dense-front plan leaves its front rows to the dense front's backward solve)."""
+    from conftest import grid
+    from olfgpu import native
+    _, p = grid("grid2000")
+    flag = {"scaled": 0, "deferred": native.PLAN_DEFERRED_L, "dense": native.PLAN_DENSE_FRONT}[plan]
+    s = native.Structure(p, flag)
+    f, ops, fw, bw = s.levels()
+    assert f[0] == 0 and f[-1] == s.n_lu_blocks and np.all(np.diff(f) > 0)
+    assert int(ops.sum()) == s.block_ops
+    assert fw[0] == 0 and fw[-1] == s.n_bus and np.all(np.diff(fw) > 0)
+    assert bw[0] == 0 and np.all(np.diff(bw) > 0)
+    front = s.n_bus - int(bw[-1])
+    if plan == "dense":
+        assert 4 <= front <= 32
+    else:
+        assert front == 0
+
+
+def test_plan_variants_shorten_the_dependency_chain(engine_lib):
+    """The deferred-L plan advances about one level per pivot, the dense-front plan removes the root separators'
+    levels: both have fewer factorization levels than the scaled plan of the same structure, with the same blocks."""
+    from conftest import grid
+    from olfgpu import native
+    _, p = grid("grid2000")
+    scaled = native.Structure(p)
+    deferred = native.Structure(p, native.PLAN_DEFERRED_L)
+    dense = native.Structure(p, native.PLAN_DENSE_FRONT)
+    assert deferred.factor_levels < scaled.factor_levels
+    assert dense.factor_levels < scaled.factor_levels
+    assert scaled.n_lu_blocks == deferred.n_lu_blocks == dense.n_lu_blocks
