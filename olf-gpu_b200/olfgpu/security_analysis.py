@@ -40,13 +40,18 @@ class SecurityAnalysis:
     """Holds the structure and one context per chunk width, reused across calls (GpuBatchContextCache)."""
 
     def __init__(self, packed: Packed, precision: int = native.FP64, refinement_steps: int = 1,
-                 reactive_limits: bool = False, ordering: int = native.PLAN_DENSE_FRONT, max_chunk: int = 4096):
+                 reactive_limits: bool = False, ordering: int = native.PLAN_DENSE_FRONT, max_chunk: int = 4096,
+                 schedule: Optional[tuple] = None):
+        """``schedule``: None keeps the engine's default (level launches with 2-lane narrow tiles); otherwise the
+        arguments of BatchContext.set_schedule, e.g. (native.AUTOTUNE,) to time every schedule on the first batch
+        of each chunk width, or (native.LEVELS_SHARED_ALL, 0, 256)."""
         self.packed = packed
         self.structure = native.Structure(packed, ordering)
         self.precision = precision
         self.refinement_steps = refinement_steps
         self.reactive_limits = reactive_limits and packed.rl is not None
         self.max_chunk = max_chunk
+        self.schedule = schedule
         self._contexts = {}
 
     def context(self, width: int) -> native.BatchContext:
@@ -55,6 +60,8 @@ class SecurityAnalysis:
             ctx = native.BatchContext(self.structure, width, native.BATCHED_LU,
                                       self.packed.rl if self.reactive_limits else None)
             ctx.set_linear_solver_settings(self.precision, self.refinement_steps)
+            if self.schedule is not None:
+                ctx.set_schedule(*self.schedule)
             self._contexts[width] = ctx
         return ctx
 
