@@ -98,6 +98,74 @@ def workload(rank: int, count: int = N_OUTAGES):
     return g, p, outs
 
 
+# The engine's launch structure (engine.cu / kernels.cu), used to count the kernels a step launches: narrow levels
+# hold <= 48 tasks; the shared-memory factorization region holds <= 110 KB of FP64 blocks (3,520 slots) in levels of
+# <= 256 tasks; a shared-memory solve region holds <= 2,048 rows.
+NARROW, REGION_SLOTS, REGION_THREADS, SOLVE_REGION_SLOTS = 48, 110 * 1024 // 32, 256, 2048
+# kernels of one learned-start prediction: input GEMM, 4 x (edge projection, PQ GEMM, message, update GEMM), output
+# GEMM, compact inputs, start composition and scatter
+GNN_LAUNCHES = 1 + 4 * 4 + 1 + 1 + 2
+
+
+def launches_per_solve(s, sched, rounds: int, dense: bool, deferred: bool, mixed: bool, refine_rounds: int) -> int:
+    """Kernels one batch solve launches: per factorizing round the factorization (level launches, the range or the
+    shared-memory region, the dense front), the solves, step and advance; per round the start, fill, test and lane
+    count; per solve the install and result gathers (6).  Matches the ncu launch lists: 802 per FP64 solve of the
+    9,241-bus / 500-outage batch under schedule 4, 782 under the level schedule with 2-lane tiles (scaled plan)."""
+    schedule, lanes = int(sched[0]), int(sched[1])
+    f, _, fw, bw = s.levels()
+    wf, wfw, wbw = np.diff(f), np.diff(fw), np.diff(bw)
+    nl, nf, nb = len(wf), len(wfw), len(wbw)
+    factor_to = nl - 1 if dense else nl
+    factor_from = factor_to
+    while factor_from > 0 and wf[factor_from - 1] <= NARROW:
+        factor_from -= 1
+    region_from = factor_to
+    if not deferred:
+        region_from = factor_from
+        while region_from < factor_to and f[factor_to] - f[region_from] > REGION_SLOTS:
+            region_from += 1
+    for lv in range(region_from, factor_to):
+        if wf[lv] > REGION_THREADS:
+            region_from = lv + 1
+    fwd_from = nf
+    while fwd_from > 0 and wfw[fwd_from - 1] <= NARROW:
+        fwd_from -= 1
+    bwd_until = 0
+    while bwd_until < nb and wbw[bwd_until] <= NARROW:
+        bwd_until += 1
+    fwd_region = 0 < fw[nf] - fw[fwd_from] <= SOLVE_REGION_SLOTS
+    bwd_region = 0 < bw[bwd_until] <= SOLVE_REGION_SLOTS
+    front = 1 if dense else 0
+    if schedule == 1:                       # the whole Newton loop in one persistent launch
+        return 1 + 6
+    if schedule == 2:                       # cooperative sweeps: one launch per factorization and per sweep
+        factor, solve = 1 + 1 + front, 2 + front + 2
+    else:
+        if schedule in (3, 4) and f[factor_to] - f[region_from] > 0:
+            factor = region_from + 2 + (nl - factor_to)
+        elif lanes > 0:
+            factor = factor_from + 1 + (nl - factor_to)
+        else:
+            factor = nl
+        factor += 1 + front                 # lane trouble flags, dense front
+        solve = 2 + front                   # right-hand side, scatter, dense front rows
+        if schedule == 4 and fwd_region:
+            solve += fwd_from + 2
+        elif schedule == 4 or lanes <= 0:
+            solve += nf
+        else:
+            solve += fwd_from + 1
+        if schedule == 4 and bwd_region:
+            solve += 1 + (nb - bwd_until)
+        elif schedule == 4 or lanes <= 0:
+            solve += nb
+        else:
+            solve += 1 + (nb - bwd_until)
+    per_round = factor + solve + 2 + (1 if mixed else 0)   # step, advance, (mixed) FP64-refactor lane count
+    return int(rounds * per_round + (rounds + 1) * 4 + 6 + refine_rounds * 3)
+
+
 def algorithmic_bytes(s, p, iterations_total: int, precision_bytes: int, refinement: int):
     """Bytes one scenario-iteration must move (J once, LU written and read once, six n-vectors), summed."""
     nnz_lu = s.n_lu_blocks * 4
@@ -311,9 +379,14 @@ def run_engine(args, rank: int, world: int):
                       "solve_levels": s.forward_levels + s.backward_levels, "block_ops": s.block_ops},
         "clocks": sampler.summary(),
     }
-    levels = s.factor_levels + (s.forward_levels + s.backward_levels + 2) * (1 + refinement)
-    per_iter = 1 + 1 + 1 + levels + refinement + 2
-    line["gpu_launches"] = int(per_iter * (tot_iters / args.steps / ns + 1) * args.steps)
+    rounds = max(ph["iterations"], 1)
+    per_solve = launches_per_solve(s, sched, rounds, args.plan == "dense", args.plan == "deferred",
+                                   precision == native.MIXED, (rounds - 1) if refinement > 0 else 0)
+    if learned is not None:
+        per_solve += GNN_LAUNCHES + 6          # the prediction, the two-start selection (2 fills and 4 small kernels)
+    line["gpu_launches"] = int(per_solve * args.steps)
+    line["gpu_launches_basis"] = (f"{per_solve} per step: the level structure under the schedule in force over "
+                                  f"{rounds} factorizing Newton rounds (the same count as the ncu launch lists)")
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, outs, args.cpu_sample)
     if world > 1:
