@@ -47,6 +47,37 @@ int olfgpu_create_structure(int n, int nCb, const double* cbParams, const int* c
                             const int* shIndices, int nIdentityRows, const int* identityRows, int ordering,
                             int64_t* structureOut);
 
+/*
+ * StructureNative.createStructure with the reference's full argument list, in its order (structure_jni.cu:7-137;
+ * StructureNative.java:49-59): every Java array as a pointer and its length (null / 0 when absent).  Element counts
+ * come from the index strides (closed 12, open 6, shunt 5).  The families this engine does not model must be empty
+ * (HVDC AC emulation, DISTR_Q, zero-impedance branches, DISTR_RHO, DISTR_SHUNT_B, load models, reactive relocation
+ * candidates), and the per-element "none" arrays must hold -1 only (closedBranchPhaseControlSide,
+ * openBranchAlternateReactiveDestination, the relocation group maps; reactiveRelocationGroupStart empty or [0]);
+ * otherwise the call fails naming the argument.  ordering as olfgpu_create_structure.
+ */
+int olfgpu_create_structure_full(
+    int n, const double* cbParams, int cbParamsLength, const int* cbIndices, int cbIndicesLength,
+    const double* obParams, int obParamsLength, const int* obIndices, int obIndicesLength, const double* shParams,
+    int shParamsLength, const int* shIndices, int shIndicesLength, const double* hvdcParams, int hvdcParamsLength,
+    const int* hvdcIndices, int hvdcIndicesLength, const int* distrQElement, int distrQElementLength,
+    const int* distrQSide, int distrQSideLength, const double* distrQWeight, int distrQWeightLength,
+    const int* distrQRow, int distrQRowLength, const int* distrQKind, int distrQKindLength, const double* zibParams,
+    int zibParamsLength, const int* zibIndices, int zibIndicesLength, const int* distrRhoRow, int distrRhoRowLength,
+    const int* distrRhoColumn, int distrRhoColumnLength, const double* distrRhoCoefficient,
+    int distrRhoCoefficientLength, const int* distrShuntBRow, int distrShuntBRowLength, const int* distrShuntBColumn,
+    int distrShuntBColumnLength, const double* distrShuntBCoefficient, int distrShuntBCoefficientLength,
+    const int* cbPhaseControlSide, int cbPhaseControlSideLength, const double* loadModelParams,
+    int loadModelParamsLength, const int* loadModelIndices, int loadModelIndicesLength,
+    const int* reactiveRelocationGroupStart, int reactiveRelocationGroupStartLength,
+    const int* reactiveRelocationCandidateRows, int reactiveRelocationCandidateRowsLength,
+    const int* obAlternateReactiveDestination, int obAlternateReactiveDestinationLength,
+    const int* zibAlternateReactiveDestination, int zibAlternateReactiveDestinationLength,
+    const int* reactiveRelocationDependentBaseGroup, int reactiveRelocationDependentBaseGroupLength,
+    const int* reactiveRelocationBaseTargetRow, int reactiveRelocationBaseTargetRowLength,
+    const int* reactiveRelocationDependentGroupOfRow, int reactiveRelocationDependentGroupOfRowLength,
+    const int* identityRows, int identityRowsLength, int ordering, int64_t* structureOut);
+
 /* StructureNative.destroyStructure (structure_jni.cu:143-149): drops the caller's reference; contexts keep theirs. */
 int olfgpu_destroy_structure(int64_t structure);
 
@@ -70,6 +101,14 @@ int olfgpu_structure_export(int64_t structure, int* rowMap, int* rowPtr, int* co
 int olfgpu_structure_levels(int64_t structure, int* factorLevelPtr, int* forwardLevelPtr, int* backwardLevelPtr,
                             int64_t* levelOps);
 
+/*
+ * The subtree bins of the structure's wide levels (no counterpart in the reference; the schedule 5 of
+ * olfgpu_set_schedule runs them): plans them on the host, checks that they keep every dependency of the factorization
+ * and of both sweeps (fails naming the first violation otherwise), and writes {bins, LU blocks in bins, most levels of
+ * a bin, LU blocks left on the wide levels, positions in bins, wide factorization levels} into stats6.
+ */
+int olfgpu_structure_subtrees(int64_t structure, int64_t* stats6);
+
 /* StructureNative.recommendBatchSize (structure_jni.cu:151-180): the bank that fits 70 % of free device memory. */
 int olfgpu_recommend_batch_size(int64_t structure, int maxCap, int mode, int* batchOut);
 
@@ -85,6 +124,56 @@ int olfgpu_create_batch_context(int64_t structure, int nScenarios, int mode, int
                                 const double* rlTargetV, const double* rlNomV, const int* rlPRow,
                                 const double* rlStaticP, const int* rlIdRank, int64_t* contextOut);
 
+/*
+ * BatchSolveNative.createBatchContext with the reference's full argument list (batch_solve_jni.cu:29-81;
+ * BatchSolveNative.java:41-48), arrays as pointer + length.  The reactive-limit entries (voltage row, Q limits, load Q,
+ * target V; all of one length) are installed without their forced-PV election keys, which
+ * olfgpu_set_reactive_limit_strongest_pv_keys supplies before the first solve (a solve with entries but no keys
+ * fails, as batch_solve_jni.cu:103-111 does).  reactiveLimitFlags must be 0 (voltage-monitoring SVCs are not
+ * modelled), rowSlope zero (no voltage slope), and the distributed-slack tables empty; slackBusPhiRow,
+ * slackBusTargetP, the factor mode and the margins only concern distributed slack and are ignored.
+ */
+int olfgpu_create_batch_context_full(
+    int64_t structure, int nScenarios, int mode, const int* rlVoltageRow, int rlVoltageRowLength,
+    const double* rlMinQ, int rlMinQLength, const double* rlMaxQ, int rlMaxQLength, const double* rlLoadQ,
+    int rlLoadQLength, const double* rlTargetV, int rlTargetVLength, const signed char* rlFlags, int rlFlagsLength,
+    const double* rowSlope, int rowSlopeLength, const int* dsBusPhiRow, int dsBusPhiRowLength,
+    const double* dsBusFactor, int dsBusFactorLength, int slackBusPhiRow, double slackBusTargetP,
+    const double* dsBusBaseTargetP, int dsBusBaseTargetPLength, const double* dsBusMaxDelta, int dsBusMaxDeltaLength,
+    const double* dsBusMinDelta, int dsBusMinDeltaLength, int dsFactorMode, const double* dsBusMarginUp,
+    int dsBusMarginUpLength, const double* dsBusMarginDown, int dsBusMarginDownLength, double slackBusMarginUp,
+    double slackBusMarginDown, int64_t* contextOut);
+
+/* ReactiveLimitsNative.setBatchReactiveLimitStrongestPvKeys (reactive_limits_jni.cu:118-145): per reactive-limit
+ * entry its nominal V, P row (-1: static P), static P and id rank; count must equal the entries. */
+int olfgpu_set_reactive_limit_strongest_pv_keys(int64_t context, const double* nomV, const int* pRow,
+                                                const double* staticP, const int* idRank, int count);
+
+/*
+ * Bank slots (BatchSolveNative.beginBatchInstall / readBatchHandedBackSlots / setBatchStatesToHost,
+ * batch_solve_jni.cu:404-465): olfgpu_begin_batch_install chooses the bank slots the next full solve installs its
+ * scenarios into (local scenario j into bankSlots[j], each slot at most once; count 0: the whole bank, j into j); the
+ * other slots stay idle during that solve.  olfgpu_read_handed_back_slots writes the slots of the last full solve's
+ * result rows, in row order (count receives their number).  With olfgpu_set_states_to_host(ctx, 0) the full solve's
+ * result rows are [iterations, ||F||inf, status] alone (rows of 3) and the states stay on the device, where
+ * olfgpu_read_batch_states copies the states of chosen slots ([nSlots][n]).  olfgpu_states_to_host reads the switch.
+ */
+int olfgpu_begin_batch_install(int64_t context, const int* bankSlots, int count);
+int olfgpu_read_handed_back_slots(int64_t context, int* slots, int maxCount, int* count);
+int olfgpu_set_states_to_host(int64_t context, int statesToHost);
+int olfgpu_states_to_host(int64_t context, int* statesToHost);
+int olfgpu_read_batch_states(int64_t context, int nSlots, const int* slots, double* out);
+
+/* DriverNative.setBatchOuterLoops (driver_jni.cu:11-18): the reactive-limit outer loop on or off for the following
+ * solves; the distributed-slack outer loop is not available (enabling it fails). */
+int olfgpu_set_outer_loops(int64_t context, int distributedSlack, int reactiveLimits);
+
+/* A context's sizes and counters: n, elements, bank size, scenarios the next full solve installs, batched Newton
+ * iterations of the last solve (BatchReadbackNative.readBatchNewtonLoopIterations), full solves run
+ * (BatchReadbackNative.readBatchSolveCount).  Any pointer may be null. */
+int olfgpu_context_info(int64_t context, int* n, int* nElements, int* nScenarios, int* installed,
+                        int* batchedIterations, int64_t* solveCount);
+
 /* BatchSolveNative.destroyBatchContext (batch_solve_jni.cu:396-401). */
 int olfgpu_destroy_batch_context(int64_t context);
 
@@ -98,10 +187,11 @@ int olfgpu_set_linear_solver_settings(int64_t context, int precision, int refine
 
 /*
  * Mixed-precision controls (no counterpart in the reference; precision 1 only).  The refinement steps run only in
- * iterations where some factorizing scenario's max |F| is below refineBelow (default 1e-5; infinity: every iteration):
- * far from convergence the next Newton iteration corrects the FP32 solve's error itself.  Each step computes the FP64
- * residual r = -F - J dx and runs its correction solve only while some scenario's max |r| exceeds a tenth of the
- * mismatch tolerance.  A scenario whose FP32
+ * iterations where some factorizing scenario's max |F| is below refineBelow (default 1e-2, every step
+ * that can land below the tolerance; infinity: every iteration):
+ * far from convergence the next Newton iteration corrects the FP32 solve's error itself.  Each step of such a
+ * scenario computes the FP64 residual r = -F - J dx and the correction solve, until the correction is below the bound
+ * of olfgpu_set_refinement_bound.  A scenario whose FP32
  * factorization meets a pivot block with growth above growthLimit (condition estimate max|D| max|inv D|, or max|D|
  * over the largest entry of its Jacobian block; default 1e4) is flagged: in the level schedule its factorization and
  * solve are redone in FP64 in the same iteration (and every later one of the solve); the persistent schedules give
@@ -148,6 +238,70 @@ int olfgpu_solve_batch_context(int64_t context, const double* x0Base, const doub
                                int nScenarios, int nElements, const unsigned char* disabled, int nTargetOverrides,
                                const int* targetOverrideIndex, const double* targetOverrideValue, int maxIter,
                                double tol, double reactiveLimitTol, int maxOuter, int maxPqPvSwitch, double* out);
+
+/*
+ * BatchSolveNative.solveBatchContext with the reference's full argument list, in its order (batch_solve_jni.cu:84-100;
+ * BatchSolveNative.java:106-125): every Java array argument is a pointer and its length (null or length 0 when the
+ * caller has none), so a JNI shim forwards each one as it comes.  Supported beyond olfgpu_solve_batch_context:
+ *   convEpsPerEq > 0: OLF's stopping criterion ||F||2 < sqrt(convEpsPerEq^2 n) (newton_iteration.cu:105,241-250)
+ *     instead of ||F||inf < tol;
+ *   stateVectorScalingMode 0 NONE or 2 MAX_VOLTAGE_CHANGE with maxDv, maxDphi and varType [n] (0 BUS_V, 1 BUS_PHI;
+ *     state_vector_scaling.cu:53-97); 1 LINE_SEARCH is rejected;
+ *   skipReactiveLimitsPhase != 0: this solve runs without the reactive-limit outer loop;
+ *   x0PerScenario [nScenarios * n] (the reference's x0Full).
+ * Rejected with an error naming the argument when non-empty (families this engine does not model): the distributed-
+ * slack overrides and anchor shifts, the reactive-limit target-V / delta / capability-curve overrides, the shunt and
+ * closed-branch parameter overrides, the reactive-limit seed state, the zero-impedance branch lists (and
+ * nBaseClosedZeroImpedanceBranches != 0), and pauseAtEnded != 0.  slackDistTol and rejectSlackDistributionFailure
+ * only concern distributed slack and are accepted and ignored.  out [nScenarios][n + 3] as olfgpu_solve_batch_context.
+ */
+int olfgpu_solve_batch_context_full(
+    int64_t context, const double* x0Base, int x0BaseLength, const double* targetBase, int targetBaseLength,
+    const int* rowModeEntries, int rowModeEntriesLength, const int* baseRowMode, int baseRowModeLength,
+    const unsigned char* disabledMask, int nScenarios, int nElements, const int* targetOverrideIndex,
+    int targetOverrideIndexLength, const double* targetOverrideValue, int targetOverrideValueLength,
+    const int* distributedSlackOverrideBus, int distributedSlackOverrideBusLength,
+    const double* distributedSlackOverrideFactorDelta, int distributedSlackOverrideFactorDeltaLength,
+    const double* distributedSlackOverrideBaseTargetPDelta, int distributedSlackOverrideBaseTargetPDeltaLength,
+    const double* distributedSlackOverrideMaxDelta, int distributedSlackOverrideMaxDeltaLength,
+    const double* distributedSlackOverrideMinDelta, int distributedSlackOverrideMinDeltaLength,
+    const double* distributedSlackBusAnchorShift, int distributedSlackBusAnchorShiftLength,
+    const double* slackBusAnchorShift, int slackBusAnchorShiftLength,
+    const int* reactiveLimitTargetVOverrideScenarioEntry, int reactiveLimitTargetVOverrideScenarioEntryLength,
+    const double* reactiveLimitTargetVOverrideValue, int reactiveLimitTargetVOverrideValueLength,
+    const int* reactiveLimitDeltaOverrideScenarioEntry, int reactiveLimitDeltaOverrideScenarioEntryLength,
+    const double* reactiveLimitDeltaOverrideValues, int reactiveLimitDeltaOverrideValuesLength,
+    const int* reactiveCapabilityCurveOverrideScenarioCurve, int reactiveCapabilityCurveOverrideScenarioCurveLength,
+    const double* reactiveCapabilityCurveOverrideStepScale, int reactiveCapabilityCurveOverrideStepScaleLength,
+    int maxIter, double tol, double reactiveLimitTol, double slackDistTol, double convEpsPerEq,
+    int stateVectorScalingMode, double maxDv, double maxDphi, const int* varType, int varTypeLength,
+    const double* x0PerScenario, int x0PerScenarioLength, const int* shuntOvSlotElem, int shuntOvSlotElemLength,
+    const double* shuntOvGb, int shuntOvGbLength, const int* reactiveLimitsSeedState, int reactiveLimitsSeedStateLength,
+    const int* closedBranchParameterOverrideScenarioElement, int closedBranchParameterOverrideScenarioElementLength,
+    const double* closedBranchParameterOverrideValues, int closedBranchParameterOverrideValuesLength,
+    int maxOuterIterations, int maxPqPvSwitch, int rejectSlackDistributionFailure, int skipReactiveLimitsPhase,
+    int nBaseClosedZeroImpedanceBranches, const int* zeroImpedanceBranchCloseScenarioElement,
+    int zeroImpedanceBranchCloseScenarioElementLength, const int* zeroImpedanceBranchOpenScenarioElement,
+    int zeroImpedanceBranchOpenScenarioElementLength, int pauseAtEnded, double* out);
+
+/*
+ * ReactiveLimitsNative.setBatchRealisticCheck (reactive_limits_jni.cu:172-195; realistic_voltage_check.cu:23-44):
+ * rowChecked [n] marks the voltage rows OLF's realistic-voltage check reads; a converged scenario with a checked
+ * voltage outside [minV, maxV] ends UNREALISTIC_STATE (status 2), its state kept.  enabled = 0 (or rowChecked null)
+ * clears the check.  The level and cooperative schedules apply it.
+ */
+int olfgpu_set_realistic_check(int64_t context, const unsigned char* rowChecked, double minV, double maxV, int enabled);
+
+/*
+ * Mixed precision (no counterpart in the reference): in an iteration where a scenario's max |F| is below refineBelow
+ * (olfgpu_set_mixed_precision_controls), the scenario refines its FP32 solve (FP64 residual, correction solve) until
+ * the correction's max |d| falls to correctionBound or below (default 1e-11), at most refinementSteps times: its last
+ * Newton step is then FP64-accurate.  With olfgpu_set_fp64_restart enabled (the default), a scenario whose mixed-
+ * precision solve fails (diverged, iteration budget, failed linear solve) restarts once with FP64 factorizations and
+ * solves from its start, so it ends as the FP64 engine ends it (level and cooperative schedules, no reactive limits).
+ */
+int olfgpu_set_refinement_bound(int64_t context, double correctionBound);
+int olfgpu_set_fp64_restart(int64_t context, int enable);
 
 /*
  * Statistics of the context's last solve: device milliseconds of its Newton iterations (CUDA events on the context's
@@ -305,9 +459,11 @@ int olfgpu_gnn_compose_start_compact(int nScenarios, int nb, const float* predBa
  * Scratch: one fixed 64 MiB device array inside the library, which every GPU that loads the library holds until the
  * process exits; a batch whose Jacobian, factors and work vectors do not fit is rejected with an error naming the
  * largest batch that fits.  The structure must already be on the current device (creating a batch context on it
- * uploads it).  The first call on each device looks up the array's address (set-up, no allocation); make that first
- * call before any stream capture.  All calls share the one array and it keeps the previous call's contents (what must
- * start at zero is cleared on every call): calls whose work overlaps on the GPU race, so order them on one stream.
+ * uploads it).  The first call on each device looks up the array's address (set-up, no allocation), and so does the
+ * first call after the device's CUDA context was re-created (cudaDeviceReset); make that first call before any stream
+ * capture.  All calls share the one array and it keeps the previous call's contents (what must start at zero is
+ * cleared on every call): calls whose work overlaps on the GPU race, so order them on one stream.  A scenario whose
+ * factorization meets a (near-)singular 2x2 pivot gets NaN in every entry of its outDevice row.
  */
 int olfgpu_linear_solve_noalloc(int64_t structure, int nScenarios, const double* csrValsDevice,
                                 const double* rhsDevice, double* outDevice, int precision, void* stream);

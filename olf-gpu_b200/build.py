@@ -31,6 +31,24 @@ def _compile(src: str, verbose: bool) -> str:
     return obj
 
 
+JNI_SRC = os.path.join(HERE, "jni", "olfgpu_jni.cpp")
+JNI_LIB = os.path.join(OUT, "libolfgpu.so")
+
+
+def _build_jni(verbose: bool) -> str:
+    """The JNI layer (lib/libolfgpu.so, the library name the Java side loads): plain C++ over the engine's C ABI,
+    linked against lib/libolfgpu_b200.so (found next to it at run time); only the JNI symbols are exported."""
+    deps = [JNI_SRC, os.path.join(HERE, "jni", "jni.h"), os.path.join(HERE, "..", "include", "olfgpu_b200.h"), LIB]
+    if os.path.exists(JNI_LIB) and all(os.path.getmtime(JNI_LIB) >= os.path.getmtime(d) for d in deps):
+        return JNI_LIB
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-fvisibility=hidden", "-Wall", "-o", JNI_LIB, JNI_SRC,
+           "-L" + OUT, "-lolfgpu_b200", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+    return JNI_LIB
+
+
 def build(verbose: bool = False) -> str:
     os.makedirs(OUT, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
@@ -40,6 +58,7 @@ def build(verbose: bool = False) -> str:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
+    _build_jni(verbose)
     return LIB
 
 

@@ -102,6 +102,88 @@ extern "C" int olfgpu_create_structure(int n, int nCb, const double* cbParams, c
     });
 }
 
+extern "C" int olfgpu_create_structure_full(
+    int n, const double* cbParams, int cbParamsLength, const int* cbIndices, int cbIndicesLength,
+    const double* obParams, int obParamsLength, const int* obIndices, int obIndicesLength, const double* shParams,
+    int shParamsLength, const int* shIndices, int shIndicesLength, const double* hvdcParams, int hvdcParamsLength,
+    const int* hvdcIndices, int hvdcIndicesLength, const int* distrQElement, int distrQElementLength,
+    const int* distrQSide, int distrQSideLength, const double* distrQWeight, int distrQWeightLength,
+    const int* distrQRow, int distrQRowLength, const int* distrQKind, int distrQKindLength, const double* zibParams,
+    int zibParamsLength, const int* zibIndices, int zibIndicesLength, const int* distrRhoRow, int distrRhoRowLength,
+    const int* distrRhoColumn, int distrRhoColumnLength, const double* distrRhoCoefficient,
+    int distrRhoCoefficientLength, const int* distrShuntBRow, int distrShuntBRowLength, const int* distrShuntBColumn,
+    int distrShuntBColumnLength, const double* distrShuntBCoefficient, int distrShuntBCoefficientLength,
+    const int* cbPhaseControlSide, int cbPhaseControlSideLength, const double* loadModelParams,
+    int loadModelParamsLength, const int* loadModelIndices, int loadModelIndicesLength,
+    const int* reactiveRelocationGroupStart, int reactiveRelocationGroupStartLength,
+    const int* reactiveRelocationCandidateRows, int reactiveRelocationCandidateRowsLength,
+    const int* obAlternateReactiveDestination, int obAlternateReactiveDestinationLength,
+    const int* zibAlternateReactiveDestination, int zibAlternateReactiveDestinationLength,
+    const int* reactiveRelocationDependentBaseGroup, int reactiveRelocationDependentBaseGroupLength,
+    const int* reactiveRelocationBaseTargetRow, int reactiveRelocationBaseTargetRowLength,
+    const int* reactiveRelocationDependentGroupOfRow, int reactiveRelocationDependentGroupOfRowLength,
+    const int* identityRows, int identityRowsLength, int ordering, int64_t* structureOut) {
+    return guarded([&] {
+        if (!structureOut) throw std::runtime_error("null output handle");
+        *structureOut = 0;
+        // element counts from the index strides (structure_jni.cu:55-63)
+        const int nCb = cbIndicesLength / 12, nOb = obIndicesLength / 6, nSh = shIndicesLength / 5;
+        if (cbIndicesLength % 12 || cbParamsLength != nCb * 8) throw std::runtime_error("closed-branch arrays: bad lengths");
+        if (obIndicesLength % 6 || obParamsLength != nOb * 7) throw std::runtime_error("open-branch arrays: bad lengths");
+        if (shIndicesLength % 5 || shParamsLength != nSh * 2) throw std::runtime_error("shunt arrays: bad lengths");
+        (void)hvdcParams; (void)hvdcIndices; (void)distrQElement; (void)distrQSide; (void)distrQWeight; (void)distrQRow;
+        (void)distrQKind; (void)zibParams; (void)zibIndices; (void)distrRhoRow; (void)distrRhoColumn;
+        (void)distrRhoCoefficient; (void)distrShuntBRow; (void)distrShuntBColumn; (void)distrShuntBCoefficient;
+        (void)loadModelParams; (void)loadModelIndices; (void)reactiveRelocationCandidateRows;
+        (void)zibAlternateReactiveDestination;
+        const std::pair<const char*, int> empty[] = {
+            {"hvdcAcEmulationParameters", hvdcParamsLength}, {"hvdcAcEmulationIndices", hvdcIndicesLength},
+            {"distrQElement", distrQElementLength}, {"distrQSide", distrQSideLength},
+            {"distrQWeight", distrQWeightLength}, {"distrQRow", distrQRowLength}, {"distrQKind", distrQKindLength},
+            {"zeroImpedanceBranchParameters", zibParamsLength}, {"zeroImpedanceBranchIndices", zibIndicesLength},
+            {"distrRhoRow", distrRhoRowLength}, {"distrRhoColumn", distrRhoColumnLength},
+            {"distrRhoCoefficient", distrRhoCoefficientLength}, {"distrShuntBRow", distrShuntBRowLength},
+            {"distrShuntBColumn", distrShuntBColumnLength}, {"distrShuntBCoefficient", distrShuntBCoefficientLength},
+            {"loadModelParameters", loadModelParamsLength}, {"loadModelIndices", loadModelIndicesLength},
+            {"reactiveRelocationCandidateRows", reactiveRelocationCandidateRowsLength},
+            {"zeroImpedanceBranchAlternateReactiveDestination", zibAlternateReactiveDestinationLength},
+        };
+        for (const auto& e : empty) {
+            if (e.second != 0) {
+                throw std::runtime_error(std::string("createStructure: ") + e.first +
+                                         " is not supported by this engine (pass null or an empty array)");
+            }
+        }
+        // arrays that may carry "none" entries: every entry must say none
+        auto allNone = [](const char* what, const int* a, int len) {
+            for (int k = 0; k < len; k++) {
+                if (a[k] != -1) {
+                    throw std::runtime_error(std::string("createStructure: ") + what + " holds an entry (" +
+                                             std::to_string(a[k]) + " at " + std::to_string(k) +
+                                             "): not supported by this engine");
+                }
+            }
+        };
+        allNone("closedBranchPhaseControlSide", cbPhaseControlSide, cbPhaseControlSideLength);
+        allNone("openBranchAlternateReactiveDestination", obAlternateReactiveDestination,
+                obAlternateReactiveDestinationLength);
+        allNone("reactiveRelocationDependentBaseGroup", reactiveRelocationDependentBaseGroup,
+                reactiveRelocationDependentBaseGroupLength);
+        allNone("reactiveRelocationBaseTargetRow", reactiveRelocationBaseTargetRow, reactiveRelocationBaseTargetRowLength);
+        allNone("reactiveRelocationDependentGroupOfRow", reactiveRelocationDependentGroupOfRow,
+                reactiveRelocationDependentGroupOfRowLength);
+        // reactiveRelocationGroupStart = [0] (or empty) when there is no relocation group
+        if (reactiveRelocationGroupStartLength > 1 ||
+            (reactiveRelocationGroupStartLength == 1 && reactiveRelocationGroupStart[0] != 0)) {
+            throw std::runtime_error("createStructure: reactive relocation groups are not supported by this engine");
+        }
+        auto s = std::make_shared<NetStructure>();
+        s->host = buildStructure(n, nCb, cbParams, cbIndices, nOb, obParams, obIndices, nSh, shParams, shIndices,
+                                 identityRowsLength, identityRows, ordering);
+        *structureOut = reinterpret_cast<int64_t>(new StructurePtr(s));
+    });
+}
+
 extern "C" int olfgpu_destroy_structure(int64_t structure) {
     return guarded([&] { delete reinterpret_cast<StructurePtr*>(structure); });
 }
@@ -166,6 +248,30 @@ extern "C" int olfgpu_structure_levels(int64_t structure, int* factorLevelPtr, i
     });
 }
 
+extern "C" int olfgpu_structure_subtrees(int64_t structure, int64_t* stats6) {
+    return guarded([&] {
+        const BlockPlan& p = structureOf(structure)->host.plan;
+        const NarrowBounds nbd = narrowBounds(p);
+        const SubtreeBinsHost h = planSubtreeBins(p, nbd);
+        const std::string err = checkSubtreeBins(p, nbd, h);
+        if (!err.empty()) throw std::runtime_error("subtree bins: " + err);
+        if (stats6) {
+            int maxLevels = 0;
+            for (int b = 0; b < h.nBins; b++) maxLevels = std::max(maxLevels, h.levPtr[b + 1] - h.levPtr[b]);
+            int topWide = 0;
+            for (int l = 0; l < nbd.factorFrom; l++) topWide += h.topLevelPtr[l + 1] - h.topLevelPtr[l];
+            int binPos = 0;
+            for (int v : h.bwdBinOf) binPos += v >= 0;
+            stats6[0] = h.nBins * 100 + static_cast<int>(h.phasePtr.size()) - 1;
+            stats6[1] = static_cast<int64_t>(h.task.size());
+            stats6[2] = maxLevels;
+            stats6[3] = topWide;
+            stats6[4] = binPos;
+            stats6[5] = nbd.factorFrom;
+        }
+    });
+}
+
 extern "C" int olfgpu_recommend_batch_size(int64_t structure, int maxCap, int mode, int* batchOut) {
     return guarded([&] {
         if (!batchOut) throw std::runtime_error("null output");
@@ -200,6 +306,69 @@ extern "C" int olfgpu_create_batch_context(int64_t structure, int nScenarios, in
     });
 }
 
+extern "C" int olfgpu_create_batch_context_full(
+    int64_t structure, int nScenarios, int mode, const int* rlVoltageRow, int rlVoltageRowLength,
+    const double* rlMinQ, int rlMinQLength, const double* rlMaxQ, int rlMaxQLength, const double* rlLoadQ,
+    int rlLoadQLength, const double* rlTargetV, int rlTargetVLength, const signed char* rlFlags, int rlFlagsLength,
+    const double* rowSlope, int rowSlopeLength, const int* dsBusPhiRow, int dsBusPhiRowLength,
+    const double* dsBusFactor, int dsBusFactorLength, int slackBusPhiRow, double slackBusTargetP,
+    const double* dsBusBaseTargetP, int dsBusBaseTargetPLength, const double* dsBusMaxDelta, int dsBusMaxDeltaLength,
+    const double* dsBusMinDelta, int dsBusMinDeltaLength, int dsFactorMode, const double* dsBusMarginUp,
+    int dsBusMarginUpLength, const double* dsBusMarginDown, int dsBusMarginDownLength, double slackBusMarginUp,
+    double slackBusMarginDown, int64_t* contextOut) {
+    return guarded([&] {
+        if (!contextOut) throw std::runtime_error("null output handle");
+        *contextOut = 0;
+        const int nRl = rlVoltageRowLength;
+        if (rlMinQLength != nRl || rlMaxQLength != nRl || rlLoadQLength != nRl || rlTargetVLength != nRl ||
+            (rlFlagsLength != 0 && rlFlagsLength != nRl)) {
+            throw std::runtime_error("createBatchContext: reactive-limit arrays differ in length");
+        }
+        for (int i = 0; i < rlFlagsLength; i++) {
+            if (rlFlags[i] != 0) {
+                throw std::runtime_error("createBatchContext: reactive-limit entry " + std::to_string(i) +
+                                         " is a voltage-monitoring SVC (flag 1): not supported by this engine");
+            }
+        }
+        for (int r = 0; r < rowSlopeLength; r++) {
+            if (rowSlope[r] != 0.0) {
+                throw std::runtime_error("createBatchContext: voltage slope on row " + std::to_string(r) +
+                                         " is not supported by this engine");
+            }
+        }
+        (void)dsBusPhiRow; (void)dsBusFactor; (void)slackBusPhiRow; (void)slackBusTargetP; (void)dsBusBaseTargetP;
+        (void)dsBusMaxDelta; (void)dsBusMinDelta; (void)dsFactorMode; (void)dsBusMarginUp; (void)dsBusMarginDown;
+        (void)slackBusMarginUp; (void)slackBusMarginDown;
+        const std::pair<const char*, int> ds[] = {
+            {"distributedSlackBusPhiRow", dsBusPhiRowLength}, {"distributedSlackBusFactor", dsBusFactorLength},
+            {"distributedSlackBusBaseTargetP", dsBusBaseTargetPLength},
+            {"distributedSlackBusMaxDelta", dsBusMaxDeltaLength}, {"distributedSlackBusMinDelta", dsBusMinDeltaLength},
+            {"distributedSlackBusMarginUp", dsBusMarginUpLength},
+            {"distributedSlackBusMarginDown", dsBusMarginDownLength}};
+        for (const auto& e : ds) {
+            if (e.second != 0) {
+                throw std::runtime_error(std::string("createBatchContext: ") + e.first +
+                                         " (distributed slack) is not supported by this engine");
+            }
+        }
+        BatchContext* c = createContext(structureOf(structure), nScenarios, mode, nRl, rlVoltageRow, rlMinQ, rlMaxQ,
+                                        rlLoadQ, rlTargetV, nullptr, nullptr, nullptr, nullptr);
+        *contextOut = reinterpret_cast<int64_t>(c);
+    });
+}
+
+extern "C" int olfgpu_set_reactive_limit_strongest_pv_keys(int64_t context, const double* nomV, const int* pRow,
+                                                           const double* staticP, const int* idRank, int count) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        if (c.rl.nRl == 0) return;
+        if (count != c.rl.nRl || !nomV || !pRow || !staticP || !idRank) {
+            throw std::runtime_error("setBatchReactiveLimitStrongestPvKeys: array length != nReactiveLimitEntries");
+        }
+        setStrongestPvKeys(c, nomV, pRow, staticP, idRank);
+    });
+}
+
 extern "C" int olfgpu_destroy_batch_context(int64_t context) {
     return guarded([&] { delete reinterpret_cast<BatchContext*>(context); });
 }
@@ -222,11 +391,14 @@ extern "C" int olfgpu_set_schedule(int64_t context, int schedule, int lanesPerTi
             return;
         }
         if (schedule != SCHEDULE_LEVELS && schedule != SCHEDULE_PERSISTENT && schedule != SCHEDULE_COOP &&
-            schedule != SCHEDULE_LEVELS_SHARED && schedule != SCHEDULE_LEVELS_SHARED_ALL) {
+            schedule != SCHEDULE_LEVELS_SHARED && schedule != SCHEDULE_LEVELS_SHARED_ALL &&
+            schedule != SCHEDULE_SUBTREES) {
             throw std::runtime_error("unknown schedule");
         }
-        c.regionFactor = schedule == SCHEDULE_LEVELS_SHARED || schedule == SCHEDULE_LEVELS_SHARED_ALL;
-        c.regionSolve = schedule == SCHEDULE_LEVELS_SHARED_ALL;
+        c.regionFactor = schedule == SCHEDULE_LEVELS_SHARED || schedule == SCHEDULE_LEVELS_SHARED_ALL ||
+                         schedule == SCHEDULE_SUBTREES;
+        c.regionSolve = schedule == SCHEDULE_LEVELS_SHARED_ALL || schedule == SCHEDULE_SUBTREES;
+        c.subtrees = schedule == SCHEDULE_SUBTREES;
         if (c.regionFactor) schedule = SCHEDULE_LEVELS;
         if (schedule == SCHEDULE_COOP) {
             // cooperative sweeps have no tile parameters
@@ -254,6 +426,7 @@ extern "C" int olfgpu_get_schedule(int64_t context, int* schedule, int* lanesPer
         BatchContext& c = contextOf(context);
         if (schedule) {
             *schedule = c.schedule != SCHEDULE_LEVELS ? c.schedule
+                        : c.subtrees                 ? SCHEDULE_SUBTREES
                         : c.regionSolve              ? SCHEDULE_LEVELS_SHARED_ALL
                         : c.regionFactor             ? SCHEDULE_LEVELS_SHARED
                                                      : SCHEDULE_LEVELS;
@@ -286,6 +459,291 @@ extern "C" int olfgpu_solve_batch_context(int64_t context, const double* x0Base,
                                          targetOverrideValue, maxIter, tol, reactiveLimitTol, maxOuter, maxPqPvSwitch);
         solveBatch(c, r, out);
     });
+}
+
+extern "C" int olfgpu_solve_batch_context_full(
+    int64_t context, const double* x0Base, int x0BaseLength, const double* targetBase, int targetBaseLength,
+    const int* rowModeEntries, int rowModeEntriesLength, const int* baseRowMode, int baseRowModeLength,
+    const unsigned char* disabledMask, int nScenarios, int nElements, const int* targetOverrideIndex,
+    int targetOverrideIndexLength, const double* targetOverrideValue, int targetOverrideValueLength,
+    const int* distributedSlackOverrideBus, int distributedSlackOverrideBusLength,
+    const double* distributedSlackOverrideFactorDelta, int distributedSlackOverrideFactorDeltaLength,
+    const double* distributedSlackOverrideBaseTargetPDelta, int distributedSlackOverrideBaseTargetPDeltaLength,
+    const double* distributedSlackOverrideMaxDelta, int distributedSlackOverrideMaxDeltaLength,
+    const double* distributedSlackOverrideMinDelta, int distributedSlackOverrideMinDeltaLength,
+    const double* distributedSlackBusAnchorShift, int distributedSlackBusAnchorShiftLength,
+    const double* slackBusAnchorShift, int slackBusAnchorShiftLength,
+    const int* reactiveLimitTargetVOverrideScenarioEntry, int reactiveLimitTargetVOverrideScenarioEntryLength,
+    const double* reactiveLimitTargetVOverrideValue, int reactiveLimitTargetVOverrideValueLength,
+    const int* reactiveLimitDeltaOverrideScenarioEntry, int reactiveLimitDeltaOverrideScenarioEntryLength,
+    const double* reactiveLimitDeltaOverrideValues, int reactiveLimitDeltaOverrideValuesLength,
+    const int* reactiveCapabilityCurveOverrideScenarioCurve, int reactiveCapabilityCurveOverrideScenarioCurveLength,
+    const double* reactiveCapabilityCurveOverrideStepScale, int reactiveCapabilityCurveOverrideStepScaleLength,
+    int maxIter, double tol, double reactiveLimitTol, double slackDistTol, double convEpsPerEq,
+    int stateVectorScalingMode, double maxDv, double maxDphi, const int* varType, int varTypeLength,
+    const double* x0PerScenario, int x0PerScenarioLength, const int* shuntOvSlotElem, int shuntOvSlotElemLength,
+    const double* shuntOvGb, int shuntOvGbLength, const int* reactiveLimitsSeedState, int reactiveLimitsSeedStateLength,
+    const int* closedBranchParameterOverrideScenarioElement, int closedBranchParameterOverrideScenarioElementLength,
+    const double* closedBranchParameterOverrideValues, int closedBranchParameterOverrideValuesLength,
+    int maxOuterIterations, int maxPqPvSwitch, int rejectSlackDistributionFailure, int skipReactiveLimitsPhase,
+    int nBaseClosedZeroImpedanceBranches, const int* zeroImpedanceBranchCloseScenarioElement,
+    int zeroImpedanceBranchCloseScenarioElementLength, const int* zeroImpedanceBranchOpenScenarioElement,
+    int zeroImpedanceBranchOpenScenarioElementLength, int pauseAtEnded, double* out) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        const int n = c.net->host.n;
+        // the families and overrides this engine does not model must be empty (the Java side passes null or a
+        // zero-length array when it has none); the pointers themselves are never read
+        (void)distributedSlackOverrideBus; (void)distributedSlackOverrideFactorDelta;
+        (void)distributedSlackOverrideBaseTargetPDelta; (void)distributedSlackOverrideMaxDelta;
+        (void)distributedSlackOverrideMinDelta; (void)distributedSlackBusAnchorShift; (void)slackBusAnchorShift;
+        (void)reactiveLimitTargetVOverrideScenarioEntry; (void)reactiveLimitTargetVOverrideValue;
+        (void)reactiveLimitDeltaOverrideScenarioEntry; (void)reactiveLimitDeltaOverrideValues;
+        (void)reactiveCapabilityCurveOverrideScenarioCurve; (void)reactiveCapabilityCurveOverrideStepScale;
+        (void)shuntOvSlotElem; (void)shuntOvGb; (void)reactiveLimitsSeedState;
+        (void)closedBranchParameterOverrideScenarioElement; (void)closedBranchParameterOverrideValues;
+        (void)zeroImpedanceBranchCloseScenarioElement; (void)zeroImpedanceBranchOpenScenarioElement;
+        (void)slackDistTol; (void)rejectSlackDistributionFailure;
+        const std::pair<const char*, int> unsupported[] = {
+            {"distributedSlackOverrideBus", distributedSlackOverrideBusLength},
+            {"distributedSlackOverrideFactorDelta", distributedSlackOverrideFactorDeltaLength},
+            {"distributedSlackOverrideBaseTargetPDelta", distributedSlackOverrideBaseTargetPDeltaLength},
+            {"distributedSlackOverrideMaxDelta", distributedSlackOverrideMaxDeltaLength},
+            {"distributedSlackOverrideMinDelta", distributedSlackOverrideMinDeltaLength},
+            {"distributedSlackBusAnchorShift", distributedSlackBusAnchorShiftLength},
+            {"slackBusAnchorShift", slackBusAnchorShiftLength},
+            {"reactiveLimitTargetVOverrideScenarioEntry", reactiveLimitTargetVOverrideScenarioEntryLength},
+            {"reactiveLimitTargetVOverrideValue", reactiveLimitTargetVOverrideValueLength},
+            {"reactiveLimitDeltaOverrideScenarioEntry", reactiveLimitDeltaOverrideScenarioEntryLength},
+            {"reactiveLimitDeltaOverrideValues", reactiveLimitDeltaOverrideValuesLength},
+            {"reactiveCapabilityCurveOverrideScenarioCurve", reactiveCapabilityCurveOverrideScenarioCurveLength},
+            {"reactiveCapabilityCurveOverrideStepScale", reactiveCapabilityCurveOverrideStepScaleLength},
+            {"shuntOvSlotElem", shuntOvSlotElemLength},
+            {"shuntOvGb", shuntOvGbLength},
+            {"reactiveLimitsSeedState", reactiveLimitsSeedStateLength},
+            {"closedBranchParameterOverrideScenarioElement", closedBranchParameterOverrideScenarioElementLength},
+            {"closedBranchParameterOverrideValues", closedBranchParameterOverrideValuesLength},
+            {"zeroImpedanceBranchCloseScenarioElement", zeroImpedanceBranchCloseScenarioElementLength},
+            {"zeroImpedanceBranchOpenScenarioElement", zeroImpedanceBranchOpenScenarioElementLength},
+        };
+        for (const auto& u : unsupported) {
+            if (u.second < 0) throw std::runtime_error(std::string("negative length of ") + u.first);
+            if (u.second > 0) {
+                throw std::runtime_error(std::string("solveBatchContext: ") + u.first +
+                                         " is not supported by this engine (pass null or an empty array)");
+            }
+        }
+        if (nBaseClosedZeroImpedanceBranches != 0) {
+            throw std::runtime_error("solveBatchContext: zero-impedance branches are not supported by this engine");
+        }
+        if (pauseAtEnded != 0) {
+            throw std::runtime_error("solveBatchContext: pausing at ended scenarios (pauseAtEnded) is not supported");
+        }
+        auto need = [&](const char* what, const void* p, int len, int want) {
+            if (!p) return;
+            if (len != want) {
+                throw std::runtime_error(std::string("solveBatchContext: ") + what + " has length " +
+                                         std::to_string(len) + ", expected " + std::to_string(want));
+            }
+        };
+        need("x0Base", x0Base, x0BaseLength, n);
+        need("targetBase", targetBase, targetBaseLength, n);
+        need("baseRowMode", baseRowMode, baseRowModeLength, n);
+        need("varType", varType, varTypeLength, n);
+        need("x0PerScenario", x0PerScenario, x0PerScenarioLength, nScenarios * n);
+        if (rowModeEntriesLength % 3 != 0) throw std::runtime_error("rowModeEntries must hold (scenario, row, mode) triples");
+        if (targetOverrideIndexLength != targetOverrideValueLength) {
+            throw std::runtime_error("targetOverrideIndex and targetOverrideValue differ in length");
+        }
+        // the scenarios of this solve go into the bank slots chosen by olfgpu_begin_batch_install (local scenario j
+        // into slot installSlots[j]; none chosen: the whole bank, j into j); the other slots stay idle
+        const std::vector<int> slots = c.installSlots;
+        const int nLocal = slots.empty() ? c.nS : static_cast<int>(slots.size());
+        if (nScenarios != nLocal) {
+            throw std::runtime_error("scenario count " + std::to_string(nScenarios) +
+                                     " mismatch with the installed slots (" + std::to_string(nLocal) + ")");
+        }
+        if (!slots.empty() && c.deviceStart) {
+            throw std::runtime_error("a device-resident start cannot be combined with an installation into chosen slots");
+        }
+        // expanded to the whole bank when slots are chosen
+        std::vector<unsigned char> disBank, live;
+        std::vector<double> x0Bank, ovVal;
+        std::vector<int> rmeBank, ovIdx;
+        const unsigned char* dis = disabledMask;
+        const double* x0f = x0PerScenario;
+        const int* rme = rowModeEntries;
+        const int* toi = targetOverrideIndex;
+        const double* tov = targetOverrideValue;
+        int nS = nScenarios;
+        if (!slots.empty()) {
+            nS = c.nS;
+            disBank.assign(static_cast<size_t>(nS) * nElements, 0);
+            live.assign(nS, 0);
+            for (int j = 0; j < nLocal; j++) {
+                live[slots[j]] = 1;
+                if (disabledMask) {
+                    std::memcpy(&disBank[static_cast<size_t>(slots[j]) * nElements],
+                                disabledMask + static_cast<size_t>(j) * nElements, nElements);
+                }
+            }
+            dis = disabledMask ? disBank.data() : nullptr;
+            if (x0PerScenario) {
+                x0Bank.assign(static_cast<size_t>(nS) * n, 0.0);
+                for (int s2 = 0; s2 < nS; s2++)
+                    if (x0Base) std::memcpy(&x0Bank[static_cast<size_t>(s2) * n], x0Base, sizeof(double) * n);
+                for (int j = 0; j < nLocal; j++) {
+                    std::memcpy(&x0Bank[static_cast<size_t>(slots[j]) * n], x0PerScenario + static_cast<size_t>(j) * n,
+                                sizeof(double) * n);
+                }
+                x0f = x0Bank.data();
+            }
+            rmeBank.assign(rowModeEntries ? rowModeEntries : nullptr,
+                           rowModeEntries ? rowModeEntries + rowModeEntriesLength : nullptr);
+            for (size_t k = 0; k < rmeBank.size(); k += 3) {
+                if (rmeBank[k] < 0 || rmeBank[k] >= nLocal) throw std::runtime_error("rowMode entry outside the installed slots");
+                rmeBank[k] = slots[rmeBank[k]];
+            }
+            rme = rmeBank.empty() ? nullptr : rmeBank.data();
+            ovIdx.resize(targetOverrideIndexLength);
+            for (int k = 0; k < targetOverrideIndexLength; k++) {
+                const int v = targetOverrideIndex[k];
+                if (v < 0 || v >= nLocal * n) throw std::runtime_error("target override index out of range");
+                ovIdx[k] = slots[v / n] * n + v % n;
+            }
+            toi = ovIdx.empty() ? nullptr : ovIdx.data();
+        }
+        SolveRequest r = requestOf(x0Base, x0f, targetBase, baseRowMode, rowModeEntriesLength / 3, rme, nS,
+                                   nElements, dis, targetOverrideIndexLength, toi, tov, maxIter, tol,
+                                   reactiveLimitTol, maxOuterIterations, maxPqPvSwitch);
+        r.convEpsPerEq = convEpsPerEq;
+        r.stateVectorScalingMode = stateVectorScalingMode;
+        r.maxDv = maxDv;
+        r.maxDphi = maxDphi;
+        r.varType = varType;
+        r.skipReactiveLimits = skipReactiveLimitsPhase != 0;
+        r.laneLive = live.empty() ? nullptr : live.data();
+        c.solveCount++;
+        c.handedBack.resize(nLocal);
+        for (int j = 0; j < nLocal; j++) c.handedBack[j] = slots.empty() ? j : slots[j];
+        if (slots.empty() && c.statesToHost) {
+            solveBatch(c, r, out);
+            return;
+        }
+        // result rows of the installed scenarios, in installation order: [x(n), iterations, ||F||inf, status], or the
+        // three last alone when the states stay on the device (olfgpu_set_states_to_host)
+        std::vector<double> bank(static_cast<size_t>(nS) * (n + 3));
+        solveBatch(c, r, bank.data());
+        const int width = c.statesToHost ? n + 3 : 3;
+        for (int j = 0; j < nLocal; j++) {
+            const double* row = &bank[static_cast<size_t>(c.handedBack[j]) * (n + 3)];
+            if (out) std::memcpy(out + static_cast<size_t>(j) * width, row + (n + 3 - width), sizeof(double) * width);
+        }
+    });
+}
+
+extern "C" int olfgpu_context_info(int64_t context, int* n, int* nElements, int* nScenarios, int* installed,
+                                   int* batchedIterations, int64_t* solveCount) {
+    return guarded([&] {
+        const BatchContext& c = contextOf(context);
+        if (n) *n = c.net->host.n;
+        if (nElements) *nElements = c.net->host.nElements;
+        if (nScenarios) *nScenarios = c.nS;
+        if (installed) *installed = c.installSlots.empty() ? c.nS : static_cast<int>(c.installSlots.size());
+        if (batchedIterations) *batchedIterations = c.lastIterations;
+        if (solveCount) *solveCount = c.solveCount;
+    });
+}
+
+extern "C" int olfgpu_begin_batch_install(int64_t context, const int* bankSlots, int count) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        if (count < 0 || (count > 0 && !bankSlots)) throw std::runtime_error("bad bank slot list");
+        std::vector<char> taken(c.nS, 0);
+        for (int k = 0; k < count; k++) {
+            const int s2 = bankSlots[k];
+            if (s2 < 0 || s2 >= c.nS || taken[s2]) {
+                throw std::runtime_error("bank slot " + std::to_string(s2) + " outside the bank of " +
+                                         std::to_string(c.nS) + " or installed twice");
+            }
+            taken[s2] = 1;
+        }
+        c.installSlots.assign(bankSlots, bankSlots + count);
+    });
+}
+
+extern "C" int olfgpu_read_handed_back_slots(int64_t context, int* slots, int maxCount, int* count) {
+    return guarded([&] {
+        const BatchContext& c = contextOf(context);
+        const int k = static_cast<int>(c.handedBack.size());
+        for (int j = 0; slots && j < std::min(k, maxCount); j++) slots[j] = c.handedBack[j];
+        if (count) *count = k;
+    });
+}
+
+extern "C" int olfgpu_set_states_to_host(int64_t context, int statesToHost) {
+    return guarded([&] { contextOf(context).statesToHost = statesToHost != 0; });
+}
+
+extern "C" int olfgpu_states_to_host(int64_t context, int* statesToHost) {
+    return guarded([&] {
+        if (!statesToHost) throw std::runtime_error("null output");
+        *statesToHost = contextOf(context).statesToHost ? 1 : 0;
+    });
+}
+
+extern "C" int olfgpu_read_batch_states(int64_t context, int nSlots, const int* slots, double* out) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        const int n = c.net->host.n;
+        if (nSlots < 0 || (nSlots > 0 && (!slots || !out))) throw std::runtime_error("bad slot list or output");
+        OLF_CUDA(cudaSetDevice(c.device));
+        std::vector<double> col(static_cast<size_t>(n) * c.S);
+        OLF_CUDA(cudaMemcpy(col.data(), c.x.p, col.size() * 8, cudaMemcpyDeviceToHost));
+        for (int j = 0; j < nSlots; j++) {
+            const int s2 = slots[j];
+            if (s2 < 0 || s2 >= c.nS) throw std::runtime_error("slot outside the bank");
+            for (int r = 0; r < n; r++) out[static_cast<size_t>(j) * n + r] = col[static_cast<size_t>(r) * c.S + s2];
+        }
+    });
+}
+
+extern "C" int olfgpu_set_outer_loops(int64_t context, int distributedSlack, int reactiveLimits) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        if (distributedSlack) throw std::runtime_error("the distributed-slack outer loop is not available");
+        c.reactiveLimitsLoop = reactiveLimits != 0;
+    });
+}
+
+extern "C" int olfgpu_set_realistic_check(int64_t context, const unsigned char* rowChecked, double minV, double maxV,
+                                          int enabled) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        c.hasVCheck = false;
+        if (!enabled || !rowChecked) return;
+        if (!(minV <= maxV)) throw std::runtime_error("realistic voltage band: minV must not exceed maxV");
+        const int n = c.net->host.n;
+        std::vector<int8_t> rc(n);
+        for (int r = 0; r < n; r++) rc[r] = rowChecked[r] ? 1 : 0;
+        OLF_CUDA(cudaSetDevice(c.device));
+        OLF_CUDA(cudaMemcpyAsync(c.vCheck.p, rc.data(), n, cudaMemcpyHostToDevice, c.stream));
+        OLF_CUDA(cudaStreamSynchronize(c.stream));
+        c.realisticMinV = minV;
+        c.realisticMaxV = maxV;
+        c.hasVCheck = true;
+    });
+}
+
+extern "C" int olfgpu_set_refinement_bound(int64_t context, double correctionBound) {
+    return guarded([&] {
+        if (!(correctionBound >= 0)) throw std::runtime_error("correctionBound must be >= 0");
+        contextOf(context).corrBound = correctionBound;
+    });
+}
+
+extern "C" int olfgpu_set_fp64_restart(int64_t context, int enable) {
+    return guarded([&] { contextOf(context).fp64Restart = enable != 0; });
 }
 
 extern "C" int olfgpu_set_phase_timing(int64_t context, int enable) {

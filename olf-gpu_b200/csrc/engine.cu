@@ -12,6 +12,385 @@
 namespace olfb200 {
 
 // ---------------------------------------------------------------------------------------------------------------
+// Subtree bins of the wide levels
+// ---------------------------------------------------------------------------------------------------------------
+// The elimination tree's parent of position k is the first column of its U row after the diagonal; the tasks of
+// position k (its U row and L column) update from pivots in k's subtree only, and its forward solve reads only k's
+// descendants, so a subtree is independent of every other.  A subtree qualifies when all its tasks sit below the narrow
+// factorization levels, all its positions below the narrow forward tail and at or above the backward head (the
+// shared-memory regions keep those), and it holds no dense-front position.  From the roots down, a qualifying subtree
+// whose work (block updates + tasks) fits the cap becomes a bin member; any other root turns into a top position and
+// its children are examined.  Members are packed into bins of at most the cap (largest first).  The cap is the
+// qualifying work over SUBTREE_BINS: enough bins that bins x lane groups fill the GPU at a few hundred lanes.
+constexpr int SUBTREE_BINS = 96;
+constexpr int SUBTREE_PHASES = 6;   // bins of the remaining forest, phase after phase
+constexpr int NARROW = 48;   // a level of at most this many tasks (positions) is narrow
+
+NarrowBounds narrowBounds(const BlockPlan& p) {
+    auto countOf = [](const std::vector<int>& ptr, size_t l) { return ptr[l + 1] - ptr[l]; };
+    NarrowBounds nbd{};
+    // (a dense-front plan ends with the front's assembly level, wide whatever the tree above it: it stays a level
+    // launch after the range)
+    nbd.factorTo = static_cast<int>(p.levelPtr.size()) - 1 - (p.frontF > 0 ? 1 : 0);
+    nbd.factorFrom = nbd.factorTo;
+    while (nbd.factorFrom > 0 && countOf(p.levelPtr, nbd.factorFrom - 1) <= NARROW) nbd.factorFrom--;
+    nbd.fwdFrom = static_cast<int>(p.fwdLevelPtr.size()) - 1;
+    while (nbd.fwdFrom > 0 && countOf(p.fwdLevelPtr, nbd.fwdFrom - 1) <= NARROW) nbd.fwdFrom--;
+    nbd.bwdUntil = 0;
+    while (nbd.bwdUntil < static_cast<int>(p.bwdLevelPtr.size()) - 1 && countOf(p.bwdLevelPtr, nbd.bwdUntil) <= NARROW) {
+        nbd.bwdUntil++;
+    }
+    return nbd;
+}
+
+namespace {
+
+// Bins of subtrees of the elimination forest, phase after phase: a phase takes, from the roots of the forest of
+// positions no earlier phase took, every subtree whose root may start one (eligible: monotone, every descendant of an
+// eligible root is eligible) and whose weight fits the phase's cap (the remaining weight over SUBTREE_BINS); a root
+// that may not, or does not fit, stays out and its children are examined.  Subtrees are packed into bins of at most
+// the cap, largest first.  Returns the positions of each bin and the bins of each phase.
+struct Forest {
+    std::vector<int> parent;
+    std::vector<std::vector<int>> children;
+};
+
+void binForest(const Forest& fo, const std::vector<long long>& weight, const std::vector<char>& eligible,
+               std::vector<std::vector<int>>& binPos, std::vector<int>& phasePtr, std::vector<int>& binOf) {
+    const int nb = static_cast<int>(fo.parent.size());
+    binOf.assign(nb, -1);
+    binPos.clear();
+    phasePtr = {0};
+    for (int phase = 0; phase < SUBTREE_PHASES; phase++) {
+        std::vector<long long> sub(nb, 0);
+        for (int k = 0; k < nb; k++) sub[k] = binOf[k] < 0 ? weight[k] : 0;
+        for (int k = 0; k < nb; k++)   // children precede their parent (child < parent)
+            if (fo.parent[k] >= 0 && binOf[k] < 0) sub[fo.parent[k]] += sub[k];
+        long long total = 0;
+        for (int k = 0; k < nb; k++)
+            if (binOf[k] < 0 && eligible[k] && (fo.parent[k] < 0 || !eligible[fo.parent[k]])) total += sub[k];
+        if (total == 0) break;
+        const long long cap = std::max<long long>(1, total / SUBTREE_BINS);
+        std::vector<int> members, queue;
+        for (int k = 0; k < nb; k++)
+            if (fo.parent[k] < 0) queue.push_back(k);
+        while (!queue.empty()) {
+            const int r = queue.back();
+            queue.pop_back();
+            if (binOf[r] >= 0) continue;
+            if (eligible[r] && sub[r] <= cap) {
+                if (sub[r] > 0) members.push_back(r);
+            } else {
+                for (int c : fo.children[r]) queue.push_back(c);
+            }
+        }
+        if (members.empty()) break;
+        std::sort(members.begin(), members.end(), [&](int x, int y) { return sub[x] != sub[y] ? sub[x] > sub[y] : x < y; });
+        const int first = static_cast<int>(binPos.size());
+        std::vector<long long> binWork;
+        for (int r : members) {
+            size_t k = 0;
+            while (k < binWork.size() && binWork[k] + sub[r] > cap) k++;
+            if (k == binWork.size()) {
+                binWork.push_back(0);
+                binPos.emplace_back();
+            }
+            binWork[k] += sub[r];
+            // the remaining subtree of r
+            std::vector<int> stack{r};
+            while (!stack.empty()) {
+                const int q = stack.back();
+                stack.pop_back();
+                if (binOf[q] >= 0) continue;
+                binOf[q] = first + static_cast<int>(k);
+                binPos[first + k].push_back(q);
+                for (int c : fo.children[q]) stack.push_back(c);
+            }
+        }
+        phasePtr.push_back(static_cast<int>(binPos.size()));
+    }
+}
+
+}  // namespace
+
+SubtreeBinsHost planSubtreeBins(const BlockPlan& p, const NarrowBounds& nbd) {
+    SubtreeBinsHost h;
+    const int nb = p.nb;
+    if (p.deferredL || nb < 64) return h;
+    const int nLu = p.nU + p.nL;
+    Forest fo;
+    fo.parent.assign(nb, -1);
+    fo.children.assign(nb, {});
+    std::vector<int> fl(nb, -1), bl(nb, -1);
+    h.posOf.assign(nLu, -1);
+    for (int k = 0; k < nb; k++) {
+        if (p.uPtr[k + 1] - p.uPtr[k] > 1) fo.parent[k] = p.uCol[p.uPtr[k] + 1];
+        for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) h.posOf[t] = k;
+        for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++) h.posOf[p.nU + t] = k;
+    }
+    for (int k = 0; k < nb; k++)
+        if (fo.parent[k] >= 0) fo.children[fo.parent[k]].push_back(k);
+    for (size_t l = 0; l + 1 < p.fwdLevelPtr.size(); l++)
+        for (int q = p.fwdLevelPtr[l]; q < p.fwdLevelPtr[l + 1]; q++) fl[p.fwdLevelPos[q]] = static_cast<int>(l);
+    for (size_t l = 0; l + 1 < p.bwdLevelPtr.size(); l++)
+        for (int q = p.bwdLevelPtr[l]; q < p.bwdLevelPtr[l + 1]; q++) bl[p.bwdLevelPos[q]] = static_cast<int>(l);
+    auto wide = [&](int id) { return p.level[id] < nbd.factorFrom; };
+    // factorization: a position weighs its wide-level tasks (block updates + 1 each); any root may start a bin (a
+    // wide task only reads wide blocks of its subtree).  Forward: positions of the wide forward levels (the forward
+    // level grows towards the roots); backward: positions of the wide backward levels (it grows towards the leaves),
+    // never a dense-front position (the dense front solves those).
+    std::vector<long long> wf(nb, 0), ws(nb, 0);
+    std::vector<char> anyRoot(nb, 1), fwdOk(nb, 0), bwdOk(nb, 0);
+    for (int k = 0; k < nb; k++) {
+        auto add = [&](int id) {
+            if (wide(id)) wf[k] += p.opPtr[id + 1] - p.opPtr[id] + 1;
+        };
+        for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) add(t);
+        for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++) add(p.nU + t);
+        ws[k] = (p.uPtr[k + 1] - p.uPtr[k]) + (p.lPtr[k + 1] - p.lPtr[k]);
+        fwdOk[k] = fl[k] >= 0 && fl[k] < nbd.fwdFrom;
+        bwdOk[k] = k < p.frontStart && bl[k] >= nbd.bwdUntil;
+    }
+    std::vector<std::vector<int>> fBins, wBins, bBins;
+    std::vector<int> fBinOf, wBinOf, bBinOf;
+    binForest(fo, wf, anyRoot, fBins, h.phasePtr, fBinOf);
+    binForest(fo, ws, fwdOk, wBins, h.fwdPhasePtr, wBinOf);
+    binForest(fo, ws, bwdOk, bBins, h.bwdPhasePtr, bBinOf);
+    if (fBins.empty() || wBins.empty() || bBins.empty()) return SubtreeBinsHost{};
+    auto groupInto = [](std::vector<std::pair<int, int>>& v, std::vector<int>& all, std::vector<int>& off,
+                        std::vector<int>& ptr) {
+        std::sort(v.begin(), v.end());
+        for (size_t q = 0; q < v.size(); q++) {
+            if (q > 0 && v[q].first != v[q - 1].first) off.push_back(static_cast<int>(all.size()));
+            all.push_back(v[q].second);
+        }
+        off.push_back(static_cast<int>(all.size()));
+        ptr.push_back(static_cast<int>(off.size()) - 1);
+    };
+    h.levPtr = {0};
+    h.levOff = {0};
+    h.fwdPtr = {0};
+    h.fwdOff = {0};
+    h.bwdPtr = {0};
+    h.bwdOff = {0};
+    h.taskBin.assign(nLu, -1);
+    for (size_t b = 0; b < fBins.size(); b++) {
+        std::vector<std::pair<int, int>> tk;
+        for (int k : fBins[b]) {
+            for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++)
+                if (wide(t)) tk.push_back({p.level[t], t});
+            for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++)
+                if (wide(p.nU + t)) tk.push_back({p.level[p.nU + t], p.nU + t});
+        }
+        for (auto& e : tk) h.taskBin[e.second] = static_cast<int>(b);
+        groupInto(tk, h.task, h.levOff, h.levPtr);
+    }
+    for (auto& bin : wBins) {
+        std::vector<std::pair<int, int>> v;
+        for (int k : bin) v.push_back({fl[k], k});
+        groupInto(v, h.fwdPos, h.fwdOff, h.fwdPtr);
+    }
+    for (auto& bin : bBins) {
+        std::vector<std::pair<int, int>> v;
+        for (int k : bin) v.push_back({bl[k], k});
+        groupInto(v, h.bwdPos, h.bwdOff, h.bwdPtr);
+    }
+    h.nBins = static_cast<int>(fBins.size());
+    h.fwdBinOf = wBinOf;
+    h.bwdBinOf = bBinOf;
+    // the top lists: every level's tasks (positions) outside the bins
+    auto topOf = [&](const std::vector<int>& ptr, const std::vector<int>& items, const std::vector<int>& binOfItem,
+                     std::vector<int>& outPtr, std::vector<int>& out) {
+        outPtr.assign(ptr.size(), 0);
+        out.clear();
+        for (size_t l = 0; l + 1 < ptr.size(); l++) {
+            for (int q = ptr[l]; q < ptr[l + 1]; q++)
+                if (binOfItem[items[q]] < 0) out.push_back(items[q]);
+            outPtr[l + 1] = static_cast<int>(out.size());
+        }
+    };
+    topOf(p.levelPtr, p.levelTask, h.taskBin, h.topLevelPtr, h.topTask);
+    topOf(p.fwdLevelPtr, p.fwdLevelPos, wBinOf, h.topFwdPtr, h.topFwd);
+    topOf(p.bwdLevelPtr, p.bwdLevelPos, bBinOf, h.topBwdPtr, h.topBwd);
+    return h;
+}
+
+// The invariants the bin kernels rely on, checked on the host: every LU block in exactly one of (a bin, a top level),
+// every position likewise in each sweep; a bin task's update operands and pivot belong to its bin and sit on an
+// earlier level of it; a bin position's forward columns belong to its bin on earlier forward levels; its backward
+// columns sit on earlier backward levels of its bin or outside every bin (finished before the bins' backward sweep);
+// no bin task on a narrow factorization level, no bin position in the narrow forward tail or backward head.
+std::string checkSubtreeBins(const BlockPlan& p, const NarrowBounds& nbd, const SubtreeBinsHost& h) {
+    const int nLu = p.nU + p.nL, nb = p.nb;
+    if (h.nBins == 0) return "";
+    auto phases = [](const std::vector<int>& phasePtr, int nBins) {
+        std::vector<int> ph(nBins, 0);
+        for (size_t f = 0; f + 1 < phasePtr.size(); f++)
+            for (int b = phasePtr[f]; b < phasePtr[f + 1]; b++) ph[b] = static_cast<int>(f);
+        return ph;
+    };
+    const std::vector<int> phaseOf = phases(h.phasePtr, h.nBins);
+    std::vector<int> seen(nLu, 0), binLevel(nLu, -1);
+    for (int b = 0; b < h.nBins; b++)
+        for (int v = h.levPtr[b]; v < h.levPtr[b + 1]; v++)
+            for (int q = h.levOff[v]; q < h.levOff[v + 1]; q++) {
+                const int t = h.task[q];
+                seen[t]++;
+                binLevel[t] = v - h.levPtr[b];
+                if (p.level[t] >= nbd.factorFrom) return "bin task on a narrow level";
+            }
+    for (int t : h.topTask) seen[t]++;
+    for (int t = 0; t < nLu; t++)
+        if (seen[t] != 1) return "LU block " + std::to_string(t) + " scheduled " + std::to_string(seen[t]) + " times";
+    for (int t = 0; t < nLu; t++) {
+        const int bt = h.taskBin[t];
+        if (bt < 0) continue;
+        // a block read by a bin task: earlier on the same bin, or in a bin of an earlier phase
+        auto before = [&](int src) {
+            const int bs = h.taskBin[src];
+            return bs >= 0 && (bs == bt ? binLevel[src] < binLevel[t] : phaseOf[bs] < phaseOf[bt]);
+        };
+        for (int q = p.opPtr[t]; q < p.opPtr[t + 1]; q++)
+            for (int src : {p.opL[q], p.opU[q]})
+                if (!before(src)) {
+                    return "bin task " + std::to_string(t) + " reads block " + std::to_string(src) + " not before it";
+                }
+        if (t >= p.nU && !before(p.uPtr[h.posOf[t]])) return "L block before its pivot";
+    }
+    // each sweep: every position once (front positions: not in the backward sweep, the dense front solves them)
+    auto place = [&](const std::vector<int>& ptr, const std::vector<int>& off, const std::vector<int>& pos,
+                     int nBins, const std::vector<int>& topPos, bool forward, std::vector<int>& lv) -> std::string {
+        std::vector<int> cnt(nb, 0);
+        lv.assign(nb, -1);
+        for (int b = 0; b < nBins; b++)
+            for (int v = ptr[b]; v < ptr[b + 1]; v++)
+                for (int q = off[v]; q < off[v + 1]; q++) {
+                    cnt[pos[q]]++;
+                    lv[pos[q]] = v - ptr[b];
+                }
+        for (int i : topPos) cnt[i]++;
+        for (int i = 0; i < nb; i++) {
+            const int want = forward || i < p.frontStart ? 1 : 0;
+            if (cnt[i] != want) return "position " + std::to_string(i) + " scheduled " + std::to_string(cnt[i]) + " times";
+        }
+        return "";
+    };
+    const int nFwdBins = h.fwdPhasePtr.back(), nBwdBins = h.bwdPhasePtr.back();
+    const std::vector<int> fph = phases(h.fwdPhasePtr, nFwdBins), bph = phases(h.bwdPhasePtr, nBwdBins);
+    std::vector<int> flv, blv;
+    std::string e = place(h.fwdPtr, h.fwdOff, h.fwdPos, nFwdBins, h.topFwd, true, flv);
+    if (!e.empty()) return "forward: " + e;
+    e = place(h.bwdPtr, h.bwdOff, h.bwdPos, nBwdBins, h.topBwd, false, blv);
+    if (!e.empty()) return "backward: " + e;
+    // forward: row i reads column k for every L(i, k); backward: row i reads column j for every U(i, j), j > i
+    for (int k = 0; k < nb; k++)
+        for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++) {
+            const int i = p.lRow[t];
+            const int bi = h.fwdBinOf[i], bk = h.fwdBinOf[k];
+            if (bi < 0) continue;
+            const bool okFwd = bk >= 0 && (bk == bi ? flv[k] < flv[i] : fph[bk] < fph[bi]);
+            if (!okFwd) return "forward column not before its row";
+        }
+    for (int i = 0; i < nb; i++) {
+        const int bi = h.bwdBinOf[i];
+        if (bi < 0) continue;
+        for (int q = p.uPtr[i] + 1; q < p.uPtr[i + 1]; q++) {
+            const int j = p.uCol[q], bj = h.bwdBinOf[j];
+            // top positions and later phases' bins are solved before this bin's backward sweep
+            const bool okBwd = bj < 0 || (bj == bi ? blv[j] < blv[i] : bph[bj] > bph[bi]);
+            if (!okBwd) return "backward column not before its row";
+        }
+    }
+    // no bin position in the narrow forward tail or the backward head
+    std::vector<int> fl(nb, -1), bl(nb, -1);
+    for (size_t l = 0; l + 1 < p.fwdLevelPtr.size(); l++)
+        for (int q = p.fwdLevelPtr[l]; q < p.fwdLevelPtr[l + 1]; q++) fl[p.fwdLevelPos[q]] = static_cast<int>(l);
+    for (size_t l = 0; l + 1 < p.bwdLevelPtr.size(); l++)
+        for (int q = p.bwdLevelPtr[l]; q < p.bwdLevelPtr[l + 1]; q++) bl[p.bwdLevelPos[q]] = static_cast<int>(l);
+    for (int i = 0; i < nb; i++) {
+        if (h.fwdBinOf[i] >= 0 && fl[i] >= nbd.fwdFrom) return "bin position in the narrow forward tail";
+        if (h.bwdBinOf[i] >= 0 && bl[i] < nbd.bwdUntil) return "bin position in the narrow backward head";
+    }
+    return "";
+}
+
+// Uploads the bins and the top lists (with their split factors) of a structure's device copy.
+template <typename SplitFn>
+void buildSubtreeBins(DeviceNet& d, const BlockPlan& p, const std::vector<int>& lrowLen, SplitFn splitOf) {
+    d.sub = SubtreePlan{};
+    const NarrowBounds nbd{d.factorFrom, d.factorTo, d.fwdFrom, d.bwdUntil};
+    SubtreeBinsHost h = planSubtreeBins(p, nbd);
+    if (h.nBins == 0) return;
+    d.topLevelPtr = h.topLevelPtr;
+    d.topFwdPtr = h.topFwdPtr;
+    d.topBwdPtr = h.topBwdPtr;
+    d.topLevelSplit.assign(d.topLevelPtr.size() - 1, 1);
+    for (size_t l = 0; l + 1 < d.topLevelPtr.size(); l++) {
+        int m = 0;
+        for (int q = d.topLevelPtr[l]; q < d.topLevelPtr[l + 1]; q++)
+            m = std::max(m, p.opPtr[h.topTask[q] + 1] - p.opPtr[h.topTask[q]]);
+        d.topLevelSplit[l] = splitOf(m, 12);
+    }
+    d.topFwdSplit.assign(d.topFwdPtr.size() - 1, 1);
+    for (size_t l = 0; l + 1 < d.topFwdPtr.size(); l++) {
+        int m = 0;
+        for (int q = d.topFwdPtr[l]; q < d.topFwdPtr[l + 1]; q++) m = std::max(m, lrowLen[h.topFwd[q]]);
+        d.topFwdSplit[l] = splitOf(m, 8);
+    }
+    d.topBwdSplit.assign(d.topBwdPtr.size() - 1, 1);
+    for (size_t l = 0; l + 1 < d.topBwdPtr.size(); l++) {
+        int m = 0;
+        for (int q = d.topBwdPtr[l]; q < d.topBwdPtr[l + 1]; q++) {
+            const int i = h.topBwd[q];
+            m = std::max(m, p.uPtr[i + 1] - p.uPtr[i] - 1);
+        }
+        d.topBwdSplit[l] = splitOf(m, 8);
+    }
+    d.binPhasePtr = h.phasePtr;
+    d.binFwdPhasePtr = h.fwdPhasePtr;
+    d.binBwdPhasePtr = h.bwdPhasePtr;
+    d.binLevPtr.upload(h.levPtr);
+    d.binLevOff.upload(h.levOff);
+    d.binTask.upload(h.task);
+    d.binFwdPtr.upload(h.fwdPtr);
+    d.binFwdOff.upload(h.fwdOff);
+    d.binFwdPos.upload(h.fwdPos);
+    d.binBwdPtr.upload(h.bwdPtr);
+    d.binBwdOff.upload(h.bwdOff);
+    d.binBwdPos.upload(h.bwdPos);
+    d.topLevelTaskD.upload(h.topTask.empty() ? std::vector<int>{0} : h.topTask);
+    d.topFwdPosD.upload(h.topFwd.empty() ? std::vector<int>{0} : h.topFwd);
+    d.topBwdPosD.upload(h.topBwd.empty() ? std::vector<int>{0} : h.topBwd);
+    d.binTasks = static_cast<int>(h.task.size());
+    SubtreePlan& sp = d.sub;
+    sp.nBins = h.nBins;
+    sp.nPhases = static_cast<int>(d.binPhasePtr.size()) - 1;
+    sp.phasePtr = d.binPhasePtr.data();
+    sp.nFwdPhases = static_cast<int>(d.binFwdPhasePtr.size()) - 1;
+    sp.fwdPhasePtr = d.binFwdPhasePtr.data();
+    sp.nBwdPhases = static_cast<int>(d.binBwdPhasePtr.size()) - 1;
+    sp.bwdPhasePtr = d.binBwdPhasePtr.data();
+    sp.levPtr = d.binLevPtr.as<int>();
+    sp.levOff = d.binLevOff.as<int>();
+    sp.task = d.binTask.as<int>();
+    sp.fwdPtr = d.binFwdPtr.as<int>();
+    sp.fwdOff = d.binFwdOff.as<int>();
+    sp.fwdPos = d.binFwdPos.as<int>();
+    sp.bwdPtr = d.binBwdPtr.as<int>();
+    sp.bwdOff = d.binBwdOff.as<int>();
+    sp.bwdPos = d.binBwdPos.as<int>();
+    sp.topLevelTask = d.topLevelTaskD.as<int>();
+    sp.topLevelPtr = d.topLevelPtr.data();
+    sp.topLevelSplit = d.topLevelSplit.data();
+    sp.topFwdPos = d.topFwdPosD.as<int>();
+    sp.topFwdPtr = d.topFwdPtr.data();
+    sp.topFwdSplit = d.topFwdSplit.data();
+    sp.topBwdPos = d.topBwdPosD.as<int>();
+    sp.topBwdPtr = d.topBwdPtr.data();
+    sp.topBwdSplit = d.topBwdSplit.data();
+}
+
+// ---------------------------------------------------------------------------------------------------------------
 // Device copy of a structure
 // ---------------------------------------------------------------------------------------------------------------
 std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
@@ -204,13 +583,9 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     d->persistent.bwdLongest = d->bwdLongestD.as<int>();
     d->persistent.bwdPos = d->bwdPos.as<int>();
     // the narrow levels: the factorization / forward tail and the backward head whose levels hold <= NARROW tasks
-    constexpr int NARROW = 48;
-    auto countOf = [](const std::vector<int>& ptr, size_t l) { return ptr[l + 1] - ptr[l]; };
-    // (a dense-front plan ends with the front's assembly level, wide whatever the tree above it: it stays a level
-    // launch after the range)
-    d->factorTo = static_cast<int>(p.levelPtr.size()) - 1 - (p.frontF > 0 ? 1 : 0);
-    d->factorFrom = d->factorTo;
-    while (d->factorFrom > 0 && countOf(p.levelPtr, d->factorFrom - 1) <= NARROW) d->factorFrom--;
+    const NarrowBounds nbd = narrowBounds(p);
+    d->factorTo = nbd.factorTo;
+    d->factorFrom = nbd.factorFrom;
     // the shared-memory region: the narrow factorization levels before factorTo whose blocks fit REGION_BYTES (FP64,
     // one lane: two CTAs per SM); every block they produce gets a slot, in level order, and every update its operands'
     // slots in ops.w (slot + 1 of the L block in the low 16 bits, of the U block in the high 16 bits, 0 outside).
@@ -258,12 +633,8 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     d->ops.upload(ops);
     // (a solve range up to 256 rows per level measured slower: a tile walked the backward sweep's wide middle levels at
     // 1 ms per solve, against 0.8 ms as level launches)
-    d->fwdFrom = static_cast<int>(p.fwdLevelPtr.size()) - 1;
-    while (d->fwdFrom > 0 && countOf(p.fwdLevelPtr, d->fwdFrom - 1) <= NARROW) d->fwdFrom--;
-    d->bwdUntil = 0;
-    while (d->bwdUntil < static_cast<int>(p.bwdLevelPtr.size()) - 1 && countOf(p.bwdLevelPtr, d->bwdUntil) <= NARROW) {
-        d->bwdUntil++;
-    }
+    d->fwdFrom = nbd.fwdFrom;
+    d->bwdUntil = nbd.bwdUntil;
     // shared-memory solve regions: slot k of the forward tail holds position fwdLevelPos[fwdRegionBase + k], of the
     // backward head position bwdLevelPos[k]; each L / U entry of a region row carries its column's slot + 1 (0: a
     // column outside the region, final in global memory before the region's launch).  Both fit far below the default
@@ -314,6 +685,7 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     d->levelSplitD.upload(d->levelSplit);
     d->fwdSplitD.upload(d->fwdSplit);
     d->bwdSplitD.upload(d->bwdSplit);
+    buildSubtreeBins(*d, p, lrowLen, splitOf);
     d->coop = CoopPlan{static_cast<int>(p.levelPtr.size()) - 1, static_cast<int>(p.fwdLevelPtr.size()) - 1,
                        static_cast<int>(p.bwdLevelPtr.size()) - 1, d->levelPtrD.as<int>(), d->levelSplitD.as<int>(),
                        d->fwdPtrD.as<int>(), d->fwdPos.as<int>(), d->fwdSplitD.as<int>(), d->bwdPtrD.as<int>(),
@@ -367,13 +739,29 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     return d;
 }
 
+std::shared_ptr<DeviceNet> NetStructure::onDevice(int device) {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = devs.find(device);
+    if (it != devs.end()) return it->second;
+    auto d = uploadNet(host);
+    devs[device] = d;
+    return d;
+}
+
+std::shared_ptr<DeviceNet> NetStructure::find(int device) {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = devs.find(device);
+    return it == devs.end() ? nullptr : it->second;
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // Batch context
 // ---------------------------------------------------------------------------------------------------------------
 BatchContext::~BatchContext() {
     if (graph) cudaGraphExecDestroy(graph);
     if (graphSolve) cudaGraphExecDestroy(graphSolve);
-    for (cudaGraphExec_t gx : {graphFactor, graphResidual, graphCorrect, graph64, graphStep})
+    for (cudaGraphExec_t gx : {graphFactor, graphResidual, graphCorrect, graph64, graphStep, graphSolveScored,
+                               graphStepScored})
         if (gx) cudaGraphExecDestroy(gx);
     if (hostActive) cudaFreeHost(hostActive);
     if (countReady) cudaEventDestroy(countReady);
@@ -417,6 +805,17 @@ DevBatch BatchContext::batch() const {
     b.growthLimit = growthLimit;
     b.laneMask = nullptr;
     b.resNorm = resNorm.as<unsigned long long>();
+    b.fp64Left = fp64RestartOn ? fp64Left.as<int8_t>() : nullptr;
+    // the FP64 restart starts from the base start in fallback mode (the fallback already tried the lane's own start)
+    // or when no per-scenario start was given, else from the lane's own start row
+    b.restartFull = (b.fallbackOn || !hasX0Full) ? nullptr : fullSrc;
+    b.refine = refine.as<int8_t>();
+    b.ssqPart = ssqPart.as<double>();
+    b.solveRatio = solveRatio.as<double>();
+    b.stepMax = stepMax.as<unsigned long long>();
+    b.varType = hasVarType ? varType.as<int8_t>() : nullptr;
+    b.vCheck = hasVCheck ? vCheck.as<int8_t>() : nullptr;
+    b.laneLive = hasLaneLive ? laneLive.as<int8_t>() : nullptr;
     return b;
 }
 
@@ -430,14 +829,14 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
     auto ctx = std::make_unique<BatchContext>();
     ctx->net = net;
     OLF_CUDA(cudaGetDevice(&ctx->device));
-    if (!net->dev || net->dev->device != ctx->device) net->dev = uploadNet(net->host);
+    ctx->dn = net->onDevice(ctx->device);
     const Structure& s = net->host;
-    const DevNet& v = net->dev->view;
+    const DevNet& v = ctx->dn->view;
     ctx->nS = nScenarios;
     ctx->S = (nScenarios + 31) / 32 * 32;
     const size_t S = ctx->S, n = s.n;
     OLF_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    OLF_CUDA(cudaMallocHost(&ctx->hostActive, 4 * sizeof(int)));
+    OLF_CUDA(cudaMallocHost(&ctx->hostActive, 8 * sizeof(int)));
     OLF_CUDA(cudaEventCreateWithFlags(&ctx->countReady, cudaEventDisableTiming));
     ctx->x.alloc(n * S * 8);
     ctx->target.alloc(n * S * 8);
@@ -463,7 +862,15 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
     ctx->fallbackLeft.alloc(S);
     ctx->resNorm.alloc(S * 8);
     ctx->fellBack.alloc(S);
-    ctx->nActive.alloc(16);
+    ctx->fp64Left.alloc(S);
+    ctx->refine.alloc(S);
+    ctx->ssqPart.alloc(static_cast<size_t>(SSQ_STRANDS) * S * 8);
+    ctx->solveRatio.alloc(S * 8);
+    ctx->stepMax.alloc(2 * S * 8);
+    ctx->varType.alloc(n);
+    ctx->vCheck.alloc(n);
+    ctx->laneLive.alloc(S);
+    ctx->nActive.alloc(8 * sizeof(int));
     ctx->out.alloc(static_cast<size_t>(nScenarios) * (n + 3) * 8);
     ctx->stage.alloc(n * 8 * 2 + n * 4);
     ctx->cfg.maxIter = 15;
@@ -474,15 +881,19 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
     ctx->cfg.refinementSteps = 1;
     ctx->cfg.growthLimit = ctx->growthLimit;
     ctx->cfg.refineBelow = ctx->refineBelow;
+    ctx->cfg.corrBound = ctx->corrBound;
+    ctx->cfg.batchOfOne = nScenarios == 1 ? 1 : 0;
     if (nRl > 0) {
         for (int i = 0; i < nRl; i++) {
             if (voltageRow[i] < 0 || voltageRow[i] >= s.n) throw std::runtime_error("bad reactiveLimitVoltageRow");
-            if (pRow[i] >= s.n) throw std::runtime_error("bad reactiveLimit pRow");
+            if (pRow && pRow[i] >= s.n) throw std::runtime_error("bad reactiveLimit pRow");
         }
+        // the forced-PV election keys may come later (olfgpu_set_reactive_limit_strongest_pv_keys): zeroed until then
         auto up = [&](DeviceBuffer& d, const void* src, size_t bytes) {
             d.alloc(bytes);
-            OLF_CUDA(cudaMemcpy(d.p, src, bytes, cudaMemcpyHostToDevice));
+            if (src) OLF_CUDA(cudaMemcpy(d.p, src, bytes, cudaMemcpyHostToDevice));
         };
+        ctx->rlKeys = nomV && pRow && staticP && idRank;
         up(ctx->rlVoltageRow, voltageRow, nRl * 4);
         up(ctx->rlMinQ, minQ, nRl * 8);
         up(ctx->rlMaxQ, maxQ, nRl * 8);
@@ -615,10 +1026,12 @@ __global__ void rowModeOverrideKernel(const int* triples, int count, int8_t* mod
     mode[(size_t)triples[3 * k + 1] * S + triples[3 * k]] = (int8_t)triples[3 * k + 2];
 }
 
+// Lane state at install; nActive[0] (zeroed before) counts the live lanes.
 __global__ void laneInitKernel(DevBatch b) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= b.S) return;
-    const bool live = s < b.nS;
+    const bool live = s < b.nS && (!b.laneLive || b.laneLive[s]);
+    if (live) atomicAdd(b.nActive, 1);
     b.iter[s] = 0;
     b.status[s] = live ? ST_RUNNING : ST_REJECTED;
     b.active[s] = live ? 1 : 0;
@@ -631,7 +1044,9 @@ __global__ void laneInitKernel(DevBatch b) {
     b.precision64[s] = 0;
     b.fallbackLeft[s] = live && b.fallbackOn ? 1 : 0;
     b.fellBack[s] = 0;
-    if (s == 0) *b.nActive = b.nS;
+    if (b.fp64Left) b.fp64Left[s] = live ? 1 : 0;
+    b.refine[s] = 0;
+    b.solveRatio[s] = 0.0;
 }
 
 // lanes still iterating after the batched-iteration cap (newton_iteration.cu:410-429) are REJECTED
@@ -691,7 +1106,7 @@ void dropGraph(cudaGraphExec_t& g) {
 // The lanes flagged for an FP64 refactor (mixed precision), as a batch view whose LU kernels see only them.
 DevBatch fp64View(BatchContext& ctx) {
     const size_t S = ctx.S;
-    if (!ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(ctx.net->dev->view.nLu) * 4 * S * 8);
+    if (!ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(ctx.dn->view.nLu) * 4 * S * 8);
     DevBatch b = ctx.batch();
     b.lu64 = ctx.lu64.as<double>();
     b.laneMask = ctx.precision64.as<int8_t>();
@@ -702,10 +1117,16 @@ DevBatch fp64View(BatchContext& ctx) {
 
 void captureIteration(BatchContext& ctx) {
     const int key = ctx.narrowLanes * 100000 + (ctx.regionFactor ? 50000 : 0) + (ctx.regionSolve ? 20000 : 0) +
+                    (ctx.subtrees ? 5000000 : 0) +
                     ctx.precision * 1000 +
                     ctx.refinementSteps * 10 +
                     (ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits ? 1 : 0);
-    if (ctx.graph && ctx.graphKey == key) return;
+    // the graphs bake the batch view (pointers, per-request flags) and the settings into their kernel parameters
+    const DevBatch now = ctx.batch();
+    if (ctx.graph && ctx.graphKey == key && std::memcmp(&now, &ctx.graphBatch, sizeof(DevBatch)) == 0 &&
+        std::memcmp(&ctx.cfg, &ctx.graphCfg, sizeof(Settings)) == 0) {
+        return;
+    }
     dropGraph(ctx.graph);
     dropGraph(ctx.graphSolve);
     dropGraph(ctx.graphFactor);
@@ -713,14 +1134,17 @@ void captureIteration(BatchContext& ctx) {
     dropGraph(ctx.graphCorrect);
     dropGraph(ctx.graph64);
     dropGraph(ctx.graphStep);
-    const DeviceNet& dn = *ctx.net->dev;
+    dropGraph(ctx.graphSolveScored);
+    dropGraph(ctx.graphStepScored);
+    const DeviceNet& dn = *ctx.dn;
     const DevNet& net = dn.view;
     const size_t S = ctx.S;
     const bool mixed = ctx.precision == 1;
     if (mixed && !ctx.lu32.p) ctx.lu32.alloc(static_cast<size_t>(net.nLu) * 4 * S * 4);
     if (!mixed && !ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(net.nLu) * 4 * S * 8);
     const DevBatch b = ctx.batch();
-    const bool rl = ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits;
+    const Settings cfg = ctx.cfg;
+    const bool rl = ctx.rl.nRl > 0 && cfg.reactiveLimits;
     cudaStream_t st = ctx.stream;
     const Hybrid hy = ctx.hybrid();
     const Hybrid* hp = ctx.useHybrid() ? &hy : nullptr;
@@ -729,17 +1153,22 @@ void captureIteration(BatchContext& ctx) {
     ctx.graph = captureInto(st, [&] {
         launchIterationStart(b, st);
         launchFill(net, b, true, rl, st);
-        launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, st);
-        if (rl) launchReactiveLimits(net, b, ctx.rl, ctx.cfg, st);
-        launchCountSolving(b, mixed ? ctx.cfg.refineBelow : -1.0, st);
+        if (cfg.norm2Threshold > 0.0) launchNorm2(net, b, st);
+        launchTest(net, b, cfg, rl ? ctx.rl.remainingPv : nullptr, st);
+        if (rl) launchReactiveLimits(net, b, ctx.rl, cfg, st);
+        launchCountSolving(b, mixed ? cfg.refineBelow : -1.0, cfg.maxIter, st);
     });
     if (!mixed) {
-        // part 2 (FP64): factorization, solves, step
-        ctx.graphSolve = captureInto(st, [&] {
-            launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, false, hp, st);
-            launchSolve(net, b, dn.fwd(), dn.bwd(), false, false, hp, st);
-            launchStep(net, b, false, st);
-        });
+        // part 2 (FP64): factorization, solves, (the linear-solve scoring,) step
+        for (bool scoredVariant : {false, true}) {
+            cudaGraphExec_t g = captureInto(st, [&] {
+                launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, false, hp, st);
+                launchSolve(net, b, dn.fwd(), dn.bwd(), false, false, hp, st);
+                if (scoredVariant) launchScoreSolve(net, b, cfg, st);
+                launchStep(net, b, cfg, st);
+            });
+            (scoredVariant ? ctx.graphSolveScored : ctx.graphSolve) = g;
+        }
     } else {
         ctx.graphFactor = captureInto(st, [&] {
             launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, true, hp, st);
@@ -747,23 +1176,32 @@ void captureIteration(BatchContext& ctx) {
         });
         ctx.graphSolve = captureInto(st, [&] { launchSolve(net, b, dn.fwd(), dn.bwd(), true, false, hp, st); });
         if (ctx.refinementSteps > 0) {
-            // one refinement step: the FP64 residual and its check, then (when a lane needs it) the correction solve
-            ctx.graphResidual = captureInto(st, [&] {
-                launchResidual(net, b, st);
-                launchResidualCheck(net, b, REFINE_RESIDUAL * ctx.cfg.tol, ctx.cfg.refineBelow, st);
+            // one refinement step of the lanes still refining: the FP64 residual, the correction solve (dx += d), and
+            // which lanes' correction is still above the bound
+            DevBatch br = b;
+            br.laneMask = b.refine;
+            ctx.graphResidual = captureInto(st, [&] { launchResidual(net, br, st); });
+            ctx.graphCorrect = captureInto(st, [&] {
+                launchSolve(net, br, dn.fwd(), dn.bwd(), true, true, hp, st);
+                launchCorrectionCheck(net, br, cfg.corrBound, st);
             });
-            ctx.graphCorrect = captureInto(st, [&] { launchSolve(net, b, dn.fwd(), dn.bwd(), true, true, hp, st); });
         }
-        ctx.graphStep = captureInto(st, [&] { launchStep(net, b, false, st); });
+        ctx.graphStep = captureInto(st, [&] { launchStep(net, b, cfg, st); });
+        ctx.graphStepScored = captureInto(st, [&] {
+            launchScoreSolve(net, b, cfg, st);
+            launchStep(net, b, cfg, st);
+        });
     }
     ctx.graphKey = key;
+    ctx.graphBatch = now;
+    ctx.graphCfg = ctx.cfg;
 }
 
 // Mixed precision: the FP64 refactor and solve of the flagged lanes (captured on first use: it allocates the FP64
 // factors).
 void launchFp64Redo(BatchContext& ctx) {
     if (!ctx.graph64) {
-        const DeviceNet& dn = *ctx.net->dev;
+        const DeviceNet& dn = *ctx.dn;
         const DevBatch b64 = fp64View(ctx);
         const Hybrid hy = ctx.hybrid();
         const Hybrid* hp = ctx.useHybrid() ? &hy : nullptr;
@@ -782,7 +1220,7 @@ void launchFp64Redo(BatchContext& ctx) {
 // Returns false when no lane is left iterating.
 // The factorization / one solve of an iteration under the context's schedule (level launches or cooperative sweeps).
 void factorPhase(BatchContext& ctx, const DevBatch& b, bool fp32) {
-    const DeviceNet& dn = *ctx.net->dev;
+    const DeviceNet& dn = *ctx.dn;
     if (ctx.schedule == SCHEDULE_COOP) {
         OLF_CUDA(launchFactorCoop(dn.view, b, dn.coop, fp32, ctx.stream));
         launchDenseFront(dn.view, b, fp32, ctx.stream);
@@ -794,7 +1232,7 @@ void factorPhase(BatchContext& ctx, const DevBatch& b, bool fp32) {
 }
 
 void solvePhase(BatchContext& ctx, const DevBatch& b, bool fp32, bool fromResidual) {
-    const DeviceNet& dn = *ctx.net->dev;
+    const DeviceNet& dn = *ctx.dn;
     if (ctx.schedule == SCHEDULE_COOP) {
         OLF_CUDA(launchSolveCoop(dn.view, b, dn.coop, fp32, fromResidual, ctx.stream));
         return;
@@ -803,26 +1241,31 @@ void solvePhase(BatchContext& ctx, const DevBatch& b, bool fp32, bool fromResidu
     launchSolve(dn.view, b, dn.fwd(), dn.bwd(), fp32, fromResidual, ctx.useHybrid() ? &hy : nullptr, ctx.stream);
 }
 
-// The refinement steps of a mixed-precision iteration, launched directly: FP64 residual, its per-lane check, and the
-// correction solve only while some lane's residual is above the bound.
+// The refinement steps of a mixed-precision iteration, launched directly: for the lanes still refining, the FP64
+// residual, the correction solve and the check of its size; until no lane's correction is above the bound.
 void refinementSteps(BatchContext& ctx, const DevBatch& b) {
-    const DeviceNet& dn = *ctx.net->dev;
+    const DeviceNet& dn = *ctx.dn;
     cudaStream_t st = ctx.stream;
+    DevBatch br = b;
+    br.laneMask = b.refine;
     for (int r = 0; r < ctx.refinementSteps; r++) {
-        launchResidual(dn.view, b, st);
-        launchResidualCheck(dn.view, b, REFINE_RESIDUAL * ctx.cfg.tol, ctx.cfg.refineBelow, st);
+        launchResidual(dn.view, br, st);
+        solvePhase(ctx, br, true, true);
+        launchCorrectionCheck(dn.view, br, ctx.cfg.corrBound, st);
         OLF_CUDA(cudaMemcpyAsync(ctx.hostActive + 2, static_cast<int*>(ctx.nActive.p) + 2, 4, cudaMemcpyDeviceToHost,
                                  st));
         OLF_CUDA(cudaStreamSynchronize(st));
         if (ctx.hostActive[2] <= 0) break;
-        solvePhase(ctx, b, true, true);
     }
 }
+
+// The linear-solve scoring runs in an iteration where some lane is scored (the host read the count after the test).
+bool scoreDue(const BatchContext& ctx) { return ctx.hostActive[4] > 0; }
 
 // One Newton iteration's factorization, solves, refinement, FP64 refactor and step with cooperative sweeps (the
 // cooperative launches are not captured in graphs).
 void coopIteration(BatchContext& ctx) {
-    const DeviceNet& dn = *ctx.net->dev;
+    const DeviceNet& dn = *ctx.dn;
     const bool mixed = ctx.precision == 1;
     cudaStream_t st = ctx.stream;
     const DevBatch b = ctx.batch();
@@ -843,11 +1286,12 @@ void coopIteration(BatchContext& ctx) {
             solvePhase(ctx, b64, false, false);
         }
     }
-    launchStep(dn.view, b, false, st);
+    if (scoreDue(ctx)) launchScoreSolve(dn.view, b, ctx.cfg, st);
+    launchStep(dn.view, b, ctx.cfg, st);
 }
 
 bool phaseTimedIteration(BatchContext& ctx) {
-    const DeviceNet& dn = *ctx.net->dev;
+    const DeviceNet& dn = *ctx.dn;
     const DevNet& net = dn.view;
     const bool mixed = ctx.precision == 1;
     const bool rl = ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits;
@@ -859,11 +1303,12 @@ bool phaseTimedIteration(BatchContext& ctx) {
     launchIterationStart(b, st);
     launchFill(net, b, true, rl, st);
     OLF_CUDA(cudaEventRecord(ev[1], st));
+    if (ctx.cfg.norm2Threshold > 0.0) launchNorm2(net, b, st);
     launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, st);
     if (rl) launchReactiveLimits(net, b, ctx.rl, ctx.cfg, st);
-    launchCountSolving(b, mixed ? ctx.cfg.refineBelow : -1.0, st);
+    launchCountSolving(b, mixed ? ctx.cfg.refineBelow : -1.0, ctx.cfg.maxIter, st);
     OLF_CUDA(cudaEventRecord(ev[2], st));
-    OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 12, cudaMemcpyDeviceToHost, st));
+    OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 5 * sizeof(int), cudaMemcpyDeviceToHost, st));
     OLF_CUDA(cudaStreamSynchronize(st));
     float ms[6] = {0, 0, 0, 0, 0, 0};
     OLF_CUDA(cudaEventElapsedTime(&ms[0], ev[0], ev[1]));
@@ -889,8 +1334,9 @@ bool phaseTimedIteration(BatchContext& ctx) {
                 solvePhase(ctx, b64, false, false);
             }
         }
+        if (scoreDue(ctx)) launchScoreSolve(net, b, ctx.cfg, st);
         OLF_CUDA(cudaEventRecord(ev[5], st));
-        launchStep(net, b, false, st);
+        launchStep(net, b, ctx.cfg, st);
         OLF_CUDA(cudaEventRecord(ev[6], st));
         OLF_CUDA(cudaEventSynchronize(ev[6]));
         for (int i = 2; i < 6; i++) OLF_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
@@ -939,11 +1385,22 @@ void uploadInputs(BatchContext& ctx, const SolveRequest& req) {
         OLF_CUDA(cudaMemcpyAsync(ctx.rowModeE.p, req.rowModeEntries, req.nRowModeEntries * 12, cudaMemcpyHostToDevice, st));
     }
     outageBits(ctx, req.disabled, ctx.nS, req.nElements);
+    ctx.hasLaneLive = req.laneLive != nullptr;
+    if (req.laneLive) {
+        // the staging copy outlives the asynchronous upload: it sits in the pinned outage bits' shadow vector
+        ctx.liveHost.assign(ctx.S, 0);
+        for (int s2 = 0; s2 < ctx.nS; s2++) ctx.liveHost[s2] = req.laneLive[s2] ? 1 : 0;
+        OLF_CUDA(cudaMemcpyAsync(ctx.laneLive.p, ctx.liveHost.data(), ctx.S, cudaMemcpyHostToDevice, st));
+        OLF_CUDA(cudaStreamSynchronize(st));
+    }
 }
 
 // Device-side install of the uploaded inputs: every lane gets the base vectors, then the per-scenario overrides; lane
 // state and reactive-limit state reset.  Repeatable (the autotuner reinstalls the same batch for every candidate).
 void installLanes(BatchContext& ctx) {
+    // mixed precision: a failed lane restarts once in FP64 (the persistent tiles: with every solve refined to the
+    // correction bound); not with reactive limits, whose restarts carry the outer loop's state
+    ctx.fp64RestartOn = ctx.precision == 1 && ctx.fp64Restart && !(ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits);
     const int n = ctx.net->host.n;
     const size_t S = ctx.S;
     cudaStream_t st = ctx.stream;
@@ -967,6 +1424,7 @@ void installLanes(BatchContext& ctx) {
                                                                                 ctx.nRowModeEntries,
                                                                                 ctx.mode.as<int8_t>(), ctx.S);
     }
+    OLF_CUDA(cudaMemsetAsync(ctx.nActive.p, 0, sizeof(int), st));
     laneInitKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(ctx.batch());
     if (ctx.rl.nRl > 0) {
         OLF_CUDA(cudaMemsetAsync(ctx.rlLimitType.p, 0, ctx.rlLimitType.bytes, st));
@@ -976,7 +1434,8 @@ void installLanes(BatchContext& ctx) {
 }
 
 int roundCap(const BatchContext& ctx) {
-    const int solves = ctx.fallbackStart && ctx.hasX0Base && ctx.hasX0Full ? 2 : 1;   // a fallback restart: 2 solves
+    // a fallback restart and an FP64 restart each add one solve
+    const int solves = 1 + (ctx.fallbackStart && ctx.hasX0Base && ctx.hasX0Full ? 1 : 0) + (ctx.fp64RestartOn ? 1 : 0);
     return ctx.cfg.reactiveLimits ? (ctx.cfg.maxOuter + 1) * (ctx.cfg.maxIter + 1) : solves * (ctx.cfg.maxIter + 1);
 }
 
@@ -984,7 +1443,7 @@ int roundCap(const BatchContext& ctx) {
 // Fallback mode, before the first iteration: each lane starts from whichever of its own start (x0Full) and the base
 // start (x0Base) has the smaller max |F| (two mismatch-only fills over all lanes).
 void selectStarts(BatchContext& ctx) {
-    const DeviceNet& dn = *ctx.net->dev;
+    const DeviceNet& dn = *ctx.dn;
     cudaStream_t st = ctx.stream;
     const int n = ctx.net->host.n;
     const size_t all = static_cast<size_t>(n) * ctx.S;
@@ -1005,7 +1464,7 @@ void selectStarts(BatchContext& ctx) {
 
 int runIterations(BatchContext& ctx) {
     cudaStream_t st = ctx.stream;
-    const DeviceNet& dn = *ctx.net->dev;
+    const DeviceNet& dn = *ctx.dn;
     const bool mixed = ctx.precision == 1;
     const size_t S = ctx.S;
     if (mixed && !ctx.lu32.p) ctx.lu32.alloc(static_cast<size_t>(dn.view.nLu) * 4 * S * 4);
@@ -1036,7 +1495,7 @@ int runIterations(BatchContext& ctx) {
             continue;
         }
         OLF_CUDA(cudaGraphLaunch(ctx.graph, st));
-        OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 12, cudaMemcpyDeviceToHost, st));
+        OLF_CUDA(cudaMemcpyAsync(ctx.hostActive, ctx.nActive.p, 5 * sizeof(int), cudaMemcpyDeviceToHost, st));
         OLF_CUDA(cudaStreamSynchronize(st));
         if (ctx.hostActive[0] <= 0) {
             k++;
@@ -1049,7 +1508,7 @@ int runIterations(BatchContext& ctx) {
             continue;
         }
         if (!mixed) {
-            OLF_CUDA(cudaGraphLaunch(ctx.graphSolve, st));
+            OLF_CUDA(cudaGraphLaunch(scoreDue(ctx) ? ctx.graphSolveScored : ctx.graphSolve, st));
             continue;
         }
         // mixed: FP32 factorization, then (while the FP32 solves run) the count of lanes flagged for FP64
@@ -1059,18 +1518,19 @@ int runIterations(BatchContext& ctx) {
         OLF_CUDA(cudaEventRecord(ctx.countReady, st));
         OLF_CUDA(cudaGraphLaunch(ctx.graphSolve, st));
         if (ctx.graphResidual && ctx.hostActive[2] > 0) {
+            // the lanes near convergence refine until their correction is below the bound (at most refinementSteps)
             for (int r = 0; r < ctx.refinementSteps; r++) {
                 OLF_CUDA(cudaGraphLaunch(ctx.graphResidual, st));
+                OLF_CUDA(cudaGraphLaunch(ctx.graphCorrect, st));
                 OLF_CUDA(cudaMemcpyAsync(ctx.hostActive + 2, static_cast<int*>(ctx.nActive.p) + 2, 4,
                                          cudaMemcpyDeviceToHost, st));
                 OLF_CUDA(cudaStreamSynchronize(st));
-                if (ctx.hostActive[2] <= 0) break;   // every lane's FP32 solve already meets the residual bound
-                OLF_CUDA(cudaGraphLaunch(ctx.graphCorrect, st));
+                if (ctx.hostActive[2] <= 0) break;
             }
         }
         OLF_CUDA(cudaEventSynchronize(ctx.countReady));
         if (ctx.hostActive[3] > 0) launchFp64Redo(ctx);
-        OLF_CUDA(cudaGraphLaunch(ctx.graphStep, st));
+        OLF_CUDA(cudaGraphLaunch(scoreDue(ctx) ? ctx.graphStepScored : ctx.graphStep, st));
     }
     capKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(ctx.batch());
     return k;
@@ -1081,14 +1541,15 @@ void autotune(BatchContext& ctx) {
     struct Candidate { int schedule, lanes, threads; };
     std::vector<Candidate> cands;
     for (int narrow : {0, 1, 2, 4}) cands.push_back({SCHEDULE_LEVELS, narrow, 256});
-    if (ctx.net->dev->regionSlots > 0) {
+    if (ctx.dn->regionSlots > 0) {
         for (int narrow : {0, 2}) cands.push_back({SCHEDULE_LEVELS_SHARED, narrow, 256});
     }
-    if (ctx.net->dev->fwdRegionSlots > 0 || ctx.net->dev->bwdRegionSlots > 0) {
+    if (ctx.dn->fwdRegionSlots > 0 || ctx.dn->bwdRegionSlots > 0) {
         cands.push_back({SCHEDULE_LEVELS_SHARED_ALL, 0, 256});
     }
+    if (ctx.dn->sub.nBins > 0) cands.push_back({SCHEDULE_SUBTREES, 0, 256});
     cands.push_back({SCHEDULE_COOP, 0, 512});
-    if (ctx.net->dev->view.frontF == 0) {   // the persistent tiles do not run dense-front plans
+    if (ctx.dn->view.frontF == 0) {   // the persistent tiles do not run dense-front plans
         for (int lanes : {2, 4})
             for (int threads : {256, 512}) cands.push_back({SCHEDULE_PERSISTENT, lanes, threads});
     }
@@ -1099,8 +1560,10 @@ void autotune(BatchContext& ctx) {
     Candidate pick = cands[0];
     ctx.tuning.clear();
     auto apply = [&](const Candidate& c) {
-        ctx.regionFactor = c.schedule == SCHEDULE_LEVELS_SHARED || c.schedule == SCHEDULE_LEVELS_SHARED_ALL;
-        ctx.regionSolve = c.schedule == SCHEDULE_LEVELS_SHARED_ALL;
+        ctx.regionFactor = c.schedule == SCHEDULE_LEVELS_SHARED || c.schedule == SCHEDULE_LEVELS_SHARED_ALL ||
+                           c.schedule == SCHEDULE_SUBTREES;
+        ctx.regionSolve = c.schedule == SCHEDULE_LEVELS_SHARED_ALL || c.schedule == SCHEDULE_SUBTREES;
+        ctx.subtrees = c.schedule == SCHEDULE_SUBTREES;
         ctx.schedule = ctx.regionFactor ? SCHEDULE_LEVELS : c.schedule;
         if (ctx.schedule == SCHEDULE_LEVELS) {
             ctx.narrowLanes = c.lanes;
@@ -1131,6 +1594,24 @@ void autotune(BatchContext& ctx) {
 }
 
 }  // namespace
+
+void setStrongestPvKeys(BatchContext& ctx, const double* nomV, const int* pRow, const double* staticP,
+                        const int* idRank) {
+    OLF_CUDA(cudaSetDevice(ctx.device));
+    const int nRl = ctx.rl.nRl;
+    const int n = ctx.net->host.n;
+    for (int i = 0; i < nRl; i++)
+        if (pRow[i] >= n) throw std::runtime_error("bad reactiveLimit pRow");
+    auto put = [&](DeviceBuffer& d, const void* src, size_t bytes) {
+        OLF_CUDA(cudaMemcpyAsync(d.p, src, bytes, cudaMemcpyHostToDevice, ctx.stream));
+    };
+    put(ctx.rlNomV, nomV, nRl * 8);
+    put(ctx.rlPRow, pRow, nRl * 4);
+    put(ctx.rlStaticP, staticP, nRl * 8);
+    put(ctx.rlIdRank, idRank, nRl * 4);
+    OLF_CUDA(cudaStreamSynchronize(ctx.stream));
+    ctx.rlKeys = true;
+}
 
 void stageRequest(BatchContext& ctx, const SolveRequest& req) {
     OLF_CUDA(cudaSetDevice(ctx.device));
@@ -1166,23 +1647,51 @@ void stageRequest(BatchContext& ctx, const SolveRequest& req) {
     if (ctx.fallbackStart && ctx.rl.nRl > 0) {
         throw std::runtime_error("the fallback start is not available with reactive limits");
     }
+    if (ctx.rl.nRl > 0 && !ctx.rlKeys) {
+        // batch_solve_jni.cu:103-111: without the keys OLF's strongest-bus-stays-PV rule cannot be reproduced
+        throw std::runtime_error("reactive-limit entries installed without the forced-PV election keys "
+                                 "(olfgpu_set_reactive_limit_strongest_pv_keys)");
+    }
+    if (req.stateVectorScalingMode != SVS_NONE && req.stateVectorScalingMode != SVS_MAX_VOLTAGE_CHANGE) {
+        throw std::runtime_error("state vector scaling mode " + std::to_string(req.stateVectorScalingMode) +
+                                 " is not supported (NONE 0 and MAX_VOLTAGE_CHANGE 2 are)");
+    }
+    const bool clamp = req.stateVectorScalingMode == SVS_MAX_VOLTAGE_CHANGE;
+    if (clamp && !req.varType) throw std::runtime_error("MAX_VOLTAGE_CHANGE needs the variable types (varType)");
+    if (clamp && !(req.maxDv > 0.0 && req.maxDphi > 0.0)) {
+        throw std::runtime_error("MAX_VOLTAGE_CHANGE needs positive maxDv and maxDphi");
+    }
+    if ((clamp || req.convEpsPerEq > 0.0) && ctx.schedule == SCHEDULE_PERSISTENT) {
+        throw std::runtime_error("the persistent schedule runs the ||F||inf test and the plain step only");
+    }
     Settings cfg = ctx.cfg;
     cfg.maxIter = req.maxIter;
+    cfg.norm2Threshold = req.convEpsPerEq > 0.0 ? std::sqrt(req.convEpsPerEq * req.convEpsPerEq * n) : 0.0;
+    cfg.svsMode = req.stateVectorScalingMode;
+    cfg.maxDv = req.maxDv;
+    cfg.maxDphi = req.maxDphi;
+    cfg.corrBound = ctx.corrBound;
+    cfg.realistic = ctx.hasVCheck ? 1 : 0;
+    cfg.minV = ctx.realisticMinV;
+    cfg.maxV = ctx.realisticMaxV;
+    if (clamp) {
+        std::vector<int8_t> vt(n);
+        for (int r = 0; r < n; r++) vt[r] = static_cast<int8_t>(req.varType[r] == VAR_BUS_V || req.varType[r] == VAR_BUS_PHI
+                                                                     ? req.varType[r] : -1);
+        // stream-ordered (a pageable copy is staged before the call returns, so vt may go)
+        OLF_CUDA(cudaMemcpyAsync(ctx.varType.p, vt.data(), n, cudaMemcpyHostToDevice, ctx.stream));
+    }
+    ctx.hasVarType = clamp;
     cfg.tol = req.tol;
     cfg.rlTol = req.reactiveLimitTol;
     cfg.maxOuter = req.maxOuter;
     cfg.maxSwitch = req.maxPqPvSwitch;
-    cfg.reactiveLimits = ctx.rl.nRl > 0 ? 1 : 0;
+    cfg.reactiveLimits = ctx.rl.nRl > 0 && ctx.reactiveLimitsLoop && !req.skipReactiveLimits ? 1 : 0;
     cfg.mixed = ctx.precision;
     cfg.refinementSteps = ctx.refinementSteps;
     cfg.refineBelow = ctx.refineBelow;
     cfg.growthLimit = ctx.growthLimit;
-    if (std::memcmp(&cfg, &ctx.cfg, sizeof(Settings)) != 0 && ctx.graph) {
-        // the level-launch graph bakes the settings in
-        cudaGraphExecDestroy(ctx.graph);
-        ctx.graph = nullptr;
-    }
-    ctx.cfg = cfg;
+    ctx.cfg = cfg;   // (the iteration graphs are re-captured when the settings they baked in change)
     uploadInputs(ctx, req);
     ctx.staged = true;
 }
@@ -1228,7 +1737,7 @@ MultiContext* createMultiContext(const std::vector<BatchContext*>& members) {
     for (const BatchContext* c : members) {
         if (!c) throw std::runtime_error("null batch context");
         if (c->device != device) throw std::runtime_error("the batch contexts of a multi-grid launch share one device");
-        if (c->net->dev->view.frontF > 0) {
+        if (c->dn->view.frontF > 0) {
             throw std::runtime_error("a multi-grid launch runs persistent tiles, which do not run dense-front plans");
         }
     }
@@ -1278,11 +1787,11 @@ void runMulti(MultiContext& m, bool fp32) {
     for (size_t k = 0; k < idx.size(); k++) {
         BatchContext& c = *m.members[idx[k]];
         MultiItem& it = m.hostItems[k];
-        it.net = c.net->dev->view;
+        it.net = c.dn->view;
         it.b = c.batch();
         it.rl = c.rl;
         it.cfg = c.cfg;
-        it.plan = c.net->dev->persistent;
+        it.plan = c.dn->persistent;
         it.plan.maxRounds = roundCap(c);
         it.tileBegin = tile;
         tile += tilesOf(c, m.lanesPerTile);
@@ -1357,7 +1866,7 @@ void solveMulti(MultiContext& m, double* const* outs) {
     }
     const bool fp32 = precision == 1;
     for (BatchContext* c : m.members) {
-        const size_t lu = static_cast<size_t>(c->net->dev->view.nLu) * 4 * c->S;
+        const size_t lu = static_cast<size_t>(c->dn->view.nLu) * 4 * c->S;
         if (fp32 && !c->lu32.p) c->lu32.alloc(lu * 4);
         if (!fp32 && !c->lu64.p) c->lu64.alloc(lu * 8);
     }
@@ -1396,7 +1905,7 @@ void debugFill(BatchContext& ctx, const double* xFull, const double* targetBase,
                const unsigned char* disabled, double* jOut, double* fOut) {
     OLF_CUDA(cudaSetDevice(ctx.device));
     const Structure& s = ctx.net->host;
-    const DeviceNet& dn = *ctx.net->dev;
+    const DeviceNet& dn = *ctx.dn;
     const int n = s.n;
     const size_t S = ctx.S;
     cudaStream_t st = ctx.stream;
@@ -1415,6 +1924,7 @@ void debugFill(BatchContext& ctx, const double* xFull, const double* targetBase,
     tileModeKernel<<<blocksAll, 256, 0, st>>>(stageM, ctx.mode.as<int8_t>(), n, ctx.S);
     outageBits(ctx, disabled, ctx.nS, s.nElements);
     const DevBatch b = ctx.batch();
+    OLF_CUDA(cudaMemsetAsync(ctx.nActive.p, 0, sizeof(int), st));
     laneInitKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b);
     launchFill(dn.view, b, true, false, st);
     OLF_CUDA(cudaStreamSynchronize(st));
@@ -1434,7 +1944,7 @@ void debugFill(BatchContext& ctx, const double* xFull, const double* targetBase,
 void debugLinearSolve(BatchContext& ctx, const double* csrVals, const double* rhs, int precision, double* out) {
     OLF_CUDA(cudaSetDevice(ctx.device));
     const Structure& s = ctx.net->host;
-    const DeviceNet& dn = *ctx.net->dev;
+    const DeviceNet& dn = *ctx.dn;
     const DevNet& net = dn.view;
     const int n = s.n;
     const size_t S = ctx.S;
@@ -1452,6 +1962,7 @@ void debugLinearSolve(BatchContext& ctx, const double* csrVals, const double* rh
     OLF_CUDA(cudaMemcpyAsync(ctx.J.p, J.data(), ctx.J.bytes, cudaMemcpyHostToDevice, ctx.stream));
     OLF_CUDA(cudaMemcpyAsync(ctx.F.p, F.data(), F.size() * 8, cudaMemcpyHostToDevice, ctx.stream));
     const DevBatch b = ctx.batch();
+    OLF_CUDA(cudaMemsetAsync(ctx.nActive.p, 0, sizeof(int), st));
     laneInitKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b);
     launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, fp32,
                  nullptr, st);

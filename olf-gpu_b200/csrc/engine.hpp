@@ -3,7 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -81,14 +83,49 @@ struct DeviceNet {
     // shared-memory solve regions: the forward tail [fwdFrom, nFwd) and the backward head [0, bwdUntil) (slots 0: none)
     int fwdRegionBase = 0, fwdRegionSlots = 0, bwdRegionSlots = 0;
     DeviceBuffer lrowSlot, uSlot, fwdRegionStart;
+    // subtree bins of the wide levels (sub.nBins 0: none) and the top lists of the wide levels
+    SubtreePlan sub{};
+    DeviceBuffer binLevPtr, binLevOff, binTask, binFwdPtr, binFwdOff, binFwdPos, binBwdPtr, binBwdOff, binBwdPos,
+        topLevelTaskD, topFwdPosD, topBwdPosD;
+    std::vector<int> topLevelPtr, topLevelSplit, topFwdPtr, topFwdSplit, topBwdPtr, topBwdSplit, binPhasePtr,
+        binFwdPhasePtr, binBwdPhasePtr;
+    int binTasks = 0;               // LU blocks the bins factorize (of nLu)
 };
 
+// A structure and its device copies, one per device ordinal (uploaded on first use there).  Contexts hold their own
+// device copy, so creating a context on another GPU never touches the copies that contexts on other GPUs use.
 struct NetStructure {
     Structure host;
-    std::shared_ptr<DeviceNet> dev;
+    std::mutex mu;
+    std::map<int, std::shared_ptr<DeviceNet>> devs;
+    // The copy on `device` (which the caller has made current), uploaded on first use.
+    std::shared_ptr<DeviceNet> onDevice(int device);
+    // The copy on `device`, or null when none was uploaded there.
+    std::shared_ptr<DeviceNet> find(int device);
 };
 
 std::shared_ptr<DeviceNet> uploadNet(const Structure& s);
+
+// The level schedule's narrow boundaries: factorization levels [factorFrom, factorTo) hold at most 48 tasks (the range
+// or shared-memory region), forward levels from fwdFrom and backward levels before bwdUntil likewise.
+struct NarrowBounds {
+    int factorFrom, factorTo, fwdFrom, bwdUntil;
+};
+NarrowBounds narrowBounds(const BlockPlan& p);
+
+// The subtree bins of a plan's wide levels and the top lists of every level (host arrays; see SubtreePlan).
+struct SubtreeBinsHost {
+    int nBins = 0;
+    std::vector<int> phasePtr;       // bins of phase f: [phasePtr[f], phasePtr[f + 1])
+    std::vector<int> levPtr, levOff, task, fwdPtr, fwdOff, fwdPos, bwdPtr, bwdOff, bwdPos;
+    std::vector<int> topLevelPtr, topTask, topFwdPtr, topFwd, topBwdPtr, topBwd;
+    std::vector<int> fwdPhasePtr, bwdPhasePtr;   // the forward and backward sweeps' bins per phase
+    std::vector<int> taskBin, fwdBinOf, bwdBinOf;  // factorization bin of each LU block, sweep bins of each position
+    std::vector<int> posOf;          // position of each LU block
+};
+SubtreeBinsHost planSubtreeBins(const BlockPlan& p, const NarrowBounds& nbd);
+// "" when the bins keep every dependency of the factorization and both sweeps, else the first violation.
+std::string checkSubtreeBins(const BlockPlan& p, const NarrowBounds& nbd, const SubtreeBinsHost& h);
 
 // Schedules of the Newton iterations: one launch per dependency level (captured in a CUDA graph per iteration), or
 // the persistent kernel with one CTA per lane tile running the whole loop.
@@ -99,7 +136,8 @@ enum {
     SCHEDULE_PERSISTENT = 1,
     SCHEDULE_COOP = 2,
     SCHEDULE_LEVELS_SHARED = 3,
-    SCHEDULE_LEVELS_SHARED_ALL = 4
+    SCHEDULE_LEVELS_SHARED_ALL = 4,
+    SCHEDULE_SUBTREES = 5          // schedule 4 with the wide levels' subtrees in one launch per phase (subtree bins)
 };
 
 // Mixed precision: a refinement step's correction solve runs only while some lane's FP64 residual max |r| is above
@@ -133,10 +171,17 @@ struct SolveRequest {
     double reactiveLimitTol = 1e-4;
     int maxOuter = 20;
     int maxPqPvSwitch = 3;
+    double convEpsPerEq = 0.0;       // > 0: OLF's ||F||2 < sqrt(convEpsPerEq^2 n) stopping criterion
+    int stateVectorScalingMode = 0;  // 0 NONE, 2 MAX_VOLTAGE_CHANGE
+    double maxDv = 0.1, maxDphi = 0.17453292519943295;
+    const int* varType = nullptr;    // [n] 0 BUS_V, 1 BUS_PHI (MAX_VOLTAGE_CHANGE)
+    bool skipReactiveLimits = false; // this solve runs without the reactive-limit outer loop
+    const unsigned char* laneLive = nullptr;  // [nS] or null: the bank lanes that hold a scenario of this solve
 };
 
 struct BatchContext {
     std::shared_ptr<NetStructure> net;
+    std::shared_ptr<DeviceNet> dn;     // the structure's copy on this context's device
     int device = 0;
     int nS = 0, S = 0;
     cudaStream_t stream = nullptr;
@@ -145,8 +190,24 @@ struct BatchContext {
     int refinementSteps = 1;
     // lane-interleaved state
     DeviceBuffer x, target, mode, F, J, lu64, lu32, w64, w32, dx, res, qbuf, disabled, norm, iter, status, outer,
-        totalIter, trouble, normOut, active, pending, precision64, nActive, fallbackLeft, fellBack, resNorm;
+        totalIter, trouble, normOut, active, pending, precision64, nActive, fallbackLeft, fellBack, resNorm, fp64Left,
+        refine, ssqPart, solveRatio, stepMax, varType, vCheck;
+    bool fp64Restart = true;        // mixed: a lane whose solve fails restarts once in FP64 (persistent: fully refined)
+    bool fp64RestartOn = false;     // in force for the installed batch
+    bool hasVarType = false;        // the request carried the variable types of the MAX_VOLTAGE_CHANGE clamp
+    bool hasVCheck = false;         // the realistic-voltage rows are set
+    DeviceBuffer laneLive;          // [S] installed lanes of the solve (hasLaneLive)
+    std::vector<int8_t> liveHost;
+    bool hasLaneLive = false;
+    // the boundary's slot bookkeeping (BatchSolveNative.beginBatchInstall / readBatchHandedBackSlots /
+    // setBatchStatesToHost): the bank slots the next solve installs (empty: the whole bank), the slots the last solve
+    // handed back, whether result rows carry the states, and the reactive-limit outer loop switch
+    std::vector<int> installSlots, handedBack;
+    bool statesToHost = true;
+    int64_t solveCount = 0;         // solves run through the full entry (BatchReadbackNative.readBatchSolveCount)
+    bool reactiveLimitsLoop = true;
     bool fallbackStart = false;     // lanes that fail from x0Full restart once from x0Base (both given)
+    bool rlKeys = false;            // the reactive-limit entries' forced-PV election keys are set
     const double* deviceStart = nullptr;  // caller's device array [nS][n] used as x0Full by the solves
     const double* fullSrc = nullptr;      // where the installed x0Full rows come from
     DeviceBuffer stage;             // upload staging (base vectors)
@@ -161,8 +222,9 @@ struct BatchContext {
     int narrowLanes = 2;            // level schedule: lanes per tile of the narrow-level range launches (0: none)
     bool regionFactor = false;      // level schedule: the narrow factorization levels in shared memory
     bool regionSolve = false;       // level schedule: the solves' narrow levels in shared memory too
+    bool subtrees = false;          // level schedule: the wide levels' independent subtrees as bins (schedule 5)
     Hybrid hybrid() const {
-        const DeviceNet& d = *net->dev;
+        const DeviceNet& d = *dn;
         Hybrid h{d.factorFrom, d.factorTo, d.fwdFrom, d.bwdUntil, narrowLanes, d.persistent};
         h.plan.maxRounds = 1;
         if (regionFactor && d.regionSlots > 0) {
@@ -171,6 +233,7 @@ struct BatchContext {
             h.regionSlots = d.regionSlots;
             h.regionTask = d.regionTask.as<int4>();
         }
+        if (subtrees && d.sub.nBins > 0) h.sub = &d.sub;
         if (regionSolve) {
             h.solveRegion = true;
             h.fwdRegionBase = d.fwdRegionBase;
@@ -182,7 +245,7 @@ struct BatchContext {
         }
         return h;
     }
-    bool useHybrid() const { return narrowLanes > 0 || regionFactor || regionSolve; }
+    bool useHybrid() const { return narrowLanes > 0 || regionFactor || regionSolve || subtrees; }
     std::vector<TuningResult> tuning;
     DeviceBuffer out;               // [nS][n + 3] scenario-major results
     // reactive limits
@@ -192,7 +255,7 @@ struct BatchContext {
     // host staging (pinned) and the per-scenario start states
     uint32_t* hostBitsPinned = nullptr;
     DeviceBuffer full;
-    int* hostActive = nullptr;      // pinned [4]: lanes iterating, factorizing, to refine, flagged for FP64
+    int* hostActive = nullptr;      // pinned [8]: lanes iterating, factorizing, to refine, flagged for FP64, scored
     cudaEvent_t countReady = nullptr;  // mixed: the FP64-flag count has reached the host
     // one Newton iteration as a CUDA graph (captured on first use per settings)
     cudaGraphExec_t graph = nullptr;       // fill, test, reactive limits, lane counts
@@ -201,8 +264,17 @@ struct BatchContext {
     // solve of the flagged lanes; the step
     cudaGraphExec_t graphFactor = nullptr, graphResidual = nullptr, graphCorrect = nullptr, graph64 = nullptr,
                     graphStep = nullptr;
+    // the same iteration with the linear-solve scoring before the step (FP64: factorization, solves, scoring, step;
+    // mixed: scoring, step)
+    cudaGraphExec_t graphSolveScored = nullptr, graphStepScored = nullptr;
     int graphKey = -1;
-    double refineBelow = 1e-5;      // mixed: refinement steps only in iterations where a lane's max |F| is below it
+    DevBatch graphBatch{};          // the batch view and settings the iteration graphs were captured with
+    Settings graphCfg{};
+    // mixed: a lane refines only in an iteration where its max |F| is below refineBelow; 1e-2 covers every step from
+    // which Newton can land below the tolerance, so a converged state's last step is FP64-accurate
+    double refineBelow = 1e-2;
+    double corrBound = 1e-11;       // mixed: a lane keeps refining while its last correction's max |d| is above it
+    double realisticMinV = 0.0, realisticMaxV = 0.0;   // realistic-voltage band (hasVCheck)
     double growthLimit = 1e4;       // mixed: FP32 pivot growth above which a lane refactors in FP64
     // statistics of the last solve
     int lastIterations = 0;         // batched iterations run
@@ -226,6 +298,11 @@ void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out);
 
 // Validates a request and uploads its inputs to the context (the first half of solveBatch).
 void stageRequest(BatchContext& ctx, const SolveRequest& req);
+
+// The forced-PV election keys of the context's reactive-limit entries (reactive_limits.cu:417-448): nominal V, P row
+// (-1: static P), static P, id rank, one per entry.
+void setStrongestPvKeys(BatchContext& ctx, const double* nomV, const int* pRow, const double* staticP,
+                        const int* idRank);
 
 struct MultiTuning {
     int lanesPerTile, threads, order;

@@ -205,18 +205,60 @@ void launchFill(const DevNet& net, const DevBatch& b, bool withJacobian, bool wi
 // ---------------------------------------------------------------------------------------------------------------
 // A lane whose solve failed: restarts from the fallback start when it still may (pending for this iteration, so it
 // neither factorizes nor counts an iteration; the next iteration fills at the fallback state), else retires.
+// The restart of a lane: its iteration count, trouble and scored ratio reset, pending for this iteration (it neither
+// factorizes nor counts an iteration; the next iteration fills at the restored state).
+__device__ void restartLane(const DevBatch& b, int s) {
+    b.iter[s] = 0;
+    b.trouble[s] = 0;
+    b.pending[s] = 1;
+    b.solveRatio[s] = 0.0;
+}
+
+// A lane whose solve failed: restarts from the fallback start when it still may; else, in mixed precision, restarts
+// once with FP64 factorizations and solves from its start (the FP64 engine's trajectory for that scenario, so a
+// scenario that fails does so as it does in FP64); else retires with the status.
 __device__ void failLane(const DevBatch& b, int s, int status) {
+    const size_t S = b.S;
     if (b.fallbackLeft[s]) {
         b.fallbackLeft[s] = 0;
         b.fellBack[s] = 1;
-        b.iter[s] = 0;
-        b.trouble[s] = 0;
-        b.pending[s] = 1;
-        const size_t S = b.S;
+        restartLane(b, s);
         for (int r = 0; r < b.nFallback; r++) b.x[(size_t)r * S + s] = b.fallbackX[r];
         return;
     }
+    if (b.fp64Left && b.fp64Left[s]) {
+        b.fp64Left[s] = 0;
+        b.precision64[s] = 1;
+        restartLane(b, s);
+        const int n = b.nFallback;
+        if (b.restartFull) {
+            for (int r = 0; r < n; r++) b.x[(size_t)r * S + s] = b.restartFull[(size_t)s * n + r];
+        } else {
+            for (int r = 0; r < n; r++) b.x[(size_t)r * S + s] = b.fallbackX[r];
+        }
+        return;
+    }
     b.status[s] = status;
+    b.active[s] = 0;
+    atomicSub(b.nActive, 1);
+}
+
+// OLF's realistic-voltage check of a converged state (realistic_voltage_check.cu:23-44): a checked voltage row
+// outside [minV, maxV] makes the state UNREALISTIC_STATE.
+__device__ bool unrealisticState(const DevBatch& b, const Settings& cfg, int s) {
+    if (!cfg.realistic || !b.vCheck) return false;
+    const size_t S = b.S;
+    for (int r = 0; r < b.nFallback; r++) {
+        if (!b.vCheck[r]) continue;
+        const double v = b.x[(size_t)r * S + s];
+        if (v < cfg.minV || v > cfg.maxV) return true;
+    }
+    return false;
+}
+
+// A converged lane leaves the loop CONVERGED, or UNREALISTIC_STATE when the realistic-voltage band rejects it.
+__device__ void retireConverged(const DevBatch& b, const Settings& cfg, int s) {
+    b.status[s] = unrealisticState(b, cfg, s) ? ST_UNREALISTIC_STATE : ST_CONVERGED;
     b.active[s] = 0;
     atomicSub(b.nActive, 1);
 }
@@ -228,27 +270,58 @@ __global__ void testKernel(DevBatch b, Settings cfg, int* remainingPv) {
     b.norm[s] = 0ull;
     const int it = b.iter[s];
     b.normOut[s] = nrm;
+    if (b.trouble[s]) {
+        // the last factorization met a near-singular 2x2 pivot, or its solve failed the linear-solve guard: the lane
+        // took no step (its iteration did not advance) and ends here
+        failLane(b, s, ST_LINEAR_SOLVE_FAILED);
+        return;
+    }
     if (!isfinite(nrm)) {
         failLane(b, s, ST_DIVERGED);
         return;
     }
-    if (it > 0 && b.trouble[s]) {
-        // the previous factorization met a near-singular 2x2 pivot: its step is not trusted
-        failLane(b, s, ST_LINEAR_SOLVE_FAILED);
-        return;
+    bool converged;
+    if (cfg.norm2Threshold > 0.0) {
+        const size_t S = b.S;
+        double ssq = 0.0;
+        for (int k = 0; k < SSQ_STRANDS; k++) ssq += b.ssqPart[(size_t)k * S + s];
+        converged = sqrt(ssq) < cfg.norm2Threshold;
+    } else {
+        converged = nrm < cfg.tol;
     }
-    if (it > 0 && nrm < cfg.tol && it < cfg.maxIter) {
+    if (it > 0 && converged && it < cfg.maxIter) {
         if (cfg.reactiveLimits && b.outer[s] < cfg.maxOuter) {
             b.pending[s] = 1;
             if (remainingPv) remainingPv[s] = 0;
         } else {
-            b.status[s] = ST_CONVERGED;
-            b.active[s] = 0;
-            atomicSub(b.nActive, 1);
+            retireConverged(b, cfg, s);
         }
         return;
     }
-    if (it == cfg.maxIter) failLane(b, s, ST_MAX_ITERATION_REACHED);
+    if (it == cfg.maxIter) {
+        // a budget spent on a solve that did not solve its system is a reject (newton_iteration.cu:371-392)
+        const bool badSolve = !(b.solveRatio[s] <= LIN_SOLVE_FAIL_RATIO);
+        failLane(b, s, badSolve ? (cfg.batchOfOne ? ST_LINEAR_SOLVE_FAILED : ST_REJECTED) : ST_MAX_ITERATION_REACHED);
+    }
+}
+
+// Per lane, the sum of squares of F over the rows of strand blockIdx.y * 8 + threadIdx.y (rows r = strand mod
+// SSQ_STRANDS, in row order): 32 lanes x 8 strands per CTA.
+__global__ void ssqKernel(DevNet net, DevBatch b) {
+    const int s = blockIdx.x * 32 + threadIdx.x;
+    const int k = blockIdx.y * 8 + threadIdx.y;
+    const size_t S = b.S;
+    if (s >= b.S || k >= SSQ_STRANDS || !b.active[s]) return;
+    double acc = 0.0;
+    for (int r = k; r < net.n; r += SSQ_STRANDS) {
+        const double f = b.F[(size_t)r * S + s];
+        acc += f * f;
+    }
+    b.ssqPart[(size_t)k * S + s] = acc;
+}
+
+void launchNorm2(const DevNet& net, const DevBatch& b, cudaStream_t st) {
+    ssqKernel<<<dim3(b.S / 32, SSQ_STRANDS / 8), dim3(32, 8), 0, st>>>(net, b);
 }
 
 void launchTest(const DevNet&, const DevBatch& b, const Settings& cfg, int* remainingPv, cudaStream_t st) {
@@ -303,7 +376,7 @@ __global__ void rlCheckKernel(DevBatch b, DevRl rl, Settings cfg) {
     }
 }
 
-__global__ void rlFinalizeKernel(DevBatch b, DevRl rl) {
+__global__ void rlFinalizeKernel(DevBatch b, DevRl rl, Settings cfg) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= b.S || !b.pending[s]) return;
     const size_t S = b.S;
@@ -340,10 +413,8 @@ __global__ void rlFinalizeKernel(DevBatch b, DevRl rl) {
         b.iter[s] = 0;
         b.outer[s]++;
     } else {
-        b.status[s] = ST_CONVERGED;
-        b.active[s] = 0;
         b.pending[s] = 0;
-        atomicSub(b.nActive, 1);
+        retireConverged(b, cfg, s);
     }
 }
 
@@ -351,7 +422,7 @@ void launchReactiveLimits(const DevNet&, const DevBatch& b, const DevRl& rl, con
     if (rl.nRl == 0) return;
     const size_t threads = (size_t)rl.nRl * b.S;
     rlCheckKernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(b, rl, cfg);
-    rlFinalizeKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b, rl);
+    rlFinalizeKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b, rl, cfg);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -539,19 +610,226 @@ static void launchLevel(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStr
         default: OLF_SPLIT_CASE(16, KERNEL, T_, __VA_ARGS__)                                            \
     }
 
+// ---------------------------------------------------------------------------------------------------------------
+// Subtree bins of the wide levels: one CTA per (bin, 32 lanes), 8 warps; the bin's levels in order with a CTA barrier
+// between them.  In a level with fewer tasks than warps, P warps share a task (its updates split P ways, partial sums
+// added in part order through shared memory), as the level kernels' split does.  Every barrier sits in control flow
+// that is uniform over the CTA (bin, level and round counts are the same for all its threads).
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ int binSplit(int cnt) {
+    int P = 1;
+    while (P < 8 && cnt * P * 2 <= 8) P *= 2;
+    return P;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) subtreeFactorKernel(DevNet net, DevBatch b, T* lu, SubtreePlan sp, int binBase) {
+    __shared__ T red[8][4][32];
+    const size_t S = b.S;
+    const int lane = threadIdx.x, warp = threadIdx.y;
+    const int s = blockIdx.y * 32 + lane;
+    const bool ok = s < b.S && solving(b, s);
+    const int bin = binBase + blockIdx.x;
+    const int v0 = sp.levPtr[bin], v1 = sp.levPtr[bin + 1];
+    for (int v = v0; v < v1; v++) {
+        const int first = sp.levOff[v], cnt = sp.levOff[v + 1] - first;
+        const int P = binSplit(cnt), per = 8 / P, part = warp % P, slot = warp / P;
+        for (int base = 0; base < cnt; base += per) {
+            const int k = base + slot;
+            const bool has = ok && k < cnt;
+            T a00 = 0, a01 = 0, a10 = 0, a11 = 0, amax = 0;
+            int t = 0;
+            Task tk{};
+            if (has) {
+                t = sp.task[first + k];
+                tk = net.task[t];
+                if (part == 0 && tk.aBlock >= 0) {
+                    const double* pa = b.J + (size_t)tk.aBlock * 4 * S + s;
+                    a00 = (T)pa[0];
+                    a01 = (T)pa[S];
+                    a10 = (T)pa[2 * S];
+                    a11 = (T)pa[3 * S];
+                    amax = fmax(fmax(fabs(a00), fabs(a01)), fmax(fabs(a10), fabs(a11)));
+                }
+#pragma unroll 4
+                for (int q = tk.opBegin + part; q < tk.opEnd; q += P) {
+                    const int4 op = net.ops[q];
+                    T m00, m01, m10, m11, u00, u01, u10, u11;
+                    load4(lu, (size_t)op.x, S, s, m00, m01, m10, m11);
+                    load4(lu, (size_t)op.y, S, s, u00, u01, u10, u11);
+                    a00 -= m00 * u00 + m01 * u10;
+                    a01 -= m00 * u01 + m01 * u11;
+                    a10 -= m10 * u00 + m11 * u10;
+                    a11 -= m10 * u01 + m11 * u11;
+                }
+            }
+            if (P > 1) {
+                red[warp][0][lane] = a00;
+                red[warp][1][lane] = a01;
+                red[warp][2][lane] = a10;
+                red[warp][3][lane] = a11;
+                __syncthreads();
+                if (part == 0) {
+                    for (int q = 1; q < P; q++) {
+                        a00 += red[warp + q][0][lane];
+                        a01 += red[warp + q][1][lane];
+                        a10 += red[warp + q][2][lane];
+                        a11 += red[warp + q][3][lane];
+                    }
+                }
+                __syncthreads();
+            }
+            if (!has || part != 0) continue;
+            if (tk.diag == -2) {
+                const T det = a00 * a11 - a01 * a10;
+                const T scale = fabs(a00 * a11) + fabs(a01 * a10);
+                if (!(fabs(det) > (T)1e-13 * scale) || !isfinite(det)) b.trouble[s] = TROUBLE_PIVOT;
+                const T inv = (T)1 / det;
+                if (sizeof(T) == 4) pivotGrowth(b, s, a00, a01, a10, a11, inv, amax);
+                store4(lu, (size_t)t, S, s, a11 * inv, -a01 * inv, -a10 * inv, a00 * inv);
+            } else if (tk.diag >= 0) {
+                T i00, i01, i10, i11;
+                load4(lu, (size_t)tk.diag, S, s, i00, i01, i10, i11);
+                store4(lu, (size_t)t, S, s, a00 * i00 + a01 * i10, a00 * i01 + a01 * i11, a10 * i00 + a11 * i10,
+                       a10 * i01 + a11 * i11);
+            } else {
+                store4(lu, (size_t)t, S, s, a00, a01, a10, a11);
+            }
+        }
+        __syncthreads();   // this level's blocks are written before the next level reads them
+    }
+}
+
+// The bins' forward (DIR 0: w_i -= L(i,j) w_j over the bin's positions from the leaves up) or backward sweep (DIR 1:
+// w_i = inv(D_i) (w_i - U(i,j) w_j) from the bins' roots down; every ancestor outside the bin is final before).
+template <typename T, int DIR>
+__global__ void __launch_bounds__(256) subtreeSolveKernel(DevNet net, DevBatch b, const T* lu, T* w, SubtreePlan sp,
+                                                           int binBase) {
+    __shared__ T red[8][2][32];
+    const size_t S = b.S;
+    const int lane = threadIdx.x, warp = threadIdx.y;
+    const int s = blockIdx.y * 32 + lane;
+    const bool ok = s < b.S && solving(b, s);
+    const int* ptr = DIR == 0 ? sp.fwdPtr : sp.bwdPtr;
+    const int* off = DIR == 0 ? sp.fwdOff : sp.bwdOff;
+    const int* pos = DIR == 0 ? sp.fwdPos : sp.bwdPos;
+    const int v0 = ptr[binBase + blockIdx.x], v1 = ptr[binBase + blockIdx.x + 1];
+    for (int v = v0; v < v1; v++) {
+        const int first = off[v], cnt = off[v + 1] - first;
+        const int P = binSplit(cnt), per = 8 / P, part = warp % P, slot = warp / P;
+        for (int base = 0; base < cnt; base += per) {
+            const int k = base + slot;
+            const bool has = ok && k < cnt;
+            T w0 = 0, w1 = 0;
+            int i = 0, d = 0;
+            if (has) {
+                i = pos[first + k];
+                if (part == 0) {
+                    w0 = w[(2 * (size_t)i) * S + s];
+                    w1 = w[(2 * (size_t)i + 1) * S + s];
+                }
+                if (DIR == 0) {
+                    const int q1 = net.lrowEnd[i];
+                    for (int q = net.lrowPtr[i] + part; q < q1; q += P) {
+                        const int2 e = net.lrow[q];
+                        T l00, l01, l10, l11;
+                        load4(lu, (size_t)e.x, S, s, l00, l01, l10, l11);
+                        const T y0 = w[(2 * (size_t)e.y) * S + s], y1 = w[(2 * (size_t)e.y + 1) * S + s];
+                        w0 -= l00 * y0 + l01 * y1;
+                        w1 -= l10 * y0 + l11 * y1;
+                    }
+                } else {
+                    d = net.uPtr[i];
+                    const int q1 = net.uPtr[i + 1];
+                    for (int q = d + 1 + part; q < q1; q += P) {
+                        const int j = net.uCol[q];
+                        T u00, u01, u10, u11;
+                        load4(lu, (size_t)q, S, s, u00, u01, u10, u11);
+                        const T x0 = w[(2 * (size_t)j) * S + s], x1 = w[(2 * (size_t)j + 1) * S + s];
+                        w0 -= u00 * x0 + u01 * x1;
+                        w1 -= u10 * x0 + u11 * x1;
+                    }
+                }
+            }
+            if (P > 1) {
+                red[warp][0][lane] = w0;
+                red[warp][1][lane] = w1;
+                __syncthreads();
+                if (part == 0) {
+                    for (int q = 1; q < P; q++) {
+                        w0 += red[warp + q][0][lane];
+                        w1 += red[warp + q][1][lane];
+                    }
+                }
+                __syncthreads();
+            }
+            if (!has || part != 0) continue;
+            if (DIR == 0) {
+                w[(2 * (size_t)i) * S + s] = w0;
+                w[(2 * (size_t)i + 1) * S + s] = w1;
+            } else {
+                T i00, i01, i10, i11;
+                load4(lu, (size_t)d, S, s, i00, i01, i10, i11);
+                w[(2 * (size_t)i) * S + s] = i00 * w0 + i01 * w1;
+                w[(2 * (size_t)i + 1) * S + s] = i10 * w0 + i11 * w1;
+            }
+        }
+        __syncthreads();   // this level's entries are final before the next level reads them
+    }
+}
+
+// One launch per phase: the factorization and the forward sweep in phase order, the backward sweep in reverse.
+void launchSubtreeFactor(const DevNet& net, const DevBatch& b, const SubtreePlan& sp, bool fp32, cudaStream_t st) {
+    for (int f = 0; f < sp.nPhases; f++) {
+        const int b0 = sp.phasePtr[f], nb = sp.phasePtr[f + 1] - b0;
+        if (nb <= 0) continue;
+        dim3 grid(nb, b.S / 32), block(32, 8);
+        if (fp32) subtreeFactorKernel<float><<<grid, block, 0, st>>>(net, b, b.lu32, sp, b0);
+        else subtreeFactorKernel<double><<<grid, block, 0, st>>>(net, b, b.lu64, sp, b0);
+    }
+}
+
+void launchSubtreeSolve(const DevNet& net, const DevBatch& b, const SubtreePlan& sp, bool fp32, int dir,
+                        cudaStream_t st) {
+    const int nPhases = dir == 0 ? sp.nFwdPhases : sp.nBwdPhases;
+    const int* phasePtr = dir == 0 ? sp.fwdPhasePtr : sp.bwdPhasePtr;
+    for (int k = 0; k < nPhases; k++) {
+        const int f = dir == 0 ? k : nPhases - 1 - k;
+        const int b0 = phasePtr[f], nb = phasePtr[f + 1] - b0;
+        if (nb <= 0) continue;
+        dim3 grid(nb, b.S / 32), block(32, 8);
+        if (fp32) {
+            if (dir == 0) subtreeSolveKernel<float, 0><<<grid, block, 0, st>>>(net, b, b.lu32, b.w32, sp, b0);
+            else subtreeSolveKernel<float, 1><<<grid, block, 0, st>>>(net, b, b.lu32, b.w32, sp, b0);
+        } else {
+            if (dir == 0) subtreeSolveKernel<double, 0><<<grid, block, 0, st>>>(net, b, b.lu64, b.w64, sp, b0);
+            else subtreeSolveKernel<double, 1><<<grid, block, 0, st>>>(net, b, b.lu64, b.w64, sp, b0);
+        }
+    }
+}
+
 void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtr, const int* levelSplit, int nLevels,
                   bool fp32, const Hybrid* hybrid, cudaStream_t st) {
     clearTroubleKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b);
     const bool region = hybrid && hybrid->regionSlots > 0;
     const bool range = hybrid && !region && hybrid->lanes > 0;
     const int wide = region ? hybrid->regionFrom : range ? hybrid->factorFrom : nLevels;
+    // subtree bins: one launch for the bins, then the wide levels' top tasks only
+    const SubtreePlan* sub = hybrid && hybrid->sub && hybrid->sub->nBins > 0 ? hybrid->sub : nullptr;
+    DevNet top = net;
+    if (sub) {
+        launchSubtreeFactor(net, b, *sub, fp32, st);
+        top.levelTask = sub->topLevelTask;
+    }
     for (int l = 0; l < wide; l++) {
-        const int first = levelPtr[l], count = levelPtr[l + 1] - levelPtr[l];
+        const int* ptr = sub ? sub->topLevelPtr : levelPtr;
+        const int split = sub ? sub->topLevelSplit[l] : levelSplit[l];
+        const int first = ptr[l], count = ptr[l + 1] - ptr[l];
         if (count == 0) continue;
         if (fp32) {
-            OLF_SPLIT_DISPATCH(levelSplit[l], factorLevelKernel, float, net, b, b.lu32, first, count)
+            OLF_SPLIT_DISPATCH(split, factorLevelKernel, float, top, b, b.lu32, first, count)
         } else {
-            OLF_SPLIT_DISPATCH(levelSplit[l], factorLevelKernel, double, net, b, b.lu64, first, count)
+            OLF_SPLIT_DISPATCH(split, factorLevelKernel, double, top, b, b.lu64, first, count)
         }
     }
     if (region || range) {
@@ -715,8 +993,11 @@ __global__ void scatterKernel(DevNet net, DevBatch b, const T* w, bool accumulat
     const int cP = net.nodeCol[2 * node], cV = net.nodeCol[2 * node + 1];
     const double d0 = (double)w[(2 * (size_t)i) * S + s], d1 = (double)w[(2 * (size_t)i + 1) * S + s];
     if (accumulate) {
+        // a refinement correction: dx += d, and d kept in res for the correction check
         b.dx[cP * S + s] += d0;
         b.dx[cV * S + s] += d1;
+        b.res[cP * S + s] = d0;
+        b.res[cV * S + s] = d1;
     } else {
         b.dx[cP * S + s] = d0;
         b.dx[cV * S + s] = d1;
@@ -730,32 +1011,40 @@ static void solveT(const DevNet& net, const DevBatch& b, T* w, const T* lu, cons
     const bool fp32 = sizeof(T) == 4;
     rhsKernel<T><<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b, w, fromResidual);
     const bool region = hybrid && hybrid->solveRegion;   // the narrow levels in shared memory, one CTA per lane
+    // subtree bins: the bins' forward sweep first and their backward sweep last; the wide levels run their top
+    // positions only
+    const SubtreePlan* sub = hybrid && hybrid->sub && hybrid->sub->nBins > 0 ? hybrid->sub : nullptr;
     if (!region && hybrid && hybrid->lanes <= 0) hybrid = nullptr;   // no range launches in the solves
-    auto forwardLevels = [&](int l0, int l1) {
+    const LevelSchedule fwdTop = sub ? LevelSchedule{fwd.levels, sub->topFwdPtr, sub->topFwdPos, sub->topFwdSplit} : fwd;
+    const LevelSchedule bwdTop = sub ? LevelSchedule{bwd.levels, sub->topBwdPtr, sub->topBwdPos, sub->topBwdSplit} : bwd;
+    auto forwardLevels = [&](const LevelSchedule& ls, int l0, int l1) {
         for (int l = l0; l < l1; l++) {
-            const int first = fwd.ptr[l], count = fwd.ptr[l + 1] - fwd.ptr[l];
+            const int first = ls.ptr[l], count = ls.ptr[l + 1] - ls.ptr[l];
             if (count == 0) continue;
-            OLF_SPLIT_DISPATCH(fwd.split[l], forwardLevelKernel, T, net, b, lu, w, fwd.pos, first, count)
+            OLF_SPLIT_DISPATCH(ls.split[l], forwardLevelKernel, T, net, b, lu, w, ls.pos, first, count)
         }
     };
-    auto backwardLevels = [&](int l0, int l1) {
+    auto backwardLevels = [&](const LevelSchedule& ls, int l0, int l1) {
         for (int l = l0; l < l1; l++) {
-            const int first = bwd.ptr[l], count = bwd.ptr[l + 1] - bwd.ptr[l];
+            const int first = ls.ptr[l], count = ls.ptr[l + 1] - ls.ptr[l];
             if (count == 0) continue;
-            OLF_SPLIT_DISPATCH(bwd.split[l], backwardLevelKernel, T, net, b, lu, w, bwd.pos, first, count)
+            OLF_SPLIT_DISPATCH(ls.split[l], backwardLevelKernel, T, net, b, lu, w, ls.pos, first, count)
         }
     };
+    if (sub) launchSubtreeSolve(net, b, *sub, sizeof(T) == 4, 0, st);
     const int fwdWide = hybrid ? hybrid->fwdFrom : fwd.levels;
-    forwardLevels(0, fwdWide);
+    forwardLevels(fwdTop, 0, fwdWide);
     if (region && hybrid->fwdRegionSlots > 0) launchSolveRegion(net, b, *hybrid, fp32, 0, st);
-    else if (region) forwardLevels(fwdWide, fwd.levels);
+    else if (region) forwardLevels(fwd, fwdWide, fwd.levels);
     else if (hybrid) launchSolveRange(net, b, hybrid->plan, 0, fwdWide, fwd.levels, hybrid->lanes, fp32, st);
+    else if (sub) forwardLevels(fwdTop, fwdWide, fwd.levels);
     launchDenseFrontSolve(net, b, fp32, st);   // dense-front plans: the front rows, forward then backward
     const int bwdNarrow = hybrid ? hybrid->bwdUntil : 0;
     if (region && hybrid->bwdRegionSlots > 0) launchSolveRegion(net, b, *hybrid, fp32, 1, st);
-    else if (region) backwardLevels(0, bwdNarrow);
+    else if (region) backwardLevels(bwd, 0, bwdNarrow);
     else if (hybrid) launchSolveRange(net, b, hybrid->plan, 1, 0, bwdNarrow, hybrid->lanes, fp32, st);
-    backwardLevels(bwdNarrow, bwd.levels);
+    backwardLevels(bwdTop, bwdNarrow, bwd.levels);
+    if (sub) launchSubtreeSolve(net, b, *sub, sizeof(T) == 4, 1, st);
     scatterKernel<T><<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b, w, fromResidual);
 }
 
@@ -793,21 +1082,58 @@ void launchResidual(const DevNet& net, const DevBatch& b, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// Newton step x += dx for the lanes that solved this iteration (state_vector_scaling.cu:48-57, plain NR); the
-// per-lane iteration counters advance; a pending lane (reactive limits decided) is released.
+// Newton step for the lanes that solved this iteration: x += dx (state_vector_scaling.cu:48-51, plain NR), or
+// x += f dx with the MAX_VOLTAGE_CHANGE factor f = min(1, maxDv / max |dV|, maxDphi / max |dphi|)
+// (state_vector_scaling.cu:53-97).  A lane whose factorization or solve failed (trouble) takes no step and does not
+// advance its iteration: the next test ends it.  The per-lane iteration counters advance; a pending lane (reactive
+// limits decided) is released.
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void stepKernel(DevNet net, DevBatch b) {
+__global__ void stepMaxKernel(DevNet net, DevBatch b) {
+    __shared__ double red[2][8][32];
+    const int s = blockIdx.x * 32 + threadIdx.x;
+    const size_t S = b.S;
+    double mdv = 0.0, mdphi = 0.0;
+    if (s < b.S && solving(b, s)) {
+        for (int r = blockIdx.y * 8 + threadIdx.y; r < net.n; r += 8 * gridDim.y) {
+            const double a = fabs(b.dx[(size_t)r * S + s]);
+            if (b.varType[r] == VAR_BUS_V) mdv = fmax(mdv, a);
+            else if (b.varType[r] == VAR_BUS_PHI) mdphi = fmax(mdphi, a);
+        }
+    }
+    red[0][threadIdx.y][threadIdx.x] = mdv;
+    red[1][threadIdx.y][threadIdx.x] = mdphi;
+    __syncthreads();
+    if (threadIdx.y == 0 && s < b.S) {
+        for (int k = 1; k < 8; k++) {
+            mdv = fmax(mdv, red[0][k][threadIdx.x]);
+            mdphi = fmax(mdphi, red[1][k][threadIdx.x]);
+        }
+        if (mdv != 0.0) atomicMax(&b.stepMax[s], (unsigned long long)__double_as_longlong(mdv));
+        if (mdphi != 0.0) atomicMax(&b.stepMax[S + s], (unsigned long long)__double_as_longlong(mdphi));
+    }
+}
+
+__global__ void stepKernel(DevNet net, DevBatch b, Settings cfg) {
     const size_t S = b.S;
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int s = (int)(tid % S);
     const int r = (int)(tid / S);
-    if (r >= net.n) return;
-    if (solving(b, s)) b.x[(size_t)r * S + s] += b.dx[(size_t)r * S + s];
+    if (r >= net.n || !solving(b, s) || b.trouble[s]) return;
+    if (cfg.svsMode == SVS_MAX_VOLTAGE_CHANGE) {
+        const double mdv = __longlong_as_double((long long)b.stepMax[s]);
+        const double mdphi = __longlong_as_double((long long)b.stepMax[S + s]);
+        double f = 1.0;
+        if (mdv > cfg.maxDv) f = fmin(f, cfg.maxDv / mdv);
+        if (mdphi > cfg.maxDphi) f = fmin(f, cfg.maxDphi / mdphi);
+        b.x[(size_t)r * S + s] += f * b.dx[(size_t)r * S + s];
+    } else {
+        b.x[(size_t)r * S + s] += b.dx[(size_t)r * S + s];
+    }
 }
 
 __global__ void advanceKernel(DevBatch b) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= b.S || !b.active[s] || b.pending[s]) return;
+    if (s >= b.S || !b.active[s] || b.pending[s] || b.trouble[s]) return;
     b.iter[s]++;
     b.totalIter[s]++;
 }
@@ -821,14 +1147,22 @@ __global__ void releasePendingKernel(DevBatch b) {
 // After the test: how many lanes factorize this iteration (the host skips the factor/solve graph when none does) and
 // how many of those are close enough to convergence for the refinement steps (mode 0); or, after a mixed-precision
 // factorization, how many factorizing lanes are flagged for an FP64 refactor (mode 1).
-__global__ void countLanesKernel(DevBatch b, double refineBelow, int mode) {
-    __shared__ int part[2][32];
-    int c0 = 0, c1 = 0;
+__global__ void countLanesKernel(DevBatch b, double refineBelow, int mode, int maxIter) {
+    __shared__ int part[3][32];
+    int c0 = 0, c1 = 0, c2 = 0;
     for (int s = threadIdx.x; s < b.S; s += blockDim.x) {
         const bool sv = b.active[s] && !b.pending[s];
         if (mode == 0) {
+            // mixed precision: the lanes near convergence start this iteration's refinement (a lane already redone
+            // in FP64 needs none)
+            const bool near = sv && b.normOut[s] < refineBelow && !(b.precision64 && b.precision64[s]);
             c0 += sv ? 1 : 0;
-            c1 += sv && b.normOut[s] < refineBelow ? 1 : 0;
+            c1 += near ? 1 : 0;
+            if (b.refine) b.refine[s] = near ? 1 : 0;
+            // lanes whose solve is scored this iteration (the guard's second iteration of a first solve, or the
+            // iteration before the budget)
+            const int it = b.iter[s];
+            c2 += sv && ((b.outer[s] == 0 && it == 1) || it == maxIter - 1) ? 1 : 0;
         } else {
             c0 += sv && b.precision64[s] ? 1 : 0;
         }
@@ -836,21 +1170,25 @@ __global__ void countLanesKernel(DevBatch b, double refineBelow, int mode) {
     for (int o = 16; o > 0; o >>= 1) {
         c0 += __shfl_down_sync(0xffffffffu, c0, o);
         c1 += __shfl_down_sync(0xffffffffu, c1, o);
+        c2 += __shfl_down_sync(0xffffffffu, c2, o);
     }
     if ((threadIdx.x & 31) == 0) {
         part[0][threadIdx.x >> 5] = c0;
         part[1][threadIdx.x >> 5] = c1;
+        part[2][threadIdx.x >> 5] = c2;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        int t0 = 0, t1 = 0;
+        int t0 = 0, t1 = 0, t2 = 0;
         for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
             t0 += part[0][w];
             t1 += part[1][w];
+            t2 += part[2][w];
         }
         if (mode == 0) {
             b.nActive[1] = t0;
             b.nActive[2] = t1;
+            b.nActive[4] = t2;
         } else {
             b.nActive[3] = t0;
         }
@@ -861,11 +1199,11 @@ void launchIterationStart(const DevBatch& b, cudaStream_t st) {
     releasePendingKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b);
 }
 
-void launchCountSolving(const DevBatch& b, double refineBelow, cudaStream_t st) {
-    countLanesKernel<<<1, 1024, 0, st>>>(b, refineBelow, 0);
+void launchCountSolving(const DevBatch& b, double refineBelow, int maxIter, cudaStream_t st) {
+    countLanesKernel<<<1, 1024, 0, st>>>(b, refineBelow, 0, maxIter);
 }
 
-void launchCountFp64(const DevBatch& b, cudaStream_t st) { countLanesKernel<<<1, 1024, 0, st>>>(b, 0.0, 1); }
+void launchCountFp64(const DevBatch& b, cudaStream_t st) { countLanesKernel<<<1, 1024, 0, st>>>(b, 0.0, 1, 0); }
 
 // Per-lane max |res| over the rows: 32 lanes x 8 row strands per CTA, reduced in shared memory, one atomic per CTA
 // and lane (non-negative doubles order like their bit patterns; a NaN residual sorts above every number).
@@ -911,9 +1249,92 @@ void launchResidualCheck(const DevNet& net, const DevBatch& b, double threshold,
     countResidualKernel<<<1, 1024, 0, st>>>(b, threshold, refineBelow);
 }
 
-void launchStep(const DevNet& net, const DevBatch& b, bool, cudaStream_t st) {
+// After a correction solve: the lanes still refining are those whose correction max |d| (in b.res, reduced into
+// b.resNorm) is above the bound; a NaN correction stops the lane's refinement (its next test judges it).
+__global__ void correctionCountKernel(DevBatch b, double bound) {
+    __shared__ int part[32];
+    int c = 0;
+    for (int s = threadIdx.x; s < b.S; s += blockDim.x) {
+        if (!b.refine[s]) continue;
+        const double d = __longlong_as_double((long long)b.resNorm[s]);
+        const bool more = d > bound;
+        b.refine[s] = more ? 1 : 0;
+        c += more ? 1 : 0;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
+        b.nActive[2] = t;
+    }
+}
+
+void launchCorrectionCheck(const DevNet& net, const DevBatch& b, double bound, cudaStream_t st) {
+    cudaMemsetAsync(b.resNorm, 0, sizeof(unsigned long long) * b.S, st);
+    residualMaxKernel<<<dim3(b.S / 32, 64), dim3(32, 8), 0, st>>>(net, b);
+    correctionCountKernel<<<1, 1024, 0, st>>>(b, bound);
+}
+
+// The lanes whose solve is scored this iteration: the second iteration of the first solve (no reactive-limit restart
+// yet: the linear-solve guard, newton_iteration.cu:176-183,615-647) and the iteration before the budget (its ratio is
+// read by the budget's test, newton_iteration.cu:371-392,534-546).
+__device__ __forceinline__ bool scored(const DevBatch& b, const Settings& cfg, int s) {
+    if (!solving(b, s) || b.trouble[s]) return false;
+    const int it = b.iter[s];
+    return (b.outer[s] == 0 && it == 1) || it == cfg.maxIter - 1;
+}
+
+__global__ void scoreResidualKernel(DevNet net, DevBatch b, Settings cfg) {
+    const size_t S = b.S;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = (int)(tid % S);
+    const int node = (int)(tid / S);
+    if (node >= net.nb || !scored(b, cfg, s)) return;
+    const int cP = net.nodeCol[2 * node], cV = net.nodeCol[2 * node + 1];
+    double r0 = -b.F[cP * S + s], r1 = -b.F[cV * S + s];
+    for (int t = net.aPtr[node]; t < net.aPtr[node + 1]; t++) {
+        const int j = net.aCol[t];
+        const double* J = b.J + (size_t)t * 4 * S + s;
+        const double x0 = b.dx[(size_t)net.nodeCol[2 * j] * S + s], x1 = b.dx[(size_t)net.nodeCol[2 * j + 1] * S + s];
+        r0 -= J[0] * x0 + J[S] * x1;
+        r1 -= J[2 * S] * x0 + J[3 * S] * x1;
+    }
+    b.res[cP * S + s] = r0;
+    b.res[cV * S + s] = r1;
+}
+
+// ratio = max |r| / max |F| (1e300 when F is zero or r is not finite, linResidScoreBatch in iterative_refinement.cu);
+// a guard lane above LIN_SOLVE_FAIL_RATIO (NaN included) gets TROUBLE_GUARD, a budget lane keeps the ratio.
+__global__ void scoreFinishKernel(DevBatch b, Settings cfg) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.S || !scored(b, cfg, s)) return;
+    const double r = __longlong_as_double((long long)b.resNorm[s]);
+    const double f = b.normOut[s];
+    const double ratio = (f > 0.0 && isfinite(r)) ? r / f : 1e300;
+    const int it = b.iter[s];
+    if (it == cfg.maxIter - 1) b.solveRatio[s] = ratio;
+    if (b.outer[s] == 0 && it == 1 && !(ratio <= LIN_SOLVE_FAIL_RATIO)) b.trouble[s] = TROUBLE_GUARD;
+}
+
+void launchScoreSolve(const DevNet& net, const DevBatch& b, const Settings& cfg, cudaStream_t st) {
+    const size_t all = (size_t)net.nb * b.S;
+    scoreResidualKernel<<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b, cfg);
+    cudaMemsetAsync(b.resNorm, 0, sizeof(unsigned long long) * b.S, st);
+    residualMaxKernel<<<dim3(b.S / 32, 64), dim3(32, 8), 0, st>>>(net, b);
+    scoreFinishKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b, cfg);
+}
+
+void launchStep(const DevNet& net, const DevBatch& b, const Settings& cfg, cudaStream_t st) {
     const size_t all = (size_t)net.n * b.S;
-    stepKernel<<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b);
+    if (cfg.svsMode == SVS_MAX_VOLTAGE_CHANGE && b.varType) {
+        cudaMemsetAsync(b.stepMax, 0, sizeof(unsigned long long) * 2 * b.S, st);
+        stepMaxKernel<<<dim3(b.S / 32, 64), dim3(32, 8), 0, st>>>(net, b);
+    }
+    Settings c = cfg;
+    if (!b.varType) c.svsMode = SVS_NONE;
+    stepKernel<<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b, c);
     advanceKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b);
 }
 

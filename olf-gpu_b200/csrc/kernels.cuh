@@ -108,7 +108,7 @@ struct DevBatch {
     int8_t* active;           // [S] 1 while the lane iterates
     int8_t* pending;          // [S] 1: converged this iteration, reactive limits to check
     int8_t* precision64;      // [S] 1: this lane's last factorization fell back to FP64 (mixed precision)
-    int* nActive;             // [2] lanes still iterating, lanes factorizing this iteration (read by the host)
+    int* nActive;             // [8] lanes iterating, factorizing, refining, flagged for FP64, scored (read by the host)
     // fallback start: a lane whose solve ends unconverged (diverged, iteration cap, failed linear solve) while its
     // fallbackLeft flag is set restarts once from fallbackX (the base start, [n]) and marks fellBack
     const double* fallbackX;
@@ -120,8 +120,33 @@ struct DevBatch {
     // exceeds growthLimit flags its lane in precision64; laneMask (may be null) restricts the LU kernels to flagged lanes
     double growthLimit;
     const int8_t* laneMask;
-    unsigned long long* resNorm;  // [S] max |refinement residual| as ordered bits
+    unsigned long long* resNorm;  // [S] max |refinement residual| (or correction) as ordered bits
+    // mixed precision: a lane whose solve fails (diverged, iteration cap, failed linear solve) while fp64Left is set
+    // restarts once with every factorization and solve in FP64 (precision64 stays set), from its own start row of
+    // restartFull ([nS][n] scenario-major) or, when that is null, from fallbackX; fp64Left null: no such restart
+    int8_t* fp64Left;
+    const double* restartFull;
+    int8_t* refine;           // [S] mixed: lanes whose refinement correction is still above the bound
+    double* ssqPart;          // [SSQ_STRANDS][S] partial sums of F^2 (the 2-norm test)
+    double* solveRatio;       // [S] the linear-solve residual ratio scored before the iteration budget
+    unsigned long long* stepMax;  // [2][S] max |dV| and max |dphi| of the step (MAX_VOLTAGE_CHANGE), ordered bits
+    const int8_t* varType;    // [n] 0 BUS_V, 1 BUS_PHI, -1 neither (MAX_VOLTAGE_CHANGE); may be null
+    const int8_t* vCheck;     // [n] 1: a voltage row checked against the realistic band at convergence; may be null
+    const int8_t* laneLive;   // [S] 1: the lane holds a scenario of this solve (null: lanes < nS); others stay idle
 };
+
+// Strands of the deterministic 2-norm reduction (row r of a lane goes to strand r % SSQ_STRANDS, summed in row order,
+// then the strands in strand order).
+constexpr int SSQ_STRANDS = 64;
+// The linear-solve residual ratio ||J dx + F||inf / ||F||inf above which a solve did not solve the system
+// (iterative_refinement.cuh:21-23).
+constexpr double LIN_SOLVE_FAIL_RATIO = 1e-2;
+// trouble codes of a lane's last factorization / solve: 1 near-singular 2x2 pivot, 2 the linear-solve guard failed
+enum : int { TROUBLE_PIVOT = 1, TROUBLE_GUARD = 2 };
+// State-vector scaling modes (codes/gpu_state_vector_scaling_mode.cuh) and variable types
+// (codes/gpu_ac_variable_type.cuh) of the MAX_VOLTAGE_CHANGE step clamp.
+enum : int { SVS_NONE = 0, SVS_LINE_SEARCH = 1, SVS_MAX_VOLTAGE_CHANGE = 2 };
+enum : int { VAR_BUS_V = 0, VAR_BUS_PHI = 1 };
 
 // Reactive-limit entries (ReactiveLimitsPacker.java:76) and their per-lane state.
 struct DevRl {
@@ -155,6 +180,15 @@ struct Settings {
     int refinementSteps;
     double growthLimit;       // pivot growth above which a mixed lane refactors in FP64
     double refineBelow;       // refinement steps run in an iteration where a factorizing lane's max |F| is below it
+    double corrBound;         // mixed: a lane keeps refining while its last correction's max |d| is above it
+    // OLF's stopping criterion when > 0 (newton_iteration.cu:105,241-250): converged when ||F||2 < norm2Threshold =
+    // sqrt(convEpsPerEq^2 n); else the device's ||F||inf < tol
+    double norm2Threshold;
+    int batchOfOne;           // a bad last solve at the budget ends LINEAR_SOLVE_FAILED (one scenario) or REJECTED
+    int svsMode;              // SVS_NONE or SVS_MAX_VOLTAGE_CHANGE (state_vector_scaling.cu:53-97)
+    double maxDv, maxDphi;
+    int realistic;            // 1: a converged state with a checked voltage outside [minV, maxV] is UNREALISTIC_STATE
+    double minV, maxV;
 };
 
 // Kernel launchers (stream-ordered; all lanes of the batch).
@@ -190,9 +224,39 @@ void launchSolveRange(const DevNet& net, const DevBatch& b, const PersistentPlan
 // (launchRegionFactor): slot k holds the block of task levelTask[regionBase + k]; regionTask[k] = (task, end of its
 // updates, first update with an operand in the region, pivot code: -2 pivot, -1 / -3 stored as summed, >= 0 the
 // inverted pivot's block outside the region, <= -4 its slot -4 - code).
+// Subtree bins of the wide levels: independent subtrees of the elimination tree (a position's tasks only read blocks of
+// its own subtree), packed into bins; one CTA per (bin, 32 lanes) runs its bin level by level with a barrier between
+// levels, so the wide bottom of the factorization and of the solves costs one launch each instead of one per level.
+// Factorization: bin b's levels are [levPtr[b], levPtr[b + 1]), level v holding the LU blocks task[levOff[v] ..
+// levOff[v + 1]); the forward and backward solves likewise over positions.  The wide levels' other tasks (the
+// separators above the bins: "top" tasks) keep their level launches from the top lists (device arrays; the level
+// bounds and split factors are host arrays).
+struct SubtreePlan {
+    int nBins = 0;
+    // host: the factorization's bins of phase f are [phasePtr[f], phasePtr[f + 1]), the sweeps' likewise; a phase
+    // reads its own bin's values and earlier phases' (the backward sweep: later phases')
+    int nPhases = 0, nFwdPhases = 0, nBwdPhases = 0;
+    const int *phasePtr = nullptr, *fwdPhasePtr = nullptr, *bwdPhasePtr = nullptr;
+    const int *levPtr = nullptr, *levOff = nullptr, *task = nullptr;
+    const int *fwdPtr = nullptr, *fwdOff = nullptr, *fwdPos = nullptr;
+    const int *bwdPtr = nullptr, *bwdOff = nullptr, *bwdPos = nullptr;
+    const int* topLevelTask = nullptr;   // device: top tasks grouped by level (bounds topLevelPtr, host)
+    const int *topLevelPtr = nullptr, *topLevelSplit = nullptr;
+    const int* topFwdPos = nullptr;      // device: top positions grouped by forward level
+    const int *topFwdPtr = nullptr, *topFwdSplit = nullptr;
+    const int* topBwdPos = nullptr;      // device: top positions grouped by backward level
+    const int *topBwdPtr = nullptr, *topBwdSplit = nullptr;
+};
+// The bins' factorization (before the wide levels' top tasks), forward sweep (before the top forward levels) and
+// backward sweep (after every top backward level); no-op without bins.
+void launchSubtreeFactor(const DevNet& net, const DevBatch& b, const SubtreePlan& sp, bool fp32, cudaStream_t st);
+void launchSubtreeSolve(const DevNet& net, const DevBatch& b, const SubtreePlan& sp, bool fp32, int dir,
+                        cudaStream_t st);
+
 struct Hybrid {
     int factorFrom, factorTo, fwdFrom, bwdUntil, lanes;
     PersistentPlan plan;
+    const SubtreePlan* sub = nullptr;   // subtree bins of the wide levels (null: every wide level as launches)
     int regionFrom = 0, regionBase = 0, regionSlots = 0;
     const int4* regionTask = nullptr;
     // the solves' narrow levels in shared memory (launchSolveRegion): the forward tail [fwdFrom, nFwd) (slot k: position
@@ -227,17 +291,28 @@ void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtrHost,
 void launchSolve(const DevNet& net, const DevBatch& b, const LevelSchedule& fwd, const LevelSchedule& bwd, bool fp32,
                  bool fromResidual, const Hybrid* hybrid, cudaStream_t st);
 void launchResidual(const DevNet& net, const DevBatch& b, cudaStream_t st);
-void launchStep(const DevNet& net, const DevBatch& b, bool accumulate, cudaStream_t st);
+void launchStep(const DevNet& net, const DevBatch& b, const Settings& cfg, cudaStream_t st);
 void launchIterationStart(const DevBatch& b, cudaStream_t st);
-// Lanes that factorize this iteration (nActive[1]) and, of those, lanes whose max |F| is below refineBelow
-// (nActive[2]).
-void launchCountSolving(const DevBatch& b, double refineBelow, cudaStream_t st);
+// Lanes that factorize this iteration (nActive[1]); of those, the lanes whose max |F| is below refineBelow
+// (nActive[2], marked in b.refine: they start this iteration's refinement in mixed precision) and the lanes whose solve
+// is scored this iteration (nActive[4]).
+void launchCountSolving(const DevBatch& b, double refineBelow, int maxIter, cudaStream_t st);
 // Factorizing lanes flagged for an FP64 refactor (nActive[3]).
 void launchCountFp64(const DevBatch& b, cudaStream_t st);
 // Mixed precision, after launchResidual: each lane's max |r| and the count of factorizing lanes with max |F| below
 // refineBelow whose residual is above `threshold` (nActive[2]): the correction solve of a refinement step runs only
 // when some lane needs it.
 void launchResidualCheck(const DevNet& net, const DevBatch& b, double threshold, double refineBelow, cudaStream_t st);
+// After a correction solve of the refining lanes (b.laneMask = b.refine; the solve left each correction d in b.res):
+// a lane stays refining while max |d| > bound; nActive[2] = lanes still refining.
+void launchCorrectionCheck(const DevNet& net, const DevBatch& b, double bound, cudaStream_t st);
+// The 2-norm test's sum of squares of F per lane (deterministic strands), before launchTest.
+void launchNorm2(const DevNet& net, const DevBatch& b, cudaStream_t st);
+// Linear-solve scoring (iterative_refinement.cuh:21-23, newton_iteration.cu:378-392,615-647): for the lanes at the
+// second iteration of their first solve (the guard) or one iteration before the budget, r = -F - J dx and its ratio
+// max |r| / max |F|; a guard lane above LIN_SOLVE_FAIL_RATIO is marked TROUBLE_GUARD (no step; the next test ends it
+// LINEAR_SOLVE_FAILED), a budget lane keeps the ratio for the budget's test.
+void launchScoreSolve(const DevNet& net, const DevBatch& b, const Settings& cfg, cudaStream_t st);
 // The dense front of a dense-front plan (after every factorization level); no-op without a front.  prepareDenseFront
 // raises the kernels' dynamic shared-memory limit for a front of F pivots on the current device.
 void launchDenseFront(const DevNet& net, const DevBatch& b, bool fp32, cudaStream_t st);

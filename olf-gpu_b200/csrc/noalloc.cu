@@ -20,24 +20,50 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(64) << 20;   // 64 MiB, held by 
 
 __device__ __align__(256) unsigned char gNoAllocScratch[NOALLOC_SCRATCH_BYTES];
 
-// The array's device address, looked up once per device with that device current (the symbol's host-side name is a
-// stand-in, not a device address: it is never handed to a kernel).
+// The array's device address, looked up with the device current (the symbol's host-side name is a stand-in, not a
+// device address: it is never handed to a kernel).  The lookup is cached per device and per CUDA context: after the
+// device's context is destroyed and re-created (cudaDeviceReset), the module is loaded again and the array may sit
+// elsewhere, so a new context means a new lookup.  The current context comes from the driver's cuCtxGetCurrent,
+// reached through the runtime's entry-point query (the library does not link the driver library itself).
 std::mutex gScratchMutex;
-void* gScratchAddress[128] = {};
+struct ScratchSlot {
+    void* context = nullptr;
+    void* address = nullptr;
+};
+ScratchSlot gScratch[128];
+
+void* currentContext() {
+    using CtxGetCurrent = int (*)(void**);
+    static CtxGetCurrent fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            f = nullptr;
+        }
+        return reinterpret_cast<CtxGetCurrent>(f);
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0 || !ctx) throw std::runtime_error("no current CUDA context for the no-allocation solve");
+    return ctx;
+}
 
 void* scratchAddress(int device) {
     if (device < 0 || device >= 128) throw std::runtime_error("device ordinal out of range");
+    void* ctx = currentContext();
     std::lock_guard<std::mutex> lock(gScratchMutex);
-    if (!gScratchAddress[device]) {
+    ScratchSlot& slot = gScratch[device];
+    if (slot.context != ctx || !slot.address) {
         void* p = nullptr;
         const cudaError_t err = cudaGetSymbolAddress(&p, gNoAllocScratch);
         if (err != cudaSuccess || p == nullptr) {
             throw std::runtime_error(std::string("cudaGetSymbolAddress of the no-allocation scratch failed: ") +
                                      cudaGetErrorString(err));
         }
-        gScratchAddress[device] = p;
+        slot.context = ctx;
+        slot.address = p;
     }
-    return gScratchAddress[device];
+    return slot.address;
 }
 
 size_t align256(size_t v) { return (v + 255) / 256 * 256; }
@@ -90,11 +116,13 @@ __global__ void noallocInstallKernel(const int* csrToA, const double* csrVals, c
     }
 }
 
-__global__ void noallocGatherKernel(const double* dx, double* out, int n, int nS, int S) {
+// Solution [n][S] -> out [nS][n]; a scenario whose factorization met a (near-)singular 2x2 pivot gets NaN throughout,
+// so a failed solve never passes for an answer.
+__global__ void noallocGatherKernel(const double* dx, const int* trouble, double* out, int n, int nS, int S) {
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (size_t)n * nS) return;
     const int r = (int)(tid % n), s = (int)(tid / n);
-    out[(size_t)s * n + r] = dx[(size_t)r * S + s];
+    out[(size_t)s * n + r] = trouble[s] ? __longlong_as_double(0x7ff8000000000000LL) : dx[(size_t)r * S + s];
 }
 
 }  // namespace
@@ -106,11 +134,12 @@ void linearSolveNoAlloc(const std::shared_ptr<NetStructure>& net, int nScenarios
     if (precision != 0 && precision != 1) throw std::runtime_error("precision must be 0 (FP64) or 1 (FP32)");
     int device = 0;
     OLF_CUDA(cudaGetDevice(&device));
-    if (!net->dev || net->dev->device != device) {
+    const std::shared_ptr<DeviceNet> dnp = net->find(device);
+    if (!dnp) {
         throw std::runtime_error("the structure is not resident on the current device: create a batch context on it "
                                  "first (that call uploads the structure)");
     }
-    const DeviceNet& dn = *net->dev;
+    const DeviceNet& dn = *dnp;
     const DevNet& v = dn.view;
     const bool fp32 = precision == 1;
     const size_t S = static_cast<size_t>((nScenarios + 31) / 32 * 32);
@@ -148,7 +177,7 @@ void linearSolveNoAlloc(const std::shared_ptr<NetStructure>& net, int nScenarios
                  nullptr, st);
     launchSolve(v, b, dn.fwd(), dn.bwd(), fp32, false, nullptr, st);
     const size_t outCells = static_cast<size_t>(v.n) * nScenarios;
-    noallocGatherKernel<<<(unsigned)((outCells + 255) / 256), 256, 0, st>>>(b.dx, out, v.n, nScenarios,
+    noallocGatherKernel<<<(unsigned)((outCells + 255) / 256), 256, 0, st>>>(b.dx, b.trouble, out, v.n, nScenarios,
                                                                            static_cast<int>(S));
     OLF_CUDA(cudaGetLastError());
 }

@@ -50,8 +50,10 @@ struct TileState {
     int trouble[L];
     int remainingPv[L];
     int any[L];
-    int restart[L];      // failed this iteration and restarts from the fallback start
-    int refine;          // a factorizing lane of the tile is below the refinement threshold (or flagged)
+    int restart[L];      // failed this iteration and restarts (1: from the fallback start, 2: its FP64-grade restart)
+    int refine;          // some lane of the tile is still refining
+    int refining[L];     // mixed precision: this lane refines (near convergence or flagged) and its last correction
+                         // was above the bound; a lane's refinement never depends on its tile-mates'
     unsigned long long norm[L];
     int live;            // any lane of the tile still active
 };
@@ -434,8 +436,9 @@ __device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl
                 const int it = ts.iter[tid];
                 b.normOut[s0 + tid] = nrm;
                 int st = ST_RUNNING;
-                if (!isfinite(nrm)) st = ST_DIVERGED;
-                else if (it > 0 && troubled) st = ST_LINEAR_SOLVE_FAILED;
+                // a lane whose last factorization met a near-singular pivot took no step: it ends here
+                if (troubled) st = ST_LINEAR_SOLVE_FAILED;
+                else if (!isfinite(nrm)) st = ST_DIVERGED;
                 else if (it > 0 && nrm < cfg.tol && it < cfg.maxIter) {
                     if (rlOn && ts.outer[tid] < cfg.maxOuter) {
                         ts.pending[tid] = 1;
@@ -452,6 +455,13 @@ __device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl
                     b.fellBack[s0 + tid] = 1;
                     ts.iter[tid] = 0;
                     ts.restart[tid] = 1;
+                } else if (st != ST_RUNNING && st != ST_CONVERGED && b.fp64Left && b.fp64Left[s0 + tid]) {
+                    // mixed precision: a failed lane restarts once from its start with every solve refined to the
+                    // correction bound (precision64 marks it), so it follows the FP64 trajectory
+                    b.fp64Left[s0 + tid] = 0;
+                    b.precision64[s0 + tid] = 1;
+                    ts.iter[tid] = 0;
+                    ts.restart[tid] = 2;
                 } else if (st != ST_RUNNING) {
                     ts.status[tid] = st;
                     ts.active[tid] = 0;
@@ -461,8 +471,11 @@ __device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl
             }
         }
         __syncthreads();
-        if (ts.restart[lane]) {
+        if (ts.restart[lane] == 1 || (ts.restart[lane] == 2 && !b.restartFull)) {
             for (int r = slot; r < b.nFallback; r += slots) b.x[(size_t)r * S + s] = b.fallbackX[r];
+        } else if (ts.restart[lane] == 2) {
+            const int n = b.nFallback;
+            for (int r = slot; r < n; r += slots) b.x[(size_t)r * S + s] = b.restartFull[(size_t)s * n + r];
         }
         // ---------------- reactive limits (reactive_limits.cu:321-359, 417-448) ----------------
         if (rlOn) {
@@ -555,16 +568,20 @@ __device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl
             // ---------------- solves (one pass, then the refinement passes in mixed precision) ----------------
             if (tid == 0) {
                 int r = 0;
-                for (int k = 0; k < L; k++)
-                    r |= ts.solving[k] && (b.normOut[s0 + k] < cfg.refineBelow || b.precision64[s0 + k]);
+                for (int k = 0; k < L; k++) {
+                    ts.refining[k] = ts.solving[k] && (b.normOut[s0 + k] < cfg.refineBelow || b.precision64[s0 + k]);
+                    r |= ts.refining[k];
+                }
                 ts.refine = r;
             }
             __syncthreads();
             const int passes = 1 + (sizeof(T) == 4 && ts.refine ? cfg.refinementSteps : 0);
             for (int pass = 0; pass < passes; pass++) {
+                // pass 0: every solving lane; a refinement pass: the lanes still refining
+                const bool mine = pass == 0 ? solve : (solve && ts.refining[lane] != 0);
                 if (pass > 0) {
                     // FP64 residual r = -F - J dx
-                    if (solve) {
+                    if (mine) {
                         for (int node = slot; node < net.nb; node += slots) {
                             const int cP = net.nodeCol[2 * node], cV = net.nodeCol[2 * node + 1];
                             double r0 = -b.F[cP * S + s], r1 = -b.F[cV * S + s];
@@ -583,7 +600,7 @@ __device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl
                     __syncthreads();
                 }
                 // right-hand side in elimination positions
-                if (solve) {
+                if (mine) {
                     for (int i = slot; i < net.nb; i += slots) {
                         const int node = net.perm[i];
                         const int cP = net.nodeCol[2 * node], cV = net.nodeCol[2 * node + 1];
@@ -594,12 +611,13 @@ __device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl
                     }
                 }
                 __syncthreads();
-                solveLevels<T, L>(net, b, lu, w, plan.fwdPtr, plan.fwdPos, plan.fwdLongest, 0, 0, plan.nFwd, solve, lane,
+                solveLevels<T, L>(net, b, lu, w, plan.fwdPtr, plan.fwdPos, plan.fwdLongest, 0, 0, plan.nFwd, mine, lane,
                                   slot, slots, s, red);
-                solveLevels<T, L>(net, b, lu, w, plan.bwdPtr, plan.bwdPos, plan.bwdLongest, 1, 0, plan.nBwd, solve, lane,
+                solveLevels<T, L>(net, b, lu, w, plan.bwdPtr, plan.bwdPos, plan.bwdLongest, 1, 0, plan.nBwd, mine, lane,
                                   slot, slots, s, red);
                 // back to columns: dx = w (first pass) or dx += w (refinement)
-                if (solve) {
+                double dmax = 0.0;
+                if (mine) {
                     for (int node = slot; node < net.nb; node += slots) {
                         const int i = net.iperm[node];
                         const int cP = net.nodeCol[2 * node], cV = net.nodeCol[2 * node + 1];
@@ -610,19 +628,37 @@ __device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl
                         } else {
                             b.dx[cP * S + s] += d0;
                             b.dx[cV * S + s] += d1;
+                            dmax = absMaxP(absMaxP(dmax, d0), d1);
                         }
                     }
                 }
+                if (pass > 0) {
+                    // a lane stops refining once its correction is at or below the bound (a NaN one stops too)
+                    fred[slot][lane] = dmax;
+                    __syncthreads();
+                    if (tid < L) {
+                        double m = 0.0;
+                        for (int k = 0; k < slots; k++) m = absMaxP(m, fred[k][tid]);
+                        ts.refining[tid] = ts.refining[tid] && m > cfg.corrBound;
+                    }
+                    __syncthreads();
+                    if (tid == 0) {
+                        int r = 0;
+                        for (int k = 0; k < L; k++) r |= ts.refining[k];
+                        ts.refine = r;
+                    }
+                }
                 __syncthreads();
+                if (pass > 0 && !ts.refine) break;
             }
-            // ---------------- step ----------------
-            if (solve) {
+            // ---------------- step (not for a lane whose factorization failed) ----------------
+            if (solve && !ts.trouble[lane]) {
                 for (int r = slot; r < net.n; r += slots) b.x[(size_t)r * S + s] += b.dx[(size_t)r * S + s];
             }
         }
         __syncthreads();
         if (tid < L) {
-            if (ts.solving[tid]) {
+            if (ts.solving[tid] && !ts.trouble[tid]) {
                 ts.iter[tid]++;
                 b.totalIter[s0 + tid]++;
             }

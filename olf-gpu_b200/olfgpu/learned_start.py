@@ -371,3 +371,129 @@ def solve_with_fallback(ctx, p, x0_learned, x_base: np.ndarray, disabled: np.nda
             ctx.set_device_start(None)
     _, _, tot = ctx.last_stats()
     return r, tot.copy(), ctx.last_fallbacks()
+
+
+# ----------------------------------------------------------------------------------------------------------------
+# Command line: train a checkpoint on the engine's own N-1 solutions, and evaluate learned / base / flat starts.
+# ----------------------------------------------------------------------------------------------------------------
+def _start_error(x0: np.ndarray, sol: np.ndarray, ok: np.ndarray):
+    """max |dVm|, max |dVa| and the RMS over buses between the starts and the converged states (converged rows)."""
+    if not ok.any():
+        return None
+    d = x0[ok] - sol[ok]
+    return {"max_abs_dVm_pu": float(np.abs(d[:, 1::2]).max()), "max_abs_dVa_rad": float(np.abs(d[:, 0::2]).max()),
+            "rms_dVm_pu": float(np.sqrt(np.mean(d[:, 1::2] ** 2))), "rms_dVa_rad": float(np.sqrt(np.mean(d[:, 0::2] ** 2)))}
+
+
+def _histogram(it: np.ndarray, ok: np.ndarray) -> dict:
+    vals, counts = np.unique(it[ok].astype(int), return_counts=True)
+    return {str(int(v)): int(c) for v, c in zip(vals, counts)}
+
+
+def evaluate_starts(ls: "LearnedStart", scaling: float, n_outages: int, seed: int, max_iter: int = 15,
+                    tol: float = 1e-8) -> dict:
+    """Learned vs base vs flat start on ``n_outages`` outages at the load ``scaling`` (FP64 Newton judges each start
+    alone; the learned start is also run the way the product runs it: per scenario the better start by initial
+    mismatch, and a failed scenario restarts from the base start).  Iterations, converged fraction, the iteration
+    histogram and the start error against the converged states."""
+    from . import synthetic
+    g = ls.grid.scaled(scaling)
+    p = packing.pack(g, with_reactive_limits=False)
+    p0 = packing.pack(ls.grid, with_reactive_limits=False)
+    xb = ls.solve_base(g, p0.x_base if p0.x_base is not None else p0.x_flat)
+    rng = np.random.default_rng(seed)
+    outs = np.sort(rng.choice(synthetic.outage_candidates(ls.grid), size=n_outages, replace=False)).astype(np.int32)
+    dis = p.outage_masks(outs)
+    s = native.Structure(p, native.PLAN_DENSE_FRONT)
+    ctx = native.BatchContext(s, n_outages)
+    ctx.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
+    # the judge: FP64 Newton from the base start (the converged states the starts are measured against)
+    ref = ctx.solve(xb, p.target, p.base_row_mode, dis, max_iter=max_iter, tol=tol).copy()
+    ok_ref = ref[:, -1] == native.CONVERGED
+    learned = ls.predict(p, xb, outs)
+    starts = {"learned": learned, "base": np.tile(xb, (n_outages, 1)), "flat": np.tile(p.x_flat, (n_outages, 1))}
+    report = {"grid": ls.grid.spec.name, "scaling": scaling, "outages": n_outages, "seed": seed, "tol": tol,
+              "judge_converged_fraction": float(ok_ref.mean())}
+    for name, x0 in starts.items():
+        r = ctx.solve(None, p.target, p.base_row_mode, dis, x0_full=x0, max_iter=max_iter, tol=tol)
+        ok = r[:, -1] == native.CONVERGED
+        same = ok & ok_ref
+        d = np.abs(r[same, :p.n] - ref[same, :p.n]) if same.any() else np.zeros((1, 1))
+        report[name] = {"converged_fraction": float(ok.mean()),
+                        "iterations_per_solve": float(r[ok, p.n].mean()) if ok.any() else None,
+                        "iteration_histogram": _histogram(r[:, p.n], ok),
+                        "one_iteration_fraction": float(((r[:, p.n] == 1) & ok).mean()),
+                        "start_error": _start_error(x0, ref[:, :p.n], ok_ref),
+                        "max_state_difference_vs_judge": float(d.max())}
+    r, tot, fell = solve_with_fallback(ctx, p, learned, xb, dis, max_iter=max_iter, tol=tol)
+    ok = r[:, -1] == native.CONVERGED
+    report["learned_with_fallback"] = {"converged_fraction": float(ok.mean()),
+                                       "iterations_per_solve": float(tot[ok].mean()) if ok.any() else None,
+                                       "iteration_histogram": _histogram(r[:, p.n], ok),
+                                       "scenarios_on_base_start": int(fell.size),
+                                       "same_status_as_judge": int((r[:, -1] == ref[:, -1]).sum())}
+    return report
+
+
+def main(argv=None) -> int:
+    import argparse
+    import json
+    import os
+    from . import synthetic
+    ap = argparse.ArgumentParser(prog="python -m olfgpu.learned_start",
+                                 description="Train or evaluate the learned warm start (needs a CUDA GPU).")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train", help="generate N-1 solutions with the engine and train a checkpoint on them")
+    t.add_argument("--grid", default="grid9241")
+    t.add_argument("--scalings", type=int, default=100, help="load scalings U[lo, hi] (one base case each)")
+    t.add_argument("--per-scaling", type=int, default=500, help="random non-bridge outages solved per scaling")
+    t.add_argument("--held-out", type=int, default=2, help="the last scalings are held out of training")
+    t.add_argument("--lo", type=float, default=0.8)
+    t.add_argument("--hi", type=float, default=1.2)
+    t.add_argument("--epochs", type=int, default=6)
+    t.add_argument("--batch", type=int, default=32)
+    t.add_argument("--lr", type=float, default=2e-3)
+    t.add_argument("--seed", type=int, default=9241)
+    t.add_argument("--max-seconds", type=float, default=None)
+    t.add_argument("--out", required=True, help="checkpoint path (.npz)")
+    t.add_argument("--report", default=None, help="JSON report path (default: next to the checkpoint)")
+    e = sub.add_parser("eval", help="learned vs base vs flat start on held-out outages at a fresh load scaling")
+    e.add_argument("--grid", default="grid9241")
+    e.add_argument("--checkpoint", required=True)
+    e.add_argument("--scaling", type=float, default=1.07, help="the fresh load scaling (not a training draw)")
+    e.add_argument("--outages", type=int, default=500)
+    e.add_argument("--seed", type=int, default=424242)
+    e.add_argument("--report", default=None)
+    a = ap.parse_args(argv)
+    g = synthetic.build(a.grid)
+    if a.cmd == "train":
+        t0 = time.time()
+        ls = LearnedStart(g, seed=a.seed)
+        data = ls.generate(a.scalings, a.per_scaling, seed=a.seed, lo=a.lo, hi=a.hi)
+        gen_s = time.time() - t0
+        train_idx, held = ls.split(data, a.held_out)
+        before = ls.evaluate(data, held)
+        losses = ls.train(data, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed, samples=train_idx,
+                          max_seconds=a.max_seconds)
+        after = ls.evaluate(data, held)
+        ls.save(a.out)
+        rep = {"grid": a.grid, "samples": int(data.t.shape[0]), "training_samples": int(train_idx.shape[0]),
+               "held_out_samples": int(held.shape[0]), "scalings": a.scalings, "per_scaling": a.per_scaling,
+               "load_scaling_range": [a.lo, a.hi], "epochs": a.epochs, "batch": a.batch, "lr": a.lr, "seed": a.seed,
+               "adam_steps": int(ls.net.step), "epoch_losses": [float(v) for v in losses],
+               "held_out_normalised_mse": {"network": after[0], "untrained": before[0], "base_start": after[1]},
+               "generate_seconds": round(gen_s, 1), "total_seconds": round(time.time() - t0, 1)}
+        path = a.report or os.path.splitext(a.out)[0] + ".train.json"
+    else:
+        ls = LearnedStart.load(a.checkpoint, g)
+        rep = evaluate_starts(ls, a.scaling, a.outages, a.seed)
+        rep["checkpoint"] = os.path.basename(a.checkpoint)
+        path = a.report or os.path.splitext(a.checkpoint)[0] + ".eval.json"
+    with open(path, "w") as f:
+        json.dump(rep, f, indent=1)
+    print(json.dumps(rep, indent=1))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -38,10 +38,28 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_create_multi_context", "olfgpu_destroy_multi_context", "olfgpu_set_multi_schedule",
            "olfgpu_get_multi_schedule", "olfgpu_solve_multi_context", "olfgpu_set_fallback_start",
            "olfgpu_last_fallbacks", "olfgpu_set_phase_timing", "olfgpu_last_phase_times", "olfgpu_structure_levels",
-           "olfgpu_set_device_start", "olfgpu_set_mixed_precision_controls", "olfgpu_last_fp64_refactors"]
+           "olfgpu_set_device_start", "olfgpu_set_mixed_precision_controls", "olfgpu_last_fp64_refactors",
+           "olfgpu_solve_batch_context_full", "olfgpu_set_realistic_check", "olfgpu_set_refinement_bound",
+           "olfgpu_set_fp64_restart", "olfgpu_structure_subtrees", "olfgpu_create_structure_full",
+           "olfgpu_create_batch_context_full", "olfgpu_set_reactive_limit_strongest_pv_keys",
+           "olfgpu_begin_batch_install", "olfgpu_read_handed_back_slots", "olfgpu_set_states_to_host",
+           "olfgpu_states_to_host", "olfgpu_read_batch_states", "olfgpu_set_outer_loops", "olfgpu_context_info"]
+# The arrays of BatchSolveNative.solveBatchContext this engine rejects when non-empty, in the reference's order
+UNSUPPORTED_SOLVE_ARRAYS = [
+    "distributedSlackOverrideBus", "distributedSlackOverrideFactorDelta", "distributedSlackOverrideBaseTargetPDelta",
+    "distributedSlackOverrideMaxDelta", "distributedSlackOverrideMinDelta", "distributedSlackBusAnchorShift",
+    "slackBusAnchorShift", "reactiveLimitTargetVOverrideScenarioEntry", "reactiveLimitTargetVOverrideValue",
+    "reactiveLimitDeltaOverrideScenarioEntry", "reactiveLimitDeltaOverrideValues",
+    "reactiveCapabilityCurveOverrideScenarioCurve", "reactiveCapabilityCurveOverrideStepScale"]
+_INT_SOLVE_ARRAYS = {"distributedSlackOverrideBus", "reactiveLimitTargetVOverrideScenarioEntry",
+                     "reactiveLimitDeltaOverrideScenarioEntry", "reactiveCapabilityCurveOverrideScenarioCurve"}
+# State-vector scaling modes (codes/gpu_state_vector_scaling_mode.cuh) and variable types (gpu_ac_variable_type.cuh)
+SVS_NONE, SVS_LINE_SEARCH, SVS_MAX_VOLTAGE_CHANGE = 0, 1, 2
+VAR_BUS_V, VAR_BUS_PHI = 0, 1
 # Schedules of the Newton iterations (LEVELS_SHARED: the level schedule with the narrow factorization levels in
-# shared memory; LEVELS_SHARED_ALL: the solves' narrow levels too)
-LEVELS, PERSISTENT, COOPERATIVE, LEVELS_SHARED, LEVELS_SHARED_ALL, AUTOTUNE = 0, 1, 2, 3, 4, -1
+# shared memory; LEVELS_SHARED_ALL: the solves' narrow levels too; SUBTREES: LEVELS_SHARED_ALL with the wide levels'
+# independent subtrees in one launch per phase)
+LEVELS, PERSISTENT, COOPERATIVE, LEVELS_SHARED, LEVELS_SHARED_ALL, SUBTREES, AUTOTUNE = 0, 1, 2, 3, 4, 5, -1
 # Structure orderings (0 minimum degree, 1 nested dissection, 2 natural) and the deferred-L plan flag
 MIN_DEGREE, NESTED_DISSECTION, NATURAL, PLAN_DEFERRED_L, PLAN_DENSE_FRONT = 0, 1, 2, 8, 16
 
@@ -76,6 +94,25 @@ def load(path: str = LIB_PATH):
                                              _u8p, ctypes.c_int, _ip, _dp, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp]
     L.olfgpu_stage_batch_context.argtypes = L.olfgpu_solve_batch_context.argtypes[:-1]
+    _ci, _cd = ctypes.c_int, ctypes.c_double
+    L.olfgpu_solve_batch_context_full.argtypes = (
+        [_i64, _dp, _ci, _dp, _ci, _ip, _ci, _ip, _ci, _u8p, _ci, _ci, _ip, _ci, _dp, _ci,
+         _ip, _ci, _dp, _ci, _dp, _ci, _dp, _ci, _dp, _ci, _dp, _ci, _dp, _ci,    # distributed-slack overrides
+         _ip, _ci, _dp, _ci, _ip, _ci, _dp, _ci, _ip, _ci, _dp, _ci,              # reactive-limit overrides
+         _ci, _cd, _cd, _cd, _cd, _ci, _cd, _cd, _ip, _ci, _dp, _ci,
+         _ip, _ci, _dp, _ci, _ip, _ci, _ip, _ci, _dp, _ci,
+         _ci, _ci, _ci, _ci, _ci, _ip, _ci, _ip, _ci, _ci, _dp])
+    L.olfgpu_set_realistic_check.argtypes = [_i64, _u8p, _cd, _cd, _ci]
+    L.olfgpu_set_refinement_bound.argtypes = [_i64, _cd]
+    L.olfgpu_set_fp64_restart.argtypes = [_i64, _ci]
+    L.olfgpu_structure_subtrees.argtypes = [_i64, ctypes.POINTER(_i64)]
+    L.olfgpu_read_batch_states.argtypes = [_i64, _ci, _ip, _dp]
+    L.olfgpu_begin_batch_install.argtypes = [_i64, _ip, _ci]
+    L.olfgpu_read_handed_back_slots.argtypes = [_i64, _ip, _ci, _ip]
+    L.olfgpu_set_states_to_host.argtypes = [_i64, _ci]
+    L.olfgpu_states_to_host.argtypes = [_i64, _ip]
+    L.olfgpu_set_outer_loops.argtypes = [_i64, _ci, _ci]
+    L.olfgpu_context_info.argtypes = [_i64, _ip, _ip, _ip, _ip, _ip, ctypes.POINTER(_i64)]
     L.olfgpu_create_multi_context.argtypes = [ctypes.c_int, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]
     L.olfgpu_destroy_multi_context.argtypes = [_i64]
     L.olfgpu_set_multi_schedule.argtypes = [_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]
@@ -178,6 +215,14 @@ class Structure:
                                               ops.ctypes.data_as(ctypes.POINTER(_i64))))
         return f, ops, fw, bw
 
+    def subtrees(self) -> dict:
+        """The subtree bins of the wide levels (schedule SUBTREES), planned and checked on the host."""
+        st = (_i64 * 6)()
+        _check(load().olfgpu_structure_subtrees(self.handle, st))
+        return {"bins": int(st[0]) // 100, "phases": int(st[0]) % 100, "bin_blocks": int(st[1]),
+                "max_bin_levels": int(st[2]), "top_wide_blocks": int(st[3]), "bin_positions": int(st[4]),
+                "wide_levels": int(st[5])}
+
     def recommend_batch_size(self, max_cap: int, mode: int = BATCHED_LU) -> int:
         b = ctypes.c_int(0)
         _check(load().olfgpu_recommend_batch_size(self.handle, max_cap, mode, ctypes.byref(b)))
@@ -244,8 +289,52 @@ class BatchContext:
     def solve(self, x0_base, target_base, base_row_mode, disabled, x0_full=None, row_mode_entries=None,
               target_override_index=None, target_override_value=None, max_iter: int = 15, tol: float = 1e-8,
               reactive_limit_tol: float = 1e-4, max_outer: int = 20, max_pq_pv_switch: int = 3,
-              out: Optional[np.ndarray] = None) -> np.ndarray:
-        """Per scenario [x(n), iterations, ||F||inf, status] (BatchSolveNative.solveBatchContext)."""
+              out: Optional[np.ndarray] = None, conv_eps_per_eq: float = 0.0, svs_mode: int = SVS_NONE,
+              max_dv: float = 0.1, max_dphi: float = 0.17453292519943295, var_type=None,
+              skip_reactive_limits: bool = False, unsupported: Optional[dict] = None,
+              pause_at_ended: int = 0) -> np.ndarray:
+        """Per scenario [x(n), iterations, ||F||inf, status] through the full reference-shaped entry
+        (BatchSolveNative.solveBatchContext, olfgpu_solve_batch_context_full).  ``unsupported`` maps the name of an
+        argument in UNSUPPORTED_SOLVE_ARRAYS to an array passed as given (the engine rejects non-empty ones)."""
+        n = self.structure.n
+        disabled = _c(disabled, np.uint8)
+        ns = disabled.shape[0]
+        x0b = None if x0_base is None else _c(x0_base, np.float64)
+        x0f = None if x0_full is None else _c(x0_full, np.float64)
+        tb = _c(target_base, np.float64)
+        bm = _c(base_row_mode, np.int32)
+        rme = _c(np.zeros(0) if row_mode_entries is None else row_mode_entries, np.int32).reshape(-1)
+        toi = _c(np.zeros(0) if target_override_index is None else target_override_index, np.int32)
+        tov = _c(np.zeros(0) if target_override_value is None else target_override_value, np.float64)
+        vt = None if var_type is None else _c(var_type, np.int32)
+        extra = []
+        unsupported = unsupported or {}
+        for name in UNSUPPORTED_SOLVE_ARRAYS:
+            a = unsupported.get(name)
+            if a is None:
+                extra += [None, 0]
+            else:
+                a = _c(a, np.int32 if name in _INT_SOLVE_ARRAYS else np.float64)
+                extra += [_p(a) if a.size else None, int(a.size)]
+                self._keep_unsupported = a
+        if out is None:
+            out = np.zeros((ns, n + 3))
+        ln = lambda a: 0 if a is None else int(a.size)
+        _check(load().olfgpu_solve_batch_context_full(
+            self.handle, _p(x0b), ln(x0b), _p(tb), ln(tb), _p(rme) if rme.size else None, int(rme.size), _p(bm), ln(bm),
+            _p(disabled), ns, disabled.shape[1], _p(toi) if toi.size else None, int(toi.size),
+            _p(tov) if tov.size else None, int(tov.size), *extra, max_iter, tol, reactive_limit_tol, 0.0,
+            conv_eps_per_eq, svs_mode, max_dv, max_dphi, _p(vt), ln(vt), _p(x0f), ln(x0f),
+            None, 0, None, 0, None, 0, None, 0, None, 0,
+            max_outer, max_pq_pv_switch, 0, 1 if skip_reactive_limits else 0, 0, None, 0, None, 0, pause_at_ended,
+            _p(out)))
+        return out
+
+    def solve_simple(self, x0_base, target_base, base_row_mode, disabled, x0_full=None, row_mode_entries=None,
+                     target_override_index=None, target_override_value=None, max_iter: int = 15, tol: float = 1e-8,
+                     reactive_limit_tol: float = 1e-4, max_outer: int = 20, max_pq_pv_switch: int = 3,
+                     out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The same solve through olfgpu_solve_batch_context (the short argument list)."""
         args, keep = self._request(x0_base, target_base, base_row_mode, disabled, x0_full, row_mode_entries,
                                    target_override_index, target_override_value, max_iter, tol, reactive_limit_tol,
                                    max_outer, max_pq_pv_switch)
@@ -253,6 +342,20 @@ class BatchContext:
             out = np.zeros((keep[0].shape[0], self.structure.n + 3))
         _check(load().olfgpu_solve_batch_context(self.handle, *args, _p(out)))
         return out
+
+    def set_realistic_check(self, row_checked=None, min_v: float = 0.0, max_v: float = 0.0, enabled: bool = True):
+        """ReactiveLimitsNative.setBatchRealisticCheck: rows [n] whose converged voltage must lie in [min_v, max_v]."""
+        rc = None if row_checked is None else _c(row_checked, np.uint8)
+        self._row_checked = rc
+        _check(load().olfgpu_set_realistic_check(self.handle, _p(rc), min_v, max_v, 1 if enabled else 0))
+
+    def set_refinement_bound(self, correction_bound: float = 1e-11):
+        """Mixed precision: a scenario near convergence refines until its correction max |d| <= correction_bound."""
+        _check(load().olfgpu_set_refinement_bound(self.handle, correction_bound))
+
+    def set_fp64_restart(self, enable: bool = True):
+        """Mixed precision: a scenario whose solve fails restarts once in FP64 (on by default)."""
+        _check(load().olfgpu_set_fp64_restart(self.handle, 1 if enable else 0))
 
     def stage(self, x0_base, target_base, base_row_mode, disabled, x0_full=None, row_mode_entries=None,
               target_override_index=None, target_override_value=None, max_iter: int = 15, tol: float = 1e-8,
@@ -293,7 +396,7 @@ class BatchContext:
         d["factorized_lanes"] = int(o[7])
         return d
 
-    def set_mixed_precision_controls(self, refine_below: float = 1e-5, growth_limit: float = 1e4):
+    def set_mixed_precision_controls(self, refine_below: float = 1e-2, growth_limit: float = 1e4):
         """Mixed precision: refinement only below refine_below; FP64 refactor above growth_limit pivot growth."""
         _check(load().olfgpu_set_mixed_precision_controls(self.handle, refine_below, growth_limit))
 

@@ -31,9 +31,10 @@ FIXED_VARIABLE = 0
 EQUATION = 1
 BUS_TARGET_Q = 4
 
-# Variable types for state-vector scaling (0: angle, 1: voltage magnitude)
-VAR_PHI = 0
-VAR_V = 1
+# Variable types of the MAX_VOLTAGE_CHANGE step clamp, by OLF's AcVariableType ordinal
+# (codes/gpu_ac_variable_type.cuh): 0 BUS_V (voltage magnitude), 1 BUS_PHI (angle)
+VAR_V = 0
+VAR_PHI = 1
 
 
 @dataclasses.dataclass

@@ -704,7 +704,22 @@ static void glu_solve(glu *g, const double *b, double *z)
 /* ---------------------------------------------------------------------------------------------------------------
  * Newton-Raphson with the reference's status rules, plus the reactive-limit outer loop.
  * ------------------------------------------------------------------------------------------------------------- */
-enum { ST_CONVERGED = 0, ST_MAX_ITER = 1, ST_DIVERGED = -1, ST_REJECTED = -2, ST_LINEAR_SOLVE_FAILED = -3 };
+enum { ST_CONVERGED = 0, ST_MAX_ITER = 1, ST_UNREALISTIC = 2, ST_DIVERGED = -1, ST_REJECTED = -2,
+       ST_LINEAR_SOLVE_FAILED = -3 };
+
+/* iterative_refinement.cuh:21-23: a linear solve whose residual ratio ||J dx + F||inf / ||F||inf exceeds this did not
+ * solve its system. */
+#define LIN_SOLVE_FAIL_RATIO 1e-2
+
+/* Options of the batched solve beyond the plain Newton loop (NULL: none). */
+typedef struct {
+    double conv_eps_per_eq;       /* > 0: OLF's ||F||2 < sqrt(eps^2 n) test (newton_iteration.cu:105,241-250) */
+    int svs_mode;                 /* 0 NONE, 2 MAX_VOLTAGE_CHANGE (state_vector_scaling.cu:53-97) */
+    double max_dv, max_dphi;
+    const int *var_type;          /* [n] 0 BUS_V, 1 BUS_PHI */
+    const unsigned char *v_check; /* [n] realistic-voltage rows, or NULL (realistic_voltage_check.cu:23-44) */
+    double min_v, max_v;
+} oracle_opts;
 
 typedef struct {
     int n_rl;
@@ -734,32 +749,90 @@ void oracle_solver_free(oracle_solver *o)
     free(o);
 }
 
-/* One Newton solve in place on x (mode/target may be changed only by the caller). Returns the status. */
+/* The linear-solve residual ratio of a solve J dx = -F (linResidScoreBatch, iterative_refinement.cu:42-65):
+ * max |J dx + F| / max |F|, 1e300 when F is zero or the residual is not finite. */
+static double solve_ratio(const oracle_structure *s, const double *vals, const double *dx, const double *F)
+{
+    double mr = 0.0, mf = 0.0;
+    int finite = 1;
+    for (int r = 0; r < s->n; r++) {
+        double acc = F[r];
+        for (int k = s->row_ptr[r]; k < s->row_ptr[r + 1]; k++) acc += vals[k] * dx[s->col_idx[k]];
+        if (!isfinite(acc)) finite = 0;
+        if (fabs(acc) > mr) mr = fabs(acc);
+        if (fabs(F[r]) > mf) mf = fabs(F[r]);
+    }
+    return (mf > 0.0 && finite) ? mr / mf : 1e300;
+}
+
+/* One Newton solve in place on x (mode/target may be changed only by the caller). Returns the status.
+ * newton_iteration.cu:276-397 with the linear-solve guard of :615-647: at least one iteration; the test at the budget is
+ * MAX_ITERATION_REACHED, or, when the solve before it did not solve its system (ratio above LIN_SOLVE_FAIL_RATIO),
+ * REJECTED in a batch and LINEAR_SOLVE_FAILED for a batch of one; the second iteration of a scenario's first solve
+ * (first_solve: no reactive-limit restart yet) ends LINEAR_SOLVE_FAILED when its solve fails the ratio; a singular
+ * factorization ends LINEAR_SOLVE_FAILED at the iteration that met it. */
 static int newton(const oracle_structure *s, glu *g, double *x, const double *target, const int *mode,
                   const unsigned char *dis, int max_iter, double tol, int *iters, double *norm_out, double *vals,
-                  double *ax, double *F, double *dx, double *qbuf)
+                  double *ax, double *F, double *dx, double *qbuf, int first_solve, int batch_of_one,
+                  const oracle_opts *op)
 {
     const int n = s->n;
+    const double thr2 = (op && op->conv_eps_per_eq > 0.0) ? sqrt(op->conv_eps_per_eq * op->conv_eps_per_eq * n) : 0.0;
+    double last_ratio = 0.0;
     for (int it = 0;; it++) {
         fill(s, x, target, mode, dis, vals, F, qbuf);
-        double nrm = 0.0;
+        double nrm = 0.0, ssq = 0.0;
         int finite = 1;
         for (int r = 0; r < n; r++) {
             if (!isfinite(F[r])) { finite = 0; break; }
             double a = fabs(F[r]);
             if (a > nrm) nrm = a;
+            ssq += F[r] * F[r];
         }
         *iters = it;
         *norm_out = finite ? nrm : NAN;
         if (!finite) return ST_DIVERGED;
-        if (it > 0 && nrm < tol && it < max_iter) return ST_CONVERGED;
-        if (it == max_iter) return ST_MAX_ITER;
+        int converged = thr2 > 0.0 ? sqrt(ssq) < thr2 : nrm < tol;
+        if (it > 0 && converged && it < max_iter) return ST_CONVERGED;
+        if (it == max_iter) {
+            if (!(last_ratio <= LIN_SOLVE_FAIL_RATIO)) return batch_of_one ? ST_LINEAR_SOLVE_FAILED : ST_REJECTED;
+            return ST_MAX_ITER;
+        }
         for (int k = 0; k < s->nnz; k++) ax[g->map[k]] = vals[k];
         if (glu_factor(g, ax) != 0) return ST_LINEAR_SOLVE_FAILED;
         for (int r = 0; r < n; r++) dx[r] = -F[r];
         glu_solve(g, dx, dx);
-        for (int r = 0; r < n; r++) x[r] += dx[r];
+        const int guard = first_solve && it == 1, budget = it == max_iter - 1;
+        if (guard || budget) {
+            double ratio = solve_ratio(s, vals, dx, F);
+            if (budget) last_ratio = ratio;
+            if (guard && !(ratio <= LIN_SOLVE_FAIL_RATIO)) return ST_LINEAR_SOLVE_FAILED;
+        }
+        double f = 1.0;
+        if (op && op->svs_mode == 2) {
+            /* MAX_VOLTAGE_CHANGE: the whole step scaled so max |dV| <= max_dv and max |dphi| <= max_dphi */
+            double mdv = 0.0, mdphi = 0.0;
+            for (int r = 0; r < n; r++) {
+                double a = fabs(dx[r]);
+                if (op->var_type[r] == 0) mdv = fmax(mdv, a);
+                else if (op->var_type[r] == 1) mdphi = fmax(mdphi, a);
+            }
+            if (mdv > op->max_dv) f = fmin(f, op->max_dv / mdv);
+            if (mdphi > op->max_dphi) f = fmin(f, op->max_dphi / mdphi);
+            for (int r = 0; r < n; r++) x[r] += f * dx[r];
+        } else {
+            for (int r = 0; r < n; r++) x[r] += dx[r];
+        }
     }
+}
+
+/* realistic_voltage_check.cu:23-44: a checked voltage outside [min_v, max_v] */
+static int unrealistic(const oracle_opts *op, int n, const double *x)
+{
+    if (!op || !op->v_check) return 0;
+    for (int r = 0; r < n; r++)
+        if (op->v_check[r] && (x[r] < op->min_v || x[r] > op->max_v)) return 1;
+    return 0;
 }
 
 /* reactive_limits.cu:321-359 (local controllers) + reactive_limits.cu:417-448 (forced-PV election).
@@ -822,9 +895,10 @@ static int reactive_limits_check(const oracle_rl *rl, int n, const double *x, co
  * out: per scenario [x(n), iterations, ||F||inf, status] (batch_solve_jni.cu:308-337).
  * Reactive limits: rl may be NULL; max_outer bounds the Newton restarts.  Returns 0.
  */
-int oracle_solve_batch(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
-                       const int *mode_base, const unsigned char *disabled, int n_elements, int max_iter, double tol,
-                       const oracle_rl *rl, double rl_tol, int max_outer, int max_switch, int threads, double *out)
+int oracle_solve_batch_ex(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
+                          const int *mode_base, const unsigned char *disabled, int n_elements, int max_iter, double tol,
+                          const oracle_rl *rl, double rl_tol, int max_outer, int max_switch, int threads,
+                          const oracle_opts *opts, double *out)
 {
     const oracle_structure *s = o->s;
     const int n = s->n;
@@ -858,11 +932,13 @@ int oracle_solve_batch(oracle_solver *o, int ns, const double *x0, int x0_stride
             int iters = 0, total = 0, status = ST_CONVERGED;
             double nrm = 0.0;
             for (int outer = 0;; outer++) {
-                status = newton(s, g, x, target, mode, dis, max_iter, tol, &iters, &nrm, vals, ax, F, dx, qbuf);
+                status = newton(s, g, x, target, mode, dis, max_iter, tol, &iters, &nrm, vals, ax, F, dx, qbuf,
+                                outer == 0, ns == 1, opts);
                 total += iters;
                 if (status != ST_CONVERGED || nrl == 0 || outer >= max_outer) break;
                 if (!reactive_limits_check(rl, n, x, qbuf, mode, target, lt, sc, ps, sm, st, rl_tol, max_switch)) break;
             }
+            if (status == ST_CONVERGED && unrealistic(opts, n, x)) status = ST_UNREALISTIC;
             x[n] = (double)total;
             x[n + 1] = nrm;
             x[n + 2] = (double)status;
@@ -872,6 +948,14 @@ int oracle_solve_batch(oracle_solver *o, int ns, const double *x0, int x0_stride
         free(lt); free(sc); free(ps); free(sm); free(st);
     }
     return 0;
+}
+
+int oracle_solve_batch(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
+                       const int *mode_base, const unsigned char *disabled, int n_elements, int max_iter, double tol,
+                       const oracle_rl *rl, double rl_tol, int max_outer, int max_switch, int threads, double *out)
+{
+    return oracle_solve_batch_ex(o, ns, x0, x0_stride, target_base, mode_base, disabled, n_elements, max_iter, tol, rl,
+                                 rl_tol, max_outer, max_switch, threads, NULL, out);
 }
 
 /* Solve one linear system J z = b with the oracle LU (tests of the engine's batched LU). Returns 0 or -1. */

@@ -22,11 +22,22 @@ _ip = ctypes.POINTER(ctypes.c_int)
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 
 
+def reference_root(reference: Optional[str] = None) -> Optional[str]:
+    """Where the reference sources lie: the argument, else $OLF_REFERENCE, else the default the recipe in
+    ``oracle/ref/Makefile`` names; None when no reference tree is there (the glue is then not built)."""
+    ref = reference or os.environ.get("OLF_REFERENCE")
+    if not ref:
+        out = subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), "print-ref"], capture_output=True,
+                             text=True)
+        ref = out.stdout.strip() if out.returncode == 0 else ""
+    return ref if ref and os.path.isdir(os.path.join(ref, "native", "cuda")) else None
+
+
 def build(reference: Optional[str] = None) -> None:
     """Compile the oracle (and, when the reference sources are present, the reference glue)."""
     subprocess.check_call(["make", "-s", "-C", HERE])
-    ref = reference or "/root/reference"
-    if os.path.isdir(os.path.join(ref, "native", "cuda")):
+    ref = reference_root(reference)
+    if ref:
         subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "ref"), f"REF={ref}"])
 
 
@@ -67,6 +78,7 @@ def lib():
         L.oracle_solve_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_int, _dp, _ip, _u8p, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int, _dp]
+        L.oracle_solve_batch_ex.argtypes = L.oracle_solve_batch.argtypes[:-1] + [ctypes.c_void_p, _dp]
         L.oracle_linear_solve.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
         L.oracle_closed_branch.argtypes = [_dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                            ctypes.c_double, ctypes.c_double, _dp]
@@ -79,6 +91,12 @@ def lib():
 class _Rl(ctypes.Structure):
     _fields_ = [("n_rl", ctypes.c_int), ("voltage_row", _ip), ("min_q", _dp), ("max_q", _dp), ("load_q", _dp),
                 ("target_v", _dp), ("nom_v", _dp), ("static_p", _dp), ("p_row", _ip), ("id_rank", _ip)]
+
+
+class _Opts(ctypes.Structure):
+    _fields_ = [("conv_eps_per_eq", ctypes.c_double), ("svs_mode", ctypes.c_int), ("max_dv", ctypes.c_double),
+                ("max_dphi", ctypes.c_double), ("var_type", _ip), ("v_check", _u8p), ("min_v", ctypes.c_double),
+                ("max_v", ctypes.c_double)]
 
 
 class Structure:
@@ -141,8 +159,11 @@ class Structure:
         return z
 
     def solve_batch(self, x0, disabled, max_iter=15, tol=1e-8, target=None, mode=None, reactive_limits=False,
-                    rl_tol=1e-4, max_outer=20, max_switch=3, threads=0):
-        """Per scenario [x(n), iterations, ||F||inf, status]; x0 is [n] (shared) or [nS, n]."""
+                    rl_tol=1e-4, max_outer=20, max_switch=3, threads=0, conv_eps_per_eq=0.0, svs_mode=0,
+                    max_dv=0.1, max_dphi=0.17453292519943295, var_type=None, v_check=None, min_v=0.0, max_v=0.0):
+        """Per scenario [x(n), iterations, ||F||inf, status]; x0 is [n] (shared) or [nS, n].  conv_eps_per_eq > 0:
+        OLF's 2-norm stopping test; svs_mode 2: MAX_VOLTAGE_CHANGE with var_type [n]; v_check [n]: the realistic-voltage
+        rows checked against [min_v, max_v] at convergence."""
         p = self.p
         disabled = _arr(disabled, np.uint8)
         ns = disabled.shape[0]
@@ -160,10 +181,15 @@ class Structure:
             k = self._rl_keep
             rl_struct = _Rl(k[0].shape[0], _ptr(k[0]), _ptr(k[1]), _ptr(k[2]), _ptr(k[3]), _ptr(k[4]), _ptr(k[5]),
                             _ptr(k[6]), _ptr(k[7]), _ptr(k[8]))
-        lib().oracle_solve_batch(self.solver, ns, _ptr(x0), stride, _ptr(target), _ptr(mode), _ptr(disabled),
-                                 disabled.shape[1], max_iter, tol,
-                                 ctypes.cast(ctypes.pointer(rl_struct), ctypes.c_void_p) if rl_struct else None,
-                                 rl_tol, max_outer, max_switch, threads, _ptr(out))
+        vt = None if var_type is None else _arr(var_type, np.int32)
+        vc = None if v_check is None else _arr(v_check, np.uint8)
+        opts = _Opts(conv_eps_per_eq, svs_mode, max_dv, max_dphi, None if vt is None else _ptr(vt),
+                     None if vc is None else _ptr(vc), min_v, max_v)
+        lib().oracle_solve_batch_ex(self.solver, ns, _ptr(x0), stride, _ptr(target), _ptr(mode), _ptr(disabled),
+                                    disabled.shape[1], max_iter, tol,
+                                    ctypes.cast(ctypes.pointer(rl_struct), ctypes.c_void_p) if rl_struct else None,
+                                    rl_tol, max_outer, max_switch, threads,
+                                    ctypes.cast(ctypes.pointer(opts), ctypes.c_void_p), _ptr(out))
         return out
 
 

@@ -110,7 +110,9 @@ def structures():
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else O.reference_root()
+    if not ref:
+        sys.exit("no reference tree: pass its path or set OLF_REFERENCE")
     O.build(ref)
     formulas(ref)
     structures()

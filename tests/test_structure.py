@@ -103,3 +103,18 @@ def test_plan_variants_shorten_the_dependency_chain(engine_lib):
     assert deferred.factor_levels < scaled.factor_levels
     assert dense.factor_levels < scaled.factor_levels
     assert scaled.n_lu_blocks == deferred.n_lu_blocks == dense.n_lu_blocks
+
+
+@pytest.mark.parametrize("name", ["grid2000", "grid9241", "grid13659"])
+@pytest.mark.parametrize("plan", [0, 16])
+def test_subtree_bins_keep_every_dependency(engine_lib, name, plan):
+    """The subtree bins of the wide levels (schedule 5): every LU block and every position scheduled exactly once
+    between the bins and the remaining level launches, and every block or solution entry a bin reads is produced
+    before it (same bin on an earlier level, or an earlier phase); the check runs in the library on the host."""
+    from olfgpu import native, packing, synthetic
+    g = synthetic.build(name)
+    s = native.Structure(packing.pack(g), ordering=plan)
+    st = s.subtrees()
+    assert st["bins"] > 0 and st["phases"] >= 1
+    assert st["bin_blocks"] > 0.7 * s.n_lu_blocks          # most of the factorization moves into the bins
+    assert st["max_bin_levels"] <= st["wide_levels"]

@@ -13,7 +13,8 @@ from conftest import grid
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-9   # the tolerance of the engine's FP64 linear-solve parity test
+# the tolerances of the engine's linear-solve parity test: FP64 factors, FP32 factors (relative to the FP64 answer)
+TOL = {0: 1e-9, 1: 2e-3}
 
 
 def _inputs(p, oracle_mod, ns, seed):
@@ -28,12 +29,15 @@ def _inputs(p, oracle_mod, ns, seed):
     return J, rhs
 
 
-def test_noalloc_solve_matches_the_allocating_solve(engine_lib, oracle_mod):
+@pytest.mark.parametrize("name,plan", [("grid118", 0), ("grid2000", 16)])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_noalloc_solve_matches_the_allocating_solve(engine_lib, oracle_mod, name, plan, precision):
+    """FP64 and FP32 factors, on the plain plan and on a dense-front plan (whose front runs in the scratch layout)."""
     import torch
     from olfgpu import native
-    g, p = grid("grid118")
-    ns = 40
-    s = native.Structure(p)
+    g, p = grid(name)
+    ns = 40 if name == "grid118" else 24
+    s = native.Structure(p, ordering=plan)
     ctx = native.BatchContext(s, ns)          # uploads the structure to this device (allocates, before the calls)
     dev = torch.device("cuda:0")
     J1, r1 = _inputs(p, oracle_mod, ns, 1)
@@ -45,7 +49,7 @@ def test_noalloc_solve_matches_the_allocating_solve(engine_lib, oracle_mod):
     results = []
     for k, (Jd, rd) in enumerate(((bufs[0], bufs[1]), (bufs[2], bufs[3]))):
         free_before = torch.cuda.mem_get_info(0)[0]
-        s.linear_solve_noalloc(ns, Jd.data_ptr(), rd.data_ptr(), out.data_ptr(), native.FP64, 0)
+        s.linear_solve_noalloc(ns, Jd.data_ptr(), rd.data_ptr(), out.data_ptr(), precision, 0)
         torch.cuda.synchronize()
         free_after = torch.cuda.mem_get_info(0)[0]
         if k == 1:
@@ -54,7 +58,12 @@ def test_noalloc_solve_matches_the_allocating_solve(engine_lib, oracle_mod):
     ref1 = ctx.debug_linear_solve(J1, r1, native.FP64)
     ref2 = ctx.debug_linear_solve(J2, r2, native.FP64)
     for got, ref in ((results[0], ref1), (results[1], ref2)):
-        assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < TOL
+        assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < TOL[precision]
+    if precision == 1:
+        # the same FP32 factors as the allocating entry point's FP32 solve
+        for got, (J, r) in ((results[0], (J1, r1)), (results[1], (J2, r2))):
+            ref32 = ctx.debug_linear_solve(J, r, native.MIXED)
+            assert np.max(np.abs(got - ref32)) / np.max(np.abs(ref32)) < 1e-5
     # the two calls solved different systems: the shared scratch did not leak the first into the second
     assert np.max(np.abs(results[0] - results[1])) > 1e-3
 
@@ -69,3 +78,32 @@ def test_noalloc_rejects_a_batch_beyond_its_scratch(engine_lib):
     dummy = torch.zeros(1, dtype=torch.float64, device="cuda:0")
     with pytest.raises(native.NativeError, match="scratch"):
         s.linear_solve_noalloc(big, dummy.data_ptr(), dummy.data_ptr(), dummy.data_ptr(), native.FP64, 0)
+
+
+def test_noalloc_marks_a_singular_system_with_nan(engine_lib, oracle_mod):
+    """A scenario whose factorization meets a singular pivot gets NaN throughout; the other scenarios are solved."""
+    import torch
+    from olfgpu import native
+    g, p = grid("grid118")
+    ns = 8
+    s = native.Structure(p)
+    ctx = native.BatchContext(s, ns)
+    J, r = _inputs(p, oracle_mod, ns, 3)
+    # zero the two rows and columns of one PQ bus in scenario 3: its 2x2 pivot is exactly singular
+    ex = s.export()
+    bus = int(np.flatnonzero(p.base_row_mode[0::2] == 1)[3])
+    rows = (2 * bus, 2 * bus + 1)
+    for k in range(ex["row_ptr"][rows[0]], ex["row_ptr"][rows[1] + 1]):
+        J[3, k] = 0.0
+    cols = np.isin(ex["col_idx"], rows)
+    J[3, cols] = 0.0
+    dev = torch.device("cuda:0")
+    Jd, rd = torch.from_numpy(J).to(dev), torch.from_numpy(r).to(dev)
+    out = torch.zeros((ns, p.n), dtype=torch.float64, device=dev)
+    s.linear_solve_noalloc(ns, Jd.data_ptr(), rd.data_ptr(), out.data_ptr(), native.FP64, 0)
+    got = out.cpu().numpy()
+    assert np.all(np.isnan(got[3]))
+    keep = [k for k in range(ns) if k != 3]
+    ref = ctx.debug_linear_solve(J[keep[:1] * ns], r[keep[:1] * ns], native.FP64)[0]
+    assert np.all(np.isfinite(got[keep]))
+    assert np.max(np.abs(got[keep[0]] - ref)) / np.max(np.abs(ref)) < TOL[0]
