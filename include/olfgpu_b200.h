@@ -130,8 +130,14 @@ int olfgpu_create_batch_context(int64_t structure, int nScenarios, int mode, int
  * target V; all of one length) are installed without their forced-PV election keys, which
  * olfgpu_set_reactive_limit_strongest_pv_keys supplies before the first solve (a solve with entries but no keys
  * fails, as batch_solve_jni.cu:103-111 does).  reactiveLimitFlags must be 0 (voltage-monitoring SVCs are not
- * modelled), rowSlope zero (no voltage slope), and the distributed-slack tables empty; slackBusPhiRow,
- * slackBusTargetP, the factor mode and the margins only concern distributed slack and are ignored.
+ * modelled) and rowSlope zero (no voltage slope).  Distributed slack (outerloop/distributed_slack.cu:211-616, bus
+ * level): the participants' P rows, factors (STATIC mode 0; normalised to sum 1), base targets and the bounds of their
+ * move (maxDelta >= 0 >= minDelta), the slack bus's angle row and net P target; after a scenario converges, a slack
+ * mismatch (its closed-branch P minus the target) above solveBatchContext's slackDistTol is water-filled over the
+ * participants from their base targets and the scenario re-solves, before its reactive-limit check; a distribution
+ * that leaves more than 1e-5 pu unplaced ends the scenario REJECTED when rejectSlackDistributionFailure is set, else
+ * the rest stays on the slack.  The REMAINING_MARGIN mode (1) and its margins are rejected.
+ * olfgpu_last_slack_distribution_failures writes per scenario 1 where the last solve's distribution failed.
  */
 int olfgpu_create_batch_context_full(
     int64_t structure, int nScenarios, int mode, const int* rlVoltageRow, int rlVoltageRowLength,
@@ -143,6 +149,8 @@ int olfgpu_create_batch_context_full(
     const double* dsBusMinDelta, int dsBusMinDeltaLength, int dsFactorMode, const double* dsBusMarginUp,
     int dsBusMarginUpLength, const double* dsBusMarginDown, int dsBusMarginDownLength, double slackBusMarginUp,
     double slackBusMarginDown, int64_t* contextOut);
+
+int olfgpu_last_slack_distribution_failures(int64_t context, unsigned char* failed, int* count);
 
 /* ReactiveLimitsNative.setBatchReactiveLimitStrongestPvKeys (reactive_limits_jni.cu:118-145): per reactive-limit
  * entry its nominal V, P row (-1: static P), static P and id rank; count must equal the entries. */
@@ -164,8 +172,8 @@ int olfgpu_set_states_to_host(int64_t context, int statesToHost);
 int olfgpu_states_to_host(int64_t context, int* statesToHost);
 int olfgpu_read_batch_states(int64_t context, int nSlots, const int* slots, double* out);
 
-/* DriverNative.setBatchOuterLoops (driver_jni.cu:11-18): the reactive-limit outer loop on or off for the following
- * solves; the distributed-slack outer loop is not available (enabling it fails). */
+/* DriverNative.setBatchOuterLoops (driver_jni.cu:11-18): the distributed-slack and reactive-limit outer loops on or off
+ * for the following solves (each acts only where the context holds its tables). */
 int olfgpu_set_outer_loops(int64_t context, int distributedSlack, int reactiveLimits);
 
 /* A context's sizes and counters: n, elements, bank size, scenarios the next full solve installs, batched Newton
@@ -199,6 +207,13 @@ int olfgpu_set_linear_solver_settings(int64_t context, int precision, int refine
  * flagged it (flagged [nScenarios], may be null) and their count.
  */
 int olfgpu_set_mixed_precision_controls(int64_t context, double refineBelow, double growthLimit);
+/* Mixed-precision policy (level and cooperative schedules): 0 (default) refines, as above; 1 runs an iteration in which
+ * some factorizing scenario's max |F| is below refineBelow in FP64 for all its scenarios (factorization and solves),
+ * and the other iterations in FP32 without refinement, so the last steps follow the FP64 trajectory at the cost of an
+ * FP64 factorization instead of refinement solves.  olfgpu_last_fp64_iterations reads how many iterations of the last
+ * solve ran in FP64 under policy 1. */
+int olfgpu_set_mixed_precision_policy(int64_t context, int policy);
+int olfgpu_last_fp64_iterations(int64_t context, int* iterations);
 int olfgpu_last_fp64_refactors(int64_t context, unsigned char* flagged, int* count);
 
 /*
@@ -249,11 +264,12 @@ int olfgpu_solve_batch_context(int64_t context, const double* x0Base, const doub
  *     state_vector_scaling.cu:53-97); 1 LINE_SEARCH is rejected;
  *   skipReactiveLimitsPhase != 0: this solve runs without the reactive-limit outer loop;
  *   x0PerScenario [nScenarios * n] (the reference's x0Full).
+ * slackDistTol and rejectSlackDistributionFailure drive the distributed-slack outer loop (olfgpu_create_batch_context_full).
  * Rejected with an error naming the argument when non-empty (families this engine does not model): the distributed-
  * slack overrides and anchor shifts, the reactive-limit target-V / delta / capability-curve overrides, the shunt and
  * closed-branch parameter overrides, the reactive-limit seed state, the zero-impedance branch lists (and
- * nBaseClosedZeroImpedanceBranches != 0), and pauseAtEnded != 0.  slackDistTol and rejectSlackDistributionFailure
- * only concern distributed slack and are accepted and ignored.  out [nScenarios][n + 3] as olfgpu_solve_batch_context.
+ * nBaseClosedZeroImpedanceBranches != 0), and pauseAtEnded != 0.  out [nScenarios][n + 3] as
+ * olfgpu_solve_batch_context.
  */
 int olfgpu_solve_batch_context_full(
     int64_t context, const double* x0Base, int x0BaseLength, const double* targetBase, int targetBaseLength,
@@ -338,6 +354,12 @@ int olfgpu_set_device_start(int64_t context, const double* x0FullDevice);
  * (may be null), and the count of non-zero entries.
  */
 int olfgpu_set_fallback_start(int64_t context, int enable);
+/* Fallback mode: a scenario that converged from its own x0Full row with max |F| above polishRatio * tol (default
+ * 1e-2; 0 switches it off) takes one more Newton step.  A state that met the tolerance may lie anywhere in its ball
+ * (on a 9,241-bus grid up to 1.5e-8 from the solution at max |F| just under 1e-8), so a scenario that converged from
+ * another start than the reference's base start is brought next to the solution, where the base-start trajectory's
+ * converged state also lies.  Its iteration count includes the step. */
+int olfgpu_set_start_polish(int64_t context, double polishRatio);
 int olfgpu_last_fallbacks(int64_t context, unsigned char* fellBack, int* count);
 
 /*
@@ -375,6 +397,34 @@ int olfgpu_solve_multi_context(int64_t multi, double* const* outs, float* device
 int olfgpu_debug_fill(int64_t context, const double* xFull, const double* targetBase, const int* baseRowMode,
                       const unsigned char* disabled, double* jacobianOut, double* mismatchOut);
 int olfgpu_debug_linear_solve(int64_t context, const double* csrVals, const double* rhs, int precision, double* out);
+
+/*
+ * Post-contingency violation screening of the context's last solve on the device (sa/olf_gpu_violations.cu:160-361;
+ * GpuViolationScreen.java).  Branch limits: nElem limited elements (elemId: closed branch e, or open branch nCb + e),
+ * each with the limit groups [groupPtr[r], groupPtr[r + 1]) (groupSide 1 / 2; groupQty 0 current I = hypot(p, q) / v,
+ * 1 active power |P|, 2 apparent power S), each group with thresholds limThreshold[limPtr[g] .. limPtr[g + 1]) in the
+ * order the caller reports them.  Bus limits: busVRow (-1 none), busHigh / busLow (NaN: no limit); realistic != 0 also
+ * flags the buses outside [minV, maxV].  A limit is a candidate once its value exceeds the threshold relaxed by band
+ * (relative); a group's later thresholds stop being candidates once one is exceeded beyond the band; an outaged branch
+ * yields nothing.  records [nScenarios][capacity] receives each scenario's candidate ids, sorted (branch limit l: l;
+ * bus i high: nLimits + 2i, low: nLimits + 2i + 1, realistic: nLimits + 2 nBus + i), counts [nScenarios] their count
+ * (above capacity: truncated).  The host re-tests candidates exactly; the screen never decides.
+ */
+int olfgpu_screen_violations(int64_t context, int nElem, const int* elemId, const int* groupPtr, const int* groupSide,
+                             const int* groupQty, const int* limPtr, const double* limThreshold, int nBus,
+                             const int* busVRow, const double* busHigh, const double* busLow, int realistic,
+                             double minV, double maxV, double band, int capacity, int* records, int* counts);
+
+/*
+ * BatchedLuNative.factorizeAndSolveTransposed (BatchedLuNative.java:121-125; lu/transposed_solve.cuh:1-30): one block-LU
+ * factorization of each scenario's J (csrVals [nScenarios][nnz], the reference-compatible CSR layout), then both
+ * J x = rhs and the transposed (adjoint) system J^T y = rhsTransposed on the same factors, the latter as two more
+ * triangular sweeps (U^T forward, L^T backward).  rhs / rhsTransposed and solution / solutionTransposed are
+ * [nScenarios][n]; a null right-hand side skips its solve.  precision 0 FP64, 1 FP32 factors.
+ */
+int olfgpu_linear_solve_transposed(int64_t context, const double* csrVals, const double* rhs,
+                                   const double* rhsTransposed, int precision, double* solution,
+                                   double* solutionTransposed);
 
 /*
  * Learned warm start (no counterpart in the reference): kernels of a message-passing graph network over the bus

@@ -13,7 +13,8 @@ LIB = os.path.join(OUT, "libolfgpu_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-Xptxas", "-O3"]
-SOURCES = ["structure.cpp", "kernels.cu", "persistent.cu", "coop.cu", "front.cu", "region.cu", "engine.cu", "noalloc.cu", "gnn.cu", "capi.cu"]
+SOURCES = ["structure.cpp", "kernels.cu", "persistent.cu", "coop.cu", "front.cu", "region.cu", "engine.cu", "noalloc.cu", "gnn.cu", "violations.cu",
+           "capi.cu"]
 
 
 def _compile(src: str, verbose: bool) -> str:

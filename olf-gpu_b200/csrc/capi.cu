@@ -336,24 +336,43 @@ extern "C" int olfgpu_create_batch_context_full(
                                          " is not supported by this engine");
             }
         }
-        (void)dsBusPhiRow; (void)dsBusFactor; (void)slackBusPhiRow; (void)slackBusTargetP; (void)dsBusBaseTargetP;
-        (void)dsBusMaxDelta; (void)dsBusMinDelta; (void)dsFactorMode; (void)dsBusMarginUp; (void)dsBusMarginDown;
-        (void)slackBusMarginUp; (void)slackBusMarginDown;
-        const std::pair<const char*, int> ds[] = {
-            {"distributedSlackBusPhiRow", dsBusPhiRowLength}, {"distributedSlackBusFactor", dsBusFactorLength},
-            {"distributedSlackBusBaseTargetP", dsBusBaseTargetPLength},
-            {"distributedSlackBusMaxDelta", dsBusMaxDeltaLength}, {"distributedSlackBusMinDelta", dsBusMinDeltaLength},
-            {"distributedSlackBusMarginUp", dsBusMarginUpLength},
-            {"distributedSlackBusMarginDown", dsBusMarginDownLength}};
-        for (const auto& e : ds) {
-            if (e.second != 0) {
-                throw std::runtime_error(std::string("createBatchContext: ") + e.first +
-                                         " (distributed slack) is not supported by this engine");
-            }
+        // distributed slack: bus-level participants with static factors (GpuDistributedSlackFactorMode STATIC 0);
+        // the REMAINING_MARGIN mode and its margins are not modelled
+        (void)dsBusMarginUp; (void)dsBusMarginDown; (void)slackBusMarginUp; (void)slackBusMarginDown;
+        const int nDs = dsBusPhiRowLength;
+        if (dsBusFactorLength != nDs || dsBusBaseTargetPLength != nDs || dsBusMaxDeltaLength != nDs ||
+            dsBusMinDeltaLength != nDs) {
+            throw std::runtime_error("createBatchContext: distributed-slack arrays differ in length");
         }
-        BatchContext* c = createContext(structureOf(structure), nScenarios, mode, nRl, rlVoltageRow, rlMinQ, rlMaxQ,
-                                        rlLoadQ, rlTargetV, nullptr, nullptr, nullptr, nullptr);
-        *contextOut = reinterpret_cast<int64_t>(c);
+        if (nDs > 0 && dsFactorMode != 0) {
+            throw std::runtime_error("createBatchContext: distributed-slack factor mode " + std::to_string(dsFactorMode) +
+                                     " (REMAINING_MARGIN) is not supported by this engine");
+        }
+        if (dsBusMarginUpLength != 0 || dsBusMarginDownLength != 0) {
+            if (dsFactorMode != 0) throw std::runtime_error("createBatchContext: margins are not supported");
+        }
+        std::unique_ptr<BatchContext> c(createContext(structureOf(structure), nScenarios, mode, nRl, rlVoltageRow, rlMinQ,
+                                                      rlMaxQ, rlLoadQ, rlTargetV, nullptr, nullptr, nullptr, nullptr));
+        if (nDs > 0) {
+            setDistributedSlack(*c, nDs, dsBusPhiRow, dsBusFactor, dsBusBaseTargetP, dsBusMaxDelta, dsBusMinDelta,
+                                slackBusPhiRow, slackBusTargetP);
+        }
+        *contextOut = reinterpret_cast<int64_t>(c.release());
+    });
+}
+
+extern "C" int olfgpu_last_slack_distribution_failures(int64_t context, unsigned char* failed, int* count) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        std::vector<unsigned char> f(c.nS, 0);
+        if (c.ds.nDs > 0) {
+            OLF_CUDA(cudaSetDevice(c.device));
+            OLF_CUDA(cudaMemcpy(f.data(), c.dsFailed.p, c.nS, cudaMemcpyDeviceToHost));
+        }
+        int k = 0;
+        for (int i = 0; i < c.nS; i++) k += f[i] ? 1 : 0;
+        if (failed) std::memcpy(failed, f.data(), c.nS);
+        if (count) *count = k;
     });
 }
 
@@ -503,7 +522,7 @@ extern "C" int olfgpu_solve_batch_context_full(
         (void)shuntOvSlotElem; (void)shuntOvGb; (void)reactiveLimitsSeedState;
         (void)closedBranchParameterOverrideScenarioElement; (void)closedBranchParameterOverrideValues;
         (void)zeroImpedanceBranchCloseScenarioElement; (void)zeroImpedanceBranchOpenScenarioElement;
-        (void)slackDistTol; (void)rejectSlackDistributionFailure;
+
         const std::pair<const char*, int> unsupported[] = {
             {"distributedSlackOverrideBus", distributedSlackOverrideBusLength},
             {"distributedSlackOverrideFactorDelta", distributedSlackOverrideFactorDeltaLength},
@@ -622,6 +641,8 @@ extern "C" int olfgpu_solve_batch_context_full(
         r.maxDphi = maxDphi;
         r.varType = varType;
         r.skipReactiveLimits = skipReactiveLimitsPhase != 0;
+        r.slackDistTol = slackDistTol;
+        r.rejectDsFailure = rejectSlackDistributionFailure != 0;
         r.laneLive = live.empty() ? nullptr : live.data();
         c.solveCount++;
         c.handedBack.resize(nLocal);
@@ -711,7 +732,7 @@ extern "C" int olfgpu_read_batch_states(int64_t context, int nSlots, const int* 
 extern "C" int olfgpu_set_outer_loops(int64_t context, int distributedSlack, int reactiveLimits) {
     return guarded([&] {
         BatchContext& c = contextOf(context);
-        if (distributedSlack) throw std::runtime_error("the distributed-slack outer loop is not available");
+        c.dsLoop = distributedSlack != 0;
         c.reactiveLimitsLoop = reactiveLimits != 0;
     });
 }
@@ -742,6 +763,13 @@ extern "C" int olfgpu_set_refinement_bound(int64_t context, double correctionBou
     });
 }
 
+extern "C" int olfgpu_set_start_polish(int64_t context, double polishRatio) {
+    return guarded([&] {
+        if (!(polishRatio >= 0 && polishRatio <= 1)) throw std::runtime_error("polishRatio must lie in [0, 1]");
+        contextOf(context).polishRatio = polishRatio;
+    });
+}
+
 extern "C" int olfgpu_set_fp64_restart(int64_t context, int enable) {
     return guarded([&] { contextOf(context).fp64Restart = enable != 0; });
 }
@@ -757,6 +785,22 @@ extern "C" int olfgpu_last_phase_times(int64_t context, double* out8) {
         for (int i = 0; i < 6; i++) out8[i] = c.phaseMs[i];
         out8[6] = static_cast<double>(c.phaseIterations);
         out8[7] = static_cast<double>(c.phaseLanes);
+    });
+}
+
+extern "C" int olfgpu_set_mixed_precision_policy(int64_t context, int policy) {
+    return guarded([&] {
+        if (policy != MIXED_REFINE && policy != MIXED_FP64_NEAR) {
+            throw std::runtime_error("mixed-precision policy " + std::to_string(policy) + " unknown (0 or 1)");
+        }
+        contextOf(context).mixedPolicy = policy;
+    });
+}
+
+extern "C" int olfgpu_last_fp64_iterations(int64_t context, int* iterations) {
+    return guarded([&] {
+        if (!iterations) throw std::runtime_error("null output");
+        *iterations = contextOf(context).fp64Iterations;
     });
 }
 
@@ -915,6 +959,46 @@ extern "C" int olfgpu_debug_fill(int64_t context, const double* xFull, const dou
 extern "C" int olfgpu_debug_linear_solve(int64_t context, const double* csrVals, const double* rhs, int precision,
                                          double* out) {
     return guarded([&] { debugLinearSolve(contextOf(context), csrVals, rhs, precision, out); });
+}
+
+extern "C" int olfgpu_screen_violations(int64_t context, int nElem, const int* elemId, const int* groupPtr,
+                                        const int* groupSide, const int* groupQty, const int* limPtr,
+                                        const double* limThreshold, int nBus, const int* busVRow,
+                                        const double* busHigh, const double* busLow, int realistic, double minV,
+                                        double maxV, double band, int capacity, int* records, int* counts) {
+    return guarded([&] {
+        if ((nElem > 0 && (!elemId || !groupPtr || !limPtr)) || (nBus > 0 && (!busVRow || !busHigh || !busLow))) {
+            throw std::runtime_error("null table with a non-zero count");
+        }
+        if (!(band >= 0.0)) throw std::runtime_error("band must be >= 0");
+        ViolationTables t;
+        t.nElem = nElem;
+        t.elemId = elemId;
+        t.groupPtr = groupPtr;
+        t.groupSide = groupSide;
+        t.groupQty = groupQty;
+        t.limPtr = limPtr;
+        t.limThreshold = limThreshold;
+        t.nBus = nBus;
+        t.busVRow = busVRow;
+        t.busHigh = busHigh;
+        t.busLow = busLow;
+        t.realistic = realistic;
+        t.minV = minV;
+        t.maxV = maxV;
+        t.band = band;
+        screenViolations(contextOf(context), t, capacity, records, counts);
+    });
+}
+
+extern "C" int olfgpu_linear_solve_transposed(int64_t context, const double* csrVals, const double* rhs,
+                                              const double* rhsTransposed, int precision, double* solution,
+                                              double* solutionTransposed) {
+    return guarded([&] {
+        if (precision != 0 && precision != 1) throw std::runtime_error("precision must be 0 (FP64) or 1 (FP32)");
+        if (!csrVals) throw std::runtime_error("null Jacobian values");
+        linearSolveBoth(contextOf(context), csrVals, rhs, rhsTransposed, precision, solution, solutionTransposed);
+    });
 }
 
 namespace olfb200 {

@@ -673,6 +673,29 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
         d->lrowSlot.upload(lrowSlot);
         d->uSlot.upload(uSlot);
     }
+    // the transposed solve's entries on the same factors: U^T has L's pattern (row i of U^T reads U(k, i) for every
+    // L(i, k)) and L^T has U's (row i of L^T reads L(j, i) for every U(i, j), j > i)
+    {
+        std::vector<int> lrowU(std::max<size_t>(lrow.size(), 1), 0), uRowL(std::max<size_t>(p.nU, 1), 0);
+        auto uBlockOf = [&](int k, int j) {
+            auto lo = p.uCol.begin() + p.uPtr[k] + 1, hi = p.uCol.begin() + p.uPtr[k + 1];
+            auto it = std::lower_bound(lo, hi, j);
+            if (it == hi || *it != j) throw std::runtime_error("transposed solve: U block lookup miss");
+            return static_cast<int>(it - p.uCol.begin());
+        };
+        auto lBlockOf = [&](int i, int k) {
+            auto lo = p.lRow.begin() + p.lPtr[k], hi = p.lRow.begin() + p.lPtr[k + 1];
+            auto it = std::lower_bound(lo, hi, i);
+            if (it == hi || *it != i) throw std::runtime_error("transposed solve: L block lookup miss");
+            return p.nU + static_cast<int>(it - p.lRow.begin());
+        };
+        for (int i = 0; i < nb; i++) {
+            for (int q = lrowPtr[i]; q < lrowPtr[i + 1]; q++) lrowU[q] = uBlockOf(lrow[q].y, i);
+            for (int q = p.uPtr[i] + 1; q < p.uPtr[i + 1]; q++) uRowL[q] = lBlockOf(p.uCol[q], i);
+        }
+        d->lrowU.upload(lrowU);
+        d->uRowL.upload(uRowL);
+    }
     d->bwdSplit.assign(p.bwdLevelPtr.size() - 1, 1);
     for (size_t l = 0; l + 1 < p.bwdLevelPtr.size(); l++) {
         int m = 0;
@@ -729,6 +752,8 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     v.iperm = d->iperm.as<int>();
     v.lrowPtr = d->lrowPtr.as<int>();
     v.lrowEnd = d->lrowEnd.as<int>();
+    v.lrowU = d->lrowU.as<int>();
+    v.uRowL = d->uRowL.as<int>();
     v.lrow = d->lrow.as<int2>();
     v.uPtr = d->uPtr.as<int>();
     v.uCol = d->uCol.as<int>();
@@ -816,6 +841,7 @@ DevBatch BatchContext::batch() const {
     b.varType = hasVarType ? varType.as<int8_t>() : nullptr;
     b.vCheck = hasVCheck ? vCheck.as<int8_t>() : nullptr;
     b.laneLive = hasLaneLive ? laneLive.as<int8_t>() : nullptr;
+    b.dsRestart = dsRestartBuf.as<int8_t>();
     return b;
 }
 
@@ -870,6 +896,7 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
     ctx->varType.alloc(n);
     ctx->vCheck.alloc(n);
     ctx->laneLive.alloc(S);
+    ctx->dsRestartBuf.alloc(S);
     ctx->nActive.alloc(8 * sizeof(int));
     ctx->out.alloc(static_cast<size_t>(nScenarios) * (n + 3) * 8);
     ctx->stage.alloc(n * 8 * 2 + n * 4);
@@ -882,6 +909,7 @@ BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, i
     ctx->cfg.growthLimit = ctx->growthLimit;
     ctx->cfg.refineBelow = ctx->refineBelow;
     ctx->cfg.corrBound = ctx->corrBound;
+    ctx->cfg.polishBelow = 0.0;
     ctx->cfg.batchOfOne = nScenarios == 1 ? 1 : 0;
     if (nRl > 0) {
         for (int i = 0; i < nRl; i++) {
@@ -1120,7 +1148,8 @@ void captureIteration(BatchContext& ctx) {
                     (ctx.subtrees ? 5000000 : 0) +
                     ctx.precision * 1000 +
                     ctx.refinementSteps * 10 +
-                    (ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits ? 1 : 0);
+                    (ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits ? 1 : 0) +
+                    (ctx.ds.nDs > 0 && ctx.cfg.distributedSlack ? 2 : 0);
     // the graphs bake the batch view (pointers, per-request flags) and the settings into their kernel parameters
     const DevBatch now = ctx.batch();
     if (ctx.graph && ctx.graphKey == key && std::memcmp(&now, &ctx.graphBatch, sizeof(DevBatch)) == 0 &&
@@ -1145,16 +1174,18 @@ void captureIteration(BatchContext& ctx) {
     const DevBatch b = ctx.batch();
     const Settings cfg = ctx.cfg;
     const bool rl = ctx.rl.nRl > 0 && cfg.reactiveLimits;
+    const bool dsOn = ctx.ds.nDs > 0 && cfg.distributedSlack;
     cudaStream_t st = ctx.stream;
     const Hybrid hy = ctx.hybrid();
     const Hybrid* hp = ctx.useHybrid() ? &hy : nullptr;
     const int nLevels = static_cast<int>(dn.levelPtr.size()) - 1;
-    // part 1: fill, test, reactive limits, lane counts
+    // part 1: fill, test, distributed slack, reactive limits, lane counts
     ctx.graph = captureInto(st, [&] {
         launchIterationStart(b, st);
-        launchFill(net, b, true, rl, st);
+        launchFill(net, b, true, rl || dsOn, st);
         if (cfg.norm2Threshold > 0.0) launchNorm2(net, b, st);
         launchTest(net, b, cfg, rl ? ctx.rl.remainingPv : nullptr, st);
+        if (dsOn) launchDistributedSlack(b, ctx.ds, cfg, st);
         if (rl) launchReactiveLimits(net, b, ctx.rl, cfg, st);
         launchCountSolving(b, mixed ? cfg.refineBelow : -1.0, cfg.maxIter, st);
     });
@@ -1262,6 +1293,12 @@ void refinementSteps(BatchContext& ctx, const DevBatch& b) {
 // The linear-solve scoring runs in an iteration where some lane is scored (the host read the count after the test).
 bool scoreDue(const BatchContext& ctx) { return ctx.hostActive[4] > 0; }
 
+// Mixed precision under MIXED_FP64_NEAR: an iteration in which some factorizing lane's max |F| is below refineBelow
+// (the count the host read after the test) runs in FP64 for all its lanes.
+bool fp64Iteration(const BatchContext& ctx) {
+    return ctx.precision == 1 && ctx.mixedPolicy == MIXED_FP64_NEAR && ctx.hostActive[2] > 0;
+}
+
 // One Newton iteration's factorization, solves, refinement, FP64 refactor and step with cooperative sweeps (the
 // cooperative launches are not captured in graphs).
 void coopIteration(BatchContext& ctx) {
@@ -1269,6 +1306,16 @@ void coopIteration(BatchContext& ctx) {
     const bool mixed = ctx.precision == 1;
     cudaStream_t st = ctx.stream;
     const DevBatch b = ctx.batch();
+    if (fp64Iteration(ctx)) {
+        ctx.fp64Iterations++;
+        launchPromoteFp64(b, st);
+        const DevBatch b64 = fp64View(ctx);
+        factorPhase(ctx, b64, false);
+        solvePhase(ctx, b64, false, false);
+        if (scoreDue(ctx)) launchScoreSolve(dn.view, b, ctx.cfg, st);
+        launchStep(dn.view, b, ctx.cfg, st);
+        return;
+    }
     factorPhase(ctx, b, mixed);
     if (mixed) {
         launchCountFp64(b, st);
@@ -1295,16 +1342,18 @@ bool phaseTimedIteration(BatchContext& ctx) {
     const DevNet& net = dn.view;
     const bool mixed = ctx.precision == 1;
     const bool rl = ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits;
+    const bool dsOn = ctx.ds.nDs > 0 && ctx.cfg.distributedSlack;
     const DevBatch b = ctx.batch();
     cudaStream_t st = ctx.stream;
     cudaEvent_t ev[7];
     for (auto& e : ev) OLF_CUDA(cudaEventCreate(&e));
     OLF_CUDA(cudaEventRecord(ev[0], st));
     launchIterationStart(b, st);
-    launchFill(net, b, true, rl, st);
+    launchFill(net, b, true, rl || dsOn, st);
     OLF_CUDA(cudaEventRecord(ev[1], st));
     if (ctx.cfg.norm2Threshold > 0.0) launchNorm2(net, b, st);
     launchTest(net, b, ctx.cfg, rl ? ctx.rl.remainingPv : nullptr, st);
+    if (dsOn) launchDistributedSlack(b, ctx.ds, ctx.cfg, st);
     if (rl) launchReactiveLimits(net, b, ctx.rl, ctx.cfg, st);
     launchCountSolving(b, mixed ? ctx.cfg.refineBelow : -1.0, ctx.cfg.maxIter, st);
     OLF_CUDA(cudaEventRecord(ev[2], st));
@@ -1315,7 +1364,23 @@ bool phaseTimedIteration(BatchContext& ctx) {
     OLF_CUDA(cudaEventElapsedTime(&ms[1], ev[1], ev[2]));
     const bool live = ctx.hostActive[0] > 0;
     const int solving = ctx.hostActive[1];
-    if (live && solving > 0) {
+    if (live && solving > 0 && fp64Iteration(ctx)) {
+        OLF_CUDA(cudaEventRecord(ev[2], st));
+        launchPromoteFp64(b, st);
+        const DevBatch b64 = fp64View(ctx);
+        factorPhase(ctx, b64, false);
+        OLF_CUDA(cudaEventRecord(ev[3], st));
+        solvePhase(ctx, b64, false, false);
+        OLF_CUDA(cudaEventRecord(ev[4], st));
+        if (scoreDue(ctx)) launchScoreSolve(net, b, ctx.cfg, st);
+        OLF_CUDA(cudaEventRecord(ev[5], st));
+        launchStep(net, b, ctx.cfg, st);
+        OLF_CUDA(cudaEventRecord(ev[6], st));
+        OLF_CUDA(cudaEventSynchronize(ev[6]));
+        for (int i = 2; i < 6; i++) OLF_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+        ctx.phaseLanes += solving;
+        ctx.fp64Iterations++;
+    } else if (live && solving > 0) {
         OLF_CUDA(cudaEventRecord(ev[2], st));
         factorPhase(ctx, b, mixed);
         if (mixed) launchCountFp64(b, st);
@@ -1400,7 +1465,8 @@ void uploadInputs(BatchContext& ctx, const SolveRequest& req) {
 void installLanes(BatchContext& ctx) {
     // mixed precision: a failed lane restarts once in FP64 (the persistent tiles: with every solve refined to the
     // correction bound); not with reactive limits, whose restarts carry the outer loop's state
-    ctx.fp64RestartOn = ctx.precision == 1 && ctx.fp64Restart && !(ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits);
+    ctx.fp64RestartOn = ctx.precision == 1 && ctx.fp64Restart && !(ctx.rl.nRl > 0 && ctx.cfg.reactiveLimits) &&
+                        !(ctx.ds.nDs > 0 && ctx.cfg.distributedSlack);
     const int n = ctx.net->host.n;
     const size_t S = ctx.S;
     cudaStream_t st = ctx.stream;
@@ -1426,6 +1492,8 @@ void installLanes(BatchContext& ctx) {
     }
     OLF_CUDA(cudaMemsetAsync(ctx.nActive.p, 0, sizeof(int), st));
     laneInitKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(ctx.batch());
+    if (ctx.ds.nDs > 0) OLF_CUDA(cudaMemsetAsync(ctx.dsFailed.p, 0, ctx.dsFailed.bytes, st));
+    OLF_CUDA(cudaMemsetAsync(ctx.dsRestartBuf.p, 0, ctx.dsRestartBuf.bytes, st));
     if (ctx.rl.nRl > 0) {
         OLF_CUDA(cudaMemsetAsync(ctx.rlLimitType.p, 0, ctx.rlLimitType.bytes, st));
         OLF_CUDA(cudaMemsetAsync(ctx.rlSwitchCount.p, 0, ctx.rlSwitchCount.bytes, st));
@@ -1436,7 +1504,8 @@ void installLanes(BatchContext& ctx) {
 int roundCap(const BatchContext& ctx) {
     // a fallback restart and an FP64 restart each add one solve
     const int solves = 1 + (ctx.fallbackStart && ctx.hasX0Base && ctx.hasX0Full ? 1 : 0) + (ctx.fp64RestartOn ? 1 : 0);
-    return ctx.cfg.reactiveLimits ? (ctx.cfg.maxOuter + 1) * (ctx.cfg.maxIter + 1) : solves * (ctx.cfg.maxIter + 1);
+    return ctx.cfg.reactiveLimits || ctx.cfg.distributedSlack ? (ctx.cfg.maxOuter + 1) * (ctx.cfg.maxIter + 1)
+                                                                : solves * (ctx.cfg.maxIter + 1);
 }
 
 // The Newton iterations under the context's schedule; returns the batched iterations run (level launches) or 0.
@@ -1480,6 +1549,7 @@ int runIterations(BatchContext& ctx) {
         return 0;
     }
     captureIteration(ctx);
+    ctx.fp64Iterations = 0;
     if (ctx.phaseTiming) {
         for (double& v : ctx.phaseMs) v = 0.0;
         ctx.phaseLanes = 0;
@@ -1509,6 +1579,13 @@ int runIterations(BatchContext& ctx) {
         }
         if (!mixed) {
             OLF_CUDA(cudaGraphLaunch(scoreDue(ctx) ? ctx.graphSolveScored : ctx.graphSolve, st));
+            continue;
+        }
+        if (fp64Iteration(ctx)) {
+            ctx.fp64Iterations++;
+            launchPromoteFp64(ctx.batch(), st);
+            launchFp64Redo(ctx);
+            OLF_CUDA(cudaGraphLaunch(scoreDue(ctx) ? ctx.graphStepScored : ctx.graphStep, st));
             continue;
         }
         // mixed: FP32 factorization, then (while the FP32 solves run) the count of lanes flagged for FP64
@@ -1549,7 +1626,11 @@ void autotune(BatchContext& ctx) {
     }
     if (ctx.dn->sub.nBins > 0) cands.push_back({SCHEDULE_SUBTREES, 0, 256});
     cands.push_back({SCHEDULE_COOP, 0, 512});
-    if (ctx.dn->view.frontF == 0) {   // the persistent tiles do not run dense-front plans
+    // the persistent tiles run neither dense-front plans, nor the distributed-slack loop, the 2-norm test or the
+    // MAX_VOLTAGE_CHANGE clamp
+    const bool persistentFits = ctx.dn->view.frontF == 0 && !ctx.cfg.distributedSlack && ctx.cfg.norm2Threshold <= 0.0 &&
+                                ctx.cfg.svsMode == 0;
+    if (persistentFits) {
         for (int lanes : {2, 4})
             for (int threads : {256, 512}) cands.push_back({SCHEDULE_PERSISTENT, lanes, threads});
     }
@@ -1594,6 +1675,53 @@ void autotune(BatchContext& ctx) {
 }
 
 }  // namespace
+
+void setDistributedSlack(BatchContext& ctx, int nDs, const int* row, const double* factor, const double* baseTarget,
+                         const double* maxDelta, const double* minDelta, int slackRow, double slackTargetP) {
+    OLF_CUDA(cudaSetDevice(ctx.device));
+    const int n = ctx.net->host.n;
+    if (nDs <= 0) {
+        ctx.ds = DevDs{};
+        return;
+    }
+    if (slackRow < 0 || slackRow >= n) throw std::runtime_error("bad slackBusPhiRow");
+    double fsum = 0.0;
+    for (int i = 0; i < nDs; i++) {
+        if (row[i] < 0 || row[i] >= n) throw std::runtime_error("bad distributedSlackBusPhiRow");
+        if (!(factor[i] >= 0.0)) throw std::runtime_error("negative distributed-slack factor");
+        if (!(minDelta[i] <= 0.0 && maxDelta[i] >= 0.0)) {
+            throw std::runtime_error("distributed-slack bounds must contain the base target");
+        }
+        fsum += factor[i];
+    }
+    if (!(fsum > 0.0)) throw std::runtime_error("distributed-slack factors sum to zero");
+    std::vector<double> f(factor, factor + nDs);
+    for (double& v : f) v /= fsum;
+    const size_t S = ctx.S;
+    auto up = [&](DeviceBuffer& d, const void* src, size_t bytes) {
+        d.alloc(bytes);
+        OLF_CUDA(cudaMemcpy(d.p, src, bytes, cudaMemcpyHostToDevice));
+    };
+    up(ctx.dsRow, row, nDs * 4);
+    up(ctx.dsFactor, f.data(), nDs * 8);
+    up(ctx.dsBase, baseTarget, nDs * 8);
+    up(ctx.dsMax, maxDelta, nDs * 8);
+    up(ctx.dsMin, minDelta, nDs * 8);
+    ctx.dsPrev.alloc(static_cast<size_t>(nDs) * S * 8);
+    ctx.dsFailed.alloc(S);
+    OLF_CUDA(cudaDeviceSynchronize());   // the pageable uploads have landed before the context's stream reads them
+    DevDs& d = ctx.ds;
+    d.nDs = nDs;
+    d.row = ctx.dsRow.as<int>();
+    d.factor = ctx.dsFactor.as<double>();
+    d.baseTarget = ctx.dsBase.as<double>();
+    d.maxDelta = ctx.dsMax.as<double>();
+    d.minDelta = ctx.dsMin.as<double>();
+    d.slackRow = slackRow;
+    d.slackTargetP = slackTargetP;
+    d.prevTarget = ctx.dsPrev.as<double>();
+    d.failed = ctx.dsFailed.as<int8_t>();
+}
 
 void setStrongestPvKeys(BatchContext& ctx, const double* nomV, const int* pRow, const double* staticP,
                         const int* idRank) {
@@ -1671,6 +1799,7 @@ void stageRequest(BatchContext& ctx, const SolveRequest& req) {
     cfg.maxDv = req.maxDv;
     cfg.maxDphi = req.maxDphi;
     cfg.corrBound = ctx.corrBound;
+    cfg.polishBelow = ctx.fallbackStart ? ctx.polishRatio * req.tol : 0.0;
     cfg.realistic = ctx.hasVCheck ? 1 : 0;
     cfg.minV = ctx.realisticMinV;
     cfg.maxV = ctx.realisticMaxV;
@@ -1687,6 +1816,15 @@ void stageRequest(BatchContext& ctx, const SolveRequest& req) {
     cfg.maxOuter = req.maxOuter;
     cfg.maxSwitch = req.maxPqPvSwitch;
     cfg.reactiveLimits = ctx.rl.nRl > 0 && ctx.reactiveLimitsLoop && !req.skipReactiveLimits ? 1 : 0;
+    cfg.distributedSlack = ctx.ds.nDs > 0 && ctx.dsLoop ? 1 : 0;
+    cfg.slackDistTol = req.slackDistTol;
+    cfg.rejectDsFailure = req.rejectDsFailure ? 1 : 0;
+    if (cfg.distributedSlack && ctx.schedule == SCHEDULE_PERSISTENT) {
+        throw std::runtime_error("the persistent schedule does not run the distributed-slack outer loop");
+    }
+    if (cfg.distributedSlack && ctx.fallbackStart) {
+        throw std::runtime_error("the fallback start is not available with distributed slack");
+    }
     cfg.mixed = ctx.precision;
     cfg.refinementSteps = ctx.refinementSteps;
     cfg.refineBelow = ctx.refineBelow;
@@ -1860,6 +1998,10 @@ void solveMulti(MultiContext& m, double* const* outs) {
     const int precision = m.members[0]->precision;
     for (BatchContext* c : m.members) {
         if (!c->staged) throw std::runtime_error("every batch context of a multi-grid launch must be staged first");
+        if (c->cfg.distributedSlack || c->cfg.norm2Threshold > 0.0 || c->cfg.svsMode != SVS_NONE || c->cfg.realistic) {
+            throw std::runtime_error("a multi-grid launch runs the plain Newton loop with reactive limits only "
+                                     "(no distributed slack, 2-norm test, step clamp or realistic band)");
+        }
         if (c->precision != precision) {
             throw std::runtime_error("the batch contexts of a multi-grid launch share one precision");
         }
@@ -1973,6 +2115,55 @@ void debugLinearSolve(BatchContext& ctx, const double* csrVals, const double* rh
     OLF_CUDA(cudaMemcpy(dx.data(), ctx.dx.p, dx.size() * 8, cudaMemcpyDeviceToHost));
     for (int sc = 0; sc < ctx.nS; sc++)
         for (int r = 0; r < n; r++) out[static_cast<size_t>(sc) * n + r] = dx[static_cast<size_t>(r) * S + sc];
+}
+
+void linearSolveBoth(BatchContext& ctx, const double* csrVals, const double* rhs, const double* rhsT, int precision,
+                     double* x, double* y) {
+    OLF_CUDA(cudaSetDevice(ctx.device));
+    const Structure& s = ctx.net->host;
+    const DeviceNet& dn = *ctx.dn;
+    const DevNet& net = dn.view;
+    const int n = s.n;
+    const size_t S = ctx.S;
+    cudaStream_t st = ctx.stream;
+    const bool fp32 = precision == 1;
+    if (fp32 && !ctx.lu32.p) ctx.lu32.alloc(static_cast<size_t>(net.nLu) * 4 * S * 4);
+    if (!fp32 && !ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(net.nLu) * 4 * S * 8);
+    std::vector<double> J(ctx.J.bytes / 8, 0.0), F(static_cast<size_t>(n) * S, 0.0), C(static_cast<size_t>(n) * S, 0.0);
+    for (int sc = 0; sc < ctx.nS; sc++) {
+        for (int k = 0; k < s.nnz; k++) {
+            J[static_cast<size_t>(dn.csrToA[k]) * S + sc] = csrVals[static_cast<size_t>(sc) * s.nnz + k];
+        }
+        for (int r = 0; r < n; r++) {
+            if (rhs) F[static_cast<size_t>(r) * S + sc] = -rhs[static_cast<size_t>(sc) * n + r];
+            if (rhsT) C[static_cast<size_t>(r) * S + sc] = rhsT[static_cast<size_t>(sc) * n + r];
+        }
+    }
+    OLF_CUDA(cudaMemcpyAsync(ctx.J.p, J.data(), ctx.J.bytes, cudaMemcpyHostToDevice, st));
+    OLF_CUDA(cudaMemcpyAsync(ctx.F.p, F.data(), F.size() * 8, cudaMemcpyHostToDevice, st));
+    OLF_CUDA(cudaMemcpyAsync(ctx.res.p, C.data(), C.size() * 8, cudaMemcpyHostToDevice, st));
+    const DevBatch b = ctx.batch();
+    OLF_CUDA(cudaMemsetAsync(ctx.nActive.p, 0, sizeof(int), st));
+    laneInitKernel<<<(ctx.S + 127) / 128, 128, 0, st>>>(b);
+    launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), static_cast<int>(dn.levelPtr.size()) - 1, fp32,
+                 nullptr, st);
+    std::vector<double> out(static_cast<size_t>(n) * S);
+    auto gather = [&](double* dst) {
+        OLF_CUDA(cudaMemcpyAsync(out.data(), ctx.dx.p, out.size() * 8, cudaMemcpyDeviceToHost, st));
+        OLF_CUDA(cudaStreamSynchronize(st));
+        for (int sc = 0; sc < ctx.nS; sc++)
+            for (int r = 0; r < n; r++) dst[static_cast<size_t>(sc) * n + r] = out[static_cast<size_t>(r) * S + sc];
+    };
+    if (rhs && x) {
+        launchSolve(net, b, dn.fwd(), dn.bwd(), fp32, false, nullptr, st);
+        gather(x);
+    }
+    if (rhsT && y) {
+        launchSolveTransposed(net, b, dn.fwd(), dn.bwd(), fp32, st);
+        gather(y);
+    }
+    OLF_CUDA(cudaStreamSynchronize(st));
+    OLF_CUDA(cudaGetLastError());
 }
 
 }  // namespace olfb200

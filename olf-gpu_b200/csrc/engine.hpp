@@ -72,7 +72,7 @@ struct DeviceNet {
     DeviceBuffer csrToAD;                         // the same map on the device
     DeviceBuffer nodeCol, sidePtr, side, cbPar, cbTrig, aPtr, aCol, aDiag, shPtr, shList, shPar, obPtr, obList, obPar;
     DeviceBuffer frontBlocks;
-    DeviceBuffer task, ops, levelTask, perm, iperm, lrowPtr, lrowEnd, lrow, uPtr, uCol, fwdPos, bwdPos;
+    DeviceBuffer task, ops, levelTask, perm, iperm, lrowPtr, lrowEnd, lrow, uPtr, uCol, fwdPos, bwdPos, lrowU, uRowL;
     DeviceBuffer levelPtrD, levelLongestD, fwdPtrD, fwdLongestD, bwdPtrD, bwdLongestD, levelSplitD, fwdSplitD, bwdSplitD;
     CoopPlan coop{};
     PersistentPlan persistent{};
@@ -140,6 +140,9 @@ enum {
     SCHEDULE_SUBTREES = 5          // schedule 4 with the wide levels' subtrees in one launch per phase (subtree bins)
 };
 
+// Mixed-precision policies (BatchContext::mixedPolicy)
+enum { MIXED_REFINE = 0, MIXED_FP64_NEAR = 1 };
+
 // Mixed precision: a refinement step's correction solve runs only while some lane's FP64 residual max |r| is above
 // this fraction of the mismatch tolerance (below it the FP32 solve is already accurate enough for the test).
 constexpr double REFINE_RESIDUAL = 0.1;
@@ -176,6 +179,8 @@ struct SolveRequest {
     double maxDv = 0.1, maxDphi = 0.17453292519943295;
     const int* varType = nullptr;    // [n] 0 BUS_V, 1 BUS_PHI (MAX_VOLTAGE_CHANGE)
     bool skipReactiveLimits = false; // this solve runs without the reactive-limit outer loop
+    double slackDistTol = 1e-2;      // distributed slack: the mismatch above which it is distributed (pu)
+    bool rejectDsFailure = false;    // distributed slack: a failed distribution ends the scenario REJECTED
     const unsigned char* laneLive = nullptr;  // [nS] or null: the bank lanes that hold a scenario of this solve
 };
 
@@ -207,6 +212,7 @@ struct BatchContext {
     int64_t solveCount = 0;         // solves run through the full entry (BatchReadbackNative.readBatchSolveCount)
     bool reactiveLimitsLoop = true;
     bool fallbackStart = false;     // lanes that fail from x0Full restart once from x0Base (both given)
+    double polishRatio = 1e-2;      // fallback mode: polish a lane converged from its own start above polishRatio * tol
     bool rlKeys = false;            // the reactive-limit entries' forced-PV election keys are set
     const double* deviceStart = nullptr;  // caller's device array [nS][n] used as x0Full by the solves
     const double* fullSrc = nullptr;      // where the installed x0Full rows come from
@@ -249,6 +255,9 @@ struct BatchContext {
     std::vector<TuningResult> tuning;
     DeviceBuffer out;               // [nS][n + 3] scenario-major results
     // reactive limits
+    DevDs ds{};                     // distributed-slack participants (ds.nDs 0: none)
+    DeviceBuffer dsRow, dsFactor, dsBase, dsMax, dsMin, dsPrev, dsFailed, dsRestartBuf;
+    bool dsLoop = true;             // the distributed-slack outer loop switch (DriverNative.setBatchOuterLoops)
     DevRl rl{};
     DeviceBuffer rlVoltageRow, rlMinQ, rlMaxQ, rlLoadQ, rlTargetV, rlNomV, rlPRow, rlStaticP, rlIdRank, rlLimitType,
         rlSwitchCount, rlPassSwitched, rlSavedMode, rlSavedTarget, rlRemainingPv, rlSwitched;
@@ -273,6 +282,9 @@ struct BatchContext {
     // mixed: a lane refines only in an iteration where its max |F| is below refineBelow; 1e-2 covers every step from
     // which Newton can land below the tolerance, so a converged state's last step is FP64-accurate
     double refineBelow = 1e-2;
+    // mixed precision: MIXED_REFINE refines the FP32 solves of the lanes below refineBelow; MIXED_FP64_NEAR factors
+    // and solves an iteration with such a lane in FP64 (all its lanes), and iterations without one in FP32, unrefined
+    int mixedPolicy = 0;
     double corrBound = 1e-11;       // mixed: a lane keeps refining while its last correction's max |d| is above it
     double realisticMinV = 0.0, realisticMaxV = 0.0;   // realistic-voltage band (hasVCheck)
     double growthLimit = 1e4;       // mixed: FP32 pivot growth above which a lane refactors in FP64
@@ -285,6 +297,7 @@ struct BatchContext {
     double phaseMs[6] = {0, 0, 0, 0, 0, 0};   // fill, test, factorization, solves, refinement, step (summed)
     long long phaseLanes = 0;       // lanes that factorized, summed over the iterations
     int phaseIterations = 0;
+    int fp64Iterations = 0;         // iterations of the last solve that MIXED_FP64_NEAR ran in FP64
     ~BatchContext();
     DevBatch batch() const;
 };
@@ -292,6 +305,11 @@ struct BatchContext {
 BatchContext* createContext(std::shared_ptr<NetStructure> net, int nScenarios, int mode, int nRl, const int* voltageRow,
                             const double* minQ, const double* maxQ, const double* loadQ, const double* targetV,
                             const double* nomV, const int* pRow, const double* staticP, const int* idRank);
+
+// Installs the distributed-slack participants of a context: P rows, factors (normalised here to sum 1), base targets,
+// bounds of their move from the base; the slack bus's angle row and net P target.
+void setDistributedSlack(BatchContext& ctx, int nDs, const int* row, const double* factor, const double* baseTarget,
+                         const double* maxDelta, const double* minDelta, int slackRow, double slackTargetP);
 
 // Runs the batch; out = [nS][n + 3] per scenario [x(n), iterations, ||F||inf, status].
 void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out);
@@ -336,5 +354,30 @@ void solveMulti(MultiContext& m, double* const* outs);
 void debugFill(BatchContext& ctx, const double* xFull, const double* targetBase, const int* baseRowMode,
                const unsigned char* disabled, double* jOut, double* fOut);
 void debugLinearSolve(BatchContext& ctx, const double* csrVals, const double* rhs, int precision, double* out);
+// Limit tables of the violation screening (host arrays; see violations.cu).
+struct ViolationTables {
+    int nElem = 0;
+    const int* elemId = nullptr;       // [nElem] element (closed branch e, or open branch nCb + e)
+    const int* groupPtr = nullptr;     // [nElem + 1] its limit groups
+    const int* groupSide = nullptr;    // [groups] 1 or 2
+    const int* groupQty = nullptr;     // [groups] 0 current I, 1 active power |P|, 2 apparent power S
+    const int* limPtr = nullptr;       // [groups + 1] its thresholds
+    const double* limThreshold = nullptr;
+    int nBus = 0;
+    const int* busVRow = nullptr;      // [nBus] the bus's V row (-1: none)
+    const double* busHigh = nullptr;   // [nBus] high / low voltage limits (NaN: none)
+    const double* busLow = nullptr;
+    int realistic = 0;                 // 1: also the buses outside [minV, maxV]
+    double minV = 0.0, maxV = 0.0;
+    double band = 1e-7;                // relative relaxation of every threshold
+};
+// Screens the context's last solve: per scenario, up to `capacity` record ids (sorted) into records [nS][capacity] and
+// the count of candidates into counts [nS] (a count above capacity: the list is truncated).
+void screenViolations(BatchContext& ctx, const ViolationTables& t, int capacity, int* records, int* counts);
+
+// One factorization of J (CSR values [nS][nnz]), then both J x = rhs and J^T y = rhsT on its factors (either rhs may be
+// null, its output then untouched); all arrays scenario-major host arrays.
+void linearSolveBoth(BatchContext& ctx, const double* csrVals, const double* rhs, const double* rhsT, int precision,
+                     double* x, double* y);
 
 }  // namespace olfb200

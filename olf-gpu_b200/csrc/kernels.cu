@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(256, 5) fillKernel(DevNet net, DevBatch b) {
         const bool idP = b.mode[cP * S + s] == MODE_FIXED_VARIABLE;
         const bool idQ = b.mode[cV * S + s] == MODE_FIXED_VARIABLE;
         const int words = b.S >> 5;
-        double fp = 0.0, fq = 0.0, qcl = 0.0;
+        double fp = 0.0, fq = 0.0, pcl = 0.0, qcl = 0.0;
         double d00 = 0.0, d01 = 0.0, d10 = 0.0, d11 = 0.0;
         double o00 = 0.0, o01 = 0.0, o10 = 0.0, o11 = 0.0;
         int curNb = -1, curBlk = -1;
@@ -82,6 +82,7 @@ __global__ void __launch_bounds__(256, 5) fillKernel(DevNet net, DevBatch b) {
                 const double q1 = r1 * v1 * (-b1 * r1 * v1 + y * r1 * v1 * ck - y * v2 * c1);
                 fp += p1;
                 fq += q1;
+                pcl += p1;
                 qcl += q1;
                 if (WITH_J) {
                     d00 += wc;                                                             // dp1dph1
@@ -104,6 +105,7 @@ __global__ void __launch_bounds__(256, 5) fillKernel(DevNet net, DevBatch b) {
                 const double q2 = v2 * (-b2 * v2 - y * r1 * v1 * c2 + y * v2 * ck);
                 fp += p2;
                 fq += q2;
+                pcl += p2;
                 qcl += q2;
                 if (WITH_J) {
                     d00 += wc;                                             // dp2dph2
@@ -167,7 +169,10 @@ __global__ void __launch_bounds__(256, 5) fillKernel(DevNet net, DevBatch b) {
         if (idQ) FQ = vi - b.target[cV * S + s];
         b.F[cP * S + s] = FP;
         b.F[cV * S + s] = FQ;
-        if (WITH_Q) b.qbuf[cV * S + s] = qcl;
+        if (WITH_Q) {   // the closed-branch flows on the bus's rows (reactive limits read Q, distributed slack P)
+            b.qbuf[cP * S + s] = pcl;
+            b.qbuf[cV * S + s] = qcl;
+        }
         if (WITH_J) {
             double* J = b.J + (size_t)net.aDiag[node] * 4 * S + s;
             J[0] = idP ? 1.0 : d00;
@@ -290,7 +295,11 @@ __global__ void testKernel(DevBatch b, Settings cfg, int* remainingPv) {
         converged = nrm < cfg.tol;
     }
     if (it > 0 && converged && it < cfg.maxIter) {
-        if (cfg.reactiveLimits && b.outer[s] < cfg.maxOuter) {
+        if (cfg.polishBelow > 0.0 && b.fallbackLeft[s] && nrm > cfg.polishBelow && it + 1 < cfg.maxIter) {
+            b.fallbackLeft[s] = 0;   // one more step from inside the tolerance ball (the lane has converged: no restart)
+            return;
+        }
+        if ((cfg.reactiveLimits || cfg.distributedSlack) && b.outer[s] < cfg.maxOuter) {
             b.pending[s] = 1;
             if (remainingPv) remainingPv[s] = 0;
         } else {
@@ -337,7 +346,7 @@ __global__ void rlCheckKernel(DevBatch b, DevRl rl, Settings cfg) {
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int s = (int)(tid % S);
     const int i = (int)(tid / S);
-    if (i >= rl.nRl || !b.pending[s]) return;
+    if (i >= rl.nRl || !b.pending[s] || (b.dsRestart && b.dsRestart[s])) return;
     const size_t e = (size_t)i * S + s;
     rl.passSwitched[e] = 0;
     const int r = rl.voltageRow[i];
@@ -378,7 +387,7 @@ __global__ void rlCheckKernel(DevBatch b, DevRl rl, Settings cfg) {
 
 __global__ void rlFinalizeKernel(DevBatch b, DevRl rl, Settings cfg) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= b.S || !b.pending[s]) return;
+    if (s >= b.S || !b.pending[s] || (b.dsRestart && b.dsRestart[s])) return;
     const size_t S = b.S;
     if (rl.remainingPv[s] == 0) {
         int best = -1, bestId = 0x7fffffff;
@@ -416,6 +425,82 @@ __global__ void rlFinalizeKernel(DevBatch b, DevRl rl, Settings cfg) {
         b.pending[s] = 0;
         retireConverged(b, cfg, s);
     }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Distributed slack (DistributedSlackOuterLoop; distributed_slack.cu:211-616, the bus-level water-fill), one thread
+// per lane that converged this iteration.  The slack bus's closed-branch P minus its target is the mismatch; above
+// slackDistTol, every participant is reset to its base target and the whole amount (the mismatch plus what the
+// participants had absorbed) is water-filled over them in proportion to their factors, each clamped to its bounds and
+// the factors renormalised over the unsaturated ones, until less than P_RESIDUE_EPS is left.  Targets that moved by
+// more than 0.9 P_RESIDUE_EPS in total make the lane re-solve (an outer iteration); an unplaced remainder above
+// P_RESIDUE_EPS is a distribution failure (REJECTED when the request asks, else left on the slack).  A lane that does
+// not re-solve goes on to the reactive-limit check, or retires.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void dsCheckKernel(DevBatch b, DevDs ds, Settings cfg) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.S || !b.pending[s]) return;
+    const size_t S = b.S;
+    const double mis = b.qbuf[(size_t)ds.slackRow * S + s] - ds.slackTargetP;
+    bool moved = false;
+    if (fabs(mis) > cfg.slackDistTol && fabs(mis) > P_RESIDUE_EPS) {
+        double absorbed = 0.0;
+        for (int i = 0; i < ds.nDs; i++) {
+            const size_t idx = (size_t)ds.row[i] * S + s;
+            absorbed += b.target[idx] - ds.baseTarget[i];
+            ds.prevTarget[(size_t)i * S + s] = b.target[idx];
+            b.target[idx] = ds.baseTarget[i];
+        }
+        double rem = mis + absorbed;
+        for (int it = 0; it < ds.nDs && fabs(rem) > P_RESIDUE_EPS; it++) {
+            double fsum = 0.0;
+            for (int i = 0; i < ds.nDs; i++) {
+                const double cum = b.target[(size_t)ds.row[i] * S + s] - ds.baseTarget[i];
+                const bool sat = rem > 0 ? cum >= ds.maxDelta[i] : cum <= ds.minDelta[i];
+                if (!sat) fsum += ds.factor[i];
+            }
+            if (fsum <= 0.0) break;   // every participant saturated: the rest stays at the slack
+            double done = 0.0;
+            for (int i = 0; i < ds.nDs; i++) {
+                const size_t idx = (size_t)ds.row[i] * S + s;
+                const double cum = b.target[idx] - ds.baseTarget[i];
+                const bool sat = rem > 0 ? cum >= ds.maxDelta[i] : cum <= ds.minDelta[i];
+                if (sat) continue;
+                const double next = fmin(fmax(cum + rem * (ds.factor[i] / fsum), ds.minDelta[i]), ds.maxDelta[i]);
+                if (next != cum) {
+                    b.target[idx] = ds.baseTarget[i] + next;
+                    done += next - cum;
+                }
+            }
+            rem -= done;
+        }
+        double shift = 0.0;
+        for (int i = 0; i < ds.nDs; i++)
+            shift += fabs(b.target[(size_t)ds.row[i] * S + s] - ds.prevTarget[(size_t)i * S + s]);
+        moved = shift > 0.9 * P_RESIDUE_EPS;
+        ds.failed[s] = fabs(rem) > P_RESIDUE_EPS ? 1 : 0;
+        if (ds.failed[s] && cfg.rejectDsFailure) {
+            b.status[s] = ST_REJECTED;
+            b.active[s] = 0;
+            b.pending[s] = 0;
+            atomicSub(b.nActive, 1);
+            return;
+        }
+    }
+    if (moved) {
+        // re-solve at the new targets (newton_iteration.cu:472-487); still pending for this iteration
+        b.iter[s] = 0;
+        b.outer[s]++;
+        b.dsRestart[s] = 1;
+    } else if (!cfg.reactiveLimits) {
+        b.pending[s] = 0;
+        retireConverged(b, cfg, s);
+    }
+}
+
+void launchDistributedSlack(const DevBatch& b, const DevDs& ds, const Settings& cfg, cudaStream_t st) {
+    if (ds.nDs == 0) return;
+    dsCheckKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b, ds, cfg);
 }
 
 void launchReactiveLimits(const DevNet&, const DevBatch& b, const DevRl& rl, const Settings& cfg, cudaStream_t st) {
@@ -1055,6 +1140,97 @@ void launchSolve(const DevNet& net, const DevBatch& b, const LevelSchedule& fwd,
 }
 
 // ---------------------------------------------------------------------------------------------------------------
+// Transposed solve J^T y = c on the same block factors (transposed_solve.cuh:1-30): the plain solve's operations
+// transposed, in reverse order.  With P J P^T = L U (L unit lower, U upper with the pivot blocks D, whose slots hold
+// inv(D)): U^T y' = c' forward, row i: y'_i = inv(D_i)^T (c'_i - sum_k U(k, i)^T y'_k) over the L pattern of row i;
+// then L^T z = y' backward, row i: z_i = y'_i - sum_j L(j, i)^T z_j over the U pattern of row i.  The level schedules
+// of the plain sweeps serve (the patterns coincide); a dense front's positions (the last frontF of the order) run in
+// order, one thread per lane, after the forward levels and before the backward ones.
+// ---------------------------------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void upperTransposedRow(const DevNet& net, const T* lu, T* w, int i, size_t S, int s) {
+    T w0 = w[(2 * (size_t)i) * S + s], w1 = w[(2 * (size_t)i + 1) * S + s];
+    for (int q = net.lrowPtr[i]; q < net.lrowPtr[i + 1]; q++) {
+        const int k = net.lrow[q].y;
+        T u00, u01, u10, u11;
+        load4(lu, (size_t)net.lrowU[q], S, s, u00, u01, u10, u11);
+        const T y0 = w[(2 * (size_t)k) * S + s], y1 = w[(2 * (size_t)k + 1) * S + s];
+        w0 -= u00 * y0 + u10 * y1;
+        w1 -= u01 * y0 + u11 * y1;
+    }
+    T i00, i01, i10, i11;
+    load4(lu, (size_t)net.uPtr[i], S, s, i00, i01, i10, i11);
+    w[(2 * (size_t)i) * S + s] = i00 * w0 + i10 * w1;
+    w[(2 * (size_t)i + 1) * S + s] = i01 * w0 + i11 * w1;
+}
+
+template <typename T>
+__device__ __forceinline__ void lowerTransposedRow(const DevNet& net, const T* lu, T* w, int i, size_t S, int s) {
+    T w0 = w[(2 * (size_t)i) * S + s], w1 = w[(2 * (size_t)i + 1) * S + s];
+    for (int q = net.uPtr[i] + 1; q < net.uPtr[i + 1]; q++) {
+        const int j = net.uCol[q];
+        T l00, l01, l10, l11;
+        load4(lu, (size_t)net.uRowL[q], S, s, l00, l01, l10, l11);
+        const T z0 = w[(2 * (size_t)j) * S + s], z1 = w[(2 * (size_t)j + 1) * S + s];
+        w0 -= l00 * z0 + l10 * z1;
+        w1 -= l01 * z0 + l11 * z1;
+    }
+    w[(2 * (size_t)i) * S + s] = w0;
+    w[(2 * (size_t)i + 1) * S + s] = w1;
+}
+
+// one level of a transposed sweep: 8 rows x 32 lanes per CTA (DIR 0: U^T forward, 1: L^T backward); front rows skipped
+template <typename T, int DIR>
+__global__ void transposedLevelKernel(DevNet net, DevBatch b, const T* lu, T* w, const int* pos, int first, int count) {
+    const int k = blockIdx.x * 8 + threadIdx.y;
+    const int s = blockIdx.y * 32 + threadIdx.x;
+    if (k >= count || s >= b.S || !solving(b, s)) return;
+    const int i = pos[first + k];
+    if (net.frontF > 0 && i >= net.frontStart) return;
+    if (DIR == 0) upperTransposedRow(net, lu, w, i, b.S, s);
+    else lowerTransposedRow(net, lu, w, i, b.S, s);
+}
+
+// the dense front's rows in order, one thread per lane (DIR 0: ascending U^T rows, 1: descending L^T rows)
+template <typename T, int DIR>
+__global__ void transposedFrontKernel(DevNet net, DevBatch b, const T* lu, T* w) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.S || !solving(b, s)) return;
+    for (int r = 0; r < net.frontF; r++) {
+        const int i = DIR == 0 ? net.frontStart + r : net.nb - 1 - r;
+        if (DIR == 0) upperTransposedRow(net, lu, w, i, b.S, s);
+        else lowerTransposedRow(net, lu, w, i, b.S, s);
+    }
+}
+
+template <typename T>
+static void solveTransposedT(const DevNet& net, const DevBatch& b, T* w, const T* lu, const LevelSchedule& fwd,
+                             const LevelSchedule& bwd, cudaStream_t st) {
+    const size_t all = (size_t)net.nb * b.S;
+    rhsKernel<T><<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b, w, true);
+    dim3 blk(32, 8);
+    for (int l = 0; l < fwd.levels; l++) {
+        const int first = fwd.ptr[l], count = fwd.ptr[l + 1] - first;
+        if (count > 0) transposedLevelKernel<T, 0><<<dim3((count + 7) / 8, b.S / 32), blk, 0, st>>>(net, b, lu, w, fwd.pos, first, count);
+    }
+    if (net.frontF > 0) {
+        transposedFrontKernel<T, 0><<<b.S / 32, 32, 0, st>>>(net, b, lu, w);
+        transposedFrontKernel<T, 1><<<b.S / 32, 32, 0, st>>>(net, b, lu, w);
+    }
+    for (int l = 0; l < bwd.levels; l++) {
+        const int first = bwd.ptr[l], count = bwd.ptr[l + 1] - first;
+        if (count > 0) transposedLevelKernel<T, 1><<<dim3((count + 7) / 8, b.S / 32), blk, 0, st>>>(net, b, lu, w, bwd.pos, first, count);
+    }
+    scatterKernel<T><<<(unsigned)((all + 255) / 256), 256, 0, st>>>(net, b, w, false);
+}
+
+void launchSolveTransposed(const DevNet& net, const DevBatch& b, const LevelSchedule& fwd, const LevelSchedule& bwd,
+                           bool fp32, cudaStream_t st) {
+    if (fp32) solveTransposedT<float>(net, b, b.w32, b.lu32, fwd, bwd, st);
+    else solveTransposedT<double>(net, b, b.w64, b.lu64, fwd, bwd, st);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
 // FP64 refinement residual r = -F - J dx, one thread per (bus, lane), J in its block rows.
 // ---------------------------------------------------------------------------------------------------------------
 __global__ void residualKernel(DevNet net, DevBatch b) {
@@ -1138,10 +1314,12 @@ __global__ void advanceKernel(DevBatch b) {
     b.totalIter[s]++;
 }
 
-// Start of an iteration: the lanes a reactive-limit check restarted last iteration solve again.
+// Start of an iteration: the lanes an outer-loop check restarted last iteration solve again.
 __global__ void releasePendingKernel(DevBatch b) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < b.S) b.pending[s] = 0;
+    if (s >= b.S) return;
+    b.pending[s] = 0;
+    if (b.dsRestart) b.dsRestart[s] = 0;
 }
 
 // After the test: how many lanes factorize this iteration (the host skips the factor/solve graph when none does) and
@@ -1204,6 +1382,14 @@ void launchCountSolving(const DevBatch& b, double refineBelow, int maxIter, cuda
 }
 
 void launchCountFp64(const DevBatch& b, cudaStream_t st) { countLanesKernel<<<1, 1024, 0, st>>>(b, 0.0, 1, 0); }
+
+// Iteration-level precision: every lane that factorizes this iteration is flagged for FP64 (for the rest of the solve)
+__global__ void promoteKernel(DevBatch b) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < b.S && solving(b, s)) b.precision64[s] = 1;
+}
+
+void launchPromoteFp64(const DevBatch& b, cudaStream_t st) { promoteKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b); }
 
 // Per-lane max |res| over the rows: 32 lanes x 8 row strands per CTA, reduced in shared memory, one atomic per CTA
 // and lane (non-negative doubles order like their bit patterns; a NaN residual sorts above every number).

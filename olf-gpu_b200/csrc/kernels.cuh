@@ -72,6 +72,8 @@ struct DevNet {
     const int2* lrow;         // (L block id, column position)
     const int* uPtr;          // [nb + 1] U blocks of each row position (diagonal first: holds the inverse)
     const int* uCol;          // column position of each U block
+    const int* lrowU;         // per L entry L(i, k) of lrow: the U block U(k, i) (transposed solve)
+    const int* uRowL;         // per U block U(i, j), j > i: the L block L(j, i) (transposed solve)
 };
 
 // Programmatic dependent launch (level kernels): pdlTrigger lets the next grid in the stream start its CTAs once
@@ -133,7 +135,27 @@ struct DevBatch {
     const int8_t* varType;    // [n] 0 BUS_V, 1 BUS_PHI, -1 neither (MAX_VOLTAGE_CHANGE); may be null
     const int8_t* vCheck;     // [n] 1: a voltage row checked against the realistic band at convergence; may be null
     const int8_t* laneLive;   // [S] 1: the lane holds a scenario of this solve (null: lanes < nS); others stay idle
+    int8_t* dsRestart;        // [S] distributed slack moved the targets this iteration: the lane re-solves (no RL check)
 };
+
+// Distributed-slack participants (bus level; BatchSolveNative.createBatchContext's tables): P rows, participation
+// factors, base targets and the bounds of their move from the base; the slack bus's angle row (its P equation is the
+// identity) and net P target; per lane the participants' targets before the last distribution and a failure flag.
+struct DevDs {
+    int nDs;
+    const int* row;
+    const double* factor;
+    const double* baseTarget;
+    const double* maxDelta;
+    const double* minDelta;
+    int slackRow;
+    double slackTargetP;
+    double* prevTarget;       // [nDs][S]
+    int8_t* failed;           // [S] the last distribution left more than P_RESIDUE_EPS unplaced
+};
+// ActivePowerDistribution's residue epsilon (1e-5 pu): below it a mismatch is not distributed, above it an unplaced
+// remainder is a distribution failure.
+constexpr double P_RESIDUE_EPS = 1e-5;
 
 // Strands of the deterministic 2-norm reduction (row r of a lane goes to strand r % SSQ_STRANDS, summed in row order,
 // then the strands in strand order).
@@ -181,6 +203,10 @@ struct Settings {
     double growthLimit;       // pivot growth above which a mixed lane refactors in FP64
     double refineBelow;       // refinement steps run in an iteration where a factorizing lane's max |F| is below it
     double corrBound;         // mixed: a lane keeps refining while its last correction's max |d| is above it
+    // fallback mode: a lane converged from its own start (the learned start) takes one more Newton step when its max
+    // |F| is above polishBelow (0: never), so its state lies near the solution rather than anywhere in the tolerance
+    // ball, and agrees with the state the base-start trajectory reaches
+    double polishBelow;
     // OLF's stopping criterion when > 0 (newton_iteration.cu:105,241-250): converged when ||F||2 < norm2Threshold =
     // sqrt(convEpsPerEq^2 n); else the device's ||F||inf < tol
     double norm2Threshold;
@@ -189,6 +215,9 @@ struct Settings {
     double maxDv, maxDphi;
     int realistic;            // 1: a converged state with a checked voltage outside [minV, maxV] is UNREALISTIC_STATE
     double minV, maxV;
+    int distributedSlack;     // 1: the distributed-slack outer loop runs on converged lanes (before reactive limits)
+    double slackDistTol;      // slack mismatch above which it is distributed (slackBusPMaxMismatch, pu)
+    int rejectDsFailure;      // 1: a lane whose distribution fails ends REJECTED (else the rest stays on the slack)
 };
 
 // Kernel launchers (stream-ordered; all lanes of the batch).
@@ -196,6 +225,9 @@ void launchFill(const DevNet& net, const DevBatch& b, bool withJacobian, bool wi
 void launchTest(const DevNet& net, const DevBatch& b, const Settings& cfg, int* remainingPv, cudaStream_t st);
 void launchReactiveLimits(const DevNet& net, const DevBatch& b, const DevRl& rl, const Settings& cfg,
                           cudaStream_t st);
+// The distributed-slack check of the lanes that converged this iteration (distributed_slack.cu:211-616, bus level),
+// after launchTest and before launchReactiveLimits.
+void launchDistributedSlack(const DevBatch& b, const DevDs& ds, const Settings& cfg, cudaStream_t st);
 // The dependency levels the persistent kernel walks (device pointers) and, per level, the longest update list of its
 // tasks/rows (sets how many threads share a task).
 struct PersistentPlan {
@@ -291,6 +323,11 @@ void launchFactor(const DevNet& net, const DevBatch& b, const int* levelPtrHost,
 void launchSolve(const DevNet& net, const DevBatch& b, const LevelSchedule& fwd, const LevelSchedule& bwd, bool fp32,
                  bool fromResidual, const Hybrid* hybrid, cudaStream_t st);
 void launchResidual(const DevNet& net, const DevBatch& b, cudaStream_t st);
+// The transposed solve J^T y = c on the factors of the last factorization (transposed_solve.cuh:1-30): U^T forward on
+// the forward levels, then L^T backward on the backward levels, the dense front's positions swept in order between;
+// c is read from b.res (n rows, lane-interleaved) and y written to b.dx.
+void launchSolveTransposed(const DevNet& net, const DevBatch& b, const LevelSchedule& fwd, const LevelSchedule& bwd,
+                           bool fp32, cudaStream_t st);
 void launchStep(const DevNet& net, const DevBatch& b, const Settings& cfg, cudaStream_t st);
 void launchIterationStart(const DevBatch& b, cudaStream_t st);
 // Lanes that factorize this iteration (nActive[1]); of those, the lanes whose max |F| is below refineBelow
@@ -299,6 +336,7 @@ void launchIterationStart(const DevBatch& b, cudaStream_t st);
 void launchCountSolving(const DevBatch& b, double refineBelow, int maxIter, cudaStream_t st);
 // Factorizing lanes flagged for an FP64 refactor (nActive[3]).
 void launchCountFp64(const DevBatch& b, cudaStream_t st);
+void launchPromoteFp64(const DevBatch& b, cudaStream_t st);
 // Mixed precision, after launchResidual: each lane's max |r| and the count of factorizing lanes with max |F| below
 // refineBelow whose residual is above `threshold` (nActive[2]): the correction solve of a refinement step runs only
 // when some lane needs it.

@@ -440,7 +440,10 @@ __device__ void newtonTile(const DevNet& net, const DevBatch& b, const DevRl& rl
                 if (troubled) st = ST_LINEAR_SOLVE_FAILED;
                 else if (!isfinite(nrm)) st = ST_DIVERGED;
                 else if (it > 0 && nrm < cfg.tol && it < cfg.maxIter) {
-                    if (rlOn && ts.outer[tid] < cfg.maxOuter) {
+                    if (cfg.polishBelow > 0.0 && b.fallbackLeft[s0 + tid] && nrm > cfg.polishBelow &&
+                        it + 1 < cfg.maxIter) {
+                        b.fallbackLeft[s0 + tid] = 0;   // one more step from inside the tolerance ball
+                    } else if (rlOn && ts.outer[tid] < cfg.maxOuter) {
                         ts.pending[tid] = 1;
                         ts.remainingPv[tid] = 0;
                         ts.any[tid] = 0;

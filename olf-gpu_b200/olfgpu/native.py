@@ -43,7 +43,9 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_set_fp64_restart", "olfgpu_structure_subtrees", "olfgpu_create_structure_full",
            "olfgpu_create_batch_context_full", "olfgpu_set_reactive_limit_strongest_pv_keys",
            "olfgpu_begin_batch_install", "olfgpu_read_handed_back_slots", "olfgpu_set_states_to_host",
-           "olfgpu_states_to_host", "olfgpu_read_batch_states", "olfgpu_set_outer_loops", "olfgpu_context_info"]
+           "olfgpu_states_to_host", "olfgpu_read_batch_states", "olfgpu_set_outer_loops", "olfgpu_context_info",
+           "olfgpu_linear_solve_transposed", "olfgpu_screen_violations", "olfgpu_last_slack_distribution_failures",
+           "olfgpu_set_start_polish", "olfgpu_set_mixed_precision_policy", "olfgpu_last_fp64_iterations"]
 # The arrays of BatchSolveNative.solveBatchContext this engine rejects when non-empty, in the reference's order
 UNSUPPORTED_SOLVE_ARRAYS = [
     "distributedSlackOverrideBus", "distributedSlackOverrideFactorDelta", "distributedSlackOverrideBaseTargetPDelta",
@@ -55,6 +57,7 @@ _INT_SOLVE_ARRAYS = {"distributedSlackOverrideBus", "reactiveLimitTargetVOverrid
                      "reactiveLimitDeltaOverrideScenarioEntry", "reactiveCapabilityCurveOverrideScenarioCurve"}
 # State-vector scaling modes (codes/gpu_state_vector_scaling_mode.cuh) and variable types (gpu_ac_variable_type.cuh)
 SVS_NONE, SVS_LINE_SEARCH, SVS_MAX_VOLTAGE_CHANGE = 0, 1, 2
+MIXED_REFINE, MIXED_FP64_NEAR = 0, 1
 VAR_BUS_V, VAR_BUS_PHI = 0, 1
 # Schedules of the Newton iterations (LEVELS_SHARED: the level schedule with the narrow factorization levels in
 # shared memory; LEVELS_SHARED_ALL: the solves' narrow levels too; SUBTREES: LEVELS_SHARED_ALL with the wide levels'
@@ -102,10 +105,22 @@ def load(path: str = LIB_PATH):
          _ci, _cd, _cd, _cd, _cd, _ci, _cd, _cd, _ip, _ci, _dp, _ci,
          _ip, _ci, _dp, _ci, _ip, _ci, _ip, _ci, _dp, _ci,
          _ci, _ci, _ci, _ci, _ci, _ip, _ci, _ip, _ci, _ci, _dp])
+    L.olfgpu_create_batch_context_full.argtypes = (
+        [_i64, _ci, _ci, _ip, _ci, _dp, _ci, _dp, _ci, _dp, _ci, _dp, _ci, ctypes.POINTER(ctypes.c_byte), _ci, _dp, _ci,
+         _ip, _ci, _dp, _ci, _ci, _cd, _dp, _ci, _dp, _ci, _dp, _ci, _ci, _dp, _ci, _dp, _ci, _cd, _cd,
+         ctypes.POINTER(_i64)])
+    L.olfgpu_last_slack_distribution_failures.argtypes = [_i64, _u8p, _ip]
+    L.olfgpu_set_reactive_limit_strongest_pv_keys.argtypes = [_i64, _dp, _ip, _dp, _ip, _ci]
     L.olfgpu_set_realistic_check.argtypes = [_i64, _u8p, _cd, _cd, _ci]
     L.olfgpu_set_refinement_bound.argtypes = [_i64, _cd]
     L.olfgpu_set_fp64_restart.argtypes = [_i64, _ci]
+    L.olfgpu_set_start_polish.argtypes = [_i64, _cd]
+    L.olfgpu_set_mixed_precision_policy.argtypes = [_i64, _ci]
+    L.olfgpu_last_fp64_iterations.argtypes = [_i64, _ip]
     L.olfgpu_structure_subtrees.argtypes = [_i64, ctypes.POINTER(_i64)]
+    L.olfgpu_linear_solve_transposed.argtypes = [_i64, _dp, _dp, _dp, _ci, _dp, _dp]
+    L.olfgpu_screen_violations.argtypes = [_i64, _ci, _ip, _ip, _ip, _ip, _ip, _dp, _ci, _ip, _dp, _dp, _ci, _cd, _cd,
+                                           _cd, _ci, _ip, _ip]
     L.olfgpu_read_batch_states.argtypes = [_i64, _ci, _ip, _dp]
     L.olfgpu_begin_batch_install.argtypes = [_i64, _ip, _ci]
     L.olfgpu_read_handed_back_slots.argtypes = [_i64, _ip, _ci, _ip]
@@ -243,11 +258,38 @@ class Structure:
 class BatchContext:
     """BatchSolveNative: a bank of ``n_scenarios`` lanes on one structure."""
 
-    def __init__(self, structure: Structure, n_scenarios: int, mode: int = BATCHED_LU, rl=None):
+    def __init__(self, structure: Structure, n_scenarios: int, mode: int = BATCHED_LU, rl=None, ds=None):
+        """``rl``: reactive-limit tables (packing.ReactiveLimits); ``ds``: bus-level distributed-slack participants
+        (packing.DistributedSlack, static factors), which go through olfgpu_create_batch_context_full."""
         L = load()
         self.structure = structure
         self.n_scenarios = n_scenarios
         h = _i64(0)
+        if ds is not None:
+            self._ds = [_c(ds.row, np.int32), _c(ds.factor, np.float64), _c(ds.base_target, np.float64),
+                        _c(ds.max_delta, np.float64), _c(ds.min_delta, np.float64)]
+            d = self._ds
+            nd = int(d[0].size)
+            if rl is not None:
+                self._rl = [_c(rl.voltage_row, np.int32), _c(rl.min_q, np.float64), _c(rl.max_q, np.float64),
+                            _c(rl.load_q, np.float64), _c(rl.target_v, np.float64)]
+                r = self._rl
+                nr = int(r[0].size)
+                rl_args = [_p(r[0]), nr, _p(r[1]), nr, _p(r[2]), nr, _p(r[3]), nr, _p(r[4]), nr]
+            else:
+                rl_args = [None, 0] * 5
+            _check(L.olfgpu_create_batch_context_full(
+                structure.handle, n_scenarios, mode, *rl_args, None, 0, None, 0,
+                _p(d[0]), nd, _p(d[1]), nd, int(ds.slack_row), float(ds.slack_target_p), _p(d[2]), nd, _p(d[3]), nd,
+                _p(d[4]), nd, 0, None, 0, None, 0, 0.0, 0.0, ctypes.byref(h)))
+            self.handle = h.value
+            if rl is not None:       # ReactiveLimitsNative.setBatchReactiveLimitStrongestPvKeys
+                self._keys = [_c(rl.nom_v, np.float64), _c(rl.p_row, np.int32), _c(rl.static_p, np.float64),
+                              _c(rl.id_rank, np.int32)]
+                k = self._keys
+                _check(L.olfgpu_set_reactive_limit_strongest_pv_keys(self.handle, _p(k[0]), _p(k[1]), _p(k[2]),
+                                                                      _p(k[3]), int(k[0].size)))
+            return
         if rl is not None:
             self._rl = [_c(rl.voltage_row, np.int32), _c(rl.min_q, np.float64), _c(rl.max_q, np.float64),
                         _c(rl.load_q, np.float64), _c(rl.target_v, np.float64), _c(rl.nom_v, np.float64),
@@ -292,7 +334,8 @@ class BatchContext:
               out: Optional[np.ndarray] = None, conv_eps_per_eq: float = 0.0, svs_mode: int = SVS_NONE,
               max_dv: float = 0.1, max_dphi: float = 0.17453292519943295, var_type=None,
               skip_reactive_limits: bool = False, unsupported: Optional[dict] = None,
-              pause_at_ended: int = 0) -> np.ndarray:
+              pause_at_ended: int = 0, slack_dist_tol: float = 1e-6,
+              reject_slack_distribution_failure: bool = False) -> np.ndarray:
         """Per scenario [x(n), iterations, ||F||inf, status] through the full reference-shaped entry
         (BatchSolveNative.solveBatchContext, olfgpu_solve_batch_context_full).  ``unsupported`` maps the name of an
         argument in UNSUPPORTED_SOLVE_ARRAYS to an array passed as given (the engine rejects non-empty ones)."""
@@ -323,10 +366,11 @@ class BatchContext:
         _check(load().olfgpu_solve_batch_context_full(
             self.handle, _p(x0b), ln(x0b), _p(tb), ln(tb), _p(rme) if rme.size else None, int(rme.size), _p(bm), ln(bm),
             _p(disabled), ns, disabled.shape[1], _p(toi) if toi.size else None, int(toi.size),
-            _p(tov) if tov.size else None, int(tov.size), *extra, max_iter, tol, reactive_limit_tol, 0.0,
+            _p(tov) if tov.size else None, int(tov.size), *extra, max_iter, tol, reactive_limit_tol, slack_dist_tol,
             conv_eps_per_eq, svs_mode, max_dv, max_dphi, _p(vt), ln(vt), _p(x0f), ln(x0f),
             None, 0, None, 0, None, 0, None, 0, None, 0,
-            max_outer, max_pq_pv_switch, 0, 1 if skip_reactive_limits else 0, 0, None, 0, None, 0, pause_at_ended,
+            max_outer, max_pq_pv_switch, 1 if reject_slack_distribution_failure else 0,
+            1 if skip_reactive_limits else 0, 0, None, 0, None, 0, pause_at_ended,
             _p(out)))
         return out
 
@@ -343,6 +387,17 @@ class BatchContext:
         _check(load().olfgpu_solve_batch_context(self.handle, *args, _p(out)))
         return out
 
+    def last_slack_distribution_failures(self) -> np.ndarray:
+        """Per scenario of the last solve, 1 where the distributed slack could not place the whole mismatch."""
+        out = np.zeros(self.n_scenarios, np.uint8)
+        cnt = ctypes.c_int(0)
+        _check(load().olfgpu_last_slack_distribution_failures(self.handle, _p(out), ctypes.byref(cnt)))
+        return out
+
+    def set_outer_loops(self, distributed_slack: bool = True, reactive_limits: bool = True):
+        """DriverNative.setBatchOuterLoops: each outer loop on or off for the following solves."""
+        _check(load().olfgpu_set_outer_loops(self.handle, 1 if distributed_slack else 0, 1 if reactive_limits else 0))
+
     def set_realistic_check(self, row_checked=None, min_v: float = 0.0, max_v: float = 0.0, enabled: bool = True):
         """ReactiveLimitsNative.setBatchRealisticCheck: rows [n] whose converged voltage must lie in [min_v, max_v]."""
         rc = None if row_checked is None else _c(row_checked, np.uint8)
@@ -352,6 +407,10 @@ class BatchContext:
     def set_refinement_bound(self, correction_bound: float = 1e-11):
         """Mixed precision: a scenario near convergence refines until its correction max |d| <= correction_bound."""
         _check(load().olfgpu_set_refinement_bound(self.handle, correction_bound))
+
+    def set_start_polish(self, ratio: float = 1e-2):
+        """Fallback mode: a scenario converged from its own start above ratio * tol takes one more Newton step."""
+        _check(load().olfgpu_set_start_polish(self.handle, ratio))
 
     def set_fp64_restart(self, enable: bool = True):
         """Mixed precision: a scenario whose solve fails restarts once in FP64 (on by default)."""
@@ -395,6 +454,16 @@ class BatchContext:
         d["iterations"] = int(o[6])
         d["factorized_lanes"] = int(o[7])
         return d
+
+    def set_mixed_precision_policy(self, policy: int = 0):
+        """0 MIXED_REFINE: FP32 LU + FP64 refinement near convergence; 1 MIXED_FP64_NEAR: iterations with a scenario
+        near convergence run in FP64."""
+        _check(load().olfgpu_set_mixed_precision_policy(self.handle, policy))
+
+    def last_fp64_iterations(self) -> int:
+        v = ctypes.c_int(0)
+        _check(load().olfgpu_last_fp64_iterations(self.handle, ctypes.byref(v)))
+        return v.value
 
     def set_mixed_precision_controls(self, refine_below: float = 1e-2, growth_limit: float = 1e4):
         """Mixed precision: refinement only below refine_below; FP64 refactor above growth_limit pivot growth."""
@@ -441,6 +510,37 @@ class BatchContext:
                            _c(disabled, np.uint8))
         _check(load().olfgpu_debug_fill(self.handle, _p(xf), _p(tb), _p(bm), _p(dis), _p(J), _p(F)))
         return J, F
+
+    def linear_solve_transposed(self, csr_vals, rhs=None, rhs_t=None, precision: int = FP64):
+        """BatchedLuNative.factorizeAndSolveTransposed: one factorization of each J, then J x = rhs and J^T y = rhs_t
+        on its factors; returns (x, y) (None where the right-hand side is None)."""
+        s = self.structure
+        v = _c(csr_vals, np.float64)
+        r = None if rhs is None else _c(rhs, np.float64)
+        rt = None if rhs_t is None else _c(rhs_t, np.float64)
+        x = None if r is None else np.zeros((self.n_scenarios, s.n))
+        y = None if rt is None else np.zeros((self.n_scenarios, s.n))
+        _check(load().olfgpu_linear_solve_transposed(self.handle, _p(v), _p(r), _p(rt), precision, _p(x), _p(y)))
+        return x, y
+
+    def screen_violations(self, elem_id, group_ptr, group_side, group_qty, lim_ptr, lim_threshold, bus_vrow=None,
+                          bus_high=None, bus_low=None, realistic: bool = False, min_v: float = 0.0, max_v: float = 0.0,
+                          band: float = 1e-7, capacity: int = 64):
+        """Violation candidates of the last solve (olfgpu_screen_violations): per scenario the sorted record ids, and
+        the per-scenario counts (above capacity: truncated)."""
+        a = [_c(v, np.int32) for v in (elem_id, group_ptr, group_side, group_qty, lim_ptr)]
+        lt = _c(lim_threshold, np.float64)
+        nb = 0 if bus_vrow is None else len(bus_vrow)
+        br = _c(np.zeros(0) if bus_vrow is None else bus_vrow, np.int32)
+        bh = _c(np.zeros(0) if bus_high is None else bus_high, np.float64)
+        bl = _c(np.zeros(0) if bus_low is None else bus_low, np.float64)
+        rec = np.zeros((self.n_scenarios, capacity), np.int32)
+        cnt = np.zeros(self.n_scenarios, np.int32)
+        _check(load().olfgpu_screen_violations(self.handle, len(elem_id), *[_p(v) if v.size else None for v in a],
+                                               _p(lt) if lt.size else None, nb, _p(br) if nb else None,
+                                               _p(bh) if nb else None, _p(bl) if nb else None, 1 if realistic else 0,
+                                               min_v, max_v, band, capacity, _p(rec), _p(cnt)))
+        return [list(rec[s, :min(cnt[s], capacity)]) for s in range(self.n_scenarios)], cnt
 
     def debug_linear_solve(self, csr_vals, rhs, precision: int = FP64):
         s = self.structure

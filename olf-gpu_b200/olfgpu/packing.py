@@ -51,6 +51,36 @@ class ReactiveLimits:
 
 
 @dataclasses.dataclass
+class DistributedSlack:
+    """Bus-level distributed-slack participants with static factors (the reference's GpuDistributedSlackFactorMode
+    STATIC, DistributedSlackNative tables): per participating bus its P row, factor, base target P and the bounds of
+    its target's move; the slack bus's angle row, whose closed-branch P is compared with slack_target_p."""
+    row: np.ndarray              # int32 [nDs]  the bus's P row (2b)
+    factor: np.ndarray           # float64 [nDs] participation factor (normalised by the engine)
+    base_target: np.ndarray      # float64 [nDs] target P before any distribution
+    max_delta: np.ndarray        # float64 [nDs] largest upward move of the target
+    min_delta: np.ndarray        # float64 [nDs] largest downward move (<= 0)
+    slack_row: int
+    slack_target_p: float
+
+
+def distributed_slack(g: Grid, p: "Packed") -> DistributedSlack:
+    """Generator buses other than the slack share the slack's mismatch in proportion to their Pmax, within
+    [0, Pmax] of generation (the P_MAX balance type with static factors)."""
+    nb = g.n_bus
+    pmax = np.zeros(nb)
+    pgen = np.zeros(nb)
+    np.add.at(pmax, g.gen_bus, g.gen_pmax)
+    np.add.at(pgen, g.gen_bus, g.gen_p)
+    buses = np.array(sorted(set(int(b) for b in g.gen_bus) - {int(g.slack)}), dtype=np.int64)
+    rows = (2 * buses).astype(np.int32)
+    slack_p = pgen[g.slack] - float(g.load_p[g.load_bus == g.slack].sum())
+    return DistributedSlack(row=rows, factor=pmax[buses].copy(), base_target=p.target[rows].copy(),
+                            max_delta=pmax[buses] - pgen[buses], min_delta=-pgen[buses],
+                            slack_row=int(2 * g.slack), slack_target_p=float(slack_p))
+
+
+@dataclasses.dataclass
 class Packed:
     n: int
     cb_params: np.ndarray        # float64 [nCb, 8]

@@ -889,19 +889,85 @@ static int reactive_limits_check(const oracle_rl *rl, int n, const double *x, co
     return 0;
 }
 
+/* Distributed-slack participants (bus level) of the batched solve (NULL: none). */
+typedef struct {
+    int n_ds;
+    const int *row;              /* participants' P rows */
+    const double *factor;        /* participation factors (normalised to sum 1 by the solve) */
+    const double *base, *max_delta, *min_delta;
+    int slack_row;               /* the slack bus's angle row: its closed-branch P is in qbuf there */
+    double slack_target_p;
+    double dist_tol;             /* slackBusPMaxMismatch (pu) */
+    int reject;                  /* a failed distribution ends the scenario REJECTED */
+} oracle_ds;
+
+#define P_RESIDUE_EPS 1e-5
+
+/* distributed_slack.cu:211-616 (bus level), after a converged solve: the slack's closed-branch P minus its target
+ * is the mismatch; above dist_tol every participant resets to its base target and the whole amount is water-filled
+ * over them in proportion to their factors within their bounds.  Returns 1 when the targets moved by more than
+ * 0.9 P_RESIDUE_EPS (the scenario re-solves); *failed when more than P_RESIDUE_EPS stayed unplaced. */
+static int distributed_slack_check(const oracle_ds *ds, const double *factor, const double *qbuf, double *target,
+                                   double *prev, int *failed)
+{
+    *failed = 0;
+    double mis = qbuf[ds->slack_row] - ds->slack_target_p;
+    if (!(fabs(mis) > ds->dist_tol && fabs(mis) > P_RESIDUE_EPS)) return 0;
+    double absorbed = 0.0;
+    for (int i = 0; i < ds->n_ds; i++) {
+        absorbed += target[ds->row[i]] - ds->base[i];
+        prev[i] = target[ds->row[i]];
+        target[ds->row[i]] = ds->base[i];
+    }
+    double rem = mis + absorbed;
+    for (int it = 0; it < ds->n_ds && fabs(rem) > P_RESIDUE_EPS; it++) {
+        double fsum = 0.0;
+        for (int i = 0; i < ds->n_ds; i++) {
+            double cum = target[ds->row[i]] - ds->base[i];
+            int sat = rem > 0 ? cum >= ds->max_delta[i] : cum <= ds->min_delta[i];
+            if (!sat) fsum += factor[i];
+        }
+        if (fsum <= 0.0) break;
+        double done = 0.0;
+        for (int i = 0; i < ds->n_ds; i++) {
+            double cum = target[ds->row[i]] - ds->base[i];
+            int sat = rem > 0 ? cum >= ds->max_delta[i] : cum <= ds->min_delta[i];
+            if (sat) continue;
+            double next = fmin(fmax(cum + rem * (factor[i] / fsum), ds->min_delta[i]), ds->max_delta[i]);
+            if (next != cum) {
+                target[ds->row[i]] = ds->base[i] + next;
+                done += next - cum;
+            }
+        }
+        rem -= done;
+    }
+    double shift = 0.0;
+    for (int i = 0; i < ds->n_ds; i++) shift += fabs(target[ds->row[i]] - prev[i]);
+    *failed = fabs(rem) > P_RESIDUE_EPS;
+    return shift > 0.9 * P_RESIDUE_EPS;
+}
+
 /*
  * Batched N-1 solve: scenario s starts from x0 (x0_stride 0: one shared start; n: one per scenario), the base
  * targets and row modes, and disables the elements flagged in disabled[s * n_elements ...].
  * out: per scenario [x(n), iterations, ||F||inf, status] (batch_solve_jni.cu:308-337).
  * Reactive limits: rl may be NULL; max_outer bounds the Newton restarts.  Returns 0.
  */
-int oracle_solve_batch_ex(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
+int oracle_solve_batch_ds(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
                           const int *mode_base, const unsigned char *disabled, int n_elements, int max_iter, double tol,
                           const oracle_rl *rl, double rl_tol, int max_outer, int max_switch, int threads,
-                          const oracle_opts *opts, double *out)
+                          const oracle_opts *opts, const oracle_ds *ds, double *out)
 {
     const oracle_structure *s = o->s;
     const int n = s->n;
+    /* the factors normalised as the engine does: a plain sum in order, then each divided by it */
+    const int nds = ds ? ds->n_ds : 0;
+    double *dsf = (double *)malloc(sizeof(double) * ((size_t)nds + 1));
+    {
+        double fsum = 0.0;
+        for (int i = 0; i < nds; i++) fsum += ds->factor[i];
+        for (int i = 0; i < nds; i++) dsf[i] = ds->factor[i] / fsum;
+    }
 #ifdef _OPENMP
     if (threads > 0) omp_set_num_threads(threads);
 #else
@@ -921,6 +987,7 @@ int oracle_solve_batch_ex(oracle_solver *o, int ns, const double *x0, int x0_str
         signed char *lt = (signed char *)malloc((size_t)nrl + 1), *sc = (signed char *)malloc((size_t)nrl + 1),
                     *ps = (signed char *)malloc((size_t)nrl + 1), *sm = (signed char *)malloc((size_t)nrl + 1);
         double *st = (double *)malloc(sizeof(double) * ((size_t)nrl + 1));
+        double *dsprev = (double *)malloc(sizeof(double) * ((size_t)nds + 1));
 #pragma omp for schedule(dynamic, 1)
         for (int sc_i = 0; sc_i < ns; sc_i++) {
             double *x = out + (size_t)sc_i * (n + 3);
@@ -935,7 +1002,17 @@ int oracle_solve_batch_ex(oracle_solver *o, int ns, const double *x0, int x0_str
                 status = newton(s, g, x, target, mode, dis, max_iter, tol, &iters, &nrm, vals, ax, F, dx, qbuf,
                                 outer == 0, ns == 1, opts);
                 total += iters;
-                if (status != ST_CONVERGED || nrl == 0 || outer >= max_outer) break;
+                if (status != ST_CONVERGED || (nrl == 0 && nds == 0) || outer >= max_outer) break;
+                if (nds > 0) {   /* distributed slack first, then reactive limits (the outer-loop order) */
+                    int failed = 0;
+                    int moved = distributed_slack_check(ds, dsf, qbuf, target, dsprev, &failed);
+                    if (failed && ds->reject) {
+                        status = ST_REJECTED;
+                        break;
+                    }
+                    if (moved) continue;
+                }
+                if (nrl == 0) break;
                 if (!reactive_limits_check(rl, n, x, qbuf, mode, target, lt, sc, ps, sm, st, rl_tol, max_switch)) break;
             }
             if (status == ST_CONVERGED && unrealistic(opts, n, x)) status = ST_UNREALISTIC;
@@ -945,9 +1022,19 @@ int oracle_solve_batch_ex(oracle_solver *o, int ns, const double *x0, int x0_str
         }
         glu_free(g);
         free(vals); free(ax); free(F); free(dx); free(qbuf); free(target); free(mode);
-        free(lt); free(sc); free(ps); free(sm); free(st);
+        free(lt); free(sc); free(ps); free(sm); free(st); free(dsprev);
     }
+    free(dsf);
     return 0;
+}
+
+int oracle_solve_batch_ex(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
+                          const int *mode_base, const unsigned char *disabled, int n_elements, int max_iter, double tol,
+                          const oracle_rl *rl, double rl_tol, int max_outer, int max_switch, int threads,
+                          const oracle_opts *opts, double *out)
+{
+    return oracle_solve_batch_ds(o, ns, x0, x0_stride, target_base, mode_base, disabled, n_elements, max_iter, tol,
+                                 rl, rl_tol, max_outer, max_switch, threads, opts, NULL, out);
 }
 
 int oracle_solve_batch(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
@@ -969,5 +1056,37 @@ int oracle_linear_solve(oracle_solver *o, const double *vals, const double *b, d
     if (rc == 0) glu_solve(g, b, z);
     free(ax);
     glu_free(g);
+    return rc;
+}
+
+/* Solve the transposed system J^T z = b with the oracle LU on the explicit transpose (tests of the engine's transposed
+ * solve on its own factors, lu/transposed_solve.cuh).  Returns 0 or -1 (singular). */
+int oracle_linear_solve_transposed(oracle_solver *o, const double *vals, const double *b, double *z)
+{
+    const oracle_structure *s = o->s;
+    const int n = s->n, nnz = s->nnz;
+    int *tp = (int *)calloc((size_t)n + 1, sizeof(int));
+    int *ti = (int *)malloc(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1));
+    double *tv = (double *)malloc(sizeof(double) * (size_t)(nnz > 0 ? nnz : 1));
+    int *fill = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    int *perm = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    for (int k = 0; k < nnz; k++) tp[s->col_idx[k] + 1]++;
+    for (int r = 0; r < n; r++) tp[r + 1] += tp[r];
+    for (int r = 0; r < n; r++) fill[r] = tp[r];
+    for (int r = 0; r < n; r++)                       /* rows ascending: each transposed row's columns ascend */
+        for (int k = s->row_ptr[r]; k < s->row_ptr[r + 1]; k++) {
+            int q = fill[s->col_idx[k]]++;
+            ti[q] = r;
+            tv[q] = vals[k];
+        }
+    min_degree(n, tp, ti, perm);
+    glu *g = glu_new(n, tp, ti, perm);
+    double *ax = (double *)malloc(sizeof(double) * (size_t)(nnz > 0 ? nnz : 1));
+    for (int k = 0; k < nnz; k++) ax[g->map[k]] = tv[k];
+    int rc = glu_factor(g, ax);
+    if (rc == 0) glu_solve(g, b, z);
+    free(ax);
+    glu_free(g);
+    free(tp); free(ti); free(tv); free(fill); free(perm);
     return rc;
 }

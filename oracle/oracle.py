@@ -79,7 +79,9 @@ def lib():
                                          ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int, _dp]
         L.oracle_solve_batch_ex.argtypes = L.oracle_solve_batch.argtypes[:-1] + [ctypes.c_void_p, _dp]
+        L.oracle_solve_batch_ds.argtypes = L.oracle_solve_batch.argtypes[:-1] + [ctypes.c_void_p, ctypes.c_void_p, _dp]
         L.oracle_linear_solve.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
+        L.oracle_linear_solve_transposed.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
         L.oracle_closed_branch.argtypes = [_dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                            ctypes.c_double, ctypes.c_double, _dp]
         L.oracle_open_branch.argtypes = [_dp, ctypes.c_double, ctypes.c_double, _dp]
@@ -91,6 +93,12 @@ def lib():
 class _Rl(ctypes.Structure):
     _fields_ = [("n_rl", ctypes.c_int), ("voltage_row", _ip), ("min_q", _dp), ("max_q", _dp), ("load_q", _dp),
                 ("target_v", _dp), ("nom_v", _dp), ("static_p", _dp), ("p_row", _ip), ("id_rank", _ip)]
+
+
+class _Ds(ctypes.Structure):
+    _fields_ = [("n_ds", ctypes.c_int), ("row", _ip), ("factor", _dp), ("base", _dp), ("max_delta", _dp),
+                ("min_delta", _dp), ("slack_row", ctypes.c_int), ("slack_target_p", ctypes.c_double),
+                ("dist_tol", ctypes.c_double), ("reject", ctypes.c_int)]
 
 
 class _Opts(ctypes.Structure):
@@ -158,12 +166,23 @@ class Structure:
             raise RuntimeError("oracle LU: singular")
         return z
 
+    def linear_solve_transposed(self, vals, b):
+        """z with J^T z = b (J given by its CSR values)."""
+        z = np.zeros(self.p.n)
+        vals, b = _arr(vals, np.float64), _arr(b, np.float64)
+        rc = lib().oracle_linear_solve_transposed(self.solver, _ptr(vals), _ptr(b), _ptr(z))
+        if rc != 0:
+            raise RuntimeError("oracle LU: singular")
+        return z
+
     def solve_batch(self, x0, disabled, max_iter=15, tol=1e-8, target=None, mode=None, reactive_limits=False,
                     rl_tol=1e-4, max_outer=20, max_switch=3, threads=0, conv_eps_per_eq=0.0, svs_mode=0,
-                    max_dv=0.1, max_dphi=0.17453292519943295, var_type=None, v_check=None, min_v=0.0, max_v=0.0):
+                    max_dv=0.1, max_dphi=0.17453292519943295, var_type=None, v_check=None, min_v=0.0, max_v=0.0,
+                    distributed_slack=None, slack_dist_tol=1e-6, reject_slack_distribution_failure=False):
         """Per scenario [x(n), iterations, ||F||inf, status]; x0 is [n] (shared) or [nS, n].  conv_eps_per_eq > 0:
         OLF's 2-norm stopping test; svs_mode 2: MAX_VOLTAGE_CHANGE with var_type [n]; v_check [n]: the realistic-voltage
-        rows checked against [min_v, max_v] at convergence."""
+        rows checked against [min_v, max_v] at convergence; distributed_slack (packing.DistributedSlack): the bus-level
+        distributed-slack outer loop, before the reactive-limit check."""
         p = self.p
         disabled = _arr(disabled, np.uint8)
         ns = disabled.shape[0]
@@ -185,11 +204,22 @@ class Structure:
         vc = None if v_check is None else _arr(v_check, np.uint8)
         opts = _Opts(conv_eps_per_eq, svs_mode, max_dv, max_dphi, None if vt is None else _ptr(vt),
                      None if vc is None else _ptr(vc), min_v, max_v)
-        lib().oracle_solve_batch_ex(self.solver, ns, _ptr(x0), stride, _ptr(target), _ptr(mode), _ptr(disabled),
+        ds_struct = None
+        if distributed_slack is not None:
+            d = distributed_slack
+            self._ds_keep = [_arr(d.row, np.int32), _arr(d.factor, np.float64), _arr(d.base_target, np.float64),
+                             _arr(d.max_delta, np.float64), _arr(d.min_delta, np.float64)]
+            k = self._ds_keep
+            ds_struct = _Ds(k[0].shape[0], _ptr(k[0]), _ptr(k[1]), _ptr(k[2]), _ptr(k[3]), _ptr(k[4]),
+                            int(d.slack_row), float(d.slack_target_p), slack_dist_tol,
+                            1 if reject_slack_distribution_failure else 0)
+        lib().oracle_solve_batch_ds(self.solver, ns, _ptr(x0), stride, _ptr(target), _ptr(mode), _ptr(disabled),
                                     disabled.shape[1], max_iter, tol,
                                     ctypes.cast(ctypes.pointer(rl_struct), ctypes.c_void_p) if rl_struct else None,
                                     rl_tol, max_outer, max_switch, threads,
-                                    ctypes.cast(ctypes.pointer(opts), ctypes.c_void_p), _ptr(out))
+                                    ctypes.cast(ctypes.pointer(opts), ctypes.c_void_p),
+                                    ctypes.cast(ctypes.pointer(ds_struct), ctypes.c_void_p) if ds_struct else None,
+                                    _ptr(out))
         return out
 
 
@@ -279,3 +309,81 @@ def ref_shunt(params, v):
     p = _arr(params, np.float64)
     ref_lib().olfref_shunt(_ptr(p), v, _ptr(o))
     return o
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# Violation screening (sa/olf_gpu_violations.cu:160-361), restated over host states.
+# ---------------------------------------------------------------------------------------------------------------
+def branch_flows(packed, x, element):
+    """(p1, q1, v1, p2, q2, v2) of one branch element at the states x [nS, n]: closed branches with the closed-branch
+    terms (closed_branch.cuh:161-229), open-ended ones with the connected side's open-branch terms (open_branch.cuh:
+    65-87), NaN on an open side."""
+    ns = x.shape[0]
+    nan = np.full(ns, np.nan)
+    if element < packed.n_cb:
+        y, g1, g2, b1, b2, ksi, r1, a1 = packed.cb_params[element]
+        ix = packed.cb_idx[element]
+        ph1, v1, ph2, v2 = x[:, ix[4]], x[:, ix[5]], x[:, ix[6]], x[:, ix[7]]
+        sk, ck = np.sin(ksi), np.cos(ksi)
+        t1, t2 = ksi - a1 - ph1 + ph2, ksi + a1 + ph1 - ph2
+        p1 = r1 * v1 * (g1 * r1 * v1 + y * r1 * v1 * sk - y * v2 * np.sin(t1))
+        q1 = r1 * v1 * (-b1 * r1 * v1 + y * r1 * v1 * ck - y * v2 * np.cos(t1))
+        p2 = v2 * (g2 * v2 - y * r1 * v1 * np.sin(t2) + y * v2 * sk)
+        q2 = v2 * (-b2 * v2 - y * r1 * v1 * np.cos(t2) + y * v2 * ck)
+        return p1, q1, v1, p2, q2, v2
+    e = element - packed.n_cb
+    y, ksi, g1, b1, g2, b2, r1 = packed.ob_params[e]
+    ix = packed.ob_idx[e]
+    sk, ck = np.sin(ksi), np.cos(ksi)
+    p1 = q1 = v1 = p2 = q2 = v2 = nan
+    if ix[4] >= 0:
+        v1 = x[:, ix[4]]
+        d2 = (g2 + y * sk) ** 2 + (-b2 + y * ck) ** 2
+        p1 = r1 * r1 * v1 * v1 * (g1 + y * y * g2 / d2 + (b2 * b2 + g2 * g2) * y * sk / d2)
+        q1 = -r1 * r1 * v1 * v1 * (b1 + y * y * b2 / d2 - (b2 * b2 + g2 * g2) * y * ck / d2)
+    if ix[5] >= 0:
+        v2 = x[:, ix[5]]
+        d1 = (g1 + y * sk) ** 2 + (-b1 + y * ck) ** 2
+        p2 = v2 * v2 * (g2 + y * y * g1 / d1 + (b1 * b1 + g1 * g1) * y * sk / d1)
+        q2 = -v2 * v2 * (b2 + y * y * b1 / d1 - (b1 * b1 + g1 * g1) * y * ck / d1)
+    return p1, q1, v1, p2, q2, v2
+
+
+def screen_violations(packed, x, disabled, elem_id, group_ptr, group_side, group_qty, lim_ptr, lim_threshold,
+                      bus_vrow, bus_high, bus_low, realistic=False, min_v=0.0, max_v=0.0, band=1e-7, values=None):
+    """Per scenario the sorted candidate ids of the screen (the engine's numbering; see include/olfgpu_b200.h).  With
+    `values` (a list) it also collects (scenario, limit id, value, threshold) of every comparison, for margins."""
+    ns = x.shape[0]
+    n_lim = int(lim_ptr[-1]) if len(lim_ptr) else 0
+    out = [[] for _ in range(ns)]
+    for r, e in enumerate(elem_id):
+        p1, q1, v1, p2, q2, v2 = branch_flows(packed, x, int(e))
+        off = disabled[:, int(e)] != 0
+        for g in range(group_ptr[r], group_ptr[r + 1]):
+            p, q, v = (p1, q1, v1) if group_side[g] == 1 else (p2, q2, v2)
+            with np.errstate(invalid="ignore", divide="ignore"):
+                val = [np.hypot(p, q) / v, np.abs(p), np.sqrt(p * p + q * q)][group_qty[g]]
+            for s in range(ns):
+                if off[s] or np.isnan(val[s]):
+                    continue
+                for l in range(lim_ptr[g], lim_ptr[g + 1]):
+                    t = lim_threshold[l]
+                    if values is not None:
+                        values.append((s, l, float(val[s]), float(t)))
+                    if val[s] > t - abs(t) * band:
+                        out[s].append(l)
+                        if val[s] > t + abs(t) * band:
+                            break
+    nb = len(bus_vrow)
+    for i in range(nb):
+        if bus_vrow[i] < 0:
+            continue
+        vv = x[:, bus_vrow[i]]
+        for s in range(ns):
+            if vv[s] > bus_high[i] - abs(bus_high[i]) * band:
+                out[s].append(n_lim + 2 * i)
+            if vv[s] < bus_low[i] + abs(bus_low[i]) * band:
+                out[s].append(n_lim + 2 * i + 1)
+            if realistic and (vv[s] < min_v or vv[s] > max_v):
+                out[s].append(n_lim + 2 * nb + i)
+    return [sorted(o) for o in out]

@@ -452,3 +452,30 @@ def test_subtree_bins_match_oracle(engine_lib, oracle_mod, precision, name):
         if precision == 0:
             assert np.array_equal(r[5][:, -1], r[4][:, -1])
             assert np.max(np.abs(r[5][:, :p.n] - r[4][:, :p.n])) < 1e-11
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-9), (1, 2e-3)])
+@pytest.mark.parametrize("name,plan", [("grid2000", 0), ("grid2000", 16), ("grid9241", 16)])
+def test_transposed_solve_matches_oracle(engine_lib, oracle_mod, precision, tol, name, plan):
+    """J^T y = c on the factors of J (the adjoint solve, lu/transposed_solve.cuh): against the oracle's LU of the
+    explicit transpose; the plain solve of the same call against the oracle's LU of J."""
+    from olfgpu import native
+    g, p = grid(name)
+    ns = 24
+    s = native.Structure(p, ordering=plan)
+    ctx = native.BatchContext(s, ns)
+    x = _perturbed_states(p, ns, 4, 0.02)
+    st = oracle_mod.Structure(p)
+    zero = np.zeros(p.n_elements, np.uint8)
+    J = np.stack([st.fill(x[k], p.target, p.base_row_mode, zero)[0] for k in range(ns)])
+    rng = np.random.default_rng(5)
+    rhs, rhs_t = rng.standard_normal((ns, p.n)), rng.standard_normal((ns, p.n))
+    xs, ys = ctx.linear_solve_transposed(J, rhs, rhs_t, precision)
+    for k in range(0, ns, 5):
+        zo = st.linear_solve(J[k], rhs[k])
+        yo = st.linear_solve_transposed(J[k], rhs_t[k])
+        assert np.max(np.abs(xs[k] - zo)) / np.max(np.abs(zo)) < tol
+        assert np.max(np.abs(ys[k] - yo)) / np.max(np.abs(yo)) < tol
+    # adjoint identity: <y, J x> = <J^T y, x> = <c, x> for the solved pairs
+    _, y_only = ctx.linear_solve_transposed(J, None, rhs_t, precision)
+    assert np.array_equal(y_only, ys)

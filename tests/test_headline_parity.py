@@ -34,7 +34,10 @@ def _check(r, ref, n):
     assert d[:, 0::2].max() <= STATE_TOL, ("Va", float(d[:, 0::2].max()))
 
 
-def test_learned_mixed_matches_oracle_on_the_benchmark_batch(engine_lib, headline):
+@pytest.mark.parametrize("policy", [0, 1])
+def test_learned_mixed_matches_oracle_on_the_benchmark_batch(engine_lib, headline, policy):
+    """Both mixed-precision policies; the scenarios that converge from their learned start take the polishing step
+    (on by default), the others run from the base start as the oracle does."""
     import torch
     from olfgpu import native
     from olfgpu.learned_start import LearnedStart
@@ -43,6 +46,7 @@ def test_learned_mixed_matches_oracle_on_the_benchmark_batch(engine_lib, headlin
     s = native.Structure(p, native.PLAN_DENSE_FRONT)
     ctx = native.BatchContext(s, ns)
     ctx.set_linear_solver_settings(native.MIXED, 3)
+    ctx.set_mixed_precision_policy(policy)
     ctx.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
     learned = LearnedStart.load(CHECKPOINT, g)
     x0_dev = torch.empty((ns, p.n), dtype=torch.float64, device="cuda")
@@ -52,6 +56,41 @@ def test_learned_mixed_matches_oracle_on_the_benchmark_batch(engine_lib, headlin
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, p.outage_masks(outs))
     _check(r, ref, p.n)
     ctx.set_device_start(None)
+
+
+def test_polishing_step_brings_learned_lanes_next_to_the_solution(engine_lib, headline):
+    """Without the polishing step a scenario that converged from its learned start may stop anywhere in the tolerance
+    ball; with it, every converged state lies within 1e-9 of the FP64 engine's polished base-start state."""
+    import torch
+    from olfgpu import native
+    from olfgpu.learned_start import LearnedStart
+    g, p, outs, ref = headline
+    ns = outs.shape[0]
+    dis = p.outage_masks(outs)
+    s = native.Structure(p, native.PLAN_DENSE_FRONT)
+    learned = LearnedStart.load(CHECKPOINT, g)
+    x0_dev = torch.empty((ns, p.n), dtype=torch.float64, device="cuda")
+    learned.predict_device(p, p.x_base, outs, out=x0_dev)
+    out = {}
+    for ratio in (0.0, 1e-2):
+        ctx = native.BatchContext(s, ns)
+        ctx.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
+        ctx.set_fallback_start(True)
+        ctx.set_start_polish(ratio)
+        ctx.set_device_start(x0_dev)
+        out[ratio] = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
+        ctx.set_device_start(None)
+    # the solution itself: the base-start states taken one step further (max |F| far below the tolerance)
+    base = native.BatchContext(s, ns)
+    base.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
+    x_star = base.solve(p.x_base, p.target, p.base_row_mode, dis, x0_full=np.ascontiguousarray(ref[:, :p.n]),
+                        tol=1e-11, max_iter=3)
+    n = p.n
+    conv = (out[1e-2][:, n + 2] == 0) & (x_star[:, n + 2] == 0)
+    assert conv.sum() > 0.9 * ns
+    polished = np.abs(out[1e-2][conv, :n] - x_star[conv, :n]).max()
+    plain = np.abs(out[0.0][conv, :n] - x_star[conv, :n]).max()
+    assert polished <= 1e-9 < plain, (polished, plain)
 
 
 @pytest.mark.parametrize("precision", [0, 1])

@@ -252,7 +252,7 @@ def test_create_context_rejects_monitoring_svc_flags(jni):
 def _solve(jni, jvm, ctx, p, dis, x0_full=None, max_iter=15, tol=1e-8, unsupported=None):
     """BatchSolveNative.solveBatchContext with the reference's argument list."""
     f = _fn(jni, "ac_solver_gpu_BatchSolveNative_solveBatchContext", _vp, 0)
-    f.argtypes = ([_vp, _vp, _i64] + [_vp] * 6 + [_vp] * 13 + [_i32, _f64, _f64, _f64, _f64, _i32, _f64, _f64] +
+    f.argtypes = ([_vp, _vp, _i64] + [_vp] * 6 + [_vp] * 14 + [_i32, _f64, _f64, _f64, _f64, _i32, _f64, _f64] +
                   [_vp] * 7 + [_i32] * 5 + [_vp] * 2 + [_i32])
     ov = [None] * 13
     for k, v in (unsupported or {}).items():
