@@ -360,6 +360,14 @@ int olfgpu_set_fallback_start(int64_t context, int enable);
  * another start than the reference's base start is brought next to the solution, where the base-start trajectory's
  * converged state also lies.  Its iteration count includes the step. */
 int olfgpu_set_start_polish(int64_t context, double polishRatio);
+
+/* Device-resident Newton loop (level schedules 0, 3, 4, 5; no counterpart in the reference, whose driver loop reads
+ * the lane counts on the host every iteration): with enable = 1 a solve runs its whole Newton loop as ONE graph launch.
+ * A conditional WHILE node runs an iteration per pass, and conditional IF / WHILE nodes take the host loop's decisions
+ * between the iteration's phases (lanes left, lanes factorizing, refinement steps, FP64 refactor, scoring).  Small
+ * kernels set them from the lane counts.  The iteration counter caps the loop as the host loop does.  Results are
+ * identical to the host-driven loop. */
+int olfgpu_set_device_loop(int64_t context, int enable);
 int olfgpu_last_fallbacks(int64_t context, unsigned char* fellBack, int* count);
 
 /*
@@ -372,9 +380,11 @@ int olfgpu_last_fallbacks(int64_t context, unsigned char* fellBack, int* count);
  * ([nScenarios_i][n_i + 3], as olfgpu_solve_batch_context; null skips the copy); deviceMs receives the device time
  * from the first install to the last result.  Members' olfgpu_last_solve_stats report their per-scenario iterations
  * afterwards.  olfgpu_set_multi_schedule fixes the tile (lanesPerTile 1, 2, 4 or 8; threads 256 or 512; order 0 as
- * given, 1 the grids with the most buses first) or, with lanesPerTile -1, lets the next solve time every candidate
- * and keep the fastest; olfgpu_get_multi_schedule reports the schedule in force and the timings
- * {lanesPerTile, threads, order, ms} of the last autotune.
+ * given, 1 the grids with the most buses first), or lanesPerTile 0: ONE graph launch whose branches are the members'
+ * device-resident Newton loops (olfgpu_set_device_loop) under their own level schedules, which run concurrently on the
+ * device (any plan, outer loop and precision policy a member supports alone).  With lanesPerTile -1 the next solve
+ * times every candidate and keeps the fastest.  olfgpu_get_multi_schedule reports the schedule in force and the
+ * timings {lanesPerTile, threads, order, ms} of the last autotune.
  */
 int olfgpu_stage_batch_context(int64_t context, const double* x0Base, const double* x0Full, const double* targetBase,
                                const int* baseRowMode, int nRowModeEntries, const int* rowModeEntries,

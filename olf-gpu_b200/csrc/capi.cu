@@ -770,6 +770,10 @@ extern "C" int olfgpu_set_start_polish(int64_t context, double polishRatio) {
     });
 }
 
+extern "C" int olfgpu_set_device_loop(int64_t context, int enable) {
+    return guarded([&] { contextOf(context).deviceLoop = enable != 0; });
+}
+
 extern "C" int olfgpu_set_fp64_restart(int64_t context, int enable) {
     return guarded([&] { contextOf(context).fp64Restart = enable != 0; });
 }
@@ -900,8 +904,13 @@ extern "C" int olfgpu_set_multi_schedule(int64_t multi, int lanesPerTile, int th
             m.autotunePending = true;
             return;
         }
+        if (lanesPerTile == 0) {   // the members' device-resident level-schedule loops, one graph
+            m.lanesPerTile = 0;
+            m.autotunePending = false;
+            return;
+        }
         if (lanesPerTile != 1 && lanesPerTile != 2 && lanesPerTile != 4 && lanesPerTile != 8) {
-            throw std::runtime_error("lanesPerTile must be 1, 2, 4 or 8 (or -1: autotune)");
+            throw std::runtime_error("lanesPerTile must be 0, 1, 2, 4 or 8 (or -1: autotune)");
         }
         if (threads != 256 && threads != 512) throw std::runtime_error("threads must be 256 or 512");
         if (order != 0 && order != 1) throw std::runtime_error("order must be 0 (as given) or 1 (most buses first)");

@@ -785,9 +785,12 @@ std::shared_ptr<DeviceNet> NetStructure::find(int device) {
 BatchContext::~BatchContext() {
     if (graph) cudaGraphExecDestroy(graph);
     if (graphSolve) cudaGraphExecDestroy(graphSolve);
-    for (cudaGraphExec_t gx : {graphFactor, graphResidual, graphCorrect, graph64, graphStep, graphSolveScored,
-                               graphStepScored})
+    for (cudaGraphExec_t gx : {graphFactor, graphResidual, graphCorrect, graph64, graph64All, graphStep,
+                               graphSolveScored, graphStepScored})
         if (gx) cudaGraphExecDestroy(gx);
+    if (loopGraph) cudaGraphExecDestroy(loopGraph);
+    for (cudaStream_t s : loopStreams)
+        if (s) cudaStreamDestroy(s);
     if (hostActive) cudaFreeHost(hostActive);
     if (countReady) cudaEventDestroy(countReady);
     if (hostBitsPinned) cudaFreeHost(hostBitsPinned);
@@ -1141,6 +1144,13 @@ DevBatch fp64View(BatchContext& ctx) {
     return b;
 }
 
+// Every factorizing lane in FP64 (an FP64 iteration of the MIXED_FP64_NEAR policy).
+DevBatch fp64AllView(BatchContext& ctx) {
+    DevBatch b = fp64View(ctx);
+    b.laneMask = nullptr;
+    return b;
+}
+
 }  // namespace
 
 void captureIteration(BatchContext& ctx) {
@@ -1162,6 +1172,7 @@ void captureIteration(BatchContext& ctx) {
     dropGraph(ctx.graphResidual);
     dropGraph(ctx.graphCorrect);
     dropGraph(ctx.graph64);
+    dropGraph(ctx.graph64All);
     dropGraph(ctx.graphStep);
     dropGraph(ctx.graphSolveScored);
     dropGraph(ctx.graphStepScored);
@@ -1246,6 +1257,23 @@ void launchFp64Redo(BatchContext& ctx) {
     OLF_CUDA(cudaGraphLaunch(ctx.graph64, ctx.stream));
 }
 
+// MIXED_FP64_NEAR: the FP64 factorization and solves of every factorizing lane (captured on first use).
+void launchFp64All(BatchContext& ctx) {
+    if (!ctx.graph64All) {
+        const DeviceNet& dn = *ctx.dn;
+        const DevBatch b64 = fp64AllView(ctx);
+        const Hybrid hy = ctx.hybrid();
+        const Hybrid* hp = ctx.useHybrid() ? &hy : nullptr;
+        cudaStream_t st = ctx.stream;
+        ctx.graph64All = captureInto(st, [&] {
+            launchFactor(dn.view, b64, dn.levelPtr.data(), dn.levelSplit.data(),
+                         static_cast<int>(dn.levelPtr.size()) - 1, false, hp, st);
+            launchSolve(dn.view, b64, dn.fwd(), dn.bwd(), false, false, hp, st);
+        });
+    }
+    OLF_CUDA(cudaGraphLaunch(ctx.graph64All, ctx.stream));
+}
+
 // One Newton iteration launched phase by phase with CUDA events between the phases (the same kernels in the same
 // order as the two captured graphs); the phase times and the lanes that factorized accumulate in the context.
 // Returns false when no lane is left iterating.
@@ -1308,8 +1336,7 @@ void coopIteration(BatchContext& ctx) {
     const DevBatch b = ctx.batch();
     if (fp64Iteration(ctx)) {
         ctx.fp64Iterations++;
-        launchPromoteFp64(b, st);
-        const DevBatch b64 = fp64View(ctx);
+        const DevBatch b64 = fp64AllView(ctx);
         factorPhase(ctx, b64, false);
         solvePhase(ctx, b64, false, false);
         if (scoreDue(ctx)) launchScoreSolve(dn.view, b, ctx.cfg, st);
@@ -1366,8 +1393,7 @@ bool phaseTimedIteration(BatchContext& ctx) {
     const int solving = ctx.hostActive[1];
     if (live && solving > 0 && fp64Iteration(ctx)) {
         OLF_CUDA(cudaEventRecord(ev[2], st));
-        launchPromoteFp64(b, st);
-        const DevBatch b64 = fp64View(ctx);
+        const DevBatch b64 = fp64AllView(ctx);
         factorPhase(ctx, b64, false);
         OLF_CUDA(cudaEventRecord(ev[3], st));
         solvePhase(ctx, b64, false, false);
@@ -1531,6 +1557,207 @@ void selectStarts(BatchContext& ctx) {
     chooseStartKernel<<<static_cast<unsigned>((all + 255) / 256), 256, 0, st>>>(b, saved, normOwn, normBase, n);
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// The Newton loop inside one graph launch: a conditional WHILE node runs one iteration per pass of its body, and the
+// decisions the host loop takes between the iteration's graphs (any lane left, any lane factorizing, refinement
+// steps, FP64 refactor, scoring) are conditional IF / WHILE nodes whose handles small kernels set from the lane
+// counts.  The iteration counter bounds the loop at the same cap as the host loop.  loopState ints: 0 iterations,
+// 1 refinement steps of the iteration, 2 this iteration factorizes in FP32 (mixed) or at all (FP64), 3 it factorizes
+// in FP64 (MIXED_FP64_NEAR), 4 FP64 iterations so far.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void loopResetKernel(int* state) {
+    for (int i = 0; i < 8; i++) state[i] = 0;
+}
+
+__global__ void loopCondKernel(cudaGraphConditionalHandle hMain, cudaGraphConditionalHandle hWork,
+                               cudaGraphConditionalHandle hScore, cudaGraphConditionalHandle hNear, const int* nActive,
+                               int* state, int cap, int mixed, int nearPolicy) {
+    const int k = ++state[0];
+    const bool live = nActive[0] > 0;
+    const bool solving = live && nActive[1] > 0;
+    const bool near = mixed && nearPolicy && solving && nActive[2] > 0;
+    const bool work = solving && !near;
+    state[1] = 0;
+    state[2] = work ? 1 : 0;
+    state[3] = near ? 1 : 0;
+    state[4] += near ? 1 : 0;
+    cudaGraphSetConditional(hMain, live && k < cap ? 1u : 0u);
+    cudaGraphSetConditional(hWork, work ? 1u : 0u);
+    cudaGraphSetConditional(hScore, solving && nActive[4] > 0 ? 1u : 0u);
+    if (mixed) cudaGraphSetConditional(hNear, near ? 1u : 0u);
+}
+
+// Mixed precision, after the FP32 factorization and solves: refinement while some lane is below refineBelow, then
+// the FP64 refactor of the lanes the FP32 factorization flagged
+__global__ void loopMixedKernel(cudaGraphConditionalHandle hRefine, cudaGraphConditionalHandle hRedo,
+                                const int* nActive, const int* state, int refineSteps) {
+    const bool far = state[2] != 0;
+    cudaGraphSetConditional(hRefine, far && refineSteps > 0 && nActive[2] > 0 ? 1u : 0u);
+    cudaGraphSetConditional(hRedo, far && nActive[3] > 0 ? 1u : 0u);
+}
+
+__global__ void refineCondKernel(cudaGraphConditionalHandle hRefine, const int* nActive, int* state, int refineSteps) {
+    const int r = ++state[1];
+    cudaGraphSetConditional(hRefine, nActive[2] > 0 && r < refineSteps ? 1u : 0u);
+}
+
+// A conditional node after the capture's current dependencies on st; returns its body graph.
+cudaGraph_t addConditional(cudaStream_t st, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type) {
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaGraph_t cg;
+    OLF_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = type;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    OLF_CUDA(cudaGraphAddNode(&node, cg, deps, nd, &p));
+    OLF_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    return p.conditional.phGraph_out[0];
+}
+
+// Captures the launches fn makes on stream cs into graph g (a conditional node's body).
+void captureBody(cudaStream_t cs, cudaGraph_t g, const std::function<void(cudaStream_t)>& fn) {
+    OLF_CUDA(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    fn(cs);
+    cudaGraph_t out;
+    OLF_CUDA(cudaStreamEndCapture(cs, &out));
+}
+
+cudaGraphConditionalHandle newHandle(cudaGraph_t owner) {
+    cudaGraphConditionalHandle h;
+    OLF_CUDA(cudaGraphConditionalHandleCreate(&h, owner, 0, cudaGraphCondAssignDefault));
+    return h;
+}
+
+// Appends one context's device-resident Newton loop to graph g as a branch with no dependencies: the loop state reset,
+// the WHILE node, the cap of lanes still iterating, and (withResults) the scenario-major result gather.  Three
+// capture streams: cs[0] for the branch, cs[1] for the WHILE body, cs[2] for the bodies nested in it.
+void appendNewtonLoop(BatchContext& ctx, cudaGraph_t g, const cudaStream_t* cs, bool withResults) {
+    const DeviceNet& dn = *ctx.dn;
+    const DevNet& net = dn.view;
+    const bool mixed = ctx.precision == 1;
+    const size_t S = ctx.S;
+    if (mixed && !ctx.lu32.p) ctx.lu32.alloc(static_cast<size_t>(net.nLu) * 4 * S * 4);
+    if (!ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(net.nLu) * 4 * S * 8);
+    if (!ctx.loopState.p) ctx.loopState.alloc(8 * sizeof(int));
+    const DevBatch b = ctx.batch();
+    const DevBatch b64 = fp64View(ctx), b64all = fp64AllView(ctx);
+    DevBatch br = b;
+    br.laneMask = b.refine;
+    const Settings cfg = ctx.cfg;
+    const bool rl = ctx.rl.nRl > 0 && cfg.reactiveLimits;
+    const bool dsOn = ctx.ds.nDs > 0 && cfg.distributedSlack;
+    const Hybrid hy = ctx.hybrid();
+    const Hybrid* hp = ctx.useHybrid() ? &hy : nullptr;
+    const int nLevels = static_cast<int>(dn.levelPtr.size()) - 1;
+    int* state = ctx.loopState.as<int>();
+    const int* nActive = static_cast<const int*>(ctx.nActive.p);
+    const int cap = roundCap(ctx);
+    const int steps = ctx.refinementSteps;
+    const bool nearPolicy = ctx.mixedPolicy == MIXED_FP64_NEAR;
+    OLF_CUDA(cudaStreamBeginCaptureToGraph(cs[0], g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    loopResetKernel<<<1, 1, 0, cs[0]>>>(state);
+    cudaGraphConditionalHandle hMain;
+    OLF_CUDA(cudaGraphConditionalHandleCreate(&hMain, g, 1, cudaGraphCondAssignDefault));
+    cudaGraph_t body = addConditional(cs[0], hMain, cudaGraphCondTypeWhile);
+    const cudaGraphConditionalHandle hWork = newHandle(body), hScore = newHandle(body);
+    const cudaGraphConditionalHandle hRefine = mixed ? newHandle(body) : 0, hRedo = mixed ? newHandle(body) : 0,
+                                     hNear = mixed ? newHandle(body) : 0;
+    captureBody(cs[1], body, [&](cudaStream_t st) {
+        launchIterationStart(b, st);
+        launchFill(net, b, true, rl || dsOn, st);
+        if (cfg.norm2Threshold > 0.0) launchNorm2(net, b, st);
+        launchTest(net, b, cfg, rl ? ctx.rl.remainingPv : nullptr, st);
+        if (dsOn) launchDistributedSlack(b, ctx.ds, cfg, st);
+        if (rl) launchReactiveLimits(net, b, ctx.rl, cfg, st);
+        launchCountSolving(b, mixed ? cfg.refineBelow : -1.0, cfg.maxIter, st);
+        loopCondKernel<<<1, 1, 0, st>>>(hMain, hWork, hScore, hNear, nActive, state, cap, mixed ? 1 : 0,
+                                        nearPolicy ? 1 : 0);
+        if (!mixed) {
+            captureBody(cs[2], addConditional(st, hWork, cudaGraphCondTypeIf), [&](cudaStream_t s2) {
+                launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, false, hp, s2);
+                launchSolve(net, b, dn.fwd(), dn.bwd(), false, false, hp, s2);
+            });
+        } else {
+            captureBody(cs[2], addConditional(st, hWork, cudaGraphCondTypeIf), [&](cudaStream_t s2) {
+                launchFactor(net, b, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, true, hp, s2);
+                launchCountFp64(b, s2);
+                launchSolve(net, b, dn.fwd(), dn.bwd(), true, false, hp, s2);
+            });
+            loopMixedKernel<<<1, 1, 0, st>>>(hRefine, hRedo, nActive, state, steps);
+            if (steps > 0) {
+                captureBody(cs[2], addConditional(st, hRefine, cudaGraphCondTypeWhile), [&](cudaStream_t s2) {
+                    launchResidual(net, br, s2);
+                    launchSolve(net, br, dn.fwd(), dn.bwd(), true, true, hp, s2);
+                    launchCorrectionCheck(net, br, cfg.corrBound, s2);
+                    refineCondKernel<<<1, 1, 0, s2>>>(hRefine, nActive, state, steps);
+                });
+            }
+            captureBody(cs[2], addConditional(st, hRedo, cudaGraphCondTypeIf), [&](cudaStream_t s2) {
+                launchFactor(net, b64, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, false, hp, s2);
+                launchSolve(net, b64, dn.fwd(), dn.bwd(), false, false, hp, s2);
+            });
+            captureBody(cs[2], addConditional(st, hNear, cudaGraphCondTypeIf), [&](cudaStream_t s2) {
+                launchFactor(net, b64all, dn.levelPtr.data(), dn.levelSplit.data(), nLevels, false, hp, s2);
+                launchSolve(net, b64all, dn.fwd(), dn.bwd(), false, false, hp, s2);
+            });
+        }
+        captureBody(cs[2], addConditional(st, hScore, cudaGraphCondTypeIf),
+                    [&](cudaStream_t s2) { launchScoreSolve(net, b, cfg, s2); });
+        launchStep(net, b, cfg, st);
+    });
+    capKernel<<<(ctx.S + 127) / 128, 128, 0, cs[0]>>>(b);
+    if (withResults) {
+        const int n = ctx.net->host.n;
+        dim3 blk(32, 8), grd((n + 31) / 32, (ctx.nS + 31) / 32);
+        resultsKernel<<<grd, blk, 0, cs[0]>>>(ctx.x.as<double>(), ctx.iter.as<int>(), ctx.normOut.as<double>(),
+                                              ctx.status.as<int>(), ctx.out.as<double>(), n, ctx.nS, ctx.S);
+    }
+    cudaGraph_t top;
+    OLF_CUDA(cudaStreamEndCapture(cs[0], &top));
+}
+
+// The key of everything a loop graph bakes in besides the batch view and settings.
+long long loopKey(const BatchContext& ctx) {
+    return ((((static_cast<long long>(ctx.narrowLanes) * 2 + (ctx.regionFactor ? 1 : 0)) * 2 + (ctx.regionSolve ? 1 : 0)) *
+                 2 + (ctx.subtrees ? 1 : 0)) * 2 + ctx.precision) * 4096 * 64 +
+           static_cast<long long>(ctx.refinementSteps) * 4096 * 2 + ctx.mixedPolicy * 4096 + roundCap(ctx);
+}
+
+// One context's Newton loop as one graph launch on its stream; returns the iterations run.
+int runDeviceLoop(BatchContext& ctx) {
+    cudaStream_t st = ctx.stream;
+    const DevBatch now = ctx.batch();
+    const long long key = loopKey(ctx);
+    if (!ctx.loopGraph || ctx.loopGraphKey != key || std::memcmp(&now, &ctx.loopBatch, sizeof(DevBatch)) != 0 ||
+        std::memcmp(&ctx.cfg, &ctx.loopCfg, sizeof(Settings)) != 0) {
+        dropGraph(ctx.loopGraph);
+        if (!ctx.loopStreams[0]) {
+            for (auto& s : ctx.loopStreams) OLF_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        }
+        cudaGraph_t g;
+        OLF_CUDA(cudaGraphCreate(&g, 0));
+        appendNewtonLoop(ctx, g, ctx.loopStreams, false);
+        OLF_CUDA(cudaGraphInstantiate(&ctx.loopGraph, g, 0));
+        cudaGraphDestroy(g);
+        ctx.loopGraphKey = key;
+        ctx.loopBatch = now;
+        ctx.loopCfg = ctx.cfg;
+    }
+    OLF_CUDA(cudaGraphLaunch(ctx.loopGraph, st));
+    OLF_CUDA(cudaMemcpyAsync(ctx.hostActive + 5, ctx.loopState.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    OLF_CUDA(cudaStreamSynchronize(st));
+    ctx.fp64Iterations = 0;
+    int st4 = 0;
+    OLF_CUDA(cudaMemcpy(&st4, static_cast<int*>(ctx.loopState.p) + 4, sizeof(int), cudaMemcpyDeviceToHost));
+    ctx.fp64Iterations = st4;
+    return ctx.hostActive[5];
+}
+
 int runIterations(BatchContext& ctx) {
     cudaStream_t st = ctx.stream;
     const DeviceNet& dn = *ctx.dn;
@@ -1540,6 +1767,10 @@ int runIterations(BatchContext& ctx) {
     if (!mixed && !ctx.lu64.p) ctx.lu64.alloc(static_cast<size_t>(dn.view.nLu) * 4 * S * 8);
     const int cap = roundCap(ctx);
     if (ctx.fallbackStart && ctx.hasX0Base && ctx.hasX0Full) selectStarts(ctx);
+    if (ctx.deviceLoop && !ctx.phaseTiming && ctx.schedule != SCHEDULE_PERSISTENT && ctx.schedule != SCHEDULE_COOP) {
+        ctx.fp64Iterations = 0;
+        return runDeviceLoop(ctx);
+    }
     if (ctx.schedule == SCHEDULE_PERSISTENT) {
         if (dn.view.frontF > 0) throw std::runtime_error("the persistent schedule does not run dense-front plans");
         PersistentPlan plan = dn.persistent;
@@ -1583,8 +1814,7 @@ int runIterations(BatchContext& ctx) {
         }
         if (fp64Iteration(ctx)) {
             ctx.fp64Iterations++;
-            launchPromoteFp64(ctx.batch(), st);
-            launchFp64Redo(ctx);
+            launchFp64All(ctx);
             OLF_CUDA(cudaGraphLaunch(scoreDue(ctx) ? ctx.graphStepScored : ctx.graphStep, st));
             continue;
         }
@@ -1864,6 +2094,9 @@ void solveBatch(BatchContext& ctx, const SolveRequest& req, double* out) {
 // ---------------------------------------------------------------------------------------------------------------
 MultiContext::~MultiContext() {
     if (graph) cudaGraphExecDestroy(graph);
+    if (loopGraph) cudaGraphExecDestroy(loopGraph);
+    for (cudaStream_t s : capStreams)
+        if (s) cudaStreamDestroy(s);
     for (cudaEvent_t e : ready) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
     if (hostItems) cudaFreeHost(hostItems);
@@ -1875,9 +2108,6 @@ MultiContext* createMultiContext(const std::vector<BatchContext*>& members) {
     for (const BatchContext* c : members) {
         if (!c) throw std::runtime_error("null batch context");
         if (c->device != device) throw std::runtime_error("the batch contexts of a multi-grid launch share one device");
-        if (c->dn->view.frontF > 0) {
-            throw std::runtime_error("a multi-grid launch runs persistent tiles, which do not run dense-front plans");
-        }
     }
     for (size_t i = 0; i < members.size(); i++)
         for (size_t j = i + 1; j < members.size(); j++)
@@ -1911,6 +2141,39 @@ std::vector<int> launchOrder(const MultiContext& m, int order) {
     return idx;
 }
 
+// The members' device-resident Newton loops as the branches of one graph (rebuilt when a member's schedule, batch view
+// or settings changed).
+void launchMultiLoops(MultiContext& m) {
+    const size_t k = m.members.size();
+    bool same = m.loopGraph && m.loopKeys.size() == k;
+    for (size_t i = 0; same && i < k; i++) {
+        const BatchContext& c = *m.members[i];
+        const DevBatch now = c.batch();
+        same = m.loopKeys[i] == loopKey(c) && std::memcmp(&now, &m.loopBatches[i], sizeof(DevBatch)) == 0 &&
+               std::memcmp(&c.cfg, &m.loopCfgs[i], sizeof(Settings)) == 0;
+    }
+    if (!same) {
+        dropGraph(m.loopGraph);
+        if (!m.capStreams[0]) {
+            for (auto& s : m.capStreams) OLF_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        }
+        cudaGraph_t g;
+        OLF_CUDA(cudaGraphCreate(&g, 0));
+        m.loopKeys.clear();
+        m.loopBatches.clear();
+        m.loopCfgs.clear();
+        for (BatchContext* c : m.members) {
+            appendNewtonLoop(*c, g, m.capStreams, true);
+            m.loopKeys.push_back(loopKey(*c));
+            m.loopBatches.push_back(c->batch());
+            m.loopCfgs.push_back(c->cfg);
+        }
+        OLF_CUDA(cudaGraphInstantiate(&m.loopGraph, g, 0));
+        cudaGraphDestroy(g);
+    }
+    OLF_CUDA(cudaGraphLaunch(m.loopGraph, m.stream));
+}
+
 // Lanes of every member reset to their staged inputs, then the one launch (and the members' result gathers).
 void runMulti(MultiContext& m, bool fp32) {
     cudaStream_t st = m.stream;
@@ -1919,6 +2182,10 @@ void runMulti(MultiContext& m, bool fp32) {
         installLanes(c);
         OLF_CUDA(cudaEventRecord(m.ready[i], c.stream));
         OLF_CUDA(cudaStreamWaitEvent(st, m.ready[i], 0));
+    }
+    if (m.lanesPerTile == 0) {
+        launchMultiLoops(m);
+        return;
     }
     const std::vector<int> idx = launchOrder(m, m.order);
     int tile = 0;
@@ -1958,6 +2225,11 @@ void runMulti(MultiContext& m, bool fp32) {
     OLF_CUDA(cudaGraphLaunch(m.graph, st));
 }
 
+bool multiTilesFit(const BatchContext& c) {
+    return c.dn->view.frontF == 0 && !c.cfg.distributedSlack && c.cfg.norm2Threshold <= 0.0 && c.cfg.svsMode == SVS_NONE &&
+           !c.cfg.realistic && !(c.precision == 1 && c.mixedPolicy == MIXED_FP64_NEAR);
+}
+
 void autotuneMulti(MultiContext& m, bool fp32) {
     cudaEvent_t e0, e1;
     OLF_CUDA(cudaEventCreate(&e0));
@@ -1965,6 +2237,21 @@ void autotuneMulti(MultiContext& m, bool fp32) {
     float best = 1e30f;
     MultiTuning pick{};
     m.tuning.clear();
+    bool tilesFit = true;      // the persistent tiles run neither dense-front plans nor the extra outer loops / tests
+    for (const BatchContext* c : m.members) tilesFit = tilesFit && multiTilesFit(*c);
+    {
+        m.lanesPerTile = 0;
+        OLF_CUDA(cudaEventRecord(e0, m.stream));
+        runMulti(m, fp32);
+        OLF_CUDA(cudaEventRecord(e1, m.stream));
+        OLF_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        OLF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        m.tuning.push_back({0, 0, 0, ms});
+        best = ms;
+        pick = m.tuning.back();
+    }
+    if (tilesFit)
     for (int lanes : {1, 2, 4, 8})
         for (int threads : {256, 512})
             for (int order : {0, 1}) {
@@ -1998,9 +2285,13 @@ void solveMulti(MultiContext& m, double* const* outs) {
     const int precision = m.members[0]->precision;
     for (BatchContext* c : m.members) {
         if (!c->staged) throw std::runtime_error("every batch context of a multi-grid launch must be staged first");
-        if (c->cfg.distributedSlack || c->cfg.norm2Threshold > 0.0 || c->cfg.svsMode != SVS_NONE || c->cfg.realistic) {
-            throw std::runtime_error("a multi-grid launch runs the plain Newton loop with reactive limits only "
-                                     "(no distributed slack, 2-norm test, step clamp or realistic band)");
+        if (m.lanesPerTile > 0 && !m.autotunePending && !multiTilesFit(*c)) {
+            throw std::runtime_error("the persistent tiles of a multi-grid launch run the plain Newton loop with "
+                                     "reactive limits only (no dense-front plan, distributed slack, 2-norm test, step "
+                                     "clamp, realistic band or FP64-near policy): use lanesPerTile 0");
+        }
+        if (m.lanesPerTile == 0 && (c->schedule == SCHEDULE_PERSISTENT || c->schedule == SCHEDULE_COOP)) {
+            throw std::runtime_error("the device-resident loops of a multi-grid launch run level schedules (0, 3, 4 or 5)");
         }
         if (c->precision != precision) {
             throw std::runtime_error("the batch contexts of a multi-grid launch share one precision");
@@ -2035,6 +2326,7 @@ void solveMulti(MultiContext& m, double* const* outs) {
     cudaEventDestroy(e1);
     for (BatchContext* c : m.members) {
         c->lastIterations = 0;
+        if (m.lanesPerTile == 0) OLF_CUDA(cudaMemcpy(&c->lastIterations, c->loopState.p, sizeof(int), cudaMemcpyDeviceToHost));
         c->lastMs = m.lastMs;
     }
     OLF_CUDA(cudaGetLastError());

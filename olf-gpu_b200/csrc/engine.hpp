@@ -273,12 +273,21 @@ struct BatchContext {
     // solve of the flagged lanes; the step
     cudaGraphExec_t graphFactor = nullptr, graphResidual = nullptr, graphCorrect = nullptr, graph64 = nullptr,
                     graphStep = nullptr;
+    cudaGraphExec_t graph64All = nullptr;  // MIXED_FP64_NEAR: FP64 factorization and solves of every factorizing lane
     // the same iteration with the linear-solve scoring before the step (FP64: factorization, solves, scoring, step;
     // mixed: scoring, step)
     cudaGraphExec_t graphSolveScored = nullptr, graphStepScored = nullptr;
     int graphKey = -1;
     DevBatch graphBatch{};          // the batch view and settings the iteration graphs were captured with
     Settings graphCfg{};
+    // the whole Newton loop as one graph launch (conditional nodes; level schedules), and what it was built with
+    bool deviceLoop = false;
+    cudaGraphExec_t loopGraph = nullptr;
+    long long loopGraphKey = -1;
+    DevBatch loopBatch{};
+    Settings loopCfg{};
+    DeviceBuffer loopState;         // int [8]: iterations, refinement steps, iteration kind, FP64 iterations
+    cudaStream_t loopStreams[3] = {nullptr, nullptr, nullptr};   // capture streams of the loop graph's bodies
     // mixed: a lane refines only in an iteration where its max |F| is below refineBelow; 1e-2 covers every step from
     // which Newton can land below the tolerance, so a converged state's last step is FP64-accurate
     double refineBelow = 1e-2;
@@ -323,7 +332,7 @@ void setStrongestPvKeys(BatchContext& ctx, const double* nomV, const int* pRow, 
                         const int* idRank);
 
 struct MultiTuning {
-    int lanesPerTile, threads, order;
+    int lanesPerTile, threads, order;   // lanesPerTile 0: every member's device-resident level-schedule loop
     float ms;
 };
 
@@ -335,6 +344,13 @@ struct MultiContext {
     cudaStream_t stream = nullptr;
     std::vector<cudaEvent_t> ready;      // per member: its lanes are installed
     int lanesPerTile = 2, threads = 256, order = 0;   // order 0: as given, 1: most buses first
+    // lanesPerTile 0: one graph whose branches are the members' own device-resident Newton loops (their level
+    // schedules, concurrent on the device), instead of the persistent tiles
+    cudaGraphExec_t loopGraph = nullptr;
+    std::vector<long long> loopKeys;
+    std::vector<DevBatch> loopBatches;
+    std::vector<Settings> loopCfgs;
+    cudaStream_t capStreams[3] = {nullptr, nullptr, nullptr};
     bool autotunePending = false;
     std::vector<MultiTuning> tuning;
     DeviceBuffer itemsDev;

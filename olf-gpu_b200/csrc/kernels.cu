@@ -1383,14 +1383,6 @@ void launchCountSolving(const DevBatch& b, double refineBelow, int maxIter, cuda
 
 void launchCountFp64(const DevBatch& b, cudaStream_t st) { countLanesKernel<<<1, 1024, 0, st>>>(b, 0.0, 1, 0); }
 
-// Iteration-level precision: every lane that factorizes this iteration is flagged for FP64 (for the rest of the solve)
-__global__ void promoteKernel(DevBatch b) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < b.S && solving(b, s)) b.precision64[s] = 1;
-}
-
-void launchPromoteFp64(const DevBatch& b, cudaStream_t st) { promoteKernel<<<(b.S + 127) / 128, 128, 0, st>>>(b); }
-
 // Per-lane max |res| over the rows: 32 lanes x 8 row strands per CTA, reduced in shared memory, one atomic per CTA
 // and lane (non-negative doubles order like their bit patterns; a NaN residual sorts above every number).
 __global__ void residualMaxKernel(DevNet net, DevBatch b) {

@@ -336,7 +336,6 @@ void launchIterationStart(const DevBatch& b, cudaStream_t st);
 void launchCountSolving(const DevBatch& b, double refineBelow, int maxIter, cudaStream_t st);
 // Factorizing lanes flagged for an FP64 refactor (nActive[3]).
 void launchCountFp64(const DevBatch& b, cudaStream_t st);
-void launchPromoteFp64(const DevBatch& b, cudaStream_t st);
 // Mixed precision, after launchResidual: each lane's max |r| and the count of factorizing lanes with max |F| below
 // refineBelow whose residual is above `threshold` (nActive[2]): the correction solve of a refinement step runs only
 // when some lane needs it.

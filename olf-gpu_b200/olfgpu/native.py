@@ -45,7 +45,8 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_begin_batch_install", "olfgpu_read_handed_back_slots", "olfgpu_set_states_to_host",
            "olfgpu_states_to_host", "olfgpu_read_batch_states", "olfgpu_set_outer_loops", "olfgpu_context_info",
            "olfgpu_linear_solve_transposed", "olfgpu_screen_violations", "olfgpu_last_slack_distribution_failures",
-           "olfgpu_set_start_polish", "olfgpu_set_mixed_precision_policy", "olfgpu_last_fp64_iterations"]
+           "olfgpu_set_start_polish", "olfgpu_set_mixed_precision_policy", "olfgpu_last_fp64_iterations",
+           "olfgpu_set_device_loop"]
 # The arrays of BatchSolveNative.solveBatchContext this engine rejects when non-empty, in the reference's order
 UNSUPPORTED_SOLVE_ARRAYS = [
     "distributedSlackOverrideBus", "distributedSlackOverrideFactorDelta", "distributedSlackOverrideBaseTargetPDelta",
@@ -116,6 +117,7 @@ def load(path: str = LIB_PATH):
     L.olfgpu_set_fp64_restart.argtypes = [_i64, _ci]
     L.olfgpu_set_start_polish.argtypes = [_i64, _cd]
     L.olfgpu_set_mixed_precision_policy.argtypes = [_i64, _ci]
+    L.olfgpu_set_device_loop.argtypes = [_i64, _ci]
     L.olfgpu_last_fp64_iterations.argtypes = [_i64, _ip]
     L.olfgpu_structure_subtrees.argtypes = [_i64, ctypes.POINTER(_i64)]
     L.olfgpu_linear_solve_transposed.argtypes = [_i64, _dp, _dp, _dp, _ci, _dp, _dp]
@@ -459,6 +461,10 @@ class BatchContext:
         """0 MIXED_REFINE: FP32 LU + FP64 refinement near convergence; 1 MIXED_FP64_NEAR: iterations with a scenario
         near convergence run in FP64."""
         _check(load().olfgpu_set_mixed_precision_policy(self.handle, policy))
+
+    def set_device_loop(self, enable: bool = True):
+        """The whole Newton loop as one graph launch (conditional graph nodes; level schedules)."""
+        _check(load().olfgpu_set_device_loop(self.handle, 1 if enable else 0))
 
     def last_fp64_iterations(self) -> int:
         v = ctypes.c_int(0)

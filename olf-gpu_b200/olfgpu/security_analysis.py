@@ -110,14 +110,16 @@ class SecurityAnalysis:
 
 
 class MultiGridAnalysis:
-    """N-1 batches of several grids solved by one persistent launch (the engine's multi-grid context).
+    """N-1 batches of several grids solved by one launch (the engine's multi-grid context).
 
     Each grid keeps its own structure and a context sized to its batch; ``solve`` stages every grid's outages and runs
     them together, returning one BatchResult per grid.  ``schedule`` is -1 (autotune on the first solve) or a fixed
-    (lanes per tile, threads, order)."""
+    (lanes per tile, threads, order): persistent tiles, or lanes per tile 0 for one graph whose branches are the grids'
+    device-resident Newton loops under ``member_schedule`` (schedule, lanes, threads of each grid's level schedule)."""
 
     def __init__(self, packed_grids: Sequence[Packed], counts: Sequence[int], precision: int = native.FP64,
-                 refinement_steps: int = 1, reactive_limits: bool = True, schedule=-1, ordering: int = 0):
+                 refinement_steps: int = 1, reactive_limits: bool = True, schedule=-1, ordering: int = 0,
+                 member_schedule=None, mixed_policy: int = native.MIXED_REFINE):
         self.packed = list(packed_grids)
         self.counts = [int(c) for c in counts]
         self.structures = [native.Structure(p, ordering) for p in self.packed]
@@ -125,6 +127,9 @@ class MultiGridAnalysis:
         for p, s, c in zip(self.packed, self.structures, self.counts):
             ctx = native.BatchContext(s, c, native.BATCHED_LU, p.rl if reactive_limits and p.rl is not None else None)
             ctx.set_linear_solver_settings(precision, refinement_steps)
+            ctx.set_mixed_precision_policy(mixed_policy)
+            if member_schedule is not None:
+                ctx.set_schedule(*member_schedule)
             self.contexts.append(ctx)
         self.multi = native.MultiContext(self.contexts)
         if schedule == -1:

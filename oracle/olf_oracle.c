@@ -996,12 +996,11 @@ int oracle_solve_batch_ds(oracle_solver *o, int ns, const double *x0, int x0_str
             memcpy(mode, mode_base, sizeof(int) * (size_t)n);
             memset(lt, 0, (size_t)nrl + 1); memset(sc, 0, (size_t)nrl + 1);
             const unsigned char *dis = disabled ? disabled + (size_t)sc_i * n_elements : NULL;
-            int iters = 0, total = 0, status = ST_CONVERGED;
+            int iters = 0, status = ST_CONVERGED;
             double nrm = 0.0;
             for (int outer = 0;; outer++) {
                 status = newton(s, g, x, target, mode, dis, max_iter, tol, &iters, &nrm, vals, ax, F, dx, qbuf,
                                 outer == 0, ns == 1, opts);
-                total += iters;
                 if (status != ST_CONVERGED || (nrl == 0 && nds == 0) || outer >= max_outer) break;
                 if (nds > 0) {   /* distributed slack first, then reactive limits (the outer-loop order) */
                     int failed = 0;
@@ -1016,7 +1015,7 @@ int oracle_solve_batch_ds(oracle_solver *o, int ns, const double *x0, int x0_str
                 if (!reactive_limits_check(rl, n, x, qbuf, mode, target, lt, sc, ps, sm, st, rl_tol, max_switch)) break;
             }
             if (status == ST_CONVERGED && unrealistic(opts, n, x)) status = ST_UNREALISTIC;
-            x[n] = (double)total;
+            x[n] = (double)iters;   /* the last inner solve's iterations (res.iters, newton_iteration.cu:338) */
             x[n + 1] = nrm;
             x[n + 2] = (double)status;
         }

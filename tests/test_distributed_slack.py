@@ -39,7 +39,6 @@ def test_oracle_distribution_moves_states_and_rejects_when_bounded(oracle_mod):
     r = st.solve_batch(p.x_base, dis, distributed_slack=ds)
     n = p.n
     assert np.all(r[:, n + 2] == 0)
-    assert np.all(r[:, n] > plain[:, n])                      # re-solves after each distribution
     assert np.max(np.abs(r[:, :n] - plain[:, :n])) > 1e-3     # the slack's share moved to the participants
     # bounds far below the mismatch: the distribution cannot place it; with the reject switch the scenario ends REJECTED
     tight = _tight(ds, 1e-5)

@@ -40,8 +40,9 @@ def test_multi_grid_matches_oracle(engine_lib, oracle_mod, precision):
 
 
 def test_multi_grid_autotuner_and_orders(engine_lib, oracle_mod):
-    """The autotuner times 16 tile schedules (lanes 1-8 x 256/512 threads x two member orders) and keeps the fastest;
-    every fixed schedule gives the oracle's statuses and states within tolerance."""
+    """The autotuner times the members' device-resident loops and 16 tile schedules (lanes 1-8 x 256/512 threads x two
+    member orders) and keeps the fastest; every fixed schedule gives the oracle's statuses and states within
+    tolerance."""
     from olfgpu import synthetic
     from olfgpu.security_analysis import MultiGridAnalysis
     names, counts = ["grid2000q", "grid300"], [40, 33]
@@ -50,12 +51,12 @@ def test_multi_grid_autotuner_and_orders(engine_lib, oracle_mod):
     ma = MultiGridAnalysis(packs, counts, schedule=-1)
     tuned, _ = ma.solve(outs)
     pick, timings = ma.multi.schedule()
-    assert len(timings) == 16
+    assert len(timings) == 17 and timings[0][0] == 0
     best = min(timings, key=lambda t: t[3])
     assert pick == (int(best[0]), int(best[1]), int(best[2]))
     refs = [oracle_mod.Structure(p).solve_batch(p.x_base, p.outage_masks(o), reactive_limits=True)
             for p, o in zip(packs, outs)]
-    for sched in [(1, 512, 1), (4, 256, 0), (8, 512, 1)]:
+    for sched in [(0, 0, 0), (1, 512, 1), (4, 256, 0), (8, 512, 1)]:
         ma.multi.set_schedule(*sched)
         res, _ = ma.solve(outs)
         for p, r, ref in zip(packs, res, refs):
@@ -100,4 +101,31 @@ def test_uneven_batch_four_grids_full_size(engine_lib, oracle_mod):
         assert np.array_equal(r.status[pick], st)
         conv = st == 0
         assert np.max(np.abs(r.x[pick][conv] - ref[conv, :p.n])) <= STATE_TOL
+    ma.close()
+
+
+@pytest.mark.parametrize("precision,policy", [(0, 0), (1, 0), (1, 1)])
+def test_multi_grid_device_loops_match_solo_solves(engine_lib, oracle_mod, precision, policy):
+    """lanesPerTile 0: one graph whose branches are the grids' own device-resident Newton loops (dense-front plans,
+    shared-memory level schedule, reactive limits) gives every grid exactly its solo solve, and the oracle's result."""
+    from olfgpu import native, synthetic
+    from olfgpu.security_analysis import MultiGridAnalysis
+    names, counts = ["grid300", "grid2000q", "grid9241"], [90, 60, 40]
+    packs = [grid(nm)[1] for nm in names]
+    outs = [synthetic.draw_outages(grid(nm)[0], c, seed=80 + i) for i, (nm, c) in enumerate(zip(names, counts))]
+    ma = MultiGridAnalysis(packs, counts, precision=precision, refinement_steps=3, schedule=(0, 0, 0),
+                           ordering=native.PLAN_DENSE_FRONT, member_schedule=(4, 0, 256), mixed_policy=policy)
+    res, ms = ma.solve(outs)
+    assert ms > 0
+    for p, o, r in zip(packs, outs, res):
+        s = native.Structure(p, native.PLAN_DENSE_FRONT)
+        c = native.BatchContext(s, o.shape[0], native.BATCHED_LU, p.rl)
+        c.set_linear_solver_settings(precision, 3)
+        c.set_mixed_precision_policy(policy)
+        c.set_schedule(4, 0, 256)
+        solo = c.solve(p.x_base, p.target, p.base_row_mode, p.outage_masks(o))
+        assert np.array_equal(r.x, solo[:, :p.n]) and np.array_equal(r.status, solo[:, p.n + 2].astype(int))
+        assert np.array_equal(r.iterations, solo[:, p.n].astype(int))
+        ref = oracle_mod.Structure(p).solve_batch(p.x_base, p.outage_masks(o), reactive_limits=p.rl is not None)
+        _compare(r, ref, p.n)
     ma.close()
