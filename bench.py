@@ -188,6 +188,9 @@ def run_engine(args, rank: int, world: int):
     ns = outs.shape[0]
     ctx = native.BatchContext(s, ns)
     ctx.set_linear_solver_settings(precision, max(refinement, 0))
+    policy = native.MIXED_FP64_NEAR if args.mixed_policy == "fp64near" else native.MIXED_REFINE
+    ctx.set_mixed_precision_policy(policy)
+    ctx.set_device_loop(args.device_loop)
     if args.schedule == "auto":
         ctx.set_schedule(native.AUTOTUNE)           # the first (warm-up) solve times the candidates
     elif args.schedule == "coop":
@@ -248,6 +251,7 @@ def run_engine(args, rank: int, world: int):
             pred_total += pred_ms
             tot_iters += int(tot.sum())
     fallbacks = int(ctx.last_fallbacks().size) if learned is not None else 0
+    fp64_iterations = ctx.last_fp64_iterations()
     torch.cuda.synchronize()
     result = out.copy()                         # the last timed solve's states, iterations and statuses
     dev = float(np.mean(dev_ms))
@@ -258,23 +262,37 @@ def run_engine(args, rank: int, world: int):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev, e2e = float(t[0]), float(t[1])
 
-    def comparison(prec, refine):
-        """The engine from the base start on the same batch at another precision: device time per step, and each
-        scenario's difference from the measured configuration's result (scenarios both converged)."""
+    def histogram(r):
+        it = r[:, p.n].astype(int)
+        return {str(int(k)): int(v) for k, v in zip(*np.unique(it, return_counts=True))}
+
+    def comparison(prec, refine, pol=native.MIXED_REFINE, start=None):
+        """The engine from the base start (or ``start`` [n], e.g. the flat start) on the same batch at a given
+        precision and policy: device time per step, iteration histogram, and each scenario's difference from the
+        measured configuration's result (scenarios both converged)."""
         c = native.BatchContext(s, ns)
         c.set_linear_solver_settings(prec, refine)
+        c.set_mixed_precision_policy(pol)
+        c.set_device_loop(args.device_loop)
         if args.schedule == "auto":
             c.set_schedule(native.AUTOTUNE)
+        else:
+            c.set_schedule(*ctx.schedule()[0])
+        xs = x0 if start is None else start
         for _ in range(args.warmup):
-            c.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
+            c.solve(xs, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
         pm = []
         for _ in range(args.steps):
-            c.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
+            c.solve(xs, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
             pm.append(c.last_stats()[0])
+        f64 = c.last_fp64_iterations()
         c.close()
         both = (result[:, p.n + 2] == 0) & (out[:, p.n + 2] == 0)
         d = np.abs(result[both, :p.n] - out[both, :p.n])
         return {"solves_per_s": round(ns / (float(np.mean(pm)) * 1e-3), 1), "ms_per_step": round(float(np.mean(pm)), 4),
+                "iterations_per_solve": round(float(out[:, p.n].mean()), 3), "iteration_histogram": histogram(out),
+                "converged_fraction": round(float((out[:, p.n + 2] == 0).mean()), 4),
+                "fp64_iterations": int(f64) if prec == native.MIXED else None,
                 "vs_measured": {
                     "max_abs_dVa_rad": float(d[:, 0::2].max()) if both.any() else None,
                     "max_abs_dVm_pu": float(d[:, 1::2].max()) if both.any() else None,
@@ -283,11 +301,15 @@ def run_engine(args, rank: int, world: int):
 
     # the plain FP64 engine from the base start on the same batch (the comparison the metric names) and, with the
     # learned start, the mixed-precision engine from the base start (what the start alone changes)
-    plain = mixed_base = None
+    plain = mixed_base = flat = refine_policy = None
     if not args.no_plain:
         plain = comparison(native.FP64, 0)
         if learned is not None and precision == native.MIXED:
-            mixed_base = comparison(native.MIXED, refinement)
+            mixed_base = comparison(native.MIXED, refinement, policy)
+        # the flat start (V = 1 or the set point, angles 0) at the measured precision and policy
+        flat = comparison(precision, refinement, policy, start=np.ascontiguousarray(p.x_flat))
+        if precision == native.MIXED and policy != native.MIXED_REFINE:
+            refine_policy = comparison(native.MIXED, max(refinement, 3), native.MIXED_REFINE)
     # roofline of the Newton iterations (HBM-bound): algorithmic bytes over the device time
     peak, peak_kind = _peaks()
     pbytes = 4 if precision == native.MIXED else 8
@@ -370,6 +392,22 @@ def run_engine(args, rank: int, world: int):
         "autotune_ms": [[int(a), int(b_), int(c_), round(float(ms), 3)] for a, b_, c_, ms in ctx.schedule()[1]],
         "plain_fp64_base_start": plain,
         "mixed_base_start": mixed_base,
+        "starts": None if plain is None else {
+            "judge": "the engine's own Newton loop at 1e-8 pu decides every start's convergence",
+            "learned" if learned is not None else "base (measured)": {
+                "ms_per_step": round(dev, 4), "iterations_per_solve": round(float(result[:, p.n].mean()), 3),
+                "iteration_histogram": histogram(result), "converged_fraction": round(conv, 4),
+                "scenarios_on_base_start": fallbacks if learned is not None else None},
+            "base": mixed_base if mixed_base is not None else plain,
+            "flat": flat},
+        "mixed_precision": None if precision != native.MIXED else {
+            "policy": args.mixed_policy, "refine_below": 1e-2,
+            "fp64_iterations_last_step": int(fp64_iterations),
+            "refine_policy_base_start": refine_policy,
+            "note": "fp64near: an iteration in which some scenario's max |F| is below 1e-2 factorizes and solves in "
+                    "FP64 (all its scenarios), the others in FP32 without refinement; refine: FP32 LU every "
+                    "iteration, FP64 refinement of the scenarios below 1e-2 to a 1e-11 correction"},
+        "device_loop": bool(args.device_loop),
         "learned_start": None if learned is None else {
             "checkpoint": os.path.relpath(args.checkpoint, ROOT), "prediction_ms_per_step": round(pred_total / args.steps, 4),
             "scenarios_on_base_start": fallbacks},
@@ -381,12 +419,17 @@ def run_engine(args, rank: int, world: int):
     }
     rounds = max(ph["iterations"], 1)
     per_solve = launches_per_solve(s, sched, rounds, args.plan == "dense", args.plan == "deferred",
-                                   precision == native.MIXED, (rounds - 1) if refinement > 0 else 0)
+                                   precision == native.MIXED and fp64_iterations < rounds,
+                                   (rounds - 1) if refinement > 0 and args.mixed_policy == "refine" else 0)
+    if args.device_loop:
+        per_solve += 2 + rounds * (2 if precision == native.MIXED else 1)   # loop reset, cap; a condition per round
     if learned is not None:
         per_solve += GNN_LAUNCHES + 6          # the prediction, the two-start selection (2 fills and 4 small kernels)
     line["gpu_launches"] = int(per_solve * args.steps)
     line["gpu_launches_basis"] = (f"{per_solve} per step: the level structure under the schedule in force over "
                                   f"{rounds} factorizing Newton rounds (the same count as the ncu launch lists)")
+    if not args.no_uneven:
+        line["uneven_batch"] = uneven_summary(args)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, outs, args.cpu_sample)
     if world > 1:
@@ -395,6 +438,60 @@ def run_engine(args, rank: int, world: int):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def uneven_summary(args):
+    """The uneven-batching workload (four grids, reactive limits on), measured inside the default line: one graph
+    whose branches are the grids' device-resident Newton loops (dense-front plans, shared-memory level schedule), the
+    same grids solved back to back one batch each, and the single persistent launch (tiles of 2 lanes)."""
+    from olfgpu import native, packing, synthetic
+    from olfgpu.security_analysis import MultiGridAnalysis
+    grids = [synthetic.build(nm) for nm, _ in UNEVEN]
+    packs = [packing.pack(g) for g in grids]
+    counts = [c for _, c in UNEVEN]
+    outs = [synthetic.draw_outages(g, c, seed=7000 + i, replace=True) for i, (g, c) in enumerate(zip(grids, counts))]
+    total = sum(counts)
+    steps = max(3, min(args.steps, 5))
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        return float(np.median([fn() for _ in range(steps)]))
+
+    res = {}
+    ma = MultiGridAnalysis(packs, counts, schedule=(0, 0, 0), ordering=native.PLAN_DENSE_FRONT,
+                           member_schedule=(native.LEVELS_SHARED_ALL, 0, 256))
+    res["one_graph_device_loops"] = timed(lambda: ma.solve(outs)[1])
+    loop_res, _ = ma.solve(outs)
+    ma.close()
+    seq = []
+    for p, o in zip(packs, outs):
+        st = native.Structure(p, native.PLAN_DENSE_FRONT)
+        c = native.BatchContext(st, o.shape[0], native.BATCHED_LU, p.rl)
+        c.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
+        c.set_device_loop(True)
+        seq.append((st, c, p, p.outage_masks(o)))
+
+    def seq_step():
+        ms = 0.0
+        for st, c, p, dis in seq:
+            c.solve(p.x_base, p.target, p.base_row_mode, dis, max_iter=15, tol=TOL)
+            ms += c.last_stats()[0]
+        return ms
+    res["per_grid_batches_back_to_back"] = timed(seq_step)
+    same = True
+    for (st, c, p, dis), r in zip(seq, loop_res):
+        solo = c.solve(p.x_base, p.target, p.base_row_mode, dis, max_iter=15, tol=TOL)
+        same = same and np.array_equal(solo[:, :p.n], r.x) and np.array_equal(solo[:, p.n + 2].astype(int), r.status)
+        c.close()
+        st.close()
+    ma = MultiGridAnalysis(packs, counts, schedule=(2, 256, 1))
+    res["persistent_tiles"] = timed(lambda: ma.solve(outs)[1])
+    ma.close()
+    return {"workload": "grid300 x1000 + grid2000q x1000 + grid9241q x500 + grid13659 x250 outages, reactive "
+                        "limits on, FP64, tol 1e-8 pu",
+            **{k: {"ms": round(v, 3), "solves_per_s": round(total / (v * 1e-3), 1)} for k, v in res.items()},
+            "one_graph_equals_solo_solves": bool(same)}
 
 
 def cpu_baseline(p, outs, sample: int):
@@ -416,7 +513,8 @@ UNEVEN = [("grid300", 1000), ("grid2000q", 1000), ("grid9241q", 500), ("grid1365
 
 def run_uneven(args, rank: int, world: int):
     """Uneven batching: four grids (300 / 2,000 / 9,241 / 13,659 buses; 1,000 / 1,000 / 500 / 250 outages, reactive
-    limits on) in ONE persistent graph-captured launch, autotuned schedule beside a fixed one and beside one
+    limits on) in ONE graph launch, the schedule picked by the multi-grid autotuner (the grids' device-resident Newton
+    loops as the graph's branches, or the persistent tiles), beside a fixed persistent-tile schedule and beside one
     level-schedule batch per grid run back to back."""
     import torch
     from olfgpu import native, packing, synthetic
@@ -446,8 +544,11 @@ def run_uneven(args, rank: int, world: int):
             wall.append((time.perf_counter() - t0) * 1e3)
         return float(np.mean(dev)), float(np.mean(wall))
 
-    ordering = native.PLAN_DEFERRED_L if args.plan == "deferred" else 0
-    ma = MultiGridAnalysis(packs, counts, precision=precision, schedule=-1, ordering=ordering)
+    ordering = {"deferred": native.PLAN_DEFERRED_L, "dense": native.PLAN_DENSE_FRONT}.get(args.plan, 0)
+    member = (native.LEVELS_SHARED_ALL, 0, 256) if args.plan == "dense" else (native.LEVELS, 2, 256)
+    policy = native.MIXED_FP64_NEAR if args.mixed_policy == "fp64near" else native.MIXED_REFINE
+    ma = MultiGridAnalysis(packs, counts, precision=precision, refinement_steps=args.refinement, schedule=-1,
+                           ordering=ordering, member_schedule=member, mixed_policy=policy)
     ma.solve(outs)                                     # autotunes on the first solve
     pick, tuning = ma.multi.schedule()
     last = {}
@@ -462,16 +563,24 @@ def run_uneven(args, rank: int, world: int):
         dev_auto, wall_auto = timed(multi_step)
     res = last["res"]
     iters = [int(r.total_iterations.sum()) for r in res]
-    fixed = (2, 256, 0)
-    ma.multi.set_schedule(*fixed)
-    dev_fixed, _ = timed(multi_step)
+    rounds = [int(c.last_stats()[1]) for c in ma.contexts]
     ma.close()
+    fixed = (2, 256, 0)                                # persistent tiles (the scaled plan: tiles run no dense front)
+    mf = MultiGridAnalysis(packs, counts, precision=precision, refinement_steps=args.refinement, schedule=fixed)
+
+    def fixed_step():
+        return mf.solve(outs)[1]
+    dev_fixed, _ = timed(fixed_step)
+    mf.close()
     # one level-schedule batch per grid, back to back (each grid's own launches)
     seq = []
     for p, o in zip(packs, outs):
         st = native.Structure(p, ordering)
         c = native.BatchContext(st, o.shape[0], native.BATCHED_LU, p.rl)
-        c.set_linear_solver_settings(precision, 1)
+        c.set_linear_solver_settings(precision, args.refinement)
+        c.set_mixed_precision_policy(policy)
+        c.set_schedule(*member)
+        c.set_device_loop(True)
         seq.append((st, c, p, p.outage_masks(o)))
 
     def seq_step():
@@ -495,8 +604,16 @@ def run_uneven(args, rank: int, world: int):
         dev_auto, wall_auto = float(t[0]), float(t[1])
     h2d = sum(p.n * 8 * 2 + p.n * 4 + p.n_elements * ((c + 31) // 32) * 4 for p, c in zip(packs, counts))
     d2h = sum(c * (p.n + 3) * 8 for p, c in zip(packs, counts))
+    loops = pick[0] == 0
+    if loops:
+        launches = 0
+        for (st, c, p, dis), r in zip(seq, rounds):
+            launches += launches_per_solve(st, member, max(r, 1), args.plan == "dense", args.plan == "deferred",
+                                           precision == native.MIXED, 0) + 2 + max(r, 1)
+    else:
+        launches = 1 + 4 + 5 * 4
     line = {
-        "metric": "N-1 solves/s, uneven batch of four grids in one persistent launch (reactive limits on)",
+        "metric": "N-1 solves/s, uneven batch of four grids in one graph launch (reactive limits on)",
         "value": round(world * total / (dev_auto * 1e-3), 1), "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_auto, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
@@ -508,7 +625,11 @@ def run_uneven(args, rank: int, world: int):
                    "autotuned_schedule": {"lanes_per_tile": pick[0], "threads": pick[1],
                                           "order": ["as given", "most buses first"][pick[2]],
                                           "ms": round(dev_auto, 3)},
+                   "autotuned_kind": ("one graph whose branches are the grids' device-resident Newton loops "
+                                      f"(member schedule {member}, plan {args.plan})" if loops else
+                                      "one persistent launch of lane tiles"),
                    "fixed_schedule": {"lanes_per_tile": fixed[0], "threads": fixed[1], "order": "as given",
+                                      "kind": "persistent tiles, scaled plan",
                                       "ms": round(dev_fixed, 3),
                                       "solves_per_s": round(total / (dev_fixed * 1e-3), 1)},
                    "per_grid_level_batches": {"ms": round(dev_seq, 3),
@@ -519,9 +640,10 @@ def run_uneven(args, rank: int, world: int):
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None,
-                     "kernel": "newtonMultiKernel (the whole Newton loop of the four grids in one launch)",
+                     "kernel": ("the four grids' Newton iterations (device-resident loops, one graph)" if loops else
+                                "newtonMultiKernel (the whole Newton loop of the four grids in one launch)"),
                      "peak_source": f"{peak_kind} copy bandwidth (hbm_gbs)"},
-        "gpu_launches": 1 + 4 + 5 * 4,
+        "gpu_launches": int(launches * args.steps),
         "iterations_per_solve": round(sum(iters) / total, 3),
         "converged_fraction": round(conv, 4),
         "clocks": sampler.summary(),
@@ -586,7 +708,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--refinement", type=int, default=1)
+    ap.add_argument("--refinement", type=int, default=3)
     ap.add_argument("--cpu-sample", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--start", default=None, choices=["base", "learned"],
@@ -603,11 +725,17 @@ def main():
                          "the solves' narrow levels too")
     ap.add_argument("--outages", type=int, default=N_OUTAGES,
                     help="outages per GPU (500 is the benchmark; smaller batches are profiling cases)")
+    ap.add_argument("--mixed-policy", default="fp64near", choices=["fp64near", "refine"],
+                    help="fp64near: iterations with a scenario near convergence run in FP64; refine: FP32 LU with "
+                         "FP64 refinement of the scenarios near convergence")
+    ap.add_argument("--device-loop", type=int, default=1, choices=[0, 1],
+                    help="1: the whole Newton loop as one graph launch (conditional nodes)")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batching measurement of the default line")
     ap.add_argument("--workload", default="n1", choices=["n1", "uneven"],
                     help="n1: the 9,241-bus N-1 batch (default); uneven: four grids in one persistent launch")
     args = ap.parse_args()
     if args.plan is None:
-        args.plan = "scaled" if args.workload == "uneven" else "dense"
+        args.plan = "dense"
     if args.start is None:
         args.start = "learned" if os.path.exists(args.checkpoint) and args.outages == N_OUTAGES else "base"
     args.warmup = max(args.warmup, 3) if args.impl == "engine" else args.warmup

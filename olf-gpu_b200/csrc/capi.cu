@@ -644,17 +644,18 @@ extern "C" int olfgpu_solve_batch_context_full(
         r.slackDistTol = slackDistTol;
         r.rejectDsFailure = rejectSlackDistributionFailure != 0;
         r.laneLive = live.empty() ? nullptr : live.data();
-        c.solveCount++;
         c.handedBack.resize(nLocal);
         for (int j = 0; j < nLocal; j++) c.handedBack[j] = slots.empty() ? j : slots[j];
         if (slots.empty() && c.statesToHost) {
             solveBatch(c, r, out);
+            c.solveCount++;             // a refused request is not a solve
             return;
         }
         // result rows of the installed scenarios, in installation order: [x(n), iterations, ||F||inf, status], or the
         // three last alone when the states stay on the device (olfgpu_set_states_to_host)
         std::vector<double> bank(static_cast<size_t>(nS) * (n + 3));
         solveBatch(c, r, bank.data());
+        c.solveCount++;
         const int width = c.statesToHost ? n + 3 : 3;
         for (int j = 0; j < nLocal; j++) {
             const double* row = &bank[static_cast<size_t>(c.handedBack[j]) * (n + 3)];

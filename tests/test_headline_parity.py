@@ -71,7 +71,7 @@ def test_polishing_step_brings_learned_lanes_next_to_the_solution(engine_lib, he
     learned = LearnedStart.load(CHECKPOINT, g)
     x0_dev = torch.empty((ns, p.n), dtype=torch.float64, device="cuda")
     learned.predict_device(p, p.x_base, outs, out=x0_dev)
-    out = {}
+    out, kept = {}, {}
     for ratio in (0.0, 1e-2):
         ctx = native.BatchContext(s, ns)
         ctx.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
@@ -79,6 +79,8 @@ def test_polishing_step_brings_learned_lanes_next_to_the_solution(engine_lib, he
         ctx.set_start_polish(ratio)
         ctx.set_device_start(x0_dev)
         out[ratio] = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
+        kept[ratio] = np.ones(ns, bool)                    # the scenarios that stayed on their learned start
+        kept[ratio][ctx.last_fallbacks()] = False
         ctx.set_device_start(None)
     # the solution itself: the base-start states taken one step further (max |F| far below the tolerance)
     base = native.BatchContext(s, ns)
@@ -88,9 +90,14 @@ def test_polishing_step_brings_learned_lanes_next_to_the_solution(engine_lib, he
     n = p.n
     conv = (out[1e-2][:, n + 2] == 0) & (x_star[:, n + 2] == 0)
     assert conv.sum() > 0.9 * ns
-    polished = np.abs(out[1e-2][conv, :n] - x_star[conv, :n]).max()
-    plain = np.abs(out[0.0][conv, :n] - x_star[conv, :n]).max()
+    learned_lanes = conv & kept[1e-2] & kept[0.0]
+    assert learned_lanes.sum() > 50
+    polished = np.abs(out[1e-2][learned_lanes, :n] - x_star[learned_lanes, :n]).max()
+    plain = np.abs(out[0.0][learned_lanes, :n] - x_star[learned_lanes, :n]).max()
     assert polished <= 1e-9 < plain, (polished, plain)
+    # the scenarios on the base start follow the oracle's own trajectory
+    base_lanes = conv & ~kept[1e-2]
+    assert np.abs(out[1e-2][base_lanes, :n] - ref[base_lanes, :n]).max() <= 1e-11
 
 
 @pytest.mark.parametrize("precision", [0, 1])
