@@ -424,8 +424,16 @@ def test_dense_front_plan_rejected_by_tiles(engine_lib):
     ctx.set_schedule(native.PERSISTENT, 2, 256)
     with pytest.raises(native.NativeError, match="dense-front"):
         ctx.solve(p.x_base, p.target, p.base_row_mode, np.zeros((4, p.n_elements), np.uint8))
+    # a multi-grid launch takes the member, but its persistent tiles refuse the plan (its device loops run it)
+    ctx.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
+    ctx.stage(p.x_base, p.target, p.base_row_mode, np.zeros((4, p.n_elements), np.uint8))
+    m = native.MultiContext([ctx])
+    m.set_schedule(2, 256, 0)
     with pytest.raises(native.NativeError, match="dense-front"):
-        native.MultiContext([ctx])
+        m.solve()
+    m.set_schedule(0, 0, 0)
+    outs, _ = m.solve()
+    assert np.all(outs[0][:, p.n + 2] == 0)
 
 
 @pytest.mark.parametrize("precision", [0, 1])
@@ -479,3 +487,22 @@ def test_transposed_solve_matches_oracle(engine_lib, oracle_mod, precision, tol,
     # adjoint identity: <y, J x> = <J^T y, x> = <c, x> for the solved pairs
     _, y_only = ctx.linear_solve_transposed(J, None, rhs_t, precision)
     assert np.array_equal(y_only, ys)
+
+
+def test_config1_every_non_bridge_outage_of_the_2000_bus_grid(engine_lib, oracle_mod):
+    """The batched N-1 configuration at full size: every non-bridge (non-parallel) single-branch outage of the
+    2,000-bus grid in ONE uniform FP64 batch sharing one structure, warm-started from the base case, tol 1e-8 pu,
+    through the device-resident loop; every scenario's status and converged state match the oracle."""
+    from olfgpu import native, synthetic
+    g, p = grid("grid2000")
+    outs = synthetic.outage_candidates(g)
+    assert outs.shape[0] > 2000
+    dis = p.outage_masks(outs)
+    s = native.Structure(p, native.PLAN_DENSE_FRONT)
+    ctx = native.BatchContext(s, outs.shape[0])
+    ctx.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
+    ctx.set_device_loop(True)
+    r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
+    ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis)
+    _compare(r, ref, p.n)
+    assert np.array_equal(r[:, p.n].astype(int), ref[:, p.n].astype(int))
