@@ -215,6 +215,32 @@ def run_engine(args, rank: int, world: int):
         ctx.set_fallback_start(True)           # per lane: the better start by initial mismatch, restart on failure
         ctx.set_device_start(x0_dev)
 
+    # concurrent parts: the batch split into lane ranges solved as concurrent device loops in one graph launch
+    cb = None
+    part_schedule = None
+    if args.parts > 1:
+        from olfgpu.security_analysis import ConcurrentBatch
+        if learned is not None:
+            learned.predict_device(p, x0, outs, out=x0_dev)
+        ctx.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)      # the single context's autotune
+        part_schedule = tuple(ctx.schedule()[0])
+        if part_schedule[0] in (native.PERSISTENT, native.COOPERATIVE):
+            part_schedule = (native.LEVELS_SHARED_ALL, 0, 256)
+        cb = ConcurrentBatch(s, ns, args.parts, precision, max(refinement, 0), policy, part_schedule)
+        if learned is not None:
+            cb.set_device_start(x0_dev)
+
+    def solve_once(c_single, c_parts, xs):
+        """One solve of the batch: device ms and per-scenario total iterations."""
+        if c_parts is not None:
+            _, ms = c_parts.solve(xs, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
+            return ms, np.concatenate([c.last_stats()[2] for c in c_parts.contexts])
+        c_single.solve(xs, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
+        ms, _, tot = c_single.last_stats()
+        return ms, tot
+
+    last = {}
+
     def step():
         """One batch: the learned-start prediction (on the device), then the solve; returns the prediction's device
         milliseconds (0 with the base start)."""
@@ -225,7 +251,7 @@ def run_engine(args, rank: int, world: int):
             ev1.record()
             ev1.synchronize()
             pred_ms = ev0.elapsed_time(ev1)
-        ctx.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
+        last["ms"], last["tot"] = solve_once(ctx, cb, x0)
         return pred_ms
 
     for _ in range(args.warmup):
@@ -246,12 +272,13 @@ def run_engine(args, rank: int, world: int):
             t0 = time.perf_counter()
             pred_ms = step()
             wall_ms.append((time.perf_counter() - t0) * 1e3)
-            ms, batched, tot = ctx.last_stats()
+            ms, tot = last["ms"], last["tot"]
             dev_ms.append(ms + pred_ms)
             pred_total += pred_ms
             tot_iters += int(tot.sum())
-    fallbacks = int(ctx.last_fallbacks().size) if learned is not None else 0
-    fp64_iterations = ctx.last_fp64_iterations()
+    solver = cb if cb is not None else ctx
+    fallbacks = int(solver.last_fallbacks().size) if learned is not None else 0
+    fp64_iterations = solver.last_fp64_iterations()
     torch.cuda.synchronize()
     result = out.copy()                         # the last timed solve's states, iterations and statuses
     dev = float(np.mean(dev_ms))
@@ -270,21 +297,24 @@ def run_engine(args, rank: int, world: int):
         """The engine from the base start (or ``start`` [n], e.g. the flat start) on the same batch at a given
         precision and policy: device time per step, iteration histogram, and each scenario's difference from the
         measured configuration's result (scenarios both converged)."""
-        c = native.BatchContext(s, ns)
-        c.set_linear_solver_settings(prec, refine)
-        c.set_mixed_precision_policy(pol)
-        c.set_device_loop(args.device_loop)
-        if args.schedule == "auto":
-            c.set_schedule(native.AUTOTUNE)
-        else:
-            c.set_schedule(*ctx.schedule()[0])
         xs = x0 if start is None else start
+        if cb is not None:
+            from olfgpu.security_analysis import ConcurrentBatch
+            c = ConcurrentBatch(s, ns, args.parts, prec, refine, pol, part_schedule)
+        else:
+            c = native.BatchContext(s, ns)
+            c.set_linear_solver_settings(prec, refine)
+            c.set_mixed_precision_policy(pol)
+            c.set_device_loop(args.device_loop)
+            if args.schedule == "auto":
+                c.set_schedule(native.AUTOTUNE)
+            else:
+                c.set_schedule(*ctx.schedule()[0])
         for _ in range(args.warmup):
-            c.solve(xs, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
+            solve_once(c, c if cb is not None else None, xs)
         pm = []
         for _ in range(args.steps):
-            c.solve(xs, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
-            pm.append(c.last_stats()[0])
+            pm.append(solve_once(c, c if cb is not None else None, xs)[0])
         f64 = c.last_fp64_iterations()
         c.close()
         both = (result[:, p.n + 2] == 0) & (out[:, p.n + 2] == 0)
@@ -312,22 +342,31 @@ def run_engine(args, rank: int, world: int):
             refine_policy = comparison(native.MIXED, max(refinement, 3), native.MIXED_REFINE)
     # roofline of the Newton iterations (HBM-bound): algorithmic bytes over the device time
     peak, peak_kind = _peaks()
-    pbytes = 4 if precision == native.MIXED else 8
-    total_bytes, b_it = algorithmic_bytes(s, p, tot_iters // args.steps, pbytes, refinement)
+    # FP32 factors only in the iterations that ran in FP32 (the FP64-near policy runs the near ones in FP64)
+    all_fp64 = precision != native.MIXED or (args.mixed_policy == "fp64near" and fp64_iterations > 0 and
+                                             fp64_iterations >= int(np.max(result[:, p.n])))
+    pbytes = 8 if all_fp64 else 4
+    refine_bytes = refinement if args.mixed_policy == "refine" else 0
+    total_bytes, b_it = algorithmic_bytes(s, p, tot_iters // args.steps, pbytes, refine_bytes)
     achieved = total_bytes / (dev * 1e-3) / 1e9
     # the dominant kernel family, the block-LU factorization (factorLevelKernel + factorRangeKernel launches of one
     # Newton iteration): one more solve of the same batch, after the timed region, with each phase bracketed by CUDA
     # events on the context's stream; algorithmic bytes of one lane's factorization = read J once (8 nnzJ) + write and
     # read the LU once (2 w nnzLU)
     ctx.set_phase_timing(True)
-    step()
+    if learned is not None:
+        learned.predict_device(p, x0, outs, out=x0_dev)
+    ctx.solve(x0, tgt, mode, dis, max_iter=15, tol=TOL, out=out)
     ph = ctx.last_phase_times()
     ctx.set_phase_timing(False)
-    fact_bytes_lane = 8 * s.nnz + 2 * pbytes * s.n_lu_blocks * 4
+    ph_fp64 = ctx.last_fp64_iterations()
+    fact_w = 8 if (precision != native.MIXED or (args.mixed_policy == "fp64near" and ph_fp64 >= ph["iterations"])) \
+        else 4
+    fact_bytes_lane = 8 * s.nnz + 2 * fact_w * s.n_lu_blocks * 4
     fact_launch_ms = ph["factor"] / max(ph["iterations"], 1)
     fact_bytes_launch = fact_bytes_lane * ph["factorized_lanes"] / max(ph["iterations"], 1)
     fact_achieved = fact_bytes_launch / (fact_launch_ms * 1e-3) / 1e9 if fact_launch_ms > 0 else 0.0
-    traffic = TRAFFIC.get(args.precision)
+    traffic = TRAFFIC["fp64" if fact_w == 8 else "mixed"]
     if traffic is not None:
         traffic = int(traffic * ph["factorized_lanes"] / max(ph["iterations"], 1))
     sched = ctx.schedule()[0]
@@ -361,7 +400,7 @@ def run_engine(args, rank: int, world: int):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "fp32-lu+fp64" if precision == native.MIXED else "f64",
+        "dtype": "f64" if all_fp64 else "fp32-lu+fp64",
         "data": "synthetic (seeded 9,241-bus grid, random non-bridge branch outages)",
         "config": {"workload": f"{GRID}: 9,241 buses, {p.n_cb} branches, {ns} outages per GPU, "
                                + ("learned warm start (GNN prediction on the device inside the step; per-lane "
@@ -408,6 +447,10 @@ def run_engine(args, rank: int, world: int):
                     "FP64 (all its scenarios), the others in FP32 without refinement; refine: FP32 LU every "
                     "iteration, FP64 refinement of the scenarios below 1e-2 to a 1e-11 correction"},
         "device_loop": bool(args.device_loop),
+        "concurrent_parts": None if cb is None else {
+            "parts": len(cb.ranges), "lanes": [b - a for a, b in cb.ranges], "part_schedule": list(part_schedule),
+            "note": "the batch split into lane ranges, each its own context on the shared structure, solved as "
+                    "concurrent device-resident Newton loops in one graph launch (results identical to one batch)"},
         "learned_start": None if learned is None else {
             "checkpoint": os.path.relpath(args.checkpoint, ROOT), "prediction_ms_per_step": round(pred_total / args.steps, 4),
             "scenarios_on_base_start": fallbacks},
@@ -731,6 +774,8 @@ def main():
     ap.add_argument("--device-loop", type=int, default=1, choices=[0, 1],
                     help="1: the whole Newton loop as one graph launch (conditional nodes)")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batching measurement of the default line")
+    ap.add_argument("--parts", type=int, default=1,
+                    help="split the batch into this many lane ranges solved as concurrent device loops in one graph")
     ap.add_argument("--workload", default="n1", choices=["n1", "uneven"],
                     help="n1: the 9,241-bus N-1 batch (default); uneven: four grids in one persistent launch")
     args = ap.parse_args()

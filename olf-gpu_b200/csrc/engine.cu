@@ -2180,6 +2180,8 @@ void runMulti(MultiContext& m, bool fp32) {
     for (size_t i = 0; i < m.members.size(); i++) {
         BatchContext& c = *m.members[i];
         installLanes(c);
+        // each member starts from its selected starts (fallback mode), as a solo solve does
+        if (c.fallbackStart && c.hasX0Base && c.hasX0Full) selectStarts(c);
         OLF_CUDA(cudaEventRecord(m.ready[i], c.stream));
         OLF_CUDA(cudaStreamWaitEvent(st, m.ready[i], 0));
     }

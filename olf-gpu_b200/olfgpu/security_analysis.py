@@ -162,3 +162,60 @@ class MultiGridAnalysis:
             results.append(BatchResult(np.asarray(outs), out[:, n + 2].astype(int), out[:, n].astype(int),
                                        out[:, n + 1], out[:, :n], tot, ms))
         return results, ms
+
+
+class ConcurrentBatch:
+    """One batch of scenarios of one network split into ``parts`` lane ranges, each its own context on the shared
+    structure, solved by ONE graph launch whose branches are the parts' device-resident Newton loops (the engine's
+    multi-grid context with lanesPerTile 0).  The parts' level kernels run concurrently, so one part's dependent-level
+    latency overlaps another's work.  Every scenario's result is that of the single batch, bit for bit (lanes never
+    interact).  ``solve`` takes the arguments of BatchContext.stage for the whole batch."""
+
+    def __init__(self, structure: native.Structure, n_scenarios: int, parts: int, precision: int = native.FP64,
+                 refinement_steps: int = 1, mixed_policy: int = native.MIXED_REFINE,
+                 schedule=(native.LEVELS_SHARED_ALL, 0, 256), rl=None):
+        self.structure = structure
+        self.n = int(n_scenarios)
+        bounds = np.linspace(0, self.n, parts + 1).round().astype(int)
+        self.ranges = [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:]) if b > a]
+        self.contexts = []
+        for a, b in self.ranges:
+            c = native.BatchContext(structure, b - a, native.BATCHED_LU, rl)
+            c.set_linear_solver_settings(precision, refinement_steps)
+            c.set_mixed_precision_policy(mixed_policy)
+            c.set_schedule(*schedule)
+            c.set_device_loop(True)
+            self.contexts.append(c)
+        self.multi = native.MultiContext(self.contexts)
+        self.multi.set_schedule(0, 0, 0)
+
+    def set_device_start(self, x0_device=None, fallback: bool = True):
+        """Per-scenario start states on the device ([nS, n] torch CUDA tensor; each part reads its rows), with the
+        base-start selection, fallback and polishing of BatchContext.set_fallback_start."""
+        for c, (a, b) in zip(self.contexts, self.ranges):
+            c.set_fallback_start(fallback and x0_device is not None)
+            c.set_device_start(None if x0_device is None else x0_device[a:b])
+
+    def solve(self, x0_base, target, base_row_mode, disabled, x0_full=None, max_iter: int = 15, tol: float = 1e-8,
+              out: Optional[np.ndarray] = None):
+        """[nS][n + 3] results in scenario order (written into ``out`` when given); returns (results, device ms)."""
+        n = self.structure.n
+        if out is None:
+            out = np.zeros((self.n, n + 3))
+        for c, (a, b) in zip(self.contexts, self.ranges):
+            c.stage(x0_base, target, base_row_mode, disabled[a:b], None if x0_full is None else x0_full[a:b],
+                    max_iter=max_iter, tol=tol)
+        views = [out[a:b] for a, b in self.ranges]
+        _, ms = self.multi.solve(views)
+        return out, ms
+
+    def last_fallbacks(self) -> np.ndarray:
+        return np.concatenate([c.last_fallbacks() + a for c, (a, _) in zip(self.contexts, self.ranges)])
+
+    def last_fp64_iterations(self) -> int:
+        return max(c.last_fp64_iterations() for c in self.contexts)
+
+    def close(self):
+        self.multi.close()
+        for c in self.contexts:
+            c.close()
