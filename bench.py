@@ -606,7 +606,7 @@ def run_uneven(args, rank: int, world: int):
         dev_auto, wall_auto = timed(multi_step)
     res = last["res"]
     iters = [int(r.total_iterations.sum()) for r in res]
-    rounds = [int(c.last_stats()[1]) for c in ma.contexts]
+    rounds = [max(int(c.last_stats()[1]) for c, _, _ in mine) for mine in ma.grid_parts]
     ma.close()
     fixed = (2, 256, 0)                                # persistent tiles (the scaled plan: tiles run no dense front)
     mf = MultiGridAnalysis(packs, counts, precision=precision, refinement_steps=args.refinement, schedule=fixed)
@@ -774,8 +774,9 @@ def main():
     ap.add_argument("--device-loop", type=int, default=1, choices=[0, 1],
                     help="1: the whole Newton loop as one graph launch (conditional nodes)")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batching measurement of the default line")
-    ap.add_argument("--parts", type=int, default=1,
-                    help="split the batch into this many lane ranges solved as concurrent device loops in one graph")
+    ap.add_argument("--parts", type=int, default=8,
+                    help="split the batch into this many lane ranges solved as concurrent device loops in one graph "
+                         "(8 measured fastest on the 500-outage batch: 13.3 vs 15.6 ms per FP64 step)")
     ap.add_argument("--workload", default="n1", choices=["n1", "uneven"],
                     help="n1: the 9,241-bus N-1 batch (default); uneven: four grids in one persistent launch")
     args = ap.parse_args()

@@ -119,18 +119,30 @@ class MultiGridAnalysis:
 
     def __init__(self, packed_grids: Sequence[Packed], counts: Sequence[int], precision: int = native.FP64,
                  refinement_steps: int = 1, reactive_limits: bool = True, schedule=-1, ordering: int = 0,
-                 member_schedule=None, mixed_policy: int = native.MIXED_REFINE):
+                 member_schedule=None, mixed_policy: int = native.MIXED_REFINE, parts=1):
+        """``parts`` (an int, or one per grid): each grid's batch split into that many lane ranges, each its own member
+        context on the grid's structure (for the device loops: more concurrent branches, the same results)."""
         self.packed = list(packed_grids)
         self.counts = [int(c) for c in counts]
+        parts = [int(parts)] * len(self.packed) if np.isscalar(parts) else [int(k) for k in parts]
         self.structures = [native.Structure(p, ordering) for p in self.packed]
         self.contexts = []
-        for p, s, c in zip(self.packed, self.structures, self.counts):
-            ctx = native.BatchContext(s, c, native.BATCHED_LU, p.rl if reactive_limits and p.rl is not None else None)
-            ctx.set_linear_solver_settings(precision, refinement_steps)
-            ctx.set_mixed_precision_policy(mixed_policy)
-            if member_schedule is not None:
-                ctx.set_schedule(*member_schedule)
-            self.contexts.append(ctx)
+        self.grid_parts = []           # per grid: [(context, first scenario, end)]
+        for p, s, c, k in zip(self.packed, self.structures, self.counts, parts):
+            bounds = np.linspace(0, c, max(1, k) + 1).round().astype(int)
+            mine = []
+            for a, b in zip(bounds[:-1], bounds[1:]):
+                if b <= a:
+                    continue
+                ctx = native.BatchContext(s, int(b - a), native.BATCHED_LU,
+                                          p.rl if reactive_limits and p.rl is not None else None)
+                ctx.set_linear_solver_settings(precision, refinement_steps)
+                ctx.set_mixed_precision_policy(mixed_policy)
+                if member_schedule is not None:
+                    ctx.set_schedule(*member_schedule)
+                self.contexts.append(ctx)
+                mine.append((ctx, int(a), int(b)))
+            self.grid_parts.append(mine)
         self.multi = native.MultiContext(self.contexts)
         if schedule == -1:
             self.multi.set_schedule(-1)
@@ -147,18 +159,25 @@ class MultiGridAnalysis:
     def solve(self, outages: Sequence[Sequence[int]], max_iter: int = 15, tol: float = 1e-8,
               reactive_limit_tol: float = 1e-4, max_outer: int = 20, max_pq_pv_switch: int = 3):
         """outages[i]: grid i's outaged closed branches (exactly counts[i]); returns ([BatchResult], device ms)."""
-        for p, ctx, c, outs in zip(self.packed, self.contexts, self.counts, outages):
+        outs_all = []
+        for p, mine, c, outs in zip(self.packed, self.grid_parts, self.counts, outages):
             outs = np.asarray(outs, dtype=np.int64)
             if outs.shape[0] != c:
                 raise ValueError(f"expected {c} outages, got {outs.shape[0]}")
             x0 = p.x_base if p.x_base is not None else p.x_flat
-            ctx.stage(x0, p.target, p.base_row_mode, p.outage_masks(outs), max_iter=max_iter, tol=tol,
-                      reactive_limit_tol=reactive_limit_tol, max_outer=max_outer, max_pq_pv_switch=max_pq_pv_switch)
-        res, ms = self.multi.solve()
+            masks = p.outage_masks(outs)
+            out = np.zeros((c, p.n + 3))
+            outs_all.append(out)
+            for ctx, a, b in mine:
+                ctx.stage(x0, p.target, p.base_row_mode, masks[a:b], max_iter=max_iter, tol=tol,
+                          reactive_limit_tol=reactive_limit_tol, max_outer=max_outer,
+                          max_pq_pv_switch=max_pq_pv_switch)
+        views = [out[a:b] for out, mine in zip(outs_all, self.grid_parts) for _, a, b in mine]
+        _, ms = self.multi.solve(views)
         results = []
-        for p, ctx, outs, out in zip(self.packed, self.contexts, outages, res):
+        for p, mine, outs, out in zip(self.packed, self.grid_parts, outages, outs_all):
             n = p.n
-            _, _, tot = ctx.last_stats()
+            tot = np.concatenate([ctx.last_stats()[2] for ctx, _, _ in mine])
             results.append(BatchResult(np.asarray(outs), out[:, n + 2].astype(int), out[:, n].astype(int),
                                        out[:, n + 1], out[:, :n], tot, ms))
         return results, ms
