@@ -2328,7 +2328,12 @@ void solveMulti(MultiContext& m, double* const* outs) {
     cudaEventDestroy(e1);
     for (BatchContext* c : m.members) {
         c->lastIterations = 0;
-        if (m.lanesPerTile == 0) OLF_CUDA(cudaMemcpy(&c->lastIterations, c->loopState.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (m.lanesPerTile == 0) {
+            int st[5] = {0, 0, 0, 0, 0};
+            OLF_CUDA(cudaMemcpy(st, c->loopState.p, sizeof(st), cudaMemcpyDeviceToHost));
+            c->lastIterations = st[0];
+            c->fp64Iterations = st[4];
+        }
         c->lastMs = m.lastMs;
     }
     OLF_CUDA(cudaGetLastError());

@@ -573,12 +573,12 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
     T a00 = 0, a01 = 0, a10 = 0, a11 = 0, amax = 0;
     int t = 0;
     Task tk{};
+    int4 op0 = make_int4(-1, -1, -1, 0);
     if (ok) {
         t = net.levelTask[first + k];
         tk = net.task[t];
-    }
-    pdlWait();   // the previous level's blocks are read from here on
-    if (ok) {
+        // before the wait: the Jacobian block (written by the fill, which precedes the factorization's launches) and
+        // the thread's first update record (static); the LU blocks of earlier levels are read after it
         if (part == 0 && tk.aBlock >= 0) {
             const double* p = b.J + (size_t)tk.aBlock * 4 * S + s;
             a00 = (T)p[0];
@@ -587,9 +587,13 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
             a11 = (T)p[3 * S];
             amax = fmax(fmax(fabs(a00), fabs(a01)), fmax(fabs(a10), fabs(a11)));
         }
+        if (tk.opBegin + part < tk.opEnd) op0 = net.ops[tk.opBegin + part];
+    }
+    pdlWait();   // the previous level's blocks are read from here on
+    if (ok) {
 #pragma unroll 4
         for (int q = tk.opBegin + part; q < tk.opEnd; q += P) {
-            const int4 op = net.ops[q];
+            const int4 op = q == tk.opBegin + part ? op0 : net.ops[q];
             T m00, m01, m10, m11, u00, u01, u10, u11;
             load4(lu, (size_t)op.x, S, s, m00, m01, m10, m11);
             load4(lu, (size_t)op.y, S, s, u00, u01, u10, u11);
@@ -977,10 +981,22 @@ __global__ void __launch_bounds__(1024) forwardLevelKernel(DevNet net, DevBatch 
     const bool ok = k < count && s < b.S && solving(b, s);
     T w0 = 0, w1 = 0;
     int i = 0, q0 = 0, q1 = 0;
+    // the thread's first two L blocks, read before the wait: the factors are final for the whole solve (its first
+    // kernel is a normal launch after the factorization) and only the solution entries depend on earlier levels
+    int2 e0 = make_int2(0, -1), e1 = make_int2(0, -1);
+    T a00 = 0, a01 = 0, a10 = 0, a11 = 0, c00 = 0, c01 = 0, c10 = 0, c11 = 0;
     if (ok) {
         i = pos[first + k];
-        q0 = net.lrowPtr[i];
+        q0 = net.lrowPtr[i] + part;
         q1 = net.lrowEnd[i];
+        if (q0 < q1) {
+            e0 = net.lrow[q0];
+            load4(lu, (size_t)e0.x, S, s, a00, a01, a10, a11);
+        }
+        if (q0 + P < q1) {
+            e1 = net.lrow[q0 + P];
+            load4(lu, (size_t)e1.x, S, s, c00, c01, c10, c11);
+        }
     }
     pdlWait();   // the previous level's solution entries are read from here on
     if (ok) {
@@ -988,8 +1004,18 @@ __global__ void __launch_bounds__(1024) forwardLevelKernel(DevNet net, DevBatch 
             w0 = w[(2 * (size_t)i) * S + s];
             w1 = w[(2 * (size_t)i + 1) * S + s];
         }
+        if (e0.y >= 0) {
+            const T y0 = w[(2 * (size_t)e0.y) * S + s], y1 = w[(2 * (size_t)e0.y + 1) * S + s];
+            w0 -= a00 * y0 + a01 * y1;
+            w1 -= a10 * y0 + a11 * y1;
+        }
+        if (e1.y >= 0) {
+            const T y0 = w[(2 * (size_t)e1.y) * S + s], y1 = w[(2 * (size_t)e1.y + 1) * S + s];
+            w0 -= c00 * y0 + c01 * y1;
+            w1 -= c10 * y0 + c11 * y1;
+        }
 #pragma unroll 4
-        for (int q = q0 + part; q < q1; q += P) {
+        for (int q = q0 + 2 * P; q < q1; q += P) {
             const int2 e = net.lrow[q];
             T l00, l01, l10, l11;
             load4(lu, (size_t)e.x, S, s, l00, l01, l10, l11);
@@ -1028,10 +1054,25 @@ __global__ void __launch_bounds__(1024) backwardLevelKernel(DevNet net, DevBatch
     const bool ok = k < count && s < b.S && solving(b, s);
     T w0 = 0, w1 = 0;
     int i = 0, d = 0, q1 = 0;
+    // the pivot inverse and the thread's first two U blocks, read before the wait (the factors are final for the
+    // whole solve; only the solution entries depend on earlier levels)
+    int j0 = -1, j1 = -1;
+    T i00 = 0, i01 = 0, i10 = 0, i11 = 0;
+    T a00 = 0, a01 = 0, a10 = 0, a11 = 0, c00 = 0, c01 = 0, c10 = 0, c11 = 0;
     if (ok) {
         i = pos[first + k];
         d = net.uPtr[i];
         q1 = net.uPtr[i + 1];
+        if (part == 0) load4(lu, (size_t)d, S, s, i00, i01, i10, i11);
+        const int qa = d + 1 + part;
+        if (qa < q1) {
+            j0 = net.uCol[qa];
+            load4(lu, (size_t)qa, S, s, a00, a01, a10, a11);
+        }
+        if (qa + P < q1) {
+            j1 = net.uCol[qa + P];
+            load4(lu, (size_t)(qa + P), S, s, c00, c01, c10, c11);
+        }
     }
     pdlWait();   // the previous level's solution entries are read from here on
     if (ok) {
@@ -1039,8 +1080,18 @@ __global__ void __launch_bounds__(1024) backwardLevelKernel(DevNet net, DevBatch
             w0 = w[(2 * (size_t)i) * S + s];
             w1 = w[(2 * (size_t)i + 1) * S + s];
         }
+        if (j0 >= 0) {
+            const T x0 = w[(2 * (size_t)j0) * S + s], x1 = w[(2 * (size_t)j0 + 1) * S + s];
+            w0 -= a00 * x0 + a01 * x1;
+            w1 -= a10 * x0 + a11 * x1;
+        }
+        if (j1 >= 0) {
+            const T x0 = w[(2 * (size_t)j1) * S + s], x1 = w[(2 * (size_t)j1 + 1) * S + s];
+            w0 -= c00 * x0 + c01 * x1;
+            w1 -= c10 * x0 + c11 * x1;
+        }
 #pragma unroll 4
-        for (int q = d + 1 + part; q < q1; q += P) {
+        for (int q = d + 1 + part + 2 * P; q < q1; q += P) {
             const int j = net.uCol[q];
             T u00, u01, u10, u11;
             load4(lu, (size_t)q, S, s, u00, u01, u10, u11);
@@ -1061,8 +1112,6 @@ __global__ void __launch_bounds__(1024) backwardLevelKernel(DevNet net, DevBatch
         }
     }
     if (!ok || part != 0) return;
-    T i00, i01, i10, i11;
-    load4(lu, (size_t)d, S, s, i00, i01, i10, i11);
     w[(2 * (size_t)i) * S + s] = i00 * w0 + i01 * w1;
     w[(2 * (size_t)i + 1) * S + s] = i10 * w0 + i11 * w1;
 }
