@@ -71,15 +71,15 @@ __device__ void factorVBlock(const DevNet& net, const DevBatch& b, T* lu, int fi
                 T d00, d01, d10, d11;
                 ld4c(lu, (size_t)op.z, S, s, d00, d01, d10, d11);
                 const T l00 = m00, l01 = m01, l10 = m10, l11 = m11;
-                m00 = l00 * d00 + l01 * d10;
-                m01 = l00 * d01 + l01 * d11;
-                m10 = l10 * d00 + l11 * d10;
-                m11 = l10 * d01 + l11 * d11;
+                m00 = dot2(l00, d00, l01, d10);
+                m01 = dot2(l00, d01, l01, d11);
+                m10 = dot2(l10, d00, l11, d10);
+                m11 = dot2(l10, d01, l11, d11);
             }
-            a00 -= m00 * u00 + m01 * u10;
-            a01 -= m00 * u01 + m01 * u11;
-            a10 -= m10 * u00 + m11 * u10;
-            a11 -= m10 * u01 + m11 * u11;
+            a00 = rnSub(a00, dot2(m00, u00, m01, u10));
+            a01 = rnSub(a01, dot2(m00, u01, m01, u11));
+            a10 = rnSub(a10, dot2(m10, u00, m11, u10));
+            a11 = rnSub(a11, dot2(m10, u01, m11, u11));
         }
     }
     if (P > 1) {
@@ -100,7 +100,7 @@ __device__ void factorVBlock(const DevNet& net, const DevBatch& b, T* lu, int fi
     }
     if (!ok || part != 0) return;
     if (tk.diag == -2) {
-        const T det = a00 * a11 - a01 * a10;
+        const T det = rnFma(a00, a11, -rnMul(a01, a10));
         const T scale = fabs(a00 * a11) + fabs(a01 * a10);
         if (!(fabs(det) > (T)1e-13 * scale) || !isfinite(det)) b.trouble[s] = 1;
         const T inv = (T)1 / det;
@@ -114,8 +114,8 @@ __device__ void factorVBlock(const DevNet& net, const DevBatch& b, T* lu, int fi
     } else if (tk.diag >= 0 && !net.deferredL) {
         T i00, i01, i10, i11;
         ld4c(lu, (size_t)tk.diag, S, s, i00, i01, i10, i11);
-        st4c(lu, (size_t)t, S, s, a00 * i00 + a01 * i10, a00 * i01 + a01 * i11, a10 * i00 + a11 * i10,
-             a10 * i01 + a11 * i11);
+        st4c(lu, (size_t)t, S, s, dot2(a00, i00, a01, i10), dot2(a00, i01, a01, i11), dot2(a10, i00, a11, i10),
+             dot2(a10, i01, a11, i11));
     } else {
         st4c(lu, (size_t)t, S, s, a00, a01, a10, a11);
     }
@@ -148,8 +148,8 @@ __global__ void __launch_bounds__(512) factorCoopKernel(DevNet net, DevBatch b, 
             T a00, a01, a10, a11, i00, i01, i10, i11;
             ld4c(lu, (size_t)id, S, s, a00, a01, a10, a11);
             ld4c(lu, (size_t)net.task[id].diag, S, s, i00, i01, i10, i11);
-            st4c(lu, (size_t)id, S, s, a00 * i00 + a01 * i10, a00 * i01 + a01 * i11, a10 * i00 + a11 * i10,
-                 a10 * i01 + a11 * i11);
+            st4c(lu, (size_t)id, S, s, dot2(a00, i00, a01, i10), dot2(a00, i01, a01, i11), dot2(a10, i00, a11, i10),
+                 dot2(a10, i01, a11, i11));
         }
     }
 }
@@ -179,8 +179,8 @@ __device__ void solveVBlock(const DevNet& net, const DevBatch& b, const T* lu, T
                 T l00, l01, l10, l11;
                 ld4c(lu, (size_t)e.x, S, s, l00, l01, l10, l11);
                 const T y0 = w[(2 * (size_t)e.y) * S + s], y1 = w[(2 * (size_t)e.y + 1) * S + s];
-                w0 -= l00 * y0 + l01 * y1;
-                w1 -= l10 * y0 + l11 * y1;
+                w0 = rnSub(w0, dot2(l00, y0, l01, y1));
+                w1 = rnSub(w1, dot2(l10, y0, l11, y1));
             }
         } else {
 #pragma unroll 4
@@ -189,8 +189,8 @@ __device__ void solveVBlock(const DevNet& net, const DevBatch& b, const T* lu, T
                 T u00, u01, u10, u11;
                 ld4c(lu, (size_t)q, S, s, u00, u01, u10, u11);
                 const T x0 = w[(2 * (size_t)j) * S + s], x1 = w[(2 * (size_t)j + 1) * S + s];
-                w0 -= u00 * x0 + u01 * x1;
-                w1 -= u10 * x0 + u11 * x1;
+                w0 = rnSub(w0, dot2(u00, x0, u01, x1));
+                w1 = rnSub(w1, dot2(u10, x0, u11, x1));
             }
         }
     }
@@ -213,8 +213,8 @@ __device__ void solveVBlock(const DevNet& net, const DevBatch& b, const T* lu, T
     } else {
         T i00, i01, i10, i11;
         ld4c(lu, (size_t)net.uPtr[i], S, s, i00, i01, i10, i11);
-        w[(2 * (size_t)i) * S + s] = i00 * w0 + i01 * w1;
-        w[(2 * (size_t)i + 1) * S + s] = i10 * w0 + i11 * w1;
+        w[(2 * (size_t)i) * S + s] = dot2(i00, w0, i01, w1);
+        w[(2 * (size_t)i + 1) * S + s] = dot2(i10, w0, i11, w1);
     }
 }
 

@@ -601,15 +601,15 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
                 T d00, d01, d10, d11;
                 load4(lu, (size_t)op.z, S, s, d00, d01, d10, d11);
                 const T l00 = m00, l01 = m01, l10 = m10, l11 = m11;
-                m00 = l00 * d00 + l01 * d10;
-                m01 = l00 * d01 + l01 * d11;
-                m10 = l10 * d00 + l11 * d10;
-                m11 = l10 * d01 + l11 * d11;
+                m00 = dot2(l00, d00, l01, d10);
+                m01 = dot2(l00, d01, l01, d11);
+                m10 = dot2(l10, d00, l11, d10);
+                m11 = dot2(l10, d01, l11, d11);
             }
-            a00 -= m00 * u00 + m01 * u10;
-            a01 -= m00 * u01 + m01 * u11;
-            a10 -= m10 * u00 + m11 * u10;
-            a11 -= m10 * u01 + m11 * u11;
+            a00 = rnSub(a00, dot2(m00, u00, m01, u10));
+            a01 = rnSub(a01, dot2(m00, u01, m01, u11));
+            a10 = rnSub(a10, dot2(m10, u00, m11, u10));
+            a11 = rnSub(a11, dot2(m10, u01, m11, u11));
         }
     }
     if (P > 1) {
@@ -629,7 +629,7 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
     }
     if (!ok || part != 0) return;
     if (tk.diag == -2) {
-        const T det = a00 * a11 - a01 * a10;
+        const T det = rnFma(a00, a11, -rnMul(a01, a10));
         const T scale = fabs(a00 * a11) + fabs(a01 * a10);
         if (!(fabs(det) > (T)1e-13 * scale) || !isfinite(det)) b.trouble[s] = 1;
         const T inv = (T)1 / det;
@@ -639,8 +639,8 @@ __global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b
         // default plan: L(i,k) = (...) inv(D_k), the pivot inverted one level earlier
         T i00, i01, i10, i11;
         load4(lu, (size_t)tk.diag, S, s, i00, i01, i10, i11);
-        store4(lu, (size_t)t, S, s, a00 * i00 + a01 * i10, a00 * i01 + a01 * i11, a10 * i00 + a11 * i10,
-               a10 * i01 + a11 * i11);
+        store4(lu, (size_t)t, S, s, dot2(a00, i00, a01, i10), dot2(a00, i01, a01, i11), dot2(a10, i00, a11, i10),
+               dot2(a10, i01, a11, i11));
     } else {
         store4(lu, (size_t)t, S, s, a00, a01, a10, a11);
     }
@@ -657,8 +657,8 @@ __global__ void scaleLKernel(DevNet net, DevBatch b, T* lu) {
     T a00, a01, a10, a11, i00, i01, i10, i11;
     load4(lu, (size_t)id, S, s, a00, a01, a10, a11);
     load4(lu, (size_t)net.task[id].diag, S, s, i00, i01, i10, i11);
-    store4(lu, (size_t)id, S, s, a00 * i00 + a01 * i10, a00 * i01 + a01 * i11, a10 * i00 + a11 * i10,
-           a10 * i01 + a11 * i11);
+    store4(lu, (size_t)id, S, s, dot2(a00, i00, a01, i10), dot2(a00, i01, a01, i11), dot2(a10, i00, a11, i10),
+           dot2(a10, i01, a11, i11));
 }
 
 __global__ void clearTroubleKernel(DevBatch b) {
@@ -770,7 +770,7 @@ __global__ void __launch_bounds__(256) subtreeFactorKernel(DevNet net, DevBatch 
             }
             if (!has || part != 0) continue;
             if (tk.diag == -2) {
-                const T det = a00 * a11 - a01 * a10;
+                const T det = rnFma(a00, a11, -rnMul(a01, a10));
                 const T scale = fabs(a00 * a11) + fabs(a01 * a10);
                 if (!(fabs(det) > (T)1e-13 * scale) || !isfinite(det)) b.trouble[s] = TROUBLE_PIVOT;
                 const T inv = (T)1 / det;
@@ -1006,13 +1006,13 @@ __global__ void __launch_bounds__(1024) forwardLevelKernel(DevNet net, DevBatch 
         }
         if (e0.y >= 0) {
             const T y0 = w[(2 * (size_t)e0.y) * S + s], y1 = w[(2 * (size_t)e0.y + 1) * S + s];
-            w0 -= a00 * y0 + a01 * y1;
-            w1 -= a10 * y0 + a11 * y1;
+            w0 = rnSub(w0, dot2(a00, y0, a01, y1));
+            w1 = rnSub(w1, dot2(a10, y0, a11, y1));
         }
         if (e1.y >= 0) {
             const T y0 = w[(2 * (size_t)e1.y) * S + s], y1 = w[(2 * (size_t)e1.y + 1) * S + s];
-            w0 -= c00 * y0 + c01 * y1;
-            w1 -= c10 * y0 + c11 * y1;
+            w0 = rnSub(w0, dot2(c00, y0, c01, y1));
+            w1 = rnSub(w1, dot2(c10, y0, c11, y1));
         }
 #pragma unroll 4
         for (int q = q0 + 2 * P; q < q1; q += P) {
@@ -1020,8 +1020,8 @@ __global__ void __launch_bounds__(1024) forwardLevelKernel(DevNet net, DevBatch 
             T l00, l01, l10, l11;
             load4(lu, (size_t)e.x, S, s, l00, l01, l10, l11);
             const T y0 = w[(2 * (size_t)e.y) * S + s], y1 = w[(2 * (size_t)e.y + 1) * S + s];
-            w0 -= l00 * y0 + l01 * y1;
-            w1 -= l10 * y0 + l11 * y1;
+            w0 = rnSub(w0, dot2(l00, y0, l01, y1));
+            w1 = rnSub(w1, dot2(l10, y0, l11, y1));
         }
     }
     if (P > 1) {
@@ -1082,13 +1082,13 @@ __global__ void __launch_bounds__(1024) backwardLevelKernel(DevNet net, DevBatch
         }
         if (j0 >= 0) {
             const T x0 = w[(2 * (size_t)j0) * S + s], x1 = w[(2 * (size_t)j0 + 1) * S + s];
-            w0 -= a00 * x0 + a01 * x1;
-            w1 -= a10 * x0 + a11 * x1;
+            w0 = rnSub(w0, dot2(a00, x0, a01, x1));
+            w1 = rnSub(w1, dot2(a10, x0, a11, x1));
         }
         if (j1 >= 0) {
             const T x0 = w[(2 * (size_t)j1) * S + s], x1 = w[(2 * (size_t)j1 + 1) * S + s];
-            w0 -= c00 * x0 + c01 * x1;
-            w1 -= c10 * x0 + c11 * x1;
+            w0 = rnSub(w0, dot2(c00, x0, c01, x1));
+            w1 = rnSub(w1, dot2(c10, x0, c11, x1));
         }
 #pragma unroll 4
         for (int q = d + 1 + part + 2 * P; q < q1; q += P) {
@@ -1096,8 +1096,8 @@ __global__ void __launch_bounds__(1024) backwardLevelKernel(DevNet net, DevBatch
             T u00, u01, u10, u11;
             load4(lu, (size_t)q, S, s, u00, u01, u10, u11);
             const T x0 = w[(2 * (size_t)j) * S + s], x1 = w[(2 * (size_t)j + 1) * S + s];
-            w0 -= u00 * x0 + u01 * x1;
-            w1 -= u10 * x0 + u11 * x1;
+            w0 = rnSub(w0, dot2(u00, x0, u01, x1));
+            w1 = rnSub(w1, dot2(u10, x0, u11, x1));
         }
     }
     if (P > 1) {
@@ -1112,8 +1112,8 @@ __global__ void __launch_bounds__(1024) backwardLevelKernel(DevNet net, DevBatch
         }
     }
     if (!ok || part != 0) return;
-    w[(2 * (size_t)i) * S + s] = i00 * w0 + i01 * w1;
-    w[(2 * (size_t)i + 1) * S + s] = i10 * w0 + i11 * w1;
+    w[(2 * (size_t)i) * S + s] = dot2(i00, w0, i01, w1);
+    w[(2 * (size_t)i + 1) * S + s] = dot2(i10, w0, i11, w1);
 }
 
 template <typename T>

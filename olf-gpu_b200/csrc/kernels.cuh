@@ -83,6 +83,18 @@ struct DevNet {
 __device__ __forceinline__ void pdlTrigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdlWait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// The 2x2 block expressions with every rounding written out (the compiler contracts nothing here): the level kernels
+// and the cooperative sweeps, compiled separately, give the same bits.  dot2(a, x, b, y) = a x + b y as
+// fma(a, x, round(b y)).
+__device__ __forceinline__ double rnMul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rnMul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rnFma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float rnFma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double rnSub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float rnSub(float a, float b) { return __fsub_rn(a, b); }
+template <typename T>
+__device__ __forceinline__ T dot2(T a, T x, T b, T y) { return rnFma(a, x, rnMul(b, y)); }
+
 // Per-batch device state (lane-interleaved arrays).
 struct DevBatch {
     int S;                    // lane stride (multiple of 32)
