@@ -432,7 +432,7 @@ def run_engine(args, rank: int, world: int):
         "plain_fp64_base_start": plain,
         "mixed_base_start": mixed_base,
         "starts": None if plain is None else {
-            "judge": "the engine's own Newton loop at 1e-8 pu decides every start's convergence",
+            "referee": "the engine's own Newton loop at 1e-8 pu decides every start's convergence",
             "learned" if learned is not None else "base (measured)": {
                 "ms_per_step": round(dev, 4), "iterations_per_solve": round(float(result[:, p.n].mean()), 3),
                 "iteration_histogram": histogram(result), "converged_fraction": round(conv, 4),

@@ -1477,7 +1477,7 @@ void launchResidualCheck(const DevNet& net, const DevBatch& b, double threshold,
 }
 
 // After a correction solve: the lanes still refining are those whose correction max |d| (in b.res, reduced into
-// b.resNorm) is above the bound; a NaN correction stops the lane's refinement (its next test judges it).
+// b.resNorm) is above the bound; a NaN correction stops the lane's refinement (its next test decides its status).
 __global__ void correctionCountKernel(DevBatch b, double bound) {
     __shared__ int part[32];
     int c = 0;

@@ -392,7 +392,7 @@ def _histogram(it: np.ndarray, ok: np.ndarray) -> dict:
 
 def evaluate_starts(ls: "LearnedStart", scaling: float, n_outages: int, seed: int, max_iter: int = 15,
                     tol: float = 1e-8) -> dict:
-    """Learned vs base vs flat start on ``n_outages`` outages at the load ``scaling`` (FP64 Newton judges each start
+    """Learned vs base vs flat start on ``n_outages`` outages at the load ``scaling`` (FP64 Newton referees each start
     alone; the learned start is also run the way the product runs it: per scenario the better start by initial
     mismatch, and a failed scenario restarts from the base start).  Iterations, converged fraction, the iteration
     histogram and the start error against the converged states."""
@@ -407,13 +407,13 @@ def evaluate_starts(ls: "LearnedStart", scaling: float, n_outages: int, seed: in
     s = native.Structure(p, native.PLAN_DENSE_FRONT)
     ctx = native.BatchContext(s, n_outages)
     ctx.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
-    # the judge: FP64 Newton from the base start (the converged states the starts are measured against)
+    # the referee: FP64 Newton from the base start (the converged states the starts are measured against)
     ref = ctx.solve(xb, p.target, p.base_row_mode, dis, max_iter=max_iter, tol=tol).copy()
     ok_ref = ref[:, -1] == native.CONVERGED
     learned = ls.predict(p, xb, outs)
     starts = {"learned": learned, "base": np.tile(xb, (n_outages, 1)), "flat": np.tile(p.x_flat, (n_outages, 1))}
     report = {"grid": ls.grid.spec.name, "scaling": scaling, "outages": n_outages, "seed": seed, "tol": tol,
-              "judge_converged_fraction": float(ok_ref.mean())}
+              "referee_converged_fraction": float(ok_ref.mean())}
     for name, x0 in starts.items():
         r = ctx.solve(None, p.target, p.base_row_mode, dis, x0_full=x0, max_iter=max_iter, tol=tol)
         ok = r[:, -1] == native.CONVERGED
@@ -424,14 +424,14 @@ def evaluate_starts(ls: "LearnedStart", scaling: float, n_outages: int, seed: in
                         "iteration_histogram": _histogram(r[:, p.n], ok),
                         "one_iteration_fraction": float(((r[:, p.n] == 1) & ok).mean()),
                         "start_error": _start_error(x0, ref[:, :p.n], ok_ref),
-                        "max_state_difference_vs_judge": float(d.max())}
+                        "max_state_difference_vs_referee": float(d.max())}
     r, tot, fell = solve_with_fallback(ctx, p, learned, xb, dis, max_iter=max_iter, tol=tol)
     ok = r[:, -1] == native.CONVERGED
     report["learned_with_fallback"] = {"converged_fraction": float(ok.mean()),
                                        "iterations_per_solve": float(tot[ok].mean()) if ok.any() else None,
                                        "iteration_histogram": _histogram(r[:, p.n], ok),
                                        "scenarios_on_base_start": int(fell.size),
-                                       "same_status_as_judge": int((r[:, -1] == ref[:, -1]).sum())}
+                                       "same_status_as_referee": int((r[:, -1] == ref[:, -1]).sum())}
     return report
 
 
