@@ -441,7 +441,10 @@ int olfgpu_linear_solve_transposed(int64_t context, const double* csrVals, const
  * graph, BF16 weights and activations with FP32 accumulation, on caller-owned device buffers, enqueued on `stream`.
  * Row-major matrices; M rows = samples x buses.
  *   gemm:     Y = [A1 | A2] . W (+ bias), z = relu ? max(Y, 0) : Y (saved to saveZ if given), out = z (+ residual);
- *             shapes (K1, K2, N) in {(16,0,64), (64,0,128), (64,64,64), (64,0,16), (128,0,64)}; tensor cores.
+ *             shapes (K1, K2, N) in {(16,0,64), (64,0,128), (64,64,64), (64,0,16), (128,0,64)}; fifth-generation
+ *             tensor cores (tcgen05.mma, FP32 accumulators in tensor memory, 128-row tiles).  Its completion wait is
+ *             bounded; olfgpu_gnn_tc_timeouts reads how many tiles gave up waiting since the library was loaded
+ *             (synchronises the device; always 0 on a working GPU).
  *   gemm_dw:  dW = [A1 | A2]^T dZ and db = column sums of dZ, summed over at most maxChunks row chunks in a fixed order
  *             (partial holds maxChunks * (K * N + N) floats); shapes (16,0,64), (64,0,128), (64,64,64), (64,0,16).
  *   copy_cols: dst[r, dstCol0 + c] (+)= src[r, srcCol0 + c], FP32.
@@ -453,6 +456,7 @@ int olfgpu_linear_solve_transposed(int64_t context, const double* csrVals, const
  * olfgpu_gnn_last_error() reports the calling thread's last failure of these functions.
  */
 const char* olfgpu_gnn_last_error(void);
+int olfgpu_gnn_tc_timeouts(int* count);
 int olfgpu_gnn_gemm(int M, int K1, int K2, int N, const void* A1, const void* A2, const void* W, const float* bias,
                     int relu, const void* residual, void* outBf16, float* outF32, int ldo, void* saveZ, void* stream);
 int olfgpu_gnn_gemm_dw(int M, int K1, int K2, int N, const void* A1, const void* A2, const void* dZ, float* dW,

@@ -1,7 +1,7 @@
 // Kernels of the learned warm start: a message-passing graph network over the bus graph, BF16 weights and
-// activations with FP32 accumulation.  Tensor-core GEMMs (mma.sync m16n8k16 BF16 -> FP32) for the dense layers and
-// their weight gradients; CUDA-core gather kernels for the messages.  Every reduction runs in a fixed order, so
-// forward and backward are deterministic.
+// activations with FP32 accumulation.  The dense layers' GEMMs run on the fifth-generation tensor cores (tcgen05.mma,
+// accumulators in tensor memory; gemmTcKernel); their weight gradients on mma.sync m16n8k16 tiles; CUDA-core gather
+// kernels for the messages.  Every reduction runs in a fixed order, so forward and backward are deterministic.
 //
 // Shapes: M rows = samples x buses; feature widths K, N are multiples of 16 / 8 (<= 128).
 #include <cuda_bf16.h>
@@ -31,61 +31,142 @@ __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
+// ---------------------------------------------------------------------------------------------------------------
 // Y[M x N] = [A1 | A2][M x (K1 + K2)] . W[(K1 + K2) x N] (+ bias), z = relu ? max(Y, 0) : Y, saved to saveZ when given;
-// out = z (+ residual) to outB (bf16) and / or outF (fp32).  4 warps per CTA, each warp 16 rows x N columns; W staged
-// transposed in shared memory.  Rows are walked grid-stride in 64-row chunks.
-template <int K1, int K2, int N>
-__global__ void __launch_bounds__(128) gemmKernel(int M, const __nv_bfloat16* __restrict__ A1,
-                                                  const __nv_bfloat16* __restrict__ A2,
-                                                  const __nv_bfloat16* __restrict__ W, const float* __restrict__ bias,
-                                                  int relu, const __nv_bfloat16* __restrict__ residual,
-                                                  __nv_bfloat16* outB, float* outF, int ldo,
-                                                  __nv_bfloat16* saveZ) {
-    constexpr int K = K1 + K2;
-    constexpr int KP = K + 8;   // padded row of the transposed weights (bank spread)
-    constexpr int NT = N / 8;
-    __shared__ __align__(16) __nv_bfloat16 wt[N * KP];
-    for (int i = threadIdx.x; i < K * N; i += blockDim.x) {
-        const int k = i / N, n = i % N;
-        wt[n * KP + k] = W[i];
+// out = z (+ residual) to outB (bf16) and / or outF (fp32), on the fifth-generation tensor cores.
+// One CTA of 4 warps per 128-row tile (grid-stride): the
+// tile of [A1 | A2] and W^T sit in shared memory in the K-major canonical layout without swizzle (8-row x 16-byte core
+// matrices; between the two 8-column halves of a 16-wide K step LBO bytes, between 8-row groups SBO = 128 bytes); one
+// thread issues the K / 16 MMAs (M = 128, N, K = 16, BF16 x BF16 -> FP32) into a tensor-memory accumulator of 128
+// lanes x N columns and commits them to an mbarrier; every warp then reads its 32 lanes (rows) with tcgen05.ld and
+// runs the epilogue of gemmKernel.  The mbarrier wait is bounded: on timeout the CTA records it (gTcTimeouts), frees
+// its tensor memory and leaves.  The dynamic shared memory is padded to 56 KB so at most four CTAs share an SM and
+// their tensor-memory allocations (<= 128 of 512 columns each) never wait on one another.
+// ---------------------------------------------------------------------------------------------------------------
+__device__ int gTcTimeouts = 0;
+
+constexpr int TC_SMEM_BYTES = 56 * 1024;
+
+__device__ __forceinline__ uint32_t smemU32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// Shared-memory matrix descriptor (K-major, no swizzle): start >> 4 at [0,14), LBO >> 4 at [16,30), SBO >> 4 at
+// [32,46), descriptor version 1 at [46,48), base offset 0, layout type 0 (no swizzle) at [61,64).
+__device__ __forceinline__ uint64_t ummaDesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), BF16 A and B (bits 7-9, 10-12 = 1), both
+// K-major, N >> 3 at bit 17, M >> 4 at bit 24 (M = 128).
+template <int N>
+constexpr uint32_t ummaInstrDesc() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbarWait(uint32_t mbar, uint32_t parity) {
+    for (int i = 0; i < (1 << 22); i++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(mbar), "r"(parity)
+                     : "memory");
+        if (done) return true;
     }
+    return false;
+}
+
+template <int K1, int K2, int N>
+__global__ void __launch_bounds__(128) gemmTcKernel(int M, const __nv_bfloat16* __restrict__ A1,
+                                                    const __nv_bfloat16* __restrict__ A2,
+                                                    const __nv_bfloat16* __restrict__ W, const float* __restrict__ bias,
+                                                    int relu, const __nv_bfloat16* __restrict__ residual,
+                                                    __nv_bfloat16* outB, float* outF, int ldo,
+                                                    __nv_bfloat16* saveZ) {
+    constexpr int K = K1 + K2;
+    constexpr int KC = K / 8;                           // 16-byte chunks of a row
+    constexpr int TMEM_COLS = N < 32 ? 32 : N;          // a power of two >= 32
+    static_assert(K % 16 == 0 && N % 16 == 0 && N <= 256, "tcgen05 tile: K multiple of 16, N multiple of 16");
+    static_assert((TMEM_COLS & (TMEM_COLS - 1)) == 0, "tensor-memory allocation: a power of two columns");
+    static_assert((128 * K + N * K) * 2 + 16 <= TC_SMEM_BYTES, "tile does not fit the shared memory");
+    extern __shared__ __align__(1024) unsigned char tcSmem[];
+    unsigned char* sA = tcSmem;                         // 128 x K, core matrix (row / 8, chunk) at (chunk * 16 + row / 8) * 128
+    unsigned char* sB = sA + 128 * K * 2;               // W^T, N x K, core matrix (n / 8, chunk) at (chunk * N / 8 + n / 8) * 128
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sB + N * K * 2);
+    uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(mbar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < K * N; i += 128) {
+        const int k = i / N, n = i % N;
+        *reinterpret_cast<__nv_bfloat16*>(sB + ((k >> 3) * (N / 8) + (n >> 3)) * 128 + (n & 7) * 16 + (k & 7) * 2) = W[i];
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemU32(mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemU32(tmemSlot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = lane >> 2, t = lane & 3;
-    for (int base = (blockIdx.x * 4 + warp) * 16; base < M; base += gridDim.x * 64) {
-        float acc[NT][4];
-#pragma unroll
-        for (int j = 0; j < NT; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
-        const int r0 = base + g, r1 = base + g + 8;
-#pragma unroll
-        for (int ks = 0; ks < K / 16; ks++) {
-            const int kb = ks * 16;
-            const __nv_bfloat16* src = kb < K1 ? A1 : A2;
-            const int ld = kb < K1 ? K1 : K2;
-            const int kc = kb < K1 ? kb : kb - K1;
-            uint32_t a[4];
-            const uint32_t z = 0u;
-            a[0] = r0 < M ? *reinterpret_cast<const uint32_t*>(src + (size_t)r0 * ld + kc + 2 * t) : z;
-            a[1] = r1 < M ? *reinterpret_cast<const uint32_t*>(src + (size_t)r1 * ld + kc + 2 * t) : z;
-            a[2] = r0 < M ? *reinterpret_cast<const uint32_t*>(src + (size_t)r0 * ld + kc + 2 * t + 8) : z;
-            a[3] = r1 < M ? *reinterpret_cast<const uint32_t*>(src + (size_t)r1 * ld + kc + 2 * t + 8) : z;
-#pragma unroll
-            for (int j = 0; j < NT; j++) {
-                const __nv_bfloat16* wrow = wt + (j * 8 + g) * KP + kb;
-                uint32_t bfrag[2];
-                bfrag[0] = *reinterpret_cast<const uint32_t*>(wrow + 2 * t);
-                bfrag[1] = *reinterpret_cast<const uint32_t*>(wrow + 2 * t + 8);
-                mma16816(acc[j], a, bfrag);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmemSlot;
+    uint32_t parity = 0;
+    for (int tile = blockIdx.x; tile * 128 < M; tile += gridDim.x) {
+        const int base = tile * 128;
+        for (int i = tid; i < 128 * KC; i += 128) {
+            const int r = i / KC, c = i % KC, k = c * 8;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (base + r < M) {
+                v = k < K1 ? *reinterpret_cast<const uint4*>(A1 + (size_t)(base + r) * K1 + k)
+                           : *reinterpret_cast<const uint4*>(A2 + (size_t)(base + r) * K2 + (k - K1));
             }
+            *reinterpret_cast<uint4*>(sA + (c * 16 + (r >> 3)) * 128 + (r & 7) * 16) = v;
         }
+        // the tile's generic-proxy stores become visible to the tensor cores' reads
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smemU32(sA), b0 = smemU32(sB);
 #pragma unroll
-        for (int j = 0; j < NT; j++) {
-            const int c = j * 8 + 2 * t;
+            for (int ks = 0; ks < K / 16; ks++) {
+                const uint64_t da = ummaDesc(a0 + 2 * ks * 16 * 128, 16 * 128, 128);
+                const uint64_t db = ummaDesc(b0 + 2 * ks * (N / 8) * 128, (N / 8) * 128, 128);
+                asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                             "l"(da), "l"(db), "r"(ummaInstrDesc<N>()), "r"(ks > 0 ? 1u : 0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smemU32(mbar))
+                         : "memory");
+        }
+        __syncwarp();
+        const bool done = mbarWait(smemU32(mbar), parity);
+        if (__syncthreads_or(!done)) {   // the whole CTA leaves together
+            if (tid == 0) atomicAdd(&gTcTimeouts, 1);
+            break;
+        }
+        parity ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int r = base + warp * 32 + lane;
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int r = h == 0 ? r0 : r1;
-                if (r >= M) continue;
-                float v0 = acc[j][2 * h], v1 = acc[j][2 * h + 1];
+        for (int cb = 0; cb < N / 16; cb++) {
+            uint32_t v[16];
+            const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 16);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                         "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                           "=r"(v[14]), "=r"(v[15])
+                         : "r"(addr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (r >= M) continue;
+#pragma unroll
+            for (int j = 0; j < 16; j += 2) {
+                const int c = cb * 16 + j;
+                float v0 = __uint_as_float(v[j]), v1 = __uint_as_float(v[j + 1]);
                 if (bias) {
                     v0 += bias[c];
                     v1 += bias[c + 1];
@@ -94,7 +175,6 @@ __global__ void __launch_bounds__(128) gemmKernel(int M, const __nv_bfloat16* __
                     v0 = fmaxf(v0, 0.f);
                     v1 = fmaxf(v1, 0.f);
                 }
-                // column pairs (c, c + 1): one 4-byte bf16x2 / 8-byte float2 access each
                 if (saveZ) *reinterpret_cast<__nv_bfloat162*>(saveZ + (size_t)r * N + c) = __floats2bfloat162_rn(v0, v1);
                 if (residual) {
                     const float2 rv =
@@ -106,7 +186,26 @@ __global__ void __launch_bounds__(128) gemmKernel(int M, const __nv_bfloat16* __
                 if (outF) *reinterpret_cast<float2*>(outF + (size_t)r * ldo + c) = make_float2(v0, v1);
             }
         }
+        // every warp's tensor-memory reads are done before the next tile's MMAs overwrite the accumulator
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
     }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+}
+
+template <int K1, int K2, int N>
+void launchGemmTc(int M, const __nv_bfloat16* a1, const __nv_bfloat16* a2, const __nv_bfloat16* w, const float* bias,
+                  int relu, const __nv_bfloat16* res, __nv_bfloat16* ob, float* of, int ldo, __nv_bfloat16* sz,
+                  cudaStream_t st) {
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(gemmTcKernel<K1, K2, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES);
+    if (attr != cudaSuccess) throw std::runtime_error(std::string("tcgen05 GEMM set-up: ") + cudaGetErrorString(attr));
+    if (M <= 0) return;
+    const long long tiles = (M + 127) / 128;
+    const int grid = (int)(tiles < 148 * 4 ? tiles : 148 * 4);
+    gemmTcKernel<K1, K2, N><<<grid, 128, TC_SMEM_BYTES, st>>>(M, a1, a2, w, bias, relu, res, ob, of, ldo, sz);
 }
 
 // Partial weight gradients: chunk c of the rows contributes P_c[K x N] = [A1|A2]_c^T dZ_c and colsum(dZ_c); one CTA
@@ -408,10 +507,6 @@ __global__ void copyColsKernel(long long count, int ncols, const float* src, int
     *d = accumulate ? *d + v : v;
 }
 
-int gridFor(long long rows, int per) {
-    long long blocks = (rows + per - 1) / per;
-    return (int)(blocks < 148 * 16 ? (blocks < 1 ? 1 : blocks) : 148 * 16);
-}
 
 }  // namespace
 
@@ -505,11 +600,18 @@ __global__ void composeStartKernel(int nS, int nb, const float* pred, int ldp, l
 
 extern "C" const char* olfgpu_gnn_last_error(void) { return gnnError.c_str(); }
 
+extern "C" int olfgpu_gnn_tc_timeouts(int* count) {
+    return gnnGuard([&] {
+        if (!count) throw std::runtime_error("null output");
+        const cudaError_t e = cudaMemcpyFromSymbol(count, gTcTimeouts, sizeof(int));
+        if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+    });
+}
+
 extern "C" int olfgpu_gnn_gemm(int M, int K1, int K2, int N, const void* A1, const void* A2, const void* W,
                                const float* bias, int relu, const void* residual, void* outBf16, float* outF32,
                                int ldo, void* saveZ, void* stream) {
     return gnnGuard([&] {
-        const int grid = gridFor(M, 64);
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         auto a1 = static_cast<const __nv_bfloat16*>(A1);
         auto a2 = static_cast<const __nv_bfloat16*>(A2);
@@ -517,7 +619,7 @@ extern "C" int olfgpu_gnn_gemm(int M, int K1, int K2, int N, const void* A1, con
         auto res = static_cast<const __nv_bfloat16*>(residual);
         auto ob = static_cast<__nv_bfloat16*>(outBf16);
         auto sz = static_cast<__nv_bfloat16*>(saveZ);
-#define OLF_GEMM(a, b2, c) gemmKernel<a, b2, c><<<grid, 128, 0, st>>>(M, a1, a2, w, bias, relu, res, ob, outF32, ldo, sz)
+#define OLF_GEMM(a, b2, c) launchGemmTc<a, b2, c>(M, a1, a2, w, bias, relu, res, ob, outF32, ldo, sz, st)
         if (K1 == 16 && K2 == 0 && N == 64) OLF_GEMM(16, 0, 64);
         else if (K1 == 64 && K2 == 0 && N == 128) OLF_GEMM(64, 0, 128);
         else if (K1 == 64 && K2 == 64 && N == 64) OLF_GEMM(64, 64, 64);

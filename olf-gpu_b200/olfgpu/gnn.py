@@ -37,6 +37,7 @@ def _lib():
         L.olfgpu_gnn_last_error.restype = ctypes.c_char_p
         sig = {
             "olfgpu_gnn_gemm": [i, i, i, i, vp, vp, vp, vp, i, vp, vp, vp, i, vp, vp],
+            "olfgpu_gnn_tc_timeouts": [vp],
             "olfgpu_gnn_gemm_dw": [i, i, i, i, vp, vp, vp, vp, vp, vp, i, vp],
             "olfgpu_gnn_message_forward": [i, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp],
             "olfgpu_gnn_message_backward": [i, i, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp],
@@ -69,6 +70,27 @@ def _call(name, *args):
 
 def _ptr(t):
     return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def tc_timeouts() -> int:
+    """Tensor-core GEMM tiles that gave up waiting for their MMAs since the library was loaded (0 on a working GPU)."""
+    v = ctypes.c_int(0)
+    _call("olfgpu_gnn_tc_timeouts", ctypes.byref(v))
+    return v.value
+
+
+def gemm(a1, a2, w, bias=None, relu=False, residual=None, out_f32=False, save_z=False):
+    """Y = [a1 | a2] . w (+ bias), z = relu(Y) or Y, out = z (+ residual), on the tensor cores; BF16 CUDA tensors in.
+    Returns (out, z or None): out BF16 [M, N] (FP32 with out_f32)."""
+    import torch
+    M, K1 = a1.shape
+    K2 = 0 if a2 is None else a2.shape[1]
+    N = w.shape[1]
+    out = torch.empty((M, N), dtype=torch.float32 if out_f32 else torch.bfloat16, device=a1.device)
+    z = torch.empty((M, N), dtype=torch.bfloat16, device=a1.device) if save_z else None
+    _call("olfgpu_gnn_gemm", M, K1, K2, N, _ptr(a1), _ptr(a2), _ptr(w), _ptr(bias), 1 if relu else 0, _ptr(residual),
+          None if out_f32 else _ptr(out), _ptr(out) if out_f32 else None, N, _ptr(z), _stream())
+    return out, z
 
 
 def _stream():

@@ -16,12 +16,14 @@ def _bf16_round(a):
     return torch.from_numpy(np.asarray(a, np.float32)).to(torch.bfloat16).to(torch.float64).numpy()
 
 
+@pytest.mark.parametrize("M", [1000, 128 * 700 + 37])
 @pytest.mark.parametrize("k1,k2,n", [(16, 0, 64), (64, 0, 128), (64, 64, 64), (64, 0, 16), (128, 0, 64)])
-def test_gemm_matches_float64(engine_lib, k1, k2, n):
+def test_gemm_matches_float64(engine_lib, k1, k2, n, M):
+    """The tensor-core GEMM (tcgen05, 128-row tiles; the larger M walks more tiles than CTAs) with bias, ReLU,
+    residual, the saved pre-residual z and FP32 output; none of its waits gave up."""
     import torch
     from olfgpu import gnn
     rng = np.random.default_rng(k1 + k2 + n)
-    M = 1000
     a1 = rng.standard_normal((M, k1)).astype(np.float32)
     a2 = rng.standard_normal((M, k2)).astype(np.float32) if k2 else None
     w = (rng.standard_normal((k1 + k2, n)) / 8).astype(np.float32)
@@ -40,6 +42,12 @@ def test_gemm_matches_float64(engine_lib, k1, k2, n):
     ref = ref_z + _bf16_round(res)
     assert np.max(np.abs(out.cpu().numpy() - ref)) / np.max(np.abs(ref)) < 1e-5
     assert np.max(np.abs(z.float().cpu().numpy() - ref_z)) / np.max(np.abs(ref_z)) < 1e-2
+    # the BF16 output without bias, ReLU or residual
+    ob, _ = gnn.gemm(A1, A2, W)
+    torch.cuda.synchronize()
+    ref_y = aa @ _bf16_round(w)
+    assert np.max(np.abs(ob.float().cpu().numpy() - ref_y)) / np.max(np.abs(ref_y)) < 1e-2
+    assert gnn.tc_timeouts() == 0
 
 
 @pytest.mark.parametrize("k1,k2,n", [(16, 0, 64), (64, 0, 128), (64, 64, 64), (64, 0, 16)])
