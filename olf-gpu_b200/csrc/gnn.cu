@@ -7,6 +7,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -34,18 +35,39 @@ __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], 
 // ---------------------------------------------------------------------------------------------------------------
 // Y[M x N] = [A1 | A2][M x (K1 + K2)] . W[(K1 + K2) x N] (+ bias), z = relu ? max(Y, 0) : Y, saved to saveZ when given;
 // out = z (+ residual) to outB (bf16) and / or outF (fp32), on the fifth-generation tensor cores.
-// One CTA of 4 warps per 128-row tile (grid-stride): the
-// tile of [A1 | A2] and W^T sit in shared memory in the K-major canonical layout without swizzle (8-row x 16-byte core
-// matrices; between the two 8-column halves of a 16-wide K step LBO bytes, between 8-row groups SBO = 128 bytes); one
-// thread issues the K / 16 MMAs (M = 128, N, K = 16, BF16 x BF16 -> FP32) into a tensor-memory accumulator of 128
-// lanes x N columns and commits them to an mbarrier; every warp then reads its 32 lanes (rows) with tcgen05.ld and
-// runs the epilogue of gemmKernel.  The mbarrier wait is bounded: on timeout the CTA records it (gTcTimeouts), frees
-// its tensor memory and leaves.  The dynamic shared memory is padded to 56 KB so at most four CTAs share an SM and
-// their tensor-memory allocations (<= 128 of 512 columns each) never wait on one another.
+// A persistent CTA of 4 warps walks 128-row tiles (grid-stride).  W^T and the bias stay in shared memory; the tiles of
+// [A1 | A2] stream through two shared-memory buffers with cp.async (16-byte copies, rows past M zero-filled), the next
+// tile's copies in flight while the current tile multiplies and runs its epilogue.  Both operands use the K-major
+// canonical layout without swizzle (8-row x 16-byte core matrices; between the two 8-column halves of a 16-wide K step
+// LBO bytes, between 8-row groups SBO = 128 bytes); eight consecutive threads copy the eight rows of one core matrix,
+// so their shared-memory writes fill one 128-byte line.  One thread issues the K / 16 MMAs (M = 128, N, K = 16,
+// BF16 x BF16 -> FP32) into a tensor-memory accumulator of 128 lanes x N columns and commits them to an mbarrier;
+// every warp then reads its 32 lanes (rows) with tcgen05.ld and writes 16 columns per 16-byte store.  The mbarrier
+// wait is bounded: on timeout the CTA records it (gTcTimeouts), drains its copies, frees its tensor memory and leaves.
+// The launch pads the dynamic shared memory so that no more CTAs share an SM than its 512 tensor-memory columns hold
+// (N columns each): their allocations never wait on one another.
 // ---------------------------------------------------------------------------------------------------------------
 __device__ int gTcTimeouts = 0;
 
-constexpr int TC_SMEM_BYTES = 56 * 1024;
+// Shared memory of one CTA: two A buffers (128 x K), W^T (N x K), the bias (N floats), the mbarrier and the
+// tensor-memory address.
+constexpr int tcSmemBytes(int K, int N) { return 2 * 128 * K * 2 + N * K * 2 + N * 4 + 16; }
+// The dynamic shared memory a launch asks for: at least the tile's, and enough that at most 512 / columns CTAs fit
+// on one SM (228 KB of shared memory, 1 KB reserved per CTA).
+constexpr int tcLaunchSmem(int K, int N) {
+    return tcSmemBytes(K, N) > 233472 / (512 / (N < 32 ? 32 : N) + 1) ? tcSmemBytes(K, N)
+                                                                       : 233472 / (512 / (N < 32 ? 32 : N) + 1);
+}
+
+__device__ __forceinline__ void cpAsync16(uint32_t dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+
+__device__ __forceinline__ uint32_t packBf2(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
 
 __device__ __forceinline__ uint32_t smemU32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
@@ -85,20 +107,42 @@ __global__ void __launch_bounds__(128) gemmTcKernel(int M, const __nv_bfloat16* 
                                                     __nv_bfloat16* saveZ) {
     constexpr int K = K1 + K2;
     constexpr int KC = K / 8;                           // 16-byte chunks of a row
+    constexpr int CL = KC < 4 ? KC : 4;                 // chunks of one row that a warp copies together
+    constexpr int CH = KC / CL;
     constexpr int TMEM_COLS = N < 32 ? 32 : N;          // a power of two >= 32
-    static_assert(K % 16 == 0 && N % 16 == 0 && N <= 256, "tcgen05 tile: K multiple of 16, N multiple of 16");
+    static_assert(K % 16 == 0 && K1 % 8 == 0 && N % 16 == 0 && N <= 256, "tcgen05 tile: K multiple of 16, N of 16");
     static_assert((TMEM_COLS & (TMEM_COLS - 1)) == 0, "tensor-memory allocation: a power of two columns");
-    static_assert((128 * K + N * K) * 2 + 16 <= TC_SMEM_BYTES, "tile does not fit the shared memory");
+    static_assert(tcSmemBytes(K, N) <= 227 * 1024, "tile does not fit the shared memory");
     extern __shared__ __align__(1024) unsigned char tcSmem[];
-    unsigned char* sA = tcSmem;                         // 128 x K, core matrix (row / 8, chunk) at (chunk * 16 + row / 8) * 128
-    unsigned char* sB = sA + 128 * K * 2;               // W^T, N x K, core matrix (n / 8, chunk) at (chunk * N / 8 + n / 8) * 128
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(sB + N * K * 2);
+    // A buffer b: 128 x K, core matrix (row / 8, chunk) at (chunk * 16 + row / 8) * 128
+    unsigned char* sB = tcSmem + 2 * 128 * K * 2;       // W^T, N x K, core matrix (n / 8, chunk) at (chunk * N / 8 + n / 8) * 128
+    float* sBias = reinterpret_cast<float*>(sB + N * K * 2);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sBias + N);
     uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(mbar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles = (M + 127) / 128;
+    const uint32_t sA0 = smemU32(tcSmem);
+    auto copyTile = [&](int tile, int buf) {
+        const int base = tile * 128;
+        const uint32_t dst0 = sA0 + (uint32_t)(buf * 128 * K * 2);
+#pragma unroll
+        for (int it = 0; it < KC; it++) {
+            const int i = it * 128 + tid;
+            const int rest = (i >> 3) / CL;
+            const int c = (rest % CH) * CL + (i >> 3) % CL, r = (rest / CH) * 8 + (i & 7);
+            const bool valid = base + r < M;
+            const size_t row = valid ? (size_t)(base + r) : 0;
+            const __nv_bfloat16* src = c * 8 < K1 ? A1 + row * K1 + c * 8 : A2 + row * K2 + (c * 8 - K1);
+            cpAsync16(dst0 + (uint32_t)((c * 16 + (r >> 3)) * 128 + (r & 7) * 16), src, valid);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (blockIdx.x < tiles) copyTile(blockIdx.x, 0);
     for (int i = tid; i < K * N; i += 128) {
         const int k = i / N, n = i % N;
         *reinterpret_cast<__nv_bfloat16*>(sB + ((k >> 3) * (N / 8) + (n >> 3)) * 128 + (n & 7) * 16 + (k & 7) * 2) = W[i];
     }
+    for (int i = tid; i < N; i += 128) sBias[i] = bias ? bias[i] : 0.f;
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemU32(mbar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -113,23 +157,21 @@ __global__ void __launch_bounds__(128) gemmTcKernel(int M, const __nv_bfloat16* 
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmemSlot;
     uint32_t parity = 0;
-    for (int tile = blockIdx.x; tile * 128 < M; tile += gridDim.x) {
-        const int base = tile * 128;
-        for (int i = tid; i < 128 * KC; i += 128) {
-            const int r = i / KC, c = i % KC, k = c * 8;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (base + r < M) {
-                v = k < K1 ? *reinterpret_cast<const uint4*>(A1 + (size_t)(base + r) * K1 + k)
-                           : *reinterpret_cast<const uint4*>(A2 + (size_t)(base + r) * K2 + (k - K1));
-            }
-            *reinterpret_cast<uint4*>(sA + (c * 16 + (r >> 3)) * 128 + (r & 7) * 16) = v;
+    int buf = 0;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, buf ^= 1) {
+        // the other buffer was read by the previous tile's MMAs, which have completed
+        if (tile + (int)gridDim.x < tiles) {
+            copyTile(tile + gridDim.x, buf ^ 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
-        // the tile's generic-proxy stores become visible to the tensor cores' reads
+        // the tile's copies become visible to the tensor cores' reads
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t a0 = smemU32(sA), b0 = smemU32(sB);
+            const uint32_t a0 = sA0 + (uint32_t)(buf * 128 * K * 2), b0 = smemU32(sB);
 #pragma unroll
             for (int ks = 0; ks < K / 16; ks++) {
                 const uint64_t da = ummaDesc(a0 + 2 * ks * 16 * 128, 16 * 128, 128);
@@ -144,13 +186,14 @@ __global__ void __launch_bounds__(128) gemmTcKernel(int M, const __nv_bfloat16* 
         }
         __syncwarp();
         const bool done = mbarWait(smemU32(mbar), parity);
-        if (__syncthreads_or(!done)) {   // the whole CTA leaves together
+        if (__syncthreads_or(!done)) {   // the whole CTA leaves together, its copies drained
             if (tid == 0) atomicAdd(&gTcTimeouts, 1);
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
             break;
         }
         parity ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const int r = base + warp * 32 + lane;
+        const int r = tile * 128 + warp * 32 + lane;
 #pragma unroll
         for (int cb = 0; cb < N / 16; cb++) {
             uint32_t v[16];
@@ -163,27 +206,44 @@ __global__ void __launch_bounds__(128) gemmTcKernel(int M, const __nv_bfloat16* 
                          : "r"(addr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (r >= M) continue;
+            float f[16];
 #pragma unroll
-            for (int j = 0; j < 16; j += 2) {
-                const int c = cb * 16 + j;
-                float v0 = __uint_as_float(v[j]), v1 = __uint_as_float(v[j + 1]);
-                if (bias) {
-                    v0 += bias[c];
-                    v1 += bias[c + 1];
+            for (int j = 0; j < 16; j++) {
+                f[j] = __uint_as_float(v[j]) + sBias[cb * 16 + j];
+                if (relu) f[j] = fmaxf(f[j], 0.f);
+            }
+            const size_t rowN = (size_t)r * N + cb * 16;
+            if (saveZ) {
+                uint4* z = reinterpret_cast<uint4*>(saveZ + rowN);
+                z[0] = make_uint4(packBf2(f[0], f[1]), packBf2(f[2], f[3]), packBf2(f[4], f[5]), packBf2(f[6], f[7]));
+                z[1] = make_uint4(packBf2(f[8], f[9]), packBf2(f[10], f[11]), packBf2(f[12], f[13]),
+                                  packBf2(f[14], f[15]));
+            }
+            if (residual) {
+                const uint4* rp = reinterpret_cast<const uint4*>(residual + rowN);
+                const uint4 q[2] = {rp[0], rp[1]};
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const uint32_t w4[4] = {q[h].x, q[h].y, q[h].z, q[h].w};
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const float2 rv = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w4[j]));
+                        f[h * 8 + 2 * j] += rv.x;
+                        f[h * 8 + 2 * j + 1] += rv.y;
+                    }
                 }
-                if (relu) {
-                    v0 = fmaxf(v0, 0.f);
-                    v1 = fmaxf(v1, 0.f);
-                }
-                if (saveZ) *reinterpret_cast<__nv_bfloat162*>(saveZ + (size_t)r * N + c) = __floats2bfloat162_rn(v0, v1);
-                if (residual) {
-                    const float2 rv =
-                        __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(residual + (size_t)r * N + c));
-                    v0 += rv.x;
-                    v1 += rv.y;
-                }
-                if (outB) *reinterpret_cast<__nv_bfloat162*>(outB + (size_t)r * ldo + c) = __floats2bfloat162_rn(v0, v1);
-                if (outF) *reinterpret_cast<float2*>(outF + (size_t)r * ldo + c) = make_float2(v0, v1);
+            }
+            const size_t rowO = (size_t)r * ldo + cb * 16;
+            if (outB) {
+                uint4* o = reinterpret_cast<uint4*>(outB + rowO);
+                o[0] = make_uint4(packBf2(f[0], f[1]), packBf2(f[2], f[3]), packBf2(f[4], f[5]), packBf2(f[6], f[7]));
+                o[1] = make_uint4(packBf2(f[8], f[9]), packBf2(f[10], f[11]), packBf2(f[12], f[13]),
+                                  packBf2(f[14], f[15]));
+            }
+            if (outF) {
+                float4* o = reinterpret_cast<float4*>(outF + rowO);
+#pragma unroll
+                for (int j = 0; j < 4; j++) o[j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
             }
         }
         // every warp's tensor-memory reads are done before the next tile's MMAs overwrite the accumulator
@@ -199,17 +259,43 @@ template <int K1, int K2, int N>
 void launchGemmTc(int M, const __nv_bfloat16* a1, const __nv_bfloat16* a2, const __nv_bfloat16* w, const float* bias,
                   int relu, const __nv_bfloat16* res, __nv_bfloat16* ob, float* of, int ldo, __nv_bfloat16* sz,
                   cudaStream_t st) {
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(gemmTcKernel<K1, K2, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES);
-    if (attr != cudaSuccess) throw std::runtime_error(std::string("tcgen05 GEMM set-up: ") + cudaGetErrorString(attr));
+    constexpr int smem = tcLaunchSmem(K1 + K2, N);
+    // CTAs resident on the device: per SM the fewest that the shared memory (228 KB, 1 KB reserved per CTA), the
+    // tensor memory (512 columns), the registers (64 K, 8-register granules) and the threads (2048) allow
+    static const int resident = [] {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaFuncSetAttribute(gemmTcKernel<K1, K2, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(gemmTcKernel<K1, K2, N>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+            return -1;
+        cudaFuncAttributes fa{};
+        if (cudaFuncGetAttributes(&fa, gemmTcKernel<K1, K2, N>) != cudaSuccess) return -1;
+        const int regs = (fa.numRegs + 7) / 8 * 8;
+        int perSm = 2048 / 128;
+        perSm = std::min(perSm, 233472 / (smem + 1024));
+        perSm = std::min(perSm, 512 / (N < 32 ? 32 : N));
+        perSm = std::min(perSm, 65536 / (regs * 128));
+        return sms * std::max(perSm, 1);
+    }();
+    if (resident < 0) throw std::runtime_error("tcgen05 GEMM set-up: shared-memory attribute refused");
     if (M <= 0) return;
+    // 16-byte copies and stores: row pointers and the output stride must keep 16-byte alignment
+    auto misaligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) != 0; };
+    if (misaligned(a1) || (K2 > 0 && misaligned(a2)) || misaligned(res) || misaligned(ob) || misaligned(of) ||
+        misaligned(sz) || (ob && ldo % 8 != 0) || (of && ldo % 4 != 0) || ldo < N)
+        throw std::runtime_error("GEMM operands must be 16-byte aligned, ldo >= N and ldo * element size a multiple of 16");
     const long long tiles = (M + 127) / 128;
-    const int grid = (int)(tiles < 148 * 4 ? tiles : 148 * 4);
-    gemmTcKernel<K1, K2, N><<<grid, 128, TC_SMEM_BYTES, st>>>(M, a1, a2, w, bias, relu, res, ob, of, ldo, sz);
+    const int grid = (int)(tiles < resident ? tiles : resident);
+    gemmTcKernel<K1, K2, N><<<grid, 128, smem, st>>>(M, a1, a2, w, bias, relu, res, ob, of, ldo, sz);
 }
 
 // Partial weight gradients: chunk c of the rows contributes P_c[K x N] = [A1|A2]_c^T dZ_c and colsum(dZ_c); one CTA
-// per chunk, 16-row slices staged in shared memory, tensor-core tiles (m over K, n over N, k over rows).
+// per chunk.  32-row slices stream through two shared-memory buffers with cp.async (16-byte copies, rows past the
+// chunk zero-filled), the next slice in flight while the tensor-core tiles (m over K, n over N, k over rows) consume
+// the current one.
 template <int K1, int K2, int N>
 __global__ void __launch_bounds__(128) gemmDwKernel(int M, int rowsPerChunk, const __nv_bfloat16* __restrict__ A1,
                                                     const __nv_bfloat16* __restrict__ A2,
@@ -217,45 +303,65 @@ __global__ void __launch_bounds__(128) gemmDwKernel(int M, int rowsPerChunk, con
     constexpr int K = K1 + K2;
     constexpr int MT = K / 16, NT = N / 8, TILES = MT * NT;
     constexpr int PER_WARP = (TILES + 3) / 4;
-    __shared__ __align__(16) __nv_bfloat16 as[16][K + 8];
-    __shared__ __align__(16) __nv_bfloat16 ds[16][N + 8];
+    constexpr int SR = 32;                              // rows per slice
+    __shared__ __align__(16) __nv_bfloat16 as[2][SR][K + 8];
+    __shared__ __align__(16) __nv_bfloat16 ds[2][SR][N + 8];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     const int row0 = blockIdx.x * rowsPerChunk;
     const int row1 = min(M, row0 + rowsPerChunk);
+    auto stage = [&](int base, int buf) {
+        for (int i = threadIdx.x; i < SR * (K / 8); i += 128) {
+            const int r = i / (K / 8), c = i % (K / 8), row = base + r;
+            const bool valid = row < row1;
+            const size_t rr = valid ? (size_t)row : (size_t)row0;
+            const __nv_bfloat16* src = c * 8 < K1 ? A1 + rr * K1 + c * 8 : A2 + rr * K2 + (c * 8 - K1);
+            cpAsync16(smemU32(&as[buf][r][c * 8]), src, valid);
+        }
+        for (int i = threadIdx.x; i < SR * (N / 8); i += 128) {
+            const int r = i / (N / 8), c = i % (N / 8), row = base + r;
+            const bool valid = row < row1;
+            cpAsync16(smemU32(&ds[buf][r][c * 8]), dZ + (valid ? (size_t)row : (size_t)row0) * N + c * 8, valid);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
     float acc[PER_WARP][4];
 #pragma unroll
     for (int i = 0; i < PER_WARP; i++) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
     float colsum = 0.f;   // thread tid < N sums column tid of dZ
-    for (int base = row0; base < row1; base += 16) {
-        for (int i = threadIdx.x; i < 16 * K; i += blockDim.x) {
-            const int r = i / K, k = i % K, row = base + r;
-            __nv_bfloat16 v = __float2bfloat16(0.f);
-            if (row < row1) v = k < K1 ? A1[(size_t)row * K1 + k] : A2[(size_t)row * K2 + (k - K1)];
-            as[r][k] = v;
-        }
-        for (int i = threadIdx.x; i < 16 * N; i += blockDim.x) {
-            const int r = i / N, n = i % N, row = base + r;
-            ds[r][n] = row < row1 ? dZ[(size_t)row * N + n] : __float2bfloat16(0.f);
+    if (row0 < row1) stage(row0, 0);
+    int buf = 0;
+    for (int base = row0; base < row1; base += SR, buf ^= 1) {
+        // the other buffer was consumed in the previous slice, before its closing barrier
+        if (base + SR < row1) {
+            stage(base + SR, buf ^ 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
         __syncthreads();
         if (threadIdx.x < N) {
-            for (int r = 0; r < 16; r++) colsum += __bfloat162float(ds[r][threadIdx.x]);
+            for (int r = 0; r < SR; r++) colsum += __bfloat162float(ds[buf][r][threadIdx.x]);
         }
 #pragma unroll
-        for (int i = 0; i < PER_WARP; i++) {
-            const int tile = warp * PER_WARP + i;
-            if (tile >= TILES) break;
-            const int m0 = (tile / NT) * 16, n0 = (tile % NT) * 8;
-            uint32_t a[4], b[2];
-            // A_mma(m, kk) = as[kk][m0 + m]; B_mma(kk, n) = ds[kk][n0 + n]
-            a[0] = pack2(as[2 * t][m0 + g], as[2 * t + 1][m0 + g]);
-            a[1] = pack2(as[2 * t][m0 + g + 8], as[2 * t + 1][m0 + g + 8]);
-            a[2] = pack2(as[2 * t + 8][m0 + g], as[2 * t + 9][m0 + g]);
-            a[3] = pack2(as[2 * t + 8][m0 + g + 8], as[2 * t + 9][m0 + g + 8]);
-            b[0] = pack2(ds[2 * t][n0 + g], ds[2 * t + 1][n0 + g]);
-            b[1] = pack2(ds[2 * t + 8][n0 + g], ds[2 * t + 9][n0 + g]);
-            mma16816(acc[i], a, b);
+        for (int s0 = 0; s0 < SR; s0 += 16) {
+            const __nv_bfloat16(*a16)[K + 8] = &as[buf][s0];
+            const __nv_bfloat16(*d16)[N + 8] = &ds[buf][s0];
+#pragma unroll
+            for (int i = 0; i < PER_WARP; i++) {
+                const int tile = warp * PER_WARP + i;
+                if (tile >= TILES) break;
+                const int m0 = (tile / NT) * 16, n0 = (tile % NT) * 8;
+                uint32_t a[4], b[2];
+                // A_mma(m, kk) = a16[kk][m0 + m]; B_mma(kk, n) = d16[kk][n0 + n]
+                a[0] = pack2(a16[2 * t][m0 + g], a16[2 * t + 1][m0 + g]);
+                a[1] = pack2(a16[2 * t][m0 + g + 8], a16[2 * t + 1][m0 + g + 8]);
+                a[2] = pack2(a16[2 * t + 8][m0 + g], a16[2 * t + 9][m0 + g]);
+                a[3] = pack2(a16[2 * t + 8][m0 + g + 8], a16[2 * t + 9][m0 + g + 8]);
+                b[0] = pack2(d16[2 * t][n0 + g], d16[2 * t + 1][n0 + g]);
+                b[1] = pack2(d16[2 * t + 8][n0 + g], d16[2 * t + 9][n0 + g]);
+                mma16816(acc[i], a, b);
+            }
         }
         __syncthreads();
     }
@@ -424,15 +530,44 @@ __global__ void edgeProjectKernel(int nEdges, const float* Es, const float* We, 
     C[i] = s;
 }
 
-// dWe[4 x 64] = Es^T dC, dbmsg[64] = column sums of dC (edge order), one thread per output.
-__global__ void edgeProjectBackwardKernel(int nEdges, const float* Es, const float* dC, float* dWe, float* dbmsg) {
-    const int i = threadIdx.x + blockIdx.x * blockDim.x;
-    if (i >= 5 * 64) return;
-    const int k = i / 64, f = i % 64;
-    float s = 0.f;
-    for (int e = 0; e < nEdges; e++) s += (k < 4 ? Es[e * 4 + k] : 1.f) * dC[(size_t)e * 64 + f];
-    if (k < 4) dWe[k * 64 + f] = s;
-    else dbmsg[f] = s;
+// dWe[4 x 64] = Es^T dC, dbmsg[64] = column sums of dC.  One CTA per 8 columns: thread t sums the edges t, t + 256,
+// t + 512, ... in that order (two 16-byte loads of dC and one of Es per edge), then a fixed-shape tree adds the 256
+// partial sums, so the result does not depend on timing.
+constexpr int EPB_THREADS = 256;
+__global__ void __launch_bounds__(EPB_THREADS) edgeProjectBackwardKernel(int nEdges, const float* __restrict__ Es,
+                                                                          const float* __restrict__ dC, float* dWe,
+                                                                          float* dbmsg) {
+    __shared__ float part[40][EPB_THREADS];   // (k, column) x thread
+    const int t = threadIdx.x, f0 = blockIdx.x * 8;
+    float acc[5][8] = {};
+    for (int e = t; e < nEdges; e += EPB_THREADS) {
+        const float4 es = *reinterpret_cast<const float4*>(Es + (size_t)e * 4);
+        const float4 c0 = *reinterpret_cast<const float4*>(dC + (size_t)e * 64 + f0);
+        const float4 c1 = *reinterpret_cast<const float4*>(dC + (size_t)e * 64 + f0 + 4);
+        const float ev[4] = {es.x, es.y, es.z, es.w};
+        const float cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) acc[k][j] = fmaf(ev[k], cv[j], acc[k][j]);
+            acc[4][j] += cv[j];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 5; k++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) part[k * 8 + j][t] = acc[k][j];
+    __syncthreads();
+    for (int stride = EPB_THREADS / 2; stride > 0; stride >>= 1) {
+        if (t < stride)
+            for (int q = 0; q < 40; q++) part[q][t] += part[q][t + stride];
+        __syncthreads();
+    }
+    if (t < 40) {
+        const int k = t / 8, j = t % 8;
+        if (k < 4) dWe[k * 64 + f0 + j] = part[t][0];
+        else dbmsg[f0 + j] = part[t][0];
+    }
 }
 
 // dz = dOut * [z > 0] (relu) or dOut, stored bf16 [M x N] from fp32 [M x ldd]; optionally adds dOut to accum.
@@ -641,6 +776,8 @@ extern "C" int olfgpu_gnn_gemm_dw(int M, int K1, int K2, int N, const void* A1, 
         auto a1 = static_cast<const __nv_bfloat16*>(A1);
         auto a2 = static_cast<const __nv_bfloat16*>(A2);
         auto dz = static_cast<const __nv_bfloat16*>(dZ);
+        if ((reinterpret_cast<uintptr_t>(A1) | reinterpret_cast<uintptr_t>(A2) | reinterpret_cast<uintptr_t>(dZ)) & 15)
+            throw std::runtime_error("weight-gradient operands must be 16-byte aligned");
 #define OLF_DW(a, b2, c) gemmDwKernel<a, b2, c><<<chunks, 128, 0, st>>>(M, rows, a1, a2, dz, partial)
         if (K1 == 16 && K2 == 0 && N == 64) OLF_DW(16, 0, 64);
         else if (K1 == 64 && K2 == 0 && N == 128) OLF_DW(64, 0, 128);
@@ -689,8 +826,10 @@ extern "C" int olfgpu_gnn_edge_project(int nEdges, const float* Es, const float*
 extern "C" int olfgpu_gnn_edge_project_backward(int nEdges, const float* Es, const float* dC, float* dWe,
                                                 float* dbmsg, void* stream) {
     return gnnGuard([&] {
-        edgeProjectBackwardKernel<<<(5 * 64 + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(nEdges, Es, dC,
-                                                                                                     dWe, dbmsg);
+        if ((reinterpret_cast<uintptr_t>(Es) | reinterpret_cast<uintptr_t>(dC)) & 15)
+            throw std::runtime_error("edge features and their gradients must be 16-byte aligned");
+        edgeProjectBackwardKernel<<<64 / 8, EPB_THREADS, 0, static_cast<cudaStream_t>(stream)>>>(nEdges, Es, dC, dWe,
+                                                                                                 dbmsg);
     });
 }
 
