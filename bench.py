@@ -12,6 +12,7 @@ KLU in a JVM, does not run here: no JVM, no OLF jars, no network).
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -47,36 +48,51 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms during the timed region: ONE looping nvidia-smi
+    process (``-lms 100``), started before the region and past its first sample when the region begins, so no process
+    start or NVML initialisation falls inside the timed steps."""
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.samples = []
-        self._stop = threading.Event()
+        self._proc = None
         self._t = None
+        self._first = threading.Event()
 
-    def _run(self):
-        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                vals = [v.strip() for v in out.stdout.strip().split(",")]
-                if len(vals) == 6:
-                    self.samples.append(vals)
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._proc.stdout:
+            vals = [v.strip() for v in line.strip().split(",")]
+            if len(vals) == 6:
+                self.samples.append(vals)
+                self._first.set()
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                           "--format=csv,noheader,nounits", "-lms", "100"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self._proc = None
+            return self
+        self._t = threading.Thread(target=self._read, daemon=True)
         self._t.start()
+        self._first.wait(10)                    # the first sample is in: the process is up
+        self.samples.clear()                    # only samples taken during the region count
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._proc is not None:
+            deadline = time.time() + 0.5          # a region shorter than the period still gets its sample
+            while not self.samples and time.time() < deadline:
+                time.sleep(0.01)
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=10)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+            self._t.join(timeout=10)
 
     def summary(self):
         if not self.samples:
@@ -218,6 +234,7 @@ def run_engine(args, rank: int, world: int):
     # concurrent parts: the batch split into lane ranges solved as concurrent device loops in one graph launch
     cb = None
     part_schedule = None
+    part_tuning = []
     if args.parts > 1:
         from olfgpu.security_analysis import ConcurrentBatch
         if learned is not None:
@@ -229,6 +246,12 @@ def run_engine(args, rank: int, world: int):
         cb = ConcurrentBatch(s, ns, args.parts, precision, max(refinement, 0), policy, part_schedule)
         if learned is not None:
             cb.set_device_start(x0_dev)
+        if args.schedule == "auto":
+            # the parts interleave their level kernels: the single batch's pick and the shared-memory level
+            # schedules are timed again as concurrent parts
+            part_tuning = cb.autotune(x0, tgt, mode, dis, [part_schedule, (native.LEVELS_SHARED_ALL, 0, 256),
+                                                           (native.SUBTREES, 0, 256)], max_iter=15, tol=TOL, out=out)
+            part_schedule = cb.schedule
 
     def solve_once(c_single, c_parts, xs):
         """One solve of the batch: device ms and per-scenario total iterations."""
@@ -262,12 +285,14 @@ def run_engine(args, rank: int, world: int):
     # the learned start, the device span of the whole pipelined loop
     dev_ms, wall_ms, tot_iters = [], [], 0
     sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    torch.cuda.synchronize()
     pred_total = 0.0
+    gc.collect()
+    gc.disable()                                # no collector pause inside the timed steps
     with sampler:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
         for _ in range(args.steps):
             t0 = time.perf_counter()
             pred_ms = step()
@@ -276,6 +301,7 @@ def run_engine(args, rank: int, world: int):
             dev_ms.append(ms + pred_ms)
             pred_total += pred_ms
             tot_iters += int(tot.sum())
+    gc.enable()
     solver = cb if cb is not None else ctx
     fallbacks = int(solver.last_fallbacks().size) if learned is not None else 0
     fp64_iterations = solver.last_fp64_iterations()
@@ -449,6 +475,7 @@ def run_engine(args, rank: int, world: int):
         "device_loop": bool(args.device_loop),
         "concurrent_parts": None if cb is None else {
             "parts": len(cb.ranges), "lanes": [b - a for a, b in cb.ranges], "part_schedule": list(part_schedule),
+            "part_autotune_ms": [[list(c), round(ms, 3)] for c, ms in part_tuning],
             "note": "the batch split into lane ranges, each its own context on the shared structure, solved as "
                     "concurrent device-resident Newton loops in one graph launch (results identical to one batch)"},
         "learned_start": None if learned is None else {
@@ -456,6 +483,7 @@ def run_engine(args, rank: int, world: int):
             "scenarios_on_base_start": fallbacks},
         "iterations_per_solve": round(tot_iters / args.steps / ns, 3),
         "converged_fraction": round(conv, 4),
+        "step_ms": {"device": [round(v, 3) for v in dev_ms], "wall": [round(v, 3) for v in wall_ms]},
         "structure": {"n": s.n, "nnzJ": s.nnz, "nnzLU": s.n_lu_blocks * 4, "factor_levels": s.factor_levels,
                       "solve_levels": s.forward_levels + s.backward_levels, "block_ops": s.block_ops},
         "clocks": sampler.summary(),

@@ -1636,7 +1636,8 @@ cudaGraphConditionalHandle newHandle(cudaGraph_t owner) {
 // Appends one context's device-resident Newton loop to graph g as a branch with no dependencies: the loop state reset,
 // the WHILE node, the cap of lanes still iterating, and (withResults) the scenario-major result gather.  Three
 // capture streams: cs[0] for the branch, cs[1] for the WHILE body, cs[2] for the bodies nested in it.
-void appendNewtonLoop(BatchContext& ctx, cudaGraph_t g, const cudaStream_t* cs, bool withResults) {
+void appendNewtonLoop(BatchContext& ctx, cudaGraph_t g, const cudaStream_t* cs, bool withResults,
+                      cudaEvent_t resultsDone) {
     const DeviceNet& dn = *ctx.dn;
     const DevNet& net = dn.view;
     const bool mixed = ctx.precision == 1;
@@ -1716,6 +1717,8 @@ void appendNewtonLoop(BatchContext& ctx, cudaGraph_t g, const cudaStream_t* cs, 
         dim3 blk(32, 8), grd((n + 31) / 32, (ctx.nS + 31) / 32);
         resultsKernel<<<grd, blk, 0, cs[0]>>>(ctx.x.as<double>(), ctx.iter.as<int>(), ctx.normOut.as<double>(),
                                               ctx.status.as<int>(), ctx.out.as<double>(), n, ctx.nS, ctx.S);
+        // an event node: a stream outside the graph can wait for this branch's results alone
+        if (resultsDone) OLF_CUDA(cudaEventRecordWithFlags(resultsDone, cs[0], cudaEventRecordExternal));
     }
     cudaGraph_t top;
     OLF_CUDA(cudaStreamEndCapture(cs[0], &top));
@@ -1741,7 +1744,7 @@ int runDeviceLoop(BatchContext& ctx) {
         }
         cudaGraph_t g;
         OLF_CUDA(cudaGraphCreate(&g, 0));
-        appendNewtonLoop(ctx, g, ctx.loopStreams, false);
+        appendNewtonLoop(ctx, g, ctx.loopStreams, false, nullptr);
         OLF_CUDA(cudaGraphInstantiate(&ctx.loopGraph, g, 0));
         cudaGraphDestroy(g);
         ctx.loopGraphKey = key;
@@ -2098,6 +2101,7 @@ MultiContext::~MultiContext() {
     for (cudaStream_t s : capStreams)
         if (s) cudaStreamDestroy(s);
     for (cudaEvent_t e : ready) cudaEventDestroy(e);
+    for (cudaEvent_t e : done) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
     if (hostItems) cudaFreeHost(hostItems);
 }
@@ -2119,6 +2123,8 @@ MultiContext* createMultiContext(const std::vector<BatchContext*>& members) {
     OLF_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
     m->ready.resize(members.size());
     for (auto& e : m->ready) OLF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    m->done.resize(members.size());
+    for (auto& e : m->done) OLF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     m->itemsDev.alloc(members.size() * sizeof(MultiItem));
     OLF_CUDA(cudaMallocHost(&m->hostItems, members.size() * sizeof(MultiItem)));
     return m.release();
@@ -2162,8 +2168,9 @@ void launchMultiLoops(MultiContext& m) {
         m.loopKeys.clear();
         m.loopBatches.clear();
         m.loopCfgs.clear();
-        for (BatchContext* c : m.members) {
-            appendNewtonLoop(*c, g, m.capStreams, true);
+        for (size_t i = 0; i < k; i++) {
+            BatchContext* c = m.members[i];
+            appendNewtonLoop(*c, g, m.capStreams, true, m.done[i]);
             m.loopKeys.push_back(loopKey(*c));
             m.loopBatches.push_back(c->batch());
             m.loopCfgs.push_back(c->cfg);
@@ -2318,11 +2325,19 @@ void solveMulti(MultiContext& m, double* const* outs) {
     for (size_t i = 0; i < m.members.size(); i++) {
         BatchContext& c = *m.members[i];
         if (outs && outs[i]) {
+            // device loops: a member's results go to the host on its own stream as soon as its branch of the graph
+            // has gathered them, while the other branches still run; persistent tiles: after the launch
+            cudaStream_t cs = st;
+            if (m.lanesPerTile == 0) {
+                cs = c.stream;
+                OLF_CUDA(cudaStreamWaitEvent(cs, m.done[i], 0));
+            }
             OLF_CUDA(cudaMemcpyAsync(outs[i], c.out.p, static_cast<size_t>(c.nS) * (c.net->host.n + 3) * 8,
-                                     cudaMemcpyDeviceToHost, st));
+                                     cudaMemcpyDeviceToHost, cs));
         }
     }
     OLF_CUDA(cudaStreamSynchronize(st));
+    for (BatchContext* c : m.members) OLF_CUDA(cudaStreamSynchronize(c->stream));
     OLF_CUDA(cudaEventElapsedTime(&m.lastMs, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -343,6 +343,7 @@ struct MultiContext {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::vector<cudaEvent_t> ready;      // per member: its lanes are installed
+    std::vector<cudaEvent_t> done;       // per member: its results are gathered (an event node of the loop graph)
     int lanesPerTile = 2, threads = 256, order = 0;   // order 0: as given, 1: most buses first
     // lanesPerTile 0: one graph whose branches are the members' own device-resident Newton loops (their level
     // schedules, concurrent on the device), instead of the persistent tiles

@@ -221,6 +221,7 @@ class LearnedStart:
             if max_seconds is not None and time.time() - t0 > max_seconds:
                 break
         torch.cuda.synchronize()
+        self.last_train_seconds, self.last_train_steps = time.time() - t0, step
         return losses
 
     # ------------------------------------------------------------------------------------------------------------
@@ -482,7 +483,9 @@ def main(argv=None) -> int:
                "load_scaling_range": [a.lo, a.hi], "epochs": a.epochs, "batch": a.batch, "lr": a.lr, "seed": a.seed,
                "adam_steps": int(ls.net.step), "epoch_losses": [float(v) for v in losses],
                "held_out_normalised_mse": {"network": after[0], "untrained": before[0], "base_start": after[1]},
-               "generate_seconds": round(gen_s, 1), "total_seconds": round(time.time() - t0, 1)}
+               "generate_seconds": round(gen_s, 1), "train_seconds": round(ls.last_train_seconds, 2),
+               "ms_per_adam_step": round(1e3 * ls.last_train_seconds / max(1, ls.last_train_steps), 3),
+               "total_seconds": round(time.time() - t0, 1)}
         path = a.report or os.path.splitext(a.out)[0] + ".train.json"
     else:
         ls = LearnedStart.load(a.checkpoint, g)

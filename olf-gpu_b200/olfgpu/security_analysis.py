@@ -205,8 +205,31 @@ class ConcurrentBatch:
             c.set_schedule(*schedule)
             c.set_device_loop(True)
             self.contexts.append(c)
+        self.schedule = tuple(schedule)
         self.multi = native.MultiContext(self.contexts)
         self.multi.set_schedule(0, 0, 0)
+
+    def set_schedule(self, schedule):
+        """Every part's level schedule, (schedule, lanes per tile, threads) as BatchContext.set_schedule."""
+        for c in self.contexts:
+            c.set_schedule(*schedule)
+        self.schedule = tuple(schedule)
+
+    def autotune(self, x0_base, target, base_row_mode, disabled, candidates, x0_full=None, repeats: int = 2,
+                 **kw):
+        """Times each candidate schedule on this batch split into its parts (the concurrent parts interleave their
+        level kernels, so the fastest schedule of one batch need not be the fastest here): per candidate one solve
+        to build its graphs, then the best of ``repeats`` timed solves.  Keeps the fastest and returns
+        [(schedule, ms)].  Every candidate's results are those of the single batch, bit for bit."""
+        timings = []
+        for cand in dict.fromkeys(tuple(c) for c in candidates):
+            self.set_schedule(cand)
+            self.solve(x0_base, target, base_row_mode, disabled, x0_full, **kw)
+            ms = min(self.solve(x0_base, target, base_row_mode, disabled, x0_full, **kw)[1] for _ in range(repeats))
+            timings.append((cand, float(ms)))
+        best = min(timings, key=lambda t: t[1])[0]
+        self.set_schedule(best)
+        return timings
 
     def set_device_start(self, x0_device=None, fallback: bool = True):
         """Per-scenario start states on the device ([nS, n] torch CUDA tensor; each part reads its rows), with the
