@@ -32,10 +32,12 @@ GRID = "grid9241"
 N_OUTAGES = 500
 TOL = 1e-8
 CHECKPOINT = os.path.join(ROOT, "olf-gpu_b200", "checkpoints", "warmstart_grid9241.npz")
-# DRAM bytes (read + write) of one lane's factorization (dense-front plan, narrow levels in shared memory), from an
-# ncu capture of the 89 factorization launches of the first Newton iteration of a 64-outage batch (FP64: 490.9 MB,
-# FP32 LU: 288.3 MB over 64 lanes); scaled to a launch by the lanes it factorizes
-TRAFFIC = {"fp64": 7.67e6, "mixed": 4.51e6}
+# DRAM bytes (read + write) of one lane's factorization (narrow levels in shared memory), from ncu captures of the
+# launches of the first factorization of a 64-outage batch: the dense-front plan on plain minimum degree (89 launches;
+# FP64 490.9 MB, FP32 LU 288.3 MB over 64 lanes) and on the shallow-tree order (120 launches; 663.8 MB, 374.6 MB);
+# scaled to a launch by the lanes it factorizes
+TRAFFIC = {("dense", "fp64"): 7.67e6, ("dense", "mixed"): 4.51e6,
+           ("shallow", "fp64"): 10.37e6, ("shallow", "mixed"): 5.85e6}
 
 
 def _peaks():
@@ -105,6 +107,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def plan_flags(plan: str) -> int:
+    """Structure ordering flags of a --plan choice: scaled (minimum degree), deferred (deferred-L), dense (minimum
+    degree + dense front), shallow (minimum degree relaxed toward a shallow elimination tree + dense front)."""
+    from olfgpu import native
+    return {"deferred": native.PLAN_DEFERRED_L, "dense": native.PLAN_DENSE_FRONT,
+            "shallow": native.PLAN_DENSE_FRONT | native.MIN_DEGREE_SHALLOW}.get(plan, 0)
+
+
+def dense_front(plan: str) -> bool:
+    return plan in ("dense", "shallow")
+
+
 def workload(rank: int, count: int = N_OUTAGES):
     from olfgpu import packing, synthetic
     g = synthetic.build(GRID)
@@ -136,14 +150,13 @@ def launches_per_solve(s, sched, rounds: int, dense: bool, deferred: bool, mixed
     factor_from = factor_to
     while factor_from > 0 and wf[factor_from - 1] <= NARROW:
         factor_from -= 1
+    # the shared-memory region: the narrow levels from the top of the tree down while a level holds <=
+    # REGION_THREADS tasks and the blocks fit REGION_SLOTS
     region_from = factor_to
     if not deferred:
-        region_from = factor_from
-        while region_from < factor_to and f[factor_to] - f[region_from] > REGION_SLOTS:
-            region_from += 1
-    for lv in range(region_from, factor_to):
-        if wf[lv] > REGION_THREADS:
-            region_from = lv + 1
+        while (region_from > factor_from and wf[region_from - 1] <= REGION_THREADS
+               and f[factor_to] - f[region_from - 1] <= REGION_SLOTS):
+            region_from -= 1
     fwd_from = nf
     while fwd_from > 0 and wfw[fwd_from - 1] <= NARROW:
         fwd_from -= 1
@@ -200,7 +213,7 @@ def run_engine(args, rank: int, world: int):
     g, p, outs = workload(rank, args.outages)
     precision = native.MIXED if args.precision == "mixed" else native.FP64
     refinement = args.refinement if precision == native.MIXED else 0
-    s = native.Structure(p, {"deferred": native.PLAN_DEFERRED_L, "dense": native.PLAN_DENSE_FRONT}.get(args.plan, 0))
+    s = native.Structure(p, plan_flags(args.plan))
     ns = outs.shape[0]
     ctx = native.BatchContext(s, ns)
     ctx.set_linear_solver_settings(precision, max(refinement, 0))
@@ -392,7 +405,7 @@ def run_engine(args, rank: int, world: int):
     fact_launch_ms = ph["factor"] / max(ph["iterations"], 1)
     fact_bytes_launch = fact_bytes_lane * ph["factorized_lanes"] / max(ph["iterations"], 1)
     fact_achieved = fact_bytes_launch / (fact_launch_ms * 1e-3) / 1e9 if fact_launch_ms > 0 else 0.0
-    traffic = TRAFFIC["fp64" if fact_w == 8 else "mixed"]
+    traffic = TRAFFIC.get((args.plan, "fp64" if fact_w == 8 else "mixed"))
     if traffic is not None:
         traffic = int(traffic * ph["factorized_lanes"] / max(ph["iterations"], 1))
     sched = ctx.schedule()[0]
@@ -403,7 +416,7 @@ def run_engine(args, rank: int, world: int):
         fact_kernel += " + factorRangeKernel narrow levels"
     elif sched[0] == native.COOPERATIVE:
         fact_kernel = "block-LU factorization of one Newton iteration (factorCoopKernel"
-    fact_kernel += (" + denseFrontKernel)" if args.plan == "dense" else ")")
+    fact_kernel += (" + denseFrontKernel)" if dense_front(args.plan) else ")")
     if ph["iterations"] == 0:
         # the autotuner picked the persistent schedule: one launch runs the whole Newton loop of the batch
         fact_kernel = "newtonPersistentKernel (the whole Newton loop of the batch in one launch)"
@@ -489,7 +502,7 @@ def run_engine(args, rank: int, world: int):
         "clocks": sampler.summary(),
     }
     rounds = max(ph["iterations"], 1)
-    per_solve = launches_per_solve(s, sched, rounds, args.plan == "dense", args.plan == "deferred",
+    per_solve = launches_per_solve(s, sched, rounds, dense_front(args.plan), args.plan == "deferred",
                                    precision == native.MIXED and fp64_iterations < rounds,
                                    (rounds - 1) if refinement > 0 and args.mixed_policy == "refine" else 0)
     if args.device_loop:
@@ -513,8 +526,9 @@ def run_engine(args, rank: int, world: int):
 
 def uneven_summary(args):
     """The uneven-batching workload (four grids, reactive limits on), measured inside the default line: one graph
-    whose branches are the grids' device-resident Newton loops (dense-front plans, shared-memory level schedule), the
-    same grids solved back to back one batch each, and the single persistent launch (tiles of 2 lanes)."""
+    whose branches are the grids' device-resident Newton loops (the --plan's dense-front plans, shared-memory level
+    schedule), the same grids solved back to back one batch each, and the single persistent launch (tiles of 2
+    lanes, which run the scaled plan)."""
     from olfgpu import native, packing, synthetic
     from olfgpu.security_analysis import MultiGridAnalysis
     grids = [synthetic.build(nm) for nm, _ in UNEVEN]
@@ -530,14 +544,15 @@ def uneven_summary(args):
         return float(np.median([fn() for _ in range(steps)]))
 
     res = {}
-    ma = MultiGridAnalysis(packs, counts, schedule=(0, 0, 0), ordering=native.PLAN_DENSE_FRONT,
+    front = plan_flags(args.plan) if dense_front(args.plan) else native.PLAN_DENSE_FRONT
+    ma = MultiGridAnalysis(packs, counts, schedule=(0, 0, 0), ordering=front,
                            member_schedule=(native.LEVELS_SHARED_ALL, 0, 256))
     res["one_graph_device_loops"] = timed(lambda: ma.solve(outs)[1])
     loop_res, _ = ma.solve(outs)
     ma.close()
     seq = []
     for p, o in zip(packs, outs):
-        st = native.Structure(p, native.PLAN_DENSE_FRONT)
+        st = native.Structure(p, front)
         c = native.BatchContext(st, o.shape[0], native.BATCHED_LU, p.rl)
         c.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
         c.set_device_loop(True)
@@ -615,8 +630,8 @@ def run_uneven(args, rank: int, world: int):
             wall.append((time.perf_counter() - t0) * 1e3)
         return float(np.mean(dev)), float(np.mean(wall))
 
-    ordering = {"deferred": native.PLAN_DEFERRED_L, "dense": native.PLAN_DENSE_FRONT}.get(args.plan, 0)
-    member = (native.LEVELS_SHARED_ALL, 0, 256) if args.plan == "dense" else (native.LEVELS, 2, 256)
+    ordering = plan_flags(args.plan)
+    member = (native.LEVELS_SHARED_ALL, 0, 256) if dense_front(args.plan) else (native.LEVELS, 2, 256)
     policy = native.MIXED_FP64_NEAR if args.mixed_policy == "fp64near" else native.MIXED_REFINE
     ma = MultiGridAnalysis(packs, counts, precision=precision, refinement_steps=args.refinement, schedule=-1,
                            ordering=ordering, member_schedule=member, mixed_policy=policy)
@@ -679,7 +694,7 @@ def run_uneven(args, rank: int, world: int):
     if loops:
         launches = 0
         for (st, c, p, dis), r in zip(seq, rounds):
-            launches += launches_per_solve(st, member, max(r, 1), args.plan == "dense", args.plan == "deferred",
+            launches += launches_per_solve(st, member, max(r, 1), dense_front(args.plan), args.plan == "deferred",
                                            precision == native.MIXED, 0) + 2 + max(r, 1)
     else:
         launches = 1 + 4 + 5 * 4
@@ -786,10 +801,11 @@ def main():
                     help="start states: the base case, or the learned warm start (default when its checkpoint exists)")
     ap.add_argument("--checkpoint", default=CHECKPOINT)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
-    ap.add_argument("--plan", default=None, choices=["scaled", "deferred", "dense"],
-                    help="block-LU plan: L scaled at its task, deferred (half the levels) or dense (the trailing "
-                         "block factorized in shared memory; default for the N-1 workload, whose autotuned schedules "
-                         "all run it); the uneven workload's persistent launch runs the scaled plan")
+    ap.add_argument("--plan", default=None, choices=["scaled", "deferred", "dense", "shallow"],
+                    help="block-LU plan: L scaled at its task, deferred (half the levels), dense (minimum degree, the "
+                         "trailing block factorized in shared memory) or shallow (dense, on minimum degree relaxed "
+                         "toward a shallow elimination tree: 123 instead of 201 levels on the 9,241-bus grid; the "
+                         "default for the N-1 workload); the uneven workload's persistent launch runs the scaled plan")
     ap.add_argument("--schedule", default="auto", choices=["auto", "levels", "coop", "shared", "shared-all"],
                     help="auto: the engine's autotuner picks the Newton-iteration schedule on the first solve; "
                          "shared: level launches with the narrow factorization levels in shared memory; shared-all: "
@@ -809,7 +825,7 @@ def main():
                     help="n1: the 9,241-bus N-1 batch (default); uneven: four grids in one persistent launch")
     args = ap.parse_args()
     if args.plan is None:
-        args.plan = "dense"
+        args.plan = "shallow"
     if args.start is None:
         args.start = "learned" if os.path.exists(args.checkpoint) and args.outages == N_OUTAGES else "base"
     args.warmup = max(args.warmup, 3) if args.impl == "engine" else args.warmup

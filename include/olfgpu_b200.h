@@ -37,7 +37,8 @@ const char* olfgpu_last_error(void);
  * The families this engine does not model (HVDC AC emulation, DISTR_Q/RHO/SHUNT_B, zero-impedance branches, load
  * models, reactive relocation, transformer/shunt voltage-control columns) must be empty: a non-empty one, or a
  * control column >= 0, is rejected with an error.  ordering: 0 minimum degree (default), 1 nested dissection,
- * 2 natural; plus 8 for the deferred-L block-LU plan (the L factor stays unscaled during the factorization: about
+ * 2 natural, 3 minimum degree relaxed toward a shallow elimination tree (fewer dependency levels at about the same
+ * fill; 3 + 16 = 19 is the fastest measured plan); plus 8 for the deferred-L block-LU plan (the L factor stays unscaled during the factorization: about
  * half the dependency levels, one more 2x2 block read per update), or 16 for the dense-front plan (the trailing
  * pivots whose blocks are all present, up to 32, are factorized as one dense front in shared memory; not runnable by
  * the persistent schedules or the multi-grid launch).

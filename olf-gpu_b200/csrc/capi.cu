@@ -251,7 +251,7 @@ extern "C" int olfgpu_structure_levels(int64_t structure, int* factorLevelPtr, i
 extern "C" int olfgpu_structure_subtrees(int64_t structure, int64_t* stats6) {
     return guarded([&] {
         const BlockPlan& p = structureOf(structure)->host.plan;
-        const NarrowBounds nbd = narrowBounds(p);
+        const NarrowBounds nbd = binBounds(p);
         const SubtreeBinsHost h = planSubtreeBins(p, nbd);
         const std::string err = checkSubtreeBins(p, nbd, h);
         if (!err.empty()) throw std::runtime_error("subtree bins: " + err);

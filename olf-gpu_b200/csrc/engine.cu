@@ -26,6 +26,28 @@ constexpr int SUBTREE_BINS = 96;
 constexpr int SUBTREE_PHASES = 6;   // bins of the remaining forest, phase after phase
 constexpr int NARROW = 48;   // a level of at most this many tasks (positions) is narrow
 
+// The shared-memory factorization region: the narrow levels below factorTo, from the top of the tree down, while each
+// fits one round of the region's CTA (at most REGION_THREADS tasks) and their blocks fit REGION_BYTES (FP64, one lane:
+// two CTAs per SM).  (Taking the moderately wide levels under them too, up to REGION_THREADS tasks, as far as the
+// slots reach, measured the same step time on the shallow-tree plan with a third fewer launches: not kept.)
+constexpr size_t REGION_BYTES = 110 * 1024;
+
+int regionStart(const BlockPlan& p, const NarrowBounds& nbd) {
+    if (p.deferredL) return nbd.factorTo;   // (deferred-L updates also read the pivot's inverse: range launches)
+    int from = nbd.factorTo;
+    while (from > nbd.factorFrom && p.levelPtr[from] - p.levelPtr[from - 1] <= REGION_THREADS &&
+           static_cast<size_t>(p.levelPtr[nbd.factorTo] - p.levelPtr[from - 1]) * 32 <= REGION_BYTES) {
+        from--;
+    }
+    return from;
+}
+
+NarrowBounds binBounds(const BlockPlan& p) {
+    NarrowBounds nbd = narrowBounds(p);
+    nbd.factorFrom = std::min(nbd.factorFrom, regionStart(p, nbd));   // the bins stop where the region starts
+    return nbd;
+}
+
 NarrowBounds narrowBounds(const BlockPlan& p) {
     auto countOf = [](const std::vector<int>& ptr, size_t l) { return ptr[l + 1] - ptr[l]; };
     NarrowBounds nbd{};
@@ -318,7 +340,7 @@ std::string checkSubtreeBins(const BlockPlan& p, const NarrowBounds& nbd, const 
 template <typename SplitFn>
 void buildSubtreeBins(DeviceNet& d, const BlockPlan& p, const std::vector<int>& lrowLen, SplitFn splitOf) {
     d.sub = SubtreePlan{};
-    const NarrowBounds nbd{d.factorFrom, d.factorTo, d.fwdFrom, d.bwdUntil};
+    const NarrowBounds nbd = binBounds(p);
     SubtreeBinsHost h = planSubtreeBins(p, nbd);
     if (h.nBins == 0) return;
     d.topLevelPtr = h.topLevelPtr;
@@ -586,22 +608,10 @@ std::shared_ptr<DeviceNet> uploadNet(const Structure& s) {
     const NarrowBounds nbd = narrowBounds(p);
     d->factorTo = nbd.factorTo;
     d->factorFrom = nbd.factorFrom;
-    // the shared-memory region: the narrow factorization levels before factorTo whose blocks fit REGION_BYTES (FP64,
-    // one lane: two CTAs per SM); every block they produce gets a slot, in level order, and every update its operands'
-    // slots in ops.w (slot + 1 of the L block in the low 16 bits, of the U block in the high 16 bits, 0 outside).
-    // Deferred-L plans keep the range launches (their updates also read the pivot's inverse).
-    constexpr size_t REGION_BYTES = 110 * 1024;
-    d->regionFrom = d->factorTo;
-    if (!p.deferredL) {
-        d->regionFrom = d->factorFrom;
-        while (d->regionFrom < d->factorTo &&
-               static_cast<size_t>(p.levelPtr[d->factorTo] - p.levelPtr[d->regionFrom]) * 32 > REGION_BYTES) {
-            d->regionFrom++;
-        }
-    }
-    for (int l = d->regionFrom; l < d->factorTo; l++) {   // one round of the CTA per level
-        if (p.levelPtr[l + 1] - p.levelPtr[l] > REGION_THREADS) d->regionFrom = l + 1;
-    }
+    // the shared-memory region (regionStart): every block its levels produce gets a slot, in level order, and every
+    // update its operands' slots in ops.w (slot + 1 of the L block in the low 16 bits, of the U block in the high 16
+    // bits, 0 outside)
+    d->regionFrom = regionStart(p, nbd);
     d->regionBase = p.levelPtr[d->regionFrom];
     d->regionSlots = p.levelPtr[d->factorTo] - d->regionBase;
     if (d->regionSlots > 0) {

@@ -112,6 +112,10 @@ struct NarrowBounds {
     int factorFrom, factorTo, fwdFrom, bwdUntil;
 };
 NarrowBounds narrowBounds(const BlockPlan& p);
+// The first level of the shared-memory factorization region (nbd.factorTo: none), and the bounds the subtree bins
+// use: the narrow bounds with the wide levels ending where the region starts.
+int regionStart(const BlockPlan& p, const NarrowBounds& nbd);
+NarrowBounds binBounds(const BlockPlan& p);
 
 // The subtree bins of a plan's wide levels and the top lists of every level (host arrays; see SubtreePlan).
 struct SubtreeBinsHost {

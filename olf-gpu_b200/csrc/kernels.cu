@@ -549,6 +549,12 @@ __device__ __forceinline__ void store4(T* base, size_t blk, size_t S, int s, T a
     p[3 * S] = d;
 }
 
+// Register cap of the factorization level kernels: blocks of 32 x max(4, P) threads, at least as many resident per SM
+// as this many registers a thread allow.
+#ifndef OLF_FACTOR_MAX_REGS
+#define OLF_FACTOR_MAX_REGS 64
+#endif
+
 // Launch geometry of one level: P threads share each task (or row) of the level, splitting its update list P ways;
 // blocks are 32 lanes x max(4, P) threads (4 rows measured 1.5 % faster than 8 on the 500-lane batch, 16 rows 5 %
 // slower).  The P partial sums are added in a fixed order (part 0 first), so the result does not depend on
@@ -560,7 +566,8 @@ struct Split {
 };
 
 template <typename T, int P>
-__global__ void __launch_bounds__(1024) factorLevelKernel(DevNet net, DevBatch b, T* lu, int first, int count) {
+__global__ void __launch_bounds__(32 * Split<P>::ROWS, 65536 / (OLF_FACTOR_MAX_REGS * 32 * Split<P>::ROWS))
+    factorLevelKernel(DevNet net, DevBatch b, T* lu, int first, int count) {
     constexpr int TPB = Split<P>::TPB, ROWS = Split<P>::ROWS;
     __shared__ T red[ROWS][4][32];
     const size_t S = b.S;

@@ -71,7 +71,7 @@ Structure buildStructure(int n, int ncb, const double* cbPar, const int* cbIx, i
 
 // Orderings of the bus graph for the block LU (low bits), and the plan variant flag: PLAN_DEFERRED_L keeps the L
 // factor unscaled during the factorization (half the dependency levels, one more block read per update).
-enum Ordering { ORDER_MIN_DEGREE = 0, ORDER_NESTED_DISSECTION = 1, ORDER_NATURAL = 2 };
+enum Ordering { ORDER_MIN_DEGREE = 0, ORDER_NESTED_DISSECTION = 1, ORDER_NATURAL = 2, ORDER_MIN_DEGREE_SHALLOW = 3 };
 constexpr int PLAN_DEFERRED_L = 8;
 // Plan flag: the trailing positions of the elimination order whose blocks are all present (at most MAX_FRONT pivots,
 // the root separators of the elimination tree) are factorized as one dense front in shared memory instead of one

@@ -134,7 +134,7 @@ JNIEXPORT jlong JNICALL OLF_JNI(ac_equations_vector_gpu, StructureNative, create
         ptr(drC), len(drC), ptr(drK), len(drK), ptr(dbR), len(dbR), ptr(dbC), len(dbC), ptr(dbK), len(dbK), ptr(pcs),
         len(pcs), ptr(lmP), len(lmP), ptr(lmI), len(lmI), ptr(rrG), len(rrG), ptr(rrC), len(rrC), ptr(obA), len(obA),
         ptr(zA), len(zA), ptr(rrB), len(rrB), ptr(rrT), len(rrT), ptr(rrD), len(rrD), ptr(idr), len(idr),
-        16 /* minimum degree with the dense-front block-LU plan, the engine's fastest */, &h);
+        16 | 3 /* minimum degree toward a shallow elimination tree, dense-front block-LU plan: the engine's fastest */, &h);
     return ok(env, rc, "GPU structure creation") ? static_cast<jlong>(h) : 0;
 }
 

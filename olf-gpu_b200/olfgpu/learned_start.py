@@ -405,7 +405,7 @@ def evaluate_starts(ls: "LearnedStart", scaling: float, n_outages: int, seed: in
     rng = np.random.default_rng(seed)
     outs = np.sort(rng.choice(synthetic.outage_candidates(ls.grid), size=n_outages, replace=False)).astype(np.int32)
     dis = p.outage_masks(outs)
-    s = native.Structure(p, native.PLAN_DENSE_FRONT)
+    s = native.Structure(p, native.PLAN_DEFAULT)
     ctx = native.BatchContext(s, n_outages)
     ctx.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
     # the referee: FP64 Newton from the base start (the converged states the starts are measured against)

@@ -65,7 +65,9 @@ VAR_BUS_V, VAR_BUS_PHI = 0, 1
 # independent subtrees in one launch per phase)
 LEVELS, PERSISTENT, COOPERATIVE, LEVELS_SHARED, LEVELS_SHARED_ALL, SUBTREES, AUTOTUNE = 0, 1, 2, 3, 4, 5, -1
 # Structure orderings (0 minimum degree, 1 nested dissection, 2 natural) and the deferred-L plan flag
-MIN_DEGREE, NESTED_DISSECTION, NATURAL, PLAN_DEFERRED_L, PLAN_DENSE_FRONT = 0, 1, 2, 8, 16
+MIN_DEGREE, NESTED_DISSECTION, NATURAL, MIN_DEGREE_SHALLOW, PLAN_DEFERRED_L, PLAN_DENSE_FRONT = 0, 1, 2, 3, 8, 16
+# The fastest measured plan: minimum degree relaxed toward a shallow elimination tree, with the dense front
+PLAN_DEFAULT = PLAN_DENSE_FRONT | MIN_DEGREE_SHALLOW
 
 
 class NativeError(RuntimeError):

@@ -7,6 +7,7 @@ chunks sized by ``recommendBatchSize`` (``GpuBatchChunkSolver.solveQualifiedInCh
 """
 from __future__ import annotations
 
+import concurrent.futures
 import dataclasses
 from typing import Optional, Sequence
 
@@ -40,7 +41,7 @@ class SecurityAnalysis:
     """Holds the structure and one context per chunk width, reused across calls (GpuBatchContextCache)."""
 
     def __init__(self, packed: Packed, precision: int = native.FP64, refinement_steps: int = 1,
-                 reactive_limits: bool = False, ordering: int = native.PLAN_DENSE_FRONT, max_chunk: int = 4096,
+                 reactive_limits: bool = False, ordering: int = native.PLAN_DEFAULT, max_chunk: int = 4096,
                  schedule: Optional[tuple] = (native.LEVELS_SHARED_ALL, 0, 256)):
         """``schedule``: the arguments of BatchContext.set_schedule for every chunk's context: by default level
         launches with the narrow levels of every phase in shared memory (the fastest measured on the 9,241-bus
@@ -208,6 +209,7 @@ class ConcurrentBatch:
         self.schedule = tuple(schedule)
         self.multi = native.MultiContext(self.contexts)
         self.multi.set_schedule(0, 0, 0)
+        self._pool = None
 
     def set_schedule(self, schedule):
         """Every part's level schedule, (schedule, lanes per tile, threads) as BatchContext.set_schedule."""
@@ -244,9 +246,17 @@ class ConcurrentBatch:
         n = self.structure.n
         if out is None:
             out = np.zeros((self.n, n + 3))
-        for c, (a, b) in zip(self.contexts, self.ranges):
+
+        def stage(k):
+            (a, b), c = self.ranges[k], self.contexts[k]
             c.stage(x0_base, target, base_row_mode, disabled[a:b], None if x0_full is None else x0_full[a:b],
                     max_iter=max_iter, tol=tol)
+        # the parts' host work (validation, outage bit packing) and uploads run side by side: the library call
+        # releases the interpreter lock, and each part has its own buffers and stream
+        if self._pool is None:
+            self._pool = concurrent.futures.ThreadPoolExecutor(max_workers=len(self.contexts))
+        for f in [self._pool.submit(stage, k) for k in range(len(self.contexts))]:
+            f.result()
         views = [out[a:b] for a, b in self.ranges]
         _, ms = self.multi.solve(views)
         return out, ms
@@ -258,6 +268,9 @@ class ConcurrentBatch:
         return max(c.last_fp64_iterations() for c in self.contexts)
 
     def close(self):
+        if self._pool is not None:
+            self._pool.shutdown()
+            self._pool = None
         self.multi.close()
         for c in self.contexts:
             c.close()

@@ -400,14 +400,16 @@ def test_cooperative_sweeps_match_level_launches(engine_lib, precision):
                                                     (3, 2, 512), (4, 0, 256), (5, 0, 256)])
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("name", ["grid2000", "grid9241"])
-def test_dense_front_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes, threads, precision, name):
-    """The dense-front plan (the trailing dense block factorized in shared memory) gives the oracle's statuses and
-    states, with fewer dependency levels."""
+@pytest.mark.parametrize("plan", [16, 19])
+def test_dense_front_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes, threads, precision, name, plan):
+    """The dense-front plans (the trailing dense block factorized in shared memory; on plain minimum degree, 16, and
+    on minimum degree toward a shallow elimination tree, 19) give the oracle's statuses and states, with fewer
+    dependency levels."""
     from olfgpu import native, synthetic
     g, p = grid(name)
     outs = synthetic.draw_outages(g, 64, seed=96)
     dis = p.outage_masks(outs)
-    s = native.Structure(p, ordering=native.PLAN_DENSE_FRONT)
+    s = native.Structure(p, ordering=plan)
     assert s.factor_levels < native.Structure(p).factor_levels
     ctx = native.BatchContext(s, outs.shape[0])
     ctx.set_linear_solver_settings(precision, 1)
@@ -447,7 +449,7 @@ def test_subtree_bins_match_oracle(engine_lib, oracle_mod, precision, name):
     outs = synthetic.draw_outages(g, 96, seed=97)
     dis = p.outage_masks(outs)
     ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis)
-    for plan in (0, native.PLAN_DENSE_FRONT):
+    for plan in (0, native.PLAN_DENSE_FRONT, native.PLAN_DEFAULT):
         s = native.Structure(p, ordering=plan)
         assert s.subtrees()["bins"] > 0
         r = {}
@@ -463,7 +465,7 @@ def test_subtree_bins_match_oracle(engine_lib, oracle_mod, precision, name):
 
 
 @pytest.mark.parametrize("precision,tol", [(0, 1e-9), (1, 2e-3)])
-@pytest.mark.parametrize("name,plan", [("grid2000", 0), ("grid2000", 16), ("grid9241", 16)])
+@pytest.mark.parametrize("name,plan", [("grid2000", 0), ("grid2000", 16), ("grid9241", 16), ("grid9241", 19)])
 def test_transposed_solve_matches_oracle(engine_lib, oracle_mod, precision, tol, name, plan):
     """J^T y = c on the factors of J (the adjoint solve, lu/transposed_solve.cuh): against the oracle's LU of the
     explicit transpose; the plain solve of the same call against the oracle's LU of J."""
@@ -498,7 +500,7 @@ def test_config1_every_non_bridge_outage_of_the_2000_bus_grid(engine_lib, oracle
     outs = synthetic.outage_candidates(g)
     assert outs.shape[0] > 2000
     dis = p.outage_masks(outs)
-    s = native.Structure(p, native.PLAN_DENSE_FRONT)
+    s = native.Structure(p, native.PLAN_DEFAULT)
     ctx = native.BatchContext(s, outs.shape[0])
     ctx.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
     ctx.set_device_loop(True)

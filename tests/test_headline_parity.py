@@ -1,6 +1,6 @@
 """Parity on the benchmark's own configuration (needs a B200): the 9,241-bus grid's 500 drawn outages, the learned
-warm start with the base-start fallback, FP32 LU with FP64 refinement and the dense-front plan under the shared-memory
-level schedule: every scenario's status equals the FP64 oracle's and every converged state is within 1e-8 pu / rad of
+warm start with the base-start fallback, FP32 LU with FP64 refinement and the dense-front plans (on plain minimum
+degree, and on the shallow-tree minimum degree the benchmark runs) under the shared-memory level schedule: every scenario's status equals the FP64 oracle's and every converged state is within 1e-8 pu / rad of
 it; the plain FP64 engine on the same batch agrees too."""
 import os
 
@@ -34,8 +34,12 @@ def _check(r, ref, n):
     assert d[:, 0::2].max() <= STATE_TOL, ("Va", float(d[:, 0::2].max()))
 
 
+PLANS = {"dense": 16, "shallow": 19}     # native.PLAN_DENSE_FRONT, native.PLAN_DEFAULT
+
+
+@pytest.mark.parametrize("plan", sorted(PLANS))
 @pytest.mark.parametrize("policy", [0, 1])
-def test_learned_mixed_matches_oracle_on_the_benchmark_batch(engine_lib, headline, policy):
+def test_learned_mixed_matches_oracle_on_the_benchmark_batch(engine_lib, headline, policy, plan):
     """Both mixed-precision policies; the scenarios that converge from their learned start take the polishing step
     (on by default), the others run from the base start as the oracle does."""
     import torch
@@ -43,7 +47,7 @@ def test_learned_mixed_matches_oracle_on_the_benchmark_batch(engine_lib, headlin
     from olfgpu.learned_start import LearnedStart
     g, p, outs, ref = headline
     ns = outs.shape[0]
-    s = native.Structure(p, native.PLAN_DENSE_FRONT)
+    s = native.Structure(p, PLANS[plan])
     ctx = native.BatchContext(s, ns)
     ctx.set_linear_solver_settings(native.MIXED, 3)
     ctx.set_mixed_precision_policy(policy)
@@ -100,11 +104,12 @@ def test_polishing_step_brings_learned_lanes_next_to_the_solution(engine_lib, he
     assert np.abs(out[1e-2][base_lanes, :n] - ref[base_lanes, :n]).max() <= 1e-11
 
 
+@pytest.mark.parametrize("plan", sorted(PLANS))
 @pytest.mark.parametrize("precision", [0, 1])
-def test_base_start_matches_oracle_on_the_benchmark_batch(engine_lib, headline, precision):
+def test_base_start_matches_oracle_on_the_benchmark_batch(engine_lib, headline, precision, plan):
     from olfgpu import native
     g, p, outs, ref = headline
-    s = native.Structure(p, native.PLAN_DENSE_FRONT)
+    s = native.Structure(p, PLANS[plan])
     ctx = native.BatchContext(s, outs.shape[0])
     ctx.set_linear_solver_settings(precision, 3)
     ctx.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)

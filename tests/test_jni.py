@@ -186,7 +186,7 @@ def test_create_structure_through_jni_matches_the_c_abi(jni):
     info = np.zeros(9, np.int32)
     ops = _i64(0)
     assert L.olfgpu_structure_info(h, info.ctypes.data_as(native._ip), ctypes.byref(ops)) == 0
-    ref = native.Structure(p, ordering=native.PLAN_DENSE_FRONT)
+    ref = native.Structure(p, ordering=native.PLAN_DEFAULT)
     assert info[0] == ref.n and info[1] == ref.nnz and info[3] == ref.n_lu_blocks and ops.value == ref.block_ops
     # the reference-compatible structure is the same whatever the plan
     ex = {k: np.zeros(ref.export()[k].shape, np.int32) for k in ("row_map", "row_ptr", "col_idx", "diag_pos")}
@@ -290,7 +290,7 @@ def test_solve_through_jni_equals_the_c_abi(jni):
     assert jvm.take_exception() is None
     got = _solve(jni, jvm, ctx, p, dis)
     assert got is not None, jvm.take_exception()
-    s = native.Structure(p, ordering=native.PLAN_DENSE_FRONT)
+    s = native.Structure(p, ordering=native.PLAN_DEFAULT)
     c = native.BatchContext(s, outs.shape[0], rl=p.rl)
     c.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
     ref = c.solve(p.x_base, p.target, p.base_row_mode, dis)
@@ -332,7 +332,7 @@ def test_bank_slots_and_states_left_on_the_device(jni):
     hb = _fn(jni, "ac_solver_gpu_BatchSolveNative_readBatchHandedBackSlots", _vp, 0)
     hb.argtypes = [_vp, _vp, _i64]
     assert np.array_equal(jvm.value(hb(jvm.env, None, ctx)), slots)
-    alone = native.BatchContext(native.Structure(p, ordering=native.PLAN_DENSE_FRONT), 10)
+    alone = native.BatchContext(native.Structure(p, ordering=native.PLAN_DEFAULT), 10)
     alone.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
     ref = alone.solve(p.x_base, p.target, p.base_row_mode, dis)
     assert np.array_equal(got, ref)

@@ -70,14 +70,15 @@ def test_bad_inputs_are_errors_not_crashes(engine_lib):
         native._check(native.load().olfgpu_structure_info(0, None, None))
 
 
-@pytest.mark.parametrize("plan", ["scaled", "deferred", "dense"])
+@pytest.mark.parametrize("plan", ["scaled", "deferred", "dense", "shallow"])
 def test_level_schedules_cover_every_block_once(engine_lib, plan):
     """The factorization levels hold every LU block exactly once with every block update, and the forward and
     backward solve levels every row (a dense-front plan leaves its front rows to the dense front's backward solve)."""
     from conftest import grid
     from olfgpu import native
     _, p = grid("grid2000")
-    flag = {"scaled": 0, "deferred": native.PLAN_DEFERRED_L, "dense": native.PLAN_DENSE_FRONT}[plan]
+    flag = {"scaled": 0, "deferred": native.PLAN_DEFERRED_L, "dense": native.PLAN_DENSE_FRONT,
+            "shallow": native.PLAN_DEFAULT}[plan]
     s = native.Structure(p, flag)
     f, ops, fw, bw = s.levels()
     assert f[0] == 0 and f[-1] == s.n_lu_blocks and np.all(np.diff(f) > 0)
@@ -85,7 +86,7 @@ def test_level_schedules_cover_every_block_once(engine_lib, plan):
     assert fw[0] == 0 and fw[-1] == s.n_bus and np.all(np.diff(fw) > 0)
     assert bw[0] == 0 and np.all(np.diff(bw) > 0)
     front = s.n_bus - int(bw[-1])
-    if plan == "dense":
+    if plan in ("dense", "shallow"):
         assert 4 <= front <= 32
     else:
         assert front == 0
@@ -103,6 +104,23 @@ def test_plan_variants_shorten_the_dependency_chain(engine_lib):
     assert deferred.factor_levels < scaled.factor_levels
     assert dense.factor_levels < scaled.factor_levels
     assert scaled.n_lu_blocks == deferred.n_lu_blocks == dense.n_lu_blocks
+
+
+@pytest.mark.parametrize("name", ["grid2000", "grid9241", "grid13659"])
+def test_shallow_ordering_shortens_the_chain_at_about_the_same_fill(engine_lib, name):
+    """Minimum degree relaxed toward a shallow elimination tree: fewer factorization and solve levels than plain
+    minimum degree (with and without the dense front), at most 5 % more LU blocks."""
+    from conftest import grid
+    from olfgpu import native
+    _, p = grid(name)
+    md, sh = native.Structure(p, native.MIN_DEGREE), native.Structure(p, native.MIN_DEGREE_SHALLOW)
+    dense, default = native.Structure(p, native.PLAN_DENSE_FRONT), native.Structure(p, native.PLAN_DEFAULT)
+    assert sh.factor_levels < 0.85 * md.factor_levels
+    assert default.factor_levels < 0.85 * dense.factor_levels
+    assert default.forward_levels < dense.forward_levels and default.backward_levels < dense.backward_levels
+    assert sh.n_lu_blocks <= 1.05 * md.n_lu_blocks
+    again = native.Structure(p, native.MIN_DEGREE_SHALLOW)       # the order is deterministic
+    assert all(np.array_equal(x, y) for x, y in zip(again.levels(), sh.levels()))
 
 
 @pytest.mark.parametrize("name", ["grid2000", "grid9241", "grid13659"])
