@@ -34,10 +34,10 @@ TOL = 1e-8
 CHECKPOINT = os.path.join(ROOT, "olf-gpu_b200", "checkpoints", "warmstart_grid9241.npz")
 # DRAM bytes (read + write) of one lane's factorization (narrow levels in shared memory), from ncu captures of the
 # launches of the first factorization of a 64-outage batch: the dense-front plan on plain minimum degree (89 launches;
-# FP64 490.9 MB, FP32 LU 288.3 MB over 64 lanes) and on the shallow-tree order (120 launches; 663.8 MB, 374.6 MB);
+# FP64 490.9 MB, FP32 LU 288.3 MB over 64 lanes) and on the shallow-tree order (123 launches; 573.2 MB, 328.6 MB);
 # scaled to a launch by the lanes it factorizes
 TRAFFIC = {("dense", "fp64"): 7.67e6, ("dense", "mixed"): 4.51e6,
-           ("shallow", "fp64"): 10.37e6, ("shallow", "mixed"): 5.85e6}
+           ("shallow", "fp64"): 8.96e6, ("shallow", "mixed"): 5.13e6}
 
 
 def _peaks():
@@ -804,7 +804,7 @@ def main():
     ap.add_argument("--plan", default=None, choices=["scaled", "deferred", "dense", "shallow"],
                     help="block-LU plan: L scaled at its task, deferred (half the levels), dense (minimum degree, the "
                          "trailing block factorized in shared memory) or shallow (dense, on minimum degree relaxed "
-                         "toward a shallow elimination tree: 123 instead of 201 levels on the 9,241-bus grid; the "
+                         "toward a shallow elimination tree: 121 instead of 201 levels on the 9,241-bus grid; the "
                          "default for the N-1 workload); the uneven workload's persistent launch runs the scaled plan")
     ap.add_argument("--schedule", default="auto", choices=["auto", "levels", "coop", "shared", "shared-all"],
                     help="auto: the engine's autotuner picks the Newton-iteration schedule on the first solve; "
