@@ -1049,7 +1049,7 @@ int oracle_linear_solve(oracle_solver *o, const double *vals, const double *b, d
 {
     const oracle_structure *s = o->s;
     glu *g = glu_new(s->n, s->row_ptr, s->col_idx, o->perm);
-    double *ax = (double *)malloc(sizeof(double) * (size_t)s->nnz);
+    double *ax = (double *)calloc((size_t)(s->nnz > 0 ? s->nnz : 1), sizeof(double));
     for (int k = 0; k < s->nnz; k++) ax[g->map[k]] = vals[k];
     int rc = glu_factor(g, ax);
     if (rc == 0) glu_solve(g, b, z);
