@@ -1,8 +1,9 @@
 """ORACLE -- test infrastructure only (the tests, the smoke check and the benchmark's CPU-baseline leg).
 
 ctypes wrapper over ``oracle/lib/liboracle.so`` (the C restatement of the reference path, ``olf_oracle.c``) and, when
-it was built here from the reference's own sources, ``oracle/_ref/libolfref.so`` (the reference's host structure code
-and generated formula headers).  Neither library is ever on the product path.
+they were built here from the reference's own sources (``oracle/ref/Makefile``), ``oracle/_ref/libolfref.so`` (the
+reference's host structure code and generated formula headers) and ``oracle/_ref/libolfreflu.so`` (the reference's
+host LU).  None of these libraries is ever on the product path.
 """
 from __future__ import annotations
 
@@ -16,6 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "lib", "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libolfref.so")
+REF_LU_LIB = os.path.join(HERE, "_ref", "libolfreflu.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -309,6 +311,140 @@ def ref_shunt(params, v):
     p = _arr(params, np.float64)
     ref_lib().olfref_shunt(_ptr(p), v, _ptr(o))
     return o
+
+
+_ref_lu = None
+
+
+def ref_lu_available() -> bool:
+    return os.path.exists(REF_LU_LIB)
+
+
+def ref_lu_lib():
+    global _ref_lu
+    if _ref_lu is None:
+        R = ctypes.CDLL(REF_LU_LIB)
+        R.olfref_lu_plan.restype = ctypes.c_void_p
+        R.olfref_lu_plan.argtypes = [ctypes.c_int, _ip, _ip, _ip, _ip, ctypes.c_char_p]
+        R.olfref_lu_free.argtypes = [ctypes.c_void_p]
+        R.olfref_lu_solve.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
+        _ref_lu = R
+    return _ref_lu
+
+
+class RefLu:
+    """The reference's own host LU on one CSR pattern: the fast engine's plan (scalar_lu_plan.cu) on its
+    minimum-degree order (minimum_degree.cu), factorized and solved by the one-lane ports of
+    native/host/lu_transposed_check.cpp:74-145 (static pivots; a clamped pivot or an oversized multiplier counts as
+    trouble)."""
+
+    def __init__(self, row_ptr, col_idx):
+        R = ref_lu_lib()
+        self.row_ptr = _arr(row_ptr, np.int32)
+        self.col_idx = _arr(col_idx, np.int32)
+        self.n = self.row_ptr.shape[0] - 1
+        nnz_lu, levels = ctypes.c_int(0), ctypes.c_int(0)
+        err = ctypes.create_string_buffer(256)
+        self.h = R.olfref_lu_plan(self.n, _ptr(self.row_ptr), _ptr(self.col_idx), ctypes.byref(nnz_lu),
+                                  ctypes.byref(levels), err)
+        if not self.h:
+            raise RuntimeError("reference LU plan: " + err.value.decode())
+        self.nnz_lu, self.levels = nnz_lu.value, levels.value
+
+    def solve(self, vals, b):
+        """(x, trouble) with A x = b; A by its CSR values in the pattern's order."""
+        x = np.zeros(self.n)
+        vals, b = _arr(vals, np.float64), _arr(b, np.float64)
+        trouble = ref_lu_lib().olfref_lu_solve(self.h, _ptr(vals), _ptr(b), _ptr(x))
+        if trouble < 0:
+            raise RuntimeError("reference LU: solve failed")
+        return x, trouble
+
+    def __del__(self):
+        try:
+            if self.h:
+                ref_lu_lib().olfref_lu_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def ref_component_fill(packed, ref_struct, x, target, mode, disabled=None):
+    """J values and F of one scenario assembled from the reference's OWN components only: its generated formula
+    headers per element (``ref_closed_branch`` / ``ref_open_branch`` / ``ref_shunt``) scattered through its own
+    role-folded destinations (``ref_structure``: a J slot >= 0, an F row as -2 - row, -1 skipped), F starting at
+    -target, an outaged element skipped, and FIXED_VARIABLE rows (mode 0) replaced by the identity row with
+    F = x - target (fill_launch.cu:82-126).  Elements in packing order, outputs in table order."""
+    p = packed
+    rp, dp = ref_struct["row_ptr"], ref_struct["diag_pos"]
+    vals = np.zeros(rp[-1])
+    F = -np.asarray(target, dtype=np.float64).copy()
+
+    def scatter(out, dest):
+        for k, d in enumerate(dest):
+            if d >= 0:
+                vals[d] += out[k]
+            elif d <= -2:
+                F[-2 - d] += out[k]
+
+    for e in range(p.n_cb):
+        if disabled is not None and disabled[e]:
+            continue
+        par, q = p.cb_params[e], p.cb_idx[e]
+        r1 = x[q[9]] if q[9] >= 0 else par[6]
+        a1 = x[q[8]] if q[8] >= 0 else par[7]
+        scatter(ref_closed_branch(par, x[q[5]], r1, x[q[7]], a1, x[q[4]], x[q[6]]),
+                ref_struct["cb_dest"][e * 28:(e + 1) * 28])
+    for e in range(p.n_ob):
+        if disabled is not None and disabled[p.n_cb + e]:
+            continue
+        par, q = p.ob_params[e], p.ob_idx[e]
+        v1 = x[q[4]] if q[4] >= 0 else 1.0
+        v2 = x[q[5]] if q[5] >= 0 else 1.0
+        scatter(ref_open_branch(par, v1, v2), ref_struct["ob_dest"][e * 8:(e + 1) * 8])
+    for e in range(p.n_sh):
+        if disabled is not None and disabled[p.n_cb + p.n_ob + e]:
+            continue
+        par, q = p.sh_params[e], p.sh_idx[e]
+        scatter(ref_shunt(par, x[q[2]]), ref_struct["sh_dest"][e * 5:(e + 1) * 5])
+    for r in np.flatnonzero(np.asarray(mode) == 0):
+        vals[rp[r]:rp[r + 1]] = 0.0
+        vals[dp[r]] = 1.0
+        F[r] = x[r] - target[r]
+    return vals, F
+
+
+def newton_with(fill, solve, x0, max_iter=15, tol=1e-8):
+    """One plain Newton-Raphson solve (no outer loops) over a given fill ``fill(x) -> (vals, F)`` and linear solver
+    ``solve(vals, rhs) -> dx``, under the rules of newton_iteration.cu:276-397 as the oracle's ``newton()`` states them:
+    at least one iteration; converged when max |F| < tol before the budget; a non-finite mismatch is DIVERGED; the
+    budget spent is MAX_ITERATION_REACHED; a failed factorization is LINEAR_SOLVE_FAILED (the linear-solve guard and
+    the bad-last-solve reject are left out: they never act on a scenario that converges).  Returns [x(n), iterations,
+    ||F||inf, status] with the oracle's status codes, the row layout of ``Structure.solve_batch``.  With the
+    reference's own formulas, scatter map and host LU plugged in, it is the trajectory the tests pin the oracle
+    against."""
+    converged, max_iter_reached, diverged, linear_solve_failed = 0, 1, -1, -3
+    x = np.array(x0, dtype=np.float64, copy=True)
+    status, it, nrm = linear_solve_failed, 0, float("nan")
+    for it in range(max_iter + 1):
+        vals, F = fill(x)
+        if not np.all(np.isfinite(F)):
+            nrm, status = float("nan"), diverged
+            break
+        nrm = float(np.max(np.abs(F)))
+        if it > 0 and nrm < tol and it < max_iter:
+            status = converged
+            break
+        if it == max_iter:
+            status = max_iter_reached
+            break
+        try:
+            dx = solve(vals, -F)
+        except RuntimeError:
+            status = linear_solve_failed
+            break
+        x += dx
+    return np.concatenate([x, [it, nrm, status]])
 
 
 # ---------------------------------------------------------------------------------------------------------------

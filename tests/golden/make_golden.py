@@ -7,6 +7,13 @@
   structure_<grid>.npz   the packed arrays of a synthetic grid and the reference's own row map, CSR pattern, diagonal
                          slots and role-folded scatter map for them (native/cuda/structure/csr_pattern.cu and the
                          structure_build.cuh templates, compiled into oracle/_ref).
+  newton_<grid>.npz      Newton-Raphson solves of a synthetic grid's base case (flat start) and of seeded N-1 outages
+                         (base-case start) assembled only from the reference's own components: its generated formula
+                         headers, its row map / pattern / scatter map, and its host LU (the fast engine's plan on its
+                         minimum-degree order with the one-lane factorization and solve of
+                         native/host/lu_transposed_check.cpp, compiled into oracle/_ref/libolfreflu.so), under the
+                         Newton rules of newton_iteration.cu:276-397; plus linear systems J x = b at perturbed states
+                         solved by that LU.
 
 Usage:  python tests/golden/make_golden.py [/root/reference]
 """
@@ -109,6 +116,42 @@ def structures():
                             sh_idx=p.sh_idx, **{"ref_" + k: v for k, v in ref.items()})
 
 
+NEWTON_OUTAGES = 24
+
+
+def newton_fixtures():
+    """newton_<grid>.npz: the packed arrays, each scenario's start and outage mask, the reference-component Newton rows
+    [x(n), iterations, ||F||inf, status], and three linear systems with the reference LU's solutions."""
+    for name in ("grid118", "grid300"):
+        g = synthetic.build(name)
+        p = packing.pack(g)
+        rs = O.ref_structure(p)
+        lu = O.RefLu(rs["row_ptr"], rs["col_idx"])
+        outs = synthetic.draw_outages(g, NEWTON_OUTAGES, seed=20261203)
+        dis = np.concatenate([np.zeros((1, p.n_elements), np.uint8), p.outage_masks(outs)])
+        x0 = np.tile(p.x_base, (dis.shape[0], 1))
+        x0[0] = p.x_flat                                 # the base case from a flat start, then the N-1 outages
+        rows = np.stack([O.newton_with(
+            lambda x, k=k: O.ref_component_fill(p, rs, x, p.target, p.base_row_mode, dis[k]),
+            lambda v, b: lu.solve(v, b)[0], x0[k]) for k in range(dis.shape[0])])
+        rng = np.random.default_rng(7)
+        lin_vals, lin_b, lin_x, lin_trouble = [], [], [], []
+        for _ in range(3):
+            x = p.x_base.copy()
+            x[0::2] += rng.uniform(-0.02, 0.02, p.n_bus)
+            x[1::2] += rng.uniform(-0.02, 0.02, p.n_bus)
+            vals, _F = O.ref_component_fill(p, rs, x, p.target, p.base_row_mode)
+            b = rng.standard_normal(p.n)
+            xr, trouble = lu.solve(vals, b)
+            lin_vals.append(vals), lin_b.append(b), lin_x.append(xr), lin_trouble.append(trouble)
+        np.savez_compressed(os.path.join(HERE, f"newton_{name}.npz"), n=p.n, cb_params=p.cb_params, cb_idx=p.cb_idx,
+                            ob_params=p.ob_params, ob_idx=p.ob_idx, sh_params=p.sh_params, sh_idx=p.sh_idx,
+                            identity_rows=p.identity_rows, target=p.target, base_row_mode=p.base_row_mode,
+                            row_ptr=rs["row_ptr"], col_idx=rs["col_idx"], x0=x0, disabled=dis, ref_rows=rows,
+                            lin_vals=np.array(lin_vals), lin_b=np.array(lin_b), lin_x=np.array(lin_x),
+                            lin_trouble=np.array(lin_trouble), ref_nnz_lu=lu.nnz_lu, ref_levels=lu.levels)
+
+
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else O.reference_root()
     if not ref:
@@ -116,4 +159,5 @@ if __name__ == "__main__":
     O.build(ref)
     formulas(ref)
     structures()
+    newton_fixtures()
     print("fixtures written to", HERE)

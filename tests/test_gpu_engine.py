@@ -94,6 +94,31 @@ def test_n1_fp64_matches_oracle(engine_lib, oracle_mod, name, count):
     assert np.array_equal(r.iterations[status == 0], ref[status == 0, p.n].astype(int))
 
 
+@pytest.mark.parametrize("name", ["grid118", "grid300"])
+def test_engine_matches_reference_component_newton(engine_lib, name):
+    """The engine against the committed Newton solves made only of the reference's own code (tests/golden/
+    newton_<grid>.npz: its generated formulas, its scatter map, its host LU), with no oracle in between: the base case
+    from a flat start as a batch of one, and 24 N-1 outages from the base-case start as one batch."""
+    import os
+    from olfgpu import native
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", f"newton_{name}.npz"))
+    g, p = grid(name)
+    for k in ("cb_params", "cb_idx", "ob_params", "ob_idx", "sh_params", "sh_idx", "target", "base_row_mode"):
+        assert np.array_equal(getattr(p, k), d[k]), f"the synthetic grid no longer matches the fixture ({k})"
+    s = native.Structure(p)
+    ref = d["ref_rows"]
+    dis = d["disabled"]
+    base = native.BatchContext(s, 1)
+    base.set_linear_solver_settings(native.FP64, 1)
+    out0 = base.solve(d["x0"][0], p.target, p.base_row_mode, dis[:1])
+    n1 = native.BatchContext(s, dis.shape[0] - 1)
+    n1.set_linear_solver_settings(native.FP64, 1)
+    out1 = n1.solve(p.x_base, p.target, p.base_row_mode, dis[1:])
+    out = np.concatenate([out0, out1])
+    _compare(out, ref, p.n)
+    assert np.array_equal(out[:, p.n], ref[:, p.n]), "iteration counts differ"
+
+
 def test_n1_9241_subset_matches_oracle(engine_lib, oracle_mod):
     from olfgpu import native, synthetic
     from olfgpu.security_analysis import SecurityAnalysis

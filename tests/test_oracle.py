@@ -80,3 +80,76 @@ def test_oracle_status_rules(oracle_mod):
     t[2 * int(np.flatnonzero(p.base_row_mode == 1)[0])] = np.nan
     nan = st.solve_batch(p.x_flat, flat, target=t)
     assert nan[0, -1] == -1
+
+
+class _PN(_P):
+    """Packed arrays, targets and row modes loaded from a Newton fixture."""
+
+    def __init__(self, d):
+        super().__init__(d)
+        self.identity_rows = d["identity_rows"]
+        self.target, self.base_row_mode = d["target"], d["base_row_mode"]
+
+
+# the oracle's solve against Newton solves made of the reference's own formula headers, scatter map and host LU: the
+# two factorizations round differently (partial pivoting vs static pivots on another order), nothing else differs
+NEWTON_STATE_TOL = 1e-12
+LU_REL_TOL = 1e-11
+
+
+@pytest.mark.parametrize("name", ["grid118", "grid300"])
+def test_oracle_newton_matches_reference_components(oracle_mod, name):
+    """newton_<grid>.npz (tests/golden/make_golden.py): the base case from a flat start and 24 N-1 outages from the
+    base-case start, each solved by a Newton loop whose fill is the reference's generated formulas scattered through
+    its own scatter map and whose linear solve is its own host LU (native/host/lu_transposed_check.cpp:74-145 on the
+    plan of scalar_lu_plan.cu).  The oracle must take the same iterations to the same status and state."""
+    d = np.load(os.path.join(GOLD, f"newton_{name}.npz"))
+    p = _PN(d)
+    st = oracle_mod.Structure(p)
+    a = st.export()
+    assert np.array_equal(a["row_ptr"], d["row_ptr"]) and np.array_equal(a["col_idx"], d["col_idx"])
+    ref = d["ref_rows"]
+    out = st.solve_batch(d["x0"], d["disabled"])
+    n = p.n
+    assert np.array_equal(out[:, n + 2], ref[:, n + 2]), "statuses differ"
+    assert np.array_equal(out[:, n], ref[:, n]), "iteration counts differ"
+    conv = ref[:, n + 2] == 0
+    assert conv.all()
+    assert np.max(np.abs(out[conv, :n] - ref[conv, :n])) <= NEWTON_STATE_TOL
+
+
+@pytest.mark.parametrize("name", ["grid118", "grid300"])
+def test_oracle_linear_solve_matches_reference_host_lu(oracle_mod, name):
+    """Jacobians at perturbed states solved by the reference's host LU (newton_<grid>.npz) against the oracle's."""
+    d = np.load(os.path.join(GOLD, f"newton_{name}.npz"))
+    st = oracle_mod.Structure(_PN(d))
+    assert not d["lin_trouble"].any(), "the reference's fast engine trusts these systems"
+    for vals, b, xr in zip(d["lin_vals"], d["lin_b"], d["lin_x"]):
+        x = st.linear_solve(vals, b)
+        assert np.max(np.abs(x - xr)) / np.max(np.abs(xr)) <= LU_REL_TOL
+
+
+def test_reference_components_live_grid2000(oracle_mod):
+    """Where the reference sources are present (oracle/_ref built from them): the same pin, live, on the 2,000-bus
+    grid (its fill, LU and Newton), beyond the committed fixtures' sizes."""
+    if not (oracle_mod.ref_available() and oracle_mod.ref_lu_available()):
+        pytest.skip("oracle/_ref not built: no reference tree here")
+    from conftest import grid
+    from olfgpu import synthetic
+    g, p = grid("grid2000")
+    st = oracle_mod.Structure(p)
+    rs = oracle_mod.ref_structure(p)
+    lu = oracle_mod.RefLu(rs["row_ptr"], rs["col_idx"])
+    outs = synthetic.draw_outages(g, 4, seed=2000)
+    dis = p.outage_masks(outs)
+    vo, Fo = st.fill(p.x_base, p.target, p.base_row_mode, dis[0])
+    vr, Fr = oracle_mod.ref_component_fill(p, rs, p.x_base, p.target, p.base_row_mode, dis[0])
+    assert np.array_equal(vo, vr) and np.array_equal(Fo, Fr)
+    out = st.solve_batch(p.x_base, dis)
+    for k in range(dis.shape[0]):
+        r = oracle_mod.newton_with(
+            lambda x: oracle_mod.ref_component_fill(p, rs, x, p.target, p.base_row_mode, dis[k]),
+            lambda v, b: lu.solve(v, b)[0], p.x_base)
+        assert r[p.n + 2] == out[k, p.n + 2] == 0
+        assert r[p.n] == out[k, p.n]
+        assert np.max(np.abs(r[:p.n] - out[k, :p.n])) <= NEWTON_STATE_TOL
