@@ -173,6 +173,15 @@ int olfgpu_set_states_to_host(int64_t context, int statesToHost);
 int olfgpu_states_to_host(int64_t context, int* statesToHost);
 int olfgpu_read_batch_states(int64_t context, int nSlots, const int* slots, double* out);
 
+/* BatchReadbackNative.readBatchTargets / readBatchRowModes (batch_readback_jni.cu:13-45; read by
+ * GpuNewtonRaphson.java:194,227 and GpuBatchChunkSolver.java:1183): the per-scenario targets and row modes of chosen
+ * bank slots ([nSlots][n], slot order) as the last solve ended with them.  The outer loops rewrite both: a PV bus that
+ * the reactive-limit loop switched to PQ has its voltage row's mode and target (its Q limit less its load) changed,
+ * and the distributed slack moves its participants' P targets, so a converged state solves these equations, not the
+ * installed ones.  Row modes use the codes the solve takes (baseRowMode). */
+int olfgpu_read_batch_targets(int64_t context, int nSlots, const int* slots, double* out);
+int olfgpu_read_batch_row_modes(int64_t context, int nSlots, const int* slots, int* out);
+
 /* DriverNative.setBatchOuterLoops (driver_jni.cu:11-18): the distributed-slack and reactive-limit outer loops on or off
  * for the following solves (each acts only where the context holds its tables). */
 int olfgpu_set_outer_loops(int64_t context, int distributedSlack, int reactiveLimits);

@@ -730,6 +730,44 @@ extern "C" int olfgpu_read_batch_states(int64_t context, int nSlots, const int* 
     });
 }
 
+namespace {
+
+// Rows [nSlots][n] of chosen bank slots out of a lane-interleaved per-row device array ([n][S] of T), after the
+// context's stream has drained.
+template <typename T, typename U>
+void readSlotRows(BatchContext& c, const void* device, int nSlots, const int* slots, U* out) {
+    const int n = c.net->host.n;
+    if (nSlots < 0 || (nSlots > 0 && (!slots || !out))) throw std::runtime_error("bad slot list or output");
+    for (int j = 0; j < nSlots; j++) {
+        if (slots[j] < 0 || slots[j] >= c.nS) throw std::runtime_error("slot outside the bank");
+    }
+    OLF_CUDA(cudaSetDevice(c.device));
+    OLF_CUDA(cudaStreamSynchronize(c.stream));
+    std::vector<T> col(static_cast<size_t>(n) * c.S);
+    OLF_CUDA(cudaMemcpy(col.data(), device, col.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    for (int j = 0; j < nSlots; j++) {
+        for (int r = 0; r < n; r++) {
+            out[static_cast<size_t>(j) * n + r] = static_cast<U>(col[static_cast<size_t>(r) * c.S + slots[j]]);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" int olfgpu_read_batch_targets(int64_t context, int nSlots, const int* slots, double* out) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        readSlotRows<double>(c, c.target.p, nSlots, slots, out);
+    });
+}
+
+extern "C" int olfgpu_read_batch_row_modes(int64_t context, int nSlots, const int* slots, int* out) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        readSlotRows<int8_t>(c, c.mode.p, nSlots, slots, out);
+    });
+}
+
 extern "C" int olfgpu_set_outer_loops(int64_t context, int distributedSlack, int reactiveLimits) {
     return guarded([&] {
         BatchContext& c = contextOf(context);

@@ -384,7 +384,7 @@ JNIEXPORT void JNICALL OLF_JNI(ac_outerloop_gpu, ReactiveLimitsNative, setBatchR
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// DriverNative (driver_jni.cu:11-18), BatchReadbackNative (batch_readback_jni.cu:103-118)
+// DriverNative (driver_jni.cu:11-18), BatchReadbackNative (batch_readback_jni.cu:13-45, 103-118)
 // ---------------------------------------------------------------------------------------------------------------
 JNIEXPORT void JNICALL OLF_JNI(ac_solver_gpu, DriverNative, setBatchOuterLoops)(JNIEnv* env, jclass, jlong handle,
                                                                               jboolean distributedSlackOuterLoop,
@@ -406,6 +406,62 @@ JNIEXPORT jlong JNICALL OLF_JNI(ac_solver_gpu, BatchReadbackNative, readBatchSol
     int64_t count = 0;
     return handle && olfgpu_context_info(handle, nullptr, nullptr, nullptr, nullptr, nullptr, &count) == 0 ? count
                                                                                                           : -1;
+}
+
+}  // extern "C"
+
+namespace {
+
+// The bank slots whose rows the per-scenario readbacks return, in row order: the last solve's (its handed-back
+// slots), or the whole bank before any solve (batch_readback_jni.cu reads the installed slots the same way).  n
+// receives the row width.  False (a Java exception pending) on a failure.
+bool readbackSlots(JNIEnv* env, jlong handle, const char* what, std::vector<int>& slots, int& n) {
+    int count = 0, nS = 0;
+    if (!ok(env, olfgpu_context_info(handle, &n, nullptr, &nS, nullptr, nullptr, nullptr), what)) return false;
+    if (!ok(env, olfgpu_read_handed_back_slots(handle, nullptr, 0, &count), what)) return false;
+    if (count == 0) {
+        slots.resize(nS);
+        for (int j = 0; j < nS; j++) slots[j] = j;
+        return true;
+    }
+    slots.resize(count);
+    return ok(env, olfgpu_read_handed_back_slots(handle, slots.data(), count, &count), what);
+}
+
+}  // namespace
+
+extern "C" {
+
+// BatchReadbackNative.readBatchTargets (batch_readback_jni.cu:13-24): [slots x n] targets as the last solve ended.
+JNIEXPORT jdoubleArray JNICALL OLF_JNI(ac_solver_gpu, BatchReadbackNative, readBatchTargets)(JNIEnv* env, jclass,
+                                                                                           jlong handle) {
+    if (!handle) return nullptr;
+    std::vector<int> slots;
+    int n = 0;
+    if (!readbackSlots(env, handle, "readBatchTargets", slots, n)) return nullptr;
+    std::vector<double> host(slots.size() * static_cast<size_t>(n));
+    if (!ok(env, olfgpu_read_batch_targets(handle, len(slots), ptr(slots), host.data()), "readBatchTargets")) {
+        return nullptr;
+    }
+    jdoubleArray out = olfjni_NewDoubleArray(env, static_cast<jsize>(host.size()));
+    if (out && !host.empty()) olfjni_SetDoubleArrayRegion(env, out, 0, static_cast<jsize>(host.size()), host.data());
+    return out;
+}
+
+// BatchReadbackNative.readBatchRowModes (batch_readback_jni.cu:26-45): [slots x n] row modes as the last solve ended.
+JNIEXPORT jintArray JNICALL OLF_JNI(ac_solver_gpu, BatchReadbackNative, readBatchRowModes)(JNIEnv* env, jclass,
+                                                                                         jlong handle) {
+    if (!handle) return nullptr;
+    std::vector<int> slots;
+    int n = 0;
+    if (!readbackSlots(env, handle, "readBatchRowModes", slots, n)) return nullptr;
+    std::vector<int> host(slots.size() * static_cast<size_t>(n));
+    if (!ok(env, olfgpu_read_batch_row_modes(handle, len(slots), ptr(slots), host.data()), "readBatchRowModes")) {
+        return nullptr;
+    }
+    jintArray out = olfjni_NewIntArray(env, static_cast<jsize>(host.size()));
+    if (out && !host.empty()) olfjni_SetIntArrayRegion(env, out, 0, static_cast<jsize>(host.size()), host.data());
+    return out;
 }
 
 }  // extern "C"

@@ -46,7 +46,7 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_states_to_host", "olfgpu_read_batch_states", "olfgpu_set_outer_loops", "olfgpu_context_info",
            "olfgpu_linear_solve_transposed", "olfgpu_screen_violations", "olfgpu_last_slack_distribution_failures",
            "olfgpu_set_start_polish", "olfgpu_set_mixed_precision_policy", "olfgpu_last_fp64_iterations",
-           "olfgpu_set_device_loop"]
+           "olfgpu_set_device_loop", "olfgpu_read_batch_targets", "olfgpu_read_batch_row_modes"]
 # The arrays of BatchSolveNative.solveBatchContext this engine rejects when non-empty, in the reference's order
 UNSUPPORTED_SOLVE_ARRAYS = [
     "distributedSlackOverrideBus", "distributedSlackOverrideFactorDelta", "distributedSlackOverrideBaseTargetPDelta",
@@ -126,6 +126,8 @@ def load(path: str = LIB_PATH):
     L.olfgpu_screen_violations.argtypes = [_i64, _ci, _ip, _ip, _ip, _ip, _ip, _dp, _ci, _ip, _dp, _dp, _ci, _cd, _cd,
                                            _cd, _ci, _ip, _ip]
     L.olfgpu_read_batch_states.argtypes = [_i64, _ci, _ip, _dp]
+    L.olfgpu_read_batch_targets.argtypes = [_i64, _ci, _ip, _dp]
+    L.olfgpu_read_batch_row_modes.argtypes = [_i64, _ci, _ip, _ip]
     L.olfgpu_begin_batch_install.argtypes = [_i64, _ip, _ci]
     L.olfgpu_read_handed_back_slots.argtypes = [_i64, _ip, _ci, _ip]
     L.olfgpu_set_states_to_host.argtypes = [_i64, _ci]
@@ -396,6 +398,21 @@ class BatchContext:
         out = np.zeros(self.n_scenarios, np.uint8)
         cnt = ctypes.c_int(0)
         _check(load().olfgpu_last_slack_distribution_failures(self.handle, _p(out), ctypes.byref(cnt)))
+        return out
+
+    def read_targets(self, slots=None) -> np.ndarray:
+        """BatchReadbackNative.readBatchTargets: [slots][n] targets as the last solve ended with them (default: the
+        whole bank)."""
+        slots = _c(np.arange(self.n_scenarios) if slots is None else slots, np.int32)
+        out = np.zeros((slots.size, self.structure.n))
+        _check(load().olfgpu_read_batch_targets(self.handle, int(slots.size), _p(slots), _p(out)))
+        return out
+
+    def read_row_modes(self, slots=None) -> np.ndarray:
+        """BatchReadbackNative.readBatchRowModes: [slots][n] row modes as the last solve ended with them."""
+        slots = _c(np.arange(self.n_scenarios) if slots is None else slots, np.int32)
+        out = np.zeros((slots.size, self.structure.n), np.int32)
+        _check(load().olfgpu_read_batch_row_modes(self.handle, int(slots.size), _p(slots), _p(out)))
         return out
 
     def set_outer_loops(self, distributed_slack: bool = True, reactive_limits: bool = True):

@@ -953,10 +953,15 @@ static int distributed_slack_check(const oracle_ds *ds, const double *factor, co
  * out: per scenario [x(n), iterations, ||F||inf, status] (batch_solve_jni.cu:308-337).
  * Reactive limits: rl may be NULL; max_outer bounds the Newton restarts.  Returns 0.
  */
-int oracle_solve_batch_ds(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
-                          const int *mode_base, const unsigned char *disabled, int n_elements, int max_iter, double tol,
-                          const oracle_rl *rl, double rl_tol, int max_outer, int max_switch, int threads,
-                          const oracle_opts *opts, const oracle_ds *ds, double *out)
+/* The batched solve with the outer loops; final_target / final_mode ([ns][n], each may be NULL) receive every
+ * scenario's targets and row modes as its solve ended with them (the outer loops rewrite both: reactive_limits.cu
+ * switches PV rows to PQ at a Q limit, the distributed slack moves its participants' P targets), the per-scenario
+ * readbacks of batch_readback_jni.cu:13-45. */
+int oracle_solve_batch_final(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
+                             const int *mode_base, const unsigned char *disabled, int n_elements, int max_iter,
+                             double tol, const oracle_rl *rl, double rl_tol, int max_outer, int max_switch, int threads,
+                             const oracle_opts *opts, const oracle_ds *ds, double *out, double *final_target,
+                             int *final_mode)
 {
     const oracle_structure *s = o->s;
     const int n = s->n;
@@ -1018,6 +1023,8 @@ int oracle_solve_batch_ds(oracle_solver *o, int ns, const double *x0, int x0_str
             x[n] = (double)iters;   /* the last inner solve's iterations (res.iters, newton_iteration.cu:338) */
             x[n + 1] = nrm;
             x[n + 2] = (double)status;
+            if (final_target) memcpy(final_target + (size_t)sc_i * n, target, sizeof(double) * (size_t)n);
+            if (final_mode) memcpy(final_mode + (size_t)sc_i * n, mode, sizeof(int) * (size_t)n);
         }
         glu_free(g);
         free(vals); free(ax); free(F); free(dx); free(qbuf); free(target); free(mode);
@@ -1025,6 +1032,15 @@ int oracle_solve_batch_ds(oracle_solver *o, int ns, const double *x0, int x0_str
     }
     free(dsf);
     return 0;
+}
+
+int oracle_solve_batch_ds(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
+                          const int *mode_base, const unsigned char *disabled, int n_elements, int max_iter, double tol,
+                          const oracle_rl *rl, double rl_tol, int max_outer, int max_switch, int threads,
+                          const oracle_opts *opts, const oracle_ds *ds, double *out)
+{
+    return oracle_solve_batch_final(o, ns, x0, x0_stride, target_base, mode_base, disabled, n_elements, max_iter, tol,
+                                    rl, rl_tol, max_outer, max_switch, threads, opts, ds, out, NULL, NULL);
 }
 
 int oracle_solve_batch_ex(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,

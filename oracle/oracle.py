@@ -82,6 +82,7 @@ def lib():
                                          ctypes.c_int, ctypes.c_int, _dp]
         L.oracle_solve_batch_ex.argtypes = L.oracle_solve_batch.argtypes[:-1] + [ctypes.c_void_p, _dp]
         L.oracle_solve_batch_ds.argtypes = L.oracle_solve_batch.argtypes[:-1] + [ctypes.c_void_p, ctypes.c_void_p, _dp]
+        L.oracle_solve_batch_final.argtypes = L.oracle_solve_batch_ds.argtypes + [_dp, _ip]
         L.oracle_linear_solve.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
         L.oracle_linear_solve_transposed.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
         L.oracle_closed_branch.argtypes = [_dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -180,11 +181,13 @@ class Structure:
     def solve_batch(self, x0, disabled, max_iter=15, tol=1e-8, target=None, mode=None, reactive_limits=False,
                     rl_tol=1e-4, max_outer=20, max_switch=3, threads=0, conv_eps_per_eq=0.0, svs_mode=0,
                     max_dv=0.1, max_dphi=0.17453292519943295, var_type=None, v_check=None, min_v=0.0, max_v=0.0,
-                    distributed_slack=None, slack_dist_tol=1e-6, reject_slack_distribution_failure=False):
+                    distributed_slack=None, slack_dist_tol=1e-6, reject_slack_distribution_failure=False,
+                    final_equations=False):
         """Per scenario [x(n), iterations, ||F||inf, status]; x0 is [n] (shared) or [nS, n].  conv_eps_per_eq > 0:
         OLF's 2-norm stopping test; svs_mode 2: MAX_VOLTAGE_CHANGE with var_type [n]; v_check [n]: the realistic-voltage
         rows checked against [min_v, max_v] at convergence; distributed_slack (packing.DistributedSlack): the bus-level
-        distributed-slack outer loop, before the reactive-limit check."""
+        distributed-slack outer loop, before the reactive-limit check.  final_equations: also return each scenario's
+        targets and row modes as its solve ended with them ([nS][n] each), as (rows, targets, modes)."""
         p = self.p
         disabled = _arr(disabled, np.uint8)
         ns = disabled.shape[0]
@@ -215,13 +218,18 @@ class Structure:
             ds_struct = _Ds(k[0].shape[0], _ptr(k[0]), _ptr(k[1]), _ptr(k[2]), _ptr(k[3]), _ptr(k[4]),
                             int(d.slack_row), float(d.slack_target_p), slack_dist_tol,
                             1 if reject_slack_distribution_failure else 0)
-        lib().oracle_solve_batch_ds(self.solver, ns, _ptr(x0), stride, _ptr(target), _ptr(mode), _ptr(disabled),
-                                    disabled.shape[1], max_iter, tol,
-                                    ctypes.cast(ctypes.pointer(rl_struct), ctypes.c_void_p) if rl_struct else None,
-                                    rl_tol, max_outer, max_switch, threads,
-                                    ctypes.cast(ctypes.pointer(opts), ctypes.c_void_p),
-                                    ctypes.cast(ctypes.pointer(ds_struct), ctypes.c_void_p) if ds_struct else None,
-                                    _ptr(out))
+        final_target = np.zeros((ns, p.n)) if final_equations else None
+        final_mode = np.zeros((ns, p.n), np.int32) if final_equations else None
+        lib().oracle_solve_batch_final(self.solver, ns, _ptr(x0), stride, _ptr(target), _ptr(mode), _ptr(disabled),
+                                       disabled.shape[1], max_iter, tol,
+                                       ctypes.cast(ctypes.pointer(rl_struct), ctypes.c_void_p) if rl_struct else None,
+                                       rl_tol, max_outer, max_switch, threads,
+                                       ctypes.cast(ctypes.pointer(opts), ctypes.c_void_p),
+                                       ctypes.cast(ctypes.pointer(ds_struct), ctypes.c_void_p) if ds_struct else None,
+                                       _ptr(out), None if final_target is None else _ptr(final_target),
+                                       None if final_mode is None else _ptr(final_mode))
+        if final_equations:
+            return out, final_target, final_mode
         return out
 
 

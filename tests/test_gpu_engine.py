@@ -250,6 +250,36 @@ def test_reactive_limits_match_oracle(engine_lib, oracle_mod):
     assert np.max(np.abs(plain[:, :p.n] - ref[:, :p.n])) > 1e-4
 
 
+def test_final_targets_and_row_modes_match_oracle(engine_lib, oracle_mod):
+    """BatchReadbackNative.readBatchTargets / readBatchRowModes: after a solve with the reactive-limit outer loop, the
+    targets and row modes each converged scenario ended with equal the oracle's (its PV rows switched to PQ at a Q
+    limit), every changed row is a reactive-limit voltage row, and a chosen slot list comes back in its order."""
+    from olfgpu import native, synthetic
+    g, p = grid("grid300")
+    outs = synthetic.draw_outages(g, 40, seed=303)
+    dis = p.outage_masks(outs)
+    s = native.Structure(p)
+    ctx = native.BatchContext(s, outs.shape[0], rl=p.rl)
+    res = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
+    ref, tg, md = oracle_mod.Structure(p).solve_batch(p.x_base, dis, reactive_limits=True, final_equations=True)
+    _compare(res, ref, p.n)
+    targets, modes = ctx.read_targets(), ctx.read_row_modes()
+    conv = ref[:, p.n + 2] == 0
+    assert np.array_equal(modes[conv], md[conv])
+    assert np.max(np.abs(targets[conv] - tg[conv])) <= 1e-12
+    changed = (modes != p.base_row_mode) | (targets != p.target)
+    assert changed.any(), "the limits bind"
+    assert set(np.flatnonzero(changed.any(axis=0)).tolist()) <= set(p.rl.voltage_row.tolist())
+    slots = np.array([5, 0, 17], np.int32)
+    assert np.array_equal(ctx.read_row_modes(slots), modes[slots])
+    assert np.array_equal(ctx.read_targets(slots), targets[slots])
+    # without the outer loop the installed equations come back unchanged
+    ctx.set_outer_loops(reactive_limits=False)
+    ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
+    assert np.array_equal(ctx.read_row_modes(), np.tile(p.base_row_mode, (outs.shape[0], 1)))
+    assert np.array_equal(ctx.read_targets(), np.tile(p.target, (outs.shape[0], 1)))
+
+
 @pytest.mark.parametrize("schedule,lanes,threads", [(0, 0, 256), (0, 1, 256), (0, 2, 256), (0, 4, 256), (1, 1, 256),
                                                     (1, 2, 512), (1, 4, 512), (1, 8, 256), (2, 0, 512),
                                                     (3, 0, 512), (3, 2, 512), (4, 0, 256), (5, 0, 256)])

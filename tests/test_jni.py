@@ -32,6 +32,8 @@ HOT_SET = [
     "ac_solver_gpu_DriverNative_setBatchOuterLoops",
     "ac_solver_gpu_BatchReadbackNative_readBatchNewtonLoopIterations",
     "ac_solver_gpu_BatchReadbackNative_readBatchSolveCount",
+    "ac_solver_gpu_BatchReadbackNative_readBatchTargets",
+    "ac_solver_gpu_BatchReadbackNative_readBatchRowModes",
 ]
 
 _vp, _i32, _i64, _f64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
@@ -302,6 +304,18 @@ def test_solve_through_jni_equals_the_c_abi(jni):
     cnt = _fn(jni, "ac_solver_gpu_BatchReadbackNative_readBatchSolveCount", _i64, 0)
     cnt.argtypes = [_vp, _vp, _i64]
     assert cnt(jvm.env, None, ctx) == 1
+    # the per-scenario targets and row modes as the solve ended (the reactive-limit loop rewrote some), [scenarios x n]
+    tg = _fn(jni, "ac_solver_gpu_BatchReadbackNative_readBatchTargets", _vp, 0)
+    tg.argtypes = [_vp, _vp, _i64]
+    rm = _fn(jni, "ac_solver_gpu_BatchReadbackNative_readBatchRowModes", _vp, 0)
+    rm.argtypes = [_vp, _vp, _i64]
+    targets = jvm.value(tg(jvm.env, None, ctx))
+    modes = jvm.value(rm(jvm.env, None, ctx))
+    assert jvm.take_exception() is None
+    assert np.array_equal(targets.reshape(outs.shape[0], p.n), c.read_targets())
+    assert np.array_equal(modes.reshape(outs.shape[0], p.n), c.read_row_modes())
+    assert (modes.reshape(outs.shape[0], p.n) != p.base_row_mode).any()
+    assert tg(jvm.env, None, 0) is None and rm(jvm.env, None, 0) is None
     # an unsupported override fails as a RuntimeException naming it
     bad = _solve(jni, jvm, ctx, p, dis, unsupported={0: jvm.array([1], np.int32)})
     assert bad is None and "distributedSlackOverrideBus" in jvm.take_exception()[1]
