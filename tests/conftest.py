@@ -43,3 +43,19 @@ def grid(name):
         g = synthetic.build(name)
         _GRIDS[name] = (g, packing.pack(g))
     return _GRIDS[name]
+
+
+_ORACLE_ROWS = {}
+
+
+def oracle_rows(oracle_mod, name, x0, disabled):
+    """The oracle's batched solve (no outer loops, default settings) of a grid's scenarios, memoised per session:
+    the parametrizations of one parity test solve the same scenarios, and the oracle's rows depend only on them."""
+    import hashlib
+    import numpy as np
+    x0 = np.ascontiguousarray(x0, dtype=np.float64)
+    disabled = np.ascontiguousarray(disabled, dtype=np.uint8)
+    key = (name, hashlib.sha1(x0.tobytes()).hexdigest(), hashlib.sha1(disabled.tobytes()).hexdigest(), disabled.shape)
+    if key not in _ORACLE_ROWS:
+        _ORACLE_ROWS[key] = oracle_mod.Structure(grid(name)[1]).solve_batch(x0, disabled)
+    return _ORACLE_ROWS[key].copy()

@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from conftest import grid
+from conftest import grid, oracle_rows
 
 pytestmark = pytest.mark.gpu
 
@@ -295,7 +295,7 @@ def test_schedules_match_oracle(engine_lib, oracle_mod, schedule, lanes, threads
     ctx.set_linear_solver_settings(precision, 1)
     ctx.set_schedule(schedule, lanes, threads)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
-    ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis)
+    ref = oracle_rows(oracle_mod, "grid2000", p.x_base, dis)
     _compare(r, ref, p.n, _tol(precision))
 
 
@@ -470,7 +470,7 @@ def test_dense_front_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes
     ctx.set_linear_solver_settings(precision, 1)
     ctx.set_schedule(schedule, lanes, threads)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
-    _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n, _tol(precision))
+    _compare(r, oracle_rows(oracle_mod, name, p.x_base, dis), p.n, _tol(precision))
 
 
 def test_dense_front_plan_rejected_by_tiles(engine_lib):
