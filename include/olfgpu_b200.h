@@ -110,6 +110,20 @@ int olfgpu_structure_levels(int64_t structure, int* factorLevelPtr, int* forward
  */
 int olfgpu_structure_subtrees(int64_t structure, int64_t* stats6);
 
+/*
+ * A host check of the structure's block-LU plan (no counterpart in the reference's API; the reference checks its own
+ * LU schedules for races the same way, native/host/lu_transposed_check.cpp:175-216), from the plan's dependency data
+ * alone: the symbolic factorization is closed and every block's update list complete and ascending; every LU block is
+ * one factorization level task and every block a task reads lies on a strictly earlier level (so the tasks of one
+ * level launch share no data), the dense front's split included; every solve position is on one forward (and, outside
+ * the dense front, one backward) level and reads only entries of strictly earlier levels.  violations receives the
+ * number found (0 for a sound plan), firstViolation (capacity bytes, may be null) the first one.  plantedFault 1..3
+ * checks a copy with one planted error (a task moved one level up, an update dropped, two forward positions swapped
+ * between the first and the last level) to test the check itself; 0 checks the plan as built.
+ */
+int olfgpu_structure_check_plan(int64_t structure, int plantedFault, int64_t* violations, char* firstViolation,
+                                int capacity);
+
 /* StructureNative.recommendBatchSize (structure_jni.cu:151-180): the bank that fits 70 % of free device memory. */
 int olfgpu_recommend_batch_size(int64_t structure, int maxCap, int mode, int* batchOut);
 

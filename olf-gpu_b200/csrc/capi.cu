@@ -248,6 +248,21 @@ extern "C" int olfgpu_structure_levels(int64_t structure, int* factorLevelPtr, i
     });
 }
 
+extern "C" int olfgpu_structure_check_plan(int64_t structure, int plantedFault, int64_t* violations,
+                                           char* firstViolation, int capacity) {
+    return guarded([&] {
+        if (plantedFault < 0 || plantedFault > 3) throw std::runtime_error("plantedFault must be 0..3");
+        if (!violations) throw std::runtime_error("null output");
+        std::string first;
+        *violations = checkBlockPlan(structureOf(structure)->host.plan, plantedFault, first);
+        if (firstViolation && capacity > 0) {
+            const size_t k = std::min(first.size(), static_cast<size_t>(capacity - 1));
+            std::memcpy(firstViolation, first.data(), k);
+            firstViolation[k] = 0;
+        }
+    });
+}
+
 extern "C" int olfgpu_structure_subtrees(int64_t structure, int64_t* stats6) {
     return guarded([&] {
         const BlockPlan& p = structureOf(structure)->host.plan;

@@ -865,4 +865,173 @@ void buildPlan(Structure& s, int ordering, long long shallowWeight) {
 
 }  // namespace
 
+int64_t checkBlockPlan(const BlockPlan& plan, int plantedFault, std::string& first) {
+    BlockPlan p = plan;   // a planted fault changes this copy only
+    const int nb = p.nb, nLu = p.nU + p.nL;
+    // where every LU block sits: U block t is (uRow[t], uCol[t]); L block nU + t is (lRow[t], lCol[t])
+    std::vector<int> rowOf(nLu), colOf(nLu);
+    for (int k = 0; k < nb; k++) {
+        for (int t = p.uPtr[k]; t < p.uPtr[k + 1]; t++) rowOf[t] = k, colOf[t] = p.uCol[t];
+        for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++) rowOf[p.nU + t] = p.lRow[t], colOf[p.nU + t] = k;
+    }
+    if (plantedFault == 1) {
+        // a task moved one level up, beside a block it reads: the deepest task with an update
+        int victim = -1;
+        for (int id = 0; id < nLu; id++)
+            if (p.opPtr[id + 1] > p.opPtr[id] && (victim < 0 || p.level[id] > p.level[victim])) victim = id;
+        if (victim >= 0) {
+            p.level[victim]--;
+            p.levelPtr.assign(p.levelPtr.size(), 0);
+            for (int id = 0; id < nLu; id++) p.levelPtr[p.level[id] + 1]++;
+            for (size_t l = 0; l + 1 < p.levelPtr.size(); l++) p.levelPtr[l + 1] += p.levelPtr[l];
+            std::vector<int> w(p.levelPtr.begin(), p.levelPtr.end() - 1);
+            for (int id = 0; id < nLu; id++) p.levelTask[w[p.level[id]]++] = id;
+        }
+    } else if (plantedFault == 2) {
+        // one update dropped from the longest update list
+        int victim = 0;
+        for (int id = 1; id < nLu; id++)
+            if (p.opPtr[id + 1] - p.opPtr[id] > p.opPtr[victim + 1] - p.opPtr[victim]) victim = id;
+        const int q = p.opPtr[victim];
+        if (p.opPtr[victim + 1] > q) {
+            p.opL.erase(p.opL.begin() + q);
+            p.opU.erase(p.opU.begin() + q);
+            p.opD.erase(p.opD.begin() + q);
+            for (int id = victim + 1; id <= nLu; id++) p.opPtr[id]--;
+            for (int id = victim + 1; id < nLu; id++) p.opOuterEnd[id]--;
+            if (p.opOuterEnd[victim] > q) p.opOuterEnd[victim]--;
+        }
+    } else if (plantedFault == 3) {
+        // a forward-solve position of the last level swapped with one of the first
+        if (!p.fwdLevelPos.empty()) std::swap(p.fwdLevelPos[0], p.fwdLevelPos.back());
+    }
+    int64_t bad = 0;
+    auto fail = [&](const std::string& what) {
+        if (bad++ == 0) first = what;
+    };
+    auto blockAt = [&](int a, int b) -> int {
+        if (a <= b) {
+            if (a == b) return p.uPtr[a];
+            auto lo = p.uCol.begin() + p.uPtr[a] + 1, hi = p.uCol.begin() + p.uPtr[a + 1];
+            auto it = std::lower_bound(lo, hi, b);
+            return it != hi && *it == b ? static_cast<int>(it - p.uCol.begin()) : -1;
+        }
+        auto lo = p.lRow.begin() + p.lPtr[b], hi = p.lRow.begin() + p.lPtr[b + 1];
+        auto it = std::lower_bound(lo, hi, a);
+        return it != hi && *it == a ? p.nU + static_cast<int>(it - p.lRow.begin()) : -1;
+    };
+    auto where = [&](int id) {
+        return " (block " + std::to_string(rowOf[id]) + "," + std::to_string(colOf[id]) + ")";
+    };
+
+    // (1) closure of the symbolic factorization and the update lists: L(a, m) by rows, U(m, b) by columns, m ascending
+    std::vector<std::vector<int>> lByRow(nb), uByCol(nb);
+    for (int m = 0; m < nb; m++) {
+        for (int t = p.lPtr[m]; t < p.lPtr[m + 1]; t++) lByRow[p.lRow[t]].push_back(p.nU + t);
+        for (int t = p.uPtr[m] + 1; t < p.uPtr[m + 1]; t++) uByCol[p.uCol[t]].push_back(t);
+    }
+    for (int m = 0; m < nb; m++)
+        for (int t = p.lPtr[m]; t < p.lPtr[m + 1]; t++)
+            for (int u = p.uPtr[m] + 1; u < p.uPtr[m + 1]; u++)
+                if (blockAt(p.lRow[t], p.uCol[u]) < 0)
+                    fail("fill not closed: the update L(" + std::to_string(p.lRow[t]) + "," + std::to_string(m) +
+                         ") U(" + std::to_string(m) + "," + std::to_string(p.uCol[u]) + ") has no block");
+    for (int id = 0; id < nLu; id++) {
+        const int a = rowOf[id], b = colOf[id], top = std::min(a, b);
+        const std::vector<int>& L = lByRow[a];
+        const std::vector<int>& U = uByCol[b];
+        int q = p.opPtr[id];
+        size_t i = 0, j = 0;
+        bool ok = true;
+        while (i < L.size() && j < U.size()) {
+            const int mi = colOf[L[i]], mj = rowOf[U[j]];
+            if (mi >= top || mj >= top) break;
+            if (mi < mj) {
+                i++;
+                continue;
+            }
+            if (mj < mi) {
+                j++;
+                continue;
+            }
+            const int d = p.deferredL ? p.uPtr[mi] : -1;
+            if (q >= p.opPtr[id + 1] || p.opL[q] != L[i] || p.opU[q] != U[j] || p.opD[q] != d) ok = false;
+            q++, i++, j++;
+        }
+        if (!ok || q != p.opPtr[id + 1]) fail("update list differs from the symbolic factorization" + where(id));
+    }
+
+    // (2) factorization levels: every block once; every block a task reads lies on a strictly earlier level
+    const int nLevels = static_cast<int>(p.levelPtr.size()) - 1;
+    std::vector<int> lev(nLu, -1);
+    for (int l = 0; l < nLevels; l++)
+        for (int k = p.levelPtr[l]; k < p.levelPtr[l + 1]; k++) {
+            const int id = p.levelTask[k];
+            if (id < 0 || id >= nLu || lev[id] >= 0) fail("a block is not exactly one level task");
+            else lev[id] = l;
+        }
+    for (int id = 0; id < nLu; id++)
+        if (lev[id] < 0) fail("a block has no level task" + where(id));
+    const int fs = p.frontStart;
+    auto inFront = [&](int id) { return rowOf[id] >= fs && colOf[id] >= fs; };
+    for (int id = 0; id < nLu; id++) {
+        if (lev[id] < 0) continue;
+        const int lv = lev[id];
+        for (int q = p.opPtr[id]; q < p.opOuterEnd[id]; q++) {
+            const bool early = lev[p.opL[q]] < lv && lev[p.opU[q]] < lv && (p.opD[q] < 0 || lev[p.opD[q]] < lv);
+            if (!early) fail("a task reads a block of its own or a later level" + where(id));
+        }
+        if (inFront(id)) {
+            // the level task applies exactly the updates whose pivot precedes the front; the dense front the rest
+            const int e = p.opOuterEnd[id];
+            for (int q = p.opPtr[id]; q < p.opPtr[id + 1]; q++)
+                if ((rowOf[p.opU[q]] < fs) != (q < e))
+                    fail("a front block's level task splits its updates wrongly" + where(id));
+        } else if (p.opOuterEnd[id] != p.opPtr[id + 1]) {
+            fail("a block outside the front leaves updates to the front" + where(id));
+        }
+        if (rowOf[id] > colOf[id] && !p.deferredL && !inFront(id) && !(lev[p.uPtr[colOf[id]]] < lv))
+            fail("an L block is scaled before its pivot is inverted" + where(id));
+    }
+    if (p.frontF > 0) {
+        const int F = p.frontF;
+        for (int i = 0; i < F; i++)
+            for (int j = 0; j < F; j++) {
+                const int id = p.frontBlocks[static_cast<size_t>(i) * F + j];
+                if (id < 0 || id != blockAt(fs + i, fs + j)) fail("the dense front's block table is incomplete");
+            }
+    }
+
+    // (3) solve levels: the forward sweep reads y(k) for L(i, k), k before the front; the backward sweep x(j) for
+    // U(i, j), the front's positions solved first by the dense front
+    auto levelsOf = [&](const std::vector<int>& ptr, const std::vector<int>& pos, std::vector<int>& lv,
+                        const char* what) {
+        for (size_t l = 0; l + 1 < ptr.size(); l++)
+            for (int k = ptr[l]; k < ptr[l + 1]; k++) {
+                const int i = pos[k];
+                if (i < 0 || i >= nb || lv[i] != -2) fail(std::string(what) + ": a position is not exactly once");
+                else lv[i] = static_cast<int>(l);
+            }
+    };
+    std::vector<int> fl(nb, -2), bl(nb, -2);
+    levelsOf(p.fwdLevelPtr, p.fwdLevelPos, fl, "forward levels");
+    levelsOf(p.bwdLevelPtr, p.bwdLevelPos, bl, "backward levels");
+    for (int i = 0; i < nb; i++) {
+        if (fl[i] < 0) fail("forward levels: position " + std::to_string(i) + " missing");
+        if (i >= fs) {
+            if (bl[i] != -2) fail("backward levels: a front position on a level");
+            bl[i] = -1;
+        } else if (bl[i] < 0) {
+            fail("backward levels: position " + std::to_string(i) + " missing");
+        }
+    }
+    for (int k = 0; k < std::min(fs, nb); k++)
+        for (int t = p.lPtr[k]; t < p.lPtr[k + 1]; t++)
+            if (!(fl[k] < fl[p.lRow[t]])) fail("forward sweep: a position reads an entry of its own or a later level");
+    for (int i = 0; i < std::min(fs, nb); i++)
+        for (int t = p.uPtr[i] + 1; t < p.uPtr[i + 1]; t++)
+            if (!(bl[p.uCol[t]] < bl[i])) fail("backward sweep: a position reads an entry of its own or a later level");
+    return bad;
+}
+
 }  // namespace olfb200

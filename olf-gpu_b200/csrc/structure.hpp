@@ -81,4 +81,20 @@ constexpr int MAX_FRONT = 32;
 
 void buildBlockPlan(Structure& s, int ordering);
 
+// Verifies a block-LU plan on the host from its dependency data alone, independently of how its levels were assigned
+// (a level launch must share no data between its tasks; the reference checks its own LU schedules the same way,
+// native/host/lu_transposed_check.cpp:175-216):
+//  (1) the symbolic factorization is closed (every update L(a, m) U(m, b), m < min(a, b), lands on a block of the
+//      pattern) and every block's update list is exactly those pivots m, ascending, with their operands (and, in the
+//      deferred-L plan, the pivot inverse of m);
+//  (2) the factorization levels hold every LU block once, and every block a task reads (the operands of the updates it
+//      applies, the pivot inverse it scales by) lies on a strictly earlier level; a dense-front block's task applies
+//      exactly its updates whose pivot precedes the front, and the front's block table is complete;
+//  (3) the forward levels hold every position once, the backward levels every position outside the dense front once,
+//      and every solution entry a position reads comes from a strictly earlier level (the front first, backward).
+// plantedFault 1..3 checks a copy with one planted error instead (a task moved one level up; an update dropped; two
+// forward positions swapped between the first and the last level), for tests of the check itself.  Returns the number
+// of violations; first describes the first one.
+int64_t checkBlockPlan(const BlockPlan& plan, int plantedFault, std::string& first);
+
 }  // namespace olfb200

@@ -46,7 +46,8 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_states_to_host", "olfgpu_read_batch_states", "olfgpu_set_outer_loops", "olfgpu_context_info",
            "olfgpu_linear_solve_transposed", "olfgpu_screen_violations", "olfgpu_last_slack_distribution_failures",
            "olfgpu_set_start_polish", "olfgpu_set_mixed_precision_policy", "olfgpu_last_fp64_iterations",
-           "olfgpu_set_device_loop", "olfgpu_read_batch_targets", "olfgpu_read_batch_row_modes"]
+           "olfgpu_set_device_loop", "olfgpu_read_batch_targets", "olfgpu_read_batch_row_modes",
+           "olfgpu_structure_check_plan"]
 # The arrays of BatchSolveNative.solveBatchContext this engine rejects when non-empty, in the reference's order
 UNSUPPORTED_SOLVE_ARRAYS = [
     "distributedSlackOverrideBus", "distributedSlackOverrideFactorDelta", "distributedSlackOverrideBaseTargetPDelta",
@@ -127,6 +128,7 @@ def load(path: str = LIB_PATH):
                                            _cd, _ci, _ip, _ip]
     L.olfgpu_read_batch_states.argtypes = [_i64, _ci, _ip, _dp]
     L.olfgpu_read_batch_targets.argtypes = [_i64, _ci, _ip, _dp]
+    L.olfgpu_structure_check_plan.argtypes = [_i64, _ci, ctypes.POINTER(_i64), ctypes.c_char_p, _ci]
     L.olfgpu_read_batch_row_modes.argtypes = [_i64, _ci, _ip, _ip]
     L.olfgpu_begin_batch_install.argtypes = [_i64, _ip, _ci]
     L.olfgpu_read_handed_back_slots.argtypes = [_i64, _ip, _ci, _ip]
@@ -243,6 +245,15 @@ class Structure:
         return {"bins": int(st[0]) // 100, "phases": int(st[0]) % 100, "bin_blocks": int(st[1]),
                 "max_bin_levels": int(st[2]), "top_wide_blocks": int(st[3]), "bin_positions": int(st[4]),
                 "wide_levels": int(st[5])}
+
+    def check_plan(self, planted_fault: int = 0):
+        """(violations, first violation) of the host check of the block-LU plan: closure of the symbolic
+        factorization, every level task reading only blocks of strictly earlier levels, both sweeps likewise.
+        planted_fault 1..3 checks a copy with one planted error (tests of the check itself)."""
+        v = _i64(0)
+        msg = ctypes.create_string_buffer(512)
+        _check(load().olfgpu_structure_check_plan(self.handle, planted_fault, ctypes.byref(v), msg, 512))
+        return int(v.value), msg.value.decode()
 
     def recommend_batch_size(self, max_cap: int, mode: int = BATCHED_LU) -> int:
         b = ctypes.c_int(0)

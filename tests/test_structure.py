@@ -136,3 +136,21 @@ def test_subtree_bins_keep_every_dependency(engine_lib, name, plan):
     assert st["bins"] > 0 and st["phases"] >= 1
     assert st["bin_blocks"] > 0.7 * s.n_lu_blocks          # most of the factorization moves into the bins
     assert st["max_bin_levels"] <= st["wide_levels"]
+
+
+@pytest.mark.parametrize("name", ["grid118", "grid2000", "grid9241", "grid13659"])
+@pytest.mark.parametrize("plan", [0, 3, 8, 11, 16, 19])
+def test_block_plan_is_race_free(engine_lib, name, plan):
+    """The host check of every block-LU plan variant (plain / shallow-tree minimum degree, scaled / deferred-L, with
+    and without the dense front): the symbolic factorization is closed, every update list complete, every level task
+    reads only blocks of strictly earlier levels, and both sweeps read only entries of strictly earlier levels, so no
+    level launch shares data between its tasks.  A copy with one planted error of each kind fails the check."""
+    from conftest import grid
+    from olfgpu import native
+    _, p = grid(name)
+    s = native.Structure(p, ordering=plan)
+    assert s.check_plan() == (0, "")
+    moved, dropped, swapped = (s.check_plan(k) for k in (1, 2, 3))
+    assert moved[0] > 0 and "level" in moved[1]
+    assert dropped[0] > 0 and "update list" in dropped[1]
+    assert swapped[0] > 0 and "forward" in swapped[1]
