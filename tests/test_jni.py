@@ -157,6 +157,21 @@ def test_jni_library_exports_the_hot_set(jni):
         assert hasattr(jni, PREFIX + name), name
 
 
+def test_readbacks_of_a_null_handle_are_null(jni):
+    """BatchReadbackNative on handle 0 returns null without raising, as the reference's read-backs do
+    (batch_readback_jni.cu:16-18, 36-38, 103-116); no GPU is touched."""
+    jvm = FakeJvm()
+    for name in ("readBatchTargets", "readBatchRowModes"):
+        f = _fn(jni, "ac_solver_gpu_BatchReadbackNative_" + name, _vp, 0)
+        f.argtypes = [_vp, _vp, _i64]
+        assert f(jvm.env, None, 0) is None
+    for name, res in (("readBatchNewtonLoopIterations", _i32), ("readBatchSolveCount", _i64)):
+        f = _fn(jni, "ac_solver_gpu_BatchReadbackNative_" + name, res, 0)
+        f.argtypes = [_vp, _vp, _i64]
+        assert f(jvm.env, None, 0) == -1
+    assert jvm.take_exception() is None
+
+
 def _create_structure(jni, jvm, p, extra=None):
     """StructureNative.createStructure with the reference's 33 array arguments; `extra` replaces some by name."""
     args = {"cbP": jvm.array(p.cb_params.reshape(-1), np.float64), "cbI": jvm.array(p.cb_idx.reshape(-1), np.int32),

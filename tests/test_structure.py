@@ -68,6 +68,13 @@ def test_bad_inputs_are_errors_not_crashes(engine_lib):
         native.Structure(q)
     with pytest.raises(native.NativeError, match="invalid structure handle"):
         native._check(native.load().olfgpu_structure_info(0, None, None))
+    with pytest.raises(native.NativeError, match="invalid batch solver context"):
+        native._check(native.load().olfgpu_read_batch_targets(0, 0, None, None))
+    with pytest.raises(native.NativeError, match="invalid batch solver context"):
+        native._check(native.load().olfgpu_read_batch_row_modes(0, 0, None, None))
+    s = native.Structure(p)
+    with pytest.raises(native.NativeError, match="plantedFault"):
+        native._check(native.load().olfgpu_structure_check_plan(s.handle, 7, None, None, 0))
 
 
 @pytest.mark.parametrize("plan", ["scaled", "deferred", "dense", "shallow"])
