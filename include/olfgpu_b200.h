@@ -196,6 +196,13 @@ int olfgpu_read_batch_states(int64_t context, int nSlots, const int* slots, doub
 int olfgpu_read_batch_targets(int64_t context, int nSlots, const int* slots, double* out);
 int olfgpu_read_batch_row_modes(int64_t context, int nSlots, const int* slots, int* out);
 
+/* ReactiveLimitsNative.readBatchReactiveLimitsFinalState (reactive_limits_jni.cu:407-427; read by
+ * GpuNewtonRaphson.java:579 and GpuBatchChunkSolver.java): per chosen bank slot and reactive-limit entry
+ * ([nSlots][nEntries], slot order), the entry's state as the last solve ended: its limit type (0 still PV, 1 at MIN_Q,
+ * 2 at MAX_Q) in the low three bits and its PV -> PQ switch count above them (gpu_reactive_limits_state.cuh).
+ * nEntries (may be null) receives the context's reactive-limit entries; with none, nothing is written. */
+int olfgpu_read_reactive_limits_state(int64_t context, int nSlots, const int* slots, int* out, int* nEntries);
+
 /* DriverNative.setBatchOuterLoops (driver_jni.cu:11-18): the distributed-slack and reactive-limit outer loops on or off
  * for the following solves (each acts only where the context holds its tables). */
 int olfgpu_set_outer_loops(int64_t context, int distributedSlack, int reactiveLimits);

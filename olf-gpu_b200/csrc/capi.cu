@@ -747,12 +747,13 @@ extern "C" int olfgpu_read_batch_states(int64_t context, int nSlots, const int* 
 
 namespace {
 
-// Rows [nSlots][n] of chosen bank slots out of a lane-interleaved per-row device array ([n][S] of T), after the
+// Rows [nSlots][width] of chosen bank slots out of a lane-interleaved device table ([width][S] of T), after the
 // context's stream has drained.
 template <typename T, typename U>
-void readSlotRows(BatchContext& c, const void* device, int nSlots, const int* slots, U* out) {
-    const int n = c.net->host.n;
+void readSlotRows(BatchContext& c, const void* device, int width, int nSlots, const int* slots, U* out) {
+    const int n = width;
     if (nSlots < 0 || (nSlots > 0 && (!slots || !out))) throw std::runtime_error("bad slot list or output");
+    if (n == 0 || nSlots == 0) return;
     for (int j = 0; j < nSlots; j++) {
         if (slots[j] < 0 || slots[j] >= c.nS) throw std::runtime_error("slot outside the bank");
     }
@@ -772,14 +773,31 @@ void readSlotRows(BatchContext& c, const void* device, int nSlots, const int* sl
 extern "C" int olfgpu_read_batch_targets(int64_t context, int nSlots, const int* slots, double* out) {
     return guarded([&] {
         BatchContext& c = contextOf(context);
-        readSlotRows<double>(c, c.target.p, nSlots, slots, out);
+        readSlotRows<double>(c, c.target.p, c.net->host.n, nSlots, slots, out);
     });
 }
 
 extern "C" int olfgpu_read_batch_row_modes(int64_t context, int nSlots, const int* slots, int* out) {
     return guarded([&] {
         BatchContext& c = contextOf(context);
-        readSlotRows<int8_t>(c, c.mode.p, nSlots, slots, out);
+        readSlotRows<int8_t>(c, c.mode.p, c.net->host.n, nSlots, slots, out);
+    });
+}
+
+extern "C" int olfgpu_read_reactive_limits_state(int64_t context, int nSlots, const int* slots, int* out,
+                                                 int* nEntries) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        const int nRl = c.rl.nRl;
+        if (nEntries) *nEntries = nRl;
+        if (nRl == 0) return;
+        std::vector<int> limitType(static_cast<size_t>(std::max(nSlots, 0)) * nRl);
+        std::vector<int> switches(limitType.size());
+        readSlotRows<int8_t>(c, c.rlLimitType.p, nRl, nSlots, slots, limitType.data());
+        readSlotRows<int8_t>(c, c.rlSwitchCount.p, nRl, nSlots, slots, switches.data());
+        // GpuReactiveLimitsState: the limit type (0 none, 1 MIN_Q, 2 MAX_Q) in the low three bits, the PV -> PQ
+        // switch count above them (gpu_reactive_limits_state.cuh:10-26)
+        for (size_t k = 0; k < limitType.size(); k++) out[k] = (limitType[k] & 7) | (switches[k] << 3);
     });
 }
 

@@ -10,6 +10,8 @@
 #include "jni.h"
 
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -73,6 +75,27 @@ struct LinearSolverSettings {
     bool splitLongRows = false;
 };
 LinearSolverSettings gSettings;
+
+// NewtonSettingsNative.setBatchX0Seeds per context: (local scenario * n + row, value) pairs written over the tiled
+// base state of the next solve that is given no full per-scenario state, and consumed by that solve either way
+// (scenario_install.cu:57-74).
+struct X0Seeds {
+    std::vector<jint> index;
+    std::vector<jdouble> value;
+};
+std::mutex gSeedsMutex;
+std::map<jlong, X0Seeds> gSeeds;
+
+X0Seeds takeSeeds(jlong handle) {
+    std::lock_guard<std::mutex> lock(gSeedsMutex);
+    X0Seeds out;
+    auto it = gSeeds.find(handle);
+    if (it != gSeeds.end()) {
+        out = std::move(it->second);
+        gSeeds.erase(it);
+    }
+    return out;
+}
 
 }  // namespace
 
@@ -194,7 +217,9 @@ JNIEXPORT jlong JNICALL OLF_JNI(ac_solver_gpu, BatchSolveNative, createBatchCont
 }
 
 JNIEXPORT void JNICALL OLF_JNI(ac_solver_gpu, BatchSolveNative, destroyBatchContext)(JNIEnv*, jclass, jlong handle) {
-    if (handle) olfgpu_destroy_batch_context(handle);
+    if (!handle) return;
+    takeSeeds(handle);
+    olfgpu_destroy_batch_context(handle);
 }
 
 JNIEXPORT void JNICALL OLF_JNI(ac_solver_gpu, BatchSolveNative, setBatchStatesToHost)(JNIEnv*, jclass, jlong handle,
@@ -265,7 +290,7 @@ JNIEXPORT jobjectArray JNICALL OLF_JNI(ac_solver_gpu, BatchSolveNative, solveBat
     const auto a12 = ints(env, jReactiveCapabilityCurveOverrideScenarioCurve);
     const auto a13 = doubles(env, jReactiveCapabilityCurveOverrideStepScale);
     const auto vt = ints(env, jvarType);
-    const auto xf = doubles(env, jx0Full);
+    auto xf = doubles(env, jx0Full);
     const auto so = ints(env, jShuntOvSlotElem);
     const auto sg = doubles(env, jShuntOvGb);
     const auto rs = ints(env, jReactiveLimitsSeedState);
@@ -283,6 +308,26 @@ JNIEXPORT jobjectArray JNICALL OLF_JNI(ac_solver_gpu, BatchSolveNative, solveBat
         const int k = rl < nElements ? rl : nElements;
         if (k > 0) olfjni_GetBooleanArrayRegion(env, row, 0, k, dis.data() + static_cast<size_t>(s) * nElements);
         if (row) olfjni_DeleteLocalRef(env, row);
+    }
+    // start seeds (setBatchX0Seeds) over the tiled base state when no full per-scenario state is given; consumed
+    // by this solve either way
+    const X0Seeds seeds = takeSeeds(handle);
+    if (xf.empty() && !seeds.index.empty()) {
+        if (static_cast<int>(x0.size()) != n) {
+            throwRuntime(env, "GPU batched Newton-Raphson failed: x0Base must hold n values to take start seeds");
+            return nullptr;
+        }
+        xf.resize(static_cast<size_t>(nS) * n);
+        for (int s2 = 0; s2 < nS; s2++) std::memcpy(&xf[static_cast<size_t>(s2) * n], x0.data(), sizeof(double) * n);
+        for (size_t k = 0; k < seeds.index.size(); k++) {
+            const jint idx = seeds.index[k];
+            if (idx < 0 || static_cast<int64_t>(idx) >= static_cast<int64_t>(nS) * n) {
+                throwRuntime(env, "GPU batched Newton-Raphson failed: setBatchX0Seeds index " + std::to_string(idx) +
+                                      " outside the " + std::to_string(nS) + " installed scenarios");
+                return nullptr;
+            }
+            xf[idx] = seeds.value[k];
+        }
     }
     std::vector<double> out(static_cast<size_t>(nS) * (n + 3));
     const int rc = olfgpu_solve_batch_context_full(
@@ -462,6 +507,176 @@ JNIEXPORT jintArray JNICALL OLF_JNI(ac_solver_gpu, BatchReadbackNative, readBatc
     jintArray out = olfjni_NewIntArray(env, static_cast<jsize>(host.size()));
     if (out && !host.empty()) olfjni_SetIntArrayRegion(env, out, 0, static_cast<jsize>(host.size()), host.data());
     return out;
+}
+
+
+// ---------------------------------------------------------------------------------------------------------------
+// The rest of the native methods the SPI path (GpuNewtonRaphson.java) and the batched SA (GpuBatchChunkSolver.java)
+// call on every run, so that the Java side links against this library: settings this engine applies, the reference's
+// own answer for a context without the feature (null read-backs, ignored anchors), and an exception naming the input
+// where a caller hands in data of a family this engine does not model.
+// ---------------------------------------------------------------------------------------------------------------
+
+// NewtonSettingsNative.setBatchX0Seeds (newton_settings_jni.cu:42-63): start values over the base state of the next
+// solve given no full per-scenario state (flat index local scenario * n + row); null or empty clears them.
+JNIEXPORT void JNICALL OLF_JNI(ac_solver_gpu, NewtonSettingsNative, setBatchX0Seeds)(JNIEnv* env, jclass,
+                                                                                   jlong handle, jintArray jIdx,
+                                                                                   jdoubleArray jVal) {
+    if (!handle) return;
+    X0Seeds seeds;
+    if (jIdx && jVal) {
+        seeds.index = ints(env, jIdx);
+        seeds.value = doubles(env, jVal);
+        if (seeds.index.size() != seeds.value.size()) {
+            throwRuntime(env, "setBatchX0Seeds failed: index and value arrays differ in length");
+            return;
+        }
+    }
+    std::lock_guard<std::mutex> lock(gSeedsMutex);
+    if (seeds.index.empty()) gSeeds.erase(handle);
+    else gSeeds[handle] = std::move(seeds);
+}
+
+// NewtonSettingsNative.setBatchRowCriteria / setBatchRowCriteriaAlternate (newton_settings_jni.cu:80-120): null
+// clears the per-row stopping thresholds, which this engine never holds (its test is OLF's infinity-norm or 2-norm
+// rule); thresholds (OLF's PerEquationTypeStoppingCriteria) are refused.
+JNIEXPORT void JNICALL OLF_JNI(ac_solver_gpu, NewtonSettingsNative, setBatchRowCriteria)(
+    JNIEnv* env, jclass, jlong handle, jdoubleArray jFixedVariableRowMaxMismatch, jdoubleArray jEquationRowMaxMismatch) {
+    if (!handle || !jFixedVariableRowMaxMismatch || !jEquationRowMaxMismatch) return;
+    throwRuntime(env, "setBatchRowCriteria failed: per-equation-type stopping criteria are not supported by this engine");
+}
+
+JNIEXPORT void JNICALL OLF_JNI(ac_solver_gpu, NewtonSettingsNative, setBatchRowCriteriaAlternate)(
+    JNIEnv* env, jclass, jlong handle, jdoubleArray jAlternateRowMaxMismatch, jintArray jSelector) {
+    if (!handle || !jAlternateRowMaxMismatch || !jSelector) return;
+    throwRuntime(env,
+                 "setBatchRowCriteriaAlternate failed: per-equation-type stopping criteria are not supported by this engine");
+}
+
+// NewtonSettingsNative.setBatchActiveRowCounts: the active equation count of OLF's 2-norm threshold per scenario.
+// Every row of the families this engine models is active, so null, or a count of n for every scenario, is what it
+// already uses; a smaller count (islanded buses, rho/a1 identities) is refused.
+JNIEXPORT void JNICALL OLF_JNI(ac_solver_gpu, NewtonSettingsNative, setBatchActiveRowCounts)(JNIEnv* env, jclass,
+                                                                                           jlong handle,
+                                                                                           jintArray jActive) {
+    if (!handle || !jActive) return;
+    int n = 0;
+    if (!ok(env, olfgpu_context_info(handle, &n, nullptr, nullptr, nullptr, nullptr, nullptr), "setBatchActiveRowCounts")) {
+        return;
+    }
+    for (jint a : ints(env, jActive)) {
+        if (a != n) {
+            throwRuntime(env, "setBatchActiveRowCounts failed: an active equation count below n (islanded buses or "
+                              "rho/a1 identities) is not supported by this engine");
+            return;
+        }
+    }
+}
+
+// NewtonSettingsNative.setBatchFrozenRows: the rows an islanding outage froze; null or empty clears (islanding
+// outages are not batched by this engine, so there are none to hold).
+JNIEXPORT void JNICALL OLF_JNI(ac_solver_gpu, NewtonSettingsNative, setBatchFrozenRows)(JNIEnv* env, jclass,
+                                                                                      jlong handle, jintArray jSlotRow) {
+    if (!handle || lengthOf(env, jSlotRow) == 0) return;
+    throwRuntime(env, "setBatchFrozenRows failed: islanding outages are not supported by this engine");
+}
+
+// NewtonSettingsNative.setBatchLineSearch: the LINE_SEARCH state-vector scaling is not modelled (NONE and
+// MAX_VOLTAGE_CHANGE are); the Java side calls this only for that mode.
+JNIEXPORT void JNICALL OLF_JNI(ac_solver_gpu, NewtonSettingsNative, setBatchLineSearch)(JNIEnv* env, jclass,
+                                                                                      jlong handle, jint, jdouble) {
+    if (!handle) return;
+    throwRuntime(env, "setBatchLineSearch failed: LINE_SEARCH state-vector scaling is not supported by this engine");
+}
+
+// NewtonSettingsNative.setBatchLoopTraceSlot: the reference's print-only outer-loop trace channel; nothing to print
+// here, and a trace never changes a result.
+JNIEXPORT void JNICALL OLF_JNI(ac_solver_gpu, NewtonSettingsNative, setBatchLoopTraceSlot)(JNIEnv*, jclass, jlong,
+                                                                                         jint) {}
+
+// DistributedSlackNative.setBatchDistributedSlackGeneratorAnchors (distributed_slack_jni.cu:26-42): per scenario and
+// participating GENERATOR; this engine's participants are buses (olfgpu_create_batch_context_full), so only null or
+// empty arrays fit its zero generators.
+JNIEXPORT void JNICALL OLF_JNI(ac_outerloop_gpu, DistributedSlackNative, setBatchDistributedSlackGeneratorAnchors)(
+    JNIEnv* env, jclass, jlong handle, jdoubleArray jAnchor, jdoubleArray jStart, jdoubleArray jSeedAnchor) {
+    if (!handle) return;
+    if (lengthOf(env, jAnchor) || lengthOf(env, jStart) || lengthOf(env, jSeedAnchor)) {
+        throwRuntime(env, "setBatchDistributedSlackGeneratorAnchors failed: per-generator distributed-slack "
+                          "participants are not supported by this engine (its participants are buses)");
+    }
+}
+
+// DistributedSlackNative.setBatchSlackOnlyAnchor (distributed_slack_jni.cu:12-19): the reference installs it only
+// for a slack-only distribution and ignores it otherwise; this engine never runs one.
+JNIEXPORT void JNICALL OLF_JNI(ac_outerloop_gpu, DistributedSlackNative, setBatchSlackOnlyAnchor)(JNIEnv*, jclass,
+                                                                                                jlong, jdoubleArray) {}
+
+// ReactiveLimitsNative.setBatchForcedTargetQPre (reactive_limits_jni.cu:108-116): ignored without forced-target-Q
+// entries, as in the reference; this engine has none.
+JNIEXPORT void JNICALL OLF_JNI(ac_outerloop_gpu, ReactiveLimitsNative, setBatchForcedTargetQPre)(JNIEnv*, jclass,
+                                                                                               jlong, jdoubleArray) {}
+
+// ReactiveLimitsNative.setBatchReactiveLimitSeedTargetQ (reactive_limits_jni.cu:368-376): per-scenario seeded target
+// Q of the entries (a strategy pair's continuation); null or empty clears, values are refused.
+JNIEXPORT void JNICALL OLF_JNI(ac_outerloop_gpu, ReactiveLimitsNative, setBatchReactiveLimitSeedTargetQ)(
+    JNIEnv* env, jclass, jlong handle, jdoubleArray jTargets) {
+    if (!handle || lengthOf(env, jTargets) == 0) return;
+    throwRuntime(env, "setBatchReactiveLimitSeedTargetQ failed: seeded reactive-limit targets are not supported by "
+                      "this engine");
+}
+
+// ReactiveLimitsNative.readBatchReactiveLimitsFinalState (reactive_limits_jni.cu:407-427): [slots x entries] of
+// limit type | switch count << 3, the last solve's slots; null without reactive-limit entries.
+JNIEXPORT jintArray JNICALL OLF_JNI(ac_outerloop_gpu, ReactiveLimitsNative, readBatchReactiveLimitsFinalState)(
+    JNIEnv* env, jclass, jlong handle) {
+    if (!handle) return nullptr;
+    int nRl = 0;
+    if (!ok(env, olfgpu_read_reactive_limits_state(handle, 0, nullptr, nullptr, &nRl),
+            "readBatchReactiveLimitsFinalState") || nRl == 0) {
+        return nullptr;
+    }
+    std::vector<int> slots;
+    int n = 0;
+    if (!readbackSlots(env, handle, "readBatchReactiveLimitsFinalState", slots, n)) return nullptr;
+    std::vector<int> host(slots.size() * static_cast<size_t>(nRl));
+    if (!ok(env, olfgpu_read_reactive_limits_state(handle, len(slots), ptr(slots), host.data(), nullptr),
+            "readBatchReactiveLimitsFinalState")) {
+        return nullptr;
+    }
+    jintArray out = olfjni_NewIntArray(env, static_cast<jsize>(host.size()));
+    if (out && !host.empty()) olfjni_SetIntArrayRegion(env, out, 0, static_cast<jsize>(host.size()), host.data());
+    return out;
+}
+
+// BatchReadbackNative read-backs of what this engine does not track: the reference answers null for a context
+// without per-generator distributed-slack participants (batch_readback_jni.cu:64-79), without a slack-only
+// distribution (:50-62) or its retained share (:138-150), without the per-pass statistics (:81-101) and without the
+// last converged state (:121-136), and its callers take null as "none" (GpuNewtonRaphson.java:381 then counts the
+// solve's own iterations).
+JNIEXPORT jdoubleArray JNICALL OLF_JNI(ac_solver_gpu, BatchReadbackNative, readBatchDistributedSlackGeneratorMove)(
+    JNIEnv*, jclass, jlong) {
+    return nullptr;
+}
+
+JNIEXPORT jdoubleArray JNICALL OLF_JNI(ac_solver_gpu, BatchReadbackNative, readBatchSlackRetainedShare)(JNIEnv*,
+                                                                                                      jclass, jlong) {
+    return nullptr;
+}
+
+JNIEXPORT jdoubleArray JNICALL OLF_JNI(ac_solver_gpu, BatchReadbackNative, readBatchSlackAbsorbed)(JNIEnv*, jclass,
+                                                                                                jlong) {
+    return nullptr;
+}
+
+JNIEXPORT jintArray JNICALL OLF_JNI(ac_solver_gpu, BatchReadbackNative, readBatchOuterLoopStats)(JNIEnv*, jclass,
+                                                                                              jlong) {
+    return nullptr;
+}
+
+JNIEXPORT jdoubleArray JNICALL OLF_JNI(ac_solver_gpu, BatchReadbackNative, readBatchLastConvergedState)(JNIEnv*,
+                                                                                                     jclass, jlong,
+                                                                                                     jint) {
+    return nullptr;
 }
 
 }  // extern "C"

@@ -47,7 +47,7 @@ EXPORTS = ["olfgpu_last_error", "olfgpu_create_structure", "olfgpu_destroy_struc
            "olfgpu_linear_solve_transposed", "olfgpu_screen_violations", "olfgpu_last_slack_distribution_failures",
            "olfgpu_set_start_polish", "olfgpu_set_mixed_precision_policy", "olfgpu_last_fp64_iterations",
            "olfgpu_set_device_loop", "olfgpu_read_batch_targets", "olfgpu_read_batch_row_modes",
-           "olfgpu_structure_check_plan"]
+           "olfgpu_structure_check_plan", "olfgpu_read_reactive_limits_state"]
 # The arrays of BatchSolveNative.solveBatchContext this engine rejects when non-empty, in the reference's order
 UNSUPPORTED_SOLVE_ARRAYS = [
     "distributedSlackOverrideBus", "distributedSlackOverrideFactorDelta", "distributedSlackOverrideBaseTargetPDelta",
@@ -128,6 +128,7 @@ def load(path: str = LIB_PATH):
                                            _cd, _ci, _ip, _ip]
     L.olfgpu_read_batch_states.argtypes = [_i64, _ci, _ip, _dp]
     L.olfgpu_read_batch_targets.argtypes = [_i64, _ci, _ip, _dp]
+    L.olfgpu_read_reactive_limits_state.argtypes = [_i64, _ci, _ip, _ip, _ip]
     L.olfgpu_structure_check_plan.argtypes = [_i64, _ci, ctypes.POINTER(_i64), ctypes.c_char_p, _ci]
     L.olfgpu_read_batch_row_modes.argtypes = [_i64, _ci, _ip, _ip]
     L.olfgpu_begin_batch_install.argtypes = [_i64, _ip, _ci]

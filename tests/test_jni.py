@@ -34,6 +34,23 @@ HOT_SET = [
     "ac_solver_gpu_BatchReadbackNative_readBatchSolveCount",
     "ac_solver_gpu_BatchReadbackNative_readBatchTargets",
     "ac_solver_gpu_BatchReadbackNative_readBatchRowModes",
+    "ac_solver_gpu_BatchReadbackNative_readBatchDistributedSlackGeneratorMove",
+    "ac_solver_gpu_BatchReadbackNative_readBatchSlackRetainedShare",
+    "ac_solver_gpu_BatchReadbackNative_readBatchSlackAbsorbed",
+    "ac_solver_gpu_BatchReadbackNative_readBatchOuterLoopStats",
+    "ac_solver_gpu_BatchReadbackNative_readBatchLastConvergedState",
+    "ac_solver_gpu_NewtonSettingsNative_setBatchX0Seeds",
+    "ac_solver_gpu_NewtonSettingsNative_setBatchRowCriteria",
+    "ac_solver_gpu_NewtonSettingsNative_setBatchRowCriteriaAlternate",
+    "ac_solver_gpu_NewtonSettingsNative_setBatchActiveRowCounts",
+    "ac_solver_gpu_NewtonSettingsNative_setBatchFrozenRows",
+    "ac_solver_gpu_NewtonSettingsNative_setBatchLineSearch",
+    "ac_solver_gpu_NewtonSettingsNative_setBatchLoopTraceSlot",
+    "ac_outerloop_gpu_DistributedSlackNative_setBatchDistributedSlackGeneratorAnchors",
+    "ac_outerloop_gpu_DistributedSlackNative_setBatchSlackOnlyAnchor",
+    "ac_outerloop_gpu_ReactiveLimitsNative_setBatchForcedTargetQPre",
+    "ac_outerloop_gpu_ReactiveLimitsNative_setBatchReactiveLimitSeedTargetQ",
+    "ac_outerloop_gpu_ReactiveLimitsNative_readBatchReactiveLimitsFinalState",
 ]
 
 _vp, _i32, _i64, _f64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
@@ -161,10 +178,17 @@ def test_readbacks_of_a_null_handle_are_null(jni):
     """BatchReadbackNative on handle 0 returns null without raising, as the reference's read-backs do
     (batch_readback_jni.cu:16-18, 36-38, 103-116); no GPU is touched."""
     jvm = FakeJvm()
-    for name in ("readBatchTargets", "readBatchRowModes"):
+    for name in ("readBatchTargets", "readBatchRowModes", "readBatchDistributedSlackGeneratorMove",
+                 "readBatchSlackRetainedShare", "readBatchSlackAbsorbed", "readBatchOuterLoopStats"):
         f = _fn(jni, "ac_solver_gpu_BatchReadbackNative_" + name, _vp, 0)
         f.argtypes = [_vp, _vp, _i64]
         assert f(jvm.env, None, 0) is None
+    f = _fn(jni, "ac_solver_gpu_BatchReadbackNative_readBatchLastConvergedState", _vp, 0)
+    f.argtypes = [_vp, _vp, _i64, _i32]
+    assert f(jvm.env, None, 0, 0) is None
+    f = _fn(jni, "ac_outerloop_gpu_ReactiveLimitsNative_readBatchReactiveLimitsFinalState", _vp, 0)
+    f.argtypes = [_vp, _vp, _i64]
+    assert f(jvm.env, None, 0) is None
     for name, res in (("readBatchNewtonLoopIterations", _i32), ("readBatchSolveCount", _i64)):
         f = _fn(jni, "ac_solver_gpu_BatchReadbackNative_" + name, res, 0)
         f.argtypes = [_vp, _vp, _i64]
@@ -334,6 +358,98 @@ def test_solve_through_jni_equals_the_c_abi(jni):
     # an unsupported override fails as a RuntimeException naming it
     bad = _solve(jni, jvm, ctx, p, dis, unsupported={0: jvm.array([1], np.int32)})
     assert bad is None and "distributedSlackOverrideBus" in jvm.take_exception()[1]
+    d = _fn(jni, "ac_solver_gpu_BatchSolveNative_destroyBatchContext", None, 0)
+    d.argtypes = [_vp, _vp, _i64]
+    d(jvm.env, None, ctx)
+
+
+@pytest.mark.gpu
+def test_spi_path_settings_seeds_and_reactive_limit_state(jni):
+    """The other native methods GpuNewtonRaphson / GpuBatchChunkSolver call on every run, through the JNI table on a
+    reactive-limit context: the reactive-limit final state agrees with the row modes read back and with the C ABI; the
+    settings clear on null and refuse inputs of families the engine does not model, naming them; start seeds
+    (setBatchX0Seeds) equal a full per-scenario start through the C ABI and are consumed by that solve."""
+    from olfgpu import native, synthetic
+    g, p = grid("grid300")
+    outs = synthetic.draw_outages(g, 40, seed=303)
+    dis = p.outage_masks(outs)
+    ns, n = outs.shape[0], p.n
+    jvm = FakeJvm()
+    sh = _create_structure(jni, jvm, p)
+    ctx = _create_context(jni, jvm, sh, ns, rl=p.rl)
+    assert ctx != 0, jvm.take_exception()
+    keys = _fn(jni, "ac_outerloop_gpu_ReactiveLimitsNative_setBatchReactiveLimitStrongestPvKeys", None, 0)
+    keys.argtypes = [_vp, _vp, _i64, _vp, _vp, _vp, _vp]
+    r = p.rl
+    keys(jvm.env, None, ctx, jvm.array(r.nom_v, np.float64), jvm.array(r.p_row, np.int32),
+         jvm.array(r.static_p, np.float64), jvm.array(r.id_rank, np.int32))
+    got = _solve(jni, jvm, ctx, p, dis)
+    assert got is not None, jvm.take_exception()
+
+    def call(cls, name, restype, argtypes, *args):
+        f = _fn(jni, cls + "_" + name, restype, 0)
+        f.argtypes = [_vp, _vp, _i64] + argtypes
+        return f(jvm.env, None, ctx, *args)
+
+    # the reactive-limit state: limit type in the low bits, switch count above; at a limit exactly where the entry's
+    # voltage row was read back as an equation row
+    st = jvm.value(call("ac_outerloop_gpu_ReactiveLimitsNative", "readBatchReactiveLimitsFinalState", _vp, []))
+    nrl = r.voltage_row.shape[0]
+    st = st.reshape(ns, nrl)
+    modes = jvm.value(call("ac_solver_gpu_BatchReadbackNative", "readBatchRowModes", _vp, [])).reshape(ns, n)
+    kind, switches = st & 7, st >> 3
+    assert set(np.unique(kind).tolist()) <= {0, 1, 2} and (kind > 0).any() and (switches >= (kind > 0)).all()
+    assert np.array_equal(kind > 0, modes[:, r.voltage_row] == 1)
+    out = np.zeros((2, nrl), np.int32)
+    cnt = ctypes.c_int(0)
+    two = np.array([9, 4], np.int32)
+    lib = native.load()
+    assert lib.olfgpu_read_reactive_limits_state(ctx, 2, two.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                 ctypes.byref(cnt)) == 0
+    assert cnt.value == nrl and np.array_equal(out, st[two])
+    # settings: null clears, data of an unmodelled family is refused by name
+    call("ac_solver_gpu_NewtonSettingsNative", "setBatchRowCriteria", None, [_vp, _vp], None, None)
+    call("ac_outerloop_gpu_DistributedSlackNative", "setBatchDistributedSlackGeneratorAnchors", None,
+         [_vp, _vp, _vp], None, jvm.array(np.zeros(0), np.float64), None)
+    call("ac_solver_gpu_NewtonSettingsNative", "setBatchActiveRowCounts", None, [_vp],
+         jvm.array(np.full(ns, n), np.int32))
+    call("ac_outerloop_gpu_DistributedSlackNative", "setBatchSlackOnlyAnchor", None, [_vp],
+         jvm.array(np.ones(ns), np.float64))
+    assert jvm.take_exception() is None
+    call("ac_solver_gpu_NewtonSettingsNative", "setBatchRowCriteria", None, [_vp, _vp],
+         jvm.array(np.ones(n), np.float64), jvm.array(np.ones(n), np.float64))
+    assert "per-equation-type" in jvm.take_exception()[1]
+    call("ac_outerloop_gpu_DistributedSlackNative", "setBatchDistributedSlackGeneratorAnchors", None,
+         [_vp, _vp, _vp], jvm.array(np.ones(ns), np.float64), None, None)
+    assert "per-generator" in jvm.take_exception()[1]
+    call("ac_solver_gpu_NewtonSettingsNative", "setBatchActiveRowCounts", None, [_vp],
+         jvm.array(np.full(ns, n - 2), np.int32))
+    assert "active equation count" in jvm.take_exception()[1]
+    call("ac_solver_gpu_NewtonSettingsNative", "setBatchLineSearch", None, [_i32, _f64], 5, 0.5)
+    assert "LINE_SEARCH" in jvm.take_exception()[1]
+    for name in ("readBatchOuterLoopStats", "readBatchSlackAbsorbed", "readBatchSlackRetainedShare",
+                 "readBatchDistributedSlackGeneratorMove"):
+        assert call("ac_solver_gpu_BatchReadbackNative", name, _vp, []) is None
+    # start seeds: two scenarios start off the base state; equal to the same start given in full through the C ABI,
+    # and consumed by that solve (the next one starts from the base again)
+    eq = np.flatnonzero(p.base_row_mode == 1)           # equation rows: their start moves the whole trajectory
+    idx = np.array([3 * n + eq[1], 7 * n + eq[5]], np.int32)
+    val = np.array([p.x_base[eq[1]] + 2e-3, p.x_base[eq[5]] - 2e-3])
+    call("ac_solver_gpu_NewtonSettingsNative", "setBatchX0Seeds", None, [_vp, _vp], jvm.array(idx, np.int32),
+         jvm.array(val, np.float64))
+    seeded = _solve(jni, jvm, ctx, p, dis)
+    assert seeded is not None, jvm.take_exception()
+    full = np.tile(p.x_base, (ns, 1))
+    full.reshape(-1)[idx] = val
+    c = native.BatchContext(native.Structure(p, ordering=native.PLAN_DEFAULT), ns, rl=p.rl)
+    c.set_schedule(native.LEVELS_SHARED_ALL, 0, 256)
+    assert np.array_equal(seeded, c.solve(p.x_base, p.target, p.base_row_mode, dis, x0_full=full))
+    assert not np.array_equal(seeded, got)
+    assert np.array_equal(_solve(jni, jvm, ctx, p, dis), got)
+    call("ac_solver_gpu_NewtonSettingsNative", "setBatchX0Seeds", None, [_vp, _vp], jvm.array([ns * n], np.int32),
+         jvm.array([1.0], np.float64))
+    assert _solve(jni, jvm, ctx, p, dis) is None and "setBatchX0Seeds index" in jvm.take_exception()[1]
     d = _fn(jni, "ac_solver_gpu_BatchSolveNative_destroyBatchContext", None, 0)
     d.argtypes = [_vp, _vp, _i64]
     d(jvm.env, None, ctx)
