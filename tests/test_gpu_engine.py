@@ -202,6 +202,35 @@ def test_iteration_budget_statuses(engine_lib, oracle_mod):
         assert e[0, -3] == o[0, -3], budget
 
 
+# the state after k fixed Newton steps: the engine's block LU and the oracle's sparse LU round differently (measured
+# ~1e-14 between the oracle's LU and the reference's own host LU on these grids); the mismatch norm at its rounding floor
+# near convergence is compared with an absolute floor
+TRAJECTORY_TOL = 1e-9
+
+
+@pytest.mark.parametrize("name,start,count,steps", [("grid118", "flat", 16, 5), ("grid2000", "base", 48, 3),
+                                                    ("grid9241", "base", 16, 3)])
+def test_fixed_iteration_trajectories_match_oracle(engine_lib, oracle_mod, name, start, count, steps):
+    """The design of the reference's GPU-vs-CPU fixed-iteration test: from the same start, a budget of k Newton
+    iterations stops every lane still iterating with MAX_ITERATION_REACHED at its k-th state, which must equal the
+    oracle's after k steps, with the same mismatch norm, for k = 1 .. steps (converged lanes as usual)."""
+    from olfgpu import native, synthetic
+    g, p = grid(name)
+    x0 = p.x_flat if start == "flat" else p.x_base
+    outs = synthetic.draw_outages(g, count, seed=41)
+    dis = p.outage_masks(outs)
+    s = native.Structure(p)
+    st = oracle_mod.Structure(p)
+    n = p.n
+    for k in range(1, steps + 1):
+        e = native.BatchContext(s, count).solve(x0, p.target, p.base_row_mode, dis, max_iter=k)
+        o = st.solve_batch(x0, dis, max_iter=k)
+        assert np.array_equal(e[:, n + 2], o[:, n + 2]), k
+        assert np.array_equal(e[:, n], o[:, n]), k
+        assert np.max(np.abs(e[:, :n] - o[:, :n])) <= TRAJECTORY_TOL, k
+        assert np.all(np.abs(e[:, n + 1] - o[:, n + 1]) <= 1e-10 + 1e-6 * np.abs(o[:, n + 1])), k
+
+
 def test_per_scenario_start_and_ragged_batch(engine_lib, oracle_mod):
     from olfgpu import native, synthetic
     g, p = grid("grid118")
