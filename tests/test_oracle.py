@@ -187,3 +187,33 @@ def test_jacobian_matches_central_differences(oracle_mod, name, outage):
         fd = (st.fill(xp, p.target, p.base_row_mode, dis)[1] - st.fill(xm, p.target, p.base_row_mode, dis)[1]) / (2 * h)
         worst = max(worst, float(np.max(np.abs(fd - J[:, c]) / np.maximum(np.abs(J[:, c]), 1.0))))
     assert worst < 1e-6, worst
+
+
+def test_oracle_final_equations_after_reactive_limits(oracle_mod):
+    """The oracle's per-scenario final equations (what the engine's targets / row-mode read-backs are checked
+    against): rows that differ from the installed ones are reactive-limit voltage rows switched to an equation row at
+    a Q limit (its target the limit less the load), and every converged state solves the equations it ended with."""
+    from conftest import grid
+    from olfgpu import synthetic
+    g, p = grid("grid300")
+    outs = synthetic.draw_outages(g, 40, seed=303)
+    dis = p.outage_masks(outs)
+    st = oracle_mod.Structure(p)
+    rows, tg, md = st.solve_batch(p.x_base, dis, reactive_limits=True, final_equations=True)
+    assert np.array_equal(rows, st.solve_batch(p.x_base, dis, reactive_limits=True))
+    rl = p.rl
+    switched = 0
+    for k in range(outs.shape[0]):
+        for r in np.flatnonzero((md[k] != p.base_row_mode) | (tg[k] != p.target)):
+            i = np.flatnonzero(rl.voltage_row == r)
+            assert i.size == 1 and md[k, r] == 1
+            i = int(i[0])
+            assert tg[k, r] in (rl.min_q[i] - rl.load_q[i], rl.max_q[i] - rl.load_q[i])
+            switched += 1
+        if rows[k, p.n + 2] == 0:
+            _, F = st.fill(rows[k, :p.n], tg[k], md[k], dis[k])
+            assert np.max(np.abs(F)) < 1e-8
+    assert switched > 0
+    plain, tg0, md0 = st.solve_batch(p.x_base, dis, final_equations=True)
+    assert np.array_equal(md0, np.tile(p.base_row_mode, (outs.shape[0], 1)))
+    assert np.array_equal(tg0, np.tile(p.target, (outs.shape[0], 1)))
