@@ -424,7 +424,7 @@ def test_pivot_growth_refactors_in_fp64(engine_lib, oracle_mod, schedule):
     cm.set_mixed_precision_controls(1e-2, 1e4)
     rm = cm.solve(p.x_base, p.target, p.base_row_mode, dis)
     assert cm.last_fp64_refactors().size <= outs.shape[0] // 20
-    _compare(rm, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n, MIXED_STATE_TOL)
+    _compare(rm, oracle_rows(oracle_mod, "grid2000", p.x_base, dis), p.n, MIXED_STATE_TOL)
 
 
 @pytest.mark.parametrize("refine_below", [float("inf"), 1e-2, 1e-12])
@@ -441,7 +441,7 @@ def test_adaptive_refinement_matches_oracle(engine_lib, oracle_mod, refine_below
     ctx.set_mixed_precision_controls(refine_below, 1e4)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
     tol = UNREFINED_STATE_TOL if refine_below < 1e-9 else MIXED_STATE_TOL
-    _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n, tol)
+    _compare(r, oracle_rows(oracle_mod, "grid2000", p.x_base, dis), p.n, tol)
 
 
 @pytest.mark.parametrize("schedule,lanes,threads", [(0, 2, 256), (0, 0, 256), (1, 2, 256), (2, 0, 512),
@@ -460,7 +460,7 @@ def test_deferred_l_plan_matches_oracle(engine_lib, oracle_mod, schedule, lanes,
     ctx.set_linear_solver_settings(precision, 1)
     ctx.set_schedule(schedule, lanes, threads)
     r = ctx.solve(p.x_base, p.target, p.base_row_mode, dis)
-    _compare(r, oracle_mod.Structure(p).solve_batch(p.x_base, dis), p.n, _tol(precision))
+    _compare(r, oracle_rows(oracle_mod, "grid2000", p.x_base, dis), p.n, _tol(precision))
 
 
 @pytest.mark.parametrize("precision", [0, 1])
@@ -532,7 +532,7 @@ def test_subtree_bins_match_oracle(engine_lib, oracle_mod, precision, name):
     g, p = grid(name)
     outs = synthetic.draw_outages(g, 96, seed=97)
     dis = p.outage_masks(outs)
-    ref = oracle_mod.Structure(p).solve_batch(p.x_base, dis)
+    ref = oracle_rows(oracle_mod, name, p.x_base, dis)
     for plan in (0, native.PLAN_DENSE_FRONT, native.PLAN_DEFAULT):
         s = native.Structure(p, ordering=plan)
         assert s.subtrees()["bins"] > 0
