@@ -729,22 +729,6 @@ extern "C" int olfgpu_states_to_host(int64_t context, int* statesToHost) {
     });
 }
 
-extern "C" int olfgpu_read_batch_states(int64_t context, int nSlots, const int* slots, double* out) {
-    return guarded([&] {
-        BatchContext& c = contextOf(context);
-        const int n = c.net->host.n;
-        if (nSlots < 0 || (nSlots > 0 && (!slots || !out))) throw std::runtime_error("bad slot list or output");
-        OLF_CUDA(cudaSetDevice(c.device));
-        std::vector<double> col(static_cast<size_t>(n) * c.S);
-        OLF_CUDA(cudaMemcpy(col.data(), c.x.p, col.size() * 8, cudaMemcpyDeviceToHost));
-        for (int j = 0; j < nSlots; j++) {
-            const int s2 = slots[j];
-            if (s2 < 0 || s2 >= c.nS) throw std::runtime_error("slot outside the bank");
-            for (int r = 0; r < n; r++) out[static_cast<size_t>(j) * n + r] = col[static_cast<size_t>(r) * c.S + s2];
-        }
-    });
-}
-
 namespace {
 
 // Rows [nSlots][width] of chosen bank slots out of a lane-interleaved device table ([width][S] of T), after the
@@ -769,6 +753,13 @@ void readSlotRows(BatchContext& c, const void* device, int width, int nSlots, co
 }
 
 }  // namespace
+
+extern "C" int olfgpu_read_batch_states(int64_t context, int nSlots, const int* slots, double* out) {
+    return guarded([&] {
+        BatchContext& c = contextOf(context);
+        readSlotRows<double>(c, c.x.p, c.net->host.n, nSlots, slots, out);
+    });
+}
 
 extern "C" int olfgpu_read_batch_targets(int64_t context, int nSlots, const int* slots, double* out) {
     return guarded([&] {
