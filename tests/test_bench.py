@@ -26,3 +26,23 @@ def test_launch_count_matches_the_launch_lists(bench_mod):
     assert bench_mod.launches_per_solve(dense, (3, 2, 256), 4, True, False, False, 0) == 798
     assert bench_mod.launches_per_solve(scaled, (0, 2, 256), 4, False, False, False, 0) == 782
     assert bench_mod.launches_per_solve(dense, (4, 0, 256), 4, True, False, False, 0) == 802
+
+
+def test_reference_arm_prints_the_contract_line(tmp_path):
+    """`bench.py --impl reference` (the oracle on the host cores, a bounded sample of the same outages) prints one JSON
+    line with the engine arm's metric and unit, its own cpu_baseline and an e2e object with no device copies."""
+    import json
+    import subprocess
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0", "--cpu-sample", "4"], capture_output=True, text=True, timeout=900,
+                         cwd=str(tmp_path))
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == "solves/s"
+    assert d["value"] > 0 and d["higher_is_better"] is True and d["steps"] == 1
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"] == {"value": d["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
