@@ -1,5 +1,6 @@
 // JNI layer of the engine: the native methods of the reference's Java facades for the batched AC Newton-Raphson path
-// (StructureNative, BatchSolveNative, NewtonSettingsNative, ReactiveLimitsNative, DriverNative, BatchReadbackNative),
+// (StructureNative, BatchSolveNative, NewtonSettingsNative, ReactiveLimitsNative, DistributedSlackNative, DriverNative,
+// BatchReadbackNative),
 // with the reference's symbol names and argument lists (native/cuda/jni/*_jni.cu), forwarded to the C ABI of
 // include/olfgpu_b200.h.  Built as lib/libolfgpu.so, the name the Java side loads (GpuNativeLoader.java:32).
 //
