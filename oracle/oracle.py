@@ -336,6 +336,7 @@ def ref_lu_lib():
         R.olfref_lu_plan.argtypes = [ctypes.c_int, _ip, _ip, _ip, _ip, ctypes.c_char_p]
         R.olfref_lu_free.argtypes = [ctypes.c_void_p]
         R.olfref_lu_solve.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
+        R.olfref_lu_solve_transposed.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
         _ref_lu = R
     return _ref_lu
 
@@ -366,6 +367,15 @@ class RefLu:
         trouble = ref_lu_lib().olfref_lu_solve(self.h, _ptr(vals), _ptr(b), _ptr(x))
         if trouble < 0:
             raise RuntimeError("reference LU: solve failed")
+        return x, trouble
+
+    def solve_transposed(self, vals, b):
+        """(x, trouble) with A^T x = b on the same factors: the reference's transposed solve."""
+        x = np.zeros(self.n)
+        vals, b = _arr(vals, np.float64), _arr(b, np.float64)
+        trouble = ref_lu_lib().olfref_lu_solve_transposed(self.h, _ptr(vals), _ptr(b), _ptr(x))
+        if trouble < 0:
+            raise RuntimeError("reference LU: transposed solve failed")
         return x, trouble
 
     def __del__(self):

@@ -18,6 +18,7 @@ namespace {
 struct RefLu {
     int n = 0;
     ScalarLuPlan plan;
+    ScalarLuColumns columns;   // the factors' columns the transposed solve reads (buildScalarLuColumns)
 };
 
 void setError(char* err, const char* what) {
@@ -38,6 +39,7 @@ extern "C" void* olfref_lu_plan(int n, const int* rowPtr, const int* colIdx, int
         h->n = n;
         const std::vector<int> md = minimumDegreeOrder(n, rowPtr, colIdx);
         h->plan = buildScalarLuPlan(n, rowPtr, colIdx, md.data(), md.data());
+        h->columns = buildScalarLuColumns(h->plan);
         if (nnzLuOut) *nnzLuOut = h->plan.nnzLu;
         if (levelsOut) *levelsOut = h->plan.factorSteps();
         return h;
@@ -60,6 +62,24 @@ extern "C" int olfref_lu_solve(void* handle, const double* vals, const double* b
         const std::vector<double> lu = factorFast(h.plan, a, trouble);
         const std::vector<double> rhs(b, b + h.n);
         const std::vector<double> z = solveFast(h.plan, lu, rhs);
+        std::memcpy(x, z.data(), sizeof(double) * static_cast<size_t>(h.n));
+        return trouble;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// x with A^T x = b on the same one-lane factors: the reference's transposed solve (solveFastTransposed,
+// native/host/lu_transposed_check.cpp:145-173, over the row bodies of lu/transposed_solve.cuh).  Returns the
+// factorization's trouble count, or -1 on an error.
+extern "C" int olfref_lu_solve_transposed(void* handle, const double* vals, const double* b, double* x) {
+    try {
+        const RefLu& h = *static_cast<const RefLu*>(handle);
+        const std::vector<double> a(vals, vals + h.plan.nnzA);
+        int trouble = 0;
+        const std::vector<double> lu = factorFast(h.plan, a, trouble);
+        const std::vector<double> rhs(b, b + h.n);
+        const std::vector<double> z = solveFastTransposed(h.plan, h.columns, lu, rhs);
         std::memcpy(x, z.data(), sizeof(double) * static_cast<size_t>(h.n));
         return trouble;
     } catch (const std::exception&) {

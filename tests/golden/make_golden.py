@@ -12,8 +12,8 @@
                          headers, its row map / pattern / scatter map, and its host LU (the fast engine's plan on its
                          minimum-degree order with the one-lane factorization and solve of
                          native/host/lu_transposed_check.cpp, compiled into oracle/_ref/libolfreflu.so), under the
-                         Newton rules of newton_iteration.cu:276-397; plus linear systems J x = b at perturbed states
-                         solved by that LU.
+                         Newton rules of newton_iteration.cu:276-397; plus linear systems J x = b and J^T x = b at
+                         perturbed states solved by that LU (its transposed solve: lu/transposed_solve.cuh's row bodies).
 
 Usage:  python tests/golden/make_golden.py [/root/reference]
 """
@@ -135,7 +135,7 @@ def newton_fixtures():
             lambda x, k=k: O.ref_component_fill(p, rs, x, p.target, p.base_row_mode, dis[k]),
             lambda v, b: lu.solve(v, b)[0], x0[k]) for k in range(dis.shape[0])])
         rng = np.random.default_rng(7)
-        lin_vals, lin_b, lin_x, lin_trouble = [], [], [], []
+        lin_vals, lin_b, lin_x, lin_xt, lin_trouble = [], [], [], [], []
         for _ in range(3):
             x = p.x_base.copy()
             x[0::2] += rng.uniform(-0.02, 0.02, p.n_bus)
@@ -143,12 +143,14 @@ def newton_fixtures():
             vals, _F = O.ref_component_fill(p, rs, x, p.target, p.base_row_mode)
             b = rng.standard_normal(p.n)
             xr, trouble = lu.solve(vals, b)
-            lin_vals.append(vals), lin_b.append(b), lin_x.append(xr), lin_trouble.append(trouble)
+            xt, _ = lu.solve_transposed(vals, b)
+            lin_vals.append(vals), lin_b.append(b), lin_x.append(xr), lin_xt.append(xt), lin_trouble.append(trouble)
         np.savez_compressed(os.path.join(HERE, f"newton_{name}.npz"), n=p.n, cb_params=p.cb_params, cb_idx=p.cb_idx,
                             ob_params=p.ob_params, ob_idx=p.ob_idx, sh_params=p.sh_params, sh_idx=p.sh_idx,
                             identity_rows=p.identity_rows, target=p.target, base_row_mode=p.base_row_mode,
                             row_ptr=rs["row_ptr"], col_idx=rs["col_idx"], x0=x0, disabled=dis, ref_rows=rows,
                             lin_vals=np.array(lin_vals), lin_b=np.array(lin_b), lin_x=np.array(lin_x),
+                            lin_xt=np.array(lin_xt),
                             lin_trouble=np.array(lin_trouble), ref_nnz_lu=lu.nnz_lu, ref_levels=lu.levels)
 
 

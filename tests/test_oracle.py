@@ -120,13 +120,17 @@ def test_oracle_newton_matches_reference_components(oracle_mod, name):
 
 @pytest.mark.parametrize("name", ["grid118", "grid300"])
 def test_oracle_linear_solve_matches_reference_host_lu(oracle_mod, name):
-    """Jacobians at perturbed states solved by the reference's host LU (newton_<grid>.npz) against the oracle's."""
+    """Jacobians at perturbed states solved by the reference's host LU (newton_<grid>.npz), J x = b and J^T x = b,
+    against the oracle's."""
     d = np.load(os.path.join(GOLD, f"newton_{name}.npz"))
     st = oracle_mod.Structure(_PN(d))
     assert not d["lin_trouble"].any(), "the reference's fast engine trusts these systems"
-    for vals, b, xr in zip(d["lin_vals"], d["lin_b"], d["lin_x"]):
+    for vals, b, xr, xt in zip(d["lin_vals"], d["lin_b"], d["lin_x"], d["lin_xt"]):
         x = st.linear_solve(vals, b)
         assert np.max(np.abs(x - xr)) / np.max(np.abs(xr)) <= LU_REL_TOL
+        # the transposed solve (lu/transposed_solve.cuh on the same factors) against the oracle's on the transpose
+        y = st.linear_solve_transposed(vals, b)
+        assert np.max(np.abs(y - xt)) / np.max(np.abs(xt)) <= LU_REL_TOL
 
 
 def test_reference_components_live_grid2000(oracle_mod):
@@ -145,6 +149,11 @@ def test_reference_components_live_grid2000(oracle_mod):
     vo, Fo = st.fill(p.x_base, p.target, p.base_row_mode, dis[0])
     vr, Fr = oracle_mod.ref_component_fill(p, rs, p.x_base, p.target, p.base_row_mode, dis[0])
     assert np.array_equal(vo, vr) and np.array_equal(Fo, Fr)
+    b = np.random.default_rng(2000).standard_normal(p.n)
+    for solve, mine in ((lu.solve, st.linear_solve), (lu.solve_transposed, st.linear_solve_transposed)):
+        xr, trouble = solve(vo, b)
+        assert trouble == 0
+        assert np.max(np.abs(mine(vo, b) - xr)) / np.max(np.abs(xr)) <= LU_REL_TOL
     out = st.solve_batch(p.x_base, dis)
     for k in range(dis.shape[0]):
         r = oracle_mod.newton_with(
