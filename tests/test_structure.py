@@ -161,3 +161,35 @@ def test_block_plan_is_race_free(engine_lib, name, plan):
     assert moved[0] > 0 and "level" in moved[1]
     assert dropped[0] > 0 and "update list" in dropped[1]
     assert swapped[0] > 0 and "forward" in swapped[1]
+
+
+def test_tiny_and_empty_networks(engine_lib):
+    """Edge inputs of the structure entry point are errors or sound plans, never crashes: an empty system, a network
+    with no elements and a bus with only a shunt (a P row with no angle column: no diagonal pairing, the row map's rule)
+    are refused with the reason; the smallest meshed case, two buses and one branch, plans under every variant and
+    passes the plan check."""
+    from olfgpu import native
+
+    class _Net:
+        def __init__(self, n, cb=(), sh=()):
+            self.n = n
+            self.cb_params = np.array([c[0] for c in cb], float).reshape(-1, 8)
+            self.cb_idx = np.array([c[1] for c in cb], np.int32).reshape(-1, 12)
+            self.ob_params, self.ob_idx = np.zeros((0, 7)), np.zeros((0, 6), np.int32)
+            self.sh_params = np.array([s[0] for s in sh], float).reshape(-1, 2)
+            self.sh_idx = np.array([s[1] for s in sh], np.int32).reshape(-1, 5)
+            self.identity_rows = np.zeros(0, np.int32)
+            self.n_cb, self.n_ob, self.n_sh = len(self.cb_idx), 0, len(self.sh_idx)
+            self.n_elements = self.n_cb + self.n_sh
+
+    with pytest.raises(native.NativeError, match="empty system"):
+        native.Structure(_Net(0))
+    with pytest.raises(native.NativeError, match="no diagonal pairing"):
+        native.Structure(_Net(2))
+    with pytest.raises(native.NativeError, match="no diagonal pairing"):
+        native.Structure(_Net(2, sh=[([0.0, 0.1], [0, 1, 1, -1, -1])]))
+    branch = ([10.0, 0.0, 0.0, 0.01, 0.01, 1.4, 1.0, 0.0], [0, 1, 2, 3, 0, 1, 2, 3, -1, -1, -1, -1])
+    for plan in (0, native.PLAN_DEFERRED_L, native.PLAN_DEFAULT):
+        s = native.Structure(_Net(4, cb=[branch]), ordering=plan)
+        assert (s.n, s.nnz, s.n_lu_blocks) == (4, 16, 4)
+        assert s.check_plan() == (0, "")
