@@ -208,8 +208,8 @@ int olfgpu_read_reactive_limits_state(int64_t context, int nSlots, const int* sl
 int olfgpu_set_outer_loops(int64_t context, int distributedSlack, int reactiveLimits);
 
 /* A context's sizes and counters: n, elements, bank size, scenarios the next full solve installs, batched Newton
- * iterations of the last solve (BatchReadbackNative.readBatchNewtonLoopIterations), full solves run
- * (BatchReadbackNative.readBatchSolveCount).  Any pointer may be null. */
+ * iterations of the last solve (BatchReadbackNative.readBatchNewtonLoopIterations, batch_readback_jni.cu:103-107), full
+ * solves run (BatchReadbackNative.readBatchSolveCount, batch_readback_jni.cu:112-116).  Any pointer may be null. */
 int olfgpu_context_info(int64_t context, int* n, int* nElements, int* nScenarios, int* installed,
                         int* batchedIterations, int64_t* solveCount);
 
@@ -238,7 +238,8 @@ int olfgpu_set_linear_solver_settings(int64_t context, int precision, int refine
  * flagged it (flagged [nScenarios], may be null) and their count.
  */
 int olfgpu_set_mixed_precision_controls(int64_t context, double refineBelow, double growthLimit);
-/* Mixed-precision policy (level and cooperative schedules): 0 (default) refines, as above; 1 runs an iteration in which
+/* Mixed-precision policy (no counterpart in the reference, whose LU is FP64 only; level and cooperative schedules):
+ * 0 (default) refines, as above; 1 runs an iteration in which
  * some factorizing scenario's max |F| is below refineBelow in FP64 for all its scenarios (factorization and solves),
  * and the other iterations in FP32 without refinement, so the last steps follow the FP64 trajectory at the cost of an
  * FP64 factorization instead of refinement solves.  olfgpu_last_fp64_iterations reads how many iterations of the last
@@ -351,8 +352,9 @@ int olfgpu_set_refinement_bound(int64_t context, double correctionBound);
 int olfgpu_set_fp64_restart(int64_t context, int enable);
 
 /*
- * Statistics of the context's last solve: device milliseconds of its Newton iterations (CUDA events on the context's
- * stream), the batched iterations run, and per scenario the Newton iterations summed over all its solves
+ * Statistics of the context's last solve (no counterpart in the reference's API; its OLF_GPU_PHASE_TIME trace prints
+ * similar counters, batch_solve_jni.cu:338-391): device milliseconds of its Newton iterations (CUDA events on the
+ * context's stream), the batched iterations run, and per scenario the Newton iterations summed over all its solves
  * (totalIterations [nScenarios], may be null).
  */
 int olfgpu_last_solve_stats(int64_t context, float* deviceMs, int* batchedIterations, int* totalIterations);
@@ -385,7 +387,8 @@ int olfgpu_set_device_start(int64_t context, const double* x0FullDevice);
  * (may be null), and the count of non-zero entries.
  */
 int olfgpu_set_fallback_start(int64_t context, int enable);
-/* Fallback mode: a scenario that converged from its own x0Full row with max |F| above polishRatio * tol (default
+/* Fallback mode (no counterpart in the reference): a scenario that converged from its own x0Full row with max |F|
+ * above polishRatio * tol (default
  * 1e-2; 0 switches it off) takes one more Newton step.  A state that met the tolerance may lie anywhere in its ball
  * (on a 9,241-bus grid up to 1.5e-8 from the solution at max |F| just under 1e-8), so a scenario that converged from
  * another start than the reference's base start is brought next to the solution, where the base-start trajectory's
@@ -510,7 +513,7 @@ int olfgpu_gnn_mse(int M, int ldo, const float* out, const float* target, float*
 int olfgpu_gnn_copy_cols(int M, int ncols, const float* src, int lds, int srcCol0, float* dst, int ldd, int dstCol0,
                          int accumulate, void* stream);
 /*
- * Learned start states on the device: x0 [nScenarios][2 nb] (device) from the network's output pred
+ * Learned start states on the device (no counterpart in the reference): x0 [nScenarios][2 nb] (device) from the network's output pred
  * [nScenarios * nb][ldPred] (columns 0, 1: normalised dVm, dVa), de-normalised by stdVm / stdVa and added to the base
  * state xBase [2 nb]; rows flagged in identity [2 nb] take target [2 nb].  All pointers are device memory.
  */
@@ -519,7 +522,8 @@ int olfgpu_gnn_compose_start(int nScenarios, int nb, const float* pred, int ldPr
                              void* stream);
 
 /*
- * Learned-start inference restricted to the buses an outage can reach: a message-passing layer only moves
+ * Learned-start inference restricted to the buses an outage can reach (no counterpart in the reference): a
+ * message-passing layer only moves
  * information one hop, so after L layers a sample differs from the outage-free sample only within L hops of its
  * outaged branch.  The compact rows (sample rowSample[r], bus rowNode[r]) hold those buses; rowOf [nSamples * nb]
  * maps (sample, bus) to its row or -1, and a neighbour outside the rows reads the outage-free sample's PQbase row

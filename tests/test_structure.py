@@ -9,6 +9,19 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLD = os.path.join(ROOT, "tests", "golden")
 
 
+def test_every_declaration_names_its_reference_interface():
+    """Each entry point of include/olfgpu_b200.h is documented with the reference interface it replaces (a file:line
+    citation) or says that it has no counterpart in the reference."""
+    header = open(os.path.join(ROOT, "include", "olfgpu_b200.h")).read()
+    last, missing = "", []
+    for m in re.finditer(r"((?:/\*.*?\*/\s*)?)((?:const char\*|int)\s+(olfgpu_\w+)\s*\([^;]*\);)", header, re.S):
+        if m.group(1).strip():
+            last = m.group(1)
+        if not (re.search(r"\w+\.(cu|cuh|java|h|cpp):\d+", last) or "no counterpart" in last.lower()):
+            missing.append(m.group(3))
+    assert not missing, missing
+
+
 def test_library_exports_every_declared_symbol(engine_lib):
     header = open(os.path.join(ROOT, "include", "olfgpu_b200.h")).read()
     names = set(re.findall(r"\b(olfgpu_\w+)\s*\(", header))
