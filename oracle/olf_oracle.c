@@ -163,6 +163,8 @@ typedef struct {
     char error[256];
 } oracle_structure;
 
+/* csr_pattern.cu:85-160 (buildRowMap's pairing): equation row `row` takes variable column `col` as its diagonal,
+ * each column claimed once. */
 static int pair_rc(int *rm, int row, int col, char *err)
 {
     if (row < 0 || col < 0) return 0;
@@ -238,6 +240,8 @@ static int cmp_pair(const void *a, const void *b)
     return x < y ? -1 : (x > y ? 1 : 0);
 }
 
+/* The CSR slot of (row, col), -1 when absent: the lookup behind buildDest and diagPos (structure_build.cuh:51-66,
+ * shared_structure.cu:322-324). */
 static int csr_at(const oracle_structure *s, int row, int col)
 {
     int lo = s->row_ptr[row], hi = s->row_ptr[row + 1];
@@ -261,6 +265,9 @@ void oracle_structure_free(oracle_structure *s)
 }
 
 /* Builds the structure; returns NULL and writes err (>= 256 bytes) on failure. */
+/* Builds the structure (row map csr_pattern.cu:75-240, superset pattern shared_structure.cu:111-221 with
+ * collectPattern structure_build.cuh:32-42, destinations buildDest structure_build.cuh:51-66); returns NULL and writes
+ * err (>= 256 bytes) on failure. */
 oracle_structure *oracle_structure_build(int n, int ncb, const double *cb_par, const int *cb_ix, int nob,
                                          const double *ob_par, const int *ob_ix, int nsh, const double *sh_par,
                                          const int *sh_ix, int nid, const int *id_rows, char *err)
@@ -365,7 +372,8 @@ void oracle_structure_export(const oracle_structure *s, int *row_map, int *row_p
 }
 
 /* ---------------------------------------------------------------------------------------------------------------
- * Fill: J values (CSR) and F for one scenario, element order then output order (deterministic).
+ * Fill (fill_launch.cu:82-126, the family fills branch_fill.cu:121-191): J values (CSR) and F for one scenario, element
+ * order then output order (deterministic).
  * qbuf (optional, [n]): the closed-branch residual outputs on their rows, raw (fill_launch.cu qbuf channel).
  * ------------------------------------------------------------------------------------------------------------- */
 static void fill(const oracle_structure *s, const double *x, const double *target, const int *mode,
@@ -427,6 +435,8 @@ static void fill(const oracle_structure *s, const double *x, const double *targe
 }
 
 /* One scenario's J values and F (parity checks of the engine's fill). */
+/* One scenario's J values and F (parity checks of the engine's fill): fill_launch.cu:82-126 with the outaged
+ * elements skipped (branch_fill.cu:133). */
 void oracle_fill(const oracle_structure *s, const double *x, const double *target, const int *mode,
                  const unsigned char *disabled, double *vals, double *F)
 {
@@ -444,6 +454,8 @@ static void iv_push(ivec *a, int x)
     a->v[a->len++] = x;
 }
 
+/* The oracle's own fill-reducing order for its own LU (not a restatement: the reference orders with
+ * minimum_degree.cu, which the tests reach through oracle/ref), so its solves are independent of the engine's plan. */
 static void min_degree(int n, const int *rp, const int *ci, int *perm)
 {
     ivec *adj = (ivec *)calloc((size_t)n, sizeof(ivec));
@@ -522,7 +534,8 @@ static void min_degree(int n, const int *rp, const int *ci, int *perm)
 }
 
 /* ---------------------------------------------------------------------------------------------------------------
- * Gilbert-Peierls left-looking LU with partial pivoting (columns in a given order).
+ * Gilbert-Peierls left-looking LU with partial pivoting (columns in a given order): the oracle's own exact solver, not
+ * a restatement (the reference's LU is reached through oracle/ref and pins this one in the tests).
  * A is given by rows (CSR); it is transposed to columns first.
  * ------------------------------------------------------------------------------------------------------------- */
 typedef struct {
@@ -1034,6 +1047,7 @@ int oracle_solve_batch_final(oracle_solver *o, int ns, const double *x0, int x0_
     return 0;
 }
 
+/* The batched solve with the distributed-slack loop and no final-equation outputs (oracle_solve_batch_final). */
 int oracle_solve_batch_ds(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
                           const int *mode_base, const unsigned char *disabled, int n_elements, int max_iter, double tol,
                           const oracle_rl *rl, double rl_tol, int max_outer, int max_switch, int threads,
@@ -1043,6 +1057,7 @@ int oracle_solve_batch_ds(oracle_solver *o, int ns, const double *x0, int x0_str
                                     rl, rl_tol, max_outer, max_switch, threads, opts, ds, out, NULL, NULL);
 }
 
+/* The batched solve without distributed slack: outer_loop_driver.cu:80-460 over newton_iteration.cu:276-397. */
 int oracle_solve_batch_ex(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
                           const int *mode_base, const unsigned char *disabled, int n_elements, int max_iter, double tol,
                           const oracle_rl *rl, double rl_tol, int max_outer, int max_switch, int threads,
@@ -1052,6 +1067,7 @@ int oracle_solve_batch_ex(oracle_solver *o, int ns, const double *x0, int x0_str
                                  rl, rl_tol, max_outer, max_switch, threads, opts, NULL, out);
 }
 
+/* The batched solve with the default options (no 2-norm test, no step scaling, no realistic check). */
 int oracle_solve_batch(oracle_solver *o, int ns, const double *x0, int x0_stride, const double *target_base,
                        const int *mode_base, const unsigned char *disabled, int n_elements, int max_iter, double tol,
                        const oracle_rl *rl, double rl_tol, int max_outer, int max_switch, int threads, double *out)
@@ -1060,7 +1076,8 @@ int oracle_solve_batch(oracle_solver *o, int ns, const double *x0, int x0_stride
                                  rl_tol, max_outer, max_switch, threads, NULL, out);
 }
 
-/* Solve one linear system J z = b with the oracle LU (tests of the engine's batched LU). Returns 0 or -1. */
+/* Solve one linear system J z = b with the oracle LU (tests of the engine's batched LU; the reference's counterpart is
+ * its batched LU, lu/batched_lu.cu:66-149 and scalar_lu.cu:318-334). Returns 0 or -1. */
 int oracle_linear_solve(oracle_solver *o, const double *vals, const double *b, double *z)
 {
     const oracle_structure *s = o->s;
@@ -1075,7 +1092,7 @@ int oracle_linear_solve(oracle_solver *o, const double *vals, const double *b, d
 }
 
 /* Solve the transposed system J^T z = b with the oracle LU on the explicit transpose (tests of the engine's transposed
- * solve on its own factors, lu/transposed_solve.cuh).  Returns 0 or -1 (singular). */
+ * solve on its own factors, the reference's lu/transposed_solve.cuh:39-159).  Returns 0 or -1 (singular). */
 int oracle_linear_solve_transposed(oracle_solver *o, const double *vals, const double *b, double *z)
 {
     const oracle_structure *s = o->s;
